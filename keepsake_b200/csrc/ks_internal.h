@@ -1,0 +1,64 @@
+// Internal host-side helpers shared by the C-ABI translation units.
+#pragma once
+#include "../../include/ks_b200.h"
+
+#include <cuda_runtime.h>
+#include <string>
+
+struct ks_context
+{
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string last_error;
+    int sm_count = 148;
+};
+
+namespace ksb
+{
+
+// Records a failure on the context and returns its status.
+inline ks_status fail(ks_context *ctx, ks_status s, const std::string &msg)
+{
+    if (ctx)
+        ctx->last_error = msg;
+    return s;
+}
+
+inline ks_status cuda_fail(ks_context *ctx, cudaError_t e, const char *what)
+{
+    return fail(ctx, e == cudaErrorMemoryAllocation ? KS_ERR_OUT_OF_MEMORY : KS_ERR_CUDA,
+                std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Device buffer owned by the caller of these helpers; freed explicitly.
+template <typename T>
+struct DevBuf
+{
+    T *ptr = nullptr;
+    size_t count = 0;
+    cudaError_t alloc(size_t n)
+    {
+        release();
+        count = n;
+        if (n == 0)
+            return cudaSuccess;
+        return cudaMalloc((void **)&ptr, n * sizeof(T));
+    }
+    void release()
+    {
+        if (ptr)
+            cudaFree(ptr);
+        ptr = nullptr;
+        count = 0;
+    }
+    size_t bytes() const { return count * sizeof(T); }
+};
+
+} // namespace ksb
+
+#define KS_CUDA_TRY(ctx, expr)                                                                                         \
+    do {                                                                                                               \
+        cudaError_t _e = (expr);                                                                                       \
+        if (_e != cudaSuccess)                                                                                         \
+            return ksb::cuda_fail((ctx), _e, #expr);                                                                   \
+    } while (0)

@@ -1,0 +1,203 @@
+// Owen-scrambled Sobol (0,2) sampler with permuted Morton indices, per pixel and per sample.
+//
+// Follows the reference CPU sampler `OwenScrambledSobol02Morton` + `PTRenderSampler`
+// (sobol.h:131-248) integer for integer, including its quirks:
+//   * the Morton index is formed in 32 bits before widening (sobol.h:145),
+//   * `0x55555555u * dimension` is a 32-bit product (sobol.h:209,218),
+//   * next()/next2d() permute with the dimension *before* the increment and hash the dimension
+//     *after* it (sobol.h:148-166).
+// Only generator matrices 0 and 1 are ever read by this sampler (sobol.h:44, :160-166).  Their
+// closed forms (checked against the reference table sobol.cpp:154+ by the golden fixture):
+//   dim 0 column k = 0x80000000 >> k for k < 32, else 0
+//   dim 1 column k = P[k mod 32], P[0] = 0x80000000, P[k] = P[k-1] ^ (P[k-1] >> 1).
+#pragma once
+#include "ks_math.cuh"
+
+namespace ksb
+{
+
+KS_HD uint64_t mix_bits64(uint64_t v)
+{
+    // hash.h:206-214
+    v ^= (v >> 31);
+    v *= 0x7fb5d329728ea185ull;
+    v ^= (v >> 27);
+    v *= 0x81dadef4bc2dd44dull;
+    v ^= (v >> 33);
+    return v;
+}
+
+// MurmurHash64A of exactly 8 bytes (two little-endian int32s), seed 0: hash(int, int) in hash.h:243-252.
+KS_HD uint64_t murmur64a_2x32(uint32_t lo, uint32_t hi)
+{
+    const uint64_t m = 0xc6a4a7935bd1e995ull;
+    const int r = 47;
+    uint64_t h = 0ull ^ (8ull * m);
+    uint64_t k = (uint64_t)lo | ((uint64_t)hi << 32);
+    k *= m;
+    k ^= k >> r;
+    k *= m;
+    h ^= k;
+    h *= m;
+    h ^= h >> r;
+    h *= m;
+    h ^= h >> r;
+    return h;
+}
+
+KS_HD uint32_t reverse_bits32(uint32_t v)
+{
+#ifdef __CUDA_ARCH__
+    return __brev(v);
+#else
+    v = (v << 16u) | (v >> 16u);
+    v = ((v & 0x55555555u) << 1u) | ((v & 0xAAAAAAAAu) >> 1u);
+    v = ((v & 0x33333333u) << 2u) | ((v & 0xCCCCCCCCu) >> 2u);
+    v = ((v & 0x0F0F0F0Fu) << 4u) | ((v & 0xF0F0F0F0u) >> 4u);
+    v = ((v & 0x00FF00FFu) << 8u) | ((v & 0xFF00FF00u) >> 8u);
+    return v;
+#endif
+}
+
+KS_HD uint32_t owen_scramble(uint32_t v, uint32_t seed)
+{
+    // FastOwenScrambler (sobol.h:17-33)
+    v = reverse_bits32(v);
+    v ^= v * 0x3d20adeau;
+    v += seed;
+    v *= (seed >> 16) | 1u;
+    v ^= v * 0x05526c56u;
+    v ^= v * 0x53a22864u;
+    return reverse_bits32(v);
+}
+
+KS_HD uint32_t sobol_dim1_column(int k)
+{
+    uint32_t p = 0x80000000u;
+    for (int i = 0; i < (k & 31); ++i)
+        p ^= p >> 1;
+    return p;
+}
+
+// sobol_sample(a, dim, FastOwenScrambler(seed)) for dim in {0, 1} (sobol.h:35-49)
+KS_HD float sobol_sample_01(uint64_t a, int dim, uint32_t seed)
+{
+    uint32_t v = 0;
+    if (dim == 0) {
+        v = reverse_bits32((uint32_t)a);
+    } else {
+        // columns repeat with period 32; fold the index bits accordingly
+        uint32_t folded = (uint32_t)a ^ (uint32_t)(a >> 32);
+        // P[k] for the set bits of the folded index: P is the Pascal triangle mod 2 on reversed bits
+        uint32_t p = 0x80000000u;
+        for (int k = 0; k < 32; ++k) {
+            if (folded & (1u << k))
+                v ^= p;
+            p ^= p >> 1;
+        }
+    }
+    v = owen_scramble(v, seed);
+    float f = (float)v * 0x1p-32f;
+    return f < kOneMinusEps ? f : kOneMinusEps;
+}
+
+KS_HD uint32_t part1by1(uint32_t x)
+{
+    x &= 0x0000ffffu;
+    x = (x ^ (x << 8)) & 0x00ff00ffu;
+    x = (x ^ (x << 4)) & 0x0f0f0f0fu;
+    x = (x ^ (x << 2)) & 0x33333333u;
+    x = (x ^ (x << 1)) & 0x55555555u;
+    return x;
+}
+
+// All 24 orderings of {0,1,2,3}, in the order the reference enumerates them (sobol.h:169-199).
+KS_HD int digit_permutation(int p, int digit)
+{
+    // packed: 2 bits per entry, entry 0 in the low bits
+    constexpr uint8_t tab[24] = {
+        0xE4, 0xB4, 0xD8, 0x78, 0x6C, 0x9C, 0xE1, 0xB1, 0xC9, 0x39, 0x2D, 0x8D,
+        0xC6, 0x36, 0xD2, 0x72, 0x4E, 0x1E, 0x27, 0x87, 0x1B, 0x4B, 0x63, 0x93,
+    };
+    return (tab[p] >> (2 * digit)) & 3;
+}
+
+struct SobolSampler
+{
+    uint64_t morton_index;
+    int dimension;
+    uint32_t seed;
+    int log2_spp;
+    int n_base4_digits;
+
+    // PTRenderSampler constructor + start_pixel(pixel, index, 0) (sobol.h:139-147, 237-241)
+    KS_HD static SobolSampler start(uint32_t px, uint32_t py, uint32_t sample_index, int log2_spp,
+                                    int n_base4_digits, uint32_t seed, int dim = 0)
+    {
+        SobolSampler s;
+        s.dimension = dim;
+        s.seed = seed;
+        s.log2_spp = log2_spp;
+        s.n_base4_digits = n_base4_digits;
+        uint32_t morton = (part1by1(py) << 1) + part1by1(px);
+        s.morton_index = (uint64_t)((morton << log2_spp) | sample_index);
+        return s;
+    }
+
+    KS_HD uint64_t sample_index() const
+    {
+        uint64_t out = 0;
+        const bool pow2 = (log2_spp & 1) != 0;
+        const int last_digit = pow2 ? 1 : 0;
+        const uint64_t dim_mix = (uint64_t)(0x55555555u * (uint32_t)dimension);
+        for (int i = n_base4_digits - 1; i >= last_digit; --i) {
+            int shift = 2 * i - (pow2 ? 1 : 0);
+            int digit = (int)((morton_index >> shift) & 3);
+            uint64_t higher = morton_index >> (shift + 2);
+            int p = (int)((mix_bits64(higher ^ dim_mix) >> 24) % 24);
+            digit = digit_permutation(p, digit);
+            out |= (uint64_t)digit << shift;
+        }
+        if (pow2) {
+            int digit = (int)(morton_index & 1);
+            out |= (uint64_t)(digit ^ (int)(mix_bits64((morton_index >> 1) ^ dim_mix) & 1));
+        }
+        return out;
+    }
+
+    KS_HD float next()
+    {
+        uint64_t a = sample_index();
+        ++dimension;
+        uint32_t h = (uint32_t)murmur64a_2x32((uint32_t)dimension, seed);
+        return sobol_sample_01(a, 0, h);
+    }
+
+    KS_HD void next2d(float &u0, float &u1)
+    {
+        uint64_t a = sample_index();
+        dimension += 2;
+        uint64_t bits = murmur64a_2x32((uint32_t)dimension, seed);
+        u0 = sobol_sample_01(a, 0, (uint32_t)bits);
+        u1 = sobol_sample_01(a, 1, (uint32_t)(bits >> 32));
+    }
+};
+
+// Host-side setup of the per-render constants (sobol.h:131-138).
+inline void sobol_setup(int spp, int full_w, int full_h, int &log2_spp, int &n_base4_digits)
+{
+    auto log2i = [](uint32_t v) { return 31 - __builtin_clz(v); };
+    log2_spp = log2i((uint32_t)spp);
+    int32_t m = full_w > full_h ? full_w : full_h;
+    int32_t v = m - 1;
+    v |= v >> 1;
+    v |= v >> 2;
+    v |= v >> 4;
+    v |= v >> 8;
+    v |= v >> 16;
+    int res = v + 1;
+    int log4 = (log2_spp + 1) / 2;
+    n_base4_digits = log2i((uint32_t)res) + log4;
+}
+
+} // namespace ksb

@@ -1,0 +1,122 @@
+// Test-only C wrapper around the reference's own SBVH (cuda/sbvh.cu, cuda/sbvh.cuh),
+// compiled unmodified from the reference tree by oracle/ref_sbvh/Makefile.
+//
+// This file is part of the parity oracle, never of the product.  It exposes:
+//   * the reference builder  ksc::SBVH::SBVH(option, vertices, indices)   (cuda/sbvh.cu:396-440)
+//   * the flattened node array and the ordered primitive list             (cuda/sbvh.cuh:18-28,90-93)
+//   * closest-hit and any-hit queries ksc::SBVH::intersect / intersectBool (cuda/sbvh.cu:512-603)
+// so that tests can pin the CUDA builder's topology and the CUDA traversal's hit IDs
+// against the reference itself.
+#include "sbvh.cuh"
+
+#include <cstdint>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+namespace
+{
+struct RefHandle
+{
+    std::vector<ksc::vec3> verts;
+    std::vector<uint32_t> idx;
+    ksc::SBVH bvh;
+};
+} // namespace
+
+extern "C" {
+
+int ksref_sbvh_build(const float *vertices, uint32_t n_vertices, const uint32_t *indices, uint32_t n_tris,
+                     uint32_t max_prims_in_node, uint32_t bucket_count, float trav_weight, float alpha,
+                     void **out_handle, uint32_t *out_n_nodes, uint32_t *out_n_prims)
+{
+    if (!vertices || !indices || !out_handle || n_tris == 0)
+        return 1;
+    auto *h = new RefHandle();
+    h->verts.resize(n_vertices);
+    for (uint32_t i = 0; i < n_vertices; ++i)
+        h->verts[i] = ksc::vec3(vertices[3 * i + 0], vertices[3 * i + 1], vertices[3 * i + 2]);
+    h->idx.assign(indices, indices + 3 * (size_t)n_tris);
+    ksc::SBVHBuildOption opt;
+    opt.maxPrimsInNode = max_prims_in_node;
+    opt.bucketCount = bucket_count;
+    opt.travWeight = trav_weight;
+    opt.alpha = alpha;
+    h->bvh = ksc::SBVH(opt, ksc::span<const ksc::vec3>(h->verts.data(), h->verts.size()),
+                       ksc::span<const uint32_t>(h->idx.data(), h->idx.size()));
+    *out_handle = h;
+    *out_n_nodes = (uint32_t)h->bvh.nodes.size;
+    *out_n_prims = (uint32_t)h->bvh.primitives.size;
+    return 0;
+}
+
+// node_bounds: 6 floats per node (min xyz, max xyz); axis/right/prim_offset: one uint32 per node;
+// prims: ordered primitive (triangle) indices.
+int ksref_sbvh_export(void *handle, float *node_bounds, uint32_t *node_axis, uint32_t *node_right,
+                      uint32_t *node_prim_offset, uint32_t *prims)
+{
+    auto *h = (RefHandle *)handle;
+    for (size_t i = 0; i < h->bvh.nodes.size; ++i) {
+        const ksc::SBVHNode &n = h->bvh.nodes[i];
+        node_bounds[6 * i + 0] = n.bound.min.x;
+        node_bounds[6 * i + 1] = n.bound.min.y;
+        node_bounds[6 * i + 2] = n.bound.min.z;
+        node_bounds[6 * i + 3] = n.bound.max.x;
+        node_bounds[6 * i + 4] = n.bound.max.y;
+        node_bounds[6 * i + 5] = n.bound.max.z;
+        node_axis[i] = n.splitAxis;
+        node_right[i] = n.rightChildOffset;
+        node_prim_offset[i] = n.primOffset;
+    }
+    for (size_t i = 0; i < h->bvh.primitives.size; ++i)
+        prims[i] = h->bvh.primitives[i].shapeIndex;
+    return 0;
+}
+
+// rays: 8 floats per ray (ox oy oz tmin dx dy dz tmax).  any_hit=0: closest hit, writes tri index
+// (~0u on miss), t and the three barycentric weights; any_hit=1: writes 1/0 in tri_idx.
+// culling: 0 back-face, 1 front-face, 2 none (ksc::SBVHCulling).
+int ksref_sbvh_intersect(void *handle, const float *rays, uint32_t n, int any_hit, int culling, uint32_t *tri_idx,
+                         float *t, float *bary, int n_threads)
+{
+    auto *h = (RefHandle *)handle;
+    ksc::SBVHIsectOption opt;
+    opt.culling = (ksc::SBVHCulling)culling;
+    auto work = [&](uint32_t begin, uint32_t end) {
+        for (uint32_t i = begin; i < end; ++i) {
+            const float *r = rays + 8 * (size_t)i;
+            ksc::Ray ray(ksc::vec3(r[0], r[1], r[2]), ksc::vec3(r[4], r[5], r[6]), r[3], r[7]);
+            if (any_hit) {
+                tri_idx[i] = h->bvh.intersectBool(ray, opt) ? 1u : 0u;
+            } else {
+                ksc::SBVHIsectRecord rec = h->bvh.intersect(ray, opt);
+                tri_idx[i] = rec.tri_idx;
+                if (t)
+                    t[i] = rec.thit;
+                if (bary) {
+                    bary[3 * i + 0] = rec.coord.x;
+                    bary[3 * i + 1] = rec.coord.y;
+                    bary[3 * i + 2] = rec.coord.z;
+                }
+            }
+        }
+    };
+    if (n_threads <= 1 || n < 4096) {
+        work(0, n);
+    } else {
+        std::vector<std::thread> pool;
+        uint32_t chunk = (n + n_threads - 1) / n_threads;
+        for (int k = 0; k < n_threads; ++k) {
+            uint32_t b = k * chunk, e = std::min(n, b + chunk);
+            if (b < e)
+                pool.emplace_back(work, b, e);
+        }
+        for (auto &th : pool)
+            th.join();
+    }
+    return 0;
+}
+
+void ksref_sbvh_destroy(void *handle) { delete (RefHandle *)handle; }
+
+} // extern "C"

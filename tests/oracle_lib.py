@@ -1,0 +1,105 @@
+"""ctypes binding of the ORACLE (oracle/liboracle.so, oracle/_ref/libksref_sbvh.so).
+
+Test infrastructure only: tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg load
+this; the product never does.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_SO = os.path.join(ROOT, "oracle", "liboracle.so")
+REF_SO = os.path.join(ROOT, "oracle", "_ref", "libksref_sbvh.so")
+
+_vp = ctypes.c_void_p
+_u32 = ctypes.c_uint32
+
+
+def P(a):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+class Oracle:
+    def __init__(self):
+        self.lib = ctypes.CDLL(ORACLE_SO)
+        L = self.lib
+        L.oracle_sobol_points.argtypes = [_u32] * 11 + [_vp]
+        L.oracle_sobol_points.restype = ctypes.c_int
+        L.oracle_sobol_matrices01.argtypes = [_vp]
+        L.oracle_sobol_matrices01.restype = None
+
+    def sobol_points(self, full_w, full_h, spp, seed, x0, y0, nx, ny, s0, ns, nd):
+        out = np.empty((ny, nx, ns, nd, 3), dtype=np.float32)
+        self.lib.oracle_sobol_points(full_w, full_h, spp, seed, x0, y0, nx, ny, s0, ns, nd, P(out))
+        return out
+
+    def sobol_matrices01(self):
+        out = np.empty(104, dtype=np.uint32)
+        self.lib.oracle_sobol_matrices01(P(out))
+        return out
+
+
+class RefSBVH:
+    """The reference's own SBVH builder + traversal (cuda/sbvh.cu), compiled host-side."""
+
+    def __init__(self):
+        self.lib = ctypes.CDLL(REF_SO)
+        L = self.lib
+        L.ksref_sbvh_build.argtypes = [_vp, _u32, _vp, _u32, _u32, _u32, ctypes.c_float, ctypes.c_float,
+                                       ctypes.POINTER(_vp), ctypes.POINTER(_u32), ctypes.POINTER(_u32)]
+        L.ksref_sbvh_export.argtypes = [_vp] * 6
+        L.ksref_sbvh_intersect.argtypes = [_vp, _vp, _u32, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, ctypes.c_int]
+        L.ksref_sbvh_destroy.argtypes = [_vp]
+
+    def build(self, verts, idx, max_prims=4, buckets=12, trav_weight=1.0, alpha=1e-5):
+        verts = np.ascontiguousarray(verts, dtype=np.float32).reshape(-1, 3)
+        idx = np.ascontiguousarray(idx, dtype=np.uint32).reshape(-1)
+        h, nn, npr = _vp(), _u32(), _u32()
+        st = self.lib.ksref_sbvh_build(P(verts), len(verts), P(idx), len(idx) // 3, max_prims, buckets,
+                                       trav_weight, alpha, ctypes.byref(h), ctypes.byref(nn), ctypes.byref(npr))
+        assert st == 0
+        n, m = nn.value, npr.value
+        bounds = np.empty((n, 6), np.float32)
+        axis = np.empty(n, np.uint32)
+        right = np.empty(n, np.uint32)
+        off = np.empty(n, np.uint32)
+        prims = np.empty(m, np.uint32)
+        self.lib.ksref_sbvh_export(h, P(bounds), P(axis), P(right), P(off), P(prims))
+        return RefTree(self, h, bounds, axis, right, off, prims)
+
+
+class RefTree:
+    def __init__(self, owner, h, bounds, axis, right, off, prims):
+        self.owner, self.h = owner, h
+        self.bounds, self.axis, self.right, self.prim_offset, self.prims = bounds, axis, right, off, prims
+
+    def intersect(self, rays, any_hit=False, culling=2, threads=8):
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+        n = len(rays)
+        tri = np.empty(n, np.uint32)
+        t = np.empty(n, np.float32)
+        bary = np.empty((n, 3), np.float32)
+        self.owner.lib.ksref_sbvh_intersect(self.h, P(rays), n, int(any_hit), culling, P(tri), P(t), P(bary),
+                                            threads)
+        return (tri.astype(bool), None, None) if any_hit else (tri, t, bary)
+
+    def __del__(self):
+        try:
+            self.owner.lib.ksref_sbvh_destroy(self.h)
+        except Exception:
+            pass
+
+
+_oracle = None
+
+
+def load():
+    global _oracle
+    if _oracle is None:
+        _oracle = Oracle()
+    return _oracle
+
+
+def ref_sbvh():
+    return RefSBVH()
