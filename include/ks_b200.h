@@ -49,6 +49,135 @@ ks_status ks_sobol_points(ks_context *ctx, uint32_t full_width, uint32_t full_he
                           uint32_t x0, uint32_t y0, uint32_t nx, uint32_t ny, uint32_t s0, uint32_t ns, uint32_t nd,
                           float *out);
 
+/* ---------------------------------------------------------------------------------------------
+ * Scene description (host arrays; ks_scene_create copies everything it needs to the device).
+ * One mesh = one reference `MeshGeometry` with one `Material` (scene.cpp:315-336 pairs
+ * subscene.geometries[geom_id] with subscene.materials[geom_id]).
+ * ------------------------------------------------------------------------------------------- */
+typedef struct ks_mesh_desc {
+    const float *vertices;       /* 3 floats per vertex */
+    uint32_t n_vertices;
+    const uint32_t *indices;     /* 3 per triangle */
+    uint32_t n_triangles;
+    const float *vertex_normals; /* optional, 3 per vertex; NULL = flat shading */
+    uint32_t material;           /* index into ks_scene_desc.materials */
+    int32_t twosided;            /* MeshData::twosided (geometry.h:84); reference default 1 */
+    int32_t use_smooth_normal;   /* MeshData::use_smooth_normal (geometry.h:85) */
+} ks_mesh_desc;
+
+/* PrincipledBSDF with constant shader fields (principled_bsdf.cpp:707-733) plus the
+ * Material::emission field (material.h:45), which the TOML task reads from an `emission` key. */
+typedef struct ks_material_desc {
+    float basecolor[3];
+    float roughness;
+    float metallic;
+    float ior;
+    float specular_r0_mul;
+    float specular_trans;
+    float diffuse_trans;
+    float diffuse_trans_fwd;
+    float emissive[3];
+    int32_t microfacet;   /* 0 = GGX, 1 = Beckmann */
+    int32_t has_emission; /* Material::emission != nullptr */
+    float emission[3];
+} ks_material_desc;
+
+/* SkyLight (light.h:34-58): ambient colour or a lat-long RGB map. */
+typedef struct ks_sky_desc {
+    int32_t kind;         /* 0 none, 1 ambient, 2 lat-long map */
+    float ambient[3];
+    const float *map_rgb; /* width*height*3 floats, row 0 = theta 0 (light.cpp:33-40) */
+    uint32_t width;
+    uint32_t height;
+    float to_world[16];   /* row-major 4x4 light-to-world */
+    int32_t transform_y_up;
+    float strength;
+} ks_sky_desc;
+
+typedef struct ks_scene_desc {
+    const ks_mesh_desc *meshes;
+    uint32_t n_meshes;
+    const ks_material_desc *materials;
+    uint32_t n_materials;
+    ks_sky_desc sky;
+} ks_scene_desc;
+
+/* SBVHBuildOption (cuda/sbvh.cuh:9-16); clamped like SBVH::build (cuda/sbvh.cu:411-414). */
+typedef struct ks_sbvh_options {
+    uint32_t max_prims_in_node; /* default 4, clamped to <= 8 */
+    uint32_t bucket_count;      /* default 12, clamped to <= 16 */
+    float trav_weight;          /* default 1, clamped to [0, 10] */
+    float alpha;                /* default 1e-5, clamped to [0, 1] */
+} ks_sbvh_options;
+
+typedef struct ks_scene ks_scene;
+
+/* Copies the scene to the device and builds the light tables (Scene::build_mesh_lights,
+ * scene.cpp:315; PowerLightSampler::build, light.cpp:636; SkyLight, light.cpp:19-49). */
+ks_status ks_scene_create(ks_context *ctx, const ks_scene_desc *desc, ks_scene **out);
+void ks_scene_destroy(ks_scene *scene);
+
+/* Parallel SBVH build on the GPU over all triangles of the scene, concatenated in mesh order.
+ * Replaces ksc::SBVH::build (cuda/sbvh.cu:404-440) and Embree's rtcCommitScene (scene.cpp:60).
+ * opts may be NULL (defaults).  build_ms (optional) receives the device time of the build. */
+ks_status ks_scene_build_bvh(ks_scene *scene, const ks_sbvh_options *opts, float *build_ms);
+
+/* Counts of the flattened SBVH (cuda/sbvh.cuh:90-93): nodes and ordered primitive references. */
+ks_status ks_sbvh_counts(const ks_scene *scene, uint32_t *n_nodes, uint32_t *n_prims);
+
+/* Copies the flattened SBVH to host arrays in the reference's layout (SBVHNode, sbvh.cuh:18-28):
+ * bounds 6 floats/node (min xyz, max xyz), split axis, rightChildOffset (0 = leaf), primOffset,
+ * and the ordered primitive list (global triangle index per reference). */
+ks_status ks_sbvh_export(const ks_scene *scene, float *node_bounds, uint32_t *node_axis, uint32_t *node_right,
+                         uint32_t *node_prim_offset, uint32_t *prims);
+
+/* Ray-query parity hook: SBVH::intersect / intersectBool (cuda/sbvh.cu:512-603) over a batch of
+ * host rays, 8 floats each (ox oy oz tmin dx dy dz tmax).  any_hit = 0: tri_idx = global triangle
+ * index or 0xFFFFFFFF, t and bary (3 per ray) filled; any_hit = 1: tri_idx = 1 occluded / 0 not.
+ * culling: 0 back faces, 1 front faces, 2 none (SBVHCulling, sbvh.cuh:30-35). */
+ks_status ks_trace_rays(ks_scene *scene, const float *rays, uint32_t n, int any_hit, int culling, uint32_t *tri_idx,
+                        float *t, float *bary);
+
+/* ---------------------------------------------------------------------------------------------
+ * Camera.  The render consumes the matrices of a reference `Camera` (camera.cpp:85-94):
+ * camera_to_world, proj_to_camera = inverse(rev_inf_projection(vfov, aspect, 0.1)) and
+ * proj_to_world = inverse(rev_inf_projection * inverse(camera_to_world)); row-major 4x4.
+ * ------------------------------------------------------------------------------------------- */
+typedef struct ks_camera_desc {
+    float camera_to_world[16];
+    float proj_to_camera[16];
+    float proj_to_world[16];
+} ks_camera_desc;
+
+/* Perspective camera from a camera-to-world matrix (row-major 4x4), vertical field of view in
+ * radians and aspect ratio: Camera::Camera(to_world, vfov, aspect) (camera.cpp:85-92). */
+ks_status ks_camera_perspective(const float camera_to_world[16], float vfov, float aspect, ks_camera_desc *out);
+
+/* ---------------------------------------------------------------------------------------------
+ * Procedural scenes: seeded synthetic inputs standing in for mesh-asset loading
+ * (mesh_asset.cpp).  kind: "box_room" or "icosphere" (options apply to "icosphere").
+ * ------------------------------------------------------------------------------------------- */
+typedef struct ks_procedural_options {
+    int32_t level;        /* icosphere subdivision level (8 -> 1,310,720 triangles) */
+    float roughness_min;  /* per-patch roughness U[min, max] */
+    float roughness_max;
+    int32_t occluder;     /* 1: slab between the sphere and the sun lobe */
+    uint32_t sky_width;   /* lat-long sky resolution */
+    uint32_t sky_height;
+    uint32_t width;       /* render resolution (sets the camera aspect) */
+    uint32_t height;
+} ks_procedural_options;
+
+typedef struct ks_generated ks_generated;
+
+ks_status ks_procedural_scene(const char *kind, uint64_t seed, const ks_procedural_options *opts,
+                              ks_generated **out);
+/* The generated scene description; valid until ks_generated_destroy. */
+const ks_scene_desc *ks_generated_scene_desc(const ks_generated *g);
+/* Camera-to-world (row-major 4x4), vertical fov (radians) and aspect of the generated view. */
+ks_status ks_generated_camera(const ks_generated *g, float camera_to_world[16], float *vfov, float *aspect);
+void ks_generated_destroy(ks_generated *g);
+
 #ifdef __cplusplus
 }
 #endif

@@ -97,3 +97,199 @@ class Context:
         st = lib.ks_sobol_points(self.handle, full_w, full_h, spp, seed, x0, y0, nx, ny, s0, ns, nd, ptr(out))
         self.check(st, "ks_sobol_points")
         return out
+
+
+# ---------------------------------------------------------------------------------------------
+# Scene description structs (mirror include/ks_b200.h)
+# ---------------------------------------------------------------------------------------------
+class MeshDesc(ctypes.Structure):
+    _fields_ = [("vertices", _vp), ("n_vertices", _u32), ("indices", _vp), ("n_triangles", _u32),
+                ("vertex_normals", _vp), ("material", _u32), ("twosided", _i32), ("use_smooth_normal", _i32)]
+
+
+class MaterialDesc(ctypes.Structure):
+    _fields_ = [("basecolor", _f32 * 3), ("roughness", _f32), ("metallic", _f32), ("ior", _f32),
+                ("specular_r0_mul", _f32), ("specular_trans", _f32), ("diffuse_trans", _f32),
+                ("diffuse_trans_fwd", _f32), ("emissive", _f32 * 3), ("microfacet", _i32),
+                ("has_emission", _i32), ("emission", _f32 * 3)]
+
+
+class SkyDesc(ctypes.Structure):
+    _fields_ = [("kind", _i32), ("ambient", _f32 * 3), ("map_rgb", _vp), ("width", _u32), ("height", _u32),
+                ("to_world", _f32 * 16), ("transform_y_up", _i32), ("strength", _f32)]
+
+
+class SceneDesc(ctypes.Structure):
+    _fields_ = [("meshes", ctypes.POINTER(MeshDesc)), ("n_meshes", _u32),
+                ("materials", ctypes.POINTER(MaterialDesc)), ("n_materials", _u32), ("sky", SkyDesc)]
+
+
+class SBVHOptions(ctypes.Structure):
+    _fields_ = [("max_prims_in_node", _u32), ("bucket_count", _u32), ("trav_weight", _f32), ("alpha", _f32)]
+
+
+class CameraDesc(ctypes.Structure):
+    _fields_ = [("camera_to_world", _f32 * 16), ("proj_to_camera", _f32 * 16), ("proj_to_world", _f32 * 16)]
+
+
+class ProceduralOptions(ctypes.Structure):
+    _fields_ = [("level", _i32), ("roughness_min", _f32), ("roughness_max", _f32), ("occluder", _i32),
+                ("sky_width", _u32), ("sky_height", _u32), ("width", _u32), ("height", _u32)]
+
+
+def _sig(name, args, res=ctypes.c_int):
+    f = getattr(lib, name)
+    f.argtypes = args
+    f.restype = res
+
+
+_sig("ks_scene_create", [_vp, ctypes.POINTER(SceneDesc), ctypes.POINTER(_vp)])
+_sig("ks_scene_destroy", [_vp], None)
+_sig("ks_scene_build_bvh", [_vp, ctypes.POINTER(SBVHOptions), ctypes.POINTER(_f32)])
+_sig("ks_sbvh_counts", [_vp, ctypes.POINTER(_u32), ctypes.POINTER(_u32)])
+_sig("ks_sbvh_export", [_vp, _vp, _vp, _vp, _vp, _vp])
+_sig("ks_trace_rays", [_vp, _vp, _u32, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp])
+_sig("ks_camera_perspective", [ctypes.POINTER(_f32), _f32, _f32, ctypes.POINTER(CameraDesc)])
+_sig("ks_procedural_scene", [ctypes.c_char_p, ctypes.c_uint64, ctypes.POINTER(ProceduralOptions),
+                             ctypes.POINTER(_vp)])
+_sig("ks_generated_scene_desc", [_vp], ctypes.POINTER(SceneDesc))
+_sig("ks_generated_camera", [_vp, ctypes.POINTER(_f32), ctypes.POINTER(_f32), ctypes.POINTER(_f32)])
+_sig("ks_generated_destroy", [_vp], None)
+
+
+def _arr(p, n, dtype):
+    """Copy n elements of a C array into numpy."""
+    if not p or n == 0:
+        return np.zeros(0, dtype=dtype)
+    ct = {np.float32: ctypes.c_float, np.uint32: ctypes.c_uint32}[dtype]
+    buf = (ct * n).from_address(ctypes.cast(p, ctypes.c_void_p).value)
+    return np.frombuffer(buf, dtype=dtype).copy()
+
+
+class Generated:
+    """A seeded procedural scene (ks_procedural_scene) with numpy views of its arrays."""
+
+    def __init__(self, kind: str, seed: int = 0, level: int = 8, roughness=(0.05, 1.0), occluder=False,
+                 sky=(2048, 1024), resolution=(1024, 1024)):
+        o = ProceduralOptions(level, roughness[0], roughness[1], int(occluder), sky[0], sky[1],
+                              resolution[0], resolution[1])
+        h = _vp()
+        st = lib.ks_procedural_scene(kind.encode(), seed, ctypes.byref(o), ctypes.byref(h))
+        if st != KS_OK:
+            raise KsError(st, "ks_procedural_scene")
+        self.handle = h
+        self.desc = lib.ks_generated_scene_desc(h)
+        d = self.desc.contents
+        self.meshes = []
+        for m in range(d.n_meshes):
+            md = d.meshes[m]
+            self.meshes.append(dict(
+                vertices=_arr(md.vertices, 3 * md.n_vertices, np.float32).reshape(-1, 3),
+                indices=_arr(md.indices, 3 * md.n_triangles, np.uint32).reshape(-1, 3),
+                material=md.material, twosided=md.twosided))
+        self.materials = [d.materials[k] for k in range(d.n_materials)]
+        c2w = (_f32 * 16)()
+        vfov, aspect = _f32(), _f32()
+        lib.ks_generated_camera(h, c2w, ctypes.byref(vfov), ctypes.byref(aspect))
+        self.camera_to_world = np.array(c2w[:], dtype=np.float32)
+        self.vfov, self.aspect = vfov.value, aspect.value
+        self.sky_kind = d.sky.kind
+        self.sky_map = (_arr(d.sky.map_rgb, 3 * d.sky.width * d.sky.height, np.float32)
+                        .reshape(d.sky.height, d.sky.width, 3) if d.sky.kind == 2 else None)
+
+    def flat_geometry(self):
+        """All meshes concatenated in mesh order: (vertices [V,3], indices [T,3] global)."""
+        vs, ids, off = [], [], 0
+        for m in self.meshes:
+            vs.append(m["vertices"])
+            ids.append(m["indices"].astype(np.uint64) + off)
+            off += len(m["vertices"])
+        return np.concatenate(vs).astype(np.float32), np.concatenate(ids).astype(np.uint32)
+
+    @property
+    def n_triangles(self):
+        return sum(len(m["indices"]) for m in self.meshes)
+
+    def close(self):
+        if self.handle:
+            lib.ks_generated_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def camera_perspective(camera_to_world, vfov, aspect) -> CameraDesc:
+    c = CameraDesc()
+    m = (_f32 * 16)(*[float(x) for x in np.asarray(camera_to_world).reshape(16)])
+    st = lib.ks_camera_perspective(m, vfov, aspect, ctypes.byref(c))
+    if st != KS_OK:
+        raise KsError(st, "ks_camera_perspective")
+    return c
+
+
+def triangle_soup_desc(vertices, indices, material=None):
+    """Builds a one-mesh SceneDesc over numpy arrays; returns (desc, keepalive)."""
+    v = np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1, 3)
+    i = np.ascontiguousarray(indices, dtype=np.uint32).reshape(-1, 3)
+    mesh = MeshDesc(ptr(v), len(v), ptr(i), len(i), None, 0, 1, 1)
+    mat = material or MaterialDesc((0.8, 0.8, 0.8), 1.0, 0.0, 1.5, 0.5, 0.0, 0.0, 0.5, (0, 0, 0), 0, 0, (0, 0, 0))
+    meshes = (MeshDesc * 1)(mesh)
+    mats = (MaterialDesc * 1)(mat)
+    d = SceneDesc(meshes, 1, mats, 1, SkyDesc())
+    return d, (v, i, meshes, mats)
+
+
+class Scene:
+    """A device-resident scene (ks_scene)."""
+
+    def __init__(self, ctx: Context, desc, keepalive=None):
+        self.ctx = ctx
+        self._keep = keepalive
+        h = _vp()
+        dp = desc if isinstance(desc, ctypes.POINTER(SceneDesc)) else ctypes.byref(desc)
+        ctx.check(lib.ks_scene_create(ctx.handle, dp, ctypes.byref(h)), "ks_scene_create")
+        self.handle = h
+
+    def build_bvh(self, max_prims=4, buckets=12, trav_weight=1.0, alpha=1e-5) -> float:
+        o = SBVHOptions(max_prims, buckets, trav_weight, alpha)
+        ms = _f32()
+        self.ctx.check(lib.ks_scene_build_bvh(self.handle, ctypes.byref(o), ctypes.byref(ms)), "ks_scene_build_bvh")
+        return ms.value
+
+    def export_sbvh(self):
+        nn, npr = _u32(), _u32()
+        self.ctx.check(lib.ks_sbvh_counts(self.handle, ctypes.byref(nn), ctypes.byref(npr)), "ks_sbvh_counts")
+        n, m = nn.value, npr.value
+        bounds = np.empty((n, 6), np.float32)
+        axis = np.empty(n, np.uint32)
+        right = np.empty(n, np.uint32)
+        off = np.empty(n, np.uint32)
+        prims = np.empty(m, np.uint32)
+        self.ctx.check(lib.ks_sbvh_export(self.handle, ptr(bounds), ptr(axis), ptr(right), ptr(off), ptr(prims)),
+                       "ks_sbvh_export")
+        return dict(bounds=bounds, axis=axis, right=right, prim_offset=off, prims=prims)
+
+    def trace(self, rays, any_hit=False, culling=2):
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+        n = len(rays)
+        tri = np.empty(n, np.uint32)
+        t = np.empty(n, np.float32)
+        bary = np.empty((n, 3), np.float32)
+        self.ctx.check(lib.ks_trace_rays(self.handle, ptr(rays), n, int(any_hit), culling, ptr(tri), ptr(t),
+                                         ptr(bary)), "ks_trace_rays")
+        return (tri.astype(bool), None, None) if any_hit else (tri, t, bary)
+
+    def close(self):
+        if self.handle:
+            lib.ks_scene_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

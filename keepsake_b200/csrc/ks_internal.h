@@ -36,6 +36,17 @@ struct DevBuf
 {
     T *ptr = nullptr;
     size_t count = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+    // Grows (never shrinks) to hold n elements; contents are not preserved.
+    cudaError_t reserve(size_t n)
+    {
+        if (n <= count && ptr)
+            return cudaSuccess;
+        return alloc(n);
+    }
     cudaError_t alloc(size_t n)
     {
         release();

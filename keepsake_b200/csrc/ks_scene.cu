@@ -1,0 +1,242 @@
+// Scene lifetime, SBVH build/export entry points and the ray-query parity kernel.
+#include "ks_scene.h"
+#include "ks_traverse.cuh"
+
+#include <cstring>
+#include <new>
+
+using namespace ksb;
+
+namespace
+{
+
+__global__ void trace_kernel(const TravNode *nodes, const float4 *tris, uint32_t root_ref, uint32_t root_count,
+                             float bx0, float by0, float bz0, float bx1, float by1, float bz1, const float *rays,
+                             uint32_t n, int any_hit, int culling, uint32_t *tri_out, float *t_out, float *bary_out,
+                             int *overflow_flag)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const float *r = rays + 8 * (size_t)i;
+    RayQuery q;
+    q.o = mk(r[0], r[1], r[2]);
+    q.tmin = r[3];
+    q.d = mk(r[4], r[5], r[6]);
+    q.tmax = r[7];
+    const float bmin[3] = {bx0, by0, bz0}, bmax[3] = {bx1, by1, bz1};
+    Hit h;
+    int overflow = 0;
+    if (any_hit) {
+        bool occ = traverse<true>(nodes, tris, root_ref, root_count, bmin, bmax, q, culling, h, overflow);
+        tri_out[i] = occ ? 1u : 0u;
+    } else {
+        traverse<false>(nodes, tris, root_ref, root_count, bmin, bmax, q, culling, h, overflow);
+        tri_out[i] = h.tri;
+        if (h.tri != ~0u) {
+            t_out[i] = h.t;
+            bary_out[3 * i + 0] = h.b0;
+            bary_out[3 * i + 1] = h.b1;
+            bary_out[3 * i + 2] = h.b2;
+        } else {
+            t_out[i] = -kInf;
+            bary_out[3 * i + 0] = bary_out[3 * i + 1] = bary_out[3 * i + 2] = 0.0f;
+        }
+    }
+    if (overflow)
+        atomicOr(overflow_flag, 1);
+}
+
+bool valid_material(const ks_material_desc &m)
+{
+    auto finite = [](float x) { return x == x && x < 3.0e38f && x > -3.0e38f; };
+    for (int c = 0; c < 3; ++c)
+        if (!finite(m.basecolor[c]) || !finite(m.emission[c]))
+            return false;
+    return finite(m.roughness) && finite(m.metallic) && finite(m.ior) && finite(m.specular_r0_mul) &&
+           finite(m.specular_trans) && finite(m.diffuse_trans) && finite(m.diffuse_trans_fwd);
+}
+
+} // namespace
+
+extern "C" {
+
+ks_status ks_scene_create(ks_context *ctx, const ks_scene_desc *desc, ks_scene **out)
+{
+    if (!ctx || !desc || !out)
+        return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_create: null argument");
+    *out = nullptr;
+    if (desc->n_meshes == 0 || !desc->meshes)
+        return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_create: no meshes");
+    if (desc->n_materials == 0 || !desc->materials)
+        return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_create: no materials");
+    uint64_t n_tris = 0, n_verts = 0;
+    for (uint32_t m = 0; m < desc->n_meshes; ++m) {
+        const ks_mesh_desc &md = desc->meshes[m];
+        if (!md.vertices || !md.indices || md.n_triangles == 0 || md.n_vertices == 0)
+            return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_create: empty mesh " + std::to_string(m));
+        if (md.material >= desc->n_materials)
+            return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_create: material index out of range");
+        for (uint64_t k = 0; k < 3ull * md.n_triangles; ++k)
+            if (md.indices[k] >= md.n_vertices)
+                return fail(ctx, KS_ERR_INVALID_ARGUMENT,
+                            "ks_scene_create: vertex index out of range in mesh " + std::to_string(m));
+        n_tris += md.n_triangles;
+        n_verts += md.n_vertices;
+    }
+    if (n_tris >= (1ull << 30) || n_verts >= (1ull << 31))
+        return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_create: scene too large");
+    for (uint32_t k = 0; k < desc->n_materials; ++k)
+        if (!valid_material(desc->materials[k]))
+            return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_create: non-finite material field");
+    KS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    ks_scene *s = new (std::nothrow) ks_scene();
+    if (!s)
+        return fail(ctx, KS_ERR_OUT_OF_MEMORY, "ks_scene_create");
+    s->ctx = ctx;
+    s->n_tris = (uint32_t)n_tris;
+    s->n_verts = (uint32_t)n_verts;
+    std::vector<float> verts(3 * n_verts);
+    std::vector<uint32_t> idx(3 * n_tris), tri_mesh(n_tris);
+    uint64_t vo = 0, to = 0;
+    for (uint32_t m = 0; m < desc->n_meshes; ++m) {
+        const ks_mesh_desc &md = desc->meshes[m];
+        std::memcpy(&verts[3 * vo], md.vertices, sizeof(float) * 3 * md.n_vertices);
+        for (uint64_t k = 0; k < 3ull * md.n_triangles; ++k)
+            idx[3 * to + k] = (uint32_t)(md.indices[k] + vo);
+        for (uint64_t k = 0; k < md.n_triangles; ++k)
+            tri_mesh[to + k] = m;
+        s->host.mesh_tri_offset.push_back((uint32_t)to);
+        s->host.mesh_material.push_back(md.material);
+        s->host.mesh_twosided.push_back(md.twosided);
+        vo += md.n_vertices;
+        to += md.n_triangles;
+    }
+    s->host.mesh_tri_offset.push_back((uint32_t)to);
+    s->host.materials.assign(desc->materials, desc->materials + desc->n_materials);
+    cudaError_t e = s->verts.alloc(verts.size());
+    if (e == cudaSuccess)
+        e = s->indices.alloc(idx.size());
+    if (e == cudaSuccess)
+        e = s->tri_mesh.alloc(tri_mesh.size());
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(s->verts.ptr, verts.data(), s->verts.bytes(), cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(s->indices.ptr, idx.data(), s->indices.bytes(), cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(s->tri_mesh.ptr, tri_mesh.data(), s->tri_mesh.bytes(), cudaMemcpyHostToDevice,
+                            ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        delete s;
+        return cuda_fail(ctx, e, "ks_scene_create: upload");
+    }
+    *out = s;
+    return KS_OK;
+}
+
+void ks_scene_destroy(ks_scene *scene)
+{
+    if (!scene)
+        return;
+    cudaSetDevice(scene->ctx->device);
+    cudaStreamSynchronize(scene->ctx->stream);
+    delete scene;
+}
+
+ks_status ks_scene_build_bvh(ks_scene *scene, const ks_sbvh_options *opts, float *build_ms)
+{
+    if (!scene)
+        return KS_ERR_INVALID_ARGUMENT;
+    ks_sbvh_options o{4, 12, 1.0f, 1e-5f};
+    if (opts)
+        o = *opts;
+    KS_CUDA_TRY(scene->ctx, cudaSetDevice(scene->ctx->device));
+    scene->bvh_built = false;
+    return build_sbvh(scene, o, build_ms);
+}
+
+ks_status ks_sbvh_counts(const ks_scene *scene, uint32_t *n_nodes, uint32_t *n_prims)
+{
+    if (!scene || !n_nodes || !n_prims)
+        return KS_ERR_INVALID_ARGUMENT;
+    if (!scene->bvh_built)
+        return fail(scene->ctx, KS_ERR_NOT_BUILT, "ks_sbvh_counts: call ks_scene_build_bvh first");
+    *n_nodes = scene->n_nodes;
+    *n_prims = scene->n_prims;
+    return KS_OK;
+}
+
+ks_status ks_sbvh_export(const ks_scene *scene, float *node_bounds, uint32_t *node_axis, uint32_t *node_right,
+                         uint32_t *node_prim_offset, uint32_t *prims)
+{
+    if (!scene)
+        return KS_ERR_INVALID_ARGUMENT;
+    ks_context *ctx = scene->ctx;
+    if (!scene->bvh_built)
+        return fail(ctx, KS_ERR_NOT_BUILT, "ks_sbvh_export: call ks_scene_build_bvh first");
+    KS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    std::vector<RefNode> nodes(scene->n_nodes);
+    KS_CUDA_TRY(ctx, cudaMemcpy(nodes.data(), scene->ref_nodes.ptr, sizeof(RefNode) * nodes.size(),
+                                cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < nodes.size(); ++i) {
+        if (node_bounds)
+            for (int k = 0; k < 3; ++k) {
+                node_bounds[6 * i + k] = nodes[i].bmin[k];
+                node_bounds[6 * i + 3 + k] = nodes[i].bmax[k];
+            }
+        if (node_axis)
+            node_axis[i] = nodes[i].axis;
+        if (node_right)
+            node_right[i] = nodes[i].right;
+        if (node_prim_offset)
+            node_prim_offset[i] = nodes[i].prim_offset;
+    }
+    if (prims)
+        KS_CUDA_TRY(ctx, cudaMemcpy(prims, scene->prims.ptr, sizeof(uint32_t) * scene->n_prims,
+                                    cudaMemcpyDeviceToHost));
+    return KS_OK;
+}
+
+ks_status ks_trace_rays(ks_scene *scene, const float *rays, uint32_t n, int any_hit, int culling, uint32_t *tri_idx,
+                        float *t, float *bary)
+{
+    if (!scene || !rays || !tri_idx || (!any_hit && (!t || !bary)) || culling < 0 || culling > 2)
+        return fail(scene ? scene->ctx : nullptr, KS_ERR_INVALID_ARGUMENT, "ks_trace_rays: bad argument");
+    ks_context *ctx = scene->ctx;
+    if (!scene->bvh_built)
+        return fail(ctx, KS_ERR_NOT_BUILT, "ks_trace_rays: call ks_scene_build_bvh first");
+    if (n == 0)
+        return KS_OK;
+    KS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    DevBuf<float> d_rays, d_t, d_bary;
+    DevBuf<uint32_t> d_tri;
+    DevBuf<int> d_flag;
+    KS_CUDA_TRY(ctx, d_rays.alloc((size_t)n * 8));
+    KS_CUDA_TRY(ctx, d_tri.alloc(n));
+    KS_CUDA_TRY(ctx, d_t.alloc(n));
+    KS_CUDA_TRY(ctx, d_bary.alloc((size_t)n * 3));
+    KS_CUDA_TRY(ctx, d_flag.alloc(1));
+    cudaStream_t st = ctx->stream;
+    KS_CUDA_TRY(ctx, cudaMemcpyAsync(d_rays.ptr, rays, d_rays.bytes(), cudaMemcpyHostToDevice, st));
+    KS_CUDA_TRY(ctx, cudaMemsetAsync(d_flag.ptr, 0, sizeof(int), st));
+    const float *b = scene->scene_bound;
+    trace_kernel<<<(n + 127) / 128, 128, 0, st>>>(scene->trav_nodes.ptr, scene->prim_tris.ptr, scene->root_ref,
+                                                   scene->root_count, b[0], b[1], b[2], b[3], b[4], b[5], d_rays.ptr, n,
+                                                   any_hit, culling, d_tri.ptr, d_t.ptr, d_bary.ptr, d_flag.ptr);
+    KS_CUDA_TRY(ctx, cudaGetLastError());
+    int overflow = 0;
+    KS_CUDA_TRY(ctx, cudaMemcpyAsync(tri_idx, d_tri.ptr, d_tri.bytes(), cudaMemcpyDeviceToHost, st));
+    if (!any_hit) {
+        KS_CUDA_TRY(ctx, cudaMemcpyAsync(t, d_t.ptr, d_t.bytes(), cudaMemcpyDeviceToHost, st));
+        KS_CUDA_TRY(ctx, cudaMemcpyAsync(bary, d_bary.ptr, d_bary.bytes(), cudaMemcpyDeviceToHost, st));
+    }
+    KS_CUDA_TRY(ctx, cudaMemcpyAsync(&overflow, d_flag.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
+    KS_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    if (overflow)
+        return fail(ctx, KS_ERR_QUEUE_OVERFLOW, "ks_trace_rays: traversal stack depth exceeded");
+    return KS_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,84 @@
+// Device-resident scene: geometry, SBVH (reference layout + traversal layout), materials, lights.
+#pragma once
+#include "ks_internal.h"
+#include "ks_math.cuh"
+
+#include <vector>
+
+namespace ksb
+{
+
+// SBVH node in the reference's flattened layout (cuda/sbvh.cuh:18-28), kept for export/parity.
+struct RefNode
+{
+    float bmin[3];
+    float bmax[3];
+    uint32_t axis;
+    uint32_t right; // 0 = leaf
+    uint32_t prim_offset;
+};
+
+// Traversal node: an interior node of the flattened SBVH with both children's boxes (64 bytes).
+//   a = (L.min.x, L.min.y, L.min.z, L.max.x)   b = (L.max.y, L.max.z, R.min.x, R.min.y)
+//   c = (R.min.z, R.max.x, R.max.y, R.max.z)   d = (L.ref, R.ref, L.count | axis << 30, R.count)
+// A child ref with the top bit set is a leaf: (ref & 0x7fffffff) is its first primitive slot.
+struct TravNode
+{
+    float4 a, b, c;
+    uint4 d;
+};
+constexpr uint32_t kLeafBit = 0x80000000u;
+
+// Device copy of one material (constant principled fields + emission).
+struct MaterialGPU
+{
+    float basecolor[3];
+    float roughness, metallic, ior, specular_r0_mul, specular_trans, diffuse_trans, diffuse_trans_fwd;
+    int microfacet;
+    int has_emission;
+    float emission[3];
+    int mesh_light; // index of the MeshLightShared for emissive meshes, -1 otherwise
+};
+
+struct SceneHost
+{
+    std::vector<uint32_t> mesh_tri_offset; // first global triangle of each mesh (+ total at the end)
+    std::vector<uint32_t> mesh_material;
+    std::vector<int> mesh_twosided;
+    std::vector<ks_material_desc> materials;
+};
+
+} // namespace ksb
+
+struct ks_scene
+{
+    ks_context *ctx = nullptr;
+    uint32_t n_tris = 0;
+    uint32_t n_verts = 0;
+    ksb::SceneHost host;
+    // geometry, concatenated over meshes: vertices (float3), indices (uint3, global vertex ids),
+    // per-triangle mesh id
+    ksb::DevBuf<float> verts;
+    ksb::DevBuf<uint32_t> indices;
+    ksb::DevBuf<uint32_t> tri_mesh;
+    // SBVH in the reference layout + ordered primitive list
+    ksb::DevBuf<ksb::RefNode> ref_nodes;
+    ksb::DevBuf<uint32_t> prims;
+    uint32_t n_nodes = 0, n_prims = 0;
+    // traversal layout
+    ksb::DevBuf<ksb::TravNode> trav_nodes;
+    ksb::DevBuf<float4> prim_tris; // 3 float4 per primitive slot: v0 (+tri index bits in w), v1, v2
+    uint32_t n_trav = 0;
+    uint32_t root_ref = 0;   // ref of the root (leaf bit when the whole tree is one leaf)
+    uint32_t root_count = 0; // prim count of the root
+    bool bvh_built = false;
+    float scene_bound[6] = {0, 0, 0, 0, 0, 0};
+    // materials
+    ksb::DevBuf<ksb::MaterialGPU> materials;
+    ksb::DevBuf<uint32_t> mesh_material;
+};
+
+namespace ksb
+{
+ks_status build_sbvh(ks_scene *scene, const ks_sbvh_options &opts, float *build_ms);
+}

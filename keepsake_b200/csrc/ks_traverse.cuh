@@ -1,0 +1,289 @@
+// SBVH traversal and the watertight ray/triangle test on the device.
+//
+// Hit semantics follow the reference exactly:
+//   * RayTriHelper + isect_ray_tri: shear/scale watertight test of Woop et al. with the FP64
+//     edge fallback (cuda/ray_tri.cuh:8-97),
+//   * RayBoundHelper + isect_ray_aabb: slab test with the 0*inf guard (cuda/aabb.cuh:155-252),
+//   * SBVH::intersect / intersectBool: near child first by the sign of the ray direction on the
+//     node's split axis, leaf primitives in order, a hit replaces the current one only if
+//     tHit < tmax (cuda/sbvh.cu:512-603).
+// The node layout differs (both children's boxes are stored in the parent, so a child box is
+// tested when its parent is expanded and re-checked against the current tmax when popped).
+// Because the slab interval of a box does not depend on tmax, that re-check makes exactly the
+// decision the reference makes when it visits the child, so the sequence of triangle tests -
+// and therefore the hit, including ties - is the reference's.
+#pragma once
+#include "ks_math.cuh"
+#include "ks_scene.h"
+
+namespace ksb
+{
+
+struct RayQuery
+{
+    f3 o, d;
+    float tmin, tmax;
+};
+
+struct TriHelper
+{
+    int kx, ky, kz;
+    float shx, shy, shz;
+};
+
+struct BoxHelper
+{
+    f3 inv;
+    int neg[3];
+};
+
+KS_D TriHelper make_tri_helper(f3 dir)
+{
+    TriHelper h;
+    float ax = fabsf(dir.x), ay = fabsf(dir.y), az = fabsf(dir.z);
+    if (ax >= ay && ax >= az)
+        h.kz = 0;
+    else if (ay >= ax && ay >= az)
+        h.kz = 1;
+    else
+        h.kz = 2;
+    h.kx = (h.kz + 1) % 3;
+    h.ky = (h.kx + 1) % 3;
+    if (get(dir, h.kz) < 0.0f) {
+        int t = h.kx;
+        h.kx = h.ky;
+        h.ky = t;
+    }
+    float dz = get(dir, h.kz);
+    h.shx = get(dir, h.kx) / dz;
+    h.shy = get(dir, h.ky) / dz;
+    h.shz = 1.0f / dz;
+    return h;
+}
+
+KS_D BoxHelper make_box_helper(f3 dir)
+{
+    BoxHelper b;
+    b.inv = mk(1.0f / dir.x, 1.0f / dir.y, 1.0f / dir.z);
+    b.neg[0] = dir.x < 0.0f || (dir.x == 0.0f && signbit(dir.x));
+    b.neg[1] = dir.y < 0.0f || (dir.y == 0.0f && signbit(dir.y));
+    b.neg[2] = dir.z < 0.0f || (dir.z == 0.0f && signbit(dir.z));
+    return b;
+}
+
+// ksc::difference_of_products (cuda/math.cuh:189-195)
+KS_D float diff_of_products(float a, float b, float c, float d)
+{
+    float cd = c * d;
+    float dop = fmaf(a, b, -cd);
+    float err = fmaf(-c, d, cd);
+    return dop + err;
+}
+
+// isect_ray_tri (cuda/ray_tri.cuh:46-97).  Returns true on a hit inside (tmin, tmax).
+KS_D bool isect_tri(const RayQuery &ray, const TriHelper &h, f3 v0, f3 v1, f3 v2, float &t_out, float &b0, float &b1,
+                    float &b2)
+{
+    f3 A0 = v0 - ray.o, B0 = v1 - ray.o, C0 = v2 - ray.o;
+    f3 A = mk(get(A0, h.kx), get(A0, h.ky), get(A0, h.kz));
+    f3 B = mk(get(B0, h.kx), get(B0, h.ky), get(B0, h.kz));
+    f3 C = mk(get(C0, h.kx), get(C0, h.ky), get(C0, h.kz));
+    f3 sx = mk(A.x - h.shx * A.z, B.x - h.shx * B.z, C.x - h.shx * C.z);
+    f3 sy = mk(A.y - h.shy * A.z, B.y - h.shy * B.z, C.y - h.shy * C.z);
+    // bc = cross(sy, sx) with difference_of_products
+    float bx = diff_of_products(sy.y, sx.z, sy.z, sx.y);
+    float by = diff_of_products(sy.z, sx.x, sy.x, sx.z);
+    float bz = diff_of_products(sy.x, sx.y, sy.y, sx.x);
+    if (bx == 0.0f || by == 0.0f || bz == 0.0f) {
+        bx = (float)((double)sx.z * (double)sy.y - (double)sy.z * (double)sx.y);
+        by = (float)((double)sx.x * (double)sy.z - (double)sy.x * (double)sx.z);
+        bz = (float)((double)sx.y * (double)sy.x - (double)sy.y * (double)sx.x);
+    }
+    if ((bx < 0.0f || by < 0.0f || bz < 0.0f) && (bx > 0.0f || by > 0.0f || bz > 0.0f))
+        return false;
+    float det = bx + by + bz;
+    if (det == 0.0f)
+        return false;
+    float szx = h.shz * A.z, szy = h.shz * B.z, szz = h.shz * C.z;
+    float T = bx * szx + by * szy + bz * szz;
+    if (det < 0.0f && (T >= ray.tmin * det || T <= ray.tmax * det))
+        return false;
+    if (det > 0.0f && (T <= ray.tmin * det || T >= ray.tmax * det))
+        return false;
+    float inv_det = 1.0f / det;
+    b0 = bx * inv_det;
+    b1 = by * inv_det;
+    b2 = bz * inv_det;
+    t_out = T * inv_det;
+    return true;
+}
+
+// Slab part of isect_ray_aabb (cuda/aabb.cuh:171-236): returns false if the slabs do not
+// overlap, else the clipped-free entry/exit times.
+KS_D bool slab(const RayQuery &ray, const BoxHelper &h, const float bmin[3], const float bmax[3], float &t0,
+               float &t1)
+{
+    float tmin = (h.neg[0] ? bmax[0] : bmin[0]) - ray.o.x;
+    if (tmin != 0.0f)
+        tmin *= h.inv.x;
+    float tmax = (h.neg[0] ? bmin[0] : bmax[0]) - ray.o.x;
+    if (tmax != 0.0f)
+        tmax *= h.inv.x;
+    float tymin = (h.neg[1] ? bmax[1] : bmin[1]) - ray.o.y;
+    if (tymin != 0.0f)
+        tymin *= h.inv.y;
+    float tymax = (h.neg[1] ? bmin[1] : bmax[1]) - ray.o.y;
+    if (tymax != 0.0f)
+        tymax *= h.inv.y;
+    if (tmin > tymax || tymin > tmax)
+        return false;
+    if (tymin > tmin)
+        tmin = tymin;
+    if (tymax < tmax)
+        tmax = tymax;
+    float tzmin = (h.neg[2] ? bmax[2] : bmin[2]) - ray.o.z;
+    if (tzmin != 0.0f)
+        tzmin *= h.inv.z;
+    float tzmax = (h.neg[2] ? bmin[2] : bmax[2]) - ray.o.z;
+    if (tzmax != 0.0f)
+        tzmax *= h.inv.z;
+    if (tmin > tzmax || tzmin > tmax)
+        return false;
+    if (tzmin > tmin)
+        tmin = tzmin;
+    if (tzmax < tmax)
+        tmax = tzmax;
+    t0 = tmin;
+    t1 = tmax;
+    return true;
+}
+
+enum class Culling : int
+{
+    Back = 0,
+    Front = 1,
+    None = 2,
+};
+
+KS_D bool cull_tri(const RayQuery &ray, f3 v0, f3 v1, f3 v2, int culling)
+{
+    if (culling == (int)Culling::None)
+        return false;
+    // check = dot(dir, cross(v1 - v0, v2 - v1)) with difference_of_products (cuda/sbvh.cu:478-484)
+    f3 e0 = v1 - v0, e1 = v2 - v1;
+    f3 c = mk(diff_of_products(e0.y, e1.z, e0.z, e1.y), diff_of_products(e0.z, e1.x, e0.x, e1.z),
+              diff_of_products(e0.x, e1.y, e0.y, e1.x));
+    float check = ray.d.x * c.x + ray.d.y * c.y + ray.d.z * c.z;
+    if (check >= 0.0f && culling == (int)Culling::Back)
+        return true;
+    if (check <= 0.0f && culling == (int)Culling::Front)
+        return true;
+    return false;
+}
+
+struct Hit
+{
+    uint32_t tri; // global triangle index, ~0u on miss
+    float t, b0, b1, b2;
+};
+
+constexpr int kStackDepth = 64;
+
+// Closest hit (any_hit = false) or occlusion (any_hit = true) against the scene's SBVH.
+template <bool kAnyHit>
+KS_D bool traverse(const TravNode *__restrict__ nodes, const float4 *__restrict__ tris, uint32_t root_ref,
+                   uint32_t root_count, const float root_bmin[3], const float root_bmax[3], RayQuery ray,
+                   int culling, Hit &hit, int &overflow)
+{
+    hit.tri = ~0u;
+    const TriHelper th = make_tri_helper(ray.d);
+    const BoxHelper bh = make_box_helper(ray.d);
+    uint32_t st_ref[kStackDepth];
+    uint32_t st_cnt[kStackDepth];
+    float st_t[kStackDepth];
+    int sp = 0;
+    // the root's own box (cuda/sbvh.cu:520-527)
+    float t0, t1;
+    if (!slab(ray, bh, root_bmin, root_bmax, t0, t1) || !(t0 < ray.tmax && t1 > ray.tmin))
+        return false;
+    uint32_t ref = root_ref, cnt = root_count;
+    while (true) {
+        if (ref & kLeafBit) {
+            uint32_t first = ref & ~kLeafBit;
+            for (uint32_t k = 0; k < cnt; ++k) {
+                const float4 *p = tris + 3 * (size_t)(first + k);
+                float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2);
+                f3 v0 = mk(a.x, a.y, a.z), v1 = mk(b.x, b.y, b.z), v2 = mk(c.x, c.y, c.z);
+                if (cull_tri(ray, v0, v1, v2, culling))
+                    continue;
+                float t, b0, b1, b2;
+                if (isect_tri(ray, th, v0, v1, v2, t, b0, b1, b2)) {
+                    if (kAnyHit) {
+                        hit.tri = __float_as_uint(a.w);
+                        return true;
+                    }
+                    if (t < ray.tmax) {
+                        ray.tmax = t;
+                        hit.tri = __float_as_uint(a.w);
+                        hit.t = t;
+                        hit.b0 = b0;
+                        hit.b1 = b1;
+                        hit.b2 = b2;
+                    }
+                }
+            }
+        } else {
+            const TravNode *n = nodes + ref;
+            float4 A = __ldg(&n->a), B = __ldg(&n->b), C = __ldg(&n->c);
+            uint4 D = __ldg(&n->d);
+            float lmin[3] = {A.x, A.y, A.z}, lmax[3] = {A.w, B.x, B.y};
+            float rmin[3] = {B.z, B.w, C.x}, rmax[3] = {C.y, C.z, C.w};
+            float lt0, lt1, rt0, rt1;
+            bool lok = slab(ray, bh, lmin, lmax, lt0, lt1) && lt1 > ray.tmin && lt0 < ray.tmax;
+            bool rok = slab(ray, bh, rmin, rmax, rt0, rt1) && rt1 > ray.tmin && rt0 < ray.tmax;
+            uint32_t axis = D.z >> 30;
+            uint32_t lcnt = D.z & 0x3fffffffu, rcnt = D.w;
+            bool right_first = bh.neg[axis] != 0;
+            uint32_t near_ref = right_first ? D.y : D.x, far_ref = right_first ? D.x : D.y;
+            uint32_t near_cnt = right_first ? rcnt : lcnt, far_cnt = right_first ? lcnt : rcnt;
+            bool near_ok = right_first ? rok : lok, far_ok = right_first ? lok : rok;
+            float far_t = right_first ? lt0 : rt0;
+            if (near_ok) {
+                if (far_ok) {
+                    if (sp >= kStackDepth) {
+                        overflow = 1;
+                        return !kAnyHit && hit.tri != ~0u;
+                    }
+                    st_ref[sp] = far_ref;
+                    st_cnt[sp] = far_cnt;
+                    st_t[sp] = far_t;
+                    ++sp;
+                }
+                ref = near_ref;
+                cnt = near_cnt;
+                continue;
+            }
+            if (far_ok) {
+                ref = far_ref;
+                cnt = far_cnt;
+                continue;
+            }
+        }
+        // pop, re-checking the entry time against the current tmax
+        bool found = false;
+        while (sp > 0) {
+            --sp;
+            if (st_t[sp] < ray.tmax) {
+                ref = st_ref[sp];
+                cnt = st_cnt[sp];
+                found = true;
+                break;
+            }
+        }
+        if (!found)
+            break;
+    }
+    return hit.tri != ~0u;
+}
+
+} // namespace ksb

@@ -1,0 +1,152 @@
+// Host-only C-ABI entry points: camera matrices and procedural scenes.
+#include "../../include/ks_b200.h"
+#include "procedural.h"
+
+#include <cmath>
+#include <cstring>
+#include <new>
+
+namespace
+{
+
+using M4 = double[4][4];
+
+// Inverse of a 4x4 matrix by Gauss-Jordan elimination with partial pivoting, in double precision.
+bool invert4(const double in[4][4], double out[4][4])
+{
+    double a[4][8];
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 8; ++c)
+            a[r][c] = c < 4 ? in[r][c] : (c - 4 == r ? 1.0 : 0.0);
+    for (int col = 0; col < 4; ++col) {
+        int piv = col;
+        for (int r = col + 1; r < 4; ++r)
+            if (std::fabs(a[r][col]) > std::fabs(a[piv][col]))
+                piv = r;
+        if (a[piv][col] == 0.0)
+            return false;
+        if (piv != col)
+            for (int c = 0; c < 8; ++c)
+                std::swap(a[piv][c], a[col][c]);
+        double inv = 1.0 / a[col][col];
+        for (int c = 0; c < 8; ++c)
+            a[col][c] *= inv;
+        for (int r = 0; r < 4; ++r) {
+            if (r == col)
+                continue;
+            double f = a[r][col];
+            if (f != 0.0)
+                for (int c = 0; c < 8; ++c)
+                    a[r][c] -= f * a[col][c];
+        }
+    }
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c)
+            out[r][c] = a[r][c + 4];
+    return true;
+}
+
+void mul4(const double a[4][4], const double b[4][4], double out[4][4])
+{
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c) {
+            double s = 0;
+            for (int k = 0; k < 4; ++k)
+                s += a[r][k] * b[k][c];
+            out[r][c] = s;
+        }
+}
+
+void store(const double m[4][4], float *out)
+{
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c)
+            out[4 * r + c] = (float)m[r][c];
+}
+
+} // namespace
+
+struct ks_generated
+{
+    ksb::GeneratedScene scene;
+};
+
+extern "C" {
+
+ks_status ks_camera_perspective(const float camera_to_world[16], float vfov, float aspect, ks_camera_desc *out)
+{
+    if (!camera_to_world || !out || !(vfov > 0.0f) || !(aspect > 0.0f))
+        return KS_ERR_INVALID_ARGUMENT;
+    double c2w[4][4], w2c[4][4], proj[4][4] = {}, p2c[4][4], p2w[4][4], w2p[4][4];
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c)
+            c2w[r][c] = camera_to_world[4 * r + c];
+    if (!invert4(c2w, w2c))
+        return KS_ERR_INVALID_ARGUMENT;
+    // rev_inf_projection(vfov, aspect, near_clip = 0.1) (camera.cpp:56-70), built in float like
+    // the reference, then promoted.
+    float cot_half_vfov = 1.0f / std::tan(vfov * 0.5f);
+    proj[0][0] = cot_half_vfov / aspect;
+    proj[1][1] = -cot_half_vfov;
+    proj[2][3] = 0.1f;
+    proj[3][2] = -1.0f;
+    mul4(proj, w2c, w2p);
+    if (!invert4(proj, p2c) || !invert4(w2p, p2w))
+        return KS_ERR_INVALID_ARGUMENT;
+    std::memcpy(out->camera_to_world, camera_to_world, sizeof(float) * 16);
+    store(p2c, out->proj_to_camera);
+    store(p2w, out->proj_to_world);
+    return KS_OK;
+}
+
+ks_status ks_procedural_scene(const char *kind, uint64_t seed, const ks_procedural_options *opts, ks_generated **out)
+{
+    if (!kind || !out)
+        return KS_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    ksb::ProceduralOptions o;
+    if (opts) {
+        if (opts->level > 0)
+            o.level = opts->level;
+        if (opts->roughness_max > 0.0f) {
+            o.roughness_min = opts->roughness_min;
+            o.roughness_max = opts->roughness_max;
+        }
+        o.occluder = opts->occluder;
+        if (opts->sky_width)
+            o.sky_width = opts->sky_width;
+        if (opts->sky_height)
+            o.sky_height = opts->sky_height;
+        if (opts->width)
+            o.width = opts->width;
+        if (opts->height)
+            o.height = opts->height;
+    }
+    if (o.level > 10)
+        return KS_ERR_INVALID_ARGUMENT;
+    auto *g = new (std::nothrow) ks_generated();
+    if (!g)
+        return KS_ERR_OUT_OF_MEMORY;
+    if (!ksb::generate_scene(kind, seed, o, g->scene)) {
+        delete g;
+        return KS_ERR_INVALID_ARGUMENT;
+    }
+    *out = g;
+    return KS_OK;
+}
+
+const ks_scene_desc *ks_generated_scene_desc(const ks_generated *g) { return g ? &g->scene.desc : nullptr; }
+
+ks_status ks_generated_camera(const ks_generated *g, float camera_to_world[16], float *vfov, float *aspect)
+{
+    if (!g || !camera_to_world || !vfov || !aspect)
+        return KS_ERR_INVALID_ARGUMENT;
+    std::memcpy(camera_to_world, g->scene.camera_to_world, sizeof(float) * 16);
+    *vfov = g->scene.vfov;
+    *aspect = g->scene.aspect;
+    return KS_OK;
+}
+
+void ks_generated_destroy(ks_generated *g) { delete g; }
+
+} // extern "C"

@@ -1,0 +1,48 @@
+// Seeded procedural scenes used as synthetic inputs (host side).
+#pragma once
+#include "../../include/ks_b200.h"
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace ksb
+{
+
+struct ProceduralOptions
+{
+    int level = 8;               // icosphere subdivision level
+    float roughness_min = 0.05f; // per-patch roughness range
+    float roughness_max = 1.0f;
+    int occluder = 0;            // slab between sphere and sun
+    uint32_t sky_width = 2048;
+    uint32_t sky_height = 1024;
+    uint32_t width = 1024; // render resolution (sets the camera aspect)
+    uint32_t height = 1024;
+};
+
+struct GeneratedMesh
+{
+    std::vector<float> vertices;
+    std::vector<uint32_t> indices;
+    uint32_t material = 0;
+};
+
+struct GeneratedScene
+{
+    std::vector<GeneratedMesh> meshes;
+    std::vector<ks_material_desc> materials;
+    std::vector<float> sky_map;
+    ks_sky_desc sky{};
+    std::vector<ks_mesh_desc> mesh_descs;
+    ks_scene_desc desc{};
+    float camera_to_world[16]{};
+    float vfov = 0.7f;
+    float aspect = 1.0f;
+    uint32_t width = 256, height = 256;
+    void finalize();
+};
+
+bool generate_scene(const std::string &kind, uint64_t seed, const ProceduralOptions &opts, GeneratedScene &out);
+
+} // namespace ksb

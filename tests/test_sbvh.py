@@ -1,0 +1,147 @@
+"""SBVH parity: the GPU builder's tree against the reference builder (cuda/sbvh.cu, compiled
+host-side in oracle/_ref), and GPU ray queries against SBVH::intersect / intersectBool.
+
+Topology = node count, DFS node order, node bounds, split axes, rightChildOffset, primOffset,
+and the multiset of primitives in every leaf (their order inside a leaf comes from
+std::partition's swap order in the reference and is not part of the contract)."""
+import numpy as np
+import pytest
+
+import scenes
+
+
+def leaf_multisets(right, prim_offset, prims):
+    n = len(right)
+    ends = np.append(prim_offset[1:], len(prims))
+    out = {}
+    for i in np.nonzero(right == 0)[0]:
+        out[int(i)] = np.sort(prims[prim_offset[i]:ends[i]])
+    return out
+
+
+def assert_same_tree(got, ref):
+    assert len(got["axis"]) == len(ref.axis), "node count differs"
+    assert len(got["prims"]) == len(ref.prims), "primitive reference count differs"
+    assert np.array_equal(got["right"], ref.right), "rightChildOffset differs"
+    assert np.array_equal(got["prim_offset"], ref.prim_offset), "primOffset differs"
+    interior = ref.right != 0
+    assert np.array_equal(got["axis"][interior], ref.axis[interior]), "split axis differs"
+    # float compare (== treats -0 and +0 alike)
+    assert np.array_equal(got["bounds"], ref.bounds), "node bounds differ"
+    a = leaf_multisets(ref.right, ref.prim_offset, ref.prims)
+    b = leaf_multisets(got["right"], got["prim_offset"], got["prims"])
+    for k in a:
+        assert np.array_equal(a[k], b[k]), f"leaf {k} primitives differ"
+
+
+def test_reference_builder_runs_on_cpu():
+    import oracle_lib
+    v, i = scenes.soup(500, seed=3)
+    tree = oracle_lib.ref_sbvh().build(v, i)
+    assert len(tree.prims) >= 500 and tree.right[0] != 0
+
+
+def _check_build(ctx, v, i, **opts):
+    import keepsake_b200 as ks
+    import oracle_lib
+    d, keep = ks.triangle_soup_desc(v, i)
+    s = ks.Scene(ctx, d, keep)
+    s.build_bvh(**opts)
+    got = s.export_sbvh()
+    ref = oracle_lib.ref_sbvh().build(v, i, **{
+        "max_prims": opts.get("max_prims", 4), "buckets": opts.get("buckets", 12),
+        "trav_weight": opts.get("trav_weight", 1.0), "alpha": opts.get("alpha", 1e-5)})
+    assert_same_tree(got, ref)
+    return s, ref
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,seed", [(1, 0), (2, 1), (7, 2), (100, 3), (2000, 4), (30000, 5)])
+def test_builder_topology_soup(ctx, n, seed):
+    v, i = scenes.soup(n, seed=seed)
+    _check_build(ctx, v, i)
+
+
+@pytest.mark.gpu
+def test_builder_topology_degenerate(ctx):
+    v, i = scenes.degenerate_soup(0)
+    _check_build(ctx, v, i)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("opts", [dict(max_prims=1), dict(max_prims=8, buckets=16), dict(buckets=2),
+                                  dict(alpha=0.0), dict(alpha=1.0), dict(trav_weight=0.0), dict(trav_weight=10.0)])
+def test_builder_topology_options(ctx, opts):
+    v, i = scenes.soup(3000, seed=11, spread=4.0, size=1.5)  # overlapping: spatial splits happen
+    _check_build(ctx, v, i, **opts)
+
+
+@pytest.mark.gpu
+def test_builder_topology_box_room(ctx):
+    import keepsake_b200 as ks
+    g = ks.Generated("box_room", 0)
+    v, i = g.flat_geometry()
+    _check_build(ctx, v, i)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("level", [4, 6, 8])
+def test_builder_topology_icosphere(ctx, level):
+    import keepsake_b200 as ks
+    g = ks.Generated("icosphere", 0, level=level)
+    v, i = g.flat_geometry()
+    _check_build(ctx, v, i)
+
+
+def _check_trace(scene, ref, rays):
+    tri, t, bary = scene.trace(rays)
+    rtri, rt, rbary = ref.intersect(rays)
+    assert np.array_equal(tri, rtri), f"{(tri != rtri).sum()} of {len(rays)} hit ids differ"
+    hit = rtri != 0xFFFFFFFF
+    assert np.array_equal(t[hit].view(np.uint32), rt[hit].view(np.uint32)), "hit distances differ"
+    assert np.array_equal(bary[hit].view(np.uint32), rbary[hit].view(np.uint32)), "barycentrics differ"
+    occ, _, _ = scene.trace(rays, any_hit=True)
+    rocc, _, _ = ref.intersect(rays, any_hit=True)
+    assert np.array_equal(occ, rocc), "occlusion results differ"
+    return hit.mean()
+
+
+@pytest.mark.gpu
+def test_trace_soup_bit_exact(ctx):
+    v, i = scenes.soup(5000, seed=7)
+    s, ref = _check_build(ctx, v, i)
+    _check_trace(s, ref, scenes.random_rays(v, 20000, seed=1))
+    _check_trace(s, ref, scenes.random_rays(v, 20000, seed=2, inside=False))
+    _check_trace(s, ref, scenes.rays_at_triangles(v, i, 20000, seed=3))
+    short = scenes.random_rays(v, 20000, seed=4, tmax=0.7)
+    _check_trace(s, ref, short)
+
+
+@pytest.mark.gpu
+def test_trace_degenerate_bit_exact(ctx):
+    v, i = scenes.degenerate_soup(1)
+    s, ref = _check_build(ctx, v, i)
+    _check_trace(s, ref, scenes.rays_at_triangles(v, i, 20000, seed=5))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("culling", [0, 1])
+def test_trace_culling(ctx, culling):
+    import oracle_lib
+    v, i = scenes.soup(2000, seed=9)
+    s, ref = _check_build(ctx, v, i)
+    rays = scenes.rays_at_triangles(v, i, 10000, seed=6)
+    tri, _, _ = s.trace(rays, culling=culling)
+    rtri, _, _ = ref.intersect(rays, culling=culling)
+    assert np.array_equal(tri, rtri)
+
+
+@pytest.mark.gpu
+def test_trace_icosphere_bit_exact(ctx):
+    import keepsake_b200 as ks
+    g = ks.Generated("icosphere", 0, level=8)
+    v, i = g.flat_geometry()
+    s, ref = _check_build(ctx, v, i)
+    frac = _check_trace(s, ref, scenes.rays_at_triangles(v, i, 200000, seed=8))
+    assert frac > 0.5
+    _check_trace(s, ref, scenes.random_rays(v, 200000, seed=9, inside=False))
