@@ -154,6 +154,63 @@ typedef struct ks_camera_desc {
 ks_status ks_camera_perspective(const float camera_to_world[16], float vfov, float aspect, ks_camera_desc *out);
 
 /* ---------------------------------------------------------------------------------------------
+ * small_pt render parameters: the scalar fields of SmallPTInput (small_pt.h:17-39) with the
+ * TOML defaults of the small_pt task (small_pt.cpp:224-241).
+ * ------------------------------------------------------------------------------------------- */
+typedef struct ks_small_pt_params {
+    int32_t include_background; /* 1 unless the task has a `backdrop` (small_pt.cpp:224-229) */
+    float backdrop[3];
+    int32_t bounces;
+    int32_t render_width;
+    int32_t render_height;
+    int32_t crop_start_x;
+    int32_t crop_start_y;
+    int32_t crop_width;  /* 0 = full frame */
+    int32_t crop_height;
+    int32_t spp;
+    int32_t rng_seed;
+    int32_t scale_ray_diff;
+    float clamp_direct;   /* default 0 (off) */
+    float clamp_indirect; /* default 10 */
+    int32_t spp_prog_interval; /* default 32 */
+    float pixel_filter_width;  /* box filter width (BoxPixelFilter, render_target.h:108-125); default 1 */
+} ks_small_pt_params;
+
+/* Fills the defaults of SmallPTInput (small_pt.h:17-39) and the task (small_pt.cpp:224-241). */
+void ks_small_pt_params_default(ks_small_pt_params *p);
+
+/* Progress callback, called on the caller's thread after every spp interval with the running
+ * FP64 accumulation (prog_interval_callback, small_pt.h:38 and small_pt.cpp:64-66). */
+typedef void (*ks_progress_fn)(int spp_finished, const double *accum_rgb, const double *weights, void *user);
+
+/* SmallPT::run (small_pt.cpp:15-70) on the GPU: wavefront path tracing of the crop window.
+ * accum_rgb (W*H*3) and weights (W*H*2: hit, miss) are caller-owned HOST buffers in the layout
+ * of RenderTarget2 (render_target.h:286-287); the render ADDS into them (FP64), like
+ * RenderTarget2::add / add_miss.  cb may be NULL.  Requires ks_scene_build_bvh. */
+ks_status ks_small_pt_render(ks_scene *scene, const ks_camera_desc *camera, const ks_small_pt_params *params,
+                             ks_progress_fn cb, void *user, double *accum_rgb, double *weights);
+
+/* Same render with DEVICE buffers (W*H*3 and W*H*2 doubles on the context's device), no host
+ * copies and no callback: for callers that keep the image resident in HBM. */
+ks_status ks_small_pt_render_device(ks_scene *scene, const ks_camera_desc *camera, const ks_small_pt_params *params,
+                                    double *accum_rgb_device, double *weights_device);
+
+/* Work and device time of the last render on this scene. */
+typedef struct ks_render_stats {
+    uint64_t paths;          /* camera samples traced */
+    uint64_t extension_rays; /* closest-hit queries (camera + bounce rays) */
+    uint64_t shadow_rays;    /* any-hit queries (next-event estimation) */
+    uint32_t iterations;     /* wavefront iterations */
+    uint32_t kernel_launches;
+    float ms_total;          /* device time of the whole render */
+    float ms_extend;         /* closest-hit kernel time, summed */
+    float ms_shade;          /* shading kernel time (incl. ray generation), summed */
+    float ms_shadow;         /* any-hit kernel time, summed */
+} ks_render_stats;
+
+ks_status ks_render_stats_last(const ks_scene *scene, ks_render_stats *out);
+
+/* ---------------------------------------------------------------------------------------------
  * Procedural scenes: seeded synthetic inputs standing in for mesh-asset loading
  * (mesh_asset.cpp).  kind: "box_room" or "icosphere" (options apply to "icosphere").
  * ------------------------------------------------------------------------------------------- */

@@ -65,11 +65,14 @@ class Context:
     """One CUDA device + stream (ks_context)."""
 
     def __init__(self, device: int = 0):
+        import weakref
         h = _vp()
         st = lib.ks_context_create(device, ctypes.byref(h))
         if st != KS_OK:
             raise KsError(st, "ks_context_create")
         self.handle = h
+        # scenes must be destroyed before their context (ks_scene_destroy uses the context)
+        self._scenes = weakref.WeakSet()
 
     def check(self, st: int, what: str = ""):
         if st != KS_OK:
@@ -77,6 +80,8 @@ class Context:
 
     def close(self):
         if self.handle:
+            for sc in list(self._scenes):
+                sc.close()
             lib.ks_context_destroy(self.handle)
             self.handle = None
 
@@ -137,6 +142,25 @@ class ProceduralOptions(ctypes.Structure):
                 ("sky_width", _u32), ("sky_height", _u32), ("width", _u32), ("height", _u32)]
 
 
+class SmallPTParams(ctypes.Structure):
+    _fields_ = [("include_background", _i32), ("backdrop", _f32 * 3), ("bounces", _i32), ("render_width", _i32),
+                ("render_height", _i32), ("crop_start_x", _i32), ("crop_start_y", _i32), ("crop_width", _i32),
+                ("crop_height", _i32), ("spp", _i32), ("rng_seed", _i32), ("scale_ray_diff", _i32),
+                ("clamp_direct", _f32), ("clamp_indirect", _f32), ("spp_prog_interval", _i32),
+                ("pixel_filter_width", _f32)]
+
+    @classmethod
+    def make(cls, **kw):
+        p = cls()
+        lib.ks_small_pt_params_default(ctypes.byref(p))
+        for k, v in kw.items():
+            if k == "backdrop":
+                p.backdrop[:] = v
+            else:
+                setattr(p, k, v)
+        return p
+
+
 def _sig(name, args, res=ctypes.c_int):
     f = getattr(lib, name)
     f.argtypes = args
@@ -155,6 +179,24 @@ _sig("ks_procedural_scene", [ctypes.c_char_p, ctypes.c_uint64, ctypes.POINTER(Pr
 _sig("ks_generated_scene_desc", [_vp], ctypes.POINTER(SceneDesc))
 _sig("ks_generated_camera", [_vp, ctypes.POINTER(_f32), ctypes.POINTER(_f32), ctypes.POINTER(_f32)])
 _sig("ks_generated_destroy", [_vp], None)
+_sig("ks_small_pt_params_default", [ctypes.POINTER(SmallPTParams)], None)
+
+
+class RenderStats(ctypes.Structure):
+    _fields_ = [("paths", ctypes.c_uint64), ("extension_rays", ctypes.c_uint64), ("shadow_rays", ctypes.c_uint64),
+                ("iterations", _u32), ("kernel_launches", _u32), ("ms_total", _f32), ("ms_extend", _f32),
+                ("ms_shade", _f32), ("ms_shadow", _f32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+PROGRESS_FN = ctypes.CFUNCTYPE(None, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                               ctypes.POINTER(ctypes.c_double), _vp)
+_sig("ks_small_pt_render", [_vp, ctypes.POINTER(CameraDesc), ctypes.POINTER(SmallPTParams), PROGRESS_FN, _vp,
+                            _vp, _vp])
+_sig("ks_small_pt_render_device", [_vp, ctypes.POINTER(CameraDesc), ctypes.POINTER(SmallPTParams), _vp, _vp])
+_sig("ks_render_stats_last", [_vp, ctypes.POINTER(RenderStats)])
 
 
 def _arr(p, n, dtype):
@@ -253,6 +295,7 @@ class Scene:
         dp = desc if isinstance(desc, ctypes.POINTER(SceneDesc)) else ctypes.byref(desc)
         ctx.check(lib.ks_scene_create(ctx.handle, dp, ctypes.byref(h)), "ks_scene_create")
         self.handle = h
+        ctx._scenes.add(self)
 
     def build_bvh(self, max_prims=4, buckets=12, trav_weight=1.0, alpha=1e-5) -> float:
         o = SBVHOptions(max_prims, buckets, trav_weight, alpha)
@@ -282,6 +325,30 @@ class Scene:
         self.ctx.check(lib.ks_trace_rays(self.handle, ptr(rays), n, int(any_hit), culling, ptr(tri), ptr(t),
                                          ptr(bary)), "ks_trace_rays")
         return (tri.astype(bool), None, None) if any_hit else (tri, t, bary)
+
+    def render(self, camera: CameraDesc, params: SmallPTParams, callback=None):
+        """ks_small_pt_render into fresh host FP64 buffers; returns (accum [H,W,3], weights [H,W,2])."""
+        W, H = params.render_width, params.render_height
+        accum = np.zeros((H, W, 3), np.float64)
+        weights = np.zeros((H, W, 2), np.float64)
+        cb = PROGRESS_FN(0)
+        if callback is not None:
+            def _cb(spp, a, w, user):
+                callback(spp, np.ctypeslib.as_array(a, (H, W, 3)).copy(), np.ctypeslib.as_array(w, (H, W, 2)).copy())
+            cb = PROGRESS_FN(_cb)
+        self.ctx.check(lib.ks_small_pt_render(self.handle, ctypes.byref(camera), ctypes.byref(params), cb, None,
+                                              ptr(accum), ptr(weights)), "ks_small_pt_render")
+        return accum, weights
+
+    def render_device(self, camera: CameraDesc, params: SmallPTParams, accum_ptr: int, weights_ptr: int):
+        self.ctx.check(lib.ks_small_pt_render_device(self.handle, ctypes.byref(camera), ctypes.byref(params),
+                                                     ctypes.c_void_p(accum_ptr), ctypes.c_void_p(weights_ptr)),
+                       "ks_small_pt_render_device")
+
+    def stats(self) -> RenderStats:
+        s = RenderStats()
+        self.ctx.check(lib.ks_render_stats_last(self.handle, ctypes.byref(s)), "ks_render_stats_last")
+        return s
 
     def close(self):
         if self.handle:

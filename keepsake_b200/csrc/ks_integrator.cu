@@ -1,0 +1,709 @@
+// Wavefront small_pt integrator for sm_100a.
+//
+// SmallPT::run / trace (small_pt.cpp:15-178) restructured as a streaming wavefront:
+//
+//   raygen  -> new camera paths fill the free queue slots (sample-major over the crop window),
+//   extend  -> closest-hit SBVH traversal, one thread per ray (ks_traverse.cuh),
+//   shade   -> miss/sky MIS, emitter MIS, NEE light sample + BSDF eval (Material::sample_with_nee,
+//              material.cpp:101-167; next_event_estimate, nee.cpp:11-57), BSDF sample, Russian
+//              roulette; surviving paths and shadow rays are appended to compacted SoA queues
+//              with one atomic per warp (ballot + popc),
+//   shadow  -> any-hit traversal of the NEE shadow rays; unoccluded contributions are added to the
+//              path (or, for a path that ended this bounce, the path is accumulated).
+//
+// Per-path arithmetic follows the reference's order: L gains the emitter/sky term of the bounce
+// first, then beta * Ld of the same bounce, then the next bounce's terms, exactly like trace().
+// Sobol dimensions are carried per path (light select, light uv, lobe, wi, roulette: 6 or 7 per
+// bounce), so each path draws the same sample values as the CPU path.  Finished paths are added
+// to FP64 pixel accumulators (RenderTarget2::add / add_miss, render_target.cpp:82-107).
+#include "ks_bsdf.cuh"
+#include "ks_lights.cuh"
+#include "ks_sampler.cuh"
+#include "ks_traverse.cuh"
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+namespace ksb
+{
+SceneView make_view(const ks_scene *s);
+
+namespace
+{
+
+struct RenderParams
+{
+    int W, H, cx, cy, cw, ch;
+    int spp, seed, log2_spp, n_digits;
+    int bounces, include_background;
+    float clamp_direct, clamp_indirect;
+    float filter_r;
+    float cam_pos[3];
+    float p2w[16];
+};
+
+// Path state, structure of arrays, one float4 per field (16-byte vector loads/stores).
+struct PathBuf
+{
+    float4 *o_pdf;    // ray origin, pdf_wi_bsdf of the previous bounce
+    float4 *d_info;   // ray direction, (sobol dimension << 16 | bounce)
+    float4 *beta_pix; // throughput, pixel index
+    float4 *L_smp;    // radiance so far, sample index
+};
+
+struct ShadowBuf
+{
+    float4 *o_tmax;   // origin, tmax
+    float4 *d_target; // direction, target (next-queue slot, or kTermBit | pixel)
+    float4 *contrib;  // beta * clamped Ld
+    float4 *L_term;   // radiance of a path that ended this bounce
+};
+
+constexpr uint32_t kTermBit = 0x80000000u;
+
+KS_D uint32_t bits(float f) { return __float_as_uint(f); }
+KS_D float fbits(uint32_t u) { return __uint_as_float(u); }
+
+// One atomic per warp; every lane of the warp must call this.
+KS_D uint32_t warp_append(uint32_t *counter, bool pred)
+{
+    uint32_t mask = __ballot_sync(0xffffffffu, pred);
+    if (mask == 0)
+        return 0;
+    uint32_t lane = threadIdx.x & 31;
+    int leader = __ffs(mask) - 1;
+    uint32_t base = 0;
+    if ((int)lane == leader)
+        base = atomicAdd(counter, (uint32_t)__popc(mask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    return base + __popc(mask & ((1u << lane) - 1u));
+}
+
+KS_D void accumulate(double *accum, double *weights, uint32_t pix, f3 L)
+{
+    atomicAdd(&weights[2 * (size_t)pix], 1.0);
+    atomicAdd(&accum[3 * (size_t)pix + 0], (double)L.x);
+    atomicAdd(&accum[3 * (size_t)pix + 1], (double)L.y);
+    atomicAdd(&accum[3 * (size_t)pix + 2], (double)L.z);
+}
+
+// ---- hit record (geometry.cpp:68-163 + transform_it with the identity instance) ----------------
+struct ShadeFrame
+{
+    f3 p;
+    f3 t, b, n;    // geometric frame (after re-orthonormalisation)
+    f3 st, sb, sn; // shading frame (flat shading: same as the geometric one)
+};
+
+KS_D void reortho(f3 &t, f3 &b, f3 &n)
+{
+    // Transform::frame (maths.h:989-996) with identity: t' = normalize(t),
+    // b' = normalize(b - dot(b, t') t'), n' = normalize(cross(t', b'))
+    f3 tt = normalize(t);
+    f3 bb = normalize(b - dot(b, tt) * tt);
+    n = normalize(cross(tt, bb));
+    t = tt;
+    b = bb;
+}
+
+KS_D ShadeFrame make_frame(f3 p0, f3 p1, f3 p2, float u, float v, f3 ray_dir, bool twosided)
+{
+    ShadeFrame f;
+    f3 rd = normalize(ray_dir);
+    f3 wo_object = -rd;
+    f3 ng = normalize(cross(p1 - p0, p2 - p0));
+    float w0 = 1.0f - u - v;
+    f.p = w0 * p0 + u * p1 + v * p2;
+    f3 dpdu = p1 - p0;
+    f3 b = normalize(cross(ng, dpdu));
+    f3 t = normalize(cross(b, ng));
+    if (twosided && dot(wo_object, ng) < 0.0f) {
+        ng = -ng;
+        t = -t;
+    }
+    f3 ft = t, fb = b, fn = ng;
+    reortho(ft, fb, fn);
+    f.t = ft;
+    f.b = fb;
+    f.n = fn;
+    // flat shading: sh_frame = frame (geometry.cpp:139-141), re-orthonormalised identically
+    f.st = ft;
+    f.sb = fb;
+    f.sn = fn;
+    return f;
+}
+
+KS_D f3 sh_to_local(const ShadeFrame &f, f3 w)
+{
+    bool hw = dot(f.n, w) >= 0.0f;
+    f3 l = mk(dot(f.st, w), dot(f.sb, w), dot(f.sn, w));
+    bool hl = l.z >= 0.0f;
+    if (hw != hl)
+        l.z *= -1.0f;
+    return l;
+}
+
+KS_D f3 sh_to_world(const ShadeFrame &f, f3 l)
+{
+    bool hl = l.z >= 0.0f;
+    f3 w = f.st * l.x + f.sb * l.y + f.sn * l.z;
+    bool hw = dot(f.n, w) >= 0.0f;
+    if (hl != hw)
+        w = w - 2.0f * dot(f.n, w) * f.n;
+    return w;
+}
+
+// offset_ray (ray.h:66-81)
+KS_D f3 offset_ray(f3 p, f3 n)
+{
+    const float origin = 1.0f / 32.0f, float_scale = 1.0f / 65536.0f, int_scale = 256.0f;
+    int ox = (int)(int_scale * n.x), oy = (int)(int_scale * n.y), oz = (int)(int_scale * n.z);
+    f3 pi = mk(__int_as_float(__float_as_int(p.x) + ((p.x < 0) ? -ox : ox)),
+               __int_as_float(__float_as_int(p.y) + ((p.y < 0) ? -oy : oy)),
+               __int_as_float(__float_as_int(p.z) + ((p.z < 0) ? -oz : oz)));
+    return mk(fabsf(p.x) < origin ? p.x + float_scale * n.x : pi.x,
+              fabsf(p.y) < origin ? p.y + float_scale * n.y : pi.y,
+              fabsf(p.z) < origin ? p.z + float_scale * n.z : pi.z);
+}
+
+// spawn_ray<OffsetType::NextBounce> origin (ray.h:89-96)
+KS_D f3 spawn_origin(f3 p, f3 dir, f3 n) { return offset_ray(p, dot(dir, n) > 0.0f ? n : -n); }
+
+KS_D float power_heur(float pf, float pg)
+{
+    float f2 = pf * pf, g2 = pg * pg;
+    return f2 / (f2 + g2);
+}
+
+KS_D f3 clamp_contrib(f3 v, int bounce_for_direct, const RenderParams &rp, bool is_nee)
+{
+    // trace(): NEE uses bounce==0 -> clamp_direct, bounce>=1 -> clamp_indirect (small_pt.cpp:153-157);
+    // unidirectional hits use bounce==1 -> direct, bounce>=2 -> indirect (:97-103, :128-133).
+    int b = bounce_for_direct;
+    if (is_nee) {
+        if (b == 0 && rp.clamp_direct > 0.0f)
+            return cwise_min(v, rp.clamp_direct);
+        if (b >= 1 && rp.clamp_indirect > 0.0f)
+            return cwise_min(v, rp.clamp_indirect);
+        return v;
+    }
+    if (b == 1 && rp.clamp_direct > 0.0f)
+        return cwise_min(v, rp.clamp_direct);
+    if (b >= 2 && rp.clamp_indirect > 0.0f)
+        return cwise_min(v, rp.clamp_indirect);
+    return v;
+}
+
+KS_D TriVerts tri_verts(const SceneView &s, uint32_t tri)
+{
+    TriVerts tv;
+    uint32_t i0 = __ldg(&s.indices[3 * tri]), i1 = __ldg(&s.indices[3 * tri + 1]),
+             i2 = __ldg(&s.indices[3 * tri + 2]);
+    tv.v0 = mk(__ldg(&s.verts[3 * i0]), __ldg(&s.verts[3 * i0 + 1]), __ldg(&s.verts[3 * i0 + 2]));
+    tv.v1 = mk(__ldg(&s.verts[3 * i1]), __ldg(&s.verts[3 * i1 + 1]), __ldg(&s.verts[3 * i1 + 2]));
+    tv.v2 = mk(__ldg(&s.verts[3 * i2]), __ldg(&s.verts[3 * i2 + 1]), __ldg(&s.verts[3 * i2 + 2]));
+    return tv;
+}
+
+// ---- kernels --------------------------------------------------------------------------------
+
+__global__ void k_raygen(RenderParams rp, PathBuf pb, uint32_t base_slot, uint64_t first_path, uint32_t n_new,
+                         int s0, uint32_t n_pix)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_new)
+        return;
+    uint64_t k = first_path + i;
+    int s = s0 + (int)(k / n_pix);
+    uint32_t pl = (uint32_t)(k % n_pix);
+    int px = rp.cx + (int)(pl % (uint32_t)rp.cw), py = rp.cy + (int)(pl / (uint32_t)rp.cw);
+    SobolSampler smp = SobolSampler::start((uint32_t)px, (uint32_t)py, (uint32_t)s, rp.log2_spp, rp.n_digits,
+                                           (uint32_t)rp.seed, 0);
+    float offx = 0.0f, offy = 0.0f;
+    if (rp.spp != 1) {
+        float u0, u1;
+        smp.next2d(u0, u1);
+        offx = (1.0f - u0) * -rp.filter_r + u0 * rp.filter_r;
+        offy = (1.0f - u1) * -rp.filter_r + u1 * rp.filter_r;
+    }
+    float fx = ((px + 0.5f) + offx) / (float)rp.W;
+    float fy = ((py + 0.5f) + offy) / (float)rp.H;
+    f3 ndc = mk(fx * 2.0f - 1.0f, fy * 2.0f - 1.0f, 1.0f);
+    const float *m = rp.p2w;
+    float o[4];
+    for (int r = 0; r < 4; ++r)
+        o[r] = m[4 * r + 0] * ndc.x + m[4 * r + 1] * ndc.y + m[4 * r + 2] * ndc.z + m[4 * r + 3] * 1.0f;
+    f3 wp = mk(o[0] / o[3], o[1] / o[3], o[2] / o[3]);
+    f3 cp = mk(rp.cam_pos[0], rp.cam_pos[1], rp.cam_pos[2]);
+    f3 dir = normalize(wp - cp);
+    uint32_t slot = base_slot + i;
+    uint32_t pix = (uint32_t)py * (uint32_t)rp.W + (uint32_t)px;
+    pb.o_pdf[slot] = make_float4(cp.x, cp.y, cp.z, 0.0f);
+    pb.d_info[slot] = make_float4(dir.x, dir.y, dir.z, fbits(((uint32_t)smp.dimension << 16) | 0u));
+    pb.beta_pix[slot] = make_float4(1.0f, 1.0f, 1.0f, fbits(pix));
+    pb.L_smp[slot] = make_float4(0.0f, 0.0f, 0.0f, fbits((uint32_t)s));
+}
+
+__global__ void __launch_bounds__(128) k_extend(SceneView sv, PathBuf pb, uint32_t count, float4 *hits,
+                                                int *overflow)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        float4 a = pb.o_pdf[i], b = pb.d_info[i];
+        RayQuery q;
+        q.o = mk(a.x, a.y, a.z);
+        q.d = mk(b.x, b.y, b.z);
+        q.tmin = 0.0f;
+        q.tmax = kInf;
+        Hit h;
+        int of = 0;
+        traverse<false>(sv.nodes, sv.prim_tris, sv.root_ref, sv.root_count, sv.bmin, sv.bmax, q, 2, h, of);
+        if (of)
+            atomicOr(overflow, 1);
+        hits[i] = h.tri != ~0u ? make_float4(h.t, h.b1, h.b2, fbits(h.slot)) : make_float4(0, 0, 0, fbits(~0u));
+    }
+}
+
+__global__ void __launch_bounds__(128) k_shade(SceneView sv, RenderParams rp, PathBuf cur, PathBuf nxt,
+                                               const float4 *hits, uint32_t count, uint32_t *next_count,
+                                               ShadowBuf sb, uint32_t *shadow_count, double *accum,
+                                               double *weights)
+{
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += stride) {
+        uint32_t i = base + threadIdx.x;
+        bool valid = i < count;
+        bool cont = false, shadow = false;
+        // outputs
+        f3 n_o, n_d, n_beta, L = mk(0, 0, 0), sh_o, sh_d, sh_c;
+        float n_pdf = 0.0f, sh_tmax = 0.0f;
+        uint32_t n_info = 0, pix = 0, smp = 0;
+        bool finish = false, miss_only = false;
+        if (valid) {
+            float4 a = cur.o_pdf[i], b = cur.d_info[i], c = cur.beta_pix[i], d = cur.L_smp[i];
+            f3 ro = mk(a.x, a.y, a.z), rd = mk(b.x, b.y, b.z);
+            float pdf_wi_bsdf = a.w;
+            uint32_t info = bits(b.w);
+            int bounce = (int)(info & 0xffffu);
+            int dim = (int)(info >> 16);
+            f3 beta = mk(c.x, c.y, c.z);
+            pix = bits(c.w);
+            L = mk(d.x, d.y, d.z);
+            smp = bits(d.w);
+            float4 h = hits[i];
+            uint32_t slot = bits(h.w);
+            if (slot == ~0u) {
+                // miss: unidirectional sky strategy (small_pt.cpp:83-110)
+                if (sv.sky_kind != 0) {
+                    f3 wi = normalize(rd);
+                    f3 Le = sky_eval(sv, wi);
+                    if (bounce == 0) {
+                        if (rp.include_background)
+                            L += beta * Le;
+                    } else {
+                        float pr_light = light_probability(sv, 0);
+                        float pdf_wi_light = sky_pdf(sv, wi);
+                        float mis = power_heur(pdf_wi_bsdf, pdf_wi_light * pr_light);
+                        f3 beta_uni = clamp_contrib(Le * mis, bounce, rp, false);
+                        L += beta * beta_uni;
+                    }
+                }
+                finish = true;
+                if (bounce == 0 && !rp.include_background)
+                    miss_only = true;
+            } else {
+                const float4 *pt = sv.prim_tris + 3 * (size_t)slot;
+                float4 v0 = __ldg(pt), v1 = __ldg(pt + 1), v2 = __ldg(pt + 2);
+                uint32_t tri = bits(v0.w);
+                f3 p0 = mk(v0.x, v0.y, v0.z), p1 = mk(v1.x, v1.y, v1.z), p2 = mk(v2.x, v2.y, v2.z);
+                uint32_t mesh = __ldg(&sv.tri_mesh[tri]);
+                const MaterialGPU &mat = sv.materials[__ldg(&sv.mesh_material[mesh])];
+                ShadeFrame it = make_frame(p0, p1, p2, h.y, h.z, rd, __ldg(&sv.mesh_twosided[mesh]) != 0);
+                // emitter hit (small_pt.cpp:112-138)
+                if (mat.has_emission && sv.tri_light) {
+                    int32_t light = __ldg(&sv.tri_light[tri]);
+                    if (light >= 0) {
+                        uint32_t k = (uint32_t)light - sv.n_nonmesh;
+                        float4 e = __ldg(&sv.ml_emission[k]);
+                        f3 Le = mk(e.x, e.y, e.z);
+                        if (bounce == 0) {
+                            L += beta * Le;
+                        } else {
+                            float pr_light = light_probability(sv, (uint32_t)light);
+                            if (pr_light > 0.0f) {
+                                f3 wi = normalize(rd);
+                                TriVerts tv{p0, p1, p2};
+                                float pdf_wi_light = mesh_light_pdf(sv, k, tv, wi, h.x);
+                                float mis = power_heur(pdf_wi_bsdf, pdf_wi_light * pr_light);
+                                f3 beta_uni = clamp_contrib(Le * mis, bounce, rp, false);
+                                L += beta * beta_uni;
+                            }
+                        }
+                    }
+                }
+                if (bounce == rp.bounces) {
+                    finish = true;
+                } else {
+                    f3 wo = -normalize(rd);
+                    Principled bsdf{make_closure(mat)};
+                    uint32_t px = pix % (uint32_t)rp.W, py = pix / (uint32_t)rp.W;
+                    SobolSampler sampler =
+                        SobolSampler::start(px, py, smp, rp.log2_spp, rp.n_digits, (uint32_t)rp.seed, dim);
+                    // next_event_estimate (nee.cpp:11-57)
+                    float ul = sampler.next();
+                    uint32_t light = cdf_find(sv.power_cdf, sv.light_count, clamp_u(ul));
+                    float pr_light = sv.power_cdf[light + 1] - sv.power_cdf[light];
+                    float u0, u1;
+                    sampler.next2d(u0, u1);
+                    f3 wi = mk(0, 0, 0);
+                    float wi_dist = 0.0f, pdf_wi_light = 0.0f;
+                    f3 Le_beta;
+                    if (light < sv.n_nonmesh) {
+                        Le_beta = sky_sample(sv, u0, u1, wi, wi_dist, pdf_wi_light);
+                    } else {
+                        uint32_t k = light - sv.n_nonmesh;
+                        TriVerts tv = tri_verts(sv, __ldg(&sv.ml_tri[k]));
+                        Le_beta = mesh_light_sample(sv, k, tv, it.p, u0, u1, wi, wi_dist, pdf_wi_light);
+                    }
+                    if (!is_zero(Le_beta) && pdf_wi_light > 0.0f) {
+                        f3 wo_l = sh_to_local(it, wo), wi_l = sh_to_local(it, wi);
+                        f3 f;
+                        float pdf_b;
+                        bsdf.eval_and_pdf(wo_l, wi_l, f, pdf_b);
+                        if (!is_zero(f) && pdf_b > 0.0f) {
+                            float mis = power_heur(pdf_wi_light, pdf_b);
+                            f3 Ld = Le_beta * f * mis / pr_light;
+                            Ld = clamp_contrib(Ld, bounce, rp, true);
+                            shadow = true;
+                            sh_o = spawn_origin(it.p, wi, it.n);
+                            sh_d = wi;
+                            sh_tmax = wi_dist;
+                            sh_c = beta * Ld;
+                        }
+                    }
+                    // BSDF sampling (material.cpp:155-166)
+                    f3 wo_local = sh_to_local(it, wo);
+                    float u_lobe = sampler.next();
+                    float b0, b1;
+                    sampler.next2d(b0, b1);
+                    f3 wi_local;
+                    float pdf_wi = 0.0f;
+                    f3 sbeta = bsdf.sample(wo_local, wi_local, u_lobe, b0, b1, pdf_wi);
+                    f3 nbeta = beta * sbeta;
+                    if (max3(nbeta) == 0.0f) {
+                        finish = true;
+                    } else {
+                        f3 wnext = sh_to_world(it, wi_local);
+                        n_o = spawn_origin(it.p, wnext, it.n);
+                        n_d = wnext;
+                        n_pdf = pdf_wi;
+                        // Russian roulette (small_pt.cpp:168-175)
+                        if (max3(nbeta) < 1.0f && bounce >= 1) {
+                            float q = 1.0f - max3(nbeta);
+                            q = q < 0.0f ? 0.0f : q;
+                            if (sampler.next() < q)
+                                finish = true;
+                            else
+                                nbeta /= 1.0f - q;
+                        }
+                        if (!finish) {
+                            cont = true;
+                            n_beta = nbeta;
+                            n_info = ((uint32_t)sampler.dimension << 16) | (uint32_t)(bounce + 1);
+                        }
+                    }
+                }
+            }
+        }
+        uint32_t jc = warp_append(next_count, cont);
+        uint32_t js = warp_append(shadow_count, shadow);
+        if (cont) {
+            nxt.o_pdf[jc] = make_float4(n_o.x, n_o.y, n_o.z, n_pdf);
+            nxt.d_info[jc] = make_float4(n_d.x, n_d.y, n_d.z, fbits(n_info));
+            nxt.beta_pix[jc] = make_float4(n_beta.x, n_beta.y, n_beta.z, fbits(pix));
+            nxt.L_smp[jc] = make_float4(L.x, L.y, L.z, fbits(smp));
+        }
+        if (shadow) {
+            sb.o_tmax[js] = make_float4(sh_o.x, sh_o.y, sh_o.z, sh_tmax);
+            sb.d_target[js] = make_float4(sh_d.x, sh_d.y, sh_d.z, fbits(cont ? jc : (kTermBit | pix)));
+            sb.contrib[js] = make_float4(sh_c.x, sh_c.y, sh_c.z, 0.0f);
+            if (!cont)
+                sb.L_term[js] = make_float4(L.x, L.y, L.z, 0.0f);
+        }
+        if (valid && !cont && !shadow) {
+            if (miss_only)
+                atomicAdd(&weights[2 * (size_t)pix + 1], 1.0);
+            else
+                accumulate(accum, weights, pix, L);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(128) k_shadow(SceneView sv, ShadowBuf sb, const uint32_t *shadow_count,
+                                                PathBuf nxt, double *accum, double *weights, int *overflow)
+{
+    const uint32_t n = *shadow_count;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float4 a = sb.o_tmax[i], b = sb.d_target[i];
+        RayQuery q;
+        q.o = mk(a.x, a.y, a.z);
+        q.d = mk(b.x, b.y, b.z);
+        q.tmin = 0.0f;
+        q.tmax = a.w;
+        Hit h;
+        int of = 0;
+        bool occ = traverse<true>(sv.nodes, sv.prim_tris, sv.root_ref, sv.root_count, sv.bmin, sv.bmax, q, 2, h, of);
+        if (of)
+            atomicOr(overflow, 1);
+        uint32_t target = bits(b.w);
+        float4 c = sb.contrib[i];
+        if (target & kTermBit) {
+            float4 l = sb.L_term[i];
+            f3 L = mk(l.x, l.y, l.z);
+            if (!occ)
+                L += mk(c.x, c.y, c.z);
+            accumulate(accum, weights, target & ~kTermBit, L);
+        } else if (!occ) {
+            float4 l = nxt.L_smp[target];
+            l.x += c.x;
+            l.y += c.y;
+            l.z += c.z;
+            nxt.L_smp[target] = l;
+        }
+    }
+}
+
+} // namespace
+} // namespace ksb
+
+using namespace ksb;
+
+struct RenderWork
+{
+    DevBuf<float4> state[2][4];
+    DevBuf<float4> hits;
+    DevBuf<float4> shadow[4];
+    DevBuf<uint32_t> counters; // [next, shadow]
+    DevBuf<int> overflow;
+    uint32_t capacity = 0;
+};
+
+static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const ks_small_pt_params *in,
+                             ks_progress_fn cb, void *user, double *d_accum, double *d_weights, double *h_accum,
+                             double *h_weights)
+{
+    ks_context *ctx = scene->ctx;
+    cudaStream_t st = ctx->stream;
+    if (!scene->bvh_built || !scene->lights_built)
+        return fail(ctx, KS_ERR_NOT_BUILT, "ks_small_pt_render: call ks_scene_build_bvh first");
+    if (scene->light_count == 0)
+        return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_small_pt_render: the scene has no light");
+    const int W = in->render_width, H = in->render_height;
+    if (W <= 0 || H <= 0 || in->spp <= 0 || in->bounces < 0 || in->bounces > 0xfffe || in->spp_prog_interval <= 0)
+        return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_small_pt_render: bad resolution, spp, bounces or interval");
+    if ((uint64_t)W * H >= (1ull << 31))
+        return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_small_pt_render: resolution too large");
+    RenderParams rp{};
+    rp.W = W;
+    rp.H = H;
+    rp.cx = 0;
+    rp.cy = 0;
+    rp.cw = W;
+    rp.ch = H;
+    if (in->crop_width > 0 && in->crop_height > 0) {
+        rp.cx = std::max(in->crop_start_x, 0);
+        rp.cy = std::max(in->crop_start_y, 0);
+        rp.cw = std::min(in->crop_width, W - rp.cx);
+        rp.ch = std::min(in->crop_height, H - rp.cy);
+        if (rp.cw <= 0 || rp.ch <= 0)
+            return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_small_pt_render: empty crop window");
+    }
+    rp.spp = in->spp;
+    rp.seed = in->rng_seed;
+    sobol_setup(in->spp, W, H, rp.log2_spp, rp.n_digits);
+    rp.bounces = in->bounces;
+    rp.include_background = in->include_background;
+    rp.clamp_direct = in->clamp_direct;
+    rp.clamp_indirect = in->clamp_indirect;
+    rp.filter_r = 0.5f * (in->pixel_filter_width > 0.0f ? in->pixel_filter_width : 1.0f);
+    rp.cam_pos[0] = cam->camera_to_world[3];
+    rp.cam_pos[1] = cam->camera_to_world[7];
+    rp.cam_pos[2] = cam->camera_to_world[11];
+    std::memcpy(rp.p2w, cam->proj_to_world, sizeof(rp.p2w));
+
+    SceneView sv = make_view(scene);
+    const uint32_t n_pix = (uint32_t)rp.cw * (uint32_t)rp.ch;
+    const uint64_t max_interval = (uint64_t)n_pix * (uint64_t)std::min(in->spp, in->spp_prog_interval);
+    RenderWork w;
+    w.capacity = (uint32_t)std::min<uint64_t>(max_interval, 1u << 22);
+    for (int b = 0; b < 2; ++b)
+        for (int f = 0; f < 4; ++f)
+            KS_CUDA_TRY(ctx, w.state[b][f].alloc(w.capacity));
+    KS_CUDA_TRY(ctx, w.hits.alloc(w.capacity));
+    for (int f = 0; f < 4; ++f)
+        KS_CUDA_TRY(ctx, w.shadow[f].alloc(w.capacity));
+    KS_CUDA_TRY(ctx, w.counters.alloc(2));
+    KS_CUDA_TRY(ctx, w.overflow.alloc(1));
+    KS_CUDA_TRY(ctx, cudaMemsetAsync(w.overflow.ptr, 0, sizeof(int), st));
+    PathBuf pb[2];
+    for (int b = 0; b < 2; ++b)
+        pb[b] = PathBuf{w.state[b][0].ptr, w.state[b][1].ptr, w.state[b][2].ptr, w.state[b][3].ptr};
+    ShadowBuf sb{w.shadow[0].ptr, w.shadow[1].ptr, w.shadow[2].ptr, w.shadow[3].ptr};
+    uint32_t *h_counts = nullptr;
+    KS_CUDA_TRY(ctx, cudaMallocHost((void **)&h_counts, sizeof(uint32_t) * 2));
+    cudaEvent_t ev[5];
+    for (auto &e : ev)
+        cudaEventCreate(&e);
+    cudaEvent_t t_begin, t_end;
+    cudaEventCreate(&t_begin);
+    cudaEventCreate(&t_end);
+    cudaEventRecord(t_begin, st);
+    ks_render_stats stats{};
+    const unsigned max_grid = (unsigned)ctx->sm_count * 16;
+    int cur = 0;
+    cudaError_t err = cudaSuccess;
+    std::vector<double> cb_acc, cb_w;
+    for (int s0 = 0; s0 < in->spp && err == cudaSuccess; s0 += in->spp_prog_interval) {
+        int batch = std::min(in->spp_prog_interval, in->spp - s0);
+        uint64_t total = (uint64_t)n_pix * (uint64_t)batch, issued = 0;
+        uint32_t cur_count = 0;
+        // every path ends after at most bounces + 1 extension rays
+        const uint64_t watchdog = (total / w.capacity + 2) * (uint64_t)(in->bounces + 2) + 64;
+        uint64_t it_interval = 0;
+        while ((issued < total || cur_count > 0) && err == cudaSuccess) {
+            if (++it_interval > watchdog) {
+                err = cudaErrorUnknown;
+                stats.iterations = 0xffffffffu;
+                break;
+            }
+            uint32_t n_new = (uint32_t)std::min<uint64_t>(w.capacity - cur_count, total - issued);
+            cudaEventRecord(ev[0], st);
+            if (n_new) {
+                k_raygen<<<(n_new + 255) / 256, 256, 0, st>>>(rp, pb[cur], cur_count, issued, n_new, s0, n_pix);
+                stats.kernel_launches++;
+            }
+            issued += n_new;
+            uint32_t count = cur_count + n_new;
+            stats.extension_rays += count;
+            cudaMemsetAsync(w.counters.ptr, 0, sizeof(uint32_t) * 2, st);
+            unsigned grid = std::min<unsigned>((count + 127) / 128, max_grid);
+            cudaEventRecord(ev[1], st);
+            k_extend<<<grid, 128, 0, st>>>(sv, pb[cur], count, w.hits.ptr, w.overflow.ptr);
+            cudaEventRecord(ev[2], st);
+            k_shade<<<grid, 128, 0, st>>>(sv, rp, pb[cur], pb[1 - cur], w.hits.ptr, count, w.counters.ptr, sb,
+                                          w.counters.ptr + 1, d_accum, d_weights);
+            cudaEventRecord(ev[3], st);
+            k_shadow<<<grid, 128, 0, st>>>(sv, sb, w.counters.ptr + 1, pb[1 - cur], d_accum, d_weights,
+                                           w.overflow.ptr);
+            cudaEventRecord(ev[4], st);
+            stats.kernel_launches += 3;
+            cudaMemcpyAsync(h_counts, w.counters.ptr, sizeof(uint32_t) * 2, cudaMemcpyDeviceToHost, st);
+            err = cudaStreamSynchronize(st);
+            if (err != cudaSuccess)
+                break;
+            err = cudaGetLastError();
+            float ms;
+            cudaEventElapsedTime(&ms, ev[0], ev[1]);
+            stats.ms_shade += ms;
+            cudaEventElapsedTime(&ms, ev[1], ev[2]);
+            stats.ms_extend += ms;
+            cudaEventElapsedTime(&ms, ev[2], ev[3]);
+            stats.ms_shade += ms;
+            cudaEventElapsedTime(&ms, ev[3], ev[4]);
+            stats.ms_shadow += ms;
+            stats.shadow_rays += h_counts[1];
+            stats.iterations++;
+            cur_count = h_counts[0];
+            cur = 1 - cur;
+        }
+        stats.paths += total;
+        if (err == cudaSuccess && cb && h_accum) {
+            size_t na = (size_t)W * H * 3, nw = (size_t)W * H * 2;
+            cb_acc.resize(na);
+            cb_w.resize(nw);
+            err = cudaMemcpyAsync(cb_acc.data(), d_accum, na * sizeof(double), cudaMemcpyDeviceToHost, st);
+            if (err == cudaSuccess)
+                err = cudaMemcpyAsync(cb_w.data(), d_weights, nw * sizeof(double), cudaMemcpyDeviceToHost, st);
+            if (err == cudaSuccess)
+                err = cudaStreamSynchronize(st);
+            if (err == cudaSuccess) {
+                // the callback sees the caller's running totals (initial contents + this render)
+                for (size_t k = 0; k < na; ++k)
+                    cb_acc[k] += h_accum[k];
+                for (size_t k = 0; k < nw; ++k)
+                    cb_w[k] += h_weights[k];
+                cb(s0 + batch, cb_acc.data(), cb_w.data(), user);
+            }
+        }
+    }
+    cudaEventRecord(t_end, st);
+    cudaEventSynchronize(t_end);
+    cudaEventElapsedTime(&stats.ms_total, t_begin, t_end);
+    for (auto &e : ev)
+        cudaEventDestroy(e);
+    cudaEventDestroy(t_begin);
+    cudaEventDestroy(t_end);
+    int overflow = 0;
+    if (err == cudaSuccess)
+        err = cudaMemcpy(&overflow, w.overflow.ptr, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFreeHost(h_counts);
+    scene->last_stats = stats;
+    if (stats.iterations == 0xffffffffu)
+        return fail(ctx, KS_ERR_WATCHDOG, "ks_small_pt_render: wavefront iteration limit reached");
+    if (err != cudaSuccess)
+        return cuda_fail(ctx, err, "ks_small_pt_render");
+    if (overflow)
+        return fail(ctx, KS_ERR_QUEUE_OVERFLOW, "ks_small_pt_render: traversal stack depth exceeded");
+    return KS_OK;
+}
+
+extern "C" {
+
+ks_status ks_small_pt_render_device(ks_scene *scene, const ks_camera_desc *camera, const ks_small_pt_params *params,
+                                    double *accum_rgb_device, double *weights_device)
+{
+    if (!scene || !camera || !params || !accum_rgb_device || !weights_device)
+        return fail(scene ? scene->ctx : nullptr, KS_ERR_INVALID_ARGUMENT, "ks_small_pt_render_device: null");
+    KS_CUDA_TRY(scene->ctx, cudaSetDevice(scene->ctx->device));
+    return render_impl(scene, camera, params, nullptr, nullptr, accum_rgb_device, weights_device, nullptr, nullptr);
+}
+
+ks_status ks_small_pt_render(ks_scene *scene, const ks_camera_desc *camera, const ks_small_pt_params *params,
+                             ks_progress_fn cb, void *user, double *accum_rgb, double *weights)
+{
+    if (!scene || !camera || !params || !accum_rgb || !weights)
+        return fail(scene ? scene->ctx : nullptr, KS_ERR_INVALID_ARGUMENT, "ks_small_pt_render: null");
+    ks_context *ctx = scene->ctx;
+    KS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    if (params->render_width <= 0 || params->render_height <= 0)
+        return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_small_pt_render: bad resolution");
+    size_t na = (size_t)params->render_width * params->render_height * 3;
+    size_t nw = (size_t)params->render_width * params->render_height * 2;
+    DevBuf<double> da, dw;
+    KS_CUDA_TRY(ctx, da.alloc(na));
+    KS_CUDA_TRY(ctx, dw.alloc(nw));
+    KS_CUDA_TRY(ctx, cudaMemsetAsync(da.ptr, 0, na * sizeof(double), ctx->stream));
+    KS_CUDA_TRY(ctx, cudaMemsetAsync(dw.ptr, 0, nw * sizeof(double), ctx->stream));
+    ks_status s = render_impl(scene, camera, params, cb, user, da.ptr, dw.ptr, accum_rgb, weights);
+    if (s != KS_OK)
+        return s;
+    std::vector<double> ha(na), hw(nw);
+    KS_CUDA_TRY(ctx, cudaMemcpyAsync(ha.data(), da.ptr, na * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    KS_CUDA_TRY(ctx, cudaMemcpyAsync(hw.data(), dw.ptr, nw * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    KS_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    for (size_t k = 0; k < na; ++k)
+        accum_rgb[k] += ha[k];
+    for (size_t k = 0; k < nw; ++k)
+        weights[k] += hw[k];
+    return KS_OK;
+}
+
+ks_status ks_render_stats_last(const ks_scene *scene, ks_render_stats *out)
+{
+    if (!scene || !out)
+        return KS_ERR_INVALID_ARGUMENT;
+    *out = scene->last_stats;
+    return KS_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,376 @@
+// Light tables: sky distribution (GPU), sky power (GPU), mesh-light importance (host, a handful of
+// emissive triangles), and the PowerLightSampler CDF.
+//
+//   SkyLight::SkyLight (light.cpp:19-49): lum = sin(theta) * luminance, threshold at the mean,
+//     DistribTable2D of the thresholded values.  The conditional CDFs are float prefix sums in
+//     index order, exactly as DistribTable (distrib.cpp:9-29): one GPU thread per row keeps the
+//     reference's summation order, so the table is bit-identical to a sequential host build.
+//     The mean is a double sum (rows in order) - the reference uses an unordered float atomic.
+//   SkyLight::power (light.cpp:136-159): float row sums in column order (one thread per row),
+//     rows added in order in double.
+//   compute_mesh_light_importance (light.cpp:307-414), uniform emission branch, and the
+//     zero-importance compaction of MeshLightShared (light.cpp:524-560).
+//   PowerLightSampler::build (light.cpp:636-672).
+#include "ks_lights.cuh"
+#include "ks_scene.h"
+
+#include <cmath>
+#include <cstring>
+
+namespace ksb
+{
+namespace
+{
+
+__global__ void k_sky_rows(const float4 *map, int w, int h, const float *row_sin, float *lum, double *row_sum)
+{
+    int y = blockIdx.x * blockDim.x + threadIdx.x;
+    if (y >= h)
+        return;
+    float st = row_sin[y];
+    double s = 0.0;
+    for (int x = 0; x < w; ++x) {
+        float4 c = map[(size_t)y * w + x];
+        float l = st * luminance(mk(c.x, c.y, c.z));
+        lum[(size_t)y * w + x] = l;
+        s += l;
+    }
+    row_sum[y] = s;
+}
+
+// DistribTable(f, n) per row with f = max(lum - average, 0) (distrib.cpp:9-29).
+__global__ void k_sky_cond(const float *lum, int w, int h, float average, float *cond, float *acc, int threshold)
+{
+    int y = blockIdx.x * blockDim.x + threadIdx.x;
+    if (y >= h)
+        return;
+    float *cdf = cond + (size_t)y * (w + 1);
+    const float *f = lum + (size_t)y * w;
+    cdf[0] = 0.0f;
+    float invn = 1.0f / (float)w;
+    for (int i = 1; i < w + 1; ++i) {
+        float v = f[i - 1];
+        if (threshold) {
+            v = v - average;
+            v = v < 0.0f ? 0.0f : v; // std::max(lum - average, 0.0f)
+        }
+        cdf[i] = cdf[i - 1] + v * invn;
+    }
+    float a = cdf[w];
+    acc[y] = a;
+    if (a == 0.0f) {
+        for (int i = 0; i < w + 1; ++i)
+            cdf[i] = (float)i / (float)w;
+    } else {
+        float inva = 1.0f / a;
+        for (int i = 0; i < w + 1; ++i)
+            cdf[i] *= inva;
+    }
+    cdf[w] = 1.0f;
+}
+
+// Row sums of SkyLight::power (light.cpp:140-153); eval() through the same device code as shading.
+__global__ void k_sky_power_rows(SceneView s, double *row_sums)
+{
+    int row = blockIdx.x * blockDim.x + threadIdx.x;
+    if (row >= s.sky_h)
+        return;
+    float theta = (row + 0.5f) / (float)s.sky_h * kPi;
+    float sin_theta = sinf(theta);
+    f3 rs = mk(0, 0, 0);
+    for (int col = 0; col < s.sky_w; ++col) {
+        float phi = (col + 0.5f) / (float)s.sky_w * kTwoPi;
+        float ct = cosf(theta), st = sinf(theta), cp = cosf(phi), sp = sinf(phi);
+        f3 dir = mk(cp * st, sp * st, ct); // to_cartesian (z up), as the reference does here
+        rs += sky_eval(s, dir) * sin_theta;
+    }
+    row_sums[3 * row + 0] = rs.x;
+    row_sums[3 * row + 1] = rs.y;
+    row_sums[3 * row + 2] = rs.z;
+}
+
+// DistribTable on the host, identical to distrib.cpp:9-29.
+std::vector<float> host_cdf(const float *f, uint32_t n, float *acc_out = nullptr)
+{
+    std::vector<float> cdf(n + 1);
+    cdf[0] = 0;
+    float invn = 1.0f / (float)n;
+    for (uint32_t i = 1; i < n + 1; ++i)
+        cdf[i] = cdf[i - 1] + f[i - 1] * invn;
+    float acc = cdf[n];
+    if (acc == 0.0f) {
+        for (uint32_t i = 0; i < n + 1; ++i)
+            cdf[i] = (float)i / (float)n;
+    } else {
+        float invacc = 1.0f / acc;
+        for (uint32_t i = 0; i < n + 1; ++i)
+            cdf[i] *= invacc;
+    }
+    cdf[n] = 1.0f;
+    if (acc_out)
+        *acc_out = acc;
+    return cdf;
+}
+
+bool invert4(const float *m, float *out)
+{
+    double a[4][8];
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 8; ++c)
+            a[r][c] = c < 4 ? m[4 * r + c] : (c - 4 == r ? 1.0 : 0.0);
+    for (int col = 0; col < 4; ++col) {
+        int piv = col;
+        for (int r = col + 1; r < 4; ++r)
+            if (std::fabs(a[r][col]) > std::fabs(a[piv][col]))
+                piv = r;
+        if (a[piv][col] == 0.0)
+            return false;
+        for (int c = 0; c < 8; ++c)
+            std::swap(a[piv][c], a[col][c]);
+        double inv = 1.0 / a[col][col];
+        for (int c = 0; c < 8; ++c)
+            a[col][c] *= inv;
+        for (int r = 0; r < 4; ++r)
+            if (r != col) {
+                double f = a[r][col];
+                for (int c = 0; c < 8; ++c)
+                    a[r][c] -= f * a[col][c];
+            }
+    }
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c)
+            out[4 * r + c] = (float)a[r][c + 4];
+    return true;
+}
+
+} // namespace
+
+SceneView make_view(const ks_scene *s)
+{
+    SceneView v{};
+    v.nodes = s->trav_nodes.ptr;
+    v.prim_tris = s->prim_tris.ptr;
+    v.verts = s->verts.ptr;
+    v.indices = s->indices.ptr;
+    v.root_ref = s->root_ref;
+    v.root_count = s->root_count;
+    for (int k = 0; k < 3; ++k) {
+        v.bmin[k] = s->scene_bound[k];
+        v.bmax[k] = s->scene_bound[3 + k];
+    }
+    v.tri_mesh = s->tri_mesh.ptr;
+    v.mesh_material = s->mesh_material.ptr;
+    v.mesh_twosided = s->mesh_twosided.ptr;
+    v.materials = s->materials.ptr;
+    v.light_count = s->light_count;
+    v.n_nonmesh = s->n_nonmesh;
+    v.power_cdf = s->power_cdf.ptr;
+    v.tri_light = s->tri_light.ptr;
+    v.ml_tri = s->ml_tri.ptr;
+    v.ml_area = s->ml_area.ptr;
+    v.ml_emission = s->ml_emission.ptr;
+    v.sky_kind = s->sky_desc.kind;
+    v.sky_w = s->sky_w;
+    v.sky_h = s->sky_h;
+    std::memcpy(v.sky_l2w, s->sky_l2w, sizeof(v.sky_l2w));
+    std::memcpy(v.sky_w2l, s->sky_w2l, sizeof(v.sky_w2l));
+    v.sky_y_up = s->sky_desc.kind == 2 ? s->sky_desc.transform_y_up : 1;
+    v.sky_strength = s->sky_desc.kind == 2 ? s->sky_desc.strength : 1.0f;
+    v.sky_map = s->sky_map.ptr;
+    v.sky_cond = s->sky_cond.ptr;
+    v.sky_margin = s->sky_margin.ptr;
+    return v;
+}
+
+ks_status build_lights(ks_scene *s)
+{
+    ks_context *ctx = s->ctx;
+    cudaStream_t st = ctx->stream;
+    const ks_sky_desc &sd = s->sky_desc;
+    // ---- sky distribution ----
+    s->n_nonmesh = 0;
+    float sky_power_mean = 0.0f;
+    if (sd.kind == 1 || sd.kind == 2) {
+        s->n_nonmesh = 1;
+        int w, h;
+        std::vector<float4> map;
+        if (sd.kind == 1) {
+            w = h = 1;
+            map = {make_float4(sd.ambient[0], sd.ambient[1], sd.ambient[2], 0.0f)};
+        } else {
+            w = (int)sd.width;
+            h = (int)sd.height;
+            map.resize((size_t)w * h);
+            for (size_t i = 0; i < map.size(); ++i)
+                map[i] = make_float4(s->h_sky_map[3 * i], s->h_sky_map[3 * i + 1], s->h_sky_map[3 * i + 2], 0.0f);
+            float m4[16], inv4[16];
+            std::memcpy(m4, sd.to_world, sizeof(m4));
+            if (!invert4(m4, inv4))
+                return fail(ctx, KS_ERR_INVALID_ARGUMENT, "sky to_world is singular");
+            for (int r = 0; r < 3; ++r)
+                for (int c = 0; c < 3; ++c) {
+                    s->sky_l2w[3 * r + c] = m4[4 * r + c];
+                    s->sky_w2l[3 * r + c] = inv4[4 * r + c];
+                }
+        }
+        s->sky_w = w;
+        s->sky_h = h;
+        KS_CUDA_TRY(ctx, s->sky_map.alloc(map.size()));
+        KS_CUDA_TRY(ctx, cudaMemcpyAsync(s->sky_map.ptr, map.data(), s->sky_map.bytes(), cudaMemcpyHostToDevice, st));
+        KS_CUDA_TRY(ctx, s->sky_cond.alloc((size_t)h * (w + 1)));
+        DevBuf<float> lum, acc, row_sin;
+        DevBuf<double> row_sum;
+        KS_CUDA_TRY(ctx, lum.alloc((size_t)w * h));
+        KS_CUDA_TRY(ctx, acc.alloc(h));
+        KS_CUDA_TRY(ctx, row_sin.alloc(h));
+        KS_CUDA_TRY(ctx, row_sum.alloc((size_t)3 * h));
+        std::vector<float> h_sin(h);
+        const float pi = 3.14159265359f;
+        for (int y = 0; y < h; ++y)
+            h_sin[y] = std::sin((y + 0.5f) / (float)h * pi); // host libm, like the reference
+        if (sd.kind == 1)
+            h_sin[0] = 1.0f; // the ambient constructor uses plain luminance (light.cpp:52-57)
+        KS_CUDA_TRY(ctx, cudaMemcpyAsync(row_sin.ptr, h_sin.data(), sizeof(float) * h, cudaMemcpyHostToDevice, st));
+        k_sky_rows<<<(h + 127) / 128, 128, 0, st>>>(s->sky_map.ptr, w, h, row_sin.ptr, lum.ptr, row_sum.ptr);
+        std::vector<double> h_rows(h);
+        KS_CUDA_TRY(ctx, cudaMemcpyAsync(h_rows.data(), row_sum.ptr, sizeof(double) * h, cudaMemcpyDeviceToHost, st));
+        KS_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+        double lum_sum = 0.0;
+        for (int y = 0; y < h; ++y)
+            lum_sum += h_rows[y];
+        float average = (float)lum_sum / (size_t)((size_t)w * h);
+        k_sky_cond<<<(h + 127) / 128, 128, 0, st>>>(lum.ptr, w, h, average, s->sky_cond.ptr, acc.ptr,
+                                                    sd.kind == 2 ? 1 : 0);
+        std::vector<float> h_acc(h);
+        KS_CUDA_TRY(ctx, cudaMemcpyAsync(h_acc.data(), acc.ptr, sizeof(float) * h, cudaMemcpyDeviceToHost, st));
+        KS_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+        std::vector<float> margin = host_cdf(h_acc.data(), (uint32_t)h);
+        KS_CUDA_TRY(ctx, s->sky_margin.alloc(margin.size()));
+        KS_CUDA_TRY(ctx, cudaMemcpyAsync(s->sky_margin.ptr, margin.data(), sizeof(float) * margin.size(),
+                                         cudaMemcpyHostToDevice, st));
+        // power (light.cpp:136-159)
+        SceneView v = make_view(s);
+        k_sky_power_rows<<<(h + 127) / 128, 128, 0, st>>>(v, row_sum.ptr);
+        std::vector<double> h_pr(3 * h);
+        KS_CUDA_TRY(ctx, cudaMemcpyAsync(h_pr.data(), row_sum.ptr, sizeof(double) * 3 * h, cudaMemcpyDeviceToHost, st));
+        KS_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+        double sum[3] = {0, 0, 0};
+        for (int y = 0; y < h; ++y)
+            for (int c = 0; c < 3; ++c)
+                sum[c] += (double)(float)h_pr[3 * y + c];
+        float Phi[3] = {(float)sum[0], (float)sum[1], (float)sum[2]};
+        float scale = (pi / h) * (6.28318530718f / w);
+        float ex = s->scene_bound[3] - s->scene_bound[0], ey = s->scene_bound[4] - s->scene_bound[1],
+              ez = s->scene_bound[5] - s->scene_bound[2];
+        float radius = 0.5f * std::sqrt(ex * ex + ey * ey + ez * ez);
+        for (int c = 0; c < 3; ++c) {
+            Phi[c] *= scale;
+            Phi[c] *= pi * (radius * radius);
+        }
+        sky_power_mean = (Phi[0] + Phi[1] + Phi[2]) / 3.0f;
+    }
+    // ---- mesh lights (host: constant emission, a few triangles) ----
+    std::vector<float> h_verts(3 * (size_t)s->n_verts);
+    std::vector<uint32_t> h_idx;
+    std::vector<uint32_t> ml_tri;
+    std::vector<float> ml_area, ml_importance;
+    std::vector<float4> ml_em;
+    bool any_emission = false;
+    for (size_t m = 0; m + 1 < s->host.mesh_tri_offset.size(); ++m)
+        if (s->host.materials[s->host.mesh_material[m]].has_emission)
+            any_emission = true;
+    std::vector<int32_t> tri_light;
+    if (any_emission) {
+        h_idx.resize(3 * (size_t)s->n_tris);
+        KS_CUDA_TRY(ctx, cudaMemcpy(h_verts.data(), s->verts.ptr, s->verts.bytes(), cudaMemcpyDeviceToHost));
+        KS_CUDA_TRY(ctx, cudaMemcpy(h_idx.data(), s->indices.ptr, s->indices.bytes(), cudaMemcpyDeviceToHost));
+        tri_light.assign(s->n_tris, -1);
+        auto vert = [&](uint32_t v, float out[3]) {
+            out[0] = h_verts[3 * v];
+            out[1] = h_verts[3 * v + 1];
+            out[2] = h_verts[3 * v + 2];
+        };
+        for (size_t m = 0; m + 1 < s->host.mesh_tri_offset.size(); ++m) {
+            const ks_material_desc &mat = s->host.materials[s->host.mesh_material[m]];
+            if (!mat.has_emission)
+                continue;
+            float avg_importance = 0.212671f * mat.emission[0] + 0.715160f * mat.emission[1] +
+                                   0.072169f * mat.emission[2];
+            uint32_t first = s->host.mesh_tri_offset[m], n = s->host.mesh_tri_offset[m + 1] - first;
+            std::vector<float> importance(n), areas(n);
+            std::vector<uint32_t> prim_ids(n);
+            for (uint32_t k = 0; k < n; ++k) {
+                float v0[3], v1[3], v2[3];
+                vert(h_idx[3 * (first + k)], v0);
+                vert(h_idx[3 * (first + k) + 1], v1);
+                vert(h_idx[3 * (first + k) + 2], v2);
+                float e01[3] = {v1[0] - v0[0], v1[1] - v0[1], v1[2] - v0[2]};
+                float e12[3] = {v2[0] - v1[0], v2[1] - v1[1], v2[2] - v1[2]};
+                float c[3] = {e01[1] * e12[2] - e01[2] * e12[1], e01[2] * e12[0] - e01[0] * e12[2],
+                              e01[0] * e12[1] - e01[1] * e12[0]};
+                float area = 0.5f * std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+                importance[k] = 6.28318530718f * area * avg_importance;
+                areas[k] = area;
+                prim_ids[k] = k;
+            }
+            uint32_t N = n;
+            for (uint32_t i = 0; i < N;) {
+                if (importance[i] == 0.0f) {
+                    std::swap(prim_ids[N - 1], prim_ids[i]);
+                    std::swap(importance[N - 1], importance[i]);
+                    std::swap(areas[N - 1], areas[i]);
+                    --N;
+                } else {
+                    ++i;
+                }
+            }
+            for (uint32_t k = 0; k < N; ++k) {
+                ml_tri.push_back(first + prim_ids[k]);
+                ml_area.push_back(areas[k]);
+                ml_importance.push_back(importance[k]);
+                ml_em.push_back(make_float4(mat.emission[0], mat.emission[1], mat.emission[2], 0.0f));
+            }
+        }
+    }
+    // ---- PowerLightSampler::build ----
+    uint32_t count = s->n_nonmesh + (uint32_t)ml_tri.size();
+    s->light_count = count;
+    s->h_powers.assign(count, 0.0f);
+    uint32_t flat = 0;
+    if (s->n_nonmesh)
+        s->h_powers[flat++] = sky_power_mean;
+    for (size_t k = 0; k < ml_tri.size(); ++k) {
+        float pw = ml_importance[k];
+        s->h_powers[flat] = (pw + pw + pw) / 3.0f;
+        if (any_emission)
+            tri_light[ml_tri[k]] = (int32_t)flat;
+        ++flat;
+    }
+    if (count == 0) {
+        // nothing to sample; ks_small_pt_render refuses such a scene
+        s->lights_built = true;
+        return KS_OK;
+    }
+    s->h_power_cdf = host_cdf(s->h_powers.data(), count);
+    KS_CUDA_TRY(ctx, s->power_cdf.alloc(s->h_power_cdf.size()));
+    KS_CUDA_TRY(ctx, cudaMemcpyAsync(s->power_cdf.ptr, s->h_power_cdf.data(), sizeof(float) * s->h_power_cdf.size(),
+                                     cudaMemcpyHostToDevice, st));
+    if (any_emission) {
+        KS_CUDA_TRY(ctx, s->tri_light.alloc(tri_light.size()));
+        KS_CUDA_TRY(ctx, s->ml_tri.alloc(ml_tri.size()));
+        KS_CUDA_TRY(ctx, s->ml_area.alloc(ml_area.size()));
+        KS_CUDA_TRY(ctx, s->ml_emission.alloc(ml_em.size()));
+        KS_CUDA_TRY(ctx, cudaMemcpyAsync(s->tri_light.ptr, tri_light.data(), s->tri_light.bytes(),
+                                         cudaMemcpyHostToDevice, st));
+        KS_CUDA_TRY(ctx, cudaMemcpyAsync(s->ml_tri.ptr, ml_tri.data(), s->ml_tri.bytes(), cudaMemcpyHostToDevice, st));
+        KS_CUDA_TRY(ctx,
+                    cudaMemcpyAsync(s->ml_area.ptr, ml_area.data(), s->ml_area.bytes(), cudaMemcpyHostToDevice, st));
+        KS_CUDA_TRY(ctx, cudaMemcpyAsync(s->ml_emission.ptr, ml_em.data(), s->ml_emission.bytes(),
+                                         cudaMemcpyHostToDevice, st));
+    }
+    KS_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    s->lights_built = true;
+    return KS_OK;
+}
+
+} // namespace ksb

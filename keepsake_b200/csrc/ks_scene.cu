@@ -114,7 +114,50 @@ ks_status ks_scene_create(ks_context *ctx, const ks_scene_desc *desc, ks_scene *
     }
     s->host.mesh_tri_offset.push_back((uint32_t)to);
     s->host.materials.assign(desc->materials, desc->materials + desc->n_materials);
-    cudaError_t e = s->verts.alloc(verts.size());
+    // sky
+    const ks_sky_desc &sd = desc->sky;
+    if (sd.kind < 0 || sd.kind > 2 || (sd.kind == 2 && (!sd.map_rgb || sd.width == 0 || sd.height == 0))) {
+        delete s;
+        return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_create: bad sky description");
+    }
+    s->sky_desc = sd;
+    if (sd.kind == 2)
+        s->h_sky_map.assign(sd.map_rgb, sd.map_rgb + 3 * (size_t)sd.width * sd.height);
+    s->sky_desc.map_rgb = nullptr;
+    std::vector<MaterialGPU> mats(desc->n_materials);
+    for (uint32_t k = 0; k < desc->n_materials; ++k) {
+        const ks_material_desc &m = desc->materials[k];
+        MaterialGPU &g = mats[k];
+        for (int c = 0; c < 3; ++c) {
+            g.basecolor[c] = m.basecolor[c];
+            g.emission[c] = m.emission[c];
+        }
+        g.roughness = m.roughness;
+        g.metallic = m.metallic;
+        g.ior = m.ior;
+        g.specular_r0_mul = m.specular_r0_mul;
+        g.specular_trans = m.specular_trans;
+        g.diffuse_trans = m.diffuse_trans;
+        g.diffuse_trans_fwd = m.diffuse_trans_fwd;
+        g.microfacet = m.microfacet;
+        g.has_emission = m.has_emission;
+        g.mesh_light = -1;
+    }
+    cudaError_t e = s->materials.alloc(mats.size());
+    if (e == cudaSuccess)
+        e = s->mesh_material.alloc(s->host.mesh_material.size());
+    if (e == cudaSuccess)
+        e = s->mesh_twosided.alloc(s->host.mesh_twosided.size());
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(s->materials.ptr, mats.data(), s->materials.bytes(), cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(s->mesh_material.ptr, s->host.mesh_material.data(), s->mesh_material.bytes(),
+                            cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(s->mesh_twosided.ptr, s->host.mesh_twosided.data(), s->mesh_twosided.bytes(),
+                            cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess)
+        e = s->verts.alloc(verts.size());
     if (e == cudaSuccess)
         e = s->indices.alloc(idx.size());
     if (e == cudaSuccess)
@@ -154,7 +197,12 @@ ks_status ks_scene_build_bvh(ks_scene *scene, const ks_sbvh_options *opts, float
         o = *opts;
     KS_CUDA_TRY(scene->ctx, cudaSetDevice(scene->ctx->device));
     scene->bvh_built = false;
-    return build_sbvh(scene, o, build_ms);
+    scene->lights_built = false;
+    ks_status st = build_sbvh(scene, o, build_ms);
+    if (st != KS_OK)
+        return st;
+    // the light sampler needs the scene bound (PowerLightSampler(scene_bound), small_pt.cpp:201)
+    return build_lights(scene);
 }
 
 ks_status ks_sbvh_counts(const ks_scene *scene, uint32_t *n_nodes, uint32_t *n_prims)

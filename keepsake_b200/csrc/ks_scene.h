@@ -73,12 +73,31 @@ struct ks_scene
     uint32_t root_count = 0; // prim count of the root
     bool bvh_built = false;
     float scene_bound[6] = {0, 0, 0, 0, 0, 0};
-    // materials
+    // materials (device copies of the per-mesh tables)
     ksb::DevBuf<ksb::MaterialGPU> materials;
     ksb::DevBuf<uint32_t> mesh_material;
+    ksb::DevBuf<int> mesh_twosided;
+    // lights (PowerLightSampler over [sky] + mesh-light triangles)
+    bool lights_built = false;
+    uint32_t light_count = 0, n_nonmesh = 0;
+    std::vector<float> h_powers, h_power_cdf;
+    ksb::DevBuf<float> power_cdf;
+    ksb::DevBuf<int32_t> tri_light;
+    ksb::DevBuf<uint32_t> ml_tri;
+    ksb::DevBuf<float> ml_area;
+    ksb::DevBuf<float4> ml_emission;
+    // sky
+    ks_sky_desc sky_desc{};
+    std::vector<float> h_sky_map; // kept for the light build (kind 2)
+    float sky_l2w[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, sky_w2l[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    ksb::DevBuf<float4> sky_map;
+    ksb::DevBuf<float> sky_cond, sky_margin;
+    int sky_w = 0, sky_h = 0;
+    ks_render_stats last_stats{};
 };
 
 namespace ksb
 {
 ks_status build_sbvh(ks_scene *scene, const ks_sbvh_options &opts, float *build_ms);
+ks_status build_lights(ks_scene *scene);
 }

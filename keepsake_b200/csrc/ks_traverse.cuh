@@ -183,7 +183,8 @@ KS_D bool cull_tri(const RayQuery &ray, f3 v0, f3 v1, f3 v2, int culling)
 
 struct Hit
 {
-    uint32_t tri; // global triangle index, ~0u on miss
+    uint32_t tri;  // global triangle index, ~0u on miss
+    uint32_t slot; // primitive slot of the hit (index into the leaf-ordered triangle array)
     float t, b0, b1, b2;
 };
 
@@ -225,6 +226,7 @@ KS_D bool traverse(const TravNode *__restrict__ nodes, const float4 *__restrict_
                     if (t < ray.tmax) {
                         ray.tmax = t;
                         hit.tri = __float_as_uint(a.w);
+                        hit.slot = first + k;
                         hit.t = t;
                         hit.b0 = b0;
                         hit.b1 = b1;

@@ -149,4 +149,22 @@ ks_status ks_generated_camera(const ks_generated *g, float camera_to_world[16], 
 
 void ks_generated_destroy(ks_generated *g) { delete g; }
 
+void ks_small_pt_params_default(ks_small_pt_params *p)
+{
+    if (!p)
+        return;
+    *p = ks_small_pt_params{};
+    p->include_background = 1;
+    p->bounces = 1;
+    p->render_width = 256;
+    p->render_height = 256;
+    p->spp = 1;
+    p->rng_seed = 0;
+    p->scale_ray_diff = 1;
+    p->clamp_direct = 0.0f;
+    p->clamp_indirect = 10.0f;
+    p->spp_prog_interval = 32;
+    p->pixel_filter_width = 1.0f;
+}
+
 } // extern "C"

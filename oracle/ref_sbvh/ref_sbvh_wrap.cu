@@ -117,6 +117,38 @@ int ksref_sbvh_intersect(void *handle, const float *rays, uint32_t n, int any_hi
     return 0;
 }
 
+// One ray (8 floats as above).  Returns the triangle index (~0u on miss) or, for any_hit, 1/0.
+uint32_t ksref_sbvh_intersect1(void *handle, const float *r, int any_hit, float *t, float *bary)
+{
+    auto *h = (RefHandle *)handle;
+    ksc::SBVHIsectOption opt;
+    opt.culling = ksc::SBVHCulling::None;
+    ksc::Ray ray(ksc::vec3(r[0], r[1], r[2]), ksc::vec3(r[4], r[5], r[6]), r[3], r[7]);
+    if (any_hit)
+        return h->bvh.intersectBool(ray, opt) ? 1u : 0u;
+    ksc::SBVHIsectRecord rec = h->bvh.intersect(ray, opt);
+    if (rec.tri_idx != ~0u) {
+        *t = rec.thit;
+        bary[0] = rec.coord.x;
+        bary[1] = rec.coord.y;
+        bary[2] = rec.coord.z;
+    }
+    return rec.tri_idx;
+}
+
+// Root bounds (min xyz, max xyz).
+void ksref_sbvh_bound(void *handle, float *out)
+{
+    auto *h = (RefHandle *)handle;
+    ksc::AABB3 b = h->bvh.bound();
+    out[0] = b.min.x;
+    out[1] = b.min.y;
+    out[2] = b.min.z;
+    out[3] = b.max.x;
+    out[4] = b.max.y;
+    out[5] = b.max.z;
+}
+
 void ksref_sbvh_destroy(void *handle) { delete (RefHandle *)handle; }
 
 } // extern "C"

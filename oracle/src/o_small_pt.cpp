@@ -1,0 +1,928 @@
+// ORACLE (test infrastructure only).  CPU restatement of keepsake's small_pt path:
+//
+//   SmallPT::run / trace          small_pt.cpp:15-178
+//   next_event_estimate           nee.cpp:11-57, power_heur nee.h:18-23
+//   Material::sample_with_nee     material.cpp:101-167 (no subsurface)
+//   Camera::spawn_ray             camera.cpp:129-170 (perspective, no ray differentials: the
+//                                 constant shader fields never read them)
+//   MeshGeometry::compute_intersection  geometry.cpp:68-163 (no texcoords, flat shading)
+//   transform_it / Transform::frame      ray.h:166-183, maths.h:989-996
+//   SkyLight                      light.cpp:19-159 (in-memory lat-long map instead of a file)
+//   MeshLightShared / MeshTriLight light.cpp:307-628 (constant emission: uniform importance)
+//   PowerLightSampler             light.cpp:636-701
+//   DistribTable / DistribTable2D distrib.cpp:9-107
+//   RenderTarget2::add / add_miss render_target.cpp:82-107 (FP64 accumulation)
+//
+// Ray queries go through the reference's own SBVH (cuda/sbvh.cu, oracle/_ref).
+// The two float atomics of the reference (the sky luminance threshold light.cpp:35-48 and the
+// sky power light.cpp:136-159) have no fixed order there; here both are summed in a fixed order
+// (rows sequentially in double) so the product can reproduce them exactly.
+#include "../../include/ks_b200.h"
+#include "o_bsdf.h"
+#include "o_math.h"
+#include "o_sampler.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cstdint>
+#include <memory>
+#include <thread>
+#include <vector>
+
+extern "C" {
+int ksref_sbvh_build(const float *, uint32_t, const uint32_t *, uint32_t, uint32_t, uint32_t, float, float, void **,
+                     uint32_t *, uint32_t *);
+uint32_t ksref_sbvh_intersect1(void *, const float *, int, float *, float *);
+void ksref_sbvh_bound(void *, float *);
+void ksref_sbvh_destroy(void *);
+}
+
+namespace oracle
+{
+
+// ---- DistribTable (distrib.cpp:9-75) ----------------------------------------------------------
+struct DistribTable
+{
+    std::vector<float> cdf;
+    float acc = 0.0f;
+    DistribTable() = default;
+    DistribTable(const float *f, uint32_t n) : cdf(n + 1)
+    {
+        cdf[0] = 0;
+        float invn = 1.0f / (float)n;
+        for (uint32_t i = 1; i < n + 1; ++i)
+            cdf[i] = cdf[i - 1] + f[i - 1] * invn;
+        acc = cdf[n];
+        if (acc == 0.0f) {
+            for (uint32_t i = 0; i < n + 1; ++i)
+                cdf[i] = (float)i / (float)n;
+        } else {
+            float invacc = 1.0f / acc;
+            for (uint32_t i = 0; i < n + 1; ++i)
+                cdf[i] *= invacc;
+        }
+        cdf[n] = 1.0f;
+    }
+    uint32_t sample(float u, float &prob) const
+    {
+        u = std::clamp(u, 0.0f, std::nextafter(1.0f, 0.0f));
+        auto it = std::upper_bound(cdf.begin(), cdf.end(), u);
+        uint32_t index = (uint32_t)std::distance(cdf.begin(), std::prev(it));
+        prob = cdf[index + 1] - cdf[index];
+        return index;
+    }
+    float sample_linear(float u, float &pdf, uint32_t &index) const
+    {
+        u = std::clamp(u, 0.0f, std::nextafter(1.0f, 0.0f));
+        auto it = std::upper_bound(cdf.begin(), cdf.end(), u);
+        index = (uint32_t)std::distance(cdf.begin(), std::prev(it));
+        float n = (float)(cdf.size() - 1);
+        pdf = (cdf[index + 1] - cdf[index]) * n;
+        float du = (u - cdf[index]) / (cdf[index + 1] - cdf[index]);
+        return (index + du) / n;
+    }
+    float pdf(uint32_t index) const
+    {
+        uint32_t n = (uint32_t)(cdf.size() - 1);
+        return (cdf[index + 1] - cdf[index]) * (float)n;
+    }
+};
+
+struct DistribTable2D
+{
+    std::vector<DistribTable> cond;
+    DistribTable margin;
+    DistribTable2D() = default;
+    DistribTable2D(const float *f, uint32_t nx, uint32_t ny)
+    {
+        cond.resize(ny);
+        for (uint32_t y = 0; y < ny; ++y)
+            cond[y] = DistribTable(f + (size_t)y * nx, nx);
+        std::vector<float> marginPmf(ny);
+        for (uint32_t y = 0; y < ny; ++y)
+            marginPmf[y] = cond[y].acc;
+        margin = DistribTable(marginPmf.data(), ny);
+    }
+    void sample_linear(float u0, float u1, float &pdf, float &s0, float &s1) const
+    {
+        float pdfMargin, pdfCond;
+        uint32_t uIndex, vIndex;
+        float vSample = margin.sample_linear(u1, pdfMargin, vIndex);
+        float uSample = cond[vIndex].sample_linear(u0, pdfCond, uIndex);
+        pdf = pdfMargin * pdfCond;
+        s0 = uSample;
+        s1 = vSample;
+    }
+    float pdf(float p0, float p1) const
+    {
+        int x = std::clamp(int(p0 * (cond[0].cdf.size() - 1)), 0, (int)cond[0].cdf.size() - 2);
+        int y = std::clamp(int(p1 * cond.size()), 0, (int)cond.size() - 1);
+        return margin.pdf(y) * cond[y].pdf(x);
+    }
+};
+
+// ---- SkyLight -----------------------------------------------------------------------------------
+struct Sky
+{
+    int kind = 0; // 1 ambient, 2 map
+    int w = 1, h = 1;
+    std::vector<V3> map; // row-major, map(u, v) = map[v * w + u]
+    float l2w[16], w2l[16];
+    bool y_up = true;
+    float strength = 1.0f;
+    DistribTable2D distrib;
+
+    static void to_spherical_yup(V3 d, float &phi, float &theta)
+    {
+        theta = std::acos(std::clamp(d.y, -1.0f, 1.0f));
+        phi = std::atan2(d.z, d.x);
+        if (phi < 0.0f)
+            phi += two_pi;
+    }
+    static void to_spherical(V3 d, float &phi, float &theta)
+    {
+        theta = std::acos(std::clamp(d.z, -1.0f, 1.0f));
+        phi = std::atan2(d.y, d.x);
+        if (phi < 0.0f)
+            phi += two_pi;
+    }
+    static V3 to_cartesian_yup(float phi, float theta)
+    {
+        float ct = std::cos(theta), st = std::sin(theta), cp = std::cos(phi), sp = std::sin(phi);
+        return V3(cp * st, ct, sp * st);
+    }
+    static V3 to_cartesian(float phi, float theta)
+    {
+        float ct = std::cos(theta), st = std::sin(theta), cp = std::cos(phi), sp = std::sin(phi);
+        return V3(cp * st, sp * st, ct);
+    }
+    // lerp_helper (maths.h:760-780), TickMode::Middle
+    static void lerp_helper(float u, int res, bool repeat, int &u0, int &u1, float &t)
+    {
+        float u_scaled = u * (float)res - 0.5f;
+        u0 = (int)std::floor(u_scaled);
+        u1 = u0 + 1;
+        t = u_scaled - u0;
+        if (repeat) {
+            u0 = (u0 + res) % res;
+            u1 = (u1 + res) % res;
+        } else {
+            u0 = std::clamp(u0, 0, res - 1);
+            u1 = std::clamp(u1, 0, res - 1);
+        }
+    }
+    V3 at(int u, int v) const { return map[(size_t)v * w + u]; }
+    V3 eval(V3 wi) const
+    {
+        V3 wl = transform_dir(w2l, wi);
+        float phi, theta;
+        if (y_up)
+            to_spherical_yup(wl, phi, theta);
+        else
+            to_spherical(wl, phi, theta);
+        float uv0 = phi * inv_pi * 0.5f, uv1 = theta * inv_pi;
+        int u0, u1, v0, v1;
+        float t0, t1;
+        lerp_helper(uv0, w, true, u0, u1, t0);
+        lerp_helper(uv1, h, false, v0, v1, t1);
+        V3 L;
+        L += (1.0f - t0) * (1.0f - t1) * at(u0, v0);
+        L += (1.0f - t0) * t1 * at(u0, v1);
+        L += t0 * (1.0f - t1) * at(u1, v0);
+        L += t0 * t1 * at(u1, v1);
+        L *= strength;
+        return L;
+    }
+    V3 sample(float u0, float u1, V3 &wi, float &wi_dist, float &pdf) const
+    {
+        float s0, s1;
+        distrib.sample_linear(u0, u1, pdf, s0, s1);
+        if (pdf == 0.0f)
+            return V3();
+        float phi = s0 * 2.0f * pi;
+        float theta = s1 * pi;
+        V3 wl = y_up ? to_cartesian_yup(phi, theta) : to_cartesian(phi, theta);
+        float sin_theta = std::sin(theta);
+        pdf /= (2.0f * pi * pi * sin_theta);
+        if (sin_theta == 0.0f) {
+            pdf = 0.0f;
+            return V3();
+        }
+        wi = transform_dir(l2w, wl);
+        wi_dist = inf;
+        return eval(wi) / pdf;
+    }
+    float pdf(V3 wi) const
+    {
+        V3 wl = transform_dir(w2l, wi);
+        float phi, theta;
+        if (y_up)
+            to_spherical_yup(wl, phi, theta);
+        else
+            to_spherical(wl, phi, theta);
+        float sin_theta = std::sin(theta);
+        if (sin_theta == 0.0f)
+            return 0.0f;
+        float p = distrib.pdf(phi * inv_pi * 0.5f, theta * inv_pi);
+        p /= (2.0f * pi * pi * sin_theta);
+        return p;
+    }
+    // SkyLight::power (light.cpp:136-159); the rows' float sums are added in row order in double.
+    V3 power(const float bound[6]) const
+    {
+        double sum[3] = {0, 0, 0};
+        for (int row = 0; row < h; ++row) {
+            float theta = (row + 0.5f) / (float)h * pi;
+            float sin_theta = std::sin(theta);
+            V3 row_sum;
+            for (int col = 0; col < w; ++col) {
+                float phi = (col + 0.5f) / (float)w * two_pi;
+                V3 dir = to_cartesian(phi, theta);
+                row_sum += eval(dir) * sin_theta;
+            }
+            for (int c = 0; c < 3; ++c)
+                sum[c] += row_sum[c];
+        }
+        V3 Phi((float)sum[0], (float)sum[1], (float)sum[2]);
+        Phi *= (pi / h) * (two_pi / w);
+        V3 ext(bound[3] - bound[0], bound[4] - bound[1], bound[5] - bound[2]);
+        float scene_radius = 0.5f * norm(ext);
+        Phi *= pi * sqr(scene_radius);
+        return Phi;
+    }
+};
+
+inline bool invert_rigid_or_general(const float *m, float *out)
+{
+    double a[4][8];
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 8; ++c)
+            a[r][c] = c < 4 ? m[4 * r + c] : (c - 4 == r ? 1.0 : 0.0);
+    for (int col = 0; col < 4; ++col) {
+        int piv = col;
+        for (int r = col + 1; r < 4; ++r)
+            if (std::fabs(a[r][col]) > std::fabs(a[piv][col]))
+                piv = r;
+        if (a[piv][col] == 0.0)
+            return false;
+        for (int c = 0; c < 8; ++c)
+            std::swap(a[piv][c], a[col][c]);
+        double inv = 1.0 / a[col][col];
+        for (int c = 0; c < 8; ++c)
+            a[col][c] *= inv;
+        for (int r = 0; r < 4; ++r)
+            if (r != col) {
+                double f = a[r][col];
+                for (int c = 0; c < 8; ++c)
+                    a[r][c] -= f * a[col][c];
+            }
+    }
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c)
+            out[4 * r + c] = (float)a[r][c + 4];
+    return true;
+}
+
+// ---- mesh lights (light.cpp:307-628) ------------------------------------------------------------
+struct MeshLight
+{
+    uint32_t mesh = 0;
+    V3 emission;
+    std::vector<uint32_t> prim_ids; // local triangle ids of the mesh
+    std::vector<float> importance;
+    std::vector<float> areas;
+};
+
+// ---- scene ------------------------------------------------------------------------------------
+struct Scene
+{
+    std::vector<float> verts;
+    std::vector<uint32_t> idx;
+    std::vector<uint32_t> tri_mesh;
+    std::vector<uint32_t> mesh_tri_off;
+    std::vector<uint32_t> mesh_material;
+    std::vector<int> mesh_twosided;
+    std::vector<ks_material_desc> materials;
+    void *bvh = nullptr;
+    float bound[6];
+    std::unique_ptr<Sky> sky;
+    std::vector<MeshLight> mesh_lights;
+    std::vector<int32_t> tri_light; // global triangle -> flat light index, -1 if none
+    std::vector<uint32_t> index_psum;
+    DistribTable power_distrib;
+    uint32_t light_count = 0;
+    std::vector<float> powers;
+
+    ~Scene()
+    {
+        if (bvh)
+            ksref_sbvh_destroy(bvh);
+    }
+    V3 vert(uint32_t v) const { return V3(verts[3 * v], verts[3 * v + 1], verts[3 * v + 2]); }
+    V3 tri_vert(uint32_t t, int k) const { return vert(idx[3 * t + k]); }
+
+    float probability(uint32_t light_index) const { return power_distrib.pdf(light_index) / (float)light_count; }
+};
+
+struct Intersection
+{
+    float thit;
+    V3 p;
+    Frame frame, sh_frame;
+    V3 sh_to_local(V3 w) const
+    {
+        bool hw = dot(frame.n, w) >= 0.0f;
+        V3 l = sh_frame.to_local(w);
+        bool hl = l.z >= 0.0f;
+        if (hw != hl)
+            l.z *= -1.0f;
+        return l;
+    }
+    V3 sh_to_world(V3 l) const
+    {
+        bool hl = l.z >= 0.0f;
+        V3 w = sh_frame.to_world(l);
+        bool hw = dot(frame.n, w) >= 0.0f;
+        if (hl != hw)
+            w -= 2.0f * dot(frame.n, w) * frame.n;
+        return w;
+    }
+};
+
+// Transform::frame with the identity instance transform (maths.h:989-996): re-orthonormalises.
+inline Frame identity_transform_frame(const Frame &f)
+{
+    Frame o;
+    o.t = normalized(f.t);
+    V3 b = f.b;
+    b = normalized(b - dot(b, o.t) * o.t);
+    o.b = b;
+    o.n = normalized(cross(o.t, o.b));
+    return o;
+}
+
+// compute_intersection for a triangle hit with barycentrics (w0, w1, w2) (geometry.cpp:68-163).
+inline Intersection make_intersection(const Scene &s, uint32_t tri, float t, float w1, float w2, V3 ray_dir)
+{
+    Intersection it;
+    it.thit = t;
+    V3 rd = normalized(ray_dir);
+    V3 wo_object = -rd;
+    V3 p0 = s.tri_vert(tri, 0), p1 = s.tri_vert(tri, 1), p2 = s.tri_vert(tri, 2);
+    V3 ng = normalized(cross(p1 - p0, p2 - p0));
+    float u = w1, v = w2;
+    float w0 = 1.0f - u - v;
+    it.p = w0 * p0 + u * p1 + v * p2;
+    V3 dpdu = p1 - p0;
+    V3 b = normalized(cross(ng, dpdu));
+    V3 tt = normalized(cross(b, ng));
+    if (s.mesh_twosided[s.tri_mesh[tri]]) {
+        if (dot(wo_object, ng) < 0.0f) {
+            ng = -ng;
+            dpdu = -dpdu;
+            tt = -tt;
+        }
+    }
+    it.frame.t = tt;
+    it.frame.b = b;
+    it.frame.n = ng;
+    it.sh_frame = it.frame;
+    // transform_it with the identity instance transform
+    it.frame = identity_transform_frame(it.frame);
+    it.sh_frame = identity_transform_frame(it.sh_frame);
+    return it;
+}
+
+inline bool intersect(const Scene &s, V3 o, V3 d, float tmax, uint32_t &tri, float &t, float bary[3])
+{
+    float r[8] = {o.x, o.y, o.z, 0.0f, d.x, d.y, d.z, tmax};
+    tri = ksref_sbvh_intersect1(s.bvh, r, 0, &t, bary);
+    return tri != ~0u;
+}
+inline bool occluded(const Scene &s, V3 o, V3 d, float tmax)
+{
+    float r[8] = {o.x, o.y, o.z, 0.0f, d.x, d.y, d.z, tmax};
+    return ksref_sbvh_intersect1(s.bvh, r, 1, nullptr, nullptr) != 0;
+}
+
+// spawn_ray<OffsetType::NextBounce> (ray.h:89-96): returns the offset origin
+inline V3 spawn_origin(V3 p, V3 dir, V3 ng) { return offset_ray(p, dot(dir, ng) > 0.0f ? ng : -ng); }
+
+// MeshData::compute_geometry_normal (geometry.h:45-60), then Transform::normal with identity.
+inline V3 light_normal(const Scene &s, uint32_t tri)
+{
+    V3 v0 = s.tri_vert(tri, 0), v1 = s.tri_vert(tri, 1), v2 = s.tri_vert(tri, 2);
+    V3 e01 = v1 - v0, e12 = v2 - v1;
+    V3 ng = normalized(cross(e01, e12));
+    return normalized(ng);
+}
+
+inline V3 mesh_light_sample(const Scene &s, uint32_t light_flat, V3 p_shade, float u0, float u1, V3 &wi,
+                            float &wi_dist, float &pdf)
+{
+    uint32_t g = (uint32_t)(std::upper_bound(s.index_psum.begin(), s.index_psum.end(), light_flat) -
+                            s.index_psum.begin()) - 1;
+    uint32_t k = light_flat - s.index_psum[g];
+    const MeshLight &ml = s.mesh_lights[g - 1];
+    // sample_triangle_bary (rng.h:379-390)
+    float b0, b1;
+    if (u0 < u1) {
+        b0 = u0 / 2;
+        b1 = u1 - b0;
+    } else {
+        b1 = u1 / 2;
+        b0 = u0 - b1;
+    }
+    uint32_t tri = s.mesh_tri_off[ml.mesh] + ml.prim_ids[k];
+    V3 p0 = s.tri_vert(tri, 0), p1 = s.tri_vert(tri, 1), p2 = s.tri_vert(tri, 2);
+    float w0 = 1.0f - b0 - b1;
+    V3 position = w0 * p0 + b0 * p1 + b1 * p2;
+    V3 n = light_normal(s, tri);
+    wi = position - p_shade;
+    float wi_dist2 = sqnorm(wi);
+    if (wi_dist2 == 0.0f) {
+        wi_dist = 0.0f;
+        pdf = 0.0f;
+        return V3();
+    }
+    wi_dist = std::sqrt(wi_dist2);
+    wi /= wi_dist;
+    pdf = 1.0f / ml.areas[k];
+    float absdot = std::abs(dot(n, wi));
+    if (absdot == 0.0f) {
+        wi_dist = 0.0f;
+        pdf = 0.0f;
+        return V3();
+    }
+    pdf *= (wi_dist2 / absdot);
+    constexpr float shadow_eps = 1e-4f;
+    wi_dist = std::max(0.0f, wi_dist - shadow_eps);
+    return ml.emission / pdf;
+}
+
+inline float mesh_light_pdf(const Scene &s, uint32_t tri, uint32_t k, const MeshLight &ml, V3 wi, float wi_dist)
+{
+    if (wi_dist == 0.0f)
+        return 0.0f;
+    V3 n = light_normal(s, tri);
+    float pdf = 1.0f / ml.areas[k];
+    float absdot = std::abs(dot(n, wi));
+    if (absdot == 0.0f)
+        return 0.0f;
+    pdf *= (sqr(wi_dist) / absdot);
+    return pdf;
+}
+
+struct Counters
+{
+    uint64_t extension = 0, shadow = 0;
+};
+
+struct Camera
+{
+    float c2w[16], p2w[16];
+    V3 position() const { return V3(c2w[3], c2w[7], c2w[11]); }
+};
+
+struct Tracer
+{
+    const Scene &s;
+    const ks_small_pt_params &in;
+    Counters cnt;
+
+    // next_event_estimate (nee.cpp:11-57)
+    V3 nee(const Principled &bsdf, const Intersection &hit, V3 wo, OwenScrambledSobol02Morton &sobol)
+    {
+        float pr_light;
+        uint32_t light = s.power_distrib.sample(sobol.next(), pr_light);
+        float u0, u1;
+        sobol.next2d(u0, u1);
+        V3 wi;
+        float wi_dist = 0.0f, pdf_wi_light = 0.0f;
+        V3 Le_beta;
+        uint32_t n_nonmesh = s.index_psum[1];
+        if (light < n_nonmesh) {
+            Le_beta = s.sky->sample(u0, u1, wi, wi_dist, pdf_wi_light);
+        } else {
+            Le_beta = mesh_light_sample(s, light, hit.p, u0, u1, wi, wi_dist, pdf_wi_light);
+        }
+        V3 beta_nee;
+        if (!is_zero(Le_beta) && pdf_wi_light > 0.0f) {
+            V3 wo_local = hit.sh_to_local(wo);
+            V3 wi_local = hit.sh_to_local(wi);
+            V3 f;
+            float pdf_wi_bsdf;
+            bsdf.eval_and_pdf(wo_local, wi_local, f, pdf_wi_bsdf);
+            if (!is_zero(f) && pdf_wi_bsdf > 0.0f) {
+                V3 o = spawn_origin(hit.p, wi, hit.frame.n);
+                cnt.shadow++;
+                if (!occluded(s, o, wi, wi_dist)) {
+                    float mis_weight = power_heur(pdf_wi_light, pdf_wi_bsdf);
+                    beta_nee += Le_beta * f * mis_weight / pr_light;
+                }
+            }
+        }
+        return beta_nee;
+    }
+
+    bool trace(V3 ro, V3 rd, OwenScrambledSobol02Morton &sobol, V3 &Lout)
+    {
+        V3 L;
+        V3 beta(1, 1, 1);
+        float pdf_wi_bsdf = 0.0f;
+        for (int bounce = 0; bounce < in.bounces + 1; ++bounce) {
+            uint32_t tri;
+            float t, bary[3];
+            cnt.extension++;
+            bool isect_geom = intersect(s, ro, rd, inf, tri, t, bary);
+            if (!isect_geom) {
+                if (s.sky) {
+                    uint32_t light_index = 0;
+                    V3 wi = normalized(rd);
+                    V3 Le = s.sky->eval(wi);
+                    if (bounce == 0) {
+                        if (in.include_background)
+                            L += beta * Le;
+                    } else {
+                        float pr_light = s.probability(light_index);
+                        float pdf_wi_light = s.sky->pdf(wi);
+                        float mis_weight = power_heur(pdf_wi_bsdf, pdf_wi_light * pr_light);
+                        V3 beta_uni = Le * mis_weight;
+                        if (bounce == 1 && in.clamp_direct > 0.0f)
+                            beta_uni = cwise_min(beta_uni, in.clamp_direct);
+                        else if (bounce >= 2 && in.clamp_indirect > 0.0f)
+                            beta_uni = cwise_min(beta_uni, in.clamp_indirect);
+                        L += beta * beta_uni;
+                    }
+                }
+                if (bounce == 0 && !in.include_background) {
+                    Lout = V3();
+                    return false;
+                }
+                break;
+            }
+            Intersection it = make_intersection(s, tri, t, bary[1], bary[2], rd);
+            uint32_t mesh = s.tri_mesh[tri];
+            const ks_material_desc &mat = s.materials[s.mesh_material[mesh]];
+            if (mat.has_emission) {
+                int32_t light = s.tri_light[tri];
+                if (light >= 0) {
+                    float pr_light = s.probability((uint32_t)light);
+                    V3 wi = normalized(rd);
+                    uint32_t g = (uint32_t)(std::upper_bound(s.index_psum.begin(), s.index_psum.end(),
+                                                             (uint32_t)light) -
+                                            s.index_psum.begin()) - 1;
+                    const MeshLight &ml = s.mesh_lights[g - 1];
+                    V3 Le(ml.emission);
+                    if (bounce == 0) {
+                        L += beta * Le;
+                    } else if (pr_light > 0.0f) {
+                        uint32_t k = (uint32_t)light - s.index_psum[g];
+                        float pdf_wi_light = mesh_light_pdf(s, tri, k, ml, wi, it.thit);
+                        float mis_weight = power_heur(pdf_wi_bsdf, pdf_wi_light * pr_light);
+                        V3 beta_uni = Le * mis_weight;
+                        if (bounce == 1 && in.clamp_direct > 0.0f)
+                            beta_uni = cwise_min(beta_uni, in.clamp_direct);
+                        else if (bounce >= 2 && in.clamp_indirect > 0.0f)
+                            beta_uni = cwise_min(beta_uni, in.clamp_indirect);
+                        L += beta * beta_uni;
+                    }
+                }
+            }
+            if (bounce == in.bounces)
+                break;
+            V3 wo = -normalized(rd);
+            Principled bsdf{eval_closure(mat)};
+            // Material::sample_with_nee (material.cpp:101-167)
+            V3 Ld = nee(bsdf, it, wo, sobol);
+            V3 wo_local = it.sh_to_local(wo);
+            float u_lobe = sobol.next();
+            float u0, u1;
+            sobol.next2d(u0, u1);
+            V3 wi_local;
+            float pdf_wi = 0.0f;
+            V3 sbeta = bsdf.sample(wo_local, wi_local, u_lobe, u0, u1, pdf_wi);
+            V3 wi;
+            if (!(max_coeff(sbeta) == 0.0f || pdf_wi == 0.0f))
+                wi = it.sh_to_world(wi_local);
+            if (bounce == 0 && in.clamp_direct > 0.0f)
+                Ld = cwise_min(Ld, in.clamp_direct);
+            else if (bounce >= 1 && in.clamp_indirect > 0.0f)
+                Ld = cwise_min(Ld, in.clamp_indirect);
+            L += beta * Ld;
+            beta *= sbeta;
+            if (max_coeff(beta) == 0.0f)
+                break;
+            pdf_wi_bsdf = pdf_wi;
+            ro = spawn_origin(it.p, wi, it.frame.n);
+            rd = wi;
+            if (max_coeff(beta) < 1.0f && bounce >= 1) {
+                float q = std::max(0.0f, 1.0f - max_coeff(beta));
+                if (sobol.next() < q)
+                    break;
+                beta /= 1.0f - q;
+            }
+        }
+        Lout = L;
+        return true;
+    }
+};
+
+Scene *create_scene(const ks_scene_desc *d, const ks_sbvh_options *opts)
+{
+    auto s = std::make_unique<Scene>();
+    uint32_t vo = 0;
+    for (uint32_t m = 0; m < d->n_meshes; ++m) {
+        const ks_mesh_desc &md = d->meshes[m];
+        s->mesh_tri_off.push_back((uint32_t)s->tri_mesh.size());
+        s->verts.insert(s->verts.end(), md.vertices, md.vertices + 3 * md.n_vertices);
+        for (uint32_t k = 0; k < 3 * md.n_triangles; ++k)
+            s->idx.push_back(md.indices[k] + vo);
+        s->tri_mesh.insert(s->tri_mesh.end(), md.n_triangles, m);
+        s->mesh_material.push_back(md.material);
+        s->mesh_twosided.push_back(md.twosided);
+        vo += md.n_vertices;
+    }
+    s->mesh_tri_off.push_back((uint32_t)s->tri_mesh.size());
+    s->materials.assign(d->materials, d->materials + d->n_materials);
+    ks_sbvh_options o{4, 12, 1.0f, 1e-5f};
+    if (opts)
+        o = *opts;
+    uint32_t nn, np;
+    if (ksref_sbvh_build(s->verts.data(), vo, s->idx.data(), (uint32_t)s->tri_mesh.size(), o.max_prims_in_node,
+                         o.bucket_count, o.trav_weight, o.alpha, &s->bvh, &nn, &np) != 0)
+        return nullptr;
+    ksref_sbvh_bound(s->bvh, s->bound);
+
+    // sky light (light.cpp:19-57)
+    const ks_sky_desc &sd = d->sky;
+    if (sd.kind == 1 || sd.kind == 2) {
+        auto sky = std::make_unique<Sky>();
+        sky->kind = sd.kind;
+        if (sd.kind == 1) {
+            sky->w = sky->h = 1;
+            sky->map = {V3(sd.ambient[0], sd.ambient[1], sd.ambient[2])};
+            float id[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};
+            std::memcpy(sky->l2w, id, sizeof(id));
+            std::memcpy(sky->w2l, id, sizeof(id));
+            sky->y_up = true;
+            sky->strength = 1.0f;
+            float lum = luminance(sky->map[0]);
+            sky->distrib = DistribTable2D(&lum, 1, 1);
+        } else {
+            sky->w = (int)sd.width;
+            sky->h = (int)sd.height;
+            sky->map.resize((size_t)sky->w * sky->h);
+            for (size_t i = 0; i < sky->map.size(); ++i)
+                sky->map[i] = V3(sd.map_rgb[3 * i], sd.map_rgb[3 * i + 1], sd.map_rgb[3 * i + 2]);
+            std::memcpy(sky->l2w, sd.to_world, sizeof(float) * 16);
+            invert_rigid_or_general(sky->l2w, sky->w2l);
+            sky->y_up = sd.transform_y_up != 0;
+            sky->strength = sd.strength;
+            std::vector<float> lum((size_t)sky->w * sky->h);
+            double lum_sum = 0.0;
+            for (int y = 0; y < sky->h; ++y) {
+                float theta = (y + 0.5f) / (float)sky->h * pi;
+                float sin_theta = std::sin(theta);
+                double row = 0.0;
+                for (int x = 0; x < sky->w; ++x) {
+                    size_t i = (size_t)y * sky->w + x;
+                    lum[i] = sin_theta * luminance(sky->map[i]);
+                    row += lum[i];
+                }
+                lum_sum += row;
+            }
+            float average = (float)lum_sum / lum.size();
+            for (auto &l : lum)
+                l = std::max(l - average, 0.0f);
+            sky->distrib = DistribTable2D(lum.data(), sky->w, sky->h);
+        }
+        s->sky = std::move(sky);
+    }
+    // mesh lights (scene.cpp:315-336, light.cpp:307-560): constant emission -> uniform importance
+    for (uint32_t m = 0; m < d->n_meshes; ++m) {
+        const ks_material_desc &mat = s->materials[s->mesh_material[m]];
+        if (!mat.has_emission)
+            continue;
+        MeshLight ml;
+        ml.mesh = m;
+        ml.emission = V3(mat.emission[0], mat.emission[1], mat.emission[2]);
+        float avg_importance = luminance(ml.emission);
+        uint32_t first = s->mesh_tri_off[m], n = s->mesh_tri_off[m + 1] - first;
+        std::vector<float> importance(n), areas(n);
+        for (uint32_t k = 0; k < n; ++k) {
+            V3 v0 = s->tri_vert(first + k, 0), v1 = s->tri_vert(first + k, 1), v2 = s->tri_vert(first + k, 2);
+            V3 e01 = v1 - v0, e12 = v2 - v1;
+            float area = 0.5f * norm(cross(e01, e12));
+            importance[k] = two_pi * area * avg_importance;
+            areas[k] = area;
+        }
+        std::vector<uint32_t> prim_ids(n);
+        for (uint32_t k = 0; k < n; ++k)
+            prim_ids[k] = k;
+        uint32_t N = n;
+        for (uint32_t i = 0; i < N;) {
+            if (importance[i] == 0.0f) {
+                std::swap(prim_ids[N - 1], prim_ids[i]);
+                std::swap(importance[N - 1], importance[i]);
+                std::swap(areas[N - 1], areas[i]);
+                --N;
+            } else {
+                ++i;
+            }
+        }
+        prim_ids.resize(N);
+        importance.resize(N);
+        areas.resize(N);
+        ml.prim_ids = prim_ids;
+        ml.importance = importance;
+        ml.areas = areas;
+        s->mesh_lights.push_back(std::move(ml));
+    }
+    // PowerLightSampler::build (light.cpp:636-672)
+    uint32_t n_nonmesh = s->sky ? 1u : 0u;
+    s->index_psum.assign(1 + s->mesh_lights.size() + 1, 0);
+    uint32_t sum = 0;
+    for (uint32_t i = 0; i < (uint32_t)s->index_psum.size(); ++i) {
+        s->index_psum[i] = sum;
+        if (i < (uint32_t)s->index_psum.size() - 1)
+            sum += (i == 0 ? n_nonmesh : (uint32_t)s->mesh_lights[i - 1].prim_ids.size());
+    }
+    s->light_count = sum;
+    s->powers.assign(sum, 0.0f);
+    s->tri_light.assign(s->tri_mesh.size(), -1);
+    uint32_t flat = 0;
+    if (s->sky) {
+        V3 P = s->sky->power(s->bound);
+        s->powers[flat++] = (P.x + P.y + P.z) / 3.0f;
+    }
+    for (const MeshLight &ml : s->mesh_lights)
+        for (uint32_t j = 0; j < ml.prim_ids.size(); ++j) {
+            s->tri_light[s->mesh_tri_off[ml.mesh] + ml.prim_ids[j]] = (int32_t)flat;
+            float pw = ml.importance[j];
+            s->powers[flat++] = (pw + pw + pw) / 3.0f;
+        }
+    if (sum > 0)
+        s->power_distrib = DistribTable(s->powers.data(), sum);
+    return s.release();
+}
+
+} // namespace oracle
+
+using namespace oracle;
+
+extern "C" {
+
+void *oracle_scene_create(const ks_scene_desc *desc, const ks_sbvh_options *opts)
+{
+    return oracle::create_scene(desc, opts);
+}
+
+void oracle_scene_destroy(void *s) { delete (Scene *)s; }
+
+// Light tables for parity checks: powers (light_count floats) and the power CDF
+// (light_count + 1 floats); returns light_count.
+uint32_t oracle_light_table(void *sp, float *powers, float *cdf)
+{
+    Scene *s = (Scene *)sp;
+    for (uint32_t i = 0; i < s->light_count; ++i) {
+        if (powers)
+            powers[i] = s->powers[i];
+    }
+    if (cdf)
+        for (size_t i = 0; i < s->power_distrib.cdf.size(); ++i)
+            cdf[i] = s->power_distrib.cdf[i];
+    return s->light_count;
+}
+
+// Sky distribution for parity checks: conditional CDFs (h rows of w+1) and marginal CDF (h+1).
+int oracle_sky_tables(void *sp, float *cond, float *margin)
+{
+    Scene *s = (Scene *)sp;
+    if (!s->sky)
+        return 1;
+    const Sky &k = *s->sky;
+    for (int y = 0; y < k.h; ++y)
+        for (int x = 0; x <= k.w; ++x)
+            cond[(size_t)y * (k.w + 1) + x] = k.distrib.cond[y].cdf[x];
+    for (int y = 0; y <= k.h; ++y)
+        margin[y] = k.distrib.margin.cdf[y];
+    return 0;
+}
+
+// SmallPT::run (small_pt.cpp:15-70) on n_threads host threads over 4x4 pixel tiles
+// (parallel.h:93-113).  accum: W*H*3 doubles, weights: W*H*2 doubles (both zero-initialised by
+// the caller and accumulated into).  counts[0..1] receive extension and shadow ray counts.
+int oracle_render(void *sp, const ks_camera_desc *cam, const ks_small_pt_params *in, double *accum, double *weights,
+                  int n_threads, uint64_t *counts)
+{
+    Scene &s = *(Scene *)sp;
+    const int W = in->render_width, H = in->render_height;
+    int cx = 0, cy = 0, cw = W, ch = H;
+    if (in->crop_width > 0 && in->crop_height > 0) {
+        cx = std::max(in->crop_start_x, 0);
+        cy = std::max(in->crop_start_y, 0);
+        cw = std::min(in->crop_width, W - cx);
+        ch = std::min(in->crop_height, H - cy);
+    }
+    Camera camera;
+    std::memcpy(camera.c2w, cam->camera_to_world, sizeof(float) * 16);
+    std::memcpy(camera.p2w, cam->proj_to_world, sizeof(float) * 16);
+    const int tiles_x = (cw + 3) / 4, tiles_y = (ch + 3) / 4;
+    std::atomic<int> next_tile{0};
+    std::atomic<uint64_t> n_ext{0}, n_shadow{0};
+    const float r = 0.5f * in->pixel_filter_width;
+    auto worker = [&]() {
+        Tracer tr{s, *in, {}};
+        while (true) {
+            int tile = next_tile.fetch_add(1);
+            if (tile >= tiles_x * tiles_y)
+                break;
+            int tx = tile % tiles_x, ty = tile / tiles_x;
+            for (int oy = ty * 4; oy < std::min(ch, ty * 4 + 4); ++oy)
+                for (int ox = tx * 4; ox < std::min(cw, tx * 4 + 4); ++ox) {
+                    int px = cx + ox, py = cy + oy;
+                    size_t pix = (size_t)py * W + px;
+                    for (int smp = 0; smp < in->spp; ++smp) {
+                        PTRenderSampler sampler(W, H, px, py, in->spp, smp, in->rng_seed);
+                        float offx = 0.0f, offy = 0.0f;
+                        if (in->spp != 1) {
+                            float u0, u1;
+                            sampler.sobol.next2d(u0, u1);
+                            // BoxPixelFilter::sample: lerp(-r, r, u) = (1 - u) * -r + u * r
+                            offx = (1.0f - u0) * -r + u0 * r;
+                            offy = (1.0f - u1) * -r + u1 * r;
+                        }
+                        float fx = ((px + 0.5f) + offx) / (float)W;
+                        float fy = ((py + 0.5f) + offy) / (float)H;
+                        V3 ndc(fx * 2.0f - 1.0f, fy * 2.0f - 1.0f, 1.0f);
+                        V3 cp = camera.position();
+                        V3 world_pos = point_hdiv(camera.p2w, ndc);
+                        V3 dir = normalized(world_pos - cp);
+                        V3 L;
+                        bool hit = tr.trace(cp, dir, sampler.sobol, L);
+                        if (hit) {
+                            weights[2 * pix + 0] += 1.0;
+                            weights[2 * pix + 1] += 0.0;
+                            accum[3 * pix + 0] += (double)L.x * 1.0;
+                            accum[3 * pix + 1] += (double)L.y * 1.0;
+                            accum[3 * pix + 2] += (double)L.z * 1.0;
+                        } else {
+                            weights[2 * pix + 1] += 1.0;
+                        }
+                    }
+                }
+        }
+        n_ext += tr.cnt.extension;
+        n_shadow += tr.cnt.shadow;
+    };
+    int nt = std::max(1, n_threads);
+    std::vector<std::thread> pool;
+    for (int k = 0; k < nt; ++k)
+        pool.emplace_back(worker);
+    for (auto &t : pool)
+        t.join();
+    if (counts) {
+        counts[0] = n_ext.load();
+        counts[1] = n_shadow.load();
+    }
+    return 0;
+}
+
+// BSDF parity hooks on batches of local directions.
+void oracle_bsdf_eval(const ks_material_desc *mat, const float *wo, const float *wi, uint32_t n, float *f,
+                      float *pdf)
+{
+    Principled b{eval_closure(*mat)};
+    for (uint32_t i = 0; i < n; ++i) {
+        V3 o(wo[3 * i], wo[3 * i + 1], wo[3 * i + 2]), w(wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]);
+        V3 fv;
+        float p;
+        b.eval_and_pdf(o, w, fv, p);
+        f[3 * i] = fv.x;
+        f[3 * i + 1] = fv.y;
+        f[3 * i + 2] = fv.z;
+        pdf[i] = p;
+    }
+}
+
+void oracle_bsdf_sample(const ks_material_desc *mat, const float *wo, const float *u, uint32_t n, float *wi,
+                        float *beta, float *pdf)
+{
+    Principled b{eval_closure(*mat)};
+    for (uint32_t i = 0; i < n; ++i) {
+        V3 o(wo[3 * i], wo[3 * i + 1], wo[3 * i + 2]);
+        V3 w;
+        float p = 0.0f;
+        V3 bt = b.sample(o, w, u[3 * i], u[3 * i + 1], u[3 * i + 2], p);
+        wi[3 * i] = w.x;
+        wi[3 * i + 1] = w.y;
+        wi[3 * i + 2] = w.z;
+        beta[3 * i] = bt.x;
+        beta[3 * i + 1] = bt.y;
+        beta[3 * i + 2] = bt.z;
+        pdf[i] = p;
+    }
+}
+
+} // extern "C"

@@ -29,6 +29,41 @@ class Oracle:
         L.oracle_sobol_matrices01.argtypes = [_vp]
         L.oracle_sobol_matrices01.restype = None
 
+        L.oracle_scene_create.argtypes = [_vp, _vp]
+        L.oracle_scene_create.restype = _vp
+        L.oracle_scene_destroy.argtypes = [_vp]
+        L.oracle_scene_destroy.restype = None
+        L.oracle_light_table.argtypes = [_vp, _vp, _vp]
+        L.oracle_light_table.restype = _u32
+        L.oracle_sky_tables.argtypes = [_vp, _vp, _vp]
+        L.oracle_render.argtypes = [_vp, _vp, _vp, _vp, _vp, ctypes.c_int, _vp]
+        L.oracle_bsdf_eval.argtypes = [_vp, _vp, _vp, _u32, _vp, _vp]
+        L.oracle_bsdf_eval.restype = None
+        L.oracle_bsdf_sample.argtypes = [_vp, _vp, _vp, _u32, _vp, _vp, _vp]
+        L.oracle_bsdf_sample.restype = None
+
+    def scene(self, desc, keepalive=None):
+        return OracleScene(self, desc, keepalive)
+
+    def bsdf_eval(self, material, wo, wi):
+        wo = np.ascontiguousarray(wo, np.float32)
+        wi = np.ascontiguousarray(wi, np.float32)
+        n = len(wo)
+        f = np.empty((n, 3), np.float32)
+        pdf = np.empty(n, np.float32)
+        self.lib.oracle_bsdf_eval(ctypes.byref(material), P(wo), P(wi), n, P(f), P(pdf))
+        return f, pdf
+
+    def bsdf_sample(self, material, wo, u):
+        wo = np.ascontiguousarray(wo, np.float32)
+        u = np.ascontiguousarray(u, np.float32)
+        n = len(wo)
+        wi = np.empty((n, 3), np.float32)
+        beta = np.empty((n, 3), np.float32)
+        pdf = np.empty(n, np.float32)
+        self.lib.oracle_bsdf_sample(ctypes.byref(material), P(wo), P(u), n, P(wi), P(beta), P(pdf))
+        return wi, beta, pdf
+
     def sobol_points(self, full_w, full_h, spp, seed, x0, y0, nx, ny, s0, ns, nd):
         out = np.empty((ny, nx, ns, nd, 3), dtype=np.float32)
         self.lib.oracle_sobol_points(full_w, full_h, spp, seed, x0, y0, nx, ny, s0, ns, nd, P(out))
@@ -38,6 +73,46 @@ class Oracle:
         out = np.empty(104, dtype=np.uint32)
         self.lib.oracle_sobol_matrices01(P(out))
         return out
+
+
+class OracleScene:
+    """CPU restatement of the small_pt scene + render (oracle/src/o_small_pt.cpp)."""
+
+    def __init__(self, oracle, desc, keepalive=None):
+        self.o = oracle
+        self._keep = keepalive
+        dp = ctypes.cast(desc, _vp) if isinstance(desc, ctypes._Pointer) else ctypes.cast(ctypes.pointer(desc), _vp)
+        self.h = oracle.lib.oracle_scene_create(dp, None)
+        assert self.h, "oracle_scene_create failed"
+
+    def light_table(self):
+        n = self.o.lib.oracle_light_table(self.h, None, None)
+        powers = np.empty(n, np.float32)
+        cdf = np.empty(n + 1, np.float32)
+        self.o.lib.oracle_light_table(self.h, P(powers), P(cdf))
+        return powers, cdf
+
+    def sky_tables(self, w, h):
+        cond = np.empty((h, w + 1), np.float32)
+        margin = np.empty(h + 1, np.float32)
+        assert self.o.lib.oracle_sky_tables(self.h, P(cond), P(margin)) == 0
+        return cond, margin
+
+    def render(self, camera, params, threads=None):
+        W, H = params.render_width, params.render_height
+        accum = np.zeros((H, W, 3), np.float64)
+        weights = np.zeros((H, W, 2), np.float64)
+        counts = np.zeros(2, np.uint64)
+        threads = threads or os.cpu_count() or 1
+        self.o.lib.oracle_render(self.h, ctypes.byref(camera), ctypes.byref(params), P(accum), P(weights),
+                                 threads, P(counts))
+        return accum, weights, counts
+
+    def __del__(self):
+        try:
+            self.o.lib.oracle_scene_destroy(self.h)
+        except Exception:
+            pass
 
 
 class RefSBVH:
