@@ -95,19 +95,25 @@ def test_builder_topology_icosphere(ctx, level):
 
 def _check_trace(scene, ref, rays, max_tie_frac=0.0):
     """Hit ids, distances and barycentrics must match bit for bit.  The one documented exception
-    is an exact tie: two triangles of one leaf hit at bit-identical t (duplicate triangles, a
-    shared edge or vertex), where the first one tested wins and the test order inside a leaf
-    follows the reference's std::partition swaps, which the parallel builder does not reproduce.
-    Such rays must still report a hit at the identical distance."""
+    is a near tie: triangles hit at the same or a few-ulp-apart t (duplicate or coplanar
+    overlapping triangles, a shared edge or vertex).  The order of the triangles inside a leaf
+    follows the reference's std::partition swap order, which the parallel builder does not
+    reproduce (leaf contents are identical as multisets); with a near tie that order decides
+    which triangle is accepted first, and because the triangle test compares T against
+    tmax * det in scaled form, it can also decide whether a triangle of a later leaf passes.
+    For such rays the distances must agree within 8 ulp."""
     tri, t, bary = scene.trace(rays)
     rtri, rt, rbary = ref.intersect(rays)
     hit = rtri != 0xFFFFFFFF
     assert np.array_equal(tri != 0xFFFFFFFF, hit), "hit/miss differs"
-    assert np.array_equal(t[hit].view(np.uint32), rt[hit].view(np.uint32)), "hit distances differ"
     tie = tri != rtri
     assert tie.mean() <= max_tie_frac, f"{tie.sum()} of {len(rays)} hit ids differ (ties allowed: {max_tie_frac})"
     same = hit & ~tie
+    assert np.array_equal(t[same].view(np.uint32), rt[same].view(np.uint32)), "hit distances differ"
     assert np.array_equal(bary[same].view(np.uint32), rbary[same].view(np.uint32)), "barycentrics differ"
+    if tie.any():
+        ulps = np.abs(t[tie].view(np.int32).astype(np.int64) - rt[tie].view(np.int32).astype(np.int64))
+        assert ulps.max() <= 8, f"tie distances differ by {ulps.max()} ulp"
     occ, _, _ = scene.trace(rays, any_hit=True)
     rocc, _, _ = ref.intersect(rays, any_hit=True)
     assert np.array_equal(occ, rocc), "occlusion results differ"
