@@ -1,0 +1,322 @@
+#!/usr/bin/env python
+"""small_pt path tracing throughput on B200.
+
+Workload: the single-mesh scene: icosphere subdivided 8x (1,310,720 triangles) with seeded fBm
+radial displacement (amplitude 0.05) on a ground quad, one principled material per 1024-triangle
+patch (roughness U[0.05,1], metallic Bernoulli(0.3), basecolor U[0,1]^3), a procedural
+2048x1024 FP32 HDR sky (gradient + sun lobe of 1e4), rendered at 1024x1024, 256 spp, depth 12.
+All inputs are generated from a fixed seed (synthetic data).
+
+One step = one full render of that frame through ks_small_pt_render_device (scene and BVH
+resident in HBM, FP64 accumulators on the device).  value = Mrays/s (closest-hit + shadow
+queries) over the K timed steps, device time from CUDA events on the library's stream, max over
+ranks.  e2e = the same metric through the host-buffer C ABI (scene upload, GPU SBVH build,
+render, FP64 image download every step).
+
+--impl reference runs the CPU implementation of the path on the host cores (the oracle's
+restatement of small_pt over the reference's own SBVH traversal), each step a bounded crop of the
+same frame.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "icosphere_l8_1310722tris_1024x1024_256spp_depth12_sky2048x1024"
+W_RES, H_RES, SPP, BOUNCES = 1024, 1024, 256, 12
+# CPU sample: a centred crop of the same frame at the full 256 spp
+CPU_CROP = 128
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--e2e-steps", type=int, default=None, help="steps of the end-to-end leg (default: --steps)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    # reduced frames of the same scene, for profiling captures only (not a bench line)
+    ap.add_argument("--spp", type=int, default=None)
+    ap.add_argument("--res", type=int, default=None)
+    a = ap.parse_args()
+    global W_RES, H_RES, SPP, WORKLOAD
+    if a.spp or a.res:
+        SPP = a.spp or SPP
+        W_RES = H_RES = a.res or W_RES
+        WORKLOAD = f"icosphere_l8_1310722tris_{W_RES}x{H_RES}_{SPP}spp_depth12_sky2048x1024 (profiling case)"
+    return a
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+def make_generated(ks):
+    return ks.Generated("icosphere", 0, level=8, sky=(2048, 1024), resolution=(W_RES, H_RES))
+
+
+def cpu_crop_params(ks, crop=CPU_CROP):
+    x0 = (W_RES - crop) // 2
+    return ks.SmallPTParams.make(render_width=W_RES, render_height=H_RES, spp=SPP, bounces=BOUNCES,
+                                 crop_start_x=x0, crop_start_y=x0, crop_width=crop, crop_height=crop)
+
+
+def run_cpu(ks, g, steps, warmup, threads):
+    """The oracle (CPU restatement over the reference SBVH) on a bounded crop; returns stats."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib
+    orc = oracle_lib.load()
+    cam = ks.camera_perspective(g.camera_to_world, g.vfov, g.aspect)
+    t0 = time.perf_counter()
+    sc = orc.scene(g.desc)
+    setup_s = time.perf_counter() - t0
+    p = cpu_crop_params(ks)
+    times, rays = [], []
+    for k in range(warmup + steps):
+        t0 = time.perf_counter()
+        _, _, cnt = sc.render(cam, p, threads=threads)
+        dt = time.perf_counter() - t0
+        if k >= warmup:
+            times.append(dt)
+            rays.append(int(cnt[0]) + int(cnt[1]))
+    return dict(seconds=sum(times), rays=sum(rays), steps=steps, setup_s=setup_s,
+                sample=f"{CPU_CROP}x{CPU_CROP} centre crop of the {W_RES}x{H_RES} frame at {SPP} spp, depth "
+                       f"{BOUNCES} ({CPU_CROP * CPU_CROP * SPP} paths per step)")
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                rows.append(f)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per closest-hit query from the committed ncu summary (None if absent)."""
+    p = os.path.join(ROOT, "profiles", "k_extend_icosphere_l8.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("dram_bytes_per_query:"):
+            return float(line.split(":")[1])
+    return None
+
+
+def reference_arm(args):
+    rank, local_rank, world = dist_env()
+    if rank != 0:
+        return 0
+    import keepsake_b200 as ks
+    g = make_generated(ks)
+    threads = os.cpu_count() or 1
+    r = run_cpu(ks, g, args.steps, args.warmup, threads)
+    v = r["rays"] / r["seconds"] / 1e6
+    line = {
+        "impl": "reference", "metric": "Mrays/s (closest-hit + shadow queries), small_pt on the icosphere frame",
+        "value": v, "unit": "Mrays/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * r["seconds"] / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
+        "config": {"workload": WORKLOAD, "sample": r["sample"]},
+        "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": threads, "kind": "port", "sample": r["sample"]},
+        "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+    rank, local_rank, world = dist_env()
+    import numpy as np
+    import torch
+    torch.cuda.set_device(local_rank)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+        pg = dist
+    import keepsake_b200 as ks
+
+    ctx = ks.Context(local_rank)
+    g = make_generated(ks)
+    cam = ks.camera_perspective(g.camera_to_world, g.vfov, g.aspect)
+    # replicas: each rank renders the full frame with its own sampler seed
+    params = ks.SmallPTParams.make(render_width=W_RES, render_height=H_RES, spp=SPP, bounces=BOUNCES, rng_seed=rank)
+    scene = ks.Scene(ctx, g.desc)
+    build_ms = scene.build_bvh()
+    acc = torch.zeros((H_RES, W_RES, 3), dtype=torch.float64, device="cuda")
+    wts = torch.zeros((H_RES, W_RES, 2), dtype=torch.float64, device="cuda")
+
+    def step():
+        acc.zero_()
+        wts.zero_()
+        torch.cuda.synchronize()
+        scene.render_device(cam, params, acc.data_ptr(), wts.data_ptr())
+        return scene.stats()
+
+    for _ in range(args.warmup):
+        step()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    wall0 = time.perf_counter()
+    stats = [step() for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    wall = time.perf_counter() - wall0
+    clk = clocks.stop()
+
+    dev_ms = sum(s.ms_total for s in stats)
+    rays = sum(s.extension_rays + s.shadow_rays for s in stats)
+    paths = sum(s.paths for s in stats)
+    if pg:
+        t = torch.tensor([dev_ms], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        dev_ms = float(t.item())
+        r = torch.tensor([rays, paths], dtype=torch.float64, device="cuda")
+        pg.all_reduce(r)
+        rays, paths = int(r[0].item()), int(r[1].item())
+    value = rays / (dev_ms / 1e3) / 1e6
+
+    # roofline of the dominant kernel (closest-hit traversal); algorithmic bytes per query:
+    # 64 B per interior node fetched + 48 B per triangle tested + 32 B ray read + 16 B hit write
+    ext_ms = sum(s.ms_extend for s in stats)
+    shade_ms = sum(s.ms_shade for s in stats)
+    shadow_ms = sum(s.ms_shadow for s in stats)
+    ext_q = sum(s.extension_rays for s in stats)
+    ext_bytes = sum(s.ext_nodes * 64 + s.ext_tris * 48 for s in stats) + ext_q * (32 + 16)
+    launches = sum(s.iterations for s in stats)
+    peak, peak_kind = measured_peaks()
+    achieved = ext_bytes / (ext_ms / 1e3) / 1e9
+    tpq = profile_traffic()
+    roofline = {"kernel": "k_extend (closest-hit SBVH traversal)", "bound": "hbm", "achieved": achieved,
+                "peak": peak, "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": (tpq * ext_q / launches) if tpq else None,
+                "algorithmic_bytes_per_launch": ext_bytes / launches,
+                "nodes_per_query": sum(s.ext_nodes for s in stats) / ext_q,
+                "tris_per_query": sum(s.ext_tris for s in stats) / ext_q,
+                "share": {"extend": ext_ms / dev_ms, "shade_raygen": shade_ms / dev_ms, "shadow": shadow_ms / dev_ms}}
+
+    # ---- end to end through the host-buffer C ABI ----
+    e2e_steps = args.e2e_steps if args.e2e_steps is not None else args.steps
+    h2d = sum(m["vertices"].nbytes + m["indices"].nbytes for m in g.meshes)
+    h2d += len(g.materials) * 72 + (g.sky_map.nbytes if g.sky_map is not None else 0)
+    d2h = W_RES * H_RES * 5 * 8
+    e2e_rays, e2e_t = 0, 0.0
+    for k in range(e2e_steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sc = ks.Scene(ctx, g.desc)
+        sc.build_bvh()
+        sc.render(cam, params)
+        st = sc.stats()
+        sc.close()
+        e2e_t += time.perf_counter() - t0
+        e2e_rays += st.extension_rays + st.shadow_rays
+    if pg:
+        t = torch.tensor([e2e_t], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_t = float(t.item())
+        r = torch.tensor([e2e_rays], dtype=torch.float64, device="cuda")
+        pg.all_reduce(r)
+        e2e_rays = int(r.item())
+    e2e = {"value": e2e_rays / e2e_t / 1e6 if e2e_t > 0 else None, "unit": "Mrays/s", "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": d2h, "steps": e2e_steps, "timing": "host wall clock around synchronous C-ABI calls"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        r = run_cpu(ks, g, 1, 0, threads)
+        cpu = {"value": r["rays"] / r["seconds"] / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "port",
+               "sample": r["sample"] + "; oracle restatement of small_pt over the reference cuda/sbvh.cu traversal"}
+
+    if rank == 0:
+        line = {
+            "metric": "Mrays/s (closest-hit + shadow queries), small_pt on the icosphere frame",
+            "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded procedural scene)",
+            "config": {"workload": WORKLOAD, "triangles": g.n_triangles, "resolution": [W_RES, H_RES], "spp": SPP,
+                       "depth": BOUNCES, "parallelism": f"replicas{world}",
+                       "l2": "inputs larger than L2 (BVH + triangles + sky > 126 MB)",
+                       "bvh_build_ms": build_ms},
+            "mpaths_per_s": paths / (dev_ms / 1e3) / 1e6,
+            "wall_ms_per_step": 1000.0 * wall / args.steps,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": sum(s.kernel_launches for s in stats),
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    scene.close()
+    ctx.close()
+    if pg:
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

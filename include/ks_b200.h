@@ -206,6 +206,10 @@ typedef struct ks_render_stats {
     float ms_extend;         /* closest-hit kernel time, summed */
     float ms_shade;          /* shading kernel time (incl. ray generation), summed */
     float ms_shadow;         /* any-hit kernel time, summed */
+    uint64_t ext_nodes;      /* interior SBVH nodes fetched by closest-hit queries (64 B each) */
+    uint64_t ext_tris;       /* triangles tested by closest-hit queries (48 B each) */
+    uint64_t shadow_nodes;   /* interior nodes fetched by any-hit queries */
+    uint64_t shadow_tris;    /* triangles tested by any-hit queries */
 } ks_render_stats;
 
 ks_status ks_render_stats_last(const ks_scene *scene, ks_render_stats *out);

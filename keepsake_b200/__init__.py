@@ -185,7 +185,8 @@ _sig("ks_small_pt_params_default", [ctypes.POINTER(SmallPTParams)], None)
 class RenderStats(ctypes.Structure):
     _fields_ = [("paths", ctypes.c_uint64), ("extension_rays", ctypes.c_uint64), ("shadow_rays", ctypes.c_uint64),
                 ("iterations", _u32), ("kernel_launches", _u32), ("ms_total", _f32), ("ms_extend", _f32),
-                ("ms_shade", _f32), ("ms_shadow", _f32)]
+                ("ms_shade", _f32), ("ms_shadow", _f32), ("ext_nodes", ctypes.c_uint64),
+                ("ext_tris", ctypes.c_uint64), ("shadow_nodes", ctypes.c_uint64), ("shadow_tris", ctypes.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -245,34 +245,72 @@ __global__ void k_raygen(RenderParams rp, PathBuf pb, uint32_t base_slot, uint64
     pb.L_smp[slot] = make_float4(0.0f, 0.0f, 0.0f, fbits((uint32_t)s));
 }
 
-__global__ void __launch_bounds__(128) k_extend(SceneView sv, PathBuf pb, uint32_t count, float4 *hits,
-                                                int *overflow)
+// Adds a per-thread work count into two 64-bit device counters, one atomic per warp.
+KS_D void flush_counts(const TravCount &c, unsigned long long *dst)
 {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-        float4 a = pb.o_pdf[i], b = pb.d_info[i];
-        RayQuery q;
-        q.o = mk(a.x, a.y, a.z);
-        q.d = mk(b.x, b.y, b.z);
-        q.tmin = 0.0f;
-        q.tmax = kInf;
-        Hit h;
-        int of = 0;
-        traverse<false>(sv.nodes, sv.prim_tris, sv.root_ref, sv.root_count, sv.bmin, sv.bmax, q, 2, h, of);
-        if (of)
-            atomicOr(overflow, 1);
-        hits[i] = h.tri != ~0u ? make_float4(h.t, h.b1, h.b2, fbits(h.slot)) : make_float4(0, 0, 0, fbits(~0u));
+    unsigned long long n = c.nodes, t = c.tris;
+    for (int o = 16; o > 0; o >>= 1) {
+        n += __shfl_xor_sync(0xffffffffu, n, o);
+        t += __shfl_xor_sync(0xffffffffu, t, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(dst, n);
+        atomicAdd(dst + 1, t);
     }
 }
 
-__global__ void __launch_bounds__(128) k_shade(SceneView sv, RenderParams rp, PathBuf cur, PathBuf nxt,
-                                               const float4 *hits, uint32_t count, uint32_t *next_count,
-                                               ShadowBuf sb, uint32_t *shadow_count, double *accum,
-                                               double *weights)
+// Closest hit for every queued ray; the path index goes to the hit queue or the miss queue.
+__global__ void __launch_bounds__(128) k_extend(SceneView sv, PathBuf pb, uint32_t count, float4 *hits,
+                                                uint32_t *hit_queue, uint32_t *miss_queue, uint32_t *queue_counts,
+                                                int *overflow, unsigned long long *work)
 {
+    TravCount tc;
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += stride) {
         uint32_t i = base + threadIdx.x;
-        bool valid = i < count;
+        bool valid = i < count, is_hit = false;
+        if (valid) {
+            float4 a = pb.o_pdf[i], b = pb.d_info[i];
+            RayQuery q;
+            q.o = mk(a.x, a.y, a.z);
+            q.d = mk(b.x, b.y, b.z);
+            q.tmin = 0.0f;
+            q.tmax = kInf;
+            Hit h;
+            int of = 0;
+            traverse<false>(sv.nodes, sv.prim_tris, sv.root_ref, sv.root_count, sv.bmin, sv.bmax, q, 2, h, of,
+                            &tc);
+            if (of)
+                atomicOr(overflow, 1);
+            is_hit = h.tri != ~0u;
+            hits[i] = is_hit ? make_float4(h.t, h.b1, h.b2, fbits(h.slot)) : make_float4(0, 0, 0, fbits(~0u));
+        }
+        uint32_t jh = warp_append(queue_counts, valid && is_hit);
+        uint32_t jm = warp_append(queue_counts + 1, valid && !is_hit);
+        if (valid) {
+            if (is_hit)
+                hit_queue[jh] = i;
+            else
+                miss_queue[jm] = i;
+        }
+    }
+    flush_counts(tc, work);
+}
+
+// Shading of the paths listed in `queue` (indices into the current path buffer).  kMiss = true
+// handles the rays that left the scene, kMiss = false the rays that hit a triangle; the extension
+// kernel sorts the two kinds into separate queues so that a warp runs one of the two code paths.
+template <bool kMiss>
+__global__ void __launch_bounds__(128) k_shade(SceneView sv, RenderParams rp, PathBuf cur, PathBuf nxt,
+                                               const float4 *hits, const uint32_t *queue,
+                                               const uint32_t *queue_count, uint32_t *next_count, ShadowBuf sb,
+                                               uint32_t *shadow_count, double *accum, double *weights)
+{
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t count = *queue_count;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += stride) {
+        bool valid = base + threadIdx.x < count;
+        uint32_t i = valid ? queue[base + threadIdx.x] : 0u;
         bool cont = false, shadow = false;
         // outputs
         f3 n_o, n_d, n_beta, L = mk(0, 0, 0), sh_o, sh_d, sh_c;
@@ -292,7 +330,8 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sv, RenderParams rp, Pa
             smp = bits(d.w);
             float4 h = hits[i];
             uint32_t slot = bits(h.w);
-            if (slot == ~0u) {
+            if constexpr (kMiss) {
+                (void)slot;
                 // miss: unidirectional sky strategy (small_pt.cpp:83-110)
                 if (sv.sky_kind != 0) {
                     f3 wi = normalize(rd);
@@ -440,9 +479,11 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sv, RenderParams rp, Pa
 }
 
 __global__ void __launch_bounds__(128) k_shadow(SceneView sv, ShadowBuf sb, const uint32_t *shadow_count,
-                                                PathBuf nxt, double *accum, double *weights, int *overflow)
+                                                PathBuf nxt, double *accum, double *weights, int *overflow,
+                                                unsigned long long *work)
 {
     const uint32_t n = *shadow_count;
+    TravCount tc;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float4 a = sb.o_tmax[i], b = sb.d_target[i];
         RayQuery q;
@@ -452,7 +493,8 @@ __global__ void __launch_bounds__(128) k_shadow(SceneView sv, ShadowBuf sb, cons
         q.tmax = a.w;
         Hit h;
         int of = 0;
-        bool occ = traverse<true>(sv.nodes, sv.prim_tris, sv.root_ref, sv.root_count, sv.bmin, sv.bmax, q, 2, h, of);
+        bool occ =
+            traverse<true>(sv.nodes, sv.prim_tris, sv.root_ref, sv.root_count, sv.bmin, sv.bmax, q, 2, h, of, &tc);
         if (of)
             atomicOr(overflow, 1);
         uint32_t target = bits(b.w);
@@ -471,6 +513,7 @@ __global__ void __launch_bounds__(128) k_shadow(SceneView sv, ShadowBuf sb, cons
             nxt.L_smp[target] = l;
         }
     }
+    flush_counts(tc, work);
 }
 
 } // namespace
@@ -483,7 +526,8 @@ struct RenderWork
     DevBuf<float4> state[2][4];
     DevBuf<float4> hits;
     DevBuf<float4> shadow[4];
-    DevBuf<uint32_t> counters; // [next, shadow]
+    DevBuf<uint32_t> counters; // [next, shadow, hit queue, miss queue]
+    DevBuf<uint32_t> queue[2]; // hit / miss path indices
     DevBuf<int> overflow;
     uint32_t capacity = 0;
 };
@@ -540,10 +584,15 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
         for (int f = 0; f < 4; ++f)
             KS_CUDA_TRY(ctx, w.state[b][f].alloc(w.capacity));
     KS_CUDA_TRY(ctx, w.hits.alloc(w.capacity));
+    KS_CUDA_TRY(ctx, w.queue[0].alloc(w.capacity));
+    KS_CUDA_TRY(ctx, w.queue[1].alloc(w.capacity));
     for (int f = 0; f < 4; ++f)
         KS_CUDA_TRY(ctx, w.shadow[f].alloc(w.capacity));
-    KS_CUDA_TRY(ctx, w.counters.alloc(2));
+    KS_CUDA_TRY(ctx, w.counters.alloc(4));
     KS_CUDA_TRY(ctx, w.overflow.alloc(1));
+    DevBuf<unsigned long long> work; // ext nodes, ext tris, shadow nodes, shadow tris
+    KS_CUDA_TRY(ctx, work.alloc(4));
+    KS_CUDA_TRY(ctx, cudaMemsetAsync(work.ptr, 0, 4 * sizeof(unsigned long long), st));
     KS_CUDA_TRY(ctx, cudaMemsetAsync(w.overflow.ptr, 0, sizeof(int), st));
     PathBuf pb[2];
     for (int b = 0; b < 2; ++b)
@@ -585,18 +634,24 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
             issued += n_new;
             uint32_t count = cur_count + n_new;
             stats.extension_rays += count;
-            cudaMemsetAsync(w.counters.ptr, 0, sizeof(uint32_t) * 2, st);
+            // counters: [0] next paths, [1] shadow rays, [2] hit queue, [3] miss queue
+            cudaMemsetAsync(w.counters.ptr, 0, sizeof(uint32_t) * 4, st);
             unsigned grid = std::min<unsigned>((count + 127) / 128, max_grid);
             cudaEventRecord(ev[1], st);
-            k_extend<<<grid, 128, 0, st>>>(sv, pb[cur], count, w.hits.ptr, w.overflow.ptr);
+            k_extend<<<grid, 128, 0, st>>>(sv, pb[cur], count, w.hits.ptr, w.queue[0].ptr, w.queue[1].ptr,
+                                           w.counters.ptr + 2, w.overflow.ptr, work.ptr);
             cudaEventRecord(ev[2], st);
-            k_shade<<<grid, 128, 0, st>>>(sv, rp, pb[cur], pb[1 - cur], w.hits.ptr, count, w.counters.ptr, sb,
-                                          w.counters.ptr + 1, d_accum, d_weights);
+            k_shade<false><<<grid, 128, 0, st>>>(sv, rp, pb[cur], pb[1 - cur], w.hits.ptr, w.queue[0].ptr,
+                                                 w.counters.ptr + 2, w.counters.ptr, sb, w.counters.ptr + 1, d_accum,
+                                                 d_weights);
+            k_shade<true><<<grid, 128, 0, st>>>(sv, rp, pb[cur], pb[1 - cur], w.hits.ptr, w.queue[1].ptr,
+                                                w.counters.ptr + 3, w.counters.ptr, sb, w.counters.ptr + 1, d_accum,
+                                                d_weights);
             cudaEventRecord(ev[3], st);
             k_shadow<<<grid, 128, 0, st>>>(sv, sb, w.counters.ptr + 1, pb[1 - cur], d_accum, d_weights,
-                                           w.overflow.ptr);
+                                           w.overflow.ptr, work.ptr + 2);
             cudaEventRecord(ev[4], st);
-            stats.kernel_launches += 3;
+            stats.kernel_launches += 4;
             cudaMemcpyAsync(h_counts, w.counters.ptr, sizeof(uint32_t) * 2, cudaMemcpyDeviceToHost, st);
             err = cudaStreamSynchronize(st);
             if (err != cudaSuccess)
@@ -647,6 +702,13 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
     if (err == cudaSuccess)
         err = cudaMemcpy(&overflow, w.overflow.ptr, sizeof(int), cudaMemcpyDeviceToHost);
     cudaFreeHost(h_counts);
+    unsigned long long h_work[4] = {0, 0, 0, 0};
+    if (err == cudaSuccess)
+        err = cudaMemcpy(h_work, work.ptr, sizeof(h_work), cudaMemcpyDeviceToHost);
+    stats.ext_nodes = h_work[0];
+    stats.ext_tris = h_work[1];
+    stats.shadow_nodes = h_work[2];
+    stats.shadow_tris = h_work[3];
     scene->last_stats = stats;
     if (stats.iterations == 0xffffffffu)
         return fail(ctx, KS_ERR_WATCHDOG, "ks_small_pt_render: wavefront iteration limit reached");

@@ -89,6 +89,19 @@ __global__ void k_sky_power_rows(SceneView s, double *row_sums)
     row_sums[3 * row + 2] = rs.z;
 }
 
+// Guide tables (see cdf_find_guided): one thread per CDF row.
+__global__ void k_guide(const float *cdf, uint32_t n, uint32_t rows, uint32_t *guide)
+{
+    uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= rows)
+        return;
+    const float *c = cdf + (size_t)r * (n + 1);
+    for (uint32_t k = 0; k < kGuide; ++k) {
+        float t = (float)k / (float)kGuide;
+        guide[(size_t)r * kGuide + k] = cdf_find(c, n, t);
+    }
+}
+
 // DistribTable on the host, identical to distrib.cpp:9-29.
 std::vector<float> host_cdf(const float *f, uint32_t n, float *acc_out = nullptr)
 {
@@ -179,6 +192,8 @@ SceneView make_view(const ks_scene *s)
     v.sky_map = s->sky_map.ptr;
     v.sky_cond = s->sky_cond.ptr;
     v.sky_margin = s->sky_margin.ptr;
+    v.sky_cond_guide = s->sky_cond_guide.ptr;
+    v.sky_margin_guide = s->sky_margin_guide.ptr;
     return v;
 }
 
@@ -248,6 +263,10 @@ ks_status build_lights(ks_scene *s)
         KS_CUDA_TRY(ctx, s->sky_margin.alloc(margin.size()));
         KS_CUDA_TRY(ctx, cudaMemcpyAsync(s->sky_margin.ptr, margin.data(), sizeof(float) * margin.size(),
                                          cudaMemcpyHostToDevice, st));
+        KS_CUDA_TRY(ctx, s->sky_cond_guide.alloc((size_t)h * kGuide));
+        KS_CUDA_TRY(ctx, s->sky_margin_guide.alloc(kGuide));
+        k_guide<<<(h + 127) / 128, 128, 0, st>>>(s->sky_cond.ptr, (uint32_t)w, (uint32_t)h, s->sky_cond_guide.ptr);
+        k_guide<<<1, 32, 0, st>>>(s->sky_margin.ptr, (uint32_t)h, 1u, s->sky_margin_guide.ptr);
         // power (light.cpp:136-159)
         SceneView v = make_view(s);
         k_sky_power_rows<<<(h + 127) / 128, 128, 0, st>>>(v, row_sum.ptr);

@@ -42,6 +42,8 @@ struct SceneView
     const float4 *sky_map;
     const float *sky_cond;   // sky_h rows of sky_w + 1
     const float *sky_margin; // sky_h + 1
+    const uint32_t *sky_cond_guide;   // sky_h rows of kGuide
+    const uint32_t *sky_margin_guide; // kGuide
 };
 
 // ---- distribution tables ----------------------------------------------------------------------
@@ -73,6 +75,39 @@ KS_D float distrib_sample_linear(const float *cdf, uint32_t n, float u, float &p
     index = cdf_find(cdf, n, u);
     float nf = (float)n;
     float c0 = cdf[index], c1 = cdf[index + 1];
+    pdf = (c1 - c0) * nf;
+    float du = (u - c0) / (c1 - c0);
+    return ((float)index + du) / nf;
+}
+
+// Guide (cut-point) table of a CDF: guide[k] = upper_bound(cdf, k / G) - 1 for k < G.  For u in
+// [k/G, (k+1)/G) the bin upper_bound(cdf, u) - 1 lies in [guide[k], guide[k+1]] (guide[G] = n-1),
+// so the search touches a few entries instead of log2(n) dependent loads, with the same result.
+constexpr uint32_t kGuide = 128;
+
+KS_D uint32_t cdf_find_guided(const float *cdf, uint32_t n, const uint32_t *guide, float u)
+{
+    uint32_t k = (uint32_t)(u * (float)kGuide); // exact: kGuide is a power of two, u < 1
+    uint32_t lo = __ldg(&guide[k]);
+    uint32_t hi = k + 1 < kGuide ? __ldg(&guide[k + 1]) : n - 1;
+    // largest i in [lo, hi] with cdf[i] <= u
+    while (lo < hi) {
+        uint32_t mid = (lo + hi + 1) >> 1;
+        if (__ldg(&cdf[mid]) <= u)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+KS_D float distrib_sample_linear_guided(const float *cdf, uint32_t n, const uint32_t *guide, float u, float &pdf,
+                                        uint32_t &index)
+{
+    u = clamp_u(u);
+    index = cdf_find_guided(cdf, n, guide, u);
+    float nf = (float)n;
+    float c0 = __ldg(&cdf[index]), c1 = __ldg(&cdf[index + 1]);
     pdf = (c1 - c0) * nf;
     float du = (u - c0) / (c1 - c0);
     return ((float)index + du) / nf;
@@ -156,8 +191,9 @@ KS_D f3 sky_sample(const SceneView &s, float u0, float u1, f3 &wi, float &wi_dis
 {
     float pdf_m, pdf_c;
     uint32_t vi, ui;
-    float vs = distrib_sample_linear(s.sky_margin, (uint32_t)s.sky_h, u1, pdf_m, vi);
-    float us = distrib_sample_linear(s.sky_cond + (size_t)vi * (s.sky_w + 1), (uint32_t)s.sky_w, u0, pdf_c, ui);
+    float vs = distrib_sample_linear_guided(s.sky_margin, (uint32_t)s.sky_h, s.sky_margin_guide, u1, pdf_m, vi);
+    float us = distrib_sample_linear_guided(s.sky_cond + (size_t)vi * (s.sky_w + 1), (uint32_t)s.sky_w,
+                                            s.sky_cond_guide + (size_t)vi * kGuide, u0, pdf_c, ui);
     pdf = pdf_m * pdf_c;
     if (pdf == 0.0f)
         return mk(0, 0, 0);

@@ -71,34 +71,47 @@ KS_HD uint32_t owen_scramble(uint32_t v, uint32_t seed)
     return reverse_bits32(v);
 }
 
-KS_HD uint32_t sobol_dim1_column(int k)
+// FastOwenScrambler applied to a value given in bit-reversed form: owen_scramble(reverse(x)).
+KS_HD uint32_t owen_scramble_reversed(uint32_t x, uint32_t seed)
 {
-    uint32_t p = 0x80000000u;
-    for (int i = 0; i < (k & 31); ++i)
-        p ^= p >> 1;
-    return p;
+    x ^= x * 0x3d20adeau;
+    x += seed;
+    x *= (seed >> 16) | 1u;
+    x ^= x * 0x05526c56u;
+    x ^= x * 0x53a22864u;
+    return reverse_bits32(x);
 }
 
-// sobol_sample(a, dim, FastOwenScrambler(seed)) for dim in {0, 1} (sobol.h:35-49)
+// sobol_sample(a, dim, FastOwenScrambler(seed)) for dim in {0, 1} (sobol.h:35-49).
+//   dim 0: v = reverse(a mod 2^32)                         (columns 0x80000000 >> k, zero for k >= 32)
+//   dim 1: v = XOR of P[k mod 32] over the set bits k of a. Bit 31-j of P[k] is C(k, j) mod 2, i.e.
+//          set iff j is a bit-subset of k (Lucas), so reverse(v) is the GF(2) superset-sum transform
+//          of the folded index: five masked shift-xor steps instead of a 52-column loop.
+// The scrambler reverses its input first, so both cases hand it the reversed form directly.
 KS_HD float sobol_sample_01(uint64_t a, int dim, uint32_t seed)
 {
-    uint32_t v = 0;
-    if (dim == 0) {
-        v = reverse_bits32((uint32_t)a);
-    } else {
-        // columns repeat with period 32; fold the index bits accordingly
-        uint32_t folded = (uint32_t)a ^ (uint32_t)(a >> 32);
-        // P[k] for the set bits of the folded index: P is the Pascal triangle mod 2 on reversed bits
-        uint32_t p = 0x80000000u;
-        for (int k = 0; k < 32; ++k) {
-            if (folded & (1u << k))
-                v ^= p;
-            p ^= p >> 1;
-        }
+    uint32_t x = (uint32_t)a;
+    if (dim != 0) {
+        x ^= (uint32_t)(a >> 32); // columns repeat with period 32
+        x ^= (x >> 1) & 0x55555555u;
+        x ^= (x >> 2) & 0x33333333u;
+        x ^= (x >> 4) & 0x0f0f0f0fu;
+        x ^= (x >> 8) & 0x00ff00ffu;
+        x ^= (x >> 16) & 0x0000ffffu;
     }
-    v = owen_scramble(v, seed);
+    uint32_t v = owen_scramble_reversed(x, seed);
     float f = (float)v * 0x1p-32f;
     return f < kOneMinusEps ? f : kOneMinusEps;
+}
+
+// mix_bits (hash.h:206-214) of a value below 2^32, then (>> 24) % 24 as in sobol.h:209.
+KS_HD int digit_perm_index(uint32_t x)
+{
+    uint64_t v = mix_bits64((uint64_t)x);
+    uint64_t y = v >> 24; // < 2^40
+    // y % 24 without a 64-bit division: 2^32 = 16 (mod 24)
+    uint32_t hi = (uint32_t)(y >> 32), lo = (uint32_t)y;
+    return (int)((hi * 16u + lo % 24u) % 24u);
 }
 
 KS_HD uint32_t part1by1(uint32_t x)
@@ -144,23 +157,26 @@ struct SobolSampler
         return s;
     }
 
+    // get_sample_index (sobol.h:168-222).  The Morton index is built in 32 bits (sobol.h:145), so
+    // every `higher digits` value is below 2^32 and the loop runs in 32-bit integers; only the
+    // permuted index itself can exceed 32 bits (up to 2 * n_base4_digits).
     KS_HD uint64_t sample_index() const
     {
         uint64_t out = 0;
+        const uint32_t m = (uint32_t)morton_index;
         const bool pow2 = (log2_spp & 1) != 0;
         const int last_digit = pow2 ? 1 : 0;
-        const uint64_t dim_mix = (uint64_t)(0x55555555u * (uint32_t)dimension);
+        const uint32_t dim_mix = 0x55555555u * (uint32_t)dimension;
         for (int i = n_base4_digits - 1; i >= last_digit; --i) {
             int shift = 2 * i - (pow2 ? 1 : 0);
-            int digit = (int)((morton_index >> shift) & 3);
-            uint64_t higher = morton_index >> (shift + 2);
-            int p = (int)((mix_bits64(higher ^ dim_mix) >> 24) % 24);
-            digit = digit_permutation(p, digit);
-            out |= (uint64_t)digit << shift;
+            uint32_t digit = shift >= 32 ? 0u : ((m >> shift) & 3u);
+            uint32_t higher = shift + 2 >= 32 ? 0u : (m >> (shift + 2));
+            int p = digit_perm_index(higher ^ dim_mix);
+            out |= (uint64_t)digit_permutation(p, (int)digit) << shift;
         }
         if (pow2) {
-            int digit = (int)(morton_index & 1);
-            out |= (uint64_t)(digit ^ (int)(mix_bits64((morton_index >> 1) ^ dim_mix) & 1));
+            uint32_t digit = m & 1u;
+            out |= (uint64_t)(digit ^ (uint32_t)(mix_bits64((uint64_t)((m >> 1) ^ dim_mix)) & 1u));
         }
         return out;
     }

@@ -92,6 +92,7 @@ struct ks_scene
     float sky_l2w[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, sky_w2l[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
     ksb::DevBuf<float4> sky_map;
     ksb::DevBuf<float> sky_cond, sky_margin;
+    ksb::DevBuf<uint32_t> sky_cond_guide, sky_margin_guide;
     int sky_w = 0, sky_h = 0;
     ks_render_stats last_stats{};
 };

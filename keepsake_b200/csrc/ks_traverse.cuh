@@ -191,10 +191,16 @@ struct Hit
 constexpr int kStackDepth = 64;
 
 // Closest hit (any_hit = false) or occlusion (any_hit = true) against the scene's SBVH.
+// Work counters of one query: interior nodes fetched (64 B each) and triangles tested (48 B each).
+struct TravCount
+{
+    uint32_t nodes = 0, tris = 0;
+};
+
 template <bool kAnyHit>
 KS_D bool traverse(const TravNode *__restrict__ nodes, const float4 *__restrict__ tris, uint32_t root_ref,
                    uint32_t root_count, const float root_bmin[3], const float root_bmax[3], RayQuery ray,
-                   int culling, Hit &hit, int &overflow)
+                   int culling, Hit &hit, int &overflow, TravCount *count = nullptr)
 {
     hit.tri = ~0u;
     const TriHelper th = make_tri_helper(ray.d);
@@ -212,6 +218,8 @@ KS_D bool traverse(const TravNode *__restrict__ nodes, const float4 *__restrict_
         if (ref & kLeafBit) {
             uint32_t first = ref & ~kLeafBit;
             for (uint32_t k = 0; k < cnt; ++k) {
+                if (count)
+                    count->tris++;
                 const float4 *p = tris + 3 * (size_t)(first + k);
                 float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2);
                 f3 v0 = mk(a.x, a.y, a.z), v1 = mk(b.x, b.y, b.z), v2 = mk(c.x, c.y, c.z);
@@ -236,6 +244,8 @@ KS_D bool traverse(const TravNode *__restrict__ nodes, const float4 *__restrict_
             }
         } else {
             const TravNode *n = nodes + ref;
+            if (count)
+                count->nodes++;
             float4 A = __ldg(&n->a), B = __ldg(&n->b), C = __ldg(&n->c);
             uint4 D = __ldg(&n->d);
             float lmin[3] = {A.x, A.y, A.z}, lmax[3] = {A.w, B.x, B.y};
