@@ -138,6 +138,19 @@ ks_status ks_sbvh_export(const ks_scene *scene, float *node_bounds, uint32_t *no
 ks_status ks_trace_rays(ks_scene *scene, const float *rays, uint32_t n, int any_hit, int culling, uint32_t *tri_idx,
                         float *t, float *bary);
 
+/* ks_trace_rays without any device allocation.  No counterpart in the reference: it exists for
+ * callers that may not allocate device memory (a host application that owns the device-memory
+ * budget through its own allocator, or a frame loop that forbids cudaMalloc/cudaFree).  Rays and
+ * results are staged in one static device array of the library (KS_TRACE_NOALLOC_MAX_RAYS rays,
+ * 3.4 MB, resident on every GPU that loads the library until the process exits); larger n is
+ * rejected with KS_ERR_INVALID_ARGUMENT.  The first call on a device looks up that array's
+ * device address (cudaGetSymbolAddress): make that first call before any stream capture.  All
+ * calls share the array, so calls that overlap on the GPU (two contexts on one device, two
+ * threads) race; serialise them. */
+#define KS_TRACE_NOALLOC_MAX_RAYS 65536
+ks_status ks_trace_rays_noalloc(ks_scene *scene, const float *rays, uint32_t n, int any_hit, int culling,
+                                uint32_t *tri_idx, float *t, float *bary);
+
 /* ---------------------------------------------------------------------------------------------
  * Camera.  The render consumes the matrices of a reference `Camera` (camera.cpp:85-94):
  * camera_to_world, proj_to_camera = inverse(rev_inf_projection(vfov, aspect, 0.1)) and
