@@ -317,7 +317,7 @@ struct Principled
         }
         return pdf;
     }
-    KS_D f3 eval(f3 wo, f3 wi) const
+    KS_BIG f3 eval(f3 wo, f3 wi) const
     {
         if (wo.z == 0.0f || wi.z == 0.0f)
             return mk(0, 0, 0);
@@ -331,7 +331,7 @@ struct Principled
         f += eval_dielectric_specular(wo, wi);
         return f;
     }
-    KS_D float pdf(f3 wo, f3 wi) const
+    KS_BIG float pdf(f3 wo, f3 wi) const
     {
         if (wo.z == 0.0f || wi.z == 0.0f)
             return 0.0f;
@@ -416,7 +416,7 @@ struct Principled
         return wi;
     }
     // sample(): returns f / pdf (principled_bsdf.cpp:326-393)
-    KS_D f3 sample(f3 wo, f3 &wi, float u_lobe, float u0, float u1, float &pdf) const
+    KS_BIG f3 sample(f3 wo, f3 &wi, float u_lobe, float u0, float u1, float &pdf) const
     {
         if (wo.z == 0.0f) {
             pdf = 0.0f;

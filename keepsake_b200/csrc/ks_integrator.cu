@@ -297,12 +297,44 @@ __global__ void __launch_bounds__(128) k_extend(SceneView sv, PathBuf pb, uint32
     flush_counts(tc, work);
 }
 
+// Sobol samples of one bounce for every path in the hit queue (whose bounce is below the limit):
+// light selection (dimension d), light uv (d+1, d+2), BSDF lobe (d+3), BSDF direction (d+4,
+// d+5) and Russian roulette (d+6), exactly as sample_with_nee + trace() draw them
+// (nee.cpp:28-34, material.cpp:157-158, small_pt.cpp:168-174).  Integer-only and uniform across
+// the warp, so it runs at full occupancy instead of inside the divergent shading kernel.
+// samples[2 * i] = (light, light u, light v, lobe), samples[2 * i + 1] = (wi u, wi v, roulette, -)
+__global__ void __launch_bounds__(128) k_sample(RenderParams rp, PathBuf cur, const uint32_t *queue,
+                                                const uint32_t *queue_count, float4 *samples)
+{
+    const uint32_t count = *queue_count;
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x) {
+        uint32_t i = queue[q];
+        uint32_t info = bits(cur.d_info[i].w);
+        int bounce = (int)(info & 0xffffu);
+        if (bounce == rp.bounces)
+            continue;
+        int dim = (int)(info >> 16);
+        uint32_t pix = bits(cur.beta_pix[i].w), smp = bits(cur.L_smp[i].w);
+        SobolSampler s = SobolSampler::start(pix % (uint32_t)rp.W, pix / (uint32_t)rp.W, smp, rp.log2_spp,
+                                             rp.n_digits, (uint32_t)rp.seed, dim);
+        float a = s.next();
+        float b, c;
+        s.next2d(b, c);
+        float d = s.next();
+        float e, f;
+        s.next2d(e, f);
+        float g = s.next();
+        samples[2 * (size_t)i] = make_float4(a, b, c, d);
+        samples[2 * (size_t)i + 1] = make_float4(e, f, g, 0.0f);
+    }
+}
+
 // Shading of the paths listed in `queue` (indices into the current path buffer).  kMiss = true
 // handles the rays that left the scene, kMiss = false the rays that hit a triangle; the extension
 // kernel sorts the two kinds into separate queues so that a warp runs one of the two code paths.
 template <bool kMiss>
 __global__ void __launch_bounds__(128) k_shade(SceneView sv, RenderParams rp, PathBuf cur, PathBuf nxt,
-                                               const float4 *hits, const uint32_t *queue,
+                                               const float4 *hits, const float4 *samples, const uint32_t *queue,
                                                const uint32_t *queue_count, uint32_t *next_count, ShadowBuf sb,
                                                uint32_t *shadow_count, double *accum, double *weights)
 {
@@ -385,15 +417,13 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sv, RenderParams rp, Pa
                 } else {
                     f3 wo = -normalize(rd);
                     Principled bsdf{make_closure(mat)};
-                    uint32_t px = pix % (uint32_t)rp.W, py = pix / (uint32_t)rp.W;
-                    SobolSampler sampler =
-                        SobolSampler::start(px, py, smp, rp.log2_spp, rp.n_digits, (uint32_t)rp.seed, dim);
+                    // this bounce's Sobol values, drawn by k_sample
+                    const float4 sa = samples[2 * (size_t)i], sc = samples[2 * (size_t)i + 1];
                     // next_event_estimate (nee.cpp:11-57)
-                    float ul = sampler.next();
+                    float ul = sa.x;
                     uint32_t light = cdf_find(sv.power_cdf, sv.light_count, clamp_u(ul));
                     float pr_light = sv.power_cdf[light + 1] - sv.power_cdf[light];
-                    float u0, u1;
-                    sampler.next2d(u0, u1);
+                    float u0 = sa.y, u1 = sa.z;
                     f3 wi = mk(0, 0, 0);
                     float wi_dist = 0.0f, pdf_wi_light = 0.0f;
                     f3 Le_beta;
@@ -422,9 +452,9 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sv, RenderParams rp, Pa
                     }
                     // BSDF sampling (material.cpp:155-166)
                     f3 wo_local = sh_to_local(it, wo);
-                    float u_lobe = sampler.next();
-                    float b0, b1;
-                    sampler.next2d(b0, b1);
+                    float u_lobe = sa.w;
+                    float b0 = sc.x, b1 = sc.y;
+                    int next_dim = dim + 6;
                     f3 wi_local;
                     float pdf_wi = 0.0f;
                     f3 sbeta = bsdf.sample(wo_local, wi_local, u_lobe, b0, b1, pdf_wi);
@@ -440,7 +470,8 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sv, RenderParams rp, Pa
                         if (max3(nbeta) < 1.0f && bounce >= 1) {
                             float q = 1.0f - max3(nbeta);
                             q = q < 0.0f ? 0.0f : q;
-                            if (sampler.next() < q)
+                            next_dim = dim + 7;
+                            if (sc.z < q)
                                 finish = true;
                             else
                                 nbeta /= 1.0f - q;
@@ -448,7 +479,7 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sv, RenderParams rp, Pa
                         if (!finish) {
                             cont = true;
                             n_beta = nbeta;
-                            n_info = ((uint32_t)sampler.dimension << 16) | (uint32_t)(bounce + 1);
+                            n_info = ((uint32_t)next_dim << 16) | (uint32_t)(bounce + 1);
                         }
                     }
                 }
@@ -525,6 +556,7 @@ struct RenderWork
 {
     DevBuf<float4> state[2][4];
     DevBuf<float4> hits;
+    DevBuf<float4> samples; // 2 per path slot
     DevBuf<float4> shadow[4];
     DevBuf<uint32_t> counters; // [next, shadow, hit queue, miss queue]
     DevBuf<uint32_t> queue[2]; // hit / miss path indices
@@ -584,6 +616,7 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
         for (int f = 0; f < 4; ++f)
             KS_CUDA_TRY(ctx, w.state[b][f].alloc(w.capacity));
     KS_CUDA_TRY(ctx, w.hits.alloc(w.capacity));
+    KS_CUDA_TRY(ctx, w.samples.alloc(2 * (size_t)w.capacity));
     KS_CUDA_TRY(ctx, w.queue[0].alloc(w.capacity));
     KS_CUDA_TRY(ctx, w.queue[1].alloc(w.capacity));
     for (int f = 0; f < 4; ++f)
@@ -641,17 +674,18 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
             k_extend<<<grid, 128, 0, st>>>(sv, pb[cur], count, w.hits.ptr, w.queue[0].ptr, w.queue[1].ptr,
                                            w.counters.ptr + 2, w.overflow.ptr, work.ptr);
             cudaEventRecord(ev[2], st);
-            k_shade<false><<<grid, 128, 0, st>>>(sv, rp, pb[cur], pb[1 - cur], w.hits.ptr, w.queue[0].ptr,
-                                                 w.counters.ptr + 2, w.counters.ptr, sb, w.counters.ptr + 1, d_accum,
-                                                 d_weights);
-            k_shade<true><<<grid, 128, 0, st>>>(sv, rp, pb[cur], pb[1 - cur], w.hits.ptr, w.queue[1].ptr,
-                                                w.counters.ptr + 3, w.counters.ptr, sb, w.counters.ptr + 1, d_accum,
-                                                d_weights);
+            k_sample<<<grid, 128, 0, st>>>(rp, pb[cur], w.queue[0].ptr, w.counters.ptr + 2, w.samples.ptr);
+            k_shade<false><<<grid, 128, 0, st>>>(sv, rp, pb[cur], pb[1 - cur], w.hits.ptr, w.samples.ptr,
+                                                 w.queue[0].ptr, w.counters.ptr + 2, w.counters.ptr, sb,
+                                                 w.counters.ptr + 1, d_accum, d_weights);
+            k_shade<true><<<grid, 128, 0, st>>>(sv, rp, pb[cur], pb[1 - cur], w.hits.ptr, w.samples.ptr,
+                                                w.queue[1].ptr, w.counters.ptr + 3, w.counters.ptr, sb,
+                                                w.counters.ptr + 1, d_accum, d_weights);
             cudaEventRecord(ev[3], st);
             k_shadow<<<grid, 128, 0, st>>>(sv, sb, w.counters.ptr + 1, pb[1 - cur], d_accum, d_weights,
                                            w.overflow.ptr, work.ptr + 2);
             cudaEventRecord(ev[4], st);
-            stats.kernel_launches += 4;
+            stats.kernel_launches += 5;
             cudaMemcpyAsync(h_counts, w.counters.ptr, sizeof(uint32_t) * 2, cudaMemcpyDeviceToHost, st);
             err = cudaStreamSynchronize(st);
             if (err != cudaSuccess)

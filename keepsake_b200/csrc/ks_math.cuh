@@ -10,6 +10,13 @@
 
 #define KS_HD __host__ __device__ __forceinline__
 #define KS_D __device__ __forceinline__
+// Large shading functions called from several places: kept out of line so that the shading
+// kernel's code fits the instruction cache (KS_SHADE_INLINE=1 inlines them).
+#if defined(KS_SHADE_INLINE) && KS_SHADE_INLINE
+#define KS_BIG __device__ __forceinline__
+#else
+#define KS_BIG __device__ __noinline__
+#endif
 
 namespace ksb
 {
