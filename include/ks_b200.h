@@ -228,6 +228,48 @@ typedef struct ks_render_stats {
 ks_status ks_render_stats_last(const ks_scene *scene, ks_render_stats *out);
 
 /* ---------------------------------------------------------------------------------------------
+ * Learned guiding network.  The reference's guiding runs as Slang compute shaders
+ * (gpu/shaders/adam.slang, the vMF mixture of vmf.h / vmf.cpp); this is its CUDA counterpart:
+ *   input   16-level hash grid (2^19 entries x 2 features per level) of the position + degree-3
+ *           real spherical harmonics (16 values) of the outgoing direction = 48 values
+ *   MLP     48 -> 64 -> 64 -> 64 -> 64 -> 40, ReLU, no biases, BF16 weights and activations,
+ *           FP32 accumulation (tcgen05 tensor cores, accumulators in TMEM)
+ *   output  8 vMF lobes x (mean direction xyz, log concentration, mixture logit)
+ * Loss of a training sample (x, wo, wi, t): -t/n log q(wi | x, wo), n = rows of the batch.
+ * Parameters are kept in FP32; Adam follows adam.slang:25-51 (beta 0.9 / 0.999, eps 1e-8).
+ * ------------------------------------------------------------------------------------------- */
+typedef struct ks_guide ks_guide;
+
+typedef struct ks_guide_params {
+    float bound[6];      /* scene bound (min xyz, max xyz) that normalises positions */
+    float base_res;      /* cells per axis of the coarsest level (0 -> 16) */
+    float max_res;       /* cells per axis of the finest level (0 -> 2048) */
+    float learning_rate; /* Adam step size (0 -> 1e-2) */
+    uint64_t seed;       /* initialisation of weights and grid */
+} ks_guide_params;
+
+#define KS_GUIDE_LEVELS 16
+#define KS_GUIDE_TABLE_SIZE (1u << 19)
+#define KS_GUIDE_WEIGHTS 18432 /* 48*64 + 3*64*64 + 48*64 (output layer padded to 48 rows) */
+#define KS_GUIDE_OUTPUTS 40
+
+ks_status ks_guide_create(ks_context *ctx, const ks_guide_params *params, ks_guide **out);
+void ks_guide_destroy(ks_guide *g);
+/* Cells per axis of each level (KS_GUIDE_LEVELS values). */
+ks_status ks_guide_level_res(const ks_guide *g, uint32_t res[KS_GUIDE_LEVELS]);
+/* FP32 master parameters: mlp_weights[KS_GUIDE_WEIGHTS] (layer by layer, W[out][in] row-major),
+ * grid[KS_GUIDE_LEVELS * KS_GUIDE_TABLE_SIZE * 2].  Either pointer may be NULL. */
+ks_status ks_guide_get_weights(ks_guide *g, float *mlp_weights, float *grid);
+ks_status ks_guide_set_weights(ks_guide *g, const float *mlp_weights, const float *grid);
+/* Raw network outputs (n x KS_GUIDE_OUTPUTS) for host positions / unit directions (n x 3). */
+ks_status ks_guide_infer(ks_guide *g, const float *pos, const float *wo, uint32_t n, float *raw_out);
+/* One training batch: loss (sum over rows of -t/n log q) and gradients of the parameters; with
+ * apply_adam the gradients then drive one Adam step, else they are discarded.  loss, mlp_grad and
+ * grid_grad may be NULL. */
+ks_status ks_guide_gradients(ks_guide *g, const float *pos, const float *wo, const float *wi, const float *target,
+                             uint32_t n, int apply_adam, double *loss, float *mlp_grad, float *grid_grad);
+
+/* ---------------------------------------------------------------------------------------------
  * Procedural scenes: seeded synthetic inputs standing in for mesh-asset loading
  * (mesh_asset.cpp).  kind: "box_room" or "icosphere" (options apply to "icosphere").
  * ------------------------------------------------------------------------------------------- */

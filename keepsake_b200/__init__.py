@@ -361,3 +361,99 @@ class Scene:
             self.close()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------------------------------------
+# Learned guiding network (ks_guide_*)
+# ---------------------------------------------------------------------------------------------
+GUIDE_LEVELS = 16
+GUIDE_TABLE_SIZE = 1 << 19
+GUIDE_WEIGHTS = 18432
+GUIDE_OUTPUTS = 40
+GUIDE_LAYERS = [(64, 48), (64, 64), (64, 64), (64, 64), (48, 64)]  # (out, in) of each W
+
+
+class GuideParams(ctypes.Structure):
+    _fields_ = [("bound", _f32 * 6), ("base_res", _f32), ("max_res", _f32), ("learning_rate", _f32),
+                ("seed", ctypes.c_uint64)]
+
+
+_sig("ks_guide_create", [_vp, ctypes.POINTER(GuideParams), ctypes.POINTER(_vp)])
+_sig("ks_guide_destroy", [_vp], None)
+_sig("ks_guide_level_res", [_vp, _vp])
+_sig("ks_guide_get_weights", [_vp, _vp, _vp])
+_sig("ks_guide_set_weights", [_vp, _vp, _vp])
+_sig("ks_guide_infer", [_vp, _vp, _vp, _u32, _vp])
+_sig("ks_guide_gradients", [_vp, _vp, _vp, _vp, _vp, _u32, ctypes.c_int, _vp, _vp, _vp])
+
+
+def split_guide_weights(flat):
+    """Splits the flat weight vector into the per-layer [out][in] matrices (views)."""
+    out, o = [], 0
+    for n, k in GUIDE_LAYERS:
+        out.append(flat[o:o + n * k].reshape(n, k))
+        o += n * k
+    return out
+
+
+class Guide:
+    """The guiding network (ks_guide): hash grid + MLP + vMF mixture head, trained with Adam."""
+
+    def __init__(self, ctx: Context, bound, base_res=16.0, max_res=2048.0, learning_rate=1e-2, seed=1):
+        self.ctx = ctx
+        p = GuideParams()
+        p.bound[:] = [float(x) for x in bound]
+        p.base_res, p.max_res, p.learning_rate, p.seed = base_res, max_res, learning_rate, seed
+        h = _vp()
+        ctx.check(lib.ks_guide_create(ctx.handle, ctypes.byref(p), ctypes.byref(h)), "ks_guide_create")
+        self.handle = h
+        ctx._scenes.add(self)
+
+    def level_res(self) -> np.ndarray:
+        r = np.empty(GUIDE_LEVELS, np.uint32)
+        self.ctx.check(lib.ks_guide_level_res(self.handle, ptr(r)), "ks_guide_level_res")
+        return r
+
+    def get_weights(self, grid=True):
+        w = np.empty(GUIDE_WEIGHTS, np.float32)
+        g = np.empty((GUIDE_LEVELS, GUIDE_TABLE_SIZE, 2), np.float32) if grid else None
+        self.ctx.check(lib.ks_guide_get_weights(self.handle, ptr(w), ptr(g)), "ks_guide_get_weights")
+        return w, g
+
+    def set_weights(self, w=None, grid=None):
+        w = None if w is None else np.ascontiguousarray(w, np.float32)
+        grid = None if grid is None else np.ascontiguousarray(grid, np.float32)
+        self.ctx.check(lib.ks_guide_set_weights(self.handle, ptr(w), ptr(grid)), "ks_guide_set_weights")
+
+    def infer(self, pos, wo) -> np.ndarray:
+        pos = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
+        wo = np.ascontiguousarray(wo, np.float32).reshape(-1, 3)
+        out = np.empty((len(pos), GUIDE_OUTPUTS), np.float32)
+        self.ctx.check(lib.ks_guide_infer(self.handle, ptr(pos), ptr(wo), len(pos), ptr(out)), "ks_guide_infer")
+        return out
+
+    def gradients(self, pos, wo, wi, target, apply_adam=False, want_grads=True):
+        pos = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
+        wo = np.ascontiguousarray(wo, np.float32).reshape(-1, 3)
+        wi = np.ascontiguousarray(wi, np.float32).reshape(-1, 3)
+        target = np.ascontiguousarray(target, np.float32).reshape(-1)
+        loss = np.zeros(1, np.float64)
+        gw = np.empty(GUIDE_WEIGHTS, np.float32) if want_grads else None
+        gg = np.empty((GUIDE_LEVELS, GUIDE_TABLE_SIZE, 2), np.float32) if want_grads else None
+        self.ctx.check(lib.ks_guide_gradients(self.handle, ptr(pos), ptr(wo), ptr(wi), ptr(target), len(pos),
+                                              int(apply_adam), ptr(loss), ptr(gw), ptr(gg)), "ks_guide_gradients")
+        return float(loss[0]), gw, gg
+
+    def train_step(self, pos, wo, wi, target) -> float:
+        return self.gradients(pos, wo, wi, target, apply_adam=True, want_grads=False)[0]
+
+    def close(self):
+        if self.handle:
+            lib.ks_guide_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
