@@ -223,6 +223,10 @@ typedef struct ks_render_stats {
     uint64_t ext_tris;       /* triangles tested by closest-hit queries (48 B each) */
     uint64_t shadow_nodes;   /* interior nodes fetched by any-hit queries */
     uint64_t shadow_tris;    /* triangles tested by any-hit queries */
+    float ms_guide_infer;    /* guided renders: guide inference over the hit queues, summed */
+    float ms_guide_train;    /* guided renders: training (forward, backward, Adam), summed */
+    uint64_t guide_records;  /* guided renders: training samples captured */
+    uint32_t guide_train_steps; /* guided renders: Adam steps taken */
 } ks_render_stats;
 
 ks_status ks_render_stats_last(const ks_scene *scene, ks_render_stats *out);
@@ -231,11 +235,16 @@ ks_status ks_render_stats_last(const ks_scene *scene, ks_render_stats *out);
  * Learned guiding network.  The reference's guiding runs as Slang compute shaders
  * (gpu/shaders/adam.slang, the vMF mixture of vmf.h / vmf.cpp); this is its CUDA counterpart:
  *   input   16-level hash grid (2^19 entries x 2 features per level) of the position + degree-3
- *           real spherical harmonics (16 values) of the outgoing direction = 48 values
- *   MLP     48 -> 64 -> 64 -> 64 -> 64 -> 40, ReLU, no biases, BF16 weights and activations,
+ *           real spherical harmonics (16 values each) of the outgoing direction and of the
+ *           geometric normal on its side = 64 values
+ *   MLP     64 -> 64 -> 64 -> 64 -> 64 -> 41, ReLU, no biases, BF16 weights and activations,
  *           FP32 accumulation (tcgen05 tensor cores, accumulators in TMEM)
- *   output  8 vMF lobes x (mean direction xyz, log concentration, mixture logit)
- * Loss of a training sample (x, wo, wi, t): -t/n log q(wi | x, wo), n = rows of the batch.
+ *   output  8 vMF lobes x (mean direction xyz, log concentration, mixture logit), then the logit
+ *           z of the selection probability alpha = alpha_max * sigmoid(z) of the mixture against
+ *           the BSDF in one-sample MIS
+ * Training sample (x, wo, normal, wi, t, p_bsdf), t = f cos L / p: the mixture minimises
+ * -t/n log q(wi), the selection logit -t/n log(alpha q(wi) + (1 - alpha) p_bsdf) with q held
+ * fixed (n = rows of the batch); the reported loss is the latter.
  * Parameters are kept in FP32; Adam follows adam.slang:25-51 (beta 0.9 / 0.999, eps 1e-8).
  * ------------------------------------------------------------------------------------------- */
 typedef struct ks_guide ks_guide;
@@ -245,29 +254,64 @@ typedef struct ks_guide_params {
     float base_res;      /* cells per axis of the coarsest level (0 -> 16) */
     float max_res;       /* cells per axis of the finest level (0 -> 2048) */
     float learning_rate; /* Adam step size (0 -> 1e-2) */
+    float alpha_max;     /* largest selection probability of the mixture (0 -> 0.8) */
     uint64_t seed;       /* initialisation of weights and grid */
 } ks_guide_params;
 
 #define KS_GUIDE_LEVELS 16
 #define KS_GUIDE_TABLE_SIZE (1u << 19)
-#define KS_GUIDE_WEIGHTS 18432 /* 48*64 + 3*64*64 + 48*64 (output layer padded to 48 rows) */
-#define KS_GUIDE_OUTPUTS 40
+#define KS_GUIDE_WEIGHTS 19456 /* 4*64*64 + 48*64 (output layer padded to 48 rows) */
+#define KS_GUIDE_OUTPUTS 41
 
 ks_status ks_guide_create(ks_context *ctx, const ks_guide_params *params, ks_guide **out);
 void ks_guide_destroy(ks_guide *g);
 /* Cells per axis of each level (KS_GUIDE_LEVELS values). */
 ks_status ks_guide_level_res(const ks_guide *g, uint32_t res[KS_GUIDE_LEVELS]);
+/* Loss of the most recent training batch (ks_guide_gradients or a guided render's training). */
+ks_status ks_guide_last_loss(ks_guide *g, double *loss);
 /* FP32 master parameters: mlp_weights[KS_GUIDE_WEIGHTS] (layer by layer, W[out][in] row-major),
  * grid[KS_GUIDE_LEVELS * KS_GUIDE_TABLE_SIZE * 2].  Either pointer may be NULL. */
 ks_status ks_guide_get_weights(ks_guide *g, float *mlp_weights, float *grid);
 ks_status ks_guide_set_weights(ks_guide *g, const float *mlp_weights, const float *grid);
-/* Raw network outputs (n x KS_GUIDE_OUTPUTS) for host positions / unit directions (n x 3). */
-ks_status ks_guide_infer(ks_guide *g, const float *pos, const float *wo, uint32_t n, float *raw_out);
-/* One training batch: loss (sum over rows of -t/n log q) and gradients of the parameters; with
- * apply_adam the gradients then drive one Adam step, else they are discarded.  loss, mlp_grad and
- * grid_grad may be NULL. */
-ks_status ks_guide_gradients(ks_guide *g, const float *pos, const float *wo, const float *wi, const float *target,
-                             uint32_t n, int apply_adam, double *loss, float *mlp_grad, float *grid_grad);
+/* Raw network outputs (n x KS_GUIDE_OUTPUTS) for host positions, outgoing directions and normals
+ * (n x 3 each). */
+ks_status ks_guide_infer(ks_guide *g, const float *pos, const float *wo, const float *normal, uint32_t n,
+                         float *raw_out);
+/* One training batch: loss (sum over rows of -t/n log m) and gradients of the parameters; with
+ * apply_adam the gradients then drive one Adam step, else they are discarded.  bsdf_pdf (n
+ * values) may be NULL (p_bsdf = 0); loss, mlp_grad and grid_grad may be NULL. */
+ks_status ks_guide_gradients(ks_guide *g, const float *pos, const float *wo, const float *normal, const float *wi,
+                             const float *target, const float *bsdf_pdf, uint32_t n, int apply_adam, double *loss,
+                             float *mlp_grad, float *grid_grad);
+
+/* ---------------------------------------------------------------------------------------------
+ * Guided rendering: small_pt with the guide network as a second proposal.  At every surface
+ * vertex the direction is drawn from the guide's mixture with the probability alpha the guide
+ * outputs for that vertex, else from the BSDF, and the throughput is divided by the combined
+ * density alpha q + (1 - alpha) p_bsdf (one-sample MIS).  The MIS weights between NEE and emitter
+ * hits stay functions of the BSDF pdf exactly as in small_pt (nee.cpp:40-48, small_pt.cpp:95,126),
+ * so every pass has the expectation of the unguided render whatever the guide has learned.  The render proceeds in passes of params->spp_prog_interval samples per pixel.  During
+ * the first train_passes passes, paths record one vertex each (position, wo, sampled wi, and the
+ * radiance later gathered along wi); after each such pass the records train the guide (one Adam
+ * step per train_batch records).  Passes before guide_from_pass sample the BSDF only.
+ * No reference counterpart: the reference's small_pt samples the BSDF only.
+ * ------------------------------------------------------------------------------------------- */
+typedef struct ks_guide_render_options {
+    int32_t guide_from_pass; /* first pass that samples the guide */
+    int32_t train_passes;    /* passes that capture records and train afterwards */
+    uint32_t max_records;    /* records captured per pass (0 -> 2^19) */
+    uint32_t train_batch;    /* records per Adam step (0 -> 2^18) */
+    int32_t record_bounces;  /* the recorded vertex is drawn from bounces [0, record_bounces) (0 -> 6) */
+} ks_guide_render_options;
+
+void ks_guide_render_options_default(ks_guide_render_options *out);
+ks_status ks_small_pt_render_guided(ks_scene *scene, const ks_camera_desc *camera, const ks_small_pt_params *params,
+                                    ks_guide *guide, const ks_guide_render_options *options, ks_progress_fn progress,
+                                    void *user, double *accum_rgb, double *weights);
+ks_status ks_small_pt_render_guided_device(ks_scene *scene, const ks_camera_desc *camera,
+                                           const ks_small_pt_params *params, ks_guide *guide,
+                                           const ks_guide_render_options *options, double *accum_rgb_device,
+                                           double *weights_device);
 
 /* ---------------------------------------------------------------------------------------------
  * Procedural scenes: seeded synthetic inputs standing in for mesh-asset loading

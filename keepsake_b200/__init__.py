@@ -186,7 +186,9 @@ class RenderStats(ctypes.Structure):
     _fields_ = [("paths", ctypes.c_uint64), ("extension_rays", ctypes.c_uint64), ("shadow_rays", ctypes.c_uint64),
                 ("iterations", _u32), ("kernel_launches", _u32), ("ms_total", _f32), ("ms_extend", _f32),
                 ("ms_shade", _f32), ("ms_shadow", _f32), ("ext_nodes", ctypes.c_uint64),
-                ("ext_tris", ctypes.c_uint64), ("shadow_nodes", ctypes.c_uint64), ("shadow_tris", ctypes.c_uint64)]
+                ("ext_tris", ctypes.c_uint64), ("shadow_nodes", ctypes.c_uint64), ("shadow_tris", ctypes.c_uint64),
+                ("ms_guide_infer", _f32), ("ms_guide_train", _f32), ("guide_records", ctypes.c_uint64),
+                ("guide_train_steps", _u32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -248,6 +250,13 @@ class Generated:
             ids.append(m["indices"].astype(np.uint64) + off)
             off += len(m["vertices"])
         return np.concatenate(vs).astype(np.float32), np.concatenate(ids).astype(np.uint32)
+
+    @property
+    def bound(self):
+        """Axis-aligned bound of all vertices: (min [3], max [3])."""
+        lo = np.min([m["vertices"].min(0) for m in self.meshes], axis=0)
+        hi = np.max([m["vertices"].max(0) for m in self.meshes], axis=0)
+        return lo, hi
 
     @property
     def n_triangles(self):
@@ -341,6 +350,29 @@ class Scene:
                                               ptr(accum), ptr(weights)), "ks_small_pt_render")
         return accum, weights
 
+    def render_guided(self, camera: CameraDesc, params: SmallPTParams, guide, options=None, callback=None):
+        """ks_small_pt_render_guided into fresh host FP64 buffers (see render)."""
+        options = options or GuideRenderOptions.make()
+        W, H = params.render_width, params.render_height
+        accum = np.zeros((H, W, 3), np.float64)
+        weights = np.zeros((H, W, 2), np.float64)
+        cb = PROGRESS_FN(0)
+        if callback is not None:
+            def _cb(spp, a, w, user):
+                callback(spp, np.ctypeslib.as_array(a, (H, W, 3)).copy(), np.ctypeslib.as_array(w, (H, W, 2)).copy())
+            cb = PROGRESS_FN(_cb)
+        self.ctx.check(lib.ks_small_pt_render_guided(self.handle, ctypes.byref(camera), ctypes.byref(params),
+                                                     guide.handle, ctypes.byref(options), cb, None, ptr(accum),
+                                                     ptr(weights)), "ks_small_pt_render_guided")
+        return accum, weights
+
+    def render_guided_device(self, camera: CameraDesc, params: SmallPTParams, guide, options, accum_ptr: int,
+                             weights_ptr: int):
+        self.ctx.check(lib.ks_small_pt_render_guided_device(self.handle, ctypes.byref(camera), ctypes.byref(params),
+                                                            guide.handle, ctypes.byref(options),
+                                                            ctypes.c_void_p(accum_ptr), ctypes.c_void_p(weights_ptr)),
+                       "ks_small_pt_render_guided_device")
+
     def render_device(self, camera: CameraDesc, params: SmallPTParams, accum_ptr: int, weights_ptr: int):
         self.ctx.check(lib.ks_small_pt_render_device(self.handle, ctypes.byref(camera), ctypes.byref(params),
                                                      ctypes.c_void_p(accum_ptr), ctypes.c_void_p(weights_ptr)),
@@ -368,23 +400,46 @@ class Scene:
 # ---------------------------------------------------------------------------------------------
 GUIDE_LEVELS = 16
 GUIDE_TABLE_SIZE = 1 << 19
-GUIDE_WEIGHTS = 18432
-GUIDE_OUTPUTS = 40
-GUIDE_LAYERS = [(64, 48), (64, 64), (64, 64), (64, 64), (48, 64)]  # (out, in) of each W
+GUIDE_WEIGHTS = 19456
+GUIDE_OUTPUTS = 41
+GUIDE_LAYERS = [(64, 64), (64, 64), (64, 64), (64, 64), (48, 64)]  # (out, in) of each W; 41 of 48 rows used
 
 
 class GuideParams(ctypes.Structure):
     _fields_ = [("bound", _f32 * 6), ("base_res", _f32), ("max_res", _f32), ("learning_rate", _f32),
-                ("seed", ctypes.c_uint64)]
+                ("alpha_max", _f32), ("seed", ctypes.c_uint64)]
 
 
 _sig("ks_guide_create", [_vp, ctypes.POINTER(GuideParams), ctypes.POINTER(_vp)])
 _sig("ks_guide_destroy", [_vp], None)
 _sig("ks_guide_level_res", [_vp, _vp])
 _sig("ks_guide_get_weights", [_vp, _vp, _vp])
+_sig("ks_guide_last_loss", [_vp, _vp])
 _sig("ks_guide_set_weights", [_vp, _vp, _vp])
-_sig("ks_guide_infer", [_vp, _vp, _vp, _u32, _vp])
-_sig("ks_guide_gradients", [_vp, _vp, _vp, _vp, _vp, _u32, ctypes.c_int, _vp, _vp, _vp])
+_sig("ks_guide_infer", [_vp, _vp, _vp, _vp, _u32, _vp])
+_sig("ks_guide_gradients", [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _u32, ctypes.c_int, _vp, _vp, _vp])
+
+
+class GuideRenderOptions(ctypes.Structure):
+    _fields_ = [("guide_from_pass", _i32), ("train_passes", _i32),
+                ("max_records", _u32), ("train_batch", _u32), ("record_bounces", _i32)]
+
+    @staticmethod
+    def make(**kw):
+        o = GuideRenderOptions()
+        lib.ks_guide_render_options_default(ctypes.byref(o))
+        for k, v in kw.items():
+            if not hasattr(o, k):
+                raise AttributeError(k)
+            setattr(o, k, v)
+        return o
+
+
+_sig("ks_guide_render_options_default", [ctypes.POINTER(GuideRenderOptions)], None)
+_sig("ks_small_pt_render_guided", [_vp, ctypes.POINTER(CameraDesc), ctypes.POINTER(SmallPTParams), _vp,
+                                   ctypes.POINTER(GuideRenderOptions), PROGRESS_FN, _vp, _vp, _vp])
+_sig("ks_small_pt_render_guided_device", [_vp, ctypes.POINTER(CameraDesc), ctypes.POINTER(SmallPTParams), _vp,
+                                          ctypes.POINTER(GuideRenderOptions), _vp, _vp])
 
 
 def split_guide_weights(flat):
@@ -399,11 +454,12 @@ def split_guide_weights(flat):
 class Guide:
     """The guiding network (ks_guide): hash grid + MLP + vMF mixture head, trained with Adam."""
 
-    def __init__(self, ctx: Context, bound, base_res=16.0, max_res=2048.0, learning_rate=1e-2, seed=1):
+    def __init__(self, ctx: Context, bound, base_res=16.0, max_res=2048.0, learning_rate=1e-2, alpha_max=0.8,
+                 seed=1):
         self.ctx = ctx
         p = GuideParams()
         p.bound[:] = [float(x) for x in bound]
-        p.base_res, p.max_res, p.learning_rate, p.seed = base_res, max_res, learning_rate, seed
+        p.base_res, p.max_res, p.learning_rate, p.alpha_max, p.seed = base_res, max_res, learning_rate, alpha_max, seed
         h = _vp()
         ctx.check(lib.ks_guide_create(ctx.handle, ctypes.byref(p), ctypes.byref(h)), "ks_guide_create")
         self.handle = h
@@ -413,6 +469,11 @@ class Guide:
         r = np.empty(GUIDE_LEVELS, np.uint32)
         self.ctx.check(lib.ks_guide_level_res(self.handle, ptr(r)), "ks_guide_level_res")
         return r
+
+    def last_loss(self) -> float:
+        out = np.zeros(1, np.float64)
+        self.ctx.check(lib.ks_guide_last_loss(self.handle, ptr(out)), "ks_guide_last_loss")
+        return float(out[0])
 
     def get_weights(self, grid=True):
         w = np.empty(GUIDE_WEIGHTS, np.float32)
@@ -425,27 +486,32 @@ class Guide:
         grid = None if grid is None else np.ascontiguousarray(grid, np.float32)
         self.ctx.check(lib.ks_guide_set_weights(self.handle, ptr(w), ptr(grid)), "ks_guide_set_weights")
 
-    def infer(self, pos, wo) -> np.ndarray:
+    def infer(self, pos, wo, normal) -> np.ndarray:
         pos = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
         wo = np.ascontiguousarray(wo, np.float32).reshape(-1, 3)
+        normal = np.ascontiguousarray(normal, np.float32).reshape(-1, 3)
         out = np.empty((len(pos), GUIDE_OUTPUTS), np.float32)
-        self.ctx.check(lib.ks_guide_infer(self.handle, ptr(pos), ptr(wo), len(pos), ptr(out)), "ks_guide_infer")
+        self.ctx.check(lib.ks_guide_infer(self.handle, ptr(pos), ptr(wo), ptr(normal), len(pos), ptr(out)),
+                       "ks_guide_infer")
         return out
 
-    def gradients(self, pos, wo, wi, target, apply_adam=False, want_grads=True):
+    def gradients(self, pos, wo, normal, wi, target, bsdf_pdf=None, apply_adam=False, want_grads=True):
         pos = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
         wo = np.ascontiguousarray(wo, np.float32).reshape(-1, 3)
+        normal = np.ascontiguousarray(normal, np.float32).reshape(-1, 3)
         wi = np.ascontiguousarray(wi, np.float32).reshape(-1, 3)
         target = np.ascontiguousarray(target, np.float32).reshape(-1)
+        pb = None if bsdf_pdf is None else np.ascontiguousarray(bsdf_pdf, np.float32).reshape(-1)
         loss = np.zeros(1, np.float64)
         gw = np.empty(GUIDE_WEIGHTS, np.float32) if want_grads else None
         gg = np.empty((GUIDE_LEVELS, GUIDE_TABLE_SIZE, 2), np.float32) if want_grads else None
-        self.ctx.check(lib.ks_guide_gradients(self.handle, ptr(pos), ptr(wo), ptr(wi), ptr(target), len(pos),
-                                              int(apply_adam), ptr(loss), ptr(gw), ptr(gg)), "ks_guide_gradients")
+        self.ctx.check(lib.ks_guide_gradients(self.handle, ptr(pos), ptr(wo), ptr(normal), ptr(wi), ptr(target), ptr(pb),
+                                              len(pos), int(apply_adam), ptr(loss), ptr(gw), ptr(gg)),
+                       "ks_guide_gradients")
         return float(loss[0]), gw, gg
 
-    def train_step(self, pos, wo, wi, target) -> float:
-        return self.gradients(pos, wo, wi, target, apply_adam=True, want_grads=False)[0]
+    def train_step(self, pos, wo, normal, wi, target, bsdf_pdf=None) -> float:
+        return self.gradients(pos, wo, normal, wi, target, bsdf_pdf, apply_adam=True, want_grads=False)[0]
 
     def close(self):
         if self.handle:

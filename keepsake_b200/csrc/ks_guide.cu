@@ -12,9 +12,11 @@
 //             dW_l [out x in] += dY_l^T * X_l               (A = dY^T K-major, padded to 128 rows,
 //                                                            B = X_l^T buffer K-major)
 #include "ks_guide.cuh"
+#include "ks_guide_host.h"
 #include "ks_internal.h"
 #include "ks_tc.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -56,8 +58,8 @@ constexpr uint32_t kSmemDY = kSmemX + x_soff(kLayers); // dY^T, 128 x 128 bf16 =
 constexpr uint32_t kSmemBar = kSmemDY + 32768;
 // The allocation is padded so that every descriptor above stays inside it even if the tensor core
 // read one of them with its two strides exchanged (furthest reach: the dX A operand, dY^T base +
-// 3 K-steps + 16 M-groups x 2048 B = 159744 B).
-constexpr uint32_t kSmemTotal = 160u * 1024u;
+// 3 K-steps + 16 M-groups x 2048 B).
+constexpr uint32_t kSmemTotal = 168u * 1024u;
 static_assert(kSmemBar + 64 <= kSmemTotal && kSmemDY + 3u * 4096u + 16u * 2048u <= kSmemTotal,
               "guide MLP shared-memory plan");
 // TMEM columns
@@ -84,16 +86,21 @@ __host__ __device__ constexpr uint32_t w_off(int l, uint32_t n, uint32_t k)
 struct MlpArgs
 {
     GridParams gp;
-    const float *grid;          // kLevels * T * 2
-    const uint8_t *w_image;     // bf16 weight image (kWImage bytes)
-    uint32_t n;                 // rows
-    const float *pos, *wo;      // n x 3
-    const float *wi, *target;   // training: n x 3, n
-    float target_scale;         // multiplies the targets (1 / batch size)
-    float *out;                 // inference: n x 40 raw outputs
-    float *w_grad;              // training: kWeights
-    float *grid_grad;           // training: kLevels * T * 2
-    double *loss;               // training
+    const float *grid;        // kLevels * T * 2
+    const uint8_t *w_image;   // bf16 weight image (kWImage bytes)
+    uint32_t n;               // rows
+    uint32_t stride;          // floats between consecutive rows of pos / wo / nrm / wi (3 or 4)
+    const float *pos, *wo;    // n rows
+    const float *nrm;         // n rows: geometric normal on the side of wo
+    const float *wi, *target; // training: n rows, n
+    float target_scale;       // multiplies the targets (1 / batch size)
+    const float *pb;          // training: BSDF pdf of wi per row (null: 0)
+    uint32_t pb_stride;
+    float alpha_max;          // selection probability = alpha_max * sigmoid(output kSel)
+    float *out;               // row inference: n x 40 raw outputs
+    float *w_grad;            // training: kWeights
+    float *grid_grad;         // training: kLevels * T * 2
+    double *loss;             // training
     int *err;
 };
 
@@ -120,6 +127,112 @@ __device__ __forceinline__ bool wait_mma(uint64_t *bar, uint32_t &phase, int *ct
     return *cta_err == 0;
 }
 
+// CTA prologue shared by the kernels: weights -> shared memory, barrier init, TMEM allocation.
+// Returns the TMEM base address.
+__device__ __forceinline__ uint32_t mlp_prologue(const uint8_t *w_image, uint8_t *sw, uint64_t *bar,
+                                                 uint32_t *tmem_slot, int *cta_err, uint32_t cols)
+{
+    for (uint32_t i = threadIdx.x; i < kWImage / 16; i += kThreads)
+        reinterpret_cast<uint4 *>(sw)[i] = reinterpret_cast<const uint4 *>(w_image)[i];
+    if (threadIdx.x == 0) {
+        tc::mbar_init(bar, 1);
+        *cta_err = 0;
+    }
+    if (threadIdx.x < 32)
+        tc::tmem_alloc(tmem_slot, cols);
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    return *tmem_slot;
+}
+
+__device__ __forceinline__ void mlp_epilogue(uint32_t tmem, uint32_t cols)
+{
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    if (threadIdx.x < 32)
+        tc::tmem_dealloc(tmem, cols);
+}
+
+// Input encoding of this thread's row into X_0^T: 16 hash-grid levels x 2 features, then 16 SH
+// coefficients of wo and 16 of the normal.  Invalid rows are zero.
+__device__ __forceinline__ void encode_row(const GridParams &gp, const float *grid, bool valid, f3 pn, f3 wo,
+                                           f3 nrm, uint8_t *x0)
+{
+    const uint32_t tid = threadIdx.x;
+    for (int l = 0; l < kLevels; ++l) {
+        float f0 = 0.0f, f1 = 0.0f;
+        if (valid) {
+            Corner c;
+            level_corners(gp, l, pn, c);
+            const float2 *tab = reinterpret_cast<const float2 *>(grid) + (size_t)l * kTableSize;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                float2 e = __ldg(&tab[c.idx[k]]);
+                f0 += c.w[k] * e.x;
+                f1 += c.w[k] * e.y;
+            }
+        }
+        store_bf16(x0, xt_off(2 * l, tid), f0);
+        store_bf16(x0, xt_off(2 * l + 1, tid), f1);
+    }
+    float sh[kShCoeffs];
+    sh16(wo, sh);
+    for (int i = 0; i < kShCoeffs; ++i)
+        store_bf16(x0, xt_off(kGridFeatures + i, tid), valid ? sh[i] : 0.0f);
+    sh16(nrm, sh);
+    for (int i = 0; i < kShCoeffs; ++i)
+        store_bf16(x0, xt_off(kGridFeatures + kShCoeffs + i, tid), valid ? sh[i] : 0.0f);
+}
+
+// Forward pass of the CTA's 128-row tile: X_l^T lives in xb[l] (written here for l >= 1, X_0 by
+// the caller); the raw outputs of this thread's row end in o.  Returns false on an MMA timeout.
+__device__ __forceinline__ bool mlp_forward(uint8_t *const xb[kLayers], const uint8_t *sw, uint32_t tmem,
+                                            uint64_t *bar, uint32_t &phase, int *cta_err, int *err, float o[kOut])
+{
+    const uint32_t tid = threadIdx.x, lane_base = ((tid >> 5) * 32u) << 16;
+    for (int l = 0; l < kLayers; ++l) {
+        const int in = layer_in(l), out = layer_out(l);
+        tc::fence_smem_to_async();
+        tc::fence_before_sync();
+        __syncthreads();
+        if (tid == 0) {
+            tc::fence_after_sync();
+            const uint32_t idesc = tc::idesc_bf16(128, out, 1, 0);
+            for (int s = 0; s < in / 16; ++s) {
+                uint64_t ad = tc::smem_desc(tc::smem_addr(xb[l]) + s * 4096u, 2048u, 128u);
+                uint64_t bd = tc::smem_desc(tc::smem_addr(sw + w_soff(l)) + s * 256u, 128u, in / 8 * 128u);
+                tc::mma_bf16(tmem + kColFwd, ad, bd, idesc, s > 0);
+            }
+            tc::commit(bar);
+        }
+        if (!wait_mma(bar, phase, cta_err, err))
+            return false;
+        for (int c0 = 0; c0 < out; c0 += 16) {
+            float v[16];
+            tc::tmem_ld16(tmem + lane_base + kColFwd + c0, v);
+            if (l < kLayers - 1) {
+                for (int i = 0; i < 16; ++i)
+                    store_bf16(xb[l + 1], xt_off(c0 + i, tid), fmaxf(v[i], 0.0f));
+            } else {
+                for (int i = 0; i < 16 && c0 + i < kOut; ++i)
+                    o[c0 + i] = v[i];
+            }
+        }
+        tc::fence_before_sync();
+    }
+    return true;
+}
+
+__device__ __forceinline__ f3 load_row3(const float *p, uint32_t row, uint32_t stride)
+{
+    const float *q = p + (size_t)row * stride;
+    return mk(q[0], q[1], q[2]);
+}
+
+// Row inference (raw outputs) and training (forward, loss, backward; weight gradients accumulate
+// in TMEM across the CTA's tiles).
 template <bool kTrain>
 __global__ void __launch_bounds__(kThreads, 1) k_mlp(MlpArgs a)
 {
@@ -131,23 +244,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp(MlpArgs a)
     const uint32_t tid = threadIdx.x, warp = tid >> 5;
     constexpr uint32_t kCols = kTrain ? 512u : 64u;
 
-    // weights -> shared memory; dY buffer zeroed (rows beyond a layer's width stay zero)
-    for (uint32_t i = tid; i < kWImage / 16; i += kThreads)
-        reinterpret_cast<uint4 *>(sw)[i] = reinterpret_cast<const uint4 *>(a.w_image)[i];
     if (kTrain)
         for (uint32_t i = tid; i < 32768 / 16; i += kThreads)
             reinterpret_cast<uint4 *>(sdy)[i] = make_uint4(0, 0, 0, 0);
-    if (tid == 0) {
-        tc::mbar_init(bar, 1);
-        *cta_err = 0;
-    }
-    if (warp == 0)
-        tc::tmem_alloc(tmem_slot, kCols);
-    tc::fence_before_sync();
-    __syncthreads();
-    tc::fence_after_sync();
-    const uint32_t tmem = *tmem_slot;
+    const uint32_t tmem = mlp_prologue(a.w_image, sw, bar, tmem_slot, cta_err, kCols);
     const uint32_t lane_base = (warp * 32u) << 16;
+    uint8_t *xb[kLayers];
+    for (int l = 0; l < kLayers; ++l)
+        xb[l] = sx + x_soff(l);
     uint32_t phase = 0;
     bool first_tile = true;
     double loss_acc = 0.0;
@@ -156,67 +260,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp(MlpArgs a)
     for (uint32_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
         const uint32_t row = tile * kThreads + tid;
         const bool valid = row < a.n;
-        // ---- encoding -> X_0^T ----
-        f3 pn = mk(0, 0, 0), wo = mk(0, 0, 1);
+        f3 pn = mk(0, 0, 0), wo = mk(0, 0, 1), nrm = mk(0, 0, 1);
         if (valid) {
-            pn = normalise_position(a.gp, mk(a.pos[3 * row], a.pos[3 * row + 1], a.pos[3 * row + 2]));
-            wo = normalize(mk(a.wo[3 * row], a.wo[3 * row + 1], a.wo[3 * row + 2]));
+            pn = normalise_position(a.gp, load_row3(a.pos, row, a.stride));
+            wo = normalize(load_row3(a.wo, row, a.stride));
+            nrm = normalize(load_row3(a.nrm, row, a.stride));
         }
-        uint8_t *x0 = sx + x_soff(0);
-        for (int l = 0; l < kLevels; ++l) {
-            float f0 = 0.0f, f1 = 0.0f;
-            if (valid) {
-                Corner c;
-                level_corners(a.gp, l, pn, c);
-                const float2 *tab = reinterpret_cast<const float2 *>(a.grid) + (size_t)l * kTableSize;
-#pragma unroll
-                for (int k = 0; k < 8; ++k) {
-                    float2 e = __ldg(&tab[c.idx[k]]);
-                    f0 += c.w[k] * e.x;
-                    f1 += c.w[k] * e.y;
-                }
-            }
-            store_bf16(x0, xt_off(2 * l, tid), f0);
-            store_bf16(x0, xt_off(2 * l + 1, tid), f1);
-        }
-        float sh[kShCoeffs];
-        sh16(wo, sh);
-        for (int i = 0; i < kShCoeffs; ++i)
-            store_bf16(x0, xt_off(kGridFeatures + i, tid), valid ? sh[i] : 0.0f);
-
-        // ---- forward ----
+        encode_row(a.gp, a.grid, valid, pn, wo, nrm, xb[0]);
         float o[kOut];
-        for (int l = 0; l < kLayers; ++l) {
-            const int in = layer_in(l), out = layer_out(l);
-            tc::fence_smem_to_async();
-            tc::fence_before_sync();
-            __syncthreads();
-            if (tid == 0) {
-                tc::fence_after_sync();
-                const uint32_t idesc = tc::idesc_bf16(128, out, 1, 0);
-                for (int s = 0; s < in / 16; ++s) {
-                    uint64_t ad = tc::smem_desc(tc::smem_addr(sx + x_soff(l)) + s * 4096u, 2048u, 128u);
-                    uint64_t bd = tc::smem_desc(tc::smem_addr(sw + w_soff(l)) + s * 256u, 128u, in / 8 * 128u);
-                    tc::mma_bf16(tmem + kColFwd, ad, bd, idesc, s > 0);
-                }
-                tc::commit(bar);
-            }
-            if (!wait_mma(bar, phase, cta_err, a.err))
-                goto done;
-            for (int c0 = 0; c0 < out; c0 += 16) {
-                float v[16];
-                tc::tmem_ld16(tmem + lane_base + kColFwd + c0, v);
-                if (l < kLayers - 1) {
-                    uint8_t *xn = sx + x_soff(l + 1);
-                    for (int i = 0; i < 16; ++i)
-                        store_bf16(xn, xt_off(c0 + i, tid), fmaxf(v[i], 0.0f));
-                } else {
-                    for (int i = 0; i < 16 && c0 + i < kOut; ++i)
-                        o[c0 + i] = v[i];
-                }
-            }
-            tc::fence_before_sync();
-        }
+        if (!mlp_forward(xb, sw, tmem, bar, phase, cta_err, a.err, o))
+            goto done;
         if (!kTrain) {
             if (valid)
                 for (int i = 0; i < kOut; ++i)
@@ -227,12 +280,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp(MlpArgs a)
         {
             float g[kOut], loss = 0.0f;
             f3 wi = mk(0, 0, 1);
-            float t = 0.0f;
+            float t = 0.0f, p_b = 0.0f;
             if (valid) {
-                wi = normalize(mk(a.wi[3 * row], a.wi[3 * row + 1], a.wi[3 * row + 2]));
+                wi = normalize(load_row3(a.wi, row, a.stride));
                 t = a.target[row] * a.target_scale;
+                if (a.pb)
+                    p_b = a.pb[(size_t)row * a.pb_stride];
             }
-            mixture_loss_grad(o, wi, t, loss, g);
+            mixture_loss_grad(o, wi, t, p_b, a.alpha_max, loss, g);
             loss_acc += loss;
             for (int n = 0; n < kOutPad; ++n)
                 store_bf16(sdy, xt_off(n, tid), n < kOut ? g[n] : 0.0f);
@@ -249,7 +304,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp(MlpArgs a)
                 const uint32_t idw = tc::idesc_bf16(128, in, 0, 0);
                 for (int s = 0; s < 8; ++s) {
                     uint64_t ad = tc::smem_desc(tc::smem_addr(sdy) + s * 256u, 128u, 2048u);
-                    uint64_t bd = tc::smem_desc(tc::smem_addr(sx + x_soff(l)) + s * 256u, 128u, 2048u);
+                    uint64_t bd = tc::smem_desc(tc::smem_addr(xb[l]) + s * 256u, 128u, 2048u);
                     tc::mma_bf16(tmem + dw_col(l), ad, bd, idw, (!first_tile || s > 0) ? 1u : 0u);
                 }
                 // dX_l = dY_l W_l  (M = 128 rows, N = in, K = out)
@@ -269,9 +324,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp(MlpArgs a)
                 tc::tmem_ld16(tmem + lane_base + kColDX + c0, v);
                 if (l > 0) {
                     // dY_{l-1} = dX_l * relu'(Z_{l-1}); X_l holds relu(Z_{l-1})
-                    const uint8_t *xl = sx + x_soff(l);
                     for (int i = 0; i < 16; ++i) {
-                        float act = load_bf16(xl, xt_off(c0 + i, tid));
+                        float act = load_bf16(xb[l], xt_off(c0 + i, tid));
                         store_bf16(sdy, xt_off(c0 + i, tid), act > 0.0f ? v[i] : 0.0f);
                     }
                 } else if (valid && c0 < kGridFeatures) {
@@ -315,10 +369,77 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp(MlpArgs a)
             atomicAdd(a.loss, loss_acc);
     }
 done:
-    tc::fence_before_sync();
-    __syncthreads();
-    if (warp == 0)
-        tc::tmem_dealloc(tmem, kCols);
+    mlp_epilogue(tmem, kCols);
+}
+
+// Inference for the hit queue of a wavefront bounce: row = queue entry, input = hit position
+// (origin + t * direction) and the reversed ray direction; output = the decoded mixture of the
+// path slot (layout in ks_guide_view.cuh).  Two activation buffers alternate between layers, so a
+// CTA needs 68 KB of shared memory and three CTAs share an SM.
+struct PathArgs
+{
+    GridParams gp;
+    const float *grid;
+    const uint8_t *w_image;
+    const uint32_t *queue, *queue_count;
+    const float4 *o_pdf, *d_info, *hits;
+    const float4 *prim_tris; // 3 per SBVH primitive slot (vertices)
+    float4 *lobes;
+    uint32_t cap;
+    float alpha_max;
+    int *err;
+};
+constexpr uint32_t kPathSmemX0 = kWImage, kPathSmemX1 = kPathSmemX0 + 16384u, kPathSmemBar = kPathSmemX1 + 16384u;
+constexpr uint32_t kPathSmem = kPathSmemBar + 64;
+constexpr int kPathCtasPerSm = 3;
+
+__global__ void __launch_bounds__(kThreads, kPathCtasPerSm) k_guide_paths(PathArgs a)
+{
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint8_t *sw = smem;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + kPathSmemBar);
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + kPathSmemBar + 8);
+    int *cta_err = reinterpret_cast<int *>(smem + kPathSmemBar + 12);
+    const uint32_t tmem = mlp_prologue(a.w_image, sw, bar, tmem_slot, cta_err, 64u);
+    uint8_t *xb[kLayers];
+    for (int l = 0; l < kLayers; ++l)
+        xb[l] = smem + ((l & 1) ? kPathSmemX1 : kPathSmemX0);
+    uint32_t phase = 0;
+    const uint32_t count = *a.queue_count;
+    const uint32_t n_tiles = (count + kThreads - 1) / kThreads;
+    for (uint32_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+        const uint32_t q = tile * kThreads + threadIdx.x;
+        const bool valid = q < count;
+        uint32_t i = 0;
+        f3 pn = mk(0, 0, 0), wo = mk(0, 0, 1), nrm = mk(0, 0, 1);
+        if (valid) {
+            i = a.queue[q];
+            float4 o4 = a.o_pdf[i], d4 = a.d_info[i], h4 = a.hits[i];
+            f3 d = mk(d4.x, d4.y, d4.z);
+            pn = normalise_position(a.gp, mk(o4.x, o4.y, o4.z) + h4.x * d);
+            wo = -normalize(d);
+            const float4 *pt = a.prim_tris + 3 * (size_t)__float_as_uint(h4.w);
+            float4 v0 = __ldg(pt), v1 = __ldg(pt + 1), v2 = __ldg(pt + 2);
+            nrm = facing_normal(mk(v0.x, v0.y, v0.z), mk(v1.x, v1.y, v1.z), mk(v2.x, v2.y, v2.z), wo);
+        }
+        encode_row(a.gp, a.grid, valid, pn, wo, nrm, xb[0]);
+        float o[kOut];
+        if (!mlp_forward(xb, sw, tmem, bar, phase, cta_err, a.err, o))
+            break;
+        if (valid) {
+            Lobe lobes[kLobes];
+            decode_mixture(o, lobes);
+            // weights scaled by the selection probability: they sum to alpha
+            const float alpha = a.alpha_max * sigmoid(o[kSel]);
+            for (int j = 0; j < kLobes; ++j)
+                lobes[j].w *= alpha;
+            for (int j = 0; j < kLobes; ++j)
+                a.lobes[(size_t)j * a.cap + i] = make_float4(lobes[j].mu.x, lobes[j].mu.y, lobes[j].mu.z, lobes[j].kappa);
+            a.lobes[(size_t)8 * a.cap + i] = make_float4(lobes[0].w, lobes[1].w, lobes[2].w, lobes[3].w);
+            a.lobes[(size_t)9 * a.cap + i] = make_float4(lobes[4].w, lobes[5].w, lobes[6].w, lobes[7].w);
+        }
+    }
+    mlp_epilogue(tmem, 64u);
 }
 
 // fp32 master weights -> bf16 canonical image
@@ -392,9 +513,11 @@ ks_status check_err(ks_guide *g)
     return KS_OK;
 }
 
-// Runs the MLP over n device-resident rows.
-ks_status run_mlp(ks_guide *g, bool train, uint32_t n, const float *pos, const float *wo, const float *wi,
-                  const float *target, float *out)
+// Runs the MLP over n device-resident rows (pos / wo / wi rows `stride` floats apart, BSDF pdfs
+// pb_stride floats apart).
+ks_status run_mlp(ks_guide *g, bool train, uint32_t n, const float *pos, const float *wo, const float *nrm,
+                  const float *wi, const float *target, float *out, uint32_t stride = 3, const float *pb = nullptr,
+                  uint32_t pb_stride = 1)
 {
     if (!g->packed) {
         ks_status s = pack(g);
@@ -406,11 +529,16 @@ ks_status run_mlp(ks_guide *g, bool train, uint32_t n, const float *pos, const f
     a.grid = g->grid.ptr;
     a.w_image = g->w_image.ptr;
     a.n = n;
+    a.stride = stride;
     a.pos = pos;
     a.wo = wo;
     a.wi = wi;
     a.target = target;
+    a.nrm = nrm;
     a.target_scale = n ? 1.0f / (float)n : 0.0f;
+    a.pb = pb;
+    a.pb_stride = pb_stride;
+    a.alpha_max = g->params.alpha_max;
     a.out = out;
     a.w_grad = g->w_grad.ptr;
     a.grid_grad = g->grid_grad.ptr;
@@ -443,6 +571,59 @@ ks_status adam(ks_guide *g)
     return KS_OK;
 }
 
+ks_context *context_of(const ks_guide *g) { return g->ctx; }
+
+ks_status infer_paths(ks_guide *g, const uint32_t *queue, const uint32_t *queue_count, const float4 *o_pdf,
+                      const float4 *d_info, const float4 *hits, const float4 *prim_tris, float4 *lobes, uint32_t cap)
+{
+    if (!g->packed) {
+        ks_status s = pack(g);
+        if (s != KS_OK)
+            return s;
+    }
+    PathArgs a{};
+    a.gp = g->gp;
+    a.grid = g->grid.ptr;
+    a.w_image = g->w_image.ptr;
+    a.queue = queue;
+    a.queue_count = queue_count;
+    a.o_pdf = o_pdf;
+    a.d_info = d_info;
+    a.hits = hits;
+    a.prim_tris = prim_tris;
+    a.lobes = lobes;
+    a.cap = cap;
+    a.alpha_max = g->params.alpha_max;
+    a.err = g->err.ptr;
+    k_guide_paths<<<g->ctx->sm_count * kPathCtasPerSm, kThreads, kPathSmem, g->ctx->stream>>>(a);
+    KS_CUDA_TRY(g->ctx, cudaGetLastError());
+    return KS_OK;
+}
+
+ks_status train_rows(ks_guide *g, uint32_t n, const float4 *pos, const float4 *wo, const float4 *nrm,
+                     const float4 *wi, const float *t, uint32_t batch, uint32_t *steps)
+{
+    if (batch == 0)
+        batch = 1u << 18;
+    for (uint32_t off = 0; off < n; off += batch) {
+        uint32_t rows = std::min(batch, n - off);
+        KS_CUDA_TRY(g->ctx, cudaMemsetAsync(g->loss.ptr, 0, sizeof(double), g->ctx->stream));
+        // the BSDF pdf of each record sits in the w component of its wo row
+        ks_status s = run_mlp(g, true, rows, reinterpret_cast<const float *>(pos + off),
+                              reinterpret_cast<const float *>(wo + off), reinterpret_cast<const float *>(nrm + off),
+                              reinterpret_cast<const float *>(wi + off), t + off, nullptr, 4,
+                              reinterpret_cast<const float *>(wo + off) + 3, 4);
+        if (s == KS_OK)
+            s = adam(g);
+        if (s != KS_OK)
+            return s;
+        ++*steps;
+    }
+    return KS_OK;
+}
+
+ks_status status(ks_guide *g) { return check_err(g); }
+
 } // namespace guide_impl
 } // namespace ksb
 
@@ -471,6 +652,8 @@ ks_status ks_guide_create(ks_context *ctx, const ks_guide_params *params, ks_gui
         g->params.base_res = 16.0f;
     if (!(g->params.max_res > g->params.base_res))
         g->params.max_res = 2048.0f;
+    if (!(g->params.alpha_max > 0.0f && g->params.alpha_max <= 1.0f))
+        g->params.alpha_max = 0.8f;
     const double lscale = std::log((double)g->params.max_res / (double)g->params.base_res) / (double)(kLevels - 1);
     for (int l = 0; l < kLevels; ++l)
         g->gp.res[l] = (uint32_t)std::floor((double)g->params.base_res * std::exp(lscale * l) + 1e-9);
@@ -497,6 +680,8 @@ ks_status ks_guide_create(ks_context *ctx, const ks_guide_params *params, ks_gui
         e = cudaFuncSetAttribute(k_mlp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemTotal);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_mlp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemTotal);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_guide_paths, cudaFuncAttributeMaxDynamicSharedMemorySize, kPathSmem);
     if (e != cudaSuccess) {
         delete g;
         return cuda_fail(ctx, e, "ks_guide_create");
@@ -552,6 +737,16 @@ ks_status ks_guide_level_res(const ks_guide *g, uint32_t res[KS_GUIDE_LEVELS])
     return KS_OK;
 }
 
+ks_status ks_guide_last_loss(ks_guide *g, double *loss)
+{
+    if (!g || !loss)
+        return KS_ERR_INVALID_ARGUMENT;
+    KS_CUDA_TRY(g->ctx, cudaSetDevice(g->ctx->device));
+    KS_CUDA_TRY(g->ctx, cudaStreamSynchronize(g->ctx->stream));
+    KS_CUDA_TRY(g->ctx, cudaMemcpy(loss, g->loss.ptr, sizeof(double), cudaMemcpyDeviceToHost));
+    return KS_OK;
+}
+
 ks_status ks_guide_get_weights(ks_guide *g, float *mlp_weights, float *grid)
 {
     if (!g)
@@ -577,37 +772,43 @@ ks_status ks_guide_set_weights(ks_guide *g, const float *mlp_weights, const floa
     return KS_OK;
 }
 
-ks_status ks_guide_infer(ks_guide *g, const float *pos, const float *wo, uint32_t n, float *raw_out)
+ks_status ks_guide_infer(ks_guide *g, const float *pos, const float *wo, const float *normal, uint32_t n,
+                         float *raw_out)
 {
-    if (!g || !pos || !wo || !raw_out)
+    if (!g || !pos || !wo || !normal || !raw_out)
         return KS_ERR_INVALID_ARGUMENT;
     ks_context *ctx = g->ctx;
     KS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
     if (n == 0)
         return KS_OK;
-    DevBuf<float> dp, dw, dout;
+    DevBuf<float> dp, dw, dn, dout;
     KS_CUDA_TRY(ctx, dp.alloc(3 * (size_t)n));
     KS_CUDA_TRY(ctx, dw.alloc(3 * (size_t)n));
+    KS_CUDA_TRY(ctx, dn.alloc(3 * (size_t)n));
     KS_CUDA_TRY(ctx, dout.alloc((size_t)kOut * n));
     cudaStream_t st = ctx->stream;
     KS_CUDA_TRY(ctx, cudaMemcpyAsync(dp.ptr, pos, dp.bytes(), cudaMemcpyHostToDevice, st));
     KS_CUDA_TRY(ctx, cudaMemcpyAsync(dw.ptr, wo, dw.bytes(), cudaMemcpyHostToDevice, st));
-    ks_status s = run_mlp(g, false, n, dp.ptr, dw.ptr, nullptr, nullptr, dout.ptr);
+    KS_CUDA_TRY(ctx, cudaMemcpyAsync(dn.ptr, normal, dn.bytes(), cudaMemcpyHostToDevice, st));
+    ks_status s = run_mlp(g, false, n, dp.ptr, dw.ptr, dn.ptr, nullptr, nullptr, dout.ptr);
     if (s != KS_OK)
         return s;
     KS_CUDA_TRY(ctx, cudaMemcpyAsync(raw_out, dout.ptr, dout.bytes(), cudaMemcpyDeviceToHost, st));
     return check_err(g);
 }
 
-ks_status ks_guide_gradients(ks_guide *g, const float *pos, const float *wo, const float *wi, const float *target,
-                             uint32_t n, int apply_adam, double *loss, float *mlp_grad, float *grid_grad)
+ks_status ks_guide_gradients(ks_guide *g, const float *pos, const float *wo, const float *normal, const float *wi,
+                             const float *target, const float *bsdf_pdf, uint32_t n, int apply_adam, double *loss,
+                             float *mlp_grad, float *grid_grad)
 {
-    if (!g || !pos || !wo || !wi || !target)
+    if (!g || !pos || !wo || !normal || !wi || !target)
         return KS_ERR_INVALID_ARGUMENT;
     ks_context *ctx = g->ctx;
     KS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;
-    DevBuf<float> dp, dwo, dwi, dt;
+    DevBuf<float> dp, dwo, dn, dwi, dt, dpb;
+    KS_CUDA_TRY(ctx, dn.alloc(3 * (size_t)n + 3));
+    KS_CUDA_TRY(ctx, cudaMemcpyAsync(dn.ptr, normal, 12 * (size_t)n, cudaMemcpyHostToDevice, st));
     KS_CUDA_TRY(ctx, dp.alloc(3 * (size_t)n + 3));
     KS_CUDA_TRY(ctx, dwo.alloc(3 * (size_t)n + 3));
     KS_CUDA_TRY(ctx, dwi.alloc(3 * (size_t)n + 3));
@@ -616,8 +817,12 @@ ks_status ks_guide_gradients(ks_guide *g, const float *pos, const float *wo, con
     KS_CUDA_TRY(ctx, cudaMemcpyAsync(dwo.ptr, wo, 12 * (size_t)n, cudaMemcpyHostToDevice, st));
     KS_CUDA_TRY(ctx, cudaMemcpyAsync(dwi.ptr, wi, 12 * (size_t)n, cudaMemcpyHostToDevice, st));
     KS_CUDA_TRY(ctx, cudaMemcpyAsync(dt.ptr, target, 4 * (size_t)n, cudaMemcpyHostToDevice, st));
+    if (bsdf_pdf) {
+        KS_CUDA_TRY(ctx, dpb.alloc((size_t)n + 1));
+        KS_CUDA_TRY(ctx, cudaMemcpyAsync(dpb.ptr, bsdf_pdf, 4 * (size_t)n, cudaMemcpyHostToDevice, st));
+    }
     KS_CUDA_TRY(ctx, cudaMemsetAsync(g->loss.ptr, 0, sizeof(double), st));
-    ks_status s = run_mlp(g, true, n, dp.ptr, dwo.ptr, dwi.ptr, dt.ptr, nullptr);
+    ks_status s = run_mlp(g, true, n, dp.ptr, dwo.ptr, dn.ptr, dwi.ptr, dt.ptr, nullptr, 3, dpb.ptr, 1);
     if (s != KS_OK)
         return s;
     if (loss)

@@ -1,11 +1,14 @@
 // Learned path guiding: input encodings, the vMF mixture head and its loss gradient.
 //
-// The network maps a shading point (position, outgoing direction) to an 8-lobe von Mises-Fisher
-// mixture over incident directions:
+// The network maps a shading point (position, outgoing direction, surface normal) to an 8-lobe
+// von Mises-Fisher mixture over incident directions:
 //   input  = multiresolution hash-grid encoding of the position (16 levels x 2 features) +
-//            real spherical harmonics of the outgoing direction up to degree 3 (16 values)
-//   MLP    = 48 -> 64 -> 64 -> 64 -> 64 -> 40 (4 hidden ReLU layers, no biases)
-//   output = per lobe: mean direction (3, normalised), log concentration, mixture logit.
+//            real spherical harmonics up to degree 3 of the outgoing direction (16 values) and of
+//            the geometric normal turned towards it (16 values)
+//   MLP    = 64 -> 64 -> 64 -> 64 -> 64 -> 41 (4 hidden ReLU layers, no biases)
+//   output = per lobe: mean direction (3, normalised), log concentration, mixture logit; then one
+//            logit of the selection probability alpha = alpha_max * sigmoid(logit) with which a
+//            renderer draws from the mixture instead of the BSDF (one-sample MIS).
 // vMF evaluation and sampling follow the reference's VMF (vmf.h:10-56, max_kappa 1e4) and
 // sample_vmm (vmf.h:123-127); lobe selection is sample_small_distrib (rng.h:399-434).
 #pragma once
@@ -22,10 +25,11 @@ constexpr int kLog2T = 19;
 constexpr uint32_t kTableSize = 1u << kLog2T;
 constexpr int kGridFeatures = kLevels * kFeatPerLevel; // 32
 constexpr int kShCoeffs = 16;
-constexpr int kIn = kGridFeatures + kShCoeffs; // 48
+constexpr int kIn = kGridFeatures + 2 * kShCoeffs; // 64
 constexpr int kHidden = 64;
 constexpr int kLobes = 8;
-constexpr int kOut = kLobes * 5; // 40
+constexpr int kSel = kLobes * 5;     // index of the selection logit
+constexpr int kOut = kLobes * 5 + 1; // 41
 constexpr int kOutPad = 48;      // output layer rows padded to a multiple of 16
 constexpr int kLayers = 5;
 constexpr float kMaxKappa = 1e4f; // VMF::max_kappa (vmf.h:111)
@@ -41,7 +45,7 @@ __host__ __device__ constexpr int weight_offset(int l)
         o += layer_in(i) * layer_out(i);
     return o;
 }
-constexpr int kWeights = weight_offset(kLayers); // 18432
+constexpr int kWeights = weight_offset(kLayers); // 19456
 
 struct GridParams
 {
@@ -85,6 +89,14 @@ __device__ __forceinline__ void level_corners(const GridParams &g, int l, f3 pn,
     }
 }
 
+// Geometric normal of triangle (p0, p1, p2) on the side of the unit direction wo: the normal input
+// of the network (the same arithmetic wherever a vertex is encoded).
+__device__ __forceinline__ f3 facing_normal(f3 p0, f3 p1, f3 p2, f3 wo)
+{
+    f3 n = normalize(cross(p1 - p0, p2 - p0));
+    return dot(n, wo) < 0.0f ? -n : n;
+}
+
 __device__ __forceinline__ f3 normalise_position(const GridParams &g, f3 p)
 {
     f3 q = mk((p.x - g.bmin[0]) * g.inv_ext[0], (p.y - g.bmin[1]) * g.inv_ext[1], (p.z - g.bmin[2]) * g.inv_ext[2]);
@@ -125,7 +137,24 @@ struct Lobe
     float w;
 };
 
-// Decodes the 40 raw outputs of one sample into the mixture.
+__host__ __device__ inline float sigmoid(float x) { return 1.0f / (1.0f + expf(-x)); }
+__host__ __device__ inline float softplus(float x) { return x > 20.0f ? x : log1pf(expf(x)); }
+
+// log concentration from its raw output: a smooth clamp into (kMinLogKappa, log kMaxKappa) whose
+// derivative (sigmoid(z - lo) - sigmoid(z - hi)) stays positive, so no lobe is ever cut off from
+// the gradient by a bound.
+__host__ __device__ inline float log_kappa(float z)
+{
+    const float lo = kMinLogKappa, hi = 9.210340372f; // log(1e4)
+    return lo + softplus(z - lo) - softplus(z - hi);
+}
+__host__ __device__ inline float log_kappa_grad(float z)
+{
+    const float lo = kMinLogKappa, hi = 9.210340372f;
+    return sigmoid(z - lo) - sigmoid(z - hi);
+}
+
+// Decodes the raw outputs of one sample into the mixture.
 __device__ __forceinline__ void decode_mixture(const float o[kOut], Lobe lobes[kLobes])
 {
     float mx = -kInf;
@@ -136,8 +165,7 @@ __device__ __forceinline__ void decode_mixture(const float o[kOut], Lobe lobes[k
         f3 r = mk(o[5 * j], o[5 * j + 1], o[5 * j + 2]);
         float n = sqrtf(sqnorm(r));
         lobes[j].mu = n > 1e-20f ? r / n : mk(0.0f, 0.0f, 1.0f);
-        float lk = fminf(fmaxf(o[5 * j + 3], kMinLogKappa), logf(kMaxKappa));
-        lobes[j].kappa = expf(lk);
+        lobes[j].kappa = fminf(expf(log_kappa(o[5 * j + 3])), kMaxKappa);
         lobes[j].w = expf(o[5 * j + 4] - mx);
         sum += lobes[j].w;
     }
@@ -202,10 +230,17 @@ __device__ __forceinline__ f3 mixture_sample(const Lobe lobes[kLobes], float u0,
     return w.x * X + w.y * Y + w.z * N;
 }
 
-// Loss of one training sample, -t * log q(wi), and its gradient with respect to the 40 raw
-// outputs (exact derivative of decode_mixture + mixture_pdf).  Returns false for an unusable
-// sample (q == 0); the gradient is then zero.
-__device__ __forceinline__ bool mixture_loss_grad(const float o[kOut], f3 wi, float t, float &loss, float g[kOut])
+// Loss of one training sample and its gradient with respect to the raw outputs (exact derivatives
+// of decode_mixture + mixture_pdf + the selection sigmoid).  Two objectives over samples with
+// t = f cos L / p (the estimate of the integrand over the density the direction was drawn from):
+//   mixture:   -t log q(wi)    fits q to the integrand f cos L (its KL divergence);
+//   selection: -t log m(wi)    m = alpha q + (1 - alpha) p_bsdf, the combined proposal of one-
+//                              sample MIS, minimised over alpha alone (q held fixed), so that
+//                              alpha learns how far to trust q without starving q of gradient.
+// `loss` returns -t log m.  Returns false for an unusable sample (m == 0 or q == 0); the gradient
+// is then zero.
+__device__ __forceinline__ bool mixture_loss_grad(const float o[kOut], f3 wi, float t, float p_bsdf, float alpha_max,
+                                                  float &loss, float g[kOut])
 {
     for (int i = 0; i < kOut; ++i)
         g[i] = 0.0f;
@@ -219,20 +254,21 @@ __device__ __forceinline__ bool mixture_loss_grad(const float o[kOut], f3 wi, fl
         v[j] = vmf_eval(lobes[j].mu, lobes[j].kappa, wi);
         q += lobes[j].w * v[j];
     }
-    if (!(q > 1e-30f))
+    const float sg = sigmoid(o[kSel]), alpha = alpha_max * sg;
+    const float m = alpha * q + (1.0f - alpha) * p_bsdf;
+    if (!(m > 1e-30f) || !(q > 1e-30f))
         return false;
-    loss = -t * logf(q);
+    loss = -t * logf(m);
+    // d(-t log m)/d alpha = -t (q - p_bsdf) / m, alpha = alpha_max sigmoid(z)
+    g[kSel] = -t * (q - p_bsdf) / m * alpha_max * sg * (1.0f - sg);
     for (int j = 0; j < kLobes; ++j) {
         float r = lobes[j].w * v[j] / q; // responsibility
         // mixture logit: d(-t log q)/dz_j = -t (r_j - pi_j)
         g[5 * j + 4] = -t * (r - lobes[j].w);
         float kappa = lobes[j].kappa;
-        float lk = o[5 * j + 3];
-        // d log v / d kappa = 1/kappa - 2 / (e^{2 kappa} - 1) + (mu.w - 1); kappa = exp(lk) (clamped)
-        if (lk > kMinLogKappa && lk < logf(kMaxKappa)) {
-            float dlog = 1.0f / kappa - 2.0f / expm1f(2.0f * kappa) + (dot(lobes[j].mu, wi) - 1.0f);
-            g[5 * j + 3] = -t * r * dlog * kappa;
-        }
+        // d log v / d kappa = 1/kappa - 2 / (e^{2 kappa} - 1) + (mu.w - 1); kappa = exp(log_kappa(z))
+        float dlog = 1.0f / kappa - 2.0f / expm1f(2.0f * kappa) + (dot(lobes[j].mu, wi) - 1.0f);
+        g[5 * j + 3] = -t * r * dlog * kappa * log_kappa_grad(o[5 * j + 3]);
         // mean direction: mu = raw / |raw|, d log v / d mu = kappa * wi
         f3 raw = mk(o[5 * j], o[5 * j + 1], o[5 * j + 2]);
         float n = sqrtf(sqnorm(raw));

@@ -17,6 +17,8 @@
 // bounce), so each path draws the same sample values as the CPU path.  Finished paths are added
 // to FP64 pixel accumulators (RenderTarget2::add / add_miss, render_target.cpp:82-107).
 #include "ks_bsdf.cuh"
+#include "ks_guide_host.h"
+#include "ks_guide_view.cuh"
 #include "ks_lights.cuh"
 #include "ks_sampler.cuh"
 #include "ks_traverse.cuh"
@@ -50,6 +52,7 @@ struct PathBuf
     float4 *d_info;   // ray direction, (sobol dimension << 16 | bounce)
     float4 *beta_pix; // throughput, pixel index
     float4 *L_smp;    // radiance so far, sample index
+    uint32_t *rec;    // guided renders: training record of the path (kNoRecord: none); else null
 };
 
 struct ShadowBuf
@@ -243,6 +246,8 @@ __global__ void k_raygen(RenderParams rp, PathBuf pb, uint32_t base_slot, uint64
     pb.d_info[slot] = make_float4(dir.x, dir.y, dir.z, fbits(((uint32_t)smp.dimension << 16) | 0u));
     pb.beta_pix[slot] = make_float4(1.0f, 1.0f, 1.0f, fbits(pix));
     pb.L_smp[slot] = make_float4(0.0f, 0.0f, 0.0f, fbits((uint32_t)s));
+    if (pb.rec)
+        pb.rec[slot] = kNoRecord;
 }
 
 // Adds a per-thread work count into two 64-bit device counters, one atomic per warp.
@@ -332,11 +337,17 @@ __global__ void __launch_bounds__(128) k_sample(RenderParams rp, PathBuf cur, co
 // Shading of the paths listed in `queue` (indices into the current path buffer).  kMiss = true
 // handles the rays that left the scene, kMiss = false the rays that hit a triangle; the extension
 // kernel sorts the two kinds into separate queues so that a warp runs one of the two code paths.
-template <bool kMiss>
+// kGuided: directions are drawn from the guide's mixture or the BSDF (one-sample MIS: the
+// throughput divides by the combined density) and paths capture training records (layout in
+// ks_guide_view.cuh).  The light MIS weights keep the BSDF pdf, so the estimator has the
+// expectation of the unguided one: the reference's NEE weight omits the light-selection
+// probability that its emitter-hit weight includes, and the two only stay the same functions of
+// the direction if both keep seeing the BSDF pdf.
+template <bool kMiss, bool kGuided>
 __global__ void __launch_bounds__(128) k_shade(SceneView sv, RenderParams rp, PathBuf cur, PathBuf nxt,
                                                const float4 *hits, const float4 *samples, const uint32_t *queue,
                                                const uint32_t *queue_count, uint32_t *next_count, ShadowBuf sb,
-                                               uint32_t *shadow_count, double *accum, double *weights)
+                                               uint32_t *shadow_count, double *accum, double *weights, GuideView gv)
 {
     const uint32_t stride = gridDim.x * blockDim.x;
     const uint32_t count = *queue_count;
@@ -349,6 +360,12 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sv, RenderParams rp, Pa
         float n_pdf = 0.0f, sh_tmax = 0.0f;
         uint32_t n_info = 0, pix = 0, smp = 0;
         bool finish = false, miss_only = false;
+        // guided renders: the path's record, and a record to create at this vertex
+        uint32_t rec = kNoRecord;
+        bool want_rec = false;
+        f3 rc_p = mk(0, 0, 0), rc_wo = mk(0, 0, 0), rc_wi = mk(0, 0, 0), rc_beta = mk(0, 0, 0), rc_n = mk(0, 0, 0);
+        float rc_pb = 0.0f;
+        int rc_bounce = 0;
         if (valid) {
             float4 a = cur.o_pdf[i], b = cur.d_info[i], c = cur.beta_pix[i], d = cur.L_smp[i];
             f3 ro = mk(a.x, a.y, a.z), rd = mk(b.x, b.y, b.z);
@@ -362,6 +379,8 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sv, RenderParams rp, Pa
             smp = bits(d.w);
             float4 h = hits[i];
             uint32_t slot = bits(h.w);
+            if constexpr (kGuided)
+                rec = cur.rec[i];
             if constexpr (kMiss) {
                 (void)slot;
                 // miss: unidirectional sky strategy (small_pt.cpp:83-110)
@@ -377,6 +396,9 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sv, RenderParams rp, Pa
                         float mis = power_heur(pdf_wi_bsdf, pdf_wi_light * pr_light);
                         f3 beta_uni = clamp_contrib(Le * mis, bounce, rp, false);
                         L += beta * beta_uni;
+                        if constexpr (kGuided)
+                            if (rec != kNoRecord)
+                                record_add(gv, rec, beta * beta_uni);
                     }
                 }
                 finish = true;
@@ -408,6 +430,9 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sv, RenderParams rp, Pa
                                 float mis = power_heur(pdf_wi_bsdf, pdf_wi_light * pr_light);
                                 f3 beta_uni = clamp_contrib(Le * mis, bounce, rp, false);
                                 L += beta * beta_uni;
+                                if constexpr (kGuided)
+                                    if (rec != kNoRecord)
+                                        record_add(gv, rec, beta * beta_uni);
                             }
                         }
                     }
@@ -457,12 +482,42 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sv, RenderParams rp, Pa
                     int next_dim = dim + 6;
                     f3 wi_local;
                     float pdf_wi = 0.0f;
-                    f3 sbeta = bsdf.sample(wo_local, wi_local, u_lobe, b0, b1, pdf_wi);
+                    f3 sbeta, wnext;
+                    bool guided = false;
+                    float p_bsdf = 0.0f; // BSDF pdf of the sampled direction
+                    if constexpr (kGuided)
+                        guided = gv.active != 0;
+                    if (guided) {
+                        // one-sample MIS of the guide (probability alpha of this vertex) and the BSDF
+                        const float al = guide_alpha(gv, i);
+                        f3 fcos;
+                        float p_b = 0.0f;
+                        if (u_lobe < al) {
+                            wnext = guide_sample(gv, i, b0, b1);
+                            wi_local = sh_to_local(it, wnext);
+                            bsdf.eval_and_pdf(wo_local, wi_local, fcos, p_b);
+                        } else {
+                            float ub = fminf((u_lobe - al) / (1.0f - al), 0x1.fffffep-1f);
+                            f3 fs = bsdf.sample(wo_local, wi_local, ub, b0, b1, p_b);
+                            fcos = fs * p_b;
+                            wnext = sh_to_world(it, wi_local);
+                        }
+                        // throughput over the density the direction was drawn from; the MIS weights
+                        // with the lights keep the BSDF pdf (pdf_wi), as in the unguided estimator
+                        const float pdf_mix = is_zero(fcos) ? 0.0f : guide_pdf(gv, i, wnext) + (1.0f - al) * p_b;
+                        sbeta = pdf_mix > 0.0f ? fcos / pdf_mix : mk(0, 0, 0);
+                        pdf_wi = p_b;
+                        p_bsdf = p_b;
+                    } else {
+                        sbeta = bsdf.sample(wo_local, wi_local, u_lobe, b0, b1, pdf_wi);
+                        p_bsdf = pdf_wi;
+                    }
                     f3 nbeta = beta * sbeta;
                     if (max3(nbeta) == 0.0f) {
                         finish = true;
                     } else {
-                        f3 wnext = sh_to_world(it, wi_local);
+                        if (!guided)
+                            wnext = sh_to_world(it, wi_local);
                         n_o = spawn_origin(it.p, wnext, it.n);
                         n_d = wnext;
                         n_pdf = pdf_wi;
@@ -480,6 +535,21 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sv, RenderParams rp, Pa
                             cont = true;
                             n_beta = nbeta;
                             n_info = ((uint32_t)next_dim << 16) | (uint32_t)(bounce + 1);
+                            if constexpr (kGuided) {
+                                if (gv.rec_cap && rec == kNoRecord) {
+                                    uint32_t hh = path_hash(pix, smp);
+                                    if ((hh & 0xffffu) < gv.rec_threshold && (uint32_t)bounce == (hh >> 16) % gv.rec_bounces) {
+                                        want_rec = true;
+                                        rc_p = it.p;
+                                        rc_wo = wo;
+                                        rc_wi = wnext;
+                                        rc_beta = beta;
+                                        rc_pb = p_bsdf;
+                                        rc_n = guide::facing_normal(p0, p1, p2, wo);
+                                        rc_bounce = bounce;
+                                    }
+                                }
+                            }
                         }
                     }
                 }
@@ -487,6 +557,23 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sv, RenderParams rp, Pa
         }
         uint32_t jc = warp_append(next_count, cont);
         uint32_t js = warp_append(shadow_count, shadow);
+        const uint32_t sh_rec = rec; // the shadow ray of this vertex feeds the path's earlier record
+        if constexpr (kGuided) {
+            uint32_t jr = warp_append(gv.rec_count, want_rec);
+            if (want_rec && jr < gv.rec_cap) {
+                gv.rec_pos[jr] = make_float4(rc_p.x, rc_p.y, rc_p.z, fbits((uint32_t)rc_bounce));
+                gv.rec_wo[jr] = make_float4(rc_wo.x, rc_wo.y, rc_wo.z, rc_pb);
+                gv.rec_wi[jr] = make_float4(rc_wi.x, rc_wi.y, rc_wi.z, 0.0f);
+                gv.rec_n[jr] = make_float4(rc_n.x, rc_n.y, rc_n.z, 0.0f);
+                gv.rec_ibeta[jr] = make_float4(rc_beta.x > 0.0f ? 1.0f / rc_beta.x : 0.0f,
+                                               rc_beta.y > 0.0f ? 1.0f / rc_beta.y : 0.0f,
+                                               rc_beta.z > 0.0f ? 1.0f / rc_beta.z : 0.0f, 0.0f);
+                gv.rec_t[jr] = 0.0f;
+                rec = jr;
+            }
+            if (cont)
+                nxt.rec[jc] = rec;
+        }
         if (cont) {
             nxt.o_pdf[jc] = make_float4(n_o.x, n_o.y, n_o.z, n_pdf);
             nxt.d_info[jc] = make_float4(n_d.x, n_d.y, n_d.z, fbits(n_info));
@@ -496,7 +583,7 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sv, RenderParams rp, Pa
         if (shadow) {
             sb.o_tmax[js] = make_float4(sh_o.x, sh_o.y, sh_o.z, sh_tmax);
             sb.d_target[js] = make_float4(sh_d.x, sh_d.y, sh_d.z, fbits(cont ? jc : (kTermBit | pix)));
-            sb.contrib[js] = make_float4(sh_c.x, sh_c.y, sh_c.z, 0.0f);
+            sb.contrib[js] = make_float4(sh_c.x, sh_c.y, sh_c.z, fbits(sh_rec));
             if (!cont)
                 sb.L_term[js] = make_float4(L.x, L.y, L.z, 0.0f);
         }
@@ -511,7 +598,7 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sv, RenderParams rp, Pa
 
 __global__ void __launch_bounds__(128) k_shadow(SceneView sv, ShadowBuf sb, const uint32_t *shadow_count,
                                                 PathBuf nxt, double *accum, double *weights, int *overflow,
-                                                unsigned long long *work)
+                                                unsigned long long *work, GuideView gv)
 {
     const uint32_t n = *shadow_count;
     TravCount tc;
@@ -530,6 +617,8 @@ __global__ void __launch_bounds__(128) k_shadow(SceneView sv, ShadowBuf sb, cons
             atomicOr(overflow, 1);
         uint32_t target = bits(b.w);
         float4 c = sb.contrib[i];
+        if (gv.rec_cap && !occ && bits(c.w) != kNoRecord)
+            record_add(gv, bits(c.w), mk(c.x, c.y, c.z));
         if (target & kTermBit) {
             float4 l = sb.L_term[i];
             f3 L = mk(l.x, l.y, l.z);
@@ -564,11 +653,24 @@ struct RenderWork
     uint32_t capacity = 0;
 };
 
+// Guided renders: per-slot mixtures, record index per path, training records.
+struct GuideWork
+{
+    DevBuf<float4> lobes;
+    DevBuf<uint32_t> rec[2];
+    DevBuf<float4> rec_f4[5]; // pos, wo, wi, ibeta, normal
+    DevBuf<float> rec_t;
+    DevBuf<uint32_t> rec_count;
+};
+
 static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const ks_small_pt_params *in,
                              ks_progress_fn cb, void *user, double *d_accum, double *d_weights, double *h_accum,
-                             double *h_weights)
+                             double *h_weights, ks_guide *guide = nullptr,
+                             const ks_guide_render_options *gopt = nullptr)
 {
     ks_context *ctx = scene->ctx;
+    if (guide && guide_impl::context_of(guide) != ctx)
+        return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_small_pt_render_guided: guide and scene on different contexts");
     cudaStream_t st = ctx->stream;
     if (!scene->bvh_built || !scene->lights_built)
         return fail(ctx, KS_ERR_NOT_BUILT, "ks_small_pt_render: call ks_scene_build_bvh first");
@@ -629,11 +731,48 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
     KS_CUDA_TRY(ctx, cudaMemsetAsync(w.overflow.ptr, 0, sizeof(int), st));
     PathBuf pb[2];
     for (int b = 0; b < 2; ++b)
-        pb[b] = PathBuf{w.state[b][0].ptr, w.state[b][1].ptr, w.state[b][2].ptr, w.state[b][3].ptr};
+        pb[b] = PathBuf{w.state[b][0].ptr, w.state[b][1].ptr, w.state[b][2].ptr, w.state[b][3].ptr, nullptr};
+    GuideWork gw;
+    GuideView gv{};
+    ks_guide_render_options go{};
+    if (guide) {
+        go = *gopt;
+        if (go.guide_from_pass < 0 || go.train_passes < 0)
+            return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_small_pt_render_guided: negative pass count");
+        if (go.max_records == 0)
+            go.max_records = 1u << 19;
+        if (go.record_bounces <= 0)
+            go.record_bounces = 6;
+        KS_CUDA_TRY(ctx, gw.lobes.alloc((size_t)kGuideLobeVecs * w.capacity));
+        for (int b = 0; b < 2; ++b) {
+            KS_CUDA_TRY(ctx, gw.rec[b].alloc(w.capacity));
+            pb[b].rec = gw.rec[b].ptr;
+        }
+        if (go.train_passes > 0) {
+            for (auto &f : gw.rec_f4)
+                KS_CUDA_TRY(ctx, f.alloc(go.max_records));
+            KS_CUDA_TRY(ctx, gw.rec_t.alloc(go.max_records));
+        }
+        KS_CUDA_TRY(ctx, gw.rec_count.alloc(1));
+        KS_CUDA_TRY(ctx, cudaMemsetAsync(gw.rec_count.ptr, 0, sizeof(uint32_t), st));
+        gv.lobes = gw.lobes.ptr;
+        gv.cap = w.capacity;
+        gv.rec_pos = gw.rec_f4[0].ptr;
+        gv.rec_wo = gw.rec_f4[1].ptr;
+        gv.rec_wi = gw.rec_f4[2].ptr;
+        gv.rec_ibeta = gw.rec_f4[3].ptr;
+        gv.rec_n = gw.rec_f4[4].ptr;
+        gv.rec_t = gw.rec_t.ptr;
+        gv.rec_count = gw.rec_count.ptr;
+        gv.rec_bounces = (uint32_t)std::max(1, std::min(go.record_bounces, in->bounces));
+        // about twice max_records candidates per pass; paths that end early record nothing
+        const double per_pass = (double)n_pix * std::min(in->spp, in->spp_prog_interval);
+        gv.rec_threshold = (uint32_t)std::min(65536.0, std::ceil(65536.0 * 2.0 * go.max_records / per_pass));
+    }
     ShadowBuf sb{w.shadow[0].ptr, w.shadow[1].ptr, w.shadow[2].ptr, w.shadow[3].ptr};
     uint32_t *h_counts = nullptr;
     KS_CUDA_TRY(ctx, cudaMallocHost((void **)&h_counts, sizeof(uint32_t) * 2));
-    cudaEvent_t ev[5];
+    cudaEvent_t ev[6];
     for (auto &e : ev)
         cudaEventCreate(&e);
     cudaEvent_t t_begin, t_end;
@@ -645,8 +784,14 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
     int cur = 0;
     cudaError_t err = cudaSuccess;
     std::vector<double> cb_acc, cb_w;
-    for (int s0 = 0; s0 < in->spp && err == cudaSuccess; s0 += in->spp_prog_interval) {
+    int pass = 0;
+    for (int s0 = 0; s0 < in->spp && err == cudaSuccess; s0 += in->spp_prog_interval, ++pass) {
         int batch = std::min(in->spp_prog_interval, in->spp - s0);
+        const bool recording = guide && pass < go.train_passes;
+        if (guide) {
+            gv.active = pass >= go.guide_from_pass ? 1 : 0;
+            gv.rec_cap = recording ? go.max_records : 0u;
+        }
         uint64_t total = (uint64_t)n_pix * (uint64_t)batch, issued = 0;
         uint32_t cur_count = 0;
         // every path ends after at most bounces + 1 extension rays
@@ -674,16 +819,38 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
             k_extend<<<grid, 128, 0, st>>>(sv, pb[cur], count, w.hits.ptr, w.queue[0].ptr, w.queue[1].ptr,
                                            w.counters.ptr + 2, w.overflow.ptr, work.ptr);
             cudaEventRecord(ev[2], st);
+            if (guide && gv.active) {
+                ks_status gs = guide_impl::infer_paths(guide, w.queue[0].ptr, w.counters.ptr + 2, pb[cur].o_pdf,
+                                                       pb[cur].d_info, w.hits.ptr, sv.prim_tris, gw.lobes.ptr,
+                                                       w.capacity);
+                if (gs != KS_OK) {
+                    err = cudaErrorLaunchFailure;
+                    break;
+                }
+                stats.kernel_launches++;
+            }
+            cudaEventRecord(ev[5], st);
             k_sample<<<grid, 128, 0, st>>>(rp, pb[cur], w.queue[0].ptr, w.counters.ptr + 2, w.samples.ptr);
-            k_shade<false><<<grid, 128, 0, st>>>(sv, rp, pb[cur], pb[1 - cur], w.hits.ptr, w.samples.ptr,
-                                                 w.queue[0].ptr, w.counters.ptr + 2, w.counters.ptr, sb,
-                                                 w.counters.ptr + 1, d_accum, d_weights);
-            k_shade<true><<<grid, 128, 0, st>>>(sv, rp, pb[cur], pb[1 - cur], w.hits.ptr, w.samples.ptr,
-                                                w.queue[1].ptr, w.counters.ptr + 3, w.counters.ptr, sb,
-                                                w.counters.ptr + 1, d_accum, d_weights);
+            if (guide) {
+                k_shade<false, true><<<grid, 128, 0, st>>>(sv, rp, pb[cur], pb[1 - cur], w.hits.ptr, w.samples.ptr,
+                                                           w.queue[0].ptr, w.counters.ptr + 2, w.counters.ptr, sb,
+                                                           w.counters.ptr + 1, d_accum, d_weights, gv);
+                k_shade<true, true><<<grid, 128, 0, st>>>(sv, rp, pb[cur], pb[1 - cur], w.hits.ptr, w.samples.ptr,
+                                                          w.queue[1].ptr, w.counters.ptr + 3, w.counters.ptr, sb,
+                                                          w.counters.ptr + 1, d_accum, d_weights, gv);
+            } else {
+                k_shade<false, false><<<grid, 128, 0, st>>>(sv, rp, pb[cur], pb[1 - cur], w.hits.ptr,
+                                                            w.samples.ptr, w.queue[0].ptr, w.counters.ptr + 2,
+                                                            w.counters.ptr, sb, w.counters.ptr + 1, d_accum,
+                                                            d_weights, gv);
+                k_shade<true, false><<<grid, 128, 0, st>>>(sv, rp, pb[cur], pb[1 - cur], w.hits.ptr,
+                                                           w.samples.ptr, w.queue[1].ptr, w.counters.ptr + 3,
+                                                           w.counters.ptr, sb, w.counters.ptr + 1, d_accum,
+                                                           d_weights, gv);
+            }
             cudaEventRecord(ev[3], st);
             k_shadow<<<grid, 128, 0, st>>>(sv, sb, w.counters.ptr + 1, pb[1 - cur], d_accum, d_weights,
-                                           w.overflow.ptr, work.ptr + 2);
+                                           w.overflow.ptr, work.ptr + 2, gv);
             cudaEventRecord(ev[4], st);
             stats.kernel_launches += 5;
             cudaMemcpyAsync(h_counts, w.counters.ptr, sizeof(uint32_t) * 2, cudaMemcpyDeviceToHost, st);
@@ -696,7 +863,9 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
             stats.ms_shade += ms;
             cudaEventElapsedTime(&ms, ev[1], ev[2]);
             stats.ms_extend += ms;
-            cudaEventElapsedTime(&ms, ev[2], ev[3]);
+            cudaEventElapsedTime(&ms, ev[2], ev[5]);
+            stats.ms_guide_infer += ms;
+            cudaEventElapsedTime(&ms, ev[5], ev[3]);
             stats.ms_shade += ms;
             cudaEventElapsedTime(&ms, ev[3], ev[4]);
             stats.ms_shadow += ms;
@@ -706,6 +875,32 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
             cur = 1 - cur;
         }
         stats.paths += total;
+        if (err == cudaSuccess && recording) {
+            // train on the records of this pass, then start the next pass's capture from zero
+            uint32_t n_rec = 0;
+            err = cudaMemcpyAsync(&n_rec, gw.rec_count.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+            if (err == cudaSuccess)
+                err = cudaStreamSynchronize(st);
+            if (err != cudaSuccess)
+                break;
+            n_rec = std::min(n_rec, go.max_records);
+            stats.guide_records += n_rec;
+            cudaEventRecord(ev[0], st);
+            ks_status gs = guide_impl::train_rows(guide, n_rec, gw.rec_f4[0].ptr, gw.rec_f4[1].ptr, gw.rec_f4[4].ptr,
+                                                  gw.rec_f4[2].ptr, gw.rec_t.ptr, go.train_batch,
+                                                  &stats.guide_train_steps);
+            cudaEventRecord(ev[1], st);
+            if (gs != KS_OK) {
+                err = cudaErrorLaunchFailure;
+                break;
+            }
+            err = cudaMemsetAsync(gw.rec_count.ptr, 0, sizeof(uint32_t), st);
+            if (err == cudaSuccess)
+                err = cudaEventSynchronize(ev[1]);
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, ev[0], ev[1]);
+            stats.ms_guide_train += ms;
+        }
         if (err == cudaSuccess && cb && h_accum) {
             size_t na = (size_t)W * H * 3, nw = (size_t)W * H * 2;
             cb_acc.resize(na);
@@ -750,6 +945,8 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
         return cuda_fail(ctx, err, "ks_small_pt_render");
     if (overflow)
         return fail(ctx, KS_ERR_QUEUE_OVERFLOW, "ks_small_pt_render: traversal stack depth exceeded");
+    if (guide)
+        return guide_impl::status(guide);
     return KS_OK;
 }
 
@@ -764,8 +961,9 @@ ks_status ks_small_pt_render_device(ks_scene *scene, const ks_camera_desc *camer
     return render_impl(scene, camera, params, nullptr, nullptr, accum_rgb_device, weights_device, nullptr, nullptr);
 }
 
-ks_status ks_small_pt_render(ks_scene *scene, const ks_camera_desc *camera, const ks_small_pt_params *params,
-                             ks_progress_fn cb, void *user, double *accum_rgb, double *weights)
+static ks_status render_host(ks_scene *scene, const ks_camera_desc *camera, const ks_small_pt_params *params,
+                             ks_progress_fn cb, void *user, double *accum_rgb, double *weights, ks_guide *guide,
+                             const ks_guide_render_options *gopt)
 {
     if (!scene || !camera || !params || !accum_rgb || !weights)
         return fail(scene ? scene->ctx : nullptr, KS_ERR_INVALID_ARGUMENT, "ks_small_pt_render: null");
@@ -780,7 +978,7 @@ ks_status ks_small_pt_render(ks_scene *scene, const ks_camera_desc *camera, cons
     KS_CUDA_TRY(ctx, dw.alloc(nw));
     KS_CUDA_TRY(ctx, cudaMemsetAsync(da.ptr, 0, na * sizeof(double), ctx->stream));
     KS_CUDA_TRY(ctx, cudaMemsetAsync(dw.ptr, 0, nw * sizeof(double), ctx->stream));
-    ks_status s = render_impl(scene, camera, params, cb, user, da.ptr, dw.ptr, accum_rgb, weights);
+    ks_status s = render_impl(scene, camera, params, cb, user, da.ptr, dw.ptr, accum_rgb, weights, guide, gopt);
     if (s != KS_OK)
         return s;
     std::vector<double> ha(na), hw(nw);
@@ -792,6 +990,44 @@ ks_status ks_small_pt_render(ks_scene *scene, const ks_camera_desc *camera, cons
     for (size_t k = 0; k < nw; ++k)
         weights[k] += hw[k];
     return KS_OK;
+}
+
+ks_status ks_small_pt_render(ks_scene *scene, const ks_camera_desc *camera, const ks_small_pt_params *params,
+                             ks_progress_fn cb, void *user, double *accum_rgb, double *weights)
+{
+    return render_host(scene, camera, params, cb, user, accum_rgb, weights, nullptr, nullptr);
+}
+
+void ks_guide_render_options_default(ks_guide_render_options *o)
+{
+    if (!o)
+        return;
+    o->guide_from_pass = 1;
+    o->train_passes = 8;
+    o->max_records = 1u << 19;
+    o->train_batch = 1u << 18;
+    o->record_bounces = 6;
+}
+
+ks_status ks_small_pt_render_guided(ks_scene *scene, const ks_camera_desc *camera, const ks_small_pt_params *params,
+                                    ks_guide *guide, const ks_guide_render_options *options, ks_progress_fn cb,
+                                    void *user, double *accum_rgb, double *weights)
+{
+    if (!guide || !options)
+        return fail(scene ? scene->ctx : nullptr, KS_ERR_INVALID_ARGUMENT, "ks_small_pt_render_guided: null");
+    return render_host(scene, camera, params, cb, user, accum_rgb, weights, guide, options);
+}
+
+ks_status ks_small_pt_render_guided_device(ks_scene *scene, const ks_camera_desc *camera,
+                                           const ks_small_pt_params *params, ks_guide *guide,
+                                           const ks_guide_render_options *options, double *accum_rgb_device,
+                                           double *weights_device)
+{
+    if (!scene || !camera || !params || !guide || !options || !accum_rgb_device || !weights_device)
+        return fail(scene ? scene->ctx : nullptr, KS_ERR_INVALID_ARGUMENT, "ks_small_pt_render_guided_device: null");
+    KS_CUDA_TRY(scene->ctx, cudaSetDevice(scene->ctx->device));
+    return render_impl(scene, camera, params, nullptr, nullptr, accum_rgb_device, weights_device, nullptr, nullptr,
+                       guide, options);
 }
 
 ks_status ks_render_stats_last(const ks_scene *scene, ks_render_stats *out)

@@ -25,11 +25,12 @@ import numpy as np
 LEVELS = 16
 FEATS = 2
 N_SH = 16
-N_IN = LEVELS * FEATS + N_SH
+N_IN = LEVELS * FEATS + 2 * N_SH
 HIDDEN = 64
 LOBES = 8
-N_OUT = LOBES * 5
-LAYERS = [(64, 48), (64, 64), (64, 64), (64, 64), (48, 64)]  # (out, in); the last padded 40 -> 48
+SEL = LOBES * 5  # selection logit
+N_OUT = LOBES * 5 + 1
+LAYERS = [(64, 64), (64, 64), (64, 64), (64, 64), (48, 64)]  # (out, in); the last padded 41 -> 48
 MAX_KAPPA = 1e4
 MIN_LOG_KAPPA = -6.0
 PRIMES = (1, 2654435761, 805459861)
@@ -126,15 +127,15 @@ class Network:
         self.bmin = np.asarray(bound[:3], np.float32)
         self.bmax = np.asarray(bound[3:], np.float32)
 
-    def encode(self, pos, wo):
+    def encode(self, pos, wo, nrm):
         cs = corners(pos, self.bmin, self.bmax, self.res, self.table_size)
         feats = [np.einsum("nk,nkf->nf", w, self.grid[l][idx]) for l, (idx, w) in enumerate(cs)]
-        x0 = np.concatenate(feats + [sh16(unit(wo))], axis=1)
+        x0 = np.concatenate(feats + [sh16(unit(wo)), sh16(unit(nrm))], axis=1)
         return x0, cs
 
-    def forward(self, pos, wo, bf=False):
-        """Raw outputs (n, 40) and the per-layer inputs X_l kept for the backward pass."""
-        x, cs = self.encode(pos, wo)
+    def forward(self, pos, wo, nrm, bf=False):
+        """Raw outputs (n, 41) and the per-layer inputs X_l kept for the backward pass."""
+        x, cs = self.encode(pos, wo, nrm)
         rnd = bf16 if bf else (lambda a: a)
         xs = []
         for l, W in enumerate(self.W):
@@ -178,13 +179,33 @@ class Network:
             self.W = W
 
 
+def softplus(x):
+    return np.where(x > 20.0, x, np.log1p(np.exp(np.minimum(x, 20.0))))
+
+
+def sigmoid(x):
+    return 1.0 / (1.0 + np.exp(-x))
+
+
+LOG_KAPPA_HI = np.log(MAX_KAPPA)
+
+
+def log_kappa(z):
+    """Smooth clamp of the raw concentration output into (MIN_LOG_KAPPA, log MAX_KAPPA)."""
+    return MIN_LOG_KAPPA + softplus(z - MIN_LOG_KAPPA) - softplus(z - LOG_KAPPA_HI)
+
+
+def log_kappa_grad(z):
+    return sigmoid(z - MIN_LOG_KAPPA) - sigmoid(z - LOG_KAPPA_HI)
+
+
 def decode(o):
-    """Raw outputs (n, 40) -> mean directions (n, 8, 3), concentrations (n, 8), weights (n, 8)."""
-    o = np.asarray(o, np.float64).reshape(-1, LOBES, 5)
+    """Raw outputs (n, 41) -> mean directions (n, 8, 3), concentrations (n, 8), weights (n, 8)."""
+    o = np.asarray(o, np.float64).reshape(-1, N_OUT)[:, :SEL].reshape(-1, LOBES, 5)
     raw = o[:, :, :3]
     nrm = np.linalg.norm(raw, axis=2, keepdims=True)
     mu = np.where(nrm > 1e-20, raw / np.maximum(nrm, 1e-300), np.array([0.0, 0.0, 1.0]))
-    kappa = np.exp(np.clip(o[:, :, 3], MIN_LOG_KAPPA, np.log(MAX_KAPPA)))
+    kappa = np.minimum(np.exp(log_kappa(o[:, :, 3])), MAX_KAPPA)
     lg = o[:, :, 4] - o[:, :, 4].max(axis=1, keepdims=True)
     w = np.exp(lg)
     w /= w.sum(axis=1, keepdims=True)
@@ -203,32 +224,47 @@ def mixture_pdf(o, wi):
     return (w * vmf_eval(mu, kappa, unit(wi))).sum(axis=1)
 
 
-def loss_and_grad(o, wi, t):
-    """Per-row loss -t log q(wi) and its gradient w.r.t. the 40 raw outputs."""
-    o = np.asarray(o, np.float64).reshape(-1, LOBES, 5)
+def selection(o, alpha_max):
+    """Selection probability alpha = alpha_max * sigmoid(z) of the mixture against the BSDF."""
+    z = np.asarray(o, np.float64).reshape(-1, N_OUT)[:, SEL]
+    return alpha_max / (1.0 + np.exp(-z))
+
+
+def loss_and_grad(o, wi, t, p_bsdf=None, alpha_max=0.8):
+    """Per-row loss -t log m(wi), m = alpha q + (1 - alpha) p_bsdf (the combined proposal of
+    one-sample MIS), and the training gradient w.r.t. the 41 raw outputs: the mixture outputs
+    follow -t log q(wi), the selection logit follows -t log m with q held fixed."""
+    full = np.asarray(o, np.float64).reshape(-1, N_OUT)
+    n = len(full)
+    o = full[:, :SEL].reshape(-1, LOBES, 5)
     wi = unit(wi)
     t = np.asarray(t, np.float64)
-    mu, kappa, w = decode(o.reshape(-1, N_OUT))
+    pb = np.zeros(n) if p_bsdf is None else np.asarray(p_bsdf, np.float64)
+    mu, kappa, w = decode(full)
     v = vmf_eval(mu, kappa, wi)
     q = (w * v).sum(axis=1)
-    ok = (t > 0) & (q > 1e-30)
-    loss = np.where(ok, -t * np.log(np.where(ok, q, 1.0)), 0.0)
-    r = np.where(ok[:, None], w * v / np.where(ok, q, 1.0)[:, None], 0.0)
+    sg = 1.0 / (1.0 + np.exp(-full[:, SEL]))
+    alpha = alpha_max * sg
+    m = alpha * q + (1.0 - alpha) * pb
+    ok = (t > 0) & (q > 1e-30) & (m > 1e-30)
+    ms = np.where(ok, m, 1.0)
+    qs = np.where(ok, q, 1.0)
+    loss = np.where(ok, -t * np.log(ms), 0.0)
+    g_sel = np.where(ok, -t * (q - pb) / ms * alpha_max * sg * (1.0 - sg), 0.0)
+    r = np.where(ok[:, None], w * v / qs[:, None], 0.0)
     g = np.zeros_like(o)
     tt = np.where(ok, t, 0.0)[:, None]
     g[:, :, 4] = -tt * (r - np.where(ok[:, None], w, 0.0))
-    lk = o[:, :, 3]
-    inside = (lk > MIN_LOG_KAPPA) & (lk < np.log(MAX_KAPPA))
     cosd = np.einsum("nlk,nk->nl", mu, wi)
     with np.errstate(over="ignore"):
         dlog = 1.0 / kappa - 2.0 / np.expm1(2.0 * kappa) + (cosd - 1.0)
-    g[:, :, 3] = np.where(inside, -tt * r * dlog * kappa, 0.0)
+    g[:, :, 3] = -tt * r * dlog * kappa * log_kappa_grad(o[:, :, 3])
     raw = o[:, :, :3]
     nrm = np.linalg.norm(raw, axis=2, keepdims=True)
     gm = kappa[:, :, None] * wi[:, None, :]
     proj = (gm - (gm * mu).sum(axis=2, keepdims=True) * mu) / np.maximum(nrm, 1e-300)
     g[:, :, :3] = np.where(nrm > 1e-20, -(tt * r)[:, :, None] * proj, 0.0)
-    return loss, g.reshape(-1, N_OUT)
+    return loss, np.concatenate([g.reshape(n, SEL), g_sel[:, None]], axis=1)
 
 
 def adam(p, g, m, v, it, lr, b1=0.9, b2=0.999, eps=1e-8):
