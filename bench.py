@@ -13,6 +13,15 @@ queries) over the K timed steps, device time from CUDA events on the library's s
 ranks.  e2e = the same metric through the host-buffer C ABI (scene upload, GPU SBVH build,
 render, FP64 image download every step).
 
+time_to_relmse: the glossy scene behind an occluder (the same icosphere made glossy-heavy,
+roughness U[0.02,0.2], with an opaque slab between it and the sun) at 1920x1080, depth 12.  A
+2048-spp plain render with its own seed is the reference; plain and guided progressive renders
+(1 spp per pass, guide trained online: batches of 2^18 records, Adam lr 1e-2) run until the
+relative MSE (eps 1e-2, reduced in FP64 on the GPU after each pass, outside the timed region)
+reaches 1e-2.  The host CPU runs the same estimator on the same Sobol samples as the plain GPU
+render, so it reaches the same error at the same spp: its time is that spp count over its
+measured paths/s on the same frame.
+
 --impl reference runs the CPU implementation of the path on the host cores (the oracle's
 restatement of small_pt over the reference's own SBVH traversal), each step a bounded crop of the
 same frame.
@@ -43,6 +52,7 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--e2e-steps", type=int, default=None, help="steps of the end-to-end leg (default: --steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ttr", action="store_true", help="skip the time-to-relMSE leg")
     # reduced frames of the same scene, for profiling captures only (not a bench line)
     ap.add_argument("--spp", type=int, default=None)
     ap.add_argument("--res", type=int, default=None)
@@ -61,6 +71,112 @@ def dist_env():
 
 def make_generated(ks):
     return ks.Generated("icosphere", 0, level=8, sky=(2048, 1024), resolution=(W_RES, H_RES))
+
+
+TTR_W, TTR_H, TTR_TARGET, TTR_REF_SPP, TTR_MAX_SPP = 1920, 1080, 1e-2, 2048, 1024
+
+
+def time_to_relmse(ks, ctx, torch, with_cpu, guide_options=None, guide_params=None):
+    """Seconds (and spp) for plain and guided renders to reach relMSE 1e-2 on the glossy
+    occluded scene; the CPU estimate from the oracle's paths/s on the same frame."""
+    g = ks.Generated("icosphere", 0, level=8, sky=(2048, 1024), resolution=(TTR_W, TTR_H), roughness=(0.02, 0.2),
+                     occluder=True)
+    sc = ks.Scene(ctx, g.desc)
+    sc.build_bvh()
+    cam = ks.camera_perspective(g.camera_to_world, g.vfov, g.aspect)
+    n = TTR_W * TTR_H
+    acc = torch.zeros((n, 3), dtype=torch.float64, device="cuda")
+    wts = torch.zeros((n, 2), dtype=torch.float64, device="cuda")
+    pr = ks.SmallPTParams.make(render_width=TTR_W, render_height=TTR_H, spp=TTR_REF_SPP, bounces=BOUNCES,
+                               rng_seed=1000, spp_prog_interval=256)
+    t0 = time.perf_counter()
+    sc.render_device(cam, pr, acc.data_ptr(), wts.data_ptr())
+    torch.cuda.synchronize()
+    ref_s = time.perf_counter() - t0
+    w0, w1 = wts[:, 0], wts[:, 1]
+    w_sum = (w0 + w1).to(torch.int64).to(torch.float64)
+    w = torch.where(w_sum == 0, torch.zeros_like(w_sum), w0 / torch.clamp(w_sum, min=1))
+    fg = torch.where(w0[:, None] == 0, torch.zeros_like(acc), acc / torch.clamp(w0[:, None], min=1e-300))
+    ref = (w[:, None] * fg).contiguous()
+
+    def run(guide, max_passes=None):
+        acc.zero_()
+        wts.zero_()
+        torch.cuda.synchronize()
+        p = ks.SmallPTParams.make(render_width=TTR_W, render_height=TTR_H, spp=TTR_MAX_SPP, bounces=BOUNCES,
+                                  rng_seed=7, spp_prog_interval=1)
+        st = {"cb": 0.0, "hit": None, "last": None, "passes": []}
+        t_start = time.perf_counter()
+
+        def cb(spp):
+            t_in = time.perf_counter()
+            e = ctx.rel_mse_device(acc.data_ptr(), wts.data_ptr(), ref.data_ptr(), n, 1e-2)
+            render_s = (t_in - t_start) - st["cb"]
+            st["last"] = (spp, render_s, e)
+            st["passes"].append(render_s)
+            if e <= TTR_TARGET and st["hit"] is None:
+                st["hit"] = (spp, render_s, e)
+            st["cb"] += time.perf_counter() - t_in
+            return st["hit"] is not None or (max_passes is not None and spp >= max_passes)
+
+        opts = None
+        if guide is not None:
+            kw = dict(train_passes=1 << 20, train_batch=1 << 18, max_records=1 << 20)
+            kw.update(guide_options or {})
+            opts = ks.GuideRenderOptions.make(**kw)
+        sc.render_device_progress(cam, p, acc.data_ptr(), wts.data_ptr(), cb, guide=guide, options=opts)
+        s = sc.stats()
+        out = {"spp": None, "seconds": None, "last": {"spp": st["last"][0], "seconds": st["last"][1],
+                                                        "rel_mse": st["last"][2]}}
+        if st["hit"]:
+            out.update(spp=st["hit"][0], seconds=st["hit"][1], rel_mse=st["hit"][2])
+        # device time of the whole render call (it stops at the target), from the library's events
+        out["device_seconds"] = s.ms_total / 1e3
+        pt = [b - a for a, b in zip([0.0] + st["passes"][:-1], st["passes"])]
+        out["pass_seconds"] = {"first": pt[0] if pt else None, "median": statistics.median(pt) if pt else None}
+        out["mpaths_per_s"] = s.paths / (s.ms_total / 1e3) / 1e6 if s.ms_total > 0 else None
+        if guide is not None:
+            out.update(train_steps=s.guide_train_steps, records=s.guide_records,
+                       ms_guide_infer=s.ms_guide_infer, ms_guide_train=s.ms_guide_train, ms_total=s.ms_total)
+        return out
+
+    lo, hi = g.bound
+    bound = list(lo - 0.05) + list(hi + 0.05)
+    # untimed warm-up of both arms (first-call costs: allocations, module loading)
+    run(None, max_passes=2)
+    warm = ks.Guide(ctx, bound, seed=2, learning_rate=1e-2)
+    run(warm, max_passes=2)
+    warm.close()
+    plain = run(None)
+    gp = dict(seed=1, learning_rate=1e-2)
+    gp.update(guide_params or {})
+    guide = ks.Guide(ctx, bound, **gp)
+    guided = run(guide)
+    guide.close()
+    res = {"target_rel_mse": TTR_TARGET, "eps": 1e-2,
+           "workload": f"icosphere_l8 glossy (roughness U[0.02,0.2]) behind an occluder slab, {TTR_W}x{TTR_H}, "
+                       f"depth {BOUNCES}, 1 spp per pass",
+           "timing": "seconds: host wall clock of the render call up to the pass that reached the target, "
+                     "minus the time spent in the per-pass error evaluation; device_seconds: the library's "
+                     "CUDA-event time of the same render call",
+           "reference": {"spp": TTR_REF_SPP, "seed": 1000, "seconds": ref_s},
+           "plain": plain, "guided": guided}
+    if with_cpu and plain["spp"]:
+        threads = os.cpu_count() or 1
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle_lib
+        orc = oracle_lib.load()
+        osc = orc.scene(g.desc)
+        pc = ks.SmallPTParams.make(render_width=TTR_W, render_height=TTR_H, spp=1, bounces=BOUNCES, rng_seed=7)
+        t0 = time.perf_counter()
+        _, _, cnt = osc.render(cam, pc, threads=threads)
+        cpu_s = time.perf_counter() - t0
+        pps = n / cpu_s
+        res["cpu"] = {"seconds_est": plain["spp"] * n / pps, "spp": plain["spp"], "paths_per_s": pps,
+                      "cores": threads, "kind": "port",
+                      "sample": f"full {TTR_W}x{TTR_H} frame at 1 spp ({n} paths, {int(cnt[0]) + int(cnt[1])} rays)"}
+    sc.close()
+    return res
 
 
 def cpu_crop_params(ks, crop=CPU_CROP):
@@ -292,6 +408,10 @@ def main():
         cpu = {"value": r["rays"] / r["seconds"] / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "port",
                "sample": r["sample"] + "; oracle restatement of small_pt over the reference cuda/sbvh.cu traversal"}
 
+    ttr = None
+    if rank == 0 and world == 1 and not args.no_ttr:
+        ttr = time_to_relmse(ks, ctx, torch, not args.no_cpu_baseline)
+
     if rank == 0:
         line = {
             "metric": "Mrays/s (closest-hit + shadow queries), small_pt on the icosphere frame",
@@ -309,6 +429,7 @@ def main():
             "e2e": e2e,
             "gpu_launches": sum(s.kernel_launches for s in stats),
             "clocks": clk,
+            "time_to_relmse": ttr,
         }
         print(json.dumps(line), flush=True)
     scene.close()

@@ -305,6 +305,25 @@ typedef struct ks_guide_render_options {
 } ks_guide_render_options;
 
 void ks_guide_render_options_default(ks_guide_render_options *out);
+
+/* Progressive device render: after every pass of params->spp_prog_interval samples per pixel the
+ * stream is synchronised and progress(spp_done, user) is called with accum / weights up to date
+ * on the device; a nonzero return ends the render there.  guide may be NULL (plain small_pt) or a
+ * guide with its options (guided render).  No reference counterpart: it exists to time a render
+ * to a target error without copying images to the host. */
+typedef int (*ks_device_progress_fn)(int spp_done, void *user);
+ks_status ks_small_pt_render_device_progress(ks_scene *scene, const ks_camera_desc *camera,
+                                             const ks_small_pt_params *params, ks_guide *guide,
+                                             const ks_guide_render_options *options, ks_device_progress_fn progress,
+                                             void *user, double *accum_rgb_device, double *weights_device);
+
+/* Relative MSE of a device image against a device reference (n_pixels x 3 doubles): the image is
+ * composited like RenderTarget2::composite_and_save_to_exr (render_target.cpp:181-205, backdrop
+ * may be NULL = black), then mean over pixels and channels of (x - r)^2 / (r^2 + eps), reduced in
+ * FP64 on the GPU. */
+ks_status ks_image_rel_mse_device(ks_context *ctx, const double *accum_rgb_device, const double *weights_device,
+                                  const double *reference_rgb_device, uint32_t n_pixels, double eps,
+                                  const float backdrop[3], double *rel_mse);
 ks_status ks_small_pt_render_guided(ks_scene *scene, const ks_camera_desc *camera, const ks_small_pt_params *params,
                                     ks_guide *guide, const ks_guide_render_options *options, ks_progress_fn progress,
                                     void *user, double *accum_rgb, double *weights);

@@ -97,6 +97,16 @@ class Context:
         except Exception:
             pass
 
+    def rel_mse_device(self, accum_ptr: int, weights_ptr: int, ref_ptr: int, n_pixels: int, eps=1e-2,
+                       backdrop=None) -> float:
+        """ks_image_rel_mse_device on device buffers (raw pointers)."""
+        out = np.zeros(1, np.float64)
+        bd = None if backdrop is None else np.asarray(backdrop, np.float32)
+        self.check(lib.ks_image_rel_mse_device(self.handle, ctypes.c_void_p(accum_ptr), ctypes.c_void_p(weights_ptr),
+                                               ctypes.c_void_p(ref_ptr), n_pixels, eps, ptr(bd), ptr(out)),
+                   "ks_image_rel_mse_device")
+        return float(out[0])
+
     def sobol_points(self, full_w, full_h, spp, seed, x0, y0, nx, ny, s0, ns, nd) -> np.ndarray:
         out = np.empty((ny, nx, ns, nd, 3), dtype=np.float32)
         st = lib.ks_sobol_points(self.handle, full_w, full_h, spp, seed, x0, y0, nx, ny, s0, ns, nd, ptr(out))
@@ -200,6 +210,8 @@ _sig("ks_small_pt_render", [_vp, ctypes.POINTER(CameraDesc), ctypes.POINTER(Smal
                             _vp, _vp])
 _sig("ks_small_pt_render_device", [_vp, ctypes.POINTER(CameraDesc), ctypes.POINTER(SmallPTParams), _vp, _vp])
 _sig("ks_render_stats_last", [_vp, ctypes.POINTER(RenderStats)])
+DEVICE_PROGRESS_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_int, _vp)
+_sig("ks_image_rel_mse_device", [_vp, _vp, _vp, _vp, _u32, ctypes.c_double, _vp, _vp])
 
 
 def _arr(p, n, dtype):
@@ -373,6 +385,18 @@ class Scene:
                                                             ctypes.c_void_p(accum_ptr), ctypes.c_void_p(weights_ptr)),
                        "ks_small_pt_render_guided_device")
 
+    def render_device_progress(self, camera: CameraDesc, params: SmallPTParams, accum_ptr: int, weights_ptr: int,
+                               callback, guide=None, options=None):
+        """ks_small_pt_render_device_progress: callback(spp_done) after every pass; a true return
+        value stops the render."""
+        if guide is not None and options is None:
+            options = GuideRenderOptions.make()
+        cb = DEVICE_PROGRESS_FN(lambda spp, user: int(bool(callback(spp))))
+        self.ctx.check(lib.ks_small_pt_render_device_progress(
+            self.handle, ctypes.byref(camera), ctypes.byref(params), guide.handle if guide is not None else None,
+            ctypes.byref(options) if options is not None else None, cb, None, ctypes.c_void_p(accum_ptr),
+            ctypes.c_void_p(weights_ptr)), "ks_small_pt_render_device_progress")
+
     def render_device(self, camera: CameraDesc, params: SmallPTParams, accum_ptr: int, weights_ptr: int):
         self.ctx.check(lib.ks_small_pt_render_device(self.handle, ctypes.byref(camera), ctypes.byref(params),
                                                      ctypes.c_void_p(accum_ptr), ctypes.c_void_p(weights_ptr)),
@@ -440,6 +464,8 @@ _sig("ks_small_pt_render_guided", [_vp, ctypes.POINTER(CameraDesc), ctypes.POINT
                                    ctypes.POINTER(GuideRenderOptions), PROGRESS_FN, _vp, _vp, _vp])
 _sig("ks_small_pt_render_guided_device", [_vp, ctypes.POINTER(CameraDesc), ctypes.POINTER(SmallPTParams), _vp,
                                           ctypes.POINTER(GuideRenderOptions), _vp, _vp])
+_sig("ks_small_pt_render_device_progress", [_vp, ctypes.POINTER(CameraDesc), ctypes.POINTER(SmallPTParams), _vp,
+                                            _vp, DEVICE_PROGRESS_FN, _vp, _vp, _vp])
 
 
 def split_guide_weights(flat):

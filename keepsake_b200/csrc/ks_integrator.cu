@@ -636,6 +636,31 @@ __global__ void __launch_bounds__(128) k_shadow(SceneView sv, ShadowBuf sb, cons
     flush_counts(tc, work);
 }
 
+// Relative MSE of the composited image (RenderTarget2::composite_and_save_to_exr,
+// render_target.cpp:181-205) against a reference: sum over pixels and channels of
+// (x - r)^2 / (r^2 + eps), accumulated in FP64 (one atomic per warp).
+__global__ void k_rel_mse(const double *accum, const double *weights, const double *ref, uint32_t n, double eps,
+                          double b0, double b1, double b2, double *out)
+{
+    double acc = 0.0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double w0 = weights[2 * (size_t)i], w1 = weights[2 * (size_t)i + 1];
+        double w_sum = (double)(uint32_t)(w0 + w1);
+        double w = w_sum == 0.0 ? 0.0 : w0 / fmax(w_sum, 1.0);
+        const double bd[3] = {b0, b1, b2};
+        for (int c = 0; c < 3; ++c) {
+            double fg = w0 == 0.0 ? 0.0 : accum[3 * (size_t)i + c] / w0;
+            double x = (1.0 - w) * bd[c] + w * fg;
+            double r = ref[3 * (size_t)i + c];
+            acc += (x - r) * (x - r) / (r * r + eps);
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1)
+        acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0)
+        atomicAdd(out, acc);
+}
+
 } // namespace
 } // namespace ksb
 
@@ -666,7 +691,8 @@ struct GuideWork
 static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const ks_small_pt_params *in,
                              ks_progress_fn cb, void *user, double *d_accum, double *d_weights, double *h_accum,
                              double *h_weights, ks_guide *guide = nullptr,
-                             const ks_guide_render_options *gopt = nullptr)
+                             const ks_guide_render_options *gopt = nullptr, ks_device_progress_fn dcb = nullptr,
+                             void *duser = nullptr)
 {
     ks_context *ctx = scene->ctx;
     if (guide && guide_impl::context_of(guide) != ctx)
@@ -901,6 +927,11 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
             cudaEventElapsedTime(&ms, ev[0], ev[1]);
             stats.ms_guide_train += ms;
         }
+        if (err == cudaSuccess && dcb) {
+            err = cudaStreamSynchronize(st);
+            if (err == cudaSuccess && dcb(s0 + batch, duser) != 0)
+                break;
+        }
         if (err == cudaSuccess && cb && h_accum) {
             size_t na = (size_t)W * H * 3, nw = (size_t)W * H * 2;
             cb_acc.resize(na);
@@ -1028,6 +1059,45 @@ ks_status ks_small_pt_render_guided_device(ks_scene *scene, const ks_camera_desc
     KS_CUDA_TRY(scene->ctx, cudaSetDevice(scene->ctx->device));
     return render_impl(scene, camera, params, nullptr, nullptr, accum_rgb_device, weights_device, nullptr, nullptr,
                        guide, options);
+}
+
+ks_status ks_small_pt_render_device_progress(ks_scene *scene, const ks_camera_desc *camera,
+                                             const ks_small_pt_params *params, ks_guide *guide,
+                                             const ks_guide_render_options *options, ks_device_progress_fn progress,
+                                             void *user, double *accum_rgb_device, double *weights_device)
+{
+    if (!scene || !camera || !params || !progress || !accum_rgb_device || !weights_device || (guide && !options))
+        return fail(scene ? scene->ctx : nullptr, KS_ERR_INVALID_ARGUMENT,
+                    "ks_small_pt_render_device_progress: null argument");
+    KS_CUDA_TRY(scene->ctx, cudaSetDevice(scene->ctx->device));
+    return render_impl(scene, camera, params, nullptr, nullptr, accum_rgb_device, weights_device, nullptr, nullptr,
+                       guide, guide ? options : nullptr, progress, user);
+}
+
+ks_status ks_image_rel_mse_device(ks_context *ctx, const double *accum_rgb_device, const double *weights_device,
+                                  const double *reference_rgb_device, uint32_t n_pixels, double eps,
+                                  const float backdrop[3], double *rel_mse)
+{
+    if (!ctx || !accum_rgb_device || !weights_device || !reference_rgb_device || !rel_mse)
+        return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_image_rel_mse_device: null argument");
+    KS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    *rel_mse = 0.0;
+    if (n_pixels == 0)
+        return KS_OK;
+    DevBuf<double> sum;
+    KS_CUDA_TRY(ctx, sum.alloc(1));
+    KS_CUDA_TRY(ctx, cudaMemsetAsync(sum.ptr, 0, sizeof(double), ctx->stream));
+    const double b0 = backdrop ? backdrop[0] : 0.0, b1 = backdrop ? backdrop[1] : 0.0,
+                 b2 = backdrop ? backdrop[2] : 0.0;
+    unsigned grid = (unsigned)std::min<uint32_t>((n_pixels + 255) / 256, (uint32_t)ctx->sm_count * 8);
+    k_rel_mse<<<grid, 256, 0, ctx->stream>>>(accum_rgb_device, weights_device, reference_rgb_device, n_pixels, eps,
+                                             b0, b1, b2, sum.ptr);
+    KS_CUDA_TRY(ctx, cudaGetLastError());
+    double total = 0.0;
+    KS_CUDA_TRY(ctx, cudaMemcpyAsync(&total, sum.ptr, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    KS_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    *rel_mse = total / (3.0 * (double)n_pixels);
+    return KS_OK;
 }
 
 ks_status ks_render_stats_last(const ks_scene *scene, ks_render_stats *out)

@@ -151,3 +151,30 @@ def test_render_errors(ctx):
     with pytest.raises(ks.KsError) as e:
         s.render(cam, p)
     assert e.value.status == 1
+
+
+@pytest.mark.gpu
+def test_device_progress_and_rel_mse(ctx):
+    """ks_small_pt_render_device_progress stops where the callback asks; ks_image_rel_mse_device
+    equals the host composite + relMSE."""
+    import torch
+    import keepsake_b200 as ks
+    g, cam, _ = make_case(CASES["box_room"])
+    s = ks.Scene(ctx, g.desc)
+    s.build_bvh()
+    W, H = 64, 48
+    n = W * H
+    p = ks.SmallPTParams.make(render_width=W, render_height=H, spp=64, bounces=8, spp_prog_interval=4)
+    acc = torch.zeros((n, 3), dtype=torch.float64, device="cuda")
+    wts = torch.zeros((n, 2), dtype=torch.float64, device="cuda")
+    seen = []
+    s.render_device_progress(cam, p, acc.data_ptr(), wts.data_ptr(), lambda spp: seen.append(spp) or spp >= 12)
+    assert seen == [4, 8, 12]
+    assert float(wts[:, 0].sum() + wts[:, 1].sum()) == 12 * n
+    ref = composite(*s.render(cam, ks.SmallPTParams.make(render_width=W, render_height=H, spp=256, bounces=8,
+                                                         rng_seed=3)))
+    ref_d = torch.tensor(ref.reshape(-1, 3), dtype=torch.float64, device="cuda")
+    e_dev = ctx.rel_mse_device(acc.data_ptr(), wts.data_ptr(), ref_d.data_ptr(), n, 1e-2)
+    img = composite(acc.cpu().numpy().reshape(H, W, 3), wts.cpu().numpy().reshape(H, W, 2))
+    assert abs(e_dev - rel_mse(img, ref)) <= 1e-12 * max(1.0, rel_mse(img, ref))
+    s.close()
