@@ -10,6 +10,7 @@
 #ifndef KS_B200_H
 #define KS_B200_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -331,6 +332,26 @@ ks_status ks_small_pt_render_guided_device(ks_scene *scene, const ks_camera_desc
                                            const ks_small_pt_params *params, ks_guide *guide,
                                            const ks_guide_render_options *options, double *accum_rgb_device,
                                            double *weights_device);
+
+/* ---------------------------------------------------------------------------------------------
+ * TOML tasks: the configuration service of keepsake's test driver (ConfigService::parse +
+ * run_all_tasks, config.cpp:262-312; test/main.cpp:60-86) with the small_pt task registered as
+ * "small_pt" and "small_pt_b200" (same keys as small_pt.cpp:180-241, plus `emission` on a
+ * material).  Runs every [[task]] of config_text in order; asset paths are relative to
+ * asset_root_dir (NULL = current directory); outputs go to output_dir/<task_dir or task_N>/
+ * (config.toml and small_pt_spp<N>.pfm per spp interval).  Supported assets: [bsdf.X] of type
+ * principled_bsdf with constant fields, [material.X] {bsdf, emission}, [mesh_asset.X] of type
+ * "obj" (path), "inline" (geometry list) or "procedural" (kind box_room | icosphere).  Returns
+ * KS_ERR_PARSE, KS_ERR_IO or KS_ERR_UNSUPPORTED with a message in ks_config_last_error().
+ * C++ hosts can use the ConfigTask-shaped API of ks_b200_task.hpp instead.
+ * ------------------------------------------------------------------------------------------- */
+ks_status ks_config_run(const char *config_text, const char *asset_root_dir, const char *output_dir);
+/* Message of the last failing ks_config_run / ks_config_parse on this thread ("" if none). */
+const char *ks_config_last_error(void);
+/* Parses config_text without running anything: KS_OK or KS_ERR_PARSE (message with the line).
+ * The document, normalised (keys sorted, nested tables inline), is written to normalised
+ * (NUL-terminated, truncated to capacity; may be NULL) and its length to *length (may be NULL). */
+ks_status ks_config_parse(const char *config_text, char *normalised, size_t capacity, size_t *length);
 
 /* ---------------------------------------------------------------------------------------------
  * Procedural scenes: seeded synthetic inputs standing in for mesh-asset loading

@@ -549,3 +549,40 @@ class Guide:
             self.close()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------------------------------------
+# TOML tasks (ks_config_*)
+# ---------------------------------------------------------------------------------------------
+_sig("ks_config_run", [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p])
+_sig("ks_config_last_error", [], ctypes.c_char_p)
+_sig("ks_config_parse", [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)])
+
+
+def config_parse(text: str) -> str:
+    """Normalised form of a TOML task document (raises KsError with the line on errors)."""
+    n = ctypes.c_size_t()
+    st = lib.ks_config_parse(text.encode(), None, 0, ctypes.byref(n))
+    if st != KS_OK:
+        raise KsError(st, lib.ks_config_last_error().decode())
+    buf = ctypes.create_string_buffer(n.value + 1)
+    lib.ks_config_parse(text.encode(), buf, n.value + 1, None)
+    return buf.value.decode()
+
+
+def config_run(text: str, output_dir: str, asset_root: str = None):
+    """Runs every [[task]] of a TOML document (ks_config_run)."""
+    st = lib.ks_config_run(text.encode(), asset_root.encode() if asset_root else None, output_dir.encode())
+    if st != KS_OK:
+        raise KsError(st, lib.ks_config_last_error().decode())
+
+
+def read_pfm(path):
+    """RGB PFM file -> float32 array [H, W, 3] (top row first)."""
+    with open(path, "rb") as f:
+        magic = f.readline().strip()
+        w, h = (int(x) for x in f.readline().split())
+        scale = float(f.readline())
+        data = np.frombuffer(f.read(), dtype="<f4" if scale < 0 else ">f4")
+    assert magic == b"PF"
+    return data.reshape(h, w, 3)[::-1].astype(np.float32)

@@ -1,0 +1,933 @@
+// The TOML task boundary (include/ks_b200_task.hpp): keepsake's configuration service for the
+// small_pt path, running the GPU small_pt through the C ABI.
+//
+//   ConfigService / run_all_tasks      config.cpp:262-312 (task_dir, override, config.toml copy)
+//   asset tables                       ConfigurableTable::load, config.cpp:315-329 ("field.key")
+//   small_pt task                      small_pt.cpp:180-300
+//   create_scene / material lists      scene.cpp:345-365, mesh_asset.cpp:286-299
+//   create_principled_bsdf             principled_bsdf.cpp:707-733 (constant shader fields,
+//                                      shader_field.h:89-156)
+//   create_sky_light                   light.cpp:257-275
+//   create_camera / look_at            camera.cpp:12-31,172-205
+//   load_transform_field               config.cpp:204-260
+#include "../../include/ks_b200.h"
+#include "../../include/ks_b200_task.hpp"
+#include "procedural.h"
+#include "toml.h"
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <algorithm>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <sstream>
+#include <stdexcept>
+#include <vector>
+
+namespace fs = std::filesystem;
+using ksb::toml::Value;
+
+namespace ks_b200
+{
+
+namespace
+{
+
+struct StatusError : std::runtime_error
+{
+    ks_status status;
+    StatusError(ks_status s, const std::string &what) : std::runtime_error(what), status(s) {}
+};
+
+struct ParseError : std::runtime_error
+{
+    using std::runtime_error::runtime_error;
+};
+
+struct IoError : std::runtime_error
+{
+    using std::runtime_error::runtime_error;
+};
+
+// One geometry of a mesh asset (one MeshGeometry of a subscene).
+struct Geometry
+{
+    std::vector<float> vertices;
+    std::vector<uint32_t> indices;
+    int own_material = -1; // index into MeshAsset::materials (procedural assets)
+};
+
+struct MeshAsset
+{
+    std::vector<Geometry> geometries;
+    std::vector<ks_material_desc> materials; // procedural assets bring their own
+    std::vector<float> sky_map;              // procedural assets: their sky
+    ks_sky_desc sky{};
+};
+
+} // namespace
+
+struct ConfigServiceImpl
+{
+    ksb::toml::Table root;
+    fs::path asset_root = fs::current_path();
+    fs::path output_dir = fs::current_path();
+    std::map<std::string, ConfigTask> tasks;
+    std::map<std::string, std::shared_ptr<MeshAsset>> meshes;
+    std::map<std::string, ks_material_desc> materials;
+
+    const Value *find_asset(const std::string &path) const;
+    std::shared_ptr<MeshAsset> mesh_asset(const std::string &path);
+    ks_material_desc material(const std::string &path);
+};
+
+struct ConfigArgsInternal
+{
+    ConfigServiceImpl *service = nullptr;
+    const Value *node = nullptr;
+    std::shared_ptr<Value> owner; // keeps merged task tables alive
+    std::string where;
+};
+
+namespace
+{
+
+const Value &child(const ConfigArgsInternal &a, std::string_view key)
+{
+    if (!a.node || a.node->kind != Value::Kind::Table)
+        throw ParseError("config: '" + a.where + "' is not a table");
+    auto it = a.node->table->find(std::string(key));
+    if (it == a.node->table->end())
+        throw ParseError("config: missing key '" + std::string(key) + "' in '" + a.where + "'");
+    return it->second;
+}
+
+bool has(const ConfigArgsInternal &a, std::string_view key)
+{
+    return a.node && a.node->kind == Value::Kind::Table && a.node->table->count(std::string(key));
+}
+
+double as_number(const Value &v, const std::string &what)
+{
+    if (!v.is_number())
+        throw ParseError("config: '" + what + "' must be a number");
+    return v.number();
+}
+
+void vec_n(const Value &v, int n, float *out, const std::string &what)
+{
+    if (v.kind != Value::Kind::Array || (int)v.array->size() != n)
+        throw ParseError("config: '" + what + "' must be an array of " + std::to_string(n) + " numbers");
+    for (int i = 0; i < n; ++i)
+        out[i] = (float)as_number((*v.array)[i], what);
+}
+
+} // namespace
+
+// ---- ConfigArgs -----------------------------------------------------------------------------
+ConfigArgs::ConfigArgs(std::shared_ptr<ConfigArgsInternal> in) : internal(std::move(in)) {}
+
+ConfigArgs ConfigArgs::operator[](std::string_view key) const
+{
+    auto a = std::make_shared<ConfigArgsInternal>(*internal);
+    a->node = &child(*internal, key);
+    a->where = internal->where + "." + std::string(key);
+    return ConfigArgs(a);
+}
+
+ConfigArgs ConfigArgs::operator[](int index) const
+{
+    const Value *n = internal->node;
+    if (!n || n->kind != Value::Kind::Array || index < 0 || index >= (int)n->array->size())
+        throw ParseError("config: index " + std::to_string(index) + " out of range in '" + internal->where + "'");
+    auto a = std::make_shared<ConfigArgsInternal>(*internal);
+    a->node = &(*n->array)[index];
+    a->where = internal->where + "[" + std::to_string(index) + "]";
+    return ConfigArgs(a);
+}
+
+bool ConfigArgs::contains(std::string_view key) const { return has(*internal, key); }
+
+int ConfigArgs::array_size() const
+{
+    const Value *n = internal->node;
+    if (!n || n->kind != Value::Kind::Array)
+        throw ParseError("config: '" + internal->where + "' is not an array");
+    return (int)n->array->size();
+}
+
+int ConfigArgs::load_integer(std::string_view key) const
+{
+    const Value &v = child(*internal, key);
+    if (v.kind != Value::Kind::Integer)
+        throw ParseError("config: '" + std::string(key) + "' must be an integer");
+    return (int)v.integer;
+}
+int ConfigArgs::load_integer(std::string_view key, int d) const { return contains(key) ? load_integer(key) : d; }
+float ConfigArgs::load_float(std::string_view key) const
+{
+    return (float)as_number(child(*internal, key), std::string(key));
+}
+float ConfigArgs::load_float(std::string_view key, float d) const { return contains(key) ? load_float(key) : d; }
+bool ConfigArgs::load_bool(std::string_view key) const
+{
+    const Value &v = child(*internal, key);
+    if (v.kind != Value::Kind::Boolean)
+        throw ParseError("config: '" + std::string(key) + "' must be a boolean");
+    return v.boolean;
+}
+bool ConfigArgs::load_bool(std::string_view key, bool d) const { return contains(key) ? load_bool(key) : d; }
+std::string ConfigArgs::load_string(std::string_view key) const
+{
+    const Value &v = child(*internal, key);
+    if (v.kind != Value::Kind::String)
+        throw ParseError("config: '" + std::string(key) + "' must be a string");
+    return v.str;
+}
+std::string ConfigArgs::load_string(std::string_view key, std::string_view d) const
+{
+    return contains(key) ? load_string(key) : std::string(d);
+}
+std::string ConfigArgs::load_string(int index) const
+{
+    const Value &v = *(*this)[index].internal->node;
+    if (v.kind != Value::Kind::String)
+        throw ParseError("config: element " + std::to_string(index) + " of '" + internal->where + "' must be a string");
+    return v.str;
+}
+void ConfigArgs::load_vec3(std::string_view key, float out[3]) const
+{
+    vec_n(child(*internal, key), 3, out, std::string(key));
+}
+
+fs::path ConfigArgs::load_path(std::string_view key) const
+{
+    fs::path p = load_string(key);
+    return p.is_absolute() ? p : internal->service->asset_root / p;
+}
+
+namespace
+{
+
+void mat_mul(const double a[16], const double b[16], double out[16])
+{
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c) {
+            double s = 0.0;
+            for (int k = 0; k < 4; ++k)
+                s += a[4 * r + k] * b[4 * k + c];
+            out[4 * r + c] = s;
+        }
+}
+
+} // namespace
+
+void ConfigArgs::load_transform(std::string_view key, float out[16]) const
+{
+    ConfigArgs t = (*this)[key];
+    if (t.contains("matrix_rm") || t.contains("matrix_cm")) {
+        bool rm = t.contains("matrix_rm");
+        float m[16];
+        vec_n(child(*t.internal, rm ? "matrix_rm" : "matrix_cm"), 16, m, rm ? "matrix_rm" : "matrix_cm");
+        for (int r = 0; r < 4; ++r)
+            for (int c = 0; c < 4; ++c)
+                out[4 * r + c] = rm ? m[4 * r + c] : m[4 * c + r];
+        return;
+    }
+    float s[3] = {1, 1, 1}, tr[3] = {0, 0, 0};
+    if (t.contains("scale"))
+        t.load_vec3("scale", s);
+    if (t.contains("translation"))
+        t.load_vec3("translation", tr);
+    double R[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};
+    if (t.contains("rotation")) {
+        ConfigArgs r = t["rotation"];
+        if (r.contains("euler")) {
+            // XYZ Euler angles in degrees: R = Rx(a0) Ry(a1) Rz(a2)
+            float e[3];
+            r.load_vec3("euler", e);
+            double a[3];
+            for (int i = 0; i < 3; ++i)
+                a[i] = (double)(e[i] / 180.0f * 3.14159265358979323846f);
+            double Rx[16] = {1, 0, 0, 0, 0, std::cos(a[0]), -std::sin(a[0]), 0, 0, std::sin(a[0]), std::cos(a[0]), 0,
+                             0, 0, 0, 1};
+            double Ry[16] = {std::cos(a[1]), 0, std::sin(a[1]), 0, 0, 1, 0, 0, -std::sin(a[1]), 0, std::cos(a[1]), 0,
+                             0, 0, 0, 1};
+            double Rz[16] = {std::cos(a[2]), -std::sin(a[2]), 0, 0, std::sin(a[2]), std::cos(a[2]), 0, 0, 0, 0, 1, 0,
+                             0, 0, 0, 1};
+            double t1[16];
+            mat_mul(Rx, Ry, t1);
+            mat_mul(t1, Rz, R);
+        } else if (r.contains("quat")) {
+            float q[4];
+            vec_n(child(*r.internal, "quat"), 4, q, "quat");
+            double w = q[0], x = q[1], y = q[2], z = q[3];
+            double n = std::sqrt(w * w + x * x + y * y + z * z);
+            w /= n, x /= n, y /= n, z /= n;
+            double M[16] = {1 - 2 * (y * y + z * z), 2 * (x * y - w * z),     2 * (x * z + w * y),     0,
+                            2 * (x * y + w * z),     1 - 2 * (x * x + z * z), 2 * (y * z - w * x),     0,
+                            2 * (x * z - w * y),     2 * (y * z + w * x),     1 - 2 * (x * x + y * y), 0,
+                            0,                       0,                       0,                       1};
+            std::memcpy(R, M, sizeof(M));
+        } else {
+            throw ParseError("config: rotation must be given as (XYZ) euler angles or a quaternion");
+        }
+    }
+    // scale_rotate_translate (maths.h:863-879): T * R * S
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c) {
+            double v = R[4 * r + c] * (c < 3 ? s[c] : 1.0);
+            if (r < 3 && c == 3)
+                v = tr[r];
+            out[4 * r + c] = (float)v;
+        }
+}
+
+// ---- assets ---------------------------------------------------------------------------------
+const Value *ConfigServiceImpl::find_asset(const std::string &path) const
+{
+    size_t dot = path.find('.');
+    if (dot == std::string::npos)
+        return nullptr;
+    auto f = root.find(path.substr(0, dot));
+    if (f == root.end() || f->second.kind != Value::Kind::Table)
+        return nullptr;
+    auto k = f->second.table->find(path.substr(dot + 1));
+    return k == f->second.table->end() ? nullptr : &k->second;
+}
+
+namespace
+{
+
+ConfigArgs args_of(ConfigServiceImpl *svc, const Value *node, const std::string &where)
+{
+    auto a = std::make_shared<ConfigArgsInternal>();
+    a->service = svc;
+    a->node = node;
+    a->where = where;
+    return ConfigArgs(a);
+}
+
+// Wavefront OBJ: v lines and polygonal f lines (fan-triangulated; v, v/t, v//n, v/t/n and
+// negative indices); every o / g statement starts a new geometry.
+void load_obj(const fs::path &path, MeshAsset &out)
+{
+    std::ifstream f(path);
+    if (!f)
+        throw IoError("cannot open " + path.string());
+    std::vector<float> pos;
+    Geometry cur;
+    std::map<uint32_t, uint32_t> remap;
+    auto flush = [&]() {
+        if (!cur.indices.empty())
+            out.geometries.push_back(std::move(cur));
+        cur = Geometry();
+        remap.clear();
+    };
+    std::string line;
+    int ln = 0;
+    while (std::getline(f, line)) {
+        ++ln;
+        std::istringstream ss(line);
+        std::string tag;
+        ss >> tag;
+        if (tag == "v") {
+            float x, y, z;
+            if (!(ss >> x >> y >> z))
+                throw ParseError(path.string() + ":" + std::to_string(ln) + ": bad vertex");
+            pos.insert(pos.end(), {x, y, z});
+        } else if (tag == "o" || tag == "g") {
+            flush();
+        } else if (tag == "f") {
+            std::vector<uint32_t> poly;
+            std::string tok;
+            while (ss >> tok) {
+                long idx = std::strtol(tok.c_str(), nullptr, 10);
+                long nv = (long)pos.size() / 3;
+                long v = idx < 0 ? nv + idx : idx - 1;
+                if (idx == 0 || v < 0 || v >= nv)
+                    throw ParseError(path.string() + ":" + std::to_string(ln) + ": bad face index");
+                auto it = remap.find((uint32_t)v);
+                uint32_t local;
+                if (it == remap.end()) {
+                    local = (uint32_t)cur.vertices.size() / 3;
+                    cur.vertices.insert(cur.vertices.end(), {pos[3 * v], pos[3 * v + 1], pos[3 * v + 2]});
+                    remap[(uint32_t)v] = local;
+                } else {
+                    local = it->second;
+                }
+                poly.push_back(local);
+            }
+            for (size_t k = 2; k < poly.size(); ++k)
+                cur.indices.insert(cur.indices.end(), {poly[0], poly[k - 1], poly[k]});
+        }
+    }
+    flush();
+    if (out.geometries.empty())
+        throw ParseError(path.string() + ": no faces");
+}
+
+void flat_numbers(const Value &v, std::vector<double> &out, const std::string &what)
+{
+    if (v.kind == Value::Kind::Array) {
+        for (const Value &e : *v.array)
+            flat_numbers(e, out, what);
+    } else {
+        out.push_back(as_number(v, what));
+    }
+}
+
+} // namespace
+
+std::shared_ptr<MeshAsset> ConfigServiceImpl::mesh_asset(const std::string &path)
+{
+    auto it = meshes.find(path);
+    if (it != meshes.end())
+        return it->second;
+    const Value *node = find_asset(path);
+    if (!node || path.rfind("mesh_asset.", 0) != 0)
+        throw ParseError("config: unknown mesh asset '" + path + "'");
+    ConfigArgs a = args_of(this, node, path);
+    auto m = std::make_shared<MeshAsset>();
+    std::string type = a.load_string("type", a.contains("path") ? "obj" : "inline");
+    if (type == "procedural") {
+        // seeded synthetic scene (extension): kind "box_room" | "icosphere"
+        ksb::ProceduralOptions o;
+        o.level = a.load_integer("level", o.level);
+        if (a.contains("roughness")) {
+            float r[2];
+            vec_n(child(*a.internal, "roughness"), 2, r, "roughness");
+            o.roughness_min = r[0];
+            o.roughness_max = r[1];
+        }
+        o.occluder = a.load_bool("occluder", false) ? 1 : 0;
+        if (a.contains("sky_resolution")) {
+            float r[2];
+            vec_n(child(*a.internal, "sky_resolution"), 2, r, "sky_resolution");
+            o.sky_width = (uint32_t)r[0];
+            o.sky_height = (uint32_t)r[1];
+        }
+        ksb::GeneratedScene g;
+        if (!ksb::generate_scene(a.load_string("kind"), (uint64_t)a.load_integer("seed", 0), o, g))
+            throw ParseError("config: unknown procedural kind in '" + path + "'");
+        for (auto &gm : g.meshes) {
+            Geometry geo;
+            geo.vertices = std::move(gm.vertices);
+            geo.indices = std::move(gm.indices);
+            geo.own_material = (int)gm.material;
+            m->geometries.push_back(std::move(geo));
+        }
+        m->materials = g.materials;
+        m->sky_map = std::move(g.sky_map);
+        m->sky = g.sky;
+        m->sky.map_rgb = nullptr;
+    } else if (type == "obj") {
+        load_obj(a.load_path("path"), *m);
+    } else if (type == "inline") {
+        // extension for small scenes written in the file: geometry = [{vertices = [...], indices = [...]}]
+        ConfigArgs list = a["geometry"];
+        for (int i = 0; i < list.array_size(); ++i) {
+            ConfigArgs gi = list[i];
+            std::vector<double> v, idx;
+            flat_numbers(child(*gi.internal, "vertices"), v, "vertices");
+            flat_numbers(child(*gi.internal, "indices"), idx, "indices");
+            if (v.size() % 3 || idx.size() % 3 || idx.empty())
+                throw ParseError("config: inline geometry needs 3 numbers per vertex and per triangle");
+            Geometry geo;
+            for (double x : v)
+                geo.vertices.push_back((float)x);
+            for (double x : idx) {
+                if (x < 0 || x >= (double)(v.size() / 3))
+                    throw ParseError("config: inline geometry index out of range");
+                geo.indices.push_back((uint32_t)x);
+            }
+            m->geometries.push_back(std::move(geo));
+        }
+    } else {
+        throw StatusError(KS_ERR_UNSUPPORTED, "config: mesh asset type '" + type + "' is not supported");
+    }
+    meshes[path] = m;
+    return m;
+}
+
+ks_material_desc ConfigServiceImpl::material(const std::string &path)
+{
+    auto it = materials.find(path);
+    if (it != materials.end())
+        return it->second;
+    const Value *node = find_asset(path);
+    if (!node || path.rfind("material.", 0) != 0)
+        throw ParseError("config: unknown material '" + path + "'");
+    ConfigArgs a = args_of(this, node, path);
+    std::string bsdf_path = a.load_string("bsdf");
+    const Value *bnode = find_asset(bsdf_path);
+    if (!bnode)
+        throw ParseError("config: unknown bsdf '" + bsdf_path + "'");
+    ConfigArgs b = args_of(this, bnode, bsdf_path);
+    std::string type = b.load_string("type");
+    if (type != "principled_bsdf")
+        throw StatusError(KS_ERR_UNSUPPORTED, "config: bsdf type '" + type + "' is not supported (principled_bsdf)");
+    if (a.contains("subsurface") || a.contains("normal_map"))
+        throw StatusError(KS_ERR_UNSUPPORTED, "config: subsurface and normal maps are not supported");
+    ks_material_desc d{};
+    // a constant shader field { type = "constant", value = ... } (or, as an extension, the bare value)
+    auto field = [&](const char *key, int n, float *out, const float *dflt) {
+        if (!b.contains(key)) {
+            std::memcpy(out, dflt, sizeof(float) * n);
+            return;
+        }
+        const Value &v = child(*b.internal, key);
+        const Value *val = &v;
+        if (v.kind == Value::Kind::Table) {
+            ConfigArgs f = b[key];
+            std::string ft = f.load_string("type");
+            if (ft != "constant")
+                throw StatusError(KS_ERR_UNSUPPORTED, std::string("config: shader field type '") + ft + "' of '" +
+                                                          key + "' is not supported");
+            val = &child(*f.internal, "value");
+        }
+        if (n == 1)
+            out[0] = (float)as_number(*val, key);
+        else
+            vec_n(*val, n, out, key);
+    };
+    const float c08[3] = {0.8f, 0.8f, 0.8f}, one = 1.0f, zero = 0.0f, ior = 1.5f, half = 0.5f, z3[3] = {0, 0, 0};
+    field("basecolor", 3, d.basecolor, c08);
+    field("roughness", 1, &d.roughness, &one);
+    field("metallic", 1, &d.metallic, &zero);
+    field("ior", 1, &d.ior, &ior);
+    field("specular_r0_mul", 1, &d.specular_r0_mul, &half);
+    field("specular_trans", 1, &d.specular_trans, &zero);
+    field("diffuse_trans", 1, &d.diffuse_trans, &zero);
+    field("diffuse_trans_fwd", 1, &d.diffuse_trans_fwd, &half);
+    field("emissive", 3, d.emissive, z3);
+    std::string mf = b.load_string("microfacet", "ggx");
+    d.microfacet = mf == "beckmann" ? 1 : 0;
+    if (a.contains("emission")) {
+        a.load_vec3("emission", d.emission);
+        d.has_emission = 1;
+    }
+    materials[path] = d;
+    return d;
+}
+
+// ---- small_pt task ---------------------------------------------------------------------------
+namespace
+{
+
+void check(ks_status s, ks_context *ctx, const char *what)
+{
+    if (s != KS_OK)
+        throw StatusError(s, std::string(what) + ": " + ks_status_string(s) + (ctx ? std::string(" (") +
+                                                                                     ks_last_error(ctx) + ")"
+                                                                               : std::string()));
+}
+
+// look_at (camera.cpp:12-31), float arithmetic
+void look_at(const float pos[3], const float target[3], float up[3], float m[16])
+{
+    float back[3] = {pos[0] - target[0], pos[1] - target[1], pos[2] - target[2]};
+    float bn = std::sqrt(back[0] * back[0] + back[1] * back[1] + back[2] * back[2]);
+    for (float &x : back)
+        x /= bn;
+    float right[3] = {up[1] * back[2] - up[2] * back[1], up[2] * back[0] - up[0] * back[2],
+                      up[0] * back[1] - up[1] * back[0]};
+    float rn2 = right[0] * right[0] + right[1] * right[1] + right[2] * right[2];
+    if (rn2 < 1e-8f) {
+        // orthonormal_basis (maths.h:814-821)
+        float sign = std::copysign(1.0f, back[2]);
+        const float a = -1.0f / (sign + back[2]);
+        const float b = back[0] * back[1] * a;
+        right[0] = 1.0f + sign * back[0] * back[0] * a;
+        right[1] = sign * b;
+        right[2] = -sign * back[0];
+        up[0] = b;
+        up[1] = sign + back[1] * back[1] * a;
+        up[2] = -back[1];
+    } else {
+        float rn = std::sqrt(rn2);
+        for (float &x : right)
+            x /= rn;
+        up[0] = back[1] * right[2] - back[2] * right[1];
+        up[1] = back[2] * right[0] - back[0] * right[2];
+        up[2] = back[0] * right[1] - back[1] * right[0];
+    }
+    const float mm[16] = {right[0], up[0], back[0], pos[0], right[1], up[1], back[1], pos[1],
+                          right[2], up[2], back[2], pos[2], 0.0f,     0.0f,  0.0f,    1.0f};
+    std::memcpy(m, mm, sizeof(mm));
+}
+
+// Portable float map (little-endian RGB, bottom row first).
+void write_pfm(const fs::path &path, int w, int h, const std::vector<float> &rgb)
+{
+    std::ofstream f(path, std::ios::binary);
+    if (!f)
+        throw IoError("cannot write " + path.string());
+    f << "PF\n" << w << " " << h << "\n-1.0\n";
+    for (int y = h - 1; y >= 0; --y)
+        f.write(reinterpret_cast<const char *>(rgb.data() + (size_t)y * w * 3), sizeof(float) * 3 * w);
+    if (!f)
+        throw IoError("cannot write " + path.string());
+}
+
+std::vector<float> read_pfm(const fs::path &path, uint32_t &w, uint32_t &h)
+{
+    std::ifstream f(path, std::ios::binary);
+    if (!f)
+        throw IoError("cannot open " + path.string());
+    std::string magic;
+    double scale;
+    f >> magic >> w >> h >> scale;
+    f.get();
+    if (magic != "PF" || !f || w == 0 || h == 0)
+        throw IoError(path.string() + ": not an RGB PFM file");
+    std::vector<float> top_first((size_t)w * h * 3), rows((size_t)w * h * 3);
+    f.read(reinterpret_cast<char *>(rows.data()), sizeof(float) * rows.size());
+    if (!f)
+        throw IoError(path.string() + ": truncated");
+    if (scale > 0.0)
+        for (float &v : rows) {
+            uint32_t u;
+            std::memcpy(&u, &v, 4);
+            u = __builtin_bswap32(u);
+            std::memcpy(&v, &u, 4);
+        }
+    for (uint32_t y = 0; y < h; ++y)
+        std::memcpy(&top_first[(size_t)y * w * 3], &rows[(size_t)(h - 1 - y) * w * 3], sizeof(float) * 3 * w);
+    return top_first;
+}
+
+struct TaskOutput
+{
+    fs::path dir;
+    int w, h;
+    float backdrop[3];
+};
+
+// RenderTarget2::composite_and_save_to_exr (render_target.cpp:181-205), written as PFM
+void save_interval(int spp, const double *accum, const double *weights, void *user)
+{
+    auto *o = static_cast<TaskOutput *>(user);
+    std::vector<float> rgb((size_t)o->w * o->h * 3);
+    for (size_t i = 0; i < (size_t)o->w * o->h; ++i) {
+        double w0 = weights[2 * i], w_sum = (double)(uint32_t)(weights[2 * i] + weights[2 * i + 1]);
+        double a = w_sum == 0.0 ? 0.0 : w0 / std::max(w_sum, 1.0);
+        for (int c = 0; c < 3; ++c) {
+            double fg = w0 == 0.0 ? 0.0 : accum[3 * i + c] / w0;
+            rgb[3 * i + c] = (float)((1.0 - a) * o->backdrop[c] + a * fg);
+        }
+    }
+    char name[64];
+    std::snprintf(name, sizeof(name), "small_pt_spp%d.pfm", spp);
+    write_pfm(o->dir / name, o->w, o->h, rgb);
+}
+
+struct ContextGuard
+{
+    ks_context *ctx = nullptr;
+    ks_scene *scene = nullptr;
+    ~ContextGuard()
+    {
+        if (scene)
+            ks_scene_destroy(scene);
+        if (ctx)
+            ks_context_destroy(ctx);
+    }
+};
+
+} // namespace
+
+void small_pt_b200(const ConfigArgs &args, const fs::path &task_dir, int task_id)
+{
+    (void)task_id;
+    ConfigServiceImpl *svc = args.internal->service;
+    // ---- scene (create_scene, scene.cpp:345-365) ----
+    if (args.contains("compound_object"))
+        throw StatusError(KS_ERR_UNSUPPORTED, "config: compound_object is not supported");
+    std::shared_ptr<MeshAsset> asset = svc->mesh_asset(args.load_string("object"));
+    std::vector<ks_material_desc> mats;
+    std::vector<uint32_t> geom_mat(asset->geometries.size());
+    if (args.contains("material")) {
+        // one list per subscene (one subscene per mesh asset), one material per geometry
+        ConfigArgs lists = args["material"];
+        if (lists.array_size() != 1 || lists[0].array_size() != (int)asset->geometries.size())
+            throw ParseError("config: material list mismatch dimension");
+        std::map<std::string, uint32_t> index;
+        for (int g = 0; g < (int)asset->geometries.size(); ++g) {
+            std::string name = lists[0].load_string(g);
+            auto it = index.find(name);
+            if (it == index.end()) {
+                it = index.emplace(name, (uint32_t)mats.size()).first;
+                mats.push_back(svc->material(name));
+            }
+            geom_mat[g] = it->second;
+        }
+    } else {
+        for (size_t g = 0; g < asset->geometries.size(); ++g) {
+            if (asset->geometries[g].own_material < 0)
+                throw ParseError("config: no materials; either load materials from file(s) or provide a material list");
+            geom_mat[g] = (uint32_t)asset->geometries[g].own_material;
+        }
+        mats = asset->materials;
+    }
+    std::vector<ks_mesh_desc> meshes(asset->geometries.size());
+    for (size_t g = 0; g < meshes.size(); ++g) {
+        const Geometry &geo = asset->geometries[g];
+        meshes[g] = ks_mesh_desc{geo.vertices.data(), (uint32_t)(geo.vertices.size() / 3), geo.indices.data(),
+                                 (uint32_t)(geo.indices.size() / 3), nullptr, geom_mat[g], 1, 1};
+    }
+    ks_scene_desc desc{};
+    desc.meshes = meshes.data();
+    desc.n_meshes = (uint32_t)meshes.size();
+    desc.materials = mats.data();
+    desc.n_materials = (uint32_t)mats.size();
+    // ---- sky (create_sky_light, light.cpp:257-275) ----
+    std::vector<float> sky_map;
+    if (args.contains("sky")) {
+        ConfigArgs s = args["sky"];
+        float id[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};
+        if (s.contains("ambient")) {
+            desc.sky.kind = 1;
+            s.load_vec3("ambient", desc.sky.ambient);
+            std::memcpy(desc.sky.to_world, id, sizeof(id));
+            desc.sky.transform_y_up = 1;
+            desc.sky.strength = 1.0f;
+        } else {
+            if (s.contains("procedural")) {
+                // extension: the sky generated with a procedural mesh asset
+                std::shared_ptr<MeshAsset> src = svc->mesh_asset(s.load_string("procedural"));
+                if (src->sky.kind != 2)
+                    throw ParseError("config: that procedural asset has no sky");
+                sky_map = src->sky_map;
+                desc.sky = src->sky;
+            } else {
+                fs::path p = s.load_path("map");
+                if (p.extension() != ".pfm")
+                    throw StatusError(KS_ERR_UNSUPPORTED, "config: sky maps are read from PFM files (" + p.string() +
+                                                              ")");
+                sky_map = read_pfm(p, desc.sky.width, desc.sky.height);
+                desc.sky.kind = 2;
+                std::memcpy(desc.sky.to_world, id, sizeof(id));
+            }
+            desc.sky.map_rgb = sky_map.data();
+            if (s.contains("to_world"))
+                s.load_transform("to_world", desc.sky.to_world);
+            desc.sky.transform_y_up = s.load_bool("transform_y_up", true) ? 1 : 0;
+            desc.sky.strength = s.load_float("strength", 1.0f);
+        }
+    }
+    if (args.contains("light"))
+        throw StatusError(KS_ERR_UNSUPPORTED, "config: point / directional lights are not supported");
+    if (args.contains("camera_animation"))
+        throw StatusError(KS_ERR_UNSUPPORTED, "config: camera_animation is not supported");
+    // ---- parameters (small_pt.cpp:224-241) ----
+    ks_small_pt_params p;
+    ks_small_pt_params_default(&p);
+    if (args.contains("backdrop")) {
+        args.load_vec3("backdrop", p.backdrop);
+        p.include_background = 0;
+    } else {
+        p.include_background = 1;
+    }
+    p.bounces = args.load_integer("bounces");
+    p.clamp_direct = args.load_float("clamp_direct", 0.0f);
+    p.clamp_indirect = args.load_float("clamp_indirect", 10.0f);
+    p.render_width = args.load_integer("render_width");
+    p.render_height = args.load_integer("render_height");
+    p.crop_start_x = args.load_integer("crop_start_x", 0);
+    p.crop_start_y = args.load_integer("crop_start_y", 0);
+    p.crop_width = args.load_integer("crop_width", 0);
+    p.crop_height = args.load_integer("crop_height", 0);
+    p.spp = args.load_integer("spp");
+    p.scale_ray_diff = args.load_bool("scale_ray_diff", true) ? 1 : 0;
+    p.rng_seed = args.load_integer("rng_seed", 0);
+    p.spp_prog_interval = args.load_integer("spp_prog_interval", 32);
+    if (args.contains("pixel_filter")) {
+        ConfigArgs f = args["pixel_filter"];
+        if (f.load_string("type") != "box")
+            throw StatusError(KS_ERR_UNSUPPORTED, "config: only the box pixel filter is supported");
+        p.pixel_filter_width = f.load_float("width", 1.0f);
+    }
+    // ---- camera (create_camera, camera.cpp:172-205) ----
+    ConfigArgs c = args["camera"];
+    float c2w[16];
+    if (c.contains("to_world")) {
+        c.load_transform("to_world", c2w);
+    } else {
+        float pos[3], target[3], up[3];
+        c.load_vec3("pos", pos);
+        c.load_vec3("target", target);
+        c.load_vec3("up", up);
+        look_at(pos, target, up, c2w);
+    }
+    if (c.load_string("type") != "perspective")
+        throw StatusError(KS_ERR_UNSUPPORTED, "config: only the perspective camera is supported");
+    float aspect = c.load_float("aspect");
+    float vfov;
+    if (c.contains("vfov"))
+        vfov = c.load_float("vfov") / 180.0f * 3.14159265358979323846f;
+    else
+        vfov = 2.0f * std::atan((1.0f / aspect) * std::tan(0.5f * (c.load_float("hfov") / 180.0f *
+                                                                    3.14159265358979323846f)));
+    ks_camera_desc cam;
+    check(ks_camera_perspective(c2w, vfov, aspect, &cam), nullptr, "camera");
+    // ---- render ----
+    int device = 0;
+    if (const char *e = std::getenv("KS_B200_DEVICE"))
+        device = std::atoi(e);
+    ContextGuard g;
+    check(ks_context_create(device, &g.ctx), nullptr, "ks_context_create");
+    check(ks_scene_create(g.ctx, &desc, &g.scene), g.ctx, "ks_scene_create");
+    check(ks_scene_build_bvh(g.scene, nullptr, nullptr), g.ctx, "ks_scene_build_bvh");
+    std::vector<double> accum((size_t)p.render_width * p.render_height * 3, 0.0);
+    std::vector<double> weights((size_t)p.render_width * p.render_height * 2, 0.0);
+    TaskOutput out{task_dir, p.render_width, p.render_height, {p.backdrop[0], p.backdrop[1], p.backdrop[2]}};
+    if (p.include_background)
+        out.backdrop[0] = out.backdrop[1] = out.backdrop[2] = 0.0f;
+    check(ks_small_pt_render(g.scene, &cam, &p, save_interval, &out, accum.data(), weights.data()), g.ctx,
+          "ks_small_pt_render");
+}
+
+// ---- ConfigService ----------------------------------------------------------------------------
+ConfigService::ConfigService() : impl(std::make_unique<ConfigServiceImpl>())
+{
+    register_task("small_pt", small_pt_b200);
+    register_task("small_pt_b200", small_pt_b200);
+}
+ConfigService::~ConfigService() = default;
+
+void ConfigService::parse_file(const fs::path &file_path)
+{
+    std::ifstream f(file_path);
+    if (!f)
+        throw IoError("cannot open " + file_path.string());
+    std::stringstream ss;
+    ss << f.rdbuf();
+    parse(ss.str());
+}
+
+void ConfigService::parse(std::string_view text) { impl->root = ksb::toml::parse(std::string(text)); }
+void ConfigService::set_asset_root_dir(const fs::path &root) { impl->asset_root = fs::absolute(root); }
+void ConfigService::set_output_directory(const fs::path &dir) { impl->output_dir = dir; }
+void ConfigService::register_task(std::string_view name, const ConfigTask &task) { impl->tasks[std::string(name)] = task; }
+fs::path ConfigService::output_directory() const { return impl->output_dir; }
+
+void ConfigService::run_all_tasks() const
+{
+    auto it = impl->root.find("task");
+    if (it == impl->root.end())
+        return;
+    if (it->second.kind != Value::Kind::Array)
+        throw ParseError("config: 'task' must be an array of tables");
+    const ksb::toml::Array &tasks = *it->second.array;
+    fs::create_directories(impl->output_dir);
+    for (int task_id = 0; task_id < (int)tasks.size(); ++task_id) {
+        if (tasks[task_id].kind != Value::Kind::Table)
+            throw ParseError("config: task " + std::to_string(task_id) + " is not a table");
+        auto merged = std::make_shared<Value>(ksb::toml::clone(tasks[task_id]));
+        ksb::toml::Table &tt = *merged->table;
+        if (tt.count("override")) {
+            const Value &o = tt.at("override");
+            if (o.kind != Value::Kind::Integer || o.integer < 0 || o.integer >= task_id)
+                throw ParseError("config: override must name an earlier task");
+            const Value &base = tasks[o.integer];
+            if (base.table->count("override"))
+                throw ParseError("config: an overridden task may not override another");
+            Value m = ksb::toml::clone(base);
+            for (const auto &[k, v] : tt)
+                if (k != "override")
+                    (*m.table)[k] = v;
+            merged = std::make_shared<Value>(m);
+        }
+        const ksb::toml::Table &task = *merged->table;
+        fs::path task_dir = task.count("task_dir") && task.at("task_dir").kind == Value::Kind::String
+                                ? fs::path(task.at("task_dir").str)
+                                : fs::path("task_" + std::to_string(task_id));
+        task_dir = impl->output_dir / task_dir;
+        fs::create_directories(task_dir);
+        {
+            std::ofstream w(task_dir / "config.toml");
+            w << ksb::toml::write(task) << std::endl;
+        }
+        if (!task.count("type") || task.at("type").kind != Value::Kind::String)
+            throw ParseError("config: task " + std::to_string(task_id) + " has no type");
+        auto f = impl->tasks.find(task.at("type").str);
+        if (f == impl->tasks.end())
+            throw StatusError(KS_ERR_UNSUPPORTED, "config: unknown task type '" + task.at("type").str + "'");
+        auto a = std::make_shared<ConfigArgsInternal>();
+        a->service = impl.get();
+        a->node = merged.get();
+        a->owner = merged;
+        a->where = "task[" + std::to_string(task_id) + "]";
+        f->second(ConfigArgs(a), task_dir, task_id);
+    }
+}
+
+} // namespace ks_b200
+
+// ---- C entry point --------------------------------------------------------------------------
+namespace
+{
+thread_local std::string g_config_error;
+}
+
+extern "C" {
+
+ks_status ks_config_run(const char *config_text, const char *asset_root_dir, const char *output_dir)
+{
+    g_config_error.clear();
+    if (!config_text || !output_dir) {
+        g_config_error = "ks_config_run: null argument";
+        return KS_ERR_INVALID_ARGUMENT;
+    }
+    try {
+        ks_b200::ConfigService svc;
+        svc.parse(config_text);
+        if (asset_root_dir)
+            svc.set_asset_root_dir(asset_root_dir);
+        svc.set_output_directory(output_dir);
+        svc.run_all_tasks();
+        return KS_OK;
+    } catch (const ks_b200::StatusError &e) {
+        g_config_error = e.what();
+        return e.status;
+    } catch (const ks_b200::IoError &e) {
+        g_config_error = e.what();
+        return KS_ERR_IO;
+    } catch (const std::filesystem::filesystem_error &e) {
+        g_config_error = e.what();
+        return KS_ERR_IO;
+    } catch (const std::exception &e) {
+        g_config_error = e.what();
+        return KS_ERR_PARSE;
+    }
+}
+
+const char *ks_config_last_error(void) { return g_config_error.c_str(); }
+
+ks_status ks_config_parse(const char *config_text, char *normalised, size_t capacity, size_t *length)
+{
+    g_config_error.clear();
+    if (!config_text) {
+        g_config_error = "ks_config_parse: null argument";
+        return KS_ERR_INVALID_ARGUMENT;
+    }
+    try {
+        std::string w = ksb::toml::write(ksb::toml::parse(config_text));
+        if (length)
+            *length = w.size();
+        if (normalised && capacity) {
+            size_t n = std::min(capacity - 1, w.size());
+            std::memcpy(normalised, w.data(), n);
+            normalised[n] = '\0';
+        }
+        return KS_OK;
+    } catch (const std::exception &e) {
+        g_config_error = e.what();
+        return KS_ERR_PARSE;
+    }
+}
+
+} // extern "C"
