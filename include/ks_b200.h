@@ -95,12 +95,32 @@ typedef struct ks_sky_desc {
     float strength;
 } ks_sky_desc;
 
+/* Instancing (Scene::subscenes / SubSceneInstance, scene.h:27-49): a prototype is a run of
+ * consecutive meshes (one SubScene); an instance places a prototype with an affine object-to-
+ * world transform (row-major 3x4; the inverse is computed in double).  Mesh lights of instanced
+ * prototypes are one light per (instance, emissive triangle), like Scene::build_mesh_lights
+ * (scene.cpp:315-336).  Meshes that belong to no prototype are not rendered. */
+typedef struct ks_prototype_desc {
+    uint32_t first_mesh;
+    uint32_t n_meshes;
+} ks_prototype_desc;
+
+typedef struct ks_instance_desc {
+    uint32_t prototype;
+    float to_world[12];
+} ks_instance_desc;
+
 typedef struct ks_scene_desc {
     const ks_mesh_desc *meshes;
     uint32_t n_meshes;
     const ks_material_desc *materials;
     uint32_t n_materials;
     ks_sky_desc sky;
+    /* n_instances = 0: every mesh, untransformed (one implicit identity instance) */
+    const ks_prototype_desc *prototypes;
+    uint32_t n_prototypes;
+    const ks_instance_desc *instances;
+    uint32_t n_instances;
 } ks_scene_desc;
 
 /* SBVHBuildOption (cuda/sbvh.cuh:9-16); clamped like SBVH::build (cuda/sbvh.cu:411-414). */
@@ -355,7 +375,8 @@ ks_status ks_config_parse(const char *config_text, char *normalised, size_t capa
 
 /* ---------------------------------------------------------------------------------------------
  * Procedural scenes: seeded synthetic inputs standing in for mesh-asset loading
- * (mesh_asset.cpp).  kind: "box_room" or "icosphere" (options apply to "icosphere").
+ * (mesh_asset.cpp).  kind: "box_room", "icosphere" or "instanced" (prototypes + instances; the
+ * scene description then carries prototypes and instances).
  * ------------------------------------------------------------------------------------------- */
 typedef struct ks_procedural_options {
     int32_t level;        /* icosphere subdivision level (8 -> 1,310,720 triangles) */
@@ -366,6 +387,12 @@ typedef struct ks_procedural_options {
     uint32_t sky_height;
     uint32_t width;       /* render resolution (sets the camera aspect) */
     uint32_t height;
+    /* "instanced": sphere prototypes, instances, geodesic frequency (20 f^2 triangles per
+     * prototype), emissive triangles; 0 = defaults 8, 400, 50, 64 */
+    uint32_t prototypes;
+    uint32_t instances;
+    uint32_t frequency;
+    uint32_t emitters;
 } ks_procedural_options;
 
 typedef struct ks_generated ks_generated;

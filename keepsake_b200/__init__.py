@@ -134,9 +134,19 @@ class SkyDesc(ctypes.Structure):
                 ("to_world", _f32 * 16), ("transform_y_up", _i32), ("strength", _f32)]
 
 
+class PrototypeDesc(ctypes.Structure):
+    _fields_ = [("first_mesh", _u32), ("n_meshes", _u32)]
+
+
+class InstanceDesc(ctypes.Structure):
+    _fields_ = [("prototype", _u32), ("to_world", _f32 * 12)]
+
+
 class SceneDesc(ctypes.Structure):
     _fields_ = [("meshes", ctypes.POINTER(MeshDesc)), ("n_meshes", _u32),
-                ("materials", ctypes.POINTER(MaterialDesc)), ("n_materials", _u32), ("sky", SkyDesc)]
+                ("materials", ctypes.POINTER(MaterialDesc)), ("n_materials", _u32), ("sky", SkyDesc),
+                ("prototypes", ctypes.POINTER(PrototypeDesc)), ("n_prototypes", _u32),
+                ("instances", ctypes.POINTER(InstanceDesc)), ("n_instances", _u32)]
 
 
 class SBVHOptions(ctypes.Structure):
@@ -149,7 +159,8 @@ class CameraDesc(ctypes.Structure):
 
 class ProceduralOptions(ctypes.Structure):
     _fields_ = [("level", _i32), ("roughness_min", _f32), ("roughness_max", _f32), ("occluder", _i32),
-                ("sky_width", _u32), ("sky_height", _u32), ("width", _u32), ("height", _u32)]
+                ("sky_width", _u32), ("sky_height", _u32), ("width", _u32), ("height", _u32),
+                ("prototypes", _u32), ("instances", _u32), ("frequency", _u32), ("emitters", _u32)]
 
 
 class SmallPTParams(ctypes.Structure):
@@ -227,9 +238,9 @@ class Generated:
     """A seeded procedural scene (ks_procedural_scene) with numpy views of its arrays."""
 
     def __init__(self, kind: str, seed: int = 0, level: int = 8, roughness=(0.05, 1.0), occluder=False,
-                 sky=(2048, 1024), resolution=(1024, 1024)):
+                 sky=(2048, 1024), resolution=(1024, 1024), prototypes=0, instances=0, frequency=0, emitters=0):
         o = ProceduralOptions(level, roughness[0], roughness[1], int(occluder), sky[0], sky[1],
-                              resolution[0], resolution[1])
+                              resolution[0], resolution[1], prototypes, instances, frequency, emitters)
         h = _vp()
         st = lib.ks_procedural_scene(kind.encode(), seed, ctypes.byref(o), ctypes.byref(h))
         if st != KS_OK:
@@ -250,6 +261,9 @@ class Generated:
         lib.ks_generated_camera(h, c2w, ctypes.byref(vfov), ctypes.byref(aspect))
         self.camera_to_world = np.array(c2w[:], dtype=np.float32)
         self.vfov, self.aspect = vfov.value, aspect.value
+        self.prototypes = [(d.prototypes[k].first_mesh, d.prototypes[k].n_meshes) for k in range(d.n_prototypes)]
+        self.instances = [(d.instances[k].prototype, np.array(d.instances[k].to_world[:], np.float32).reshape(3, 4))
+                          for k in range(d.n_instances)]
         self.sky_kind = d.sky.kind
         self.sky_map = (_arr(d.sky.map_rgb, 3 * d.sky.width * d.sky.height, np.float32)
                         .reshape(d.sky.height, d.sky.width, 3) if d.sky.kind == 2 else None)
@@ -263,12 +277,42 @@ class Generated:
             off += len(m["vertices"])
         return np.concatenate(vs).astype(np.float32), np.concatenate(ids).astype(np.uint32)
 
+    def flattened(self):
+        """Instanced scenes: every instance's meshes transformed to world space (float32, the
+        product's own arithmetic order), as a list of (vertices [V,3], indices [T,3], material)."""
+        if not self.instances:
+            return [(m["vertices"], m["indices"], m["material"]) for m in self.meshes]
+        out = []
+        for proto, xf in self.instances:
+            first, n = self.prototypes[proto]
+            for m in self.meshes[first:first + n]:
+                v = m["vertices"]
+                w = np.empty_like(v)
+                for r in range(3):
+                    w[:, r] = ((xf[r, 0] * v[:, 0] + xf[r, 1] * v[:, 1]) + xf[r, 2] * v[:, 2]) + xf[r, 3]
+                out.append((w, m["indices"], m["material"]))
+        return out
+
     @property
     def bound(self):
-        """Axis-aligned bound of all vertices: (min [3], max [3])."""
-        lo = np.min([m["vertices"].min(0) for m in self.meshes], axis=0)
-        hi = np.max([m["vertices"].max(0) for m in self.meshes], axis=0)
-        return lo, hi
+        """Axis-aligned bound of the scene in world space: (min [3], max [3]) (instances: the
+        transformed corners of each prototype's box)."""
+        if not self.instances:
+            lo = np.min([m["vertices"].min(0) for m in self.meshes], axis=0)
+            hi = np.max([m["vertices"].max(0) for m in self.meshes], axis=0)
+            return lo, hi
+        boxes = []
+        for first, n in self.prototypes:
+            v = np.concatenate([m["vertices"] for m in self.meshes[first:first + n]])
+            boxes.append((v.min(0), v.max(0)))
+        pts = []
+        for proto, xf in self.instances:
+            lo, hi = boxes[proto]
+            c = np.array([[(hi if k & 1 else lo)[0], (hi if k & 2 else lo)[1], (hi if k & 4 else lo)[2]]
+                          for k in range(8)], np.float64)
+            pts.append(c @ xf[:, :3].T.astype(np.float64) + xf[:, 3])
+        pts = np.concatenate(pts)
+        return pts.min(0).astype(np.float32), pts.max(0).astype(np.float32)
 
     @property
     def n_triangles(self):
@@ -284,6 +328,34 @@ class Generated:
             self.close()
         except Exception:
             pass
+
+
+def scene_desc(meshes, materials, sky=None):
+    """A SceneDesc over Python arrays: meshes = [(vertices [V,3], indices [T,3], material)],
+    materials = [MaterialDesc].  Returns (desc, keepalive)."""
+    keep = []
+    md = (MeshDesc * len(meshes))()
+    for k, (v, idx, mat) in enumerate(meshes):
+        v = np.ascontiguousarray(v, np.float32)
+        idx = np.ascontiguousarray(idx, np.uint32)
+        keep += [v, idx]
+        md[k].vertices = v.ctypes.data
+        md[k].n_vertices = len(v)
+        md[k].indices = idx.ctypes.data
+        md[k].n_triangles = len(idx)
+        md[k].material = mat
+        md[k].twosided = 1
+        md[k].use_smooth_normal = 1
+    mats = (MaterialDesc * len(materials))(*materials)
+    keep += [md, mats]
+    d = SceneDesc()
+    d.meshes = md
+    d.n_meshes = len(meshes)
+    d.materials = mats
+    d.n_materials = len(materials)
+    if sky is not None:
+        d.sky = sky
+    return d, keep
 
 
 def camera_perspective(camera_to_world, vfov, aspect) -> CameraDesc:

@@ -384,6 +384,8 @@ struct PathArgs
     const uint32_t *queue, *queue_count;
     const float4 *o_pdf, *d_info, *hits;
     const float4 *prim_tris; // 3 per SBVH primitive slot (vertices)
+    const uint32_t *hit_inst; // instanced scenes: instance of each hit (else null)
+    const float *inst_xf;     // 12 floats per instance
     float4 *lobes;
     uint32_t cap;
     float alpha_max;
@@ -420,7 +422,17 @@ __global__ void __launch_bounds__(kThreads, kPathCtasPerSm) k_guide_paths(PathAr
             wo = -normalize(d);
             const float4 *pt = a.prim_tris + 3 * (size_t)__float_as_uint(h4.w);
             float4 v0 = __ldg(pt), v1 = __ldg(pt + 1), v2 = __ldg(pt + 2);
-            nrm = facing_normal(mk(v0.x, v0.y, v0.z), mk(v1.x, v1.y, v1.z), mk(v2.x, v2.y, v2.z), wo);
+            f3 p0 = mk(v0.x, v0.y, v0.z), p1 = mk(v1.x, v1.y, v1.z), p2 = mk(v2.x, v2.y, v2.z);
+            if (a.inst_xf) {
+                float m[12];
+                const float *src = a.inst_xf + 12 * (size_t)a.hit_inst[i];
+                for (int e = 0; e < 12; ++e)
+                    m[e] = __ldg(&src[e]);
+                p0 = xf_point(m, p0);
+                p1 = xf_point(m, p1);
+                p2 = xf_point(m, p2);
+            }
+            nrm = facing_normal(p0, p1, p2, wo);
         }
         encode_row(a.gp, a.grid, valid, pn, wo, nrm, xb[0]);
         float o[kOut];
@@ -574,7 +586,8 @@ ks_status adam(ks_guide *g)
 ks_context *context_of(const ks_guide *g) { return g->ctx; }
 
 ks_status infer_paths(ks_guide *g, const uint32_t *queue, const uint32_t *queue_count, const float4 *o_pdf,
-                      const float4 *d_info, const float4 *hits, const float4 *prim_tris, float4 *lobes, uint32_t cap)
+                      const float4 *d_info, const float4 *hits, const float4 *prim_tris, const uint32_t *hit_inst,
+                      const float *inst_xf, float4 *lobes, uint32_t cap)
 {
     if (!g->packed) {
         ks_status s = pack(g);
@@ -591,6 +604,8 @@ ks_status infer_paths(ks_guide *g, const uint32_t *queue, const uint32_t *queue_
     a.d_info = d_info;
     a.hits = hits;
     a.prim_tris = prim_tris;
+    a.hit_inst = hit_inst;
+    a.inst_xf = inst_xf;
     a.lobes = lobes;
     a.cap = cap;
     a.alpha_max = g->params.alpha_max;

@@ -198,16 +198,6 @@ KS_D f3 clamp_contrib(f3 v, int bounce_for_direct, const RenderParams &rp, bool 
     return v;
 }
 
-KS_D TriVerts tri_verts(const SceneView &s, uint32_t tri)
-{
-    TriVerts tv;
-    uint32_t i0 = __ldg(&s.indices[3 * tri]), i1 = __ldg(&s.indices[3 * tri + 1]),
-             i2 = __ldg(&s.indices[3 * tri + 2]);
-    tv.v0 = mk(__ldg(&s.verts[3 * i0]), __ldg(&s.verts[3 * i0 + 1]), __ldg(&s.verts[3 * i0 + 2]));
-    tv.v1 = mk(__ldg(&s.verts[3 * i1]), __ldg(&s.verts[3 * i1 + 1]), __ldg(&s.verts[3 * i1 + 2]));
-    tv.v2 = mk(__ldg(&s.verts[3 * i2]), __ldg(&s.verts[3 * i2 + 1]), __ldg(&s.verts[3 * i2 + 2]));
-    return tv;
-}
 
 // ---- kernels --------------------------------------------------------------------------------
 
@@ -265,9 +255,11 @@ KS_D void flush_counts(const TravCount &c, unsigned long long *dst)
 }
 
 // Closest hit for every queued ray; the path index goes to the hit queue or the miss queue.
+// kInst: two-level traversal of an instanced scene; the instance of each hit goes to hit_inst.
+template <bool kInst>
 __global__ void __launch_bounds__(128) k_extend(SceneView sv, PathBuf pb, uint32_t count, float4 *hits,
-                                                uint32_t *hit_queue, uint32_t *miss_queue, uint32_t *queue_counts,
-                                                int *overflow, unsigned long long *work)
+                                                uint32_t *hit_inst, uint32_t *hit_queue, uint32_t *miss_queue,
+                                                uint32_t *queue_counts, int *overflow, unsigned long long *work)
 {
     TravCount tc;
     const uint32_t stride = gridDim.x * blockDim.x;
@@ -283,8 +275,14 @@ __global__ void __launch_bounds__(128) k_extend(SceneView sv, PathBuf pb, uint32
             q.tmax = kInf;
             Hit h;
             int of = 0;
-            traverse<false>(sv.nodes, sv.prim_tris, sv.root_ref, sv.root_count, sv.bmin, sv.bmax, q, 2, h, of,
-                            &tc);
+            if constexpr (kInst) {
+                uint32_t inst = 0;
+                traverse_instances<false>(sv.nodes, sv.prim_tris, sv.inst, q, 2, h, inst, of, &tc);
+                hit_inst[i] = inst;
+            } else {
+                traverse<false>(sv.nodes, sv.prim_tris, sv.root_ref, sv.root_count, sv.bmin, sv.bmax, q, 2, h, of,
+                                &tc);
+            }
             if (of)
                 atomicOr(overflow, 1);
             is_hit = h.tri != ~0u;
@@ -345,7 +343,8 @@ __global__ void __launch_bounds__(128) k_sample(RenderParams rp, PathBuf cur, co
 // the direction if both keep seeing the BSDF pdf.
 template <bool kMiss, bool kGuided>
 __global__ void __launch_bounds__(128) k_shade(SceneView sv, RenderParams rp, PathBuf cur, PathBuf nxt,
-                                               const float4 *hits, const float4 *samples, const uint32_t *queue,
+                                               const float4 *hits, const uint32_t *hit_inst,
+                                               const float4 *samples, const uint32_t *queue,
                                                const uint32_t *queue_count, uint32_t *next_count, ShadowBuf sb,
                                                uint32_t *shadow_count, double *accum, double *weights, GuideView gv)
 {
@@ -409,12 +408,26 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sv, RenderParams rp, Pa
                 float4 v0 = __ldg(pt), v1 = __ldg(pt + 1), v2 = __ldg(pt + 2);
                 uint32_t tri = bits(v0.w);
                 f3 p0 = mk(v0.x, v0.y, v0.z), p1 = mk(v1.x, v1.y, v1.z), p2 = mk(v2.x, v2.y, v2.z);
+                uint32_t inst = 0;
+                if (sv.inst.n) {
+                    // instanced: the hit triangle in world space (transform_it, ray.h:166-183)
+                    inst = hit_inst[i];
+                    float m[12];
+#pragma unroll
+                    for (int e = 0; e < 12; ++e)
+                        m[e] = __ldg(&sv.inst.xf[12 * (size_t)inst + e]);
+                    p0 = xf_point(m, p0);
+                    p1 = xf_point(m, p1);
+                    p2 = xf_point(m, p2);
+                }
                 uint32_t mesh = __ldg(&sv.tri_mesh[tri]);
                 const MaterialGPU &mat = sv.materials[__ldg(&sv.mesh_material[mesh])];
                 ShadeFrame it = make_frame(p0, p1, p2, h.y, h.z, rd, __ldg(&sv.mesh_twosided[mesh]) != 0);
                 // emitter hit (small_pt.cpp:112-138)
                 if (mat.has_emission && sv.tri_light) {
                     int32_t light = __ldg(&sv.tri_light[tri]);
+                    if (light >= 0 && sv.inst.n)
+                        light += __ldg(&sv.inst_light_base[inst]); // rank within the prototype
                     if (light >= 0) {
                         uint32_t k = (uint32_t)light - sv.n_nonmesh;
                         float4 e = __ldg(&sv.ml_emission[k]);
@@ -456,7 +469,14 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sv, RenderParams rp, Pa
                         Le_beta = sky_sample(sv, u0, u1, wi, wi_dist, pdf_wi_light);
                     } else {
                         uint32_t k = light - sv.n_nonmesh;
-                        TriVerts tv = tri_verts(sv, __ldg(&sv.ml_tri[k]));
+                        TriVerts tv{mk(0, 0, 0), mk(0, 0, 0), mk(0, 0, 0)};
+                        {
+                            const float4 *mv = sv.ml_verts + 3 * (size_t)k;
+                            float4 a0 = __ldg(mv), a1 = __ldg(mv + 1), a2 = __ldg(mv + 2);
+                            tv.v0 = mk(a0.x, a0.y, a0.z);
+                            tv.v1 = mk(a1.x, a1.y, a1.z);
+                            tv.v2 = mk(a2.x, a2.y, a2.z);
+                        }
                         Le_beta = mesh_light_sample(sv, k, tv, it.p, u0, u1, wi, wi_dist, pdf_wi_light);
                     }
                     if (!is_zero(Le_beta) && pdf_wi_light > 0.0f) {
@@ -596,6 +616,7 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sv, RenderParams rp, Pa
     }
 }
 
+template <bool kInst>
 __global__ void __launch_bounds__(128) k_shadow(SceneView sv, ShadowBuf sb, const uint32_t *shadow_count,
                                                 PathBuf nxt, double *accum, double *weights, int *overflow,
                                                 unsigned long long *work, GuideView gv)
@@ -611,8 +632,14 @@ __global__ void __launch_bounds__(128) k_shadow(SceneView sv, ShadowBuf sb, cons
         q.tmax = a.w;
         Hit h;
         int of = 0;
-        bool occ =
-            traverse<true>(sv.nodes, sv.prim_tris, sv.root_ref, sv.root_count, sv.bmin, sv.bmax, q, 2, h, of, &tc);
+        bool occ;
+        if constexpr (kInst) {
+            uint32_t inst = 0;
+            occ = traverse_instances<true>(sv.nodes, sv.prim_tris, sv.inst, q, 2, h, inst, of, &tc);
+        } else {
+            occ = traverse<true>(sv.nodes, sv.prim_tris, sv.root_ref, sv.root_count, sv.bmin, sv.bmax, q, 2, h, of,
+                                 &tc);
+        }
         if (of)
             atomicOr(overflow, 1);
         uint32_t target = bits(b.w);
@@ -670,6 +697,7 @@ struct RenderWork
 {
     DevBuf<float4> state[2][4];
     DevBuf<float4> hits;
+    DevBuf<uint32_t> hit_inst; // instanced scenes: instance of each hit
     DevBuf<float4> samples; // 2 per path slot
     DevBuf<float4> shadow[4];
     DevBuf<uint32_t> counters; // [next, shadow, hit queue, miss queue]
@@ -744,6 +772,8 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
         for (int f = 0; f < 4; ++f)
             KS_CUDA_TRY(ctx, w.state[b][f].alloc(w.capacity));
     KS_CUDA_TRY(ctx, w.hits.alloc(w.capacity));
+    if (scene->n_instances)
+        KS_CUDA_TRY(ctx, w.hit_inst.alloc(w.capacity));
     KS_CUDA_TRY(ctx, w.samples.alloc(2 * (size_t)w.capacity));
     KS_CUDA_TRY(ctx, w.queue[0].alloc(w.capacity));
     KS_CUDA_TRY(ctx, w.queue[1].alloc(w.capacity));
@@ -842,13 +872,17 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
             cudaMemsetAsync(w.counters.ptr, 0, sizeof(uint32_t) * 4, st);
             unsigned grid = std::min<unsigned>((count + 127) / 128, max_grid);
             cudaEventRecord(ev[1], st);
-            k_extend<<<grid, 128, 0, st>>>(sv, pb[cur], count, w.hits.ptr, w.queue[0].ptr, w.queue[1].ptr,
-                                           w.counters.ptr + 2, w.overflow.ptr, work.ptr);
+            if (scene->n_instances)
+                k_extend<true><<<grid, 128, 0, st>>>(sv, pb[cur], count, w.hits.ptr, w.hit_inst.ptr, w.queue[0].ptr,
+                                                     w.queue[1].ptr, w.counters.ptr + 2, w.overflow.ptr, work.ptr);
+            else
+                k_extend<false><<<grid, 128, 0, st>>>(sv, pb[cur], count, w.hits.ptr, nullptr, w.queue[0].ptr,
+                                                      w.queue[1].ptr, w.counters.ptr + 2, w.overflow.ptr, work.ptr);
             cudaEventRecord(ev[2], st);
             if (guide && gv.active) {
                 ks_status gs = guide_impl::infer_paths(guide, w.queue[0].ptr, w.counters.ptr + 2, pb[cur].o_pdf,
-                                                       pb[cur].d_info, w.hits.ptr, sv.prim_tris, gw.lobes.ptr,
-                                                       w.capacity);
+                                                       pb[cur].d_info, w.hits.ptr, sv.prim_tris, w.hit_inst.ptr,
+                                                       sv.inst.xf, gw.lobes.ptr, w.capacity);
                 if (gs != KS_OK) {
                     err = cudaErrorLaunchFailure;
                     break;
@@ -858,25 +892,29 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
             cudaEventRecord(ev[5], st);
             k_sample<<<grid, 128, 0, st>>>(rp, pb[cur], w.queue[0].ptr, w.counters.ptr + 2, w.samples.ptr);
             if (guide) {
-                k_shade<false, true><<<grid, 128, 0, st>>>(sv, rp, pb[cur], pb[1 - cur], w.hits.ptr, w.samples.ptr,
+                k_shade<false, true><<<grid, 128, 0, st>>>(sv, rp, pb[cur], pb[1 - cur], w.hits.ptr, w.hit_inst.ptr, w.samples.ptr,
                                                            w.queue[0].ptr, w.counters.ptr + 2, w.counters.ptr, sb,
                                                            w.counters.ptr + 1, d_accum, d_weights, gv);
-                k_shade<true, true><<<grid, 128, 0, st>>>(sv, rp, pb[cur], pb[1 - cur], w.hits.ptr, w.samples.ptr,
+                k_shade<true, true><<<grid, 128, 0, st>>>(sv, rp, pb[cur], pb[1 - cur], w.hits.ptr, w.hit_inst.ptr, w.samples.ptr,
                                                           w.queue[1].ptr, w.counters.ptr + 3, w.counters.ptr, sb,
                                                           w.counters.ptr + 1, d_accum, d_weights, gv);
             } else {
                 k_shade<false, false><<<grid, 128, 0, st>>>(sv, rp, pb[cur], pb[1 - cur], w.hits.ptr,
-                                                            w.samples.ptr, w.queue[0].ptr, w.counters.ptr + 2,
+                                                            w.hit_inst.ptr, w.samples.ptr, w.queue[0].ptr, w.counters.ptr + 2,
                                                             w.counters.ptr, sb, w.counters.ptr + 1, d_accum,
                                                             d_weights, gv);
                 k_shade<true, false><<<grid, 128, 0, st>>>(sv, rp, pb[cur], pb[1 - cur], w.hits.ptr,
-                                                           w.samples.ptr, w.queue[1].ptr, w.counters.ptr + 3,
+                                                           w.hit_inst.ptr, w.samples.ptr, w.queue[1].ptr, w.counters.ptr + 3,
                                                            w.counters.ptr, sb, w.counters.ptr + 1, d_accum,
                                                            d_weights, gv);
             }
             cudaEventRecord(ev[3], st);
-            k_shadow<<<grid, 128, 0, st>>>(sv, sb, w.counters.ptr + 1, pb[1 - cur], d_accum, d_weights,
-                                           w.overflow.ptr, work.ptr + 2, gv);
+            if (scene->n_instances)
+                k_shadow<true><<<grid, 128, 0, st>>>(sv, sb, w.counters.ptr + 1, pb[1 - cur], d_accum, d_weights,
+                                                     w.overflow.ptr, work.ptr + 2, gv);
+            else
+                k_shadow<false><<<grid, 128, 0, st>>>(sv, sb, w.counters.ptr + 1, pb[1 - cur], d_accum, d_weights,
+                                                      w.overflow.ptr, work.ptr + 2, gv);
             cudaEventRecord(ev[4], st);
             stats.kernel_launches += 5;
             cudaMemcpyAsync(h_counts, w.counters.ptr, sizeof(uint32_t) * 2, cudaMemcpyDeviceToHost, st);

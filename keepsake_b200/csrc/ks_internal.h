@@ -1,5 +1,6 @@
 // Internal host-side helpers shared by the C-ABI translation units.
 #pragma once
+#include <utility>
 #include "../../include/ks_b200.h"
 
 #include <cuda_runtime.h>
@@ -63,6 +64,11 @@ struct DevBuf
         count = 0;
     }
     size_t bytes() const { return count * sizeof(T); }
+    void swap(DevBuf &o)
+    {
+        std::swap(ptr, o.ptr);
+        std::swap(count, o.count);
+    }
 };
 
 } // namespace ksb

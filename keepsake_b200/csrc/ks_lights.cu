@@ -161,6 +161,24 @@ bool invert4(const float *m, float *out)
 SceneView make_view(const ks_scene *s)
 {
     SceneView v{};
+    v.inst.n = s->n_instances;
+    if (s->n_instances) {
+        v.inst.tlas = s->tlas_nodes.ptr;
+        v.inst.items = s->tlas_items.ptr;
+        v.inst.root_ref = s->tlas_root_ref;
+        v.inst.root_count = s->tlas_root_count;
+        v.inst.xf = s->inst_xf.ptr;
+        v.inst.inv = s->inst_inv.ptr;
+        v.inst.proto = s->inst_proto.ptr;
+        v.inst.proto_root = s->proto_root.ptr;
+        v.inst.proto_bound = s->proto_bound.ptr;
+        for (int k = 0; k < 3; ++k) {
+            v.inst.bmin[k] = s->scene_bound[k];
+            v.inst.bmax[k] = s->scene_bound[3 + k];
+        }
+    }
+    v.ml_verts = s->ml_verts.ptr;
+    v.inst_light_base = s->inst_light_base.ptr;
     v.nodes = s->trav_nodes.ptr;
     v.prim_tris = s->prim_tris.ptr;
     v.verts = s->verts.ptr;
@@ -293,7 +311,8 @@ ks_status build_lights(ks_scene *s)
     std::vector<uint32_t> h_idx;
     std::vector<uint32_t> ml_tri;
     std::vector<float> ml_area, ml_importance;
-    std::vector<float4> ml_em;
+    std::vector<float4> ml_em, ml_verts;
+    std::vector<int32_t> inst_light_base;
     bool any_emission = false;
     for (size_t m = 0; m + 1 < s->host.mesh_tri_offset.size(); ++m)
         if (s->host.materials[s->host.mesh_material[m]].has_emission)
@@ -309,9 +328,24 @@ ks_status build_lights(ks_scene *s)
             out[1] = h_verts[3 * v + 1];
             out[2] = h_verts[3 * v + 2];
         };
+        // instanced scenes: the emissive triangles of each prototype, in light order, then one light
+        // per (instance, triangle) with world-space vertices (Scene::build_mesh_lights, scene.cpp:315)
+        const bool instanced = s->n_instances > 0;
+        std::vector<std::vector<uint32_t>> proto_tris(s->n_protos);
+        std::vector<std::vector<float4>> proto_em(s->n_protos);
+        std::vector<int> mesh_proto(s->host.mesh_material.size(), -1);
+        if (instanced)
+            for (uint32_t q = 0; q < s->n_protos; ++q)
+                for (size_t m = 0; m + 1 < s->host.mesh_tri_offset.size(); ++m)
+                    if (s->host.mesh_tri_offset[m] >= s->host.proto_tri_begin[q] &&
+                        s->host.mesh_tri_offset[m + 1] <= s->host.proto_tri_end[q] &&
+                        s->host.mesh_tri_offset[m + 1] > s->host.mesh_tri_offset[m])
+                        mesh_proto[m] = (int)q;
         for (size_t m = 0; m + 1 < s->host.mesh_tri_offset.size(); ++m) {
             const ks_material_desc &mat = s->host.materials[s->host.mesh_material[m]];
             if (!mat.has_emission)
+                continue;
+            if (instanced && mesh_proto[m] < 0)
                 continue;
             float avg_importance = 0.212671f * mat.emission[0] + 0.715160f * mat.emission[1] +
                                    0.072169f * mat.emission[2];
@@ -344,10 +378,51 @@ ks_status build_lights(ks_scene *s)
                 }
             }
             for (uint32_t k = 0; k < N; ++k) {
+                if (instanced) {
+                    int q = mesh_proto[m];
+                    tri_light[first + prim_ids[k]] = (int32_t)proto_tris[q].size(); // rank in the prototype
+                    proto_tris[q].push_back(first + prim_ids[k]);
+                    proto_em[q].push_back(make_float4(mat.emission[0], mat.emission[1], mat.emission[2], 0.0f));
+                    continue;
+                }
                 ml_tri.push_back(first + prim_ids[k]);
                 ml_area.push_back(areas[k]);
                 ml_importance.push_back(importance[k]);
                 ml_em.push_back(make_float4(mat.emission[0], mat.emission[1], mat.emission[2], 0.0f));
+                float v0[3], v1[3], v2[3];
+                vert(h_idx[3 * (first + prim_ids[k])], v0);
+                vert(h_idx[3 * (first + prim_ids[k]) + 1], v1);
+                vert(h_idx[3 * (first + prim_ids[k]) + 2], v2);
+                ml_verts.push_back(make_float4(v0[0], v0[1], v0[2], 0.0f));
+                ml_verts.push_back(make_float4(v1[0], v1[1], v1[2], 0.0f));
+                ml_verts.push_back(make_float4(v2[0], v2[1], v2[2], 0.0f));
+            }
+        }
+        if (instanced) {
+            for (uint32_t i = 0; i < s->n_instances; ++i) {
+                inst_light_base.push_back((int32_t)(s->n_nonmesh + ml_tri.size()));
+                const uint32_t q = s->host.inst_proto[i];
+                const float *xf = &s->host.inst_xf[12 * (size_t)i];
+                for (size_t r = 0; r < proto_tris[q].size(); ++r) {
+                    uint32_t t = proto_tris[q][r];
+                    f3 w[3];
+                    for (int c = 0; c < 3; ++c) {
+                        float v[3];
+                        vert(h_idx[3 * (size_t)t + c], v);
+                        w[c] = xf_point(xf, mk(v[0], v[1], v[2]));
+                    }
+                    f3 e01 = w[1] - w[0], e12 = w[2] - w[1];
+                    f3 c = cross(e01, e12);
+                    float area = 0.5f * std::sqrt(c.x * c.x + c.y * c.y + c.z * c.z);
+                    float4 em = proto_em[q][r];
+                    float avg = 0.212671f * em.x + 0.715160f * em.y + 0.072169f * em.z;
+                    ml_tri.push_back(t);
+                    ml_area.push_back(area);
+                    ml_importance.push_back(6.28318530718f * area * avg);
+                    ml_em.push_back(em);
+                    for (int c2 = 0; c2 < 3; ++c2)
+                        ml_verts.push_back(make_float4(w[c2].x, w[c2].y, w[c2].z, 0.0f));
+                }
             }
         }
     }
@@ -361,7 +436,7 @@ ks_status build_lights(ks_scene *s)
     for (size_t k = 0; k < ml_tri.size(); ++k) {
         float pw = ml_importance[k];
         s->h_powers[flat] = (pw + pw + pw) / 3.0f;
-        if (any_emission)
+        if (any_emission && s->n_instances == 0)
             tri_light[ml_tri[k]] = (int32_t)flat;
         ++flat;
     }
@@ -386,6 +461,15 @@ ks_status build_lights(ks_scene *s)
                     cudaMemcpyAsync(s->ml_area.ptr, ml_area.data(), s->ml_area.bytes(), cudaMemcpyHostToDevice, st));
         KS_CUDA_TRY(ctx, cudaMemcpyAsync(s->ml_emission.ptr, ml_em.data(), s->ml_emission.bytes(),
                                          cudaMemcpyHostToDevice, st));
+        KS_CUDA_TRY(ctx, s->ml_verts.alloc(std::max<size_t>(ml_verts.size(), 3)));
+        if (!ml_verts.empty())
+            KS_CUDA_TRY(ctx, cudaMemcpyAsync(s->ml_verts.ptr, ml_verts.data(), sizeof(float4) * ml_verts.size(),
+                                             cudaMemcpyHostToDevice, st));
+        if (!inst_light_base.empty()) {
+            KS_CUDA_TRY(ctx, s->inst_light_base.alloc(inst_light_base.size()));
+            KS_CUDA_TRY(ctx, cudaMemcpyAsync(s->inst_light_base.ptr, inst_light_base.data(),
+                                             s->inst_light_base.bytes(), cudaMemcpyHostToDevice, st));
+        }
     }
     KS_CUDA_TRY(ctx, cudaStreamSynchronize(st));
     s->lights_built = true;

@@ -8,6 +8,7 @@
 #pragma once
 #include "ks_math.cuh"
 #include "ks_scene.h"
+#include "ks_traverse.cuh"
 
 namespace ksb
 {
@@ -15,6 +16,7 @@ namespace ksb
 // Flat, read-only view of everything the shading kernels read (passed by value).
 struct SceneView
 {
+    InstanceView inst; // instances (inst.n == 0: flat scene)
     const TravNode *nodes;
     const float4 *prim_tris;
     const float *verts;      // global vertex positions (3 floats each)
@@ -33,6 +35,8 @@ struct SceneView
     const uint32_t *ml_tri;   // per mesh-light triangle (flat index - n_nonmesh): global triangle
     const float *ml_area;
     const float4 *ml_emission;
+    const float4 *ml_verts;         // 3 per mesh-light triangle: world-space vertices
+    const int32_t *inst_light_base; // instanced scenes: flat light index of each instance's first mesh light
     // sky
     int sky_kind; // 0 none, 1 ambient, 2 map
     int sky_w, sky_h;

@@ -104,6 +104,19 @@ KS_HD float std_lerp(float a, float b, float t)
     const float x = a + t * (b - a);
     return (t > 1) == (b > a) ? (b < x ? x : b) : (x < b ? x : b);
 }
+// Affine transform of a point / direction by a row-major 3x4 matrix, the same float arithmetic on
+// host and device.
+KS_HD f3 xf_point(const float *m, f3 p)
+{
+    return mk(m[0] * p.x + m[1] * p.y + m[2] * p.z + m[3], m[4] * p.x + m[5] * p.y + m[6] * p.z + m[7],
+              m[8] * p.x + m[9] * p.y + m[10] * p.z + m[11]);
+}
+KS_HD f3 xf_dir(const float *m, f3 d)
+{
+    return mk(m[0] * d.x + m[1] * d.y + m[2] * d.z, m[4] * d.x + m[5] * d.y + m[6] * d.z,
+              m[8] * d.x + m[9] * d.y + m[10] * d.z);
+}
+
 // luminance() weights (maths.h:675-679)
 KS_HD float luminance(f3 c) { return 0.212671f * c.x + 0.715160f * c.y + 0.072169f * c.z; }
 KS_HD float fsign(float x) { return x > 0.0f ? 1.0f : (x < 0.0f ? -1.0f : 0.0f); }

@@ -181,7 +181,7 @@ KS_D int ref_destination(const BRef &r, const NodeInfo &n, uint32_t buckets)
 
 // ---- kernels --------------------------------------------------------------------------------
 
-__global__ void k_init_refs(const float *verts, const uint32_t *idx, uint32_t n_tris, BRef *refs)
+__global__ void k_init_refs(const float *verts, const uint32_t *idx, uint32_t tri_begin, uint32_t n_tris, BRef *refs)
 {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_tris)
@@ -189,14 +189,14 @@ __global__ void k_init_refs(const float *verts, const uint32_t *idx, uint32_t n_
     float b[6];
     box_empty(b);
     for (int v = 0; v < 3; ++v) {
-        uint32_t vi = idx[3 * i + v];
+        uint32_t vi = idx[3 * (tri_begin + i) + v];
         float p[6] = {verts[3 * vi], verts[3 * vi + 1], verts[3 * vi + 2], 0, 0, 0};
         p[3] = p[0];
         p[4] = p[1];
         p[5] = p[2];
         box_expand(b, p);
     }
-    refs[i].lo = make_float4(b[0], b[1], b[2], __uint_as_float(i));
+    refs[i].lo = make_float4(b[0], b[1], b[2], __uint_as_float(tri_begin + i));
     refs[i].hi = make_float4(b[3], b[4], b[5], 0.0f);
 }
 
@@ -854,26 +854,22 @@ inline unsigned grid_for(uint64_t n, unsigned block) { return (unsigned)((n + bl
 
 } // namespace
 
-ks_status build_sbvh(ks_scene *scene, const ks_sbvh_options &o, float *build_ms)
+// One SBVH over the triangles [tri_begin, tri_begin + n_tris) of the global arrays; primitive
+// references keep global triangle indices.
+struct RangeOut
 {
-    ks_context *ctx = scene->ctx;
-    cudaStream_t st = ctx->stream;
-    Params p;
-    // option clamps (cuda/sbvh.cu:411-414)
-    p.max_prims = std::min(o.max_prims_in_node, 8u);
-    p.buckets = std::min(o.bucket_count, 16u);
-    p.trav_weight = std::clamp(o.trav_weight, 0.0f, 10.0f);
-    p.alpha = std::clamp(o.alpha, 0.0f, 1.0f);
-    if (p.buckets < 2)
-        return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_build_bvh: bucket_count must be >= 2");
-    const uint32_t n_tris = scene->n_tris;
-    if (n_tris == 0)
-        return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_build_bvh: scene has no triangles");
+    DevBuf<RefNode> ref_nodes;
+    DevBuf<uint32_t> prims;
+    DevBuf<TravNode> trav;
+    DevBuf<float4> prim_tris;
+    uint32_t n_nodes = 0, n_prims = 0, n_trav = 0;
+    float bound[6] = {0, 0, 0, 0, 0, 0};
+};
 
-    cudaEvent_t ev0, ev1;
-    KS_CUDA_TRY(ctx, cudaEventCreate(&ev0));
-    KS_CUDA_TRY(ctx, cudaEventCreate(&ev1));
-    KS_CUDA_TRY(ctx, cudaEventRecord(ev0, st));
+static ks_status build_range(ks_context *ctx, const float *verts, const uint32_t *indices, uint32_t tri_begin,
+                             uint32_t n_tris, const Params &p, RangeOut &out)
+{
+    cudaStream_t st = ctx->stream;
 
     DevBuf<BRef> refs_a, refs_b;
     DevBuf<LevelNode> nodes_a, nodes_b;
@@ -891,7 +887,7 @@ ks_status build_sbvh(ks_scene *scene, const ks_sbvh_options &o, float *build_ms)
     KS_CUDA_TRY(ctx, recs.alloc(rec_cap));
     KS_CUDA_TRY(ctx, flag.alloc(1));
 
-    k_init_refs<<<grid_for(n_tris, 256), 256, 0, st>>>(scene->verts.ptr, scene->indices.ptr, n_tris, refs_a.ptr);
+    k_init_refs<<<grid_for(n_tris, 256), 256, 0, st>>>(verts, indices, tri_begin, n_tris, refs_a.ptr);
     LevelNode root{0, n_tris, 0, 0};
     KS_CUDA_TRY(ctx, nodes_a.alloc(1));
     KS_CUDA_TRY(ctx, cudaMemcpyAsync(nodes_a.ptr, &root, sizeof(root), cudaMemcpyHostToDevice, st));
@@ -1007,42 +1003,301 @@ ks_status build_sbvh(ks_scene *scene, const ks_sbvh_options &o, float *build_ms)
         uint32_t b = level_begin[l], e = level_begin[l + 1];
         k_dfs<<<grid_for(e - b, 256), 256, 0, st>>>(recs.ptr, b, e);
     }
-    KS_CUDA_TRY(ctx, scene->ref_nodes.alloc(n_nodes));
-    KS_CUDA_TRY(ctx, scene->prims.alloc(pool_used));
+    KS_CUDA_TRY(ctx, out.ref_nodes.alloc(n_nodes));
+    KS_CUDA_TRY(ctx, out.prims.alloc(pool_used));
     DevBuf<uint32_t> interior_flag, interior_scan;
     KS_CUDA_TRY(ctx, interior_flag.alloc(n_nodes));
     KS_CUDA_TRY(ctx, interior_scan.alloc(n_nodes + 1));
-    k_emit<<<grid_for(n_nodes, 256), 256, 0, st>>>(recs.ptr, n_nodes, pool.ptr, scene->ref_nodes.ptr, scene->prims.ptr,
+    k_emit<<<grid_for(n_nodes, 256), 256, 0, st>>>(recs.ptr, n_nodes, pool.ptr, out.ref_nodes.ptr, out.prims.ptr,
                                                    interior_flag.ptr);
     KS_CUDA_TRY(ctx, exclusive_scan(interior_flag.ptr, interior_scan.ptr, n_nodes, scan, st));
     uint32_t n_trav = 0;
     KS_CUDA_TRY(ctx, cudaMemcpyAsync(&n_trav, interior_scan.ptr + n_nodes, 4, cudaMemcpyDeviceToHost, st));
     KS_CUDA_TRY(ctx, cudaStreamSynchronize(st));
-    KS_CUDA_TRY(ctx, scene->trav_nodes.alloc(n_trav > 0 ? n_trav : 1));
-    k_trav<<<grid_for(n_nodes, 256), 256, 0, st>>>(recs.ptr, n_nodes, interior_scan.ptr, scene->trav_nodes.ptr);
-    KS_CUDA_TRY(ctx, scene->prim_tris.alloc((size_t)pool_used * 3));
-    k_prim_tris<<<grid_for(pool_used, 256), 256, 0, st>>>(scene->prims.ptr, pool_used, scene->verts.ptr,
-                                                          scene->indices.ptr, scene->prim_tris.ptr);
+    KS_CUDA_TRY(ctx, out.trav.alloc(n_trav > 0 ? n_trav : 1));
+    k_trav<<<grid_for(n_nodes, 256), 256, 0, st>>>(recs.ptr, n_nodes, interior_scan.ptr, out.trav.ptr);
+    KS_CUDA_TRY(ctx, out.prim_tris.alloc((size_t)pool_used * 3));
+    k_prim_tris<<<grid_for(pool_used, 256), 256, 0, st>>>(out.prims.ptr, pool_used, verts, indices,
+                                                          out.prim_tris.ptr);
     KS_CUDA_TRY(ctx, cudaGetLastError());
-    KS_CUDA_TRY(ctx, cudaEventRecord(ev1, st));
-    KS_CUDA_TRY(ctx, cudaEventSynchronize(ev1));
+    RefNode root_node;
+    KS_CUDA_TRY(ctx, cudaMemcpyAsync(&root_node, out.ref_nodes.ptr, sizeof(RefNode), cudaMemcpyDeviceToHost, st));
+    KS_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    for (int k = 0; k < 3; ++k) {
+        out.bound[k] = root_node.bmin[k];
+        out.bound[3 + k] = root_node.bmax[k];
+    }
+    out.n_nodes = n_nodes;
+    out.n_prims = pool_used;
+    out.n_trav = n_trav;
+    return KS_OK;
+}
+
+// BLAS concatenation: interior refs move by the node base, leaf refs by the slot base.
+__global__ void k_offset_trav(const TravNode *src, uint32_t n, uint32_t node_base, uint32_t slot_base, TravNode *dst)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    TravNode t = src[i];
+    t.d.x = (t.d.x & kLeafBit) ? (kLeafBit | ((t.d.x & ~kLeafBit) + slot_base)) : t.d.x + node_base;
+    t.d.y = (t.d.y & kLeafBit) ? (kLeafBit | ((t.d.y & ~kLeafBit) + slot_base)) : t.d.y + node_base;
+    dst[i] = t;
+}
+
+// ---- TLAS over instance boxes (host, binned SAH; leaves of at most 2 instances) ---------------
+struct InstBox
+{
+    float lo[3], hi[3], c[3];
+    uint32_t id;
+};
+
+struct TlasBuilder
+{
+    std::vector<InstBox> items;
+    std::vector<TravNode> nodes;
+
+    static void unite(float *lo, float *hi, const InstBox &b)
+    {
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = std::min(lo[k], b.lo[k]);
+            hi[k] = std::max(hi[k], b.hi[k]);
+        }
+    }
+    static float area(const float *lo, const float *hi)
+    {
+        float dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
+        return 2.0f * (dx * dy + dy * dz + dz * dx);
+    }
+    // returns (ref, count); box of the subtree in lo/hi
+    std::pair<uint32_t, uint32_t> build(uint32_t b, uint32_t e, float *lo, float *hi)
+    {
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = kInf;
+            hi[k] = -kInf;
+        }
+        for (uint32_t i = b; i < e; ++i)
+            unite(lo, hi, items[i]);
+        if (e - b <= 2)
+            return {kLeafBit | b, e - b};
+        float clo[3] = {kInf, kInf, kInf}, chi[3] = {-kInf, -kInf, -kInf};
+        for (uint32_t i = b; i < e; ++i)
+            for (int k = 0; k < 3; ++k) {
+                clo[k] = std::min(clo[k], items[i].c[k]);
+                chi[k] = std::max(chi[k], items[i].c[k]);
+            }
+        int axis = 0;
+        for (int k = 1; k < 3; ++k)
+            if (chi[k] - clo[k] > chi[axis] - clo[axis])
+                axis = k;
+        uint32_t mid = (b + e) / 2;
+        float ext = chi[axis] - clo[axis];
+        if (ext > 0.0f) {
+            constexpr int kBins = 12;
+            float blo[kBins][3], bhi[kBins][3];
+            uint32_t bcnt[kBins] = {};
+            for (int q = 0; q < kBins; ++q)
+                for (int k = 0; k < 3; ++k) {
+                    blo[q][k] = kInf;
+                    bhi[q][k] = -kInf;
+                }
+            auto bin_of = [&](const InstBox &x) {
+                int q = (int)((x.c[axis] - clo[axis]) / ext * kBins);
+                return std::min(std::max(q, 0), kBins - 1);
+            };
+            for (uint32_t i = b; i < e; ++i) {
+                int q = bin_of(items[i]);
+                ++bcnt[q];
+                unite(blo[q], bhi[q], items[i]);
+            }
+            float best = kInf;
+            int best_q = -1;
+            for (int q = 1; q < kBins; ++q) {
+                float llo[3] = {kInf, kInf, kInf}, lhi[3] = {-kInf, -kInf, -kInf};
+                float rlo[3] = {kInf, kInf, kInf}, rhi[3] = {-kInf, -kInf, -kInf};
+                uint32_t nl = 0, nr = 0;
+                for (int j = 0; j < kBins; ++j) {
+                    if (!bcnt[j])
+                        continue;
+                    float *L = j < q ? llo : rlo, *H = j < q ? lhi : rhi;
+                    for (int k = 0; k < 3; ++k) {
+                        L[k] = std::min(L[k], blo[j][k]);
+                        H[k] = std::max(H[k], bhi[j][k]);
+                    }
+                    (j < q ? nl : nr) += bcnt[j];
+                }
+                if (!nl || !nr)
+                    continue;
+                float cost = area(llo, lhi) * nl + area(rlo, rhi) * nr;
+                if (cost < best) {
+                    best = cost;
+                    best_q = q;
+                }
+            }
+            if (best_q > 0) {
+                auto it = std::partition(items.begin() + b, items.begin() + e,
+                                         [&](const InstBox &x) { return bin_of(x) < best_q; });
+                mid = (uint32_t)(it - items.begin());
+            }
+        }
+        if (mid == b || mid == e) {
+            mid = (b + e) / 2;
+            std::nth_element(items.begin() + b, items.begin() + mid, items.begin() + e,
+                             [&](const InstBox &x, const InstBox &y) { return x.c[axis] < y.c[axis]; });
+        }
+        uint32_t me = (uint32_t)nodes.size();
+        nodes.emplace_back();
+        float llo[3], lhi[3], rlo[3], rhi[3];
+        auto L = build(b, mid, llo, lhi);
+        auto R = build(mid, e, rlo, rhi);
+        TravNode &n = nodes[me];
+        n.a = make_float4(llo[0], llo[1], llo[2], lhi[0]);
+        n.b = make_float4(lhi[1], lhi[2], rlo[0], rlo[1]);
+        n.c = make_float4(rlo[2], rhi[0], rhi[1], rhi[2]);
+        n.d = make_uint4(L.first, R.first, L.second | ((uint32_t)axis << 30), R.second);
+        return {me, 0u};
+    }
+};
+
+static ks_status build_instanced(ks_scene *scene, const Params &p)
+{
+    ks_context *ctx = scene->ctx;
+    cudaStream_t st = ctx->stream;
+    const SceneHost &h = scene->host;
+    const uint32_t n_protos = scene->n_protos;
+    std::vector<RangeOut> blas(n_protos);
+    uint32_t total_trav = 0, total_slots = 0;
+    for (uint32_t q = 0; q < n_protos; ++q) {
+        uint32_t b = h.proto_tri_begin[q], n = h.proto_tri_end[q] - b;
+        ks_status s = build_range(ctx, scene->verts.ptr, scene->indices.ptr, b, n, p, blas[q]);
+        if (s != KS_OK)
+            return s;
+        total_trav += blas[q].n_trav;
+        total_slots += blas[q].n_prims;
+    }
+    KS_CUDA_TRY(ctx, scene->trav_nodes.alloc(total_trav > 0 ? total_trav : 1));
+    KS_CUDA_TRY(ctx, scene->prim_tris.alloc((size_t)total_slots * 3));
+    std::vector<uint4> roots(n_protos);
+    std::vector<float> pbound(6 * (size_t)n_protos);
+    uint32_t node_base = 0, slot_base = 0;
+    for (uint32_t q = 0; q < n_protos; ++q) {
+        const RangeOut &r = blas[q];
+        if (r.n_trav)
+            k_offset_trav<<<grid_for(r.n_trav, 256), 256, 0, st>>>(r.trav.ptr, r.n_trav, node_base, slot_base,
+                                                                  scene->trav_nodes.ptr + node_base);
+        KS_CUDA_TRY(ctx, cudaMemcpyAsync(scene->prim_tris.ptr + 3 * (size_t)slot_base, r.prim_tris.ptr,
+                                         sizeof(float4) * 3 * (size_t)r.n_prims, cudaMemcpyDeviceToDevice, st));
+        roots[q] = make_uint4(r.n_trav ? node_base : (kLeafBit | slot_base), r.n_prims, 0, 0);
+        std::memcpy(&pbound[6 * (size_t)q], r.bound, sizeof(r.bound));
+        node_base += r.n_trav;
+        slot_base += r.n_prims;
+    }
+    KS_CUDA_TRY(ctx, cudaGetLastError());
+    // instance boxes: the 8 corners of the prototype box, transformed, padded by a relative epsilon
+    TlasBuilder tb;
+    for (uint32_t i = 0; i < scene->n_instances; ++i) {
+        const float *xf = &h.inst_xf[12 * (size_t)i];
+        const float *pb = &pbound[6 * (size_t)h.inst_proto[i]];
+        InstBox ib{{kInf, kInf, kInf}, {-kInf, -kInf, -kInf}, {0, 0, 0}, i};
+        for (int c = 0; c < 8; ++c) {
+            f3 corner = mk(pb[(c & 1) ? 3 : 0], pb[(c & 2) ? 4 : 1], pb[(c & 4) ? 5 : 2]);
+            f3 w = xf_point(xf, corner);
+            float wv[3] = {w.x, w.y, w.z};
+            for (int k = 0; k < 3; ++k) {
+                ib.lo[k] = std::min(ib.lo[k], wv[k]);
+                ib.hi[k] = std::max(ib.hi[k], wv[k]);
+            }
+        }
+        for (int k = 0; k < 3; ++k) {
+            float pad = 1e-6f * (ib.hi[k] - ib.lo[k] + std::fabs(ib.lo[k]) + std::fabs(ib.hi[k])) + 1e-30f;
+            ib.lo[k] -= pad;
+            ib.hi[k] += pad;
+            ib.c[k] = 0.5f * (ib.lo[k] + ib.hi[k]);
+        }
+        tb.items.push_back(ib);
+    }
+    float lo[3], hi[3];
+    auto root = tb.build(0, (uint32_t)tb.items.size(), lo, hi);
+    std::vector<uint32_t> items(tb.items.size());
+    for (size_t k = 0; k < items.size(); ++k)
+        items[k] = tb.items[k].id;
+    KS_CUDA_TRY(ctx, scene->tlas_nodes.alloc(std::max<size_t>(tb.nodes.size(), 1)));
+    KS_CUDA_TRY(ctx, scene->tlas_items.alloc(items.size()));
+    KS_CUDA_TRY(ctx, scene->proto_root.alloc(n_protos));
+    KS_CUDA_TRY(ctx, scene->proto_bound.alloc(pbound.size()));
+    if (!tb.nodes.empty())
+        KS_CUDA_TRY(ctx, cudaMemcpyAsync(scene->tlas_nodes.ptr, tb.nodes.data(), sizeof(TravNode) * tb.nodes.size(),
+                                         cudaMemcpyHostToDevice, st));
+    KS_CUDA_TRY(ctx, cudaMemcpyAsync(scene->tlas_items.ptr, items.data(), sizeof(uint32_t) * items.size(),
+                                     cudaMemcpyHostToDevice, st));
+    KS_CUDA_TRY(ctx, cudaMemcpyAsync(scene->proto_root.ptr, roots.data(), sizeof(uint4) * roots.size(),
+                                     cudaMemcpyHostToDevice, st));
+    KS_CUDA_TRY(ctx, cudaMemcpyAsync(scene->proto_bound.ptr, pbound.data(), sizeof(float) * pbound.size(),
+                                     cudaMemcpyHostToDevice, st));
+    KS_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    scene->tlas_root_ref = root.first;
+    scene->tlas_root_count = root.second;
+    for (int k = 0; k < 3; ++k) {
+        scene->scene_bound[k] = lo[k];
+        scene->scene_bound[3 + k] = hi[k];
+    }
+    scene->ref_nodes.release();
+    scene->prims.release();
+    scene->n_nodes = 0;
+    scene->n_prims = total_slots;
+    scene->n_trav = total_trav;
+    scene->root_ref = 0;
+    scene->root_count = 0;
+    return KS_OK;
+}
+
+ks_status build_sbvh(ks_scene *scene, const ks_sbvh_options &o, float *build_ms)
+{
+    ks_context *ctx = scene->ctx;
+    cudaStream_t st = ctx->stream;
+    Params p;
+    // option clamps (cuda/sbvh.cu:411-414)
+    p.max_prims = std::min(o.max_prims_in_node, 8u);
+    p.buckets = std::min(o.bucket_count, 16u);
+    p.trav_weight = std::clamp(o.trav_weight, 0.0f, 10.0f);
+    p.alpha = std::clamp(o.alpha, 0.0f, 1.0f);
+    if (p.buckets < 2)
+        return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_build_bvh: bucket_count must be >= 2");
+    if (scene->n_tris == 0)
+        return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_build_bvh: scene has no triangles");
+    cudaEvent_t ev0, ev1;
+    KS_CUDA_TRY(ctx, cudaEventCreate(&ev0));
+    KS_CUDA_TRY(ctx, cudaEventCreate(&ev1));
+    KS_CUDA_TRY(ctx, cudaEventRecord(ev0, st));
+    ks_status s = KS_OK;
+    if (scene->n_instances > 0) {
+        s = build_instanced(scene, p);
+    } else {
+        RangeOut r;
+        s = build_range(ctx, scene->verts.ptr, scene->indices.ptr, 0, scene->n_tris, p, r);
+        if (s == KS_OK) {
+            scene->ref_nodes.swap(r.ref_nodes);
+            scene->prims.swap(r.prims);
+            scene->trav_nodes.swap(r.trav);
+            scene->prim_tris.swap(r.prim_tris);
+            std::memcpy(scene->scene_bound, r.bound, sizeof(r.bound));
+            scene->n_nodes = r.n_nodes;
+            scene->n_prims = r.n_prims;
+            scene->n_trav = r.n_trav;
+            scene->root_count = r.n_prims;
+            scene->root_ref = r.n_trav > 0 ? 0u : kLeafBit;
+        }
+    }
     float ms = 0;
+    cudaEventRecord(ev1, st);
+    cudaEventSynchronize(ev1);
     cudaEventElapsedTime(&ms, ev0, ev1);
     cudaEventDestroy(ev0);
     cudaEventDestroy(ev1);
+    if (s != KS_OK)
+        return s;
     if (build_ms)
         *build_ms = ms;
-    RefNode root_node;
-    KS_CUDA_TRY(ctx, cudaMemcpy(&root_node, scene->ref_nodes.ptr, sizeof(RefNode), cudaMemcpyDeviceToHost));
-    for (int k = 0; k < 3; ++k) {
-        scene->scene_bound[k] = root_node.bmin[k];
-        scene->scene_bound[3 + k] = root_node.bmax[k];
-    }
-    scene->n_nodes = n_nodes;
-    scene->n_prims = pool_used;
-    scene->n_trav = n_trav;
-    scene->root_count = pool_used;
-    scene->root_ref = n_trav > 0 ? 0u : kLeafBit;
     scene->bvh_built = true;
     return KS_OK;
 }

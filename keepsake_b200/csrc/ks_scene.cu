@@ -1,11 +1,19 @@
 // Scene lifetime, SBVH build/export entry points and the ray-query parity kernel.
+#include "ks_lights.cuh"
 #include "ks_scene.h"
 #include "ks_traverse.cuh"
+
+#include <cmath>
 
 #include <cstring>
 #include <new>
 
 using namespace ksb;
+
+namespace ksb
+{
+SceneView make_view(const ks_scene *s);
+}
 
 namespace
 {
@@ -13,7 +21,7 @@ namespace
 __global__ void trace_kernel(const TravNode *nodes, const float4 *tris, uint32_t root_ref, uint32_t root_count,
                              float bx0, float by0, float bz0, float bx1, float by1, float bz1, const float *rays,
                              uint32_t n, int any_hit, int culling, uint32_t *tri_out, float *t_out, float *bary_out,
-                             int *overflow_flag)
+                             int *overflow_flag, InstanceView iv)
 {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
@@ -27,11 +35,16 @@ __global__ void trace_kernel(const TravNode *nodes, const float4 *tris, uint32_t
     const float bmin[3] = {bx0, by0, bz0}, bmax[3] = {bx1, by1, bz1};
     Hit h;
     int overflow = 0;
+    uint32_t inst = 0;
     if (any_hit) {
-        bool occ = traverse<true>(nodes, tris, root_ref, root_count, bmin, bmax, q, culling, h, overflow);
+        bool occ = iv.n ? traverse_instances<true>(nodes, tris, iv, q, culling, h, inst, overflow)
+                        : traverse<true>(nodes, tris, root_ref, root_count, bmin, bmax, q, culling, h, overflow);
         tri_out[i] = occ ? 1u : 0u;
     } else {
-        traverse<false>(nodes, tris, root_ref, root_count, bmin, bmax, q, culling, h, overflow);
+        if (iv.n)
+            traverse_instances<false>(nodes, tris, iv, q, culling, h, inst, overflow);
+        else
+            traverse<false>(nodes, tris, root_ref, root_count, bmin, bmax, q, culling, h, overflow);
         tri_out[i] = h.tri;
         if (h.tri != ~0u) {
             t_out[i] = h.t;
@@ -60,6 +73,78 @@ bool valid_material(const ks_material_desc &m)
 } // namespace
 
 extern "C" {
+
+// Validates the prototypes and instances and keeps them on the host (with inverse transforms).
+static ks_status store_instances(ks_scene *s, const ks_scene_desc *desc)
+{
+    ks_context *ctx = s->ctx;
+    if (!desc->instances || !desc->prototypes || desc->n_prototypes == 0)
+        return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_create: instances need prototypes");
+    std::vector<int> owner(desc->n_meshes, -1);
+    for (uint32_t p = 0; p < desc->n_prototypes; ++p) {
+        const ks_prototype_desc &pd = desc->prototypes[p];
+        if (pd.n_meshes == 0 || (uint64_t)pd.first_mesh + pd.n_meshes > desc->n_meshes)
+            return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_create: prototype mesh range out of bounds");
+        for (uint32_t m = pd.first_mesh; m < pd.first_mesh + pd.n_meshes; ++m) {
+            if (owner[m] >= 0)
+                return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_create: prototypes overlap");
+            owner[m] = (int)p;
+        }
+        s->host.proto_tri_begin.push_back(s->host.mesh_tri_offset[pd.first_mesh]);
+        s->host.proto_tri_end.push_back(s->host.mesh_tri_offset[pd.first_mesh + pd.n_meshes]);
+    }
+    for (uint32_t i = 0; i < desc->n_instances; ++i) {
+        const ks_instance_desc &id = desc->instances[i];
+        if (id.prototype >= desc->n_prototypes)
+            return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_create: instance prototype out of range");
+        double m[3][4];
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 4; ++c) {
+                m[r][c] = id.to_world[4 * r + c];
+                if (!std::isfinite(m[r][c]))
+                    return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_create: non-finite instance transform");
+            }
+        // inverse of the affine map: [A t]^-1 = [A^-1, -A^-1 t]
+        double det = m[0][0] * (m[1][1] * m[2][2] - m[1][2] * m[2][1]) -
+                     m[0][1] * (m[1][0] * m[2][2] - m[1][2] * m[2][0]) +
+                     m[0][2] * (m[1][0] * m[2][1] - m[1][1] * m[2][0]);
+        if (!(std::fabs(det) > 1e-30))
+            return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_create: singular instance transform");
+        double inv[3][3];
+        inv[0][0] = (m[1][1] * m[2][2] - m[1][2] * m[2][1]) / det;
+        inv[0][1] = (m[0][2] * m[2][1] - m[0][1] * m[2][2]) / det;
+        inv[0][2] = (m[0][1] * m[1][2] - m[0][2] * m[1][1]) / det;
+        inv[1][0] = (m[1][2] * m[2][0] - m[1][0] * m[2][2]) / det;
+        inv[1][1] = (m[0][0] * m[2][2] - m[0][2] * m[2][0]) / det;
+        inv[1][2] = (m[0][2] * m[1][0] - m[0][0] * m[1][2]) / det;
+        inv[2][0] = (m[1][0] * m[2][1] - m[1][1] * m[2][0]) / det;
+        inv[2][1] = (m[0][1] * m[2][0] - m[0][0] * m[2][1]) / det;
+        inv[2][2] = (m[0][0] * m[1][1] - m[0][1] * m[1][0]) / det;
+        for (int r = 0; r < 3; ++r) {
+            double t = -(inv[r][0] * m[0][3] + inv[r][1] * m[1][3] + inv[r][2] * m[2][3]);
+            for (int c = 0; c < 3; ++c)
+                s->host.inst_inv.push_back((float)inv[r][c]);
+            s->host.inst_inv.push_back((float)t);
+        }
+        for (int k = 0; k < 12; ++k)
+            s->host.inst_xf.push_back(id.to_world[k]);
+        s->host.inst_proto.push_back(id.prototype);
+    }
+    s->n_instances = desc->n_instances;
+    s->n_protos = desc->n_prototypes;
+    cudaStream_t st = ctx->stream;
+    KS_CUDA_TRY(ctx, s->inst_xf.alloc(s->host.inst_xf.size()));
+    KS_CUDA_TRY(ctx, s->inst_inv.alloc(s->host.inst_inv.size()));
+    KS_CUDA_TRY(ctx, s->inst_proto.alloc(s->host.inst_proto.size()));
+    KS_CUDA_TRY(ctx, cudaMemcpyAsync(s->inst_xf.ptr, s->host.inst_xf.data(), s->inst_xf.bytes(),
+                                     cudaMemcpyHostToDevice, st));
+    KS_CUDA_TRY(ctx, cudaMemcpyAsync(s->inst_inv.ptr, s->host.inst_inv.data(), s->inst_inv.bytes(),
+                                     cudaMemcpyHostToDevice, st));
+    KS_CUDA_TRY(ctx, cudaMemcpyAsync(s->inst_proto.ptr, s->host.inst_proto.data(), s->inst_proto.bytes(),
+                                     cudaMemcpyHostToDevice, st));
+    KS_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    return KS_OK;
+}
 
 ks_status ks_scene_create(ks_context *ctx, const ks_scene_desc *desc, ks_scene **out)
 {
@@ -114,6 +199,14 @@ ks_status ks_scene_create(ks_context *ctx, const ks_scene_desc *desc, ks_scene *
     }
     s->host.mesh_tri_offset.push_back((uint32_t)to);
     s->host.materials.assign(desc->materials, desc->materials + desc->n_materials);
+    // instancing
+    if (desc->n_instances > 0) {
+        ks_status st = store_instances(s, desc);
+        if (st != KS_OK) {
+            delete s;
+            return st;
+        }
+    }
     // sky
     const ks_sky_desc &sd = desc->sky;
     if (sd.kind < 0 || sd.kind > 2 || (sd.kind == 2 && (!sd.map_rgb || sd.width == 0 || sd.height == 0))) {
@@ -224,6 +317,8 @@ ks_status ks_sbvh_export(const ks_scene *scene, float *node_bounds, uint32_t *no
     ks_context *ctx = scene->ctx;
     if (!scene->bvh_built)
         return fail(ctx, KS_ERR_NOT_BUILT, "ks_sbvh_export: call ks_scene_build_bvh first");
+    if (scene->n_instances)
+        return fail(ctx, KS_ERR_UNSUPPORTED, "ks_sbvh_export: instanced scenes have one SBVH per prototype");
     KS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
     std::vector<RefNode> nodes(scene->n_nodes);
     KS_CUDA_TRY(ctx, cudaMemcpy(nodes.data(), scene->ref_nodes.ptr, sizeof(RefNode) * nodes.size(),
@@ -272,7 +367,8 @@ ks_status ks_trace_rays(ks_scene *scene, const float *rays, uint32_t n, int any_
     const float *b = scene->scene_bound;
     trace_kernel<<<(n + 127) / 128, 128, 0, st>>>(scene->trav_nodes.ptr, scene->prim_tris.ptr, scene->root_ref,
                                                    scene->root_count, b[0], b[1], b[2], b[3], b[4], b[5], d_rays.ptr, n,
-                                                   any_hit, culling, d_tri.ptr, d_t.ptr, d_bary.ptr, d_flag.ptr);
+                                                   any_hit, culling, d_tri.ptr, d_t.ptr, d_bary.ptr, d_flag.ptr,
+                                                   make_view(scene).inst);
     KS_CUDA_TRY(ctx, cudaGetLastError());
     int overflow = 0;
     KS_CUDA_TRY(ctx, cudaMemcpyAsync(tri_idx, d_tri.ptr, d_tri.bytes(), cudaMemcpyDeviceToHost, st));

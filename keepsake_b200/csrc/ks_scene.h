@@ -46,7 +46,12 @@ struct SceneHost
     std::vector<uint32_t> mesh_material;
     std::vector<int> mesh_twosided;
     std::vector<ks_material_desc> materials;
+    // instancing (empty: flat scene)
+    std::vector<uint32_t> proto_tri_begin, proto_tri_end; // global triangle range of each prototype
+    std::vector<uint32_t> inst_proto;
+    std::vector<float> inst_xf, inst_inv; // 12 floats (row-major 3x4) per instance
 };
+
 
 } // namespace ksb
 
@@ -95,6 +100,17 @@ struct ks_scene
     ksb::DevBuf<uint32_t> sky_cond_guide, sky_margin_guide;
     int sky_w = 0, sky_h = 0;
     ks_render_stats last_stats{};
+    // instancing: per-prototype BLAS roots inside trav_nodes / prim_tris, a TLAS over instances
+    uint32_t n_instances = 0, n_protos = 0;
+    ksb::DevBuf<float> inst_xf, inst_inv;   // 12 floats per instance
+    ksb::DevBuf<uint32_t> inst_proto;
+    ksb::DevBuf<uint4> proto_root;          // (root ref, root count) per prototype
+    ksb::DevBuf<float> proto_bound;         // 6 floats per prototype
+    ksb::DevBuf<ksb::TravNode> tlas_nodes;
+    ksb::DevBuf<uint32_t> tlas_items;       // instance ids in TLAS leaf order
+    uint32_t tlas_root_ref = 0, tlas_root_count = 0;
+    ksb::DevBuf<int32_t> inst_light_base;   // per instance: flat index of its first mesh light
+    ksb::DevBuf<float4> ml_verts;           // 3 per mesh light: world-space vertices
 };
 
 namespace ksb

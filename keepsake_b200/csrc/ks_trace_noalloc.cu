@@ -96,6 +96,8 @@ extern "C" ks_status ks_trace_rays_noalloc(ks_scene *scene, const float *rays, u
                     "ks_trace_rays_noalloc: at most 65536 rays per call (static device buffer)");
     if (!scene->bvh_built)
         return fail(ctx, KS_ERR_NOT_BUILT, "ks_trace_rays_noalloc: call ks_scene_build_bvh first");
+    if (scene->n_instances)
+        return fail(ctx, KS_ERR_UNSUPPORTED, "ks_trace_rays_noalloc: instanced scenes use ks_trace_rays");
     if (n == 0)
         return KS_OK;
     if (ctx->device < 0 || ctx->device >= kMaxDevices)

@@ -298,4 +298,129 @@ KS_D bool traverse(const TravNode *__restrict__ nodes, const float4 *__restrict_
     return hit.tri != ~0u;
 }
 
+// ---- two-level traversal (instances) --------------------------------------------------------
+// The TLAS has the TravNode layout; its leaves list instance ids (items).  At an instance the ray
+// is carried into object space by the inverse transform without renormalising its direction, so
+// the hit distance t is the same in both spaces, and the prototype's BLAS is traversed with the
+// closest distance found so far as tmax.
+struct InstanceView
+{
+    uint32_t n;                  // instances; 0 = flat scene
+    const TravNode *tlas;
+    const uint32_t *items;
+    uint32_t root_ref, root_count;
+    float bmin[3], bmax[3];
+    const float *xf, *inv;       // 12 floats (row-major 3x4) per instance
+    const uint32_t *proto;       // prototype of each instance
+    const uint4 *proto_root;     // (root ref, root count) per prototype
+    const float *proto_bound;    // 6 floats per prototype
+};
+constexpr int kTlasStackDepth = 32;
+
+template <bool kAnyHit>
+KS_D bool traverse_instances(const TravNode *__restrict__ nodes, const float4 *__restrict__ tris,
+                             const InstanceView &iv, RayQuery ray, int culling, Hit &hit, uint32_t &inst,
+                             int &overflow, TravCount *count = nullptr)
+{
+    hit.tri = ~0u;
+    inst = 0;
+    const BoxHelper bh = make_box_helper(ray.d);
+    uint32_t st_ref[kTlasStackDepth];
+    uint32_t st_cnt[kTlasStackDepth];
+    float st_t[kTlasStackDepth];
+    int sp = 0;
+    float t0, t1;
+    if (!slab(ray, bh, iv.bmin, iv.bmax, t0, t1) || !(t0 < ray.tmax && t1 > ray.tmin))
+        return false;
+    uint32_t ref = iv.root_ref, cnt = iv.root_count;
+    while (true) {
+        if (ref & kLeafBit) {
+            uint32_t first = ref & ~kLeafBit;
+            for (uint32_t k = 0; k < cnt; ++k) {
+                const uint32_t id = __ldg(&iv.items[first + k]);
+                const float *m = iv.inv + 12 * (size_t)id;
+                float mi[12];
+#pragma unroll
+                for (int e = 0; e < 12; ++e)
+                    mi[e] = __ldg(&m[e]);
+                RayQuery q;
+                q.o = xf_point(mi, ray.o);
+                q.d = xf_dir(mi, ray.d);
+                q.tmin = ray.tmin;
+                q.tmax = ray.tmax;
+                const uint32_t pr = __ldg(&iv.proto[id]);
+                const uint4 r = __ldg(&iv.proto_root[pr]);
+                float pb[6];
+#pragma unroll
+                for (int e = 0; e < 6; ++e)
+                    pb[e] = __ldg(&iv.proto_bound[6 * (size_t)pr + e]);
+                Hit h;
+                if (traverse<kAnyHit>(nodes, tris, r.x, r.y, pb, pb + 3, q, culling, h, overflow, count)) {
+                    if (kAnyHit) {
+                        hit.tri = h.tri;
+                        inst = id;
+                        return true;
+                    }
+                    if (h.t < ray.tmax) {
+                        ray.tmax = h.t;
+                        hit = h;
+                        inst = id;
+                    }
+                }
+            }
+        } else {
+            const TravNode *n = iv.tlas + ref;
+            if (count)
+                count->nodes++;
+            float4 A = __ldg(&n->a), B = __ldg(&n->b), C = __ldg(&n->c);
+            uint4 D = __ldg(&n->d);
+            float lmin[3] = {A.x, A.y, A.z}, lmax[3] = {A.w, B.x, B.y};
+            float rmin[3] = {B.z, B.w, C.x}, rmax[3] = {C.y, C.z, C.w};
+            float lt0, lt1, rt0, rt1;
+            bool lok = slab(ray, bh, lmin, lmax, lt0, lt1) && lt1 > ray.tmin && lt0 < ray.tmax;
+            bool rok = slab(ray, bh, rmin, rmax, rt0, rt1) && rt1 > ray.tmin && rt0 < ray.tmax;
+            uint32_t axis = D.z >> 30;
+            uint32_t lcnt = D.z & 0x3fffffffu, rcnt = D.w;
+            bool right_first = bh.neg[axis] != 0;
+            uint32_t near_ref = right_first ? D.y : D.x, far_ref = right_first ? D.x : D.y;
+            uint32_t near_cnt = right_first ? rcnt : lcnt, far_cnt = right_first ? lcnt : rcnt;
+            bool near_ok = right_first ? rok : lok, far_ok = right_first ? lok : rok;
+            float far_t = right_first ? lt0 : rt0;
+            if (near_ok) {
+                if (far_ok) {
+                    if (sp >= kTlasStackDepth) {
+                        overflow = 1;
+                        return !kAnyHit && hit.tri != ~0u;
+                    }
+                    st_ref[sp] = far_ref;
+                    st_cnt[sp] = far_cnt;
+                    st_t[sp] = far_t;
+                    ++sp;
+                }
+                ref = near_ref;
+                cnt = near_cnt;
+                continue;
+            }
+            if (far_ok) {
+                ref = far_ref;
+                cnt = far_cnt;
+                continue;
+            }
+        }
+        bool found = false;
+        while (sp > 0) {
+            --sp;
+            if (st_t[sp] < ray.tmax) {
+                ref = st_ref[sp];
+                cnt = st_cnt[sp];
+                found = true;
+                break;
+            }
+        }
+        if (!found)
+            break;
+    }
+    return hit.tri != ~0u;
+}
+
 } // namespace ksb

@@ -121,8 +121,16 @@ ks_status ks_procedural_scene(const char *kind, uint64_t seed, const ks_procedur
             o.width = opts->width;
         if (opts->height)
             o.height = opts->height;
+        if (opts->prototypes)
+            o.prototypes = opts->prototypes;
+        if (opts->instances)
+            o.instances = opts->instances;
+        if (opts->frequency)
+            o.frequency = opts->frequency;
+        if (opts->emitters)
+            o.emitters = opts->emitters;
     }
-    if (o.level > 10)
+    if (o.level > 10 || o.frequency > 2000 || o.prototypes > 4096 || o.instances > (1u << 24))
         return KS_ERR_INVALID_ARGUMENT;
     auto *g = new (std::nothrow) ks_generated();
     if (!g)

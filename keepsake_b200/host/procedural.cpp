@@ -9,6 +9,12 @@
 //                1024-triangle patch (roughness U[r0,r1], metallic Bernoulli(0.3), basecolor
 //                U[0,1]^3); a procedural lat-long HDR sky (gradient + sun lobe of 1e4).
 //                options.occluder adds an opaque slab between the sphere and the sun.
+//   "instanced"  `prototypes` geodesic spheres of frequency f (20 f^2 triangles each, f = 50 gives
+//                50,000) with seeded fBm radial displacement (amplitude 0.05), one principled
+//                material each; `instances` instances under random affine transforms (rotation,
+//                anisotropic scale U[0.12,0.4], translation over a 16x16 field); `emitters`
+//                emissive triangles above the field with radiance log-uniform over 3 decades
+//                (one prototype, one identity instance); a ground quad; the sky of "icosphere".
 // All randomness comes from a SplitMix64 stream seeded by the caller.
 #include "procedural.h"
 
@@ -343,6 +349,149 @@ void gen_icosphere_scene(GeneratedScene &g, uint64_t seed, const ProceduralOptio
 
 } // namespace
 
+namespace
+{
+
+// Geodesic sphere: every icosahedron face split into f^2 triangles on a barycentric grid whose
+// points are normalised integer-weighted sums of the face corners (points on shared edges come out
+// identical from both faces, so the mesh is watertight).
+void geodesic(uint32_t f, std::vector<V3> &verts, std::vector<uint32_t> &tris)
+{
+    std::vector<V3> ico;
+    std::vector<uint32_t> faces;
+    icosphere(0, ico, faces);
+    verts.clear();
+    tris.clear();
+    for (size_t fi = 0; fi < faces.size(); fi += 3) {
+        V3 A = ico[faces[fi]], B = ico[faces[fi + 1]], C = ico[faces[fi + 2]];
+        uint32_t base = (uint32_t)verts.size();
+        auto id = [&](uint32_t i, uint32_t j) {
+            // row i has f + 1 - i points
+            return base + i * (f + 1) - i * (i - 1) / 2 + j;
+        };
+        for (uint32_t i = 0; i <= f; ++i)
+            for (uint32_t j = 0; i + j <= f; ++j) {
+                double wa = f - i - j, wb = i, wc = j;
+                V3 p = (wa * A + wb * B) + wc * C;
+                verts.push_back(norm(p));
+            }
+        for (uint32_t i = 0; i < f; ++i)
+            for (uint32_t j = 0; i + j < f; ++j) {
+                tris.insert(tris.end(), {id(i, j), id(i + 1, j), id(i, j + 1)});
+                if (i + j + 1 < f)
+                    tris.insert(tris.end(), {id(i + 1, j), id(i + 1, j + 1), id(i, j + 1)});
+            }
+    }
+}
+
+// Rotation about a unit axis (Rodrigues), row-major 3x3.
+void axis_angle(V3 a, double ang, double R[9])
+{
+    double c = std::cos(ang), s = std::sin(ang), t = 1.0 - c;
+    R[0] = t * a.x * a.x + c;
+    R[1] = t * a.x * a.y - s * a.z;
+    R[2] = t * a.x * a.z + s * a.y;
+    R[3] = t * a.x * a.y + s * a.z;
+    R[4] = t * a.y * a.y + c;
+    R[5] = t * a.y * a.z - s * a.x;
+    R[6] = t * a.x * a.z - s * a.y;
+    R[7] = t * a.y * a.z + s * a.x;
+    R[8] = t * a.z * a.z + c;
+}
+
+void gen_instanced_scene(GeneratedScene &g, uint64_t seed, const ProceduralOptions &o)
+{
+    SplitMix rng(seed);
+    const uint32_t f = std::max(1u, o.frequency), n_protos = std::max(1u, o.prototypes);
+    std::vector<V3> base_verts;
+    std::vector<uint32_t> base_tris;
+    geodesic(f, base_verts, base_tris);
+    // prototypes 0..n-1: displaced spheres, one mesh and one material each
+    for (uint32_t q = 0; q < n_protos; ++q) {
+        Noise3 noise(rng);
+        GeneratedMesh m;
+        V3 off{rng.uniform() * 50.0, rng.uniform() * 50.0, rng.uniform() * 50.0};
+        for (const V3 &v : base_verts) {
+            double d = noise.fbm(3.0 * v + off, 6);
+            V3 p = (1.0 + 0.05 * d) * v;
+            m.vertices.insert(m.vertices.end(), {(float)p.x, (float)p.y, (float)p.z});
+        }
+        m.indices = base_tris;
+        ks_material_desc mat = default_material();
+        mat.roughness = rng.uniform(0.05f, 1.0f);
+        mat.metallic = rng.uniform() < 0.3 ? 1.0f : 0.0f;
+        for (int c = 0; c < 3; ++c)
+            mat.basecolor[c] = rng.uniform(0.0f, 1.0f);
+        g.materials.push_back(mat);
+        m.material = (uint32_t)g.materials.size() - 1;
+        g.meshes.push_back(std::move(m));
+        g.prototypes.push_back(ks_prototype_desc{(uint32_t)g.meshes.size() - 1, 1});
+    }
+    // instances of the spheres
+    const double field = 8.0;
+    for (uint32_t i = 0; i < o.instances; ++i) {
+        ks_instance_desc inst{};
+        inst.prototype = i % n_protos;
+        V3 axis = norm(V3{rng.uniform() - 0.5, rng.uniform() - 0.5, rng.uniform() - 0.5});
+        double R[9];
+        axis_angle(axis, rng.uniform() * 6.283185307179586, R);
+        double sc[3];
+        for (double &x : sc)
+            x = 0.12 + 0.28 * rng.uniform();
+        double ty = 0.4 * std::max({sc[0], sc[1], sc[2]}) + 0.6 * rng.uniform() * sc[1];
+        double t[3] = {(2.0 * rng.uniform() - 1.0) * field, ty, (2.0 * rng.uniform() - 1.0) * field};
+        for (int r = 0; r < 3; ++r) {
+            for (int c = 0; c < 3; ++c)
+                inst.to_world[4 * r + c] = (float)(R[3 * r + c] * sc[c]);
+            inst.to_world[4 * r + 3] = (float)t[r];
+        }
+        g.instances.push_back(inst);
+    }
+    auto identity = [](uint32_t proto) {
+        ks_instance_desc d{};
+        d.prototype = proto;
+        d.to_world[0] = d.to_world[5] = d.to_world[10] = 1.0f;
+        return d;
+    };
+    // emitters: small triangles above the field, radiance log-uniform over 3 decades
+    if (o.emitters > 0) {
+        uint32_t first = (uint32_t)g.meshes.size();
+        for (uint32_t e = 0; e < o.emitters; ++e) {
+            V3 c{(2.0 * rng.uniform() - 1.0) * field, 2.5 + 1.5 * rng.uniform(), (2.0 * rng.uniform() - 1.0) * field};
+            double r = 0.08 + 0.1 * rng.uniform(), a0 = rng.uniform() * 6.283185307179586;
+            GeneratedMesh m;
+            for (int k = 0; k < 3; ++k) {
+                double a = a0 + k * 2.0943951023931953;
+                V3 p{c.x + r * std::cos(a), c.y, c.z - r * std::sin(a)};
+                m.vertices.insert(m.vertices.end(), {(float)p.x, (float)p.y, (float)p.z});
+            }
+            m.indices = {0, 1, 2};
+            ks_material_desc mat = default_material();
+            double L = std::pow(10.0, 3.0 * rng.uniform());
+            mat.has_emission = 1;
+            for (int c2 = 0; c2 < 3; ++c2)
+                mat.emission[c2] = (float)(L * (0.6 + 0.4 * rng.uniform()));
+            g.materials.push_back(mat);
+            m.material = (uint32_t)g.materials.size() - 1;
+            g.meshes.push_back(std::move(m));
+        }
+        g.prototypes.push_back(ks_prototype_desc{first, o.emitters});
+        g.instances.push_back(identity((uint32_t)g.prototypes.size() - 1));
+    }
+    // ground
+    ks_material_desc ground = default_material();
+    ground.basecolor[0] = ground.basecolor[1] = ground.basecolor[2] = 0.5f;
+    g.materials.push_back(ground);
+    const double s = 20.0;
+    add_quad(g, {-s, 0, -s}, {-s, 0, s}, {s, 0, s}, {s, 0, -s}, (uint32_t)g.materials.size() - 1);
+    g.prototypes.push_back(ks_prototype_desc{(uint32_t)g.meshes.size() - 1, 1});
+    g.instances.push_back(identity((uint32_t)g.prototypes.size() - 1));
+    gen_sky(g, o.sky_width, o.sky_height, norm(V3{0.45, 0.6, -0.66}));
+    look_at(g, {0.0, 4.5, 12.5}, {0, 0.3, 0}, {0, 1, 0}, 40.0, (double)o.width / o.height);
+}
+
+} // namespace
+
 void GeneratedScene::finalize()
 {
     mesh_descs.resize(meshes.size());
@@ -364,6 +513,10 @@ void GeneratedScene::finalize()
     if (sky.kind == 2)
         sky.map_rgb = sky_map.data();
     desc.sky = sky;
+    desc.prototypes = prototypes.empty() ? nullptr : prototypes.data();
+    desc.n_prototypes = (uint32_t)prototypes.size();
+    desc.instances = instances.empty() ? nullptr : instances.data();
+    desc.n_instances = (uint32_t)instances.size();
 }
 
 bool generate_scene(const std::string &kind, uint64_t seed, const ProceduralOptions &opts, GeneratedScene &out)
@@ -375,6 +528,8 @@ bool generate_scene(const std::string &kind, uint64_t seed, const ProceduralOpti
         gen_box_room(out, seed);
     } else if (kind == "icosphere") {
         gen_icosphere_scene(out, seed, opts);
+    } else if (kind == "instanced") {
+        gen_instanced_scene(out, seed, opts);
     } else {
         return false;
     }

@@ -19,6 +19,12 @@ struct ProceduralOptions
     uint32_t sky_height = 1024;
     uint32_t width = 1024; // render resolution (sets the camera aspect)
     uint32_t height = 1024;
+    // "instanced": prototypes, instances, geodesic frequency (20 f^2 triangles per prototype),
+    // emissive triangles
+    uint32_t prototypes = 8;
+    uint32_t instances = 400;
+    uint32_t frequency = 50;
+    uint32_t emitters = 64;
 };
 
 struct GeneratedMesh
@@ -35,6 +41,8 @@ struct GeneratedScene
     std::vector<float> sky_map;
     ks_sky_desc sky{};
     std::vector<ks_mesh_desc> mesh_descs;
+    std::vector<ks_prototype_desc> prototypes; // empty: flat scene
+    std::vector<ks_instance_desc> instances;
     ks_scene_desc desc{};
     float camera_to_world[16]{};
     float vfov = 0.7f;
