@@ -374,6 +374,47 @@ const char *ks_config_last_error(void);
 ks_status ks_config_parse(const char *config_text, char *normalised, size_t capacity, size_t *length);
 
 /* ---------------------------------------------------------------------------------------------
+ * Batched rendering: many (scene, camera, parameters) jobs in one wavefront.  The paths of all
+ * jobs share one pool of path slots, so scenes of uneven size and frames of uneven resolution
+ * keep the GPU full; refill, the bounce loop and its termination run on the device, and the
+ * whole batch is one CUDA graph launch (a while node around two wavefront iterations) unless
+ * use_graph is 0 (then the host re-launches the iterations).  Jobs: flat (non-instanced) scenes
+ * of one context, built; frames of at most 2^21 pixels; at most 1024 jobs; accumulators on the
+ * device, added into as in ks_small_pt_render_device.  Each job's image equals its own
+ * ks_small_pt_render_device (same Sobol samples and estimator).  No reference counterpart.
+ * ------------------------------------------------------------------------------------------- */
+typedef struct ks_batch_job {
+    ks_scene *scene;
+    ks_camera_desc camera;
+    ks_small_pt_params params; /* spp_prog_interval is ignored: the whole job in one pass */
+    double *accum_rgb_device;  /* W * H * 3 */
+    double *weights_device;    /* W * H * 2 */
+} ks_batch_job;
+
+typedef struct ks_batch_options {
+    uint32_t capacity;       /* path slots (0 -> 2^22) */
+    uint32_t grid_per_sm;    /* blocks per SM of the traversal and shading kernels (0 -> 16) */
+    int32_t use_graph;       /* 1: one CUDA graph launch for the batch */
+} ks_batch_options;
+
+typedef struct ks_batch_stats {
+    uint64_t paths;
+    uint64_t extension_rays;
+    uint64_t shadow_rays;
+    uint32_t iterations;     /* wavefront iterations run on the device */
+    uint32_t graph_launches; /* 1 in graph mode */
+    float ms_total;          /* device time of the batch */
+} ks_batch_stats;
+
+ks_status ks_batch_render_device(ks_context *ctx, const ks_batch_job *jobs, uint32_t n_jobs,
+                                 const ks_batch_options *options, ks_batch_stats *stats);
+/* Autotuner: times short renders of a sample of the jobs (up to 8 jobs, at most 4 spp each, into
+ * scratch images) for path capacities 2^20 .. 2^23 and 4 .. 32 blocks per SM, and writes the
+ * fastest into *best (use_graph kept as given); best_ms (may be NULL) receives its time. */
+ks_status ks_batch_autotune(ks_context *ctx, const ks_batch_job *jobs, uint32_t n_jobs, ks_batch_options *best,
+                            float *best_ms);
+
+/* ---------------------------------------------------------------------------------------------
  * Procedural scenes: seeded synthetic inputs standing in for mesh-asset loading
  * (mesh_asset.cpp).  kind: "box_room", "icosphere" or "instanced" (prototypes + instances; the
  * scene description then carries prototypes and instances).

@@ -658,3 +658,61 @@ def read_pfm(path):
         data = np.frombuffer(f.read(), dtype="<f4" if scale < 0 else ">f4")
     assert magic == b"PF"
     return data.reshape(h, w, 3)[::-1].astype(np.float32)
+
+
+# ---------------------------------------------------------------------------------------------
+# Batched rendering (ks_batch_*)
+# ---------------------------------------------------------------------------------------------
+class BatchJob(ctypes.Structure):
+    _fields_ = [("scene", _vp), ("camera", CameraDesc), ("params", SmallPTParams), ("accum_rgb_device", _vp),
+                ("weights_device", _vp)]
+
+
+class BatchOptions(ctypes.Structure):
+    _fields_ = [("capacity", _u32), ("grid_per_sm", _u32), ("use_graph", _i32)]
+
+
+class BatchStats(ctypes.Structure):
+    _fields_ = [("paths", ctypes.c_uint64), ("extension_rays", ctypes.c_uint64), ("shadow_rays", ctypes.c_uint64),
+                ("iterations", _u32), ("graph_launches", _u32), ("ms_total", _f32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_sig("ks_batch_render_device", [_vp, ctypes.POINTER(BatchJob), _u32, ctypes.POINTER(BatchOptions),
+                                ctypes.POINTER(BatchStats)])
+_sig("ks_batch_autotune", [_vp, ctypes.POINTER(BatchJob), _u32, ctypes.POINTER(BatchOptions),
+                           ctypes.POINTER(_f32)])
+
+
+def _batch_jobs(jobs):
+    arr = (BatchJob * len(jobs))()
+    for k, (scene, camera, params, acc_ptr, wts_ptr) in enumerate(jobs):
+        arr[k].scene = scene.handle
+        arr[k].camera = camera
+        arr[k].params = params
+        arr[k].accum_rgb_device = acc_ptr
+        arr[k].weights_device = wts_ptr
+    return arr
+
+
+def batch_render(ctx: Context, jobs, capacity=0, grid_per_sm=0, use_graph=True) -> BatchStats:
+    """ks_batch_render_device; jobs = [(Scene, CameraDesc, SmallPTParams, accum_ptr, weights_ptr)]
+    with device buffers (raw pointers)."""
+    arr = _batch_jobs(jobs)
+    o = BatchOptions(capacity, grid_per_sm, int(bool(use_graph)))
+    st = BatchStats()
+    ctx.check(lib.ks_batch_render_device(ctx.handle, arr, len(jobs), ctypes.byref(o), ctypes.byref(st)),
+              "ks_batch_render_device")
+    return st
+
+
+def batch_autotune(ctx: Context, jobs, use_graph=True):
+    """ks_batch_autotune: returns (BatchOptions, ms of the best sample run)."""
+    arr = _batch_jobs(jobs)
+    o = BatchOptions(0, 0, int(bool(use_graph)))
+    ms = _f32()
+    ctx.check(lib.ks_batch_autotune(ctx.handle, arr, len(jobs), ctypes.byref(o), ctypes.byref(ms)),
+              "ks_batch_autotune")
+    return o, ms.value

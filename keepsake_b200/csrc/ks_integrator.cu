@@ -65,6 +65,43 @@ struct ShadowBuf
 
 constexpr uint32_t kTermBit = 0x80000000u;
 
+// ---- batched rendering: many (scene, camera, params) jobs in one wavefront --------------------
+// A path's job id rides in bits 21..30 of its pixel word (per-job frames of at most 2^21 pixels,
+// up to 1024 jobs); the scene view, render parameters and accumulators of a job are read from
+// device arrays.  The iteration's counts live on the device (BatchState), so the loop needs no
+// host round trip and runs as a CUDA graph with a device-side while condition.
+constexpr uint32_t kJobShift = 21;
+constexpr uint32_t kPixMask = (1u << kJobShift) - 1u;
+constexpr uint32_t kMaxJobs = 1024;
+
+struct BatchState
+{
+    unsigned long long total, issued, first_path; // paths of all jobs, paths issued, first of this refill
+    unsigned long long ext_rays, shadow_rays;     // work counters
+    uint32_t cur_count, n_new, count, base_slot;  // paths alive, refilled, traced this iteration
+    uint32_t iterations, max_iterations, error;
+};
+
+struct BatchView
+{
+    const SceneView *views;       // per job
+    const RenderParams *params;   // per job
+    double *const *accum;         // per job: W * H * 3
+    double *const *weights;       // per job: W * H * 2
+    const unsigned long long *path_begin; // n_jobs + 1: first global path index of each job
+    uint32_t n_jobs;
+    BatchState *state;
+};
+
+template <bool kBatch, class T>
+KS_D const T &job_of(const T &single, const T *table, uint32_t job)
+{
+    if constexpr (kBatch)
+        return table[job];
+    else
+        return single;
+}
+
 KS_D uint32_t bits(float f) { return __float_as_uint(f); }
 KS_D float fbits(uint32_t u) { return __uint_as_float(u); }
 
@@ -201,16 +238,11 @@ KS_D f3 clamp_contrib(f3 v, int bounce_for_direct, const RenderParams &rp, bool 
 
 // ---- kernels --------------------------------------------------------------------------------
 
-__global__ void k_raygen(RenderParams rp, PathBuf pb, uint32_t base_slot, uint64_t first_path, uint32_t n_new,
-                         int s0, uint32_t n_pix)
+// Camera sample s of pixel (px, py) into path slot `slot`: Sobol box-filter offset, ray through
+// the projection (Camera::spawn_ray, camera.cpp:129-170; film position small_pt.cpp:50-54).
+// pix_word is the pixel index (with the job id in its upper bits for batched renders).
+KS_D void camera_path(const RenderParams &rp, int px, int py, int s, uint32_t pix_word, PathBuf &pb, uint32_t slot)
 {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n_new)
-        return;
-    uint64_t k = first_path + i;
-    int s = s0 + (int)(k / n_pix);
-    uint32_t pl = (uint32_t)(k % n_pix);
-    int px = rp.cx + (int)(pl % (uint32_t)rp.cw), py = rp.cy + (int)(pl / (uint32_t)rp.cw);
     SobolSampler smp = SobolSampler::start((uint32_t)px, (uint32_t)py, (uint32_t)s, rp.log2_spp, rp.n_digits,
                                            (uint32_t)rp.seed, 0);
     float offx = 0.0f, offy = 0.0f;
@@ -230,14 +262,94 @@ __global__ void k_raygen(RenderParams rp, PathBuf pb, uint32_t base_slot, uint64
     f3 wp = mk(o[0] / o[3], o[1] / o[3], o[2] / o[3]);
     f3 cp = mk(rp.cam_pos[0], rp.cam_pos[1], rp.cam_pos[2]);
     f3 dir = normalize(wp - cp);
-    uint32_t slot = base_slot + i;
-    uint32_t pix = (uint32_t)py * (uint32_t)rp.W + (uint32_t)px;
     pb.o_pdf[slot] = make_float4(cp.x, cp.y, cp.z, 0.0f);
     pb.d_info[slot] = make_float4(dir.x, dir.y, dir.z, fbits(((uint32_t)smp.dimension << 16) | 0u));
-    pb.beta_pix[slot] = make_float4(1.0f, 1.0f, 1.0f, fbits(pix));
+    pb.beta_pix[slot] = make_float4(1.0f, 1.0f, 1.0f, fbits(pix_word));
     pb.L_smp[slot] = make_float4(0.0f, 0.0f, 0.0f, fbits((uint32_t)s));
     if (pb.rec)
         pb.rec[slot] = kNoRecord;
+}
+
+__global__ void k_raygen(const __grid_constant__ RenderParams rp, PathBuf pb, uint32_t base_slot, uint64_t first_path,
+                         uint32_t n_new, int s0, uint32_t n_pix)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_new)
+        return;
+    uint64_t k = first_path + i;
+    int s = s0 + (int)(k / n_pix);
+    uint32_t pl = (uint32_t)(k % n_pix);
+    int px = rp.cx + (int)(pl % (uint32_t)rp.cw), py = rp.cy + (int)(pl / (uint32_t)rp.cw);
+    camera_path(rp, px, py, s, (uint32_t)py * (uint32_t)rp.W + (uint32_t)px, pb, base_slot + i);
+}
+
+// Batched refill: new path i of this iteration is global path first_path + i; its job is found in
+// the jobs' path ranges, then sample-major over the job's crop window as in k_raygen.
+__global__ void k_raygen_batch(BatchView bv, PathBuf pb)
+{
+    const BatchState &st = *bv.state;
+    const uint32_t n_new = st.n_new, base_slot = st.base_slot;
+    const unsigned long long first = st.first_path;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_new; i += gridDim.x * blockDim.x) {
+        const unsigned long long k = first + i;
+        uint32_t lo = 0, hi = bv.n_jobs;
+        while (hi - lo > 1) {
+            uint32_t mid = (lo + hi) / 2;
+            if (bv.path_begin[mid] <= k)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        const RenderParams &rp = bv.params[lo];
+        const unsigned long long kk = k - bv.path_begin[lo];
+        const uint32_t n_pix = (uint32_t)rp.cw * (uint32_t)rp.ch;
+        int s = (int)(kk / n_pix);
+        uint32_t pl = (uint32_t)(kk % n_pix);
+        int px = rp.cx + (int)(pl % (uint32_t)rp.cw), py = rp.cy + (int)(pl / (uint32_t)rp.cw);
+        uint32_t pix = ((uint32_t)py * (uint32_t)rp.W + (uint32_t)px) | (lo << kJobShift);
+        camera_path(rp, px, py, s, pix, pb, base_slot + i);
+    }
+}
+
+// Batched iteration head: paths that continue from the last iteration stay in [0, alive); the
+// free slots are refilled with new paths; the queue counters restart.
+__global__ void k_batch_prep(BatchState *st, uint32_t *counters, uint32_t capacity)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0)
+        return;
+    BatchState &s = *st;
+    const uint32_t alive = counters[0];
+    const unsigned long long left = s.total - s.issued;
+    const uint32_t n_new = (uint32_t)(left < (unsigned long long)(capacity - alive) ? left : capacity - alive);
+    s.cur_count = alive;
+    s.base_slot = alive;
+    s.n_new = n_new;
+    s.first_path = s.issued;
+    s.issued += n_new;
+    s.count = alive + n_new;
+    s.ext_rays += s.count;
+    counters[0] = counters[1] = counters[2] = counters[3] = 0;
+}
+
+// Batched iteration tail: counts the shadow rays and decides whether another iteration is
+// needed; an iteration limit ends the loop with the error flag set.  In a graph the decision
+// drives the while node.
+__global__ void k_batch_advance(BatchState *st, const uint32_t *counters, cudaGraphConditionalHandle handle,
+                                int use_graph)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0)
+        return;
+    BatchState &s = *st;
+    s.shadow_rays += counters[1];
+    s.iterations += 1;
+    bool more = s.issued < s.total || counters[0] > 0;
+    if (s.iterations >= s.max_iterations) {
+        if (more)
+            s.error = 1;
+        more = false;
+    }
+    if (use_graph)
+        cudaGraphSetConditional(handle, more ? 1u : 0u);
 }
 
 // Adds a per-thread work count into two 64-bit device counters, one atomic per warp.
@@ -256,17 +368,23 @@ KS_D void flush_counts(const TravCount &c, unsigned long long *dst)
 
 // Closest hit for every queued ray; the path index goes to the hit queue or the miss queue.
 // kInst: two-level traversal of an instanced scene; the instance of each hit goes to hit_inst.
-template <bool kInst>
-__global__ void __launch_bounds__(128) k_extend(SceneView sv, PathBuf pb, uint32_t count, float4 *hits,
-                                                uint32_t *hit_inst, uint32_t *hit_queue, uint32_t *miss_queue,
-                                                uint32_t *queue_counts, int *overflow, unsigned long long *work)
+// kBatch: paths of many jobs (flat scenes), the count read from the batch state.
+template <bool kInst, bool kBatch = false>
+__global__ void __launch_bounds__(128) k_extend(const __grid_constant__ SceneView sv_in, PathBuf pb, uint32_t count,
+                                                float4 *hits, uint32_t *hit_inst, uint32_t *hit_queue,
+                                                uint32_t *miss_queue, uint32_t *queue_counts, int *overflow,
+                                                unsigned long long *work, BatchView bv)
 {
     TravCount tc;
     const uint32_t stride = gridDim.x * blockDim.x;
+    if constexpr (kBatch)
+        count = bv.state->count;
     for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += stride) {
         uint32_t i = base + threadIdx.x;
         bool valid = i < count, is_hit = false;
         if (valid) {
+            const uint32_t job = kBatch ? (bits(pb.beta_pix[i].w) >> kJobShift) : 0u;
+            const SceneView &sv = job_of<kBatch>(sv_in, bv.views, job);
             float4 a = pb.o_pdf[i], b = pb.d_info[i];
             RayQuery q;
             q.o = mk(a.x, a.y, a.z);
@@ -306,18 +424,23 @@ __global__ void __launch_bounds__(128) k_extend(SceneView sv, PathBuf pb, uint32
 // (nee.cpp:28-34, material.cpp:157-158, small_pt.cpp:168-174).  Integer-only and uniform across
 // the warp, so it runs at full occupancy instead of inside the divergent shading kernel.
 // samples[2 * i] = (light, light u, light v, lobe), samples[2 * i + 1] = (wi u, wi v, roulette, -)
-__global__ void __launch_bounds__(128) k_sample(RenderParams rp, PathBuf cur, const uint32_t *queue,
-                                                const uint32_t *queue_count, float4 *samples)
+template <bool kBatch = false>
+__global__ void __launch_bounds__(128) k_sample(const __grid_constant__ RenderParams rp_in, PathBuf cur,
+                                                const uint32_t *queue, const uint32_t *queue_count, float4 *samples,
+                                                BatchView bv)
 {
     const uint32_t count = *queue_count;
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x) {
         uint32_t i = queue[q];
+        uint32_t pix = bits(cur.beta_pix[i].w), smp = bits(cur.L_smp[i].w);
+        const RenderParams &rp = job_of<kBatch>(rp_in, bv.params, pix >> kJobShift);
+        if constexpr (kBatch)
+            pix &= kPixMask;
         uint32_t info = bits(cur.d_info[i].w);
         int bounce = (int)(info & 0xffffu);
         if (bounce == rp.bounces)
             continue;
         int dim = (int)(info >> 16);
-        uint32_t pix = bits(cur.beta_pix[i].w), smp = bits(cur.L_smp[i].w);
         SobolSampler s = SobolSampler::start(pix % (uint32_t)rp.W, pix / (uint32_t)rp.W, smp, rp.log2_spp,
                                              rp.n_digits, (uint32_t)rp.seed, dim);
         float a = s.next();
@@ -341,12 +464,15 @@ __global__ void __launch_bounds__(128) k_sample(RenderParams rp, PathBuf cur, co
 // expectation of the unguided one: the reference's NEE weight omits the light-selection
 // probability that its emitter-hit weight includes, and the two only stay the same functions of
 // the direction if both keep seeing the BSDF pdf.
-template <bool kMiss, bool kGuided>
-__global__ void __launch_bounds__(128) k_shade(SceneView sv, RenderParams rp, PathBuf cur, PathBuf nxt,
+// kBatch: paths of many jobs; the view, parameters and accumulators of a path's job come from bv.
+template <bool kMiss, bool kGuided, bool kBatch = false>
+__global__ void __launch_bounds__(128) k_shade(const __grid_constant__ SceneView sv_in,
+                                               const __grid_constant__ RenderParams rp_in, PathBuf cur, PathBuf nxt,
                                                const float4 *hits, const uint32_t *hit_inst,
                                                const float4 *samples, const uint32_t *queue,
                                                const uint32_t *queue_count, uint32_t *next_count, ShadowBuf sb,
-                                               uint32_t *shadow_count, double *accum, double *weights, GuideView gv)
+                                               uint32_t *shadow_count, double *accum_in, double *weights_in,
+                                               GuideView gv, BatchView bv)
 {
     const uint32_t stride = gridDim.x * blockDim.x;
     const uint32_t count = *queue_count;
@@ -376,6 +502,9 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sv, RenderParams rp, Pa
             pix = bits(c.w);
             L = mk(d.x, d.y, d.z);
             smp = bits(d.w);
+            const uint32_t job = kBatch ? (pix >> kJobShift) : 0u;
+            const SceneView &sv = job_of<kBatch>(sv_in, bv.views, job);
+            const RenderParams &rp = job_of<kBatch>(rp_in, bv.params, job);
             float4 h = hits[i];
             uint32_t slot = bits(h.w);
             if constexpr (kGuided)
@@ -603,27 +732,41 @@ __global__ void __launch_bounds__(128) k_shade(SceneView sv, RenderParams rp, Pa
         if (shadow) {
             sb.o_tmax[js] = make_float4(sh_o.x, sh_o.y, sh_o.z, sh_tmax);
             sb.d_target[js] = make_float4(sh_d.x, sh_d.y, sh_d.z, fbits(cont ? jc : (kTermBit | pix)));
-            sb.contrib[js] = make_float4(sh_c.x, sh_c.y, sh_c.z, fbits(sh_rec));
+            // the w component: the path's earlier record (guided), or its job (batched)
+            sb.contrib[js] = make_float4(sh_c.x, sh_c.y, sh_c.z, fbits(kBatch ? (pix >> kJobShift) : sh_rec));
             if (!cont)
                 sb.L_term[js] = make_float4(L.x, L.y, L.z, 0.0f);
         }
         if (valid && !cont && !shadow) {
+            double *accum = accum_in, *weights = weights_in;
+            uint32_t px = pix;
+            if constexpr (kBatch) {
+                accum = bv.accum[pix >> kJobShift];
+                weights = bv.weights[pix >> kJobShift];
+                px = pix & kPixMask;
+            }
             if (miss_only)
-                atomicAdd(&weights[2 * (size_t)pix + 1], 1.0);
+                atomicAdd(&weights[2 * (size_t)px + 1], 1.0);
             else
-                accumulate(accum, weights, pix, L);
+                accumulate(accum, weights, px, L);
         }
     }
 }
 
-template <bool kInst>
-__global__ void __launch_bounds__(128) k_shadow(SceneView sv, ShadowBuf sb, const uint32_t *shadow_count,
-                                                PathBuf nxt, double *accum, double *weights, int *overflow,
-                                                unsigned long long *work, GuideView gv)
+template <bool kInst, bool kBatch = false>
+__global__ void __launch_bounds__(128) k_shadow(const __grid_constant__ SceneView sv_in, ShadowBuf sb,
+                                                const uint32_t *shadow_count, PathBuf nxt, double *accum_in,
+                                                double *weights_in, int *overflow, unsigned long long *work,
+                                                GuideView gv, BatchView bv)
 {
     const uint32_t n = *shadow_count;
     TravCount tc;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float4 c = sb.contrib[i];
+        const uint32_t job = kBatch ? bits(c.w) : 0u;
+        const SceneView &sv = job_of<kBatch>(sv_in, bv.views, job);
+        double *accum = kBatch ? bv.accum[job] : accum_in;
+        double *weights = kBatch ? bv.weights[job] : weights_in;
         float4 a = sb.o_tmax[i], b = sb.d_target[i];
         RayQuery q;
         q.o = mk(a.x, a.y, a.z);
@@ -643,7 +786,6 @@ __global__ void __launch_bounds__(128) k_shadow(SceneView sv, ShadowBuf sb, cons
         if (of)
             atomicOr(overflow, 1);
         uint32_t target = bits(b.w);
-        float4 c = sb.contrib[i];
         if (gv.rec_cap && !occ && bits(c.w) != kNoRecord)
             record_add(gv, bits(c.w), mk(c.x, c.y, c.z));
         if (target & kTermBit) {
@@ -651,7 +793,7 @@ __global__ void __launch_bounds__(128) k_shadow(SceneView sv, ShadowBuf sb, cons
             f3 L = mk(l.x, l.y, l.z);
             if (!occ)
                 L += mk(c.x, c.y, c.z);
-            accumulate(accum, weights, target & ~kTermBit, L);
+            accumulate(accum, weights, kBatch ? (target & kPixMask) : (target & ~kTermBit), L);
         } else if (!occ) {
             float4 l = nxt.L_smp[target];
             l.x += c.x;
@@ -706,6 +848,40 @@ struct RenderWork
     uint32_t capacity = 0;
 };
 
+// RenderParams of one render (SmallPTInput fields + camera); false for an empty crop window.
+static bool fill_params(const ks_camera_desc *cam, const ks_small_pt_params *in, RenderParams &rp)
+{
+    const int W = in->render_width, H = in->render_height;
+    rp = RenderParams{};
+    rp.W = W;
+    rp.H = H;
+    rp.cx = 0;
+    rp.cy = 0;
+    rp.cw = W;
+    rp.ch = H;
+    if (in->crop_width > 0 && in->crop_height > 0) {
+        rp.cx = std::max(in->crop_start_x, 0);
+        rp.cy = std::max(in->crop_start_y, 0);
+        rp.cw = std::min(in->crop_width, W - rp.cx);
+        rp.ch = std::min(in->crop_height, H - rp.cy);
+        if (rp.cw <= 0 || rp.ch <= 0)
+            return false;
+    }
+    rp.spp = in->spp;
+    rp.seed = in->rng_seed;
+    sobol_setup(in->spp, W, H, rp.log2_spp, rp.n_digits);
+    rp.bounces = in->bounces;
+    rp.include_background = in->include_background;
+    rp.clamp_direct = in->clamp_direct;
+    rp.clamp_indirect = in->clamp_indirect;
+    rp.filter_r = 0.5f * (in->pixel_filter_width > 0.0f ? in->pixel_filter_width : 1.0f);
+    rp.cam_pos[0] = cam->camera_to_world[3];
+    rp.cam_pos[1] = cam->camera_to_world[7];
+    rp.cam_pos[2] = cam->camera_to_world[11];
+    std::memcpy(rp.p2w, cam->proj_to_world, sizeof(rp.p2w));
+    return true;
+}
+
 // Guided renders: per-slot mixtures, record index per path, training records.
 struct GuideWork
 {
@@ -736,32 +912,8 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
     if ((uint64_t)W * H >= (1ull << 31))
         return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_small_pt_render: resolution too large");
     RenderParams rp{};
-    rp.W = W;
-    rp.H = H;
-    rp.cx = 0;
-    rp.cy = 0;
-    rp.cw = W;
-    rp.ch = H;
-    if (in->crop_width > 0 && in->crop_height > 0) {
-        rp.cx = std::max(in->crop_start_x, 0);
-        rp.cy = std::max(in->crop_start_y, 0);
-        rp.cw = std::min(in->crop_width, W - rp.cx);
-        rp.ch = std::min(in->crop_height, H - rp.cy);
-        if (rp.cw <= 0 || rp.ch <= 0)
-            return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_small_pt_render: empty crop window");
-    }
-    rp.spp = in->spp;
-    rp.seed = in->rng_seed;
-    sobol_setup(in->spp, W, H, rp.log2_spp, rp.n_digits);
-    rp.bounces = in->bounces;
-    rp.include_background = in->include_background;
-    rp.clamp_direct = in->clamp_direct;
-    rp.clamp_indirect = in->clamp_indirect;
-    rp.filter_r = 0.5f * (in->pixel_filter_width > 0.0f ? in->pixel_filter_width : 1.0f);
-    rp.cam_pos[0] = cam->camera_to_world[3];
-    rp.cam_pos[1] = cam->camera_to_world[7];
-    rp.cam_pos[2] = cam->camera_to_world[11];
-    std::memcpy(rp.p2w, cam->proj_to_world, sizeof(rp.p2w));
+    if (!fill_params(cam, in, rp))
+        return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_small_pt_render: empty crop window");
 
     SceneView sv = make_view(scene);
     const uint32_t n_pix = (uint32_t)rp.cw * (uint32_t)rp.ch;
@@ -874,10 +1026,10 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
             cudaEventRecord(ev[1], st);
             if (scene->n_instances)
                 k_extend<true><<<grid, 128, 0, st>>>(sv, pb[cur], count, w.hits.ptr, w.hit_inst.ptr, w.queue[0].ptr,
-                                                     w.queue[1].ptr, w.counters.ptr + 2, w.overflow.ptr, work.ptr);
+                                                     w.queue[1].ptr, w.counters.ptr + 2, w.overflow.ptr, work.ptr, BatchView{});
             else
                 k_extend<false><<<grid, 128, 0, st>>>(sv, pb[cur], count, w.hits.ptr, nullptr, w.queue[0].ptr,
-                                                      w.queue[1].ptr, w.counters.ptr + 2, w.overflow.ptr, work.ptr);
+                                                      w.queue[1].ptr, w.counters.ptr + 2, w.overflow.ptr, work.ptr, BatchView{});
             cudaEventRecord(ev[2], st);
             if (guide && gv.active) {
                 ks_status gs = guide_impl::infer_paths(guide, w.queue[0].ptr, w.counters.ptr + 2, pb[cur].o_pdf,
@@ -890,31 +1042,31 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
                 stats.kernel_launches++;
             }
             cudaEventRecord(ev[5], st);
-            k_sample<<<grid, 128, 0, st>>>(rp, pb[cur], w.queue[0].ptr, w.counters.ptr + 2, w.samples.ptr);
+            k_sample<<<grid, 128, 0, st>>>(rp, pb[cur], w.queue[0].ptr, w.counters.ptr + 2, w.samples.ptr, BatchView{});
             if (guide) {
                 k_shade<false, true><<<grid, 128, 0, st>>>(sv, rp, pb[cur], pb[1 - cur], w.hits.ptr, w.hit_inst.ptr, w.samples.ptr,
                                                            w.queue[0].ptr, w.counters.ptr + 2, w.counters.ptr, sb,
-                                                           w.counters.ptr + 1, d_accum, d_weights, gv);
+                                                           w.counters.ptr + 1, d_accum, d_weights, gv, BatchView{});
                 k_shade<true, true><<<grid, 128, 0, st>>>(sv, rp, pb[cur], pb[1 - cur], w.hits.ptr, w.hit_inst.ptr, w.samples.ptr,
                                                           w.queue[1].ptr, w.counters.ptr + 3, w.counters.ptr, sb,
-                                                          w.counters.ptr + 1, d_accum, d_weights, gv);
+                                                          w.counters.ptr + 1, d_accum, d_weights, gv, BatchView{});
             } else {
                 k_shade<false, false><<<grid, 128, 0, st>>>(sv, rp, pb[cur], pb[1 - cur], w.hits.ptr,
                                                             w.hit_inst.ptr, w.samples.ptr, w.queue[0].ptr, w.counters.ptr + 2,
                                                             w.counters.ptr, sb, w.counters.ptr + 1, d_accum,
-                                                            d_weights, gv);
+                                                            d_weights, gv, BatchView{});
                 k_shade<true, false><<<grid, 128, 0, st>>>(sv, rp, pb[cur], pb[1 - cur], w.hits.ptr,
                                                            w.hit_inst.ptr, w.samples.ptr, w.queue[1].ptr, w.counters.ptr + 3,
                                                            w.counters.ptr, sb, w.counters.ptr + 1, d_accum,
-                                                           d_weights, gv);
+                                                           d_weights, gv, BatchView{});
             }
             cudaEventRecord(ev[3], st);
             if (scene->n_instances)
                 k_shadow<true><<<grid, 128, 0, st>>>(sv, sb, w.counters.ptr + 1, pb[1 - cur], d_accum, d_weights,
-                                                     w.overflow.ptr, work.ptr + 2, gv);
+                                                     w.overflow.ptr, work.ptr + 2, gv, BatchView{});
             else
                 k_shadow<false><<<grid, 128, 0, st>>>(sv, sb, w.counters.ptr + 1, pb[1 - cur], d_accum, d_weights,
-                                                      w.overflow.ptr, work.ptr + 2, gv);
+                                                      w.overflow.ptr, work.ptr + 2, gv, BatchView{});
             cudaEventRecord(ev[4], st);
             stats.kernel_launches += 5;
             cudaMemcpyAsync(h_counts, w.counters.ptr, sizeof(uint32_t) * 2, cudaMemcpyDeviceToHost, st);
@@ -1016,6 +1168,231 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
         return fail(ctx, KS_ERR_QUEUE_OVERFLOW, "ks_small_pt_render: traversal stack depth exceeded");
     if (guide)
         return guide_impl::status(guide);
+    return KS_OK;
+}
+
+// ---- batched rendering ----------------------------------------------------------------------
+struct BatchWork
+{
+    DevBuf<float4> state[2][4];
+    DevBuf<float4> hits, samples, shadow[4];
+    DevBuf<uint32_t> counters, queue[2];
+    DevBuf<int> overflow;
+    DevBuf<unsigned long long> work;
+    DevBuf<SceneView> views;
+    DevBuf<RenderParams> params;
+    DevBuf<double *> accum, weights;
+    DevBuf<unsigned long long> path_begin;
+    DevBuf<BatchState> state_dev;
+};
+
+// Validates the jobs and fills the per-job tables; returns the total path count in *total.
+static ks_status batch_tables(ks_context *ctx, const ks_batch_job *jobs, uint32_t n, BatchWork &w,
+                              unsigned long long *total, int *max_bounces)
+{
+    if (!jobs || n == 0 || n > kMaxJobs)
+        return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_batch_render_device: 1 to 1024 jobs");
+    std::vector<SceneView> views(n);
+    std::vector<RenderParams> params(n);
+    std::vector<double *> acc(n), wts(n);
+    std::vector<unsigned long long> begin(n + 1, 0);
+    *max_bounces = 0;
+    for (uint32_t j = 0; j < n; ++j) {
+        const ks_batch_job &jb = jobs[j];
+        const ks_small_pt_params &in = jb.params;
+        if (!jb.scene || jb.scene->ctx != ctx || !jb.accum_rgb_device || !jb.weights_device)
+            return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_batch_render_device: job " + std::to_string(j) +
+                                                          ": null scene/buffer or scene of another context");
+        if (!jb.scene->bvh_built || !jb.scene->lights_built)
+            return fail(ctx, KS_ERR_NOT_BUILT, "ks_batch_render_device: job " + std::to_string(j) +
+                                                   ": call ks_scene_build_bvh first");
+        if (jb.scene->light_count == 0 || jb.scene->n_instances)
+            return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_batch_render_device: job " + std::to_string(j) +
+                                                          ": scene without lights or instanced");
+        if (in.render_width <= 0 || in.render_height <= 0 || in.spp <= 0 || in.bounces < 0 || in.bounces > 0xfffe ||
+            (uint64_t)in.render_width * in.render_height > (1ull << kJobShift))
+            return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_batch_render_device: job " + std::to_string(j) +
+                                                          ": bad resolution (at most 2^21 pixels), spp or bounces");
+        if (!fill_params(&jb.camera, &in, params[j]))
+            return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_batch_render_device: empty crop window");
+        views[j] = make_view(jb.scene);
+        acc[j] = jb.accum_rgb_device;
+        wts[j] = jb.weights_device;
+        begin[j + 1] = begin[j] + (unsigned long long)params[j].cw * params[j].ch * (unsigned long long)in.spp;
+        *max_bounces = std::max(*max_bounces, in.bounces);
+    }
+    *total = begin[n];
+    cudaStream_t st = ctx->stream;
+    KS_CUDA_TRY(ctx, w.views.alloc(n));
+    KS_CUDA_TRY(ctx, w.params.alloc(n));
+    KS_CUDA_TRY(ctx, w.accum.alloc(n));
+    KS_CUDA_TRY(ctx, w.weights.alloc(n));
+    KS_CUDA_TRY(ctx, w.path_begin.alloc(n + 1));
+    KS_CUDA_TRY(ctx, cudaMemcpyAsync(w.views.ptr, views.data(), w.views.bytes(), cudaMemcpyHostToDevice, st));
+    KS_CUDA_TRY(ctx, cudaMemcpyAsync(w.params.ptr, params.data(), w.params.bytes(), cudaMemcpyHostToDevice, st));
+    KS_CUDA_TRY(ctx, cudaMemcpyAsync(w.accum.ptr, acc.data(), w.accum.bytes(), cudaMemcpyHostToDevice, st));
+    KS_CUDA_TRY(ctx, cudaMemcpyAsync(w.weights.ptr, wts.data(), w.weights.bytes(), cudaMemcpyHostToDevice, st));
+    KS_CUDA_TRY(ctx, cudaMemcpyAsync(w.path_begin.ptr, begin.data(), w.path_begin.bytes(), cudaMemcpyHostToDevice, st));
+    KS_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    return KS_OK;
+}
+
+// One wavefront iteration of a batch, enqueued on the stream (captured into the graph body).
+static void batch_iteration(ks_context *ctx, BatchWork &w, const BatchView &bv, PathBuf *pb, const ShadowBuf &sb,
+                            int cur, uint32_t capacity, unsigned grid, cudaGraphConditionalHandle handle, int use_graph)
+{
+    cudaStream_t st = ctx->stream;
+    uint32_t *cnt = w.counters.ptr;
+    const GuideView gv{};
+    k_batch_prep<<<1, 32, 0, st>>>(bv.state, cnt, capacity);
+    k_raygen_batch<<<(unsigned)ctx->sm_count * 8, 256, 0, st>>>(bv, pb[cur]);
+    k_extend<false, true><<<grid, 128, 0, st>>>(SceneView{}, pb[cur], 0u, w.hits.ptr, nullptr, w.queue[0].ptr,
+                                                w.queue[1].ptr, cnt + 2, w.overflow.ptr, w.work.ptr, bv);
+    k_sample<true><<<grid, 128, 0, st>>>(RenderParams{}, pb[cur], w.queue[0].ptr, cnt + 2, w.samples.ptr, bv);
+    k_shade<false, false, true><<<grid, 128, 0, st>>>(SceneView{}, RenderParams{}, pb[cur], pb[1 - cur], w.hits.ptr,
+                                                      nullptr, w.samples.ptr, w.queue[0].ptr, cnt + 2, cnt, sb,
+                                                      cnt + 1, nullptr, nullptr, gv, bv);
+    k_shade<true, false, true><<<grid, 128, 0, st>>>(SceneView{}, RenderParams{}, pb[cur], pb[1 - cur], w.hits.ptr,
+                                                     nullptr, w.samples.ptr, w.queue[1].ptr, cnt + 3, cnt, sb,
+                                                     cnt + 1, nullptr, nullptr, gv, bv);
+    k_shadow<false, true><<<grid, 128, 0, st>>>(SceneView{}, sb, cnt + 1, pb[1 - cur], nullptr, nullptr,
+                                                w.overflow.ptr, w.work.ptr + 2, gv, bv);
+    k_batch_advance<<<1, 32, 0, st>>>(bv.state, cnt, handle, use_graph);
+}
+
+static ks_status batch_render(ks_context *ctx, const ks_batch_job *jobs, uint32_t n, const ks_batch_options &o,
+                              ks_batch_stats *out)
+{
+    cudaStream_t st = ctx->stream;
+    BatchWork w;
+    unsigned long long total = 0;
+    int max_bounces = 0;
+    ks_status s = batch_tables(ctx, jobs, n, w, &total, &max_bounces);
+    if (s != KS_OK)
+        return s;
+    const uint32_t capacity =
+        (uint32_t)std::max<unsigned long long>(1, std::min<unsigned long long>(o.capacity ? o.capacity : 1u << 22,
+                                                                               total));
+    const unsigned grid = (unsigned)ctx->sm_count * (o.grid_per_sm ? std::min(o.grid_per_sm, 64u) : 16u);
+    for (int b = 0; b < 2; ++b)
+        for (int f = 0; f < 4; ++f)
+            KS_CUDA_TRY(ctx, w.state[b][f].alloc(capacity));
+    KS_CUDA_TRY(ctx, w.hits.alloc(capacity));
+    KS_CUDA_TRY(ctx, w.samples.alloc(2 * (size_t)capacity));
+    for (auto &q : w.queue)
+        KS_CUDA_TRY(ctx, q.alloc(capacity));
+    for (auto &f : w.shadow)
+        KS_CUDA_TRY(ctx, f.alloc(capacity));
+    KS_CUDA_TRY(ctx, w.counters.alloc(4));
+    KS_CUDA_TRY(ctx, w.overflow.alloc(1));
+    KS_CUDA_TRY(ctx, w.work.alloc(4));
+    KS_CUDA_TRY(ctx, w.state_dev.alloc(1));
+    BatchState init{};
+    init.total = total;
+    // every path ends after at most bounces + 1 extension rays
+    init.max_iterations = (uint32_t)std::min<unsigned long long>((total / capacity + 2) * (max_bounces + 2) + 64,
+                                                                  0x7fffffffull);
+    KS_CUDA_TRY(ctx, cudaMemcpyAsync(w.state_dev.ptr, &init, sizeof(init), cudaMemcpyHostToDevice, st));
+    KS_CUDA_TRY(ctx, cudaMemsetAsync(w.counters.ptr, 0, sizeof(uint32_t) * 4, st));
+    KS_CUDA_TRY(ctx, cudaMemsetAsync(w.overflow.ptr, 0, sizeof(int), st));
+    KS_CUDA_TRY(ctx, cudaMemsetAsync(w.work.ptr, 0, sizeof(unsigned long long) * 4, st));
+    BatchView bv{w.views.ptr, w.params.ptr, w.accum.ptr, w.weights.ptr, w.path_begin.ptr, n, w.state_dev.ptr};
+    PathBuf pb[2];
+    for (int b = 0; b < 2; ++b)
+        pb[b] = PathBuf{w.state[b][0].ptr, w.state[b][1].ptr, w.state[b][2].ptr, w.state[b][3].ptr, nullptr};
+    ShadowBuf sb{w.shadow[0].ptr, w.shadow[1].ptr, w.shadow[2].ptr, w.shadow[3].ptr};
+
+    cudaEvent_t e0, e1;
+    KS_CUDA_TRY(ctx, cudaEventCreate(&e0));
+    KS_CUDA_TRY(ctx, cudaEventCreate(&e1));
+    cudaError_t err = cudaSuccess;
+    uint32_t graph_launches = 0;
+    if (o.use_graph) {
+        // while (more) { iteration(buffers 0 -> 1); iteration(buffers 1 -> 0); }
+        cudaGraph_t graph = nullptr, body = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        cudaGraphConditionalHandle handle{};
+        err = cudaGraphCreate(&graph, 0);
+        if (err == cudaSuccess)
+            err = cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault);
+        cudaGraphNodeParams cp{};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = handle;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        if (err == cudaSuccess)
+            err = cudaGraphAddNode(&node, graph, nullptr, 0, &cp);
+        if (err == cudaSuccess) {
+            body = cp.conditional.phGraph_out[0];
+            err = cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+            if (err == cudaSuccess) {
+                batch_iteration(ctx, w, bv, pb, sb, 0, capacity, grid, handle, 1);
+                batch_iteration(ctx, w, bv, pb, sb, 1, capacity, grid, handle, 1);
+                cudaError_t launch_err = cudaGetLastError();
+                err = cudaStreamEndCapture(st, &body);
+                if (err == cudaSuccess)
+                    err = launch_err;
+            }
+        }
+        if (err == cudaSuccess)
+            err = cudaGraphInstantiate(&exec, graph, 0);
+        if (err == cudaSuccess) {
+            cudaEventRecord(e0, st);
+            err = cudaGraphLaunch(exec, st);
+            cudaEventRecord(e1, st);
+            graph_launches = 1;
+        }
+        if (err == cudaSuccess)
+            err = cudaStreamSynchronize(st);
+        if (exec)
+            cudaGraphExecDestroy(exec);
+        if (graph)
+            cudaGraphDestroy(graph);
+    } else {
+        cudaEventRecord(e0, st);
+        for (uint32_t pair = 0; err == cudaSuccess; ++pair) {
+            batch_iteration(ctx, w, bv, pb, sb, 0, capacity, grid, cudaGraphConditionalHandle{}, 0);
+            batch_iteration(ctx, w, bv, pb, sb, 1, capacity, grid, cudaGraphConditionalHandle{}, 0);
+            BatchState hs{};
+            uint32_t next = 0;
+            err = cudaMemcpyAsync(&hs, w.state_dev.ptr, sizeof(hs), cudaMemcpyDeviceToHost, st);
+            if (err == cudaSuccess)
+                err = cudaMemcpyAsync(&next, w.counters.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+            if (err == cudaSuccess)
+                err = cudaStreamSynchronize(st);
+            if (err != cudaSuccess || hs.error || hs.iterations >= hs.max_iterations ||
+                !(hs.issued < hs.total || next > 0))
+                break;
+        }
+        cudaEventRecord(e1, st);
+        if (err == cudaSuccess)
+            err = cudaStreamSynchronize(st);
+    }
+    float ms = 0.0f;
+    if (err == cudaSuccess)
+        cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (err != cudaSuccess)
+        return cuda_fail(ctx, err, "ks_batch_render_device");
+    BatchState hs{};
+    int overflow = 0;
+    KS_CUDA_TRY(ctx, cudaMemcpy(&hs, w.state_dev.ptr, sizeof(hs), cudaMemcpyDeviceToHost));
+    KS_CUDA_TRY(ctx, cudaMemcpy(&overflow, w.overflow.ptr, sizeof(int), cudaMemcpyDeviceToHost));
+    if (out) {
+        *out = ks_batch_stats{};
+        out->paths = hs.issued;
+        out->extension_rays = hs.ext_rays;
+        out->shadow_rays = hs.shadow_rays;
+        out->iterations = hs.iterations;
+        out->graph_launches = graph_launches;
+        out->ms_total = ms;
+    }
+    if (hs.error)
+        return fail(ctx, KS_ERR_WATCHDOG, "ks_batch_render_device: wavefront iteration limit reached");
+    if (overflow)
+        return fail(ctx, KS_ERR_QUEUE_OVERFLOW, "ks_batch_render_device: traversal stack depth exceeded");
     return KS_OK;
 }
 
@@ -1143,6 +1520,66 @@ ks_status ks_render_stats_last(const ks_scene *scene, ks_render_stats *out)
     if (!scene || !out)
         return KS_ERR_INVALID_ARGUMENT;
     *out = scene->last_stats;
+    return KS_OK;
+}
+
+ks_status ks_batch_render_device(ks_context *ctx, const ks_batch_job *jobs, uint32_t n_jobs,
+                                 const ks_batch_options *options, ks_batch_stats *stats)
+{
+    if (!ctx)
+        return KS_ERR_INVALID_ARGUMENT;
+    KS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    ks_batch_options o{0, 0, 1};
+    if (options)
+        o = *options;
+    return batch_render(ctx, jobs, n_jobs, o, stats);
+}
+
+ks_status ks_batch_autotune(ks_context *ctx, const ks_batch_job *jobs, uint32_t n_jobs, ks_batch_options *best,
+                            float *best_ms)
+{
+    if (!ctx || !jobs || !best || n_jobs == 0)
+        return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_batch_autotune: null argument");
+    KS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    // sample: up to 8 evenly spaced jobs at no more than 4 spp, into scratch images
+    const uint32_t m = std::min<uint32_t>(n_jobs, 8);
+    std::vector<ks_batch_job> sample(m);
+    std::vector<DevBuf<double>> scratch(2 * m);
+    for (uint32_t k = 0; k < m; ++k) {
+        sample[k] = jobs[(uint64_t)k * n_jobs / m];
+        sample[k].params.spp = std::min(sample[k].params.spp, 4);
+        size_t px = (size_t)std::max(0, sample[k].params.render_width) * std::max(0, sample[k].params.render_height);
+        KS_CUDA_TRY(ctx, scratch[2 * k].alloc(3 * px + 1));
+        KS_CUDA_TRY(ctx, scratch[2 * k + 1].alloc(2 * px + 1));
+        sample[k].accum_rgb_device = scratch[2 * k].ptr;
+        sample[k].weights_device = scratch[2 * k + 1].ptr;
+    }
+    const uint32_t caps[] = {1u << 20, 1u << 21, 1u << 22, 1u << 23};
+    const uint32_t grids[] = {4, 8, 16, 32};
+    ks_batch_options bo = *best;
+    float bms = 0.0f;
+    bool have = false;
+    // one untimed run first (first-launch costs)
+    ks_batch_options warm{1u << 21, 16, best->use_graph};
+    ks_status s = batch_render(ctx, sample.data(), m, warm, nullptr);
+    if (s != KS_OK)
+        return s;
+    for (uint32_t c : caps)
+        for (uint32_t g : grids) {
+            ks_batch_options o{c, g, best->use_graph};
+            ks_batch_stats st{};
+            s = batch_render(ctx, sample.data(), m, o, &st);
+            if (s != KS_OK)
+                return s;
+            if (!have || st.ms_total < bms) {
+                have = true;
+                bms = st.ms_total;
+                bo = o;
+            }
+        }
+    *best = bo;
+    if (best_ms)
+        *best_ms = bms;
     return KS_OK;
 }
 

@@ -125,8 +125,10 @@ ks_status ks_procedural_scene(const char *kind, uint64_t seed, const ks_procedur
             o.prototypes = opts->prototypes;
         if (opts->instances)
             o.instances = opts->instances;
-        if (opts->frequency)
+        if (opts->frequency) {
             o.frequency = opts->frequency;
+            o.geodesic_sphere = true;
+        }
         if (opts->emitters)
             o.emitters = opts->emitters;
     }

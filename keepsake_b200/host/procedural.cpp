@@ -4,7 +4,8 @@
 //   "box_room"   5 axis-aligned wall quads + 2 boxes rotated about y by U[0,90) deg + a 2-triangle
 //                area light of radiance (17,12,4); diffuse principled materials, basecolor
 //                U[0.1,0.9]^3.
-//   "icosphere"  icosphere subdivided `level` times (20*4^level triangles) with seeded fBm radial
+//   "icosphere"  icosphere subdivided `level` times (20*4^level triangles; or, given a frequency f,
+//                a geodesic sphere of 20 f^2 triangles) with seeded fBm radial
 //                displacement (amplitude 0.05) on a ground quad; one principled material per
 //                1024-triangle patch (roughness U[r0,r1], metallic Bernoulli(0.3), basecolor
 //                U[0,1]^3); a procedural lat-long HDR sky (gradient + sun lobe of 1e4).
@@ -212,6 +213,8 @@ struct Noise3
 };
 
 // ---- icosphere -----------------------------------------------------------------------------
+void geodesic(uint32_t f, std::vector<V3> &verts, std::vector<uint32_t> &tris);
+
 void icosphere(int level, std::vector<V3> &verts, std::vector<uint32_t> &tris)
 {
     const double t = (1.0 + std::sqrt(5.0)) / 2.0;
@@ -288,7 +291,10 @@ void gen_icosphere_scene(GeneratedScene &g, uint64_t seed, const ProceduralOptio
     Noise3 noise(rng);
     std::vector<V3> verts;
     std::vector<uint32_t> tris;
-    icosphere(o.level, verts, tris);
+    if (o.geodesic_sphere)
+        geodesic(std::max(1u, o.frequency), verts, tris);
+    else
+        icosphere(o.level, verts, tris);
     for (auto &v : verts) {
         double d = noise.fbm(3.0 * v + V3{17.3, 5.1, 9.7}, 6);
         v = (1.0 + 0.05 * d) * v;

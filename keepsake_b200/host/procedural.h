@@ -25,6 +25,7 @@ struct ProceduralOptions
     uint32_t instances = 400;
     uint32_t frequency = 50;
     uint32_t emitters = 64;
+    bool geodesic_sphere = false; // "icosphere": a geodesic sphere of `frequency` instead of `level`
 };
 
 struct GeneratedMesh
