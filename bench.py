@@ -53,6 +53,10 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=None, help="steps of the end-to-end leg (default: --steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ttr", action="store_true", help="skip the time-to-relMSE leg")
+    ap.add_argument("--no-c4", action="store_true", help="skip the batched multi-scene leg")
+    ap.add_argument("--c4-spp-div", type=int, default=8, help="divides the spp of every batched job")
+    ap.add_argument("--no-c5", action="store_true", help="skip the instanced-scene leg")
+    ap.add_argument("--c5-spp", type=int, default=16)
     # reduced frames of the same scene, for profiling captures only (not a bench line)
     ap.add_argument("--spp", type=int, default=None)
     ap.add_argument("--res", type=int, default=None)
@@ -177,6 +181,84 @@ def time_to_relmse(ks, ctx, torch, with_cpu, guide_options=None, guide_params=No
                       "sample": f"full {TTR_W}x{TTR_H} frame at 1 spp ({n} paths, {int(cnt[0]) + int(cnt[1])} rays)"}
     sc.close()
     return res
+
+
+def batched_leg(ks, ctx, torch, spp_div):
+    """C4: 64 seeded scenes built like the icosphere frame (geodesic spheres, triangles
+    log-uniform in [1e4, 2e6]), resolutions from {256^2, 512^2, 1024^2, 1920x1080}, spp from
+    {32 .. 512} divided by spp_div; one autotuned batch (one CUDA graph launch) against the same
+    jobs rendered one after another."""
+    import numpy as np
+    rng = np.random.default_rng(4)
+    resolutions = [(256, 256), (512, 512), (1024, 1024), (1920, 1080)]
+    jobs, keep, tris = [], [], []
+    for k in range(64):
+        n = float(np.exp(rng.uniform(np.log(1e4), np.log(2e6))))
+        f = max(1, int(round(np.sqrt(n / 20.0))))
+        W, H = resolutions[int(rng.integers(0, 4))]
+        spp = max(1, int(2 ** rng.integers(5, 10)) // spp_div)
+        g = ks.Generated("icosphere", 100 + k, frequency=f, sky=(2048, 1024), resolution=(W, H))
+        s = ks.Scene(ctx, g.desc, keepalive=g)
+        s.build_bvh()
+        cam = ks.camera_perspective(g.camera_to_world, g.vfov, g.aspect)
+        p = ks.SmallPTParams.make(render_width=W, render_height=H, spp=spp, bounces=BOUNCES, rng_seed=k)
+        acc = torch.zeros((H, W, 3), dtype=torch.float64, device="cuda")
+        wts = torch.zeros((H, W, 2), dtype=torch.float64, device="cuda")
+        jobs.append((s, cam, p, acc, wts))
+        keep.append(g)
+        tris.append(g.n_triangles)
+    desc = [(s, c, p, a.data_ptr(), w.data_ptr()) for s, c, p, a, w in jobs]
+    t0 = time.perf_counter()
+    opts, tune_ms = ks.batch_autotune(ctx, desc)
+    tune_s = time.perf_counter() - t0
+    for _, _, _, a, w in jobs:
+        a.zero_()
+        w.zero_()
+    st = ks.batch_render(ctx, desc, capacity=opts.capacity, grid_per_sm=opts.grid_per_sm, use_graph=True)
+    seq_ms, seq_rays = 0.0, 0
+    for s, c, p, a, w in jobs:
+        s.render_device(c, p, a.data_ptr(), w.data_ptr())
+        ss = s.stats()
+        seq_ms += ss.ms_total
+        seq_rays += ss.extension_rays + ss.shadow_rays
+    for s, *_ in jobs:
+        s.close()
+    rays = st.extension_rays + st.shadow_rays
+    return {"workload": f"64 seeded geodesic-sphere scenes ({min(tris)}..{max(tris)} triangles, log-uniform), "
+                        f"resolutions from 256^2/512^2/1024^2/1920x1080, spp 32..512 / {spp_div}, depth {BOUNCES}",
+            "paths": st.paths, "pixels": sum(p.render_width * p.render_height for _, _, p, _, _ in jobs),
+            "batched": {"ms": st.ms_total, "mrays_per_s": rays / st.ms_total / 1e3,
+                        "mpaths_per_s": st.paths / st.ms_total / 1e3, "graph_launches": st.graph_launches,
+                        "iterations": st.iterations, "capacity": opts.capacity, "grid_per_sm": opts.grid_per_sm,
+                        "autotune_s": tune_s, "autotune_best_sample_ms": tune_ms},
+            "sequential": {"ms": seq_ms, "mrays_per_s": seq_rays / seq_ms / 1e3},
+            "speedup": seq_ms / st.ms_total if st.ms_total > 0 else None}
+
+
+def instanced_leg(ks, ctx, torch, spp):
+    """C5: 400 instances of 8 displaced geodesic spheres (50k triangles each) + 64 emitters + the
+    sky, 3840x2160, depth 16, at `spp` samples per pixel."""
+    g = ks.Generated("instanced", 0, sky=(2048, 1024), resolution=(3840, 2160))
+    s = ks.Scene(ctx, g.desc, keepalive=g)
+    build_ms = s.build_bvh()
+    cam = ks.camera_perspective(g.camera_to_world, g.vfov, g.aspect)
+    p = ks.SmallPTParams.make(render_width=3840, render_height=2160, spp=spp, bounces=16)
+    acc = torch.zeros((2160, 3840, 3), dtype=torch.float64, device="cuda")
+    wts = torch.zeros((2160, 3840, 2), dtype=torch.float64, device="cuda")
+    s.render_device(cam, ks.SmallPTParams.make(render_width=3840, render_height=2160, spp=1, bounces=16),
+                    acc.data_ptr(), wts.data_ptr())
+    acc.zero_()
+    wts.zero_()
+    s.render_device(cam, p, acc.data_ptr(), wts.data_ptr())
+    st = s.stats()
+    s.close()
+    flat = sum(len(g.meshes[first + k]["indices"]) for proto, _ in g.instances
+               for first, n in [g.prototypes[proto]] for k in range(n))
+    return {"workload": f"400 instances x 8 geodesic spheres (50,000 triangles each) + 64 emitters + ground, "
+                        f"3840x2160, {spp} spp, depth 16",
+            "unique_triangles": g.n_triangles, "instanced_triangles": flat, "bvh_build_ms": build_ms,
+            "ms": st.ms_total, "mrays_per_s": (st.extension_rays + st.shadow_rays) / st.ms_total / 1e3,
+            "mpaths_per_s": st.paths / st.ms_total / 1e3}
 
 
 def cpu_crop_params(ks, crop=CPU_CROP):
@@ -318,7 +400,8 @@ def main():
     # replicas: each rank renders the full frame with its own sampler seed
     params = ks.SmallPTParams.make(render_width=W_RES, render_height=H_RES, spp=SPP, bounces=BOUNCES, rng_seed=rank)
     scene = ks.Scene(ctx, g.desc)
-    build_ms = scene.build_bvh()
+    # GPU SBVH build time: median of warm rebuilds (the first build also loads the builder's kernels)
+    build_ms = statistics.median([scene.build_bvh() for _ in range(4)][1:])
     acc = torch.zeros((H_RES, W_RES, 3), dtype=torch.float64, device="cuda")
     wts = torch.zeros((H_RES, W_RES, 2), dtype=torch.float64, device="cuda")
 
@@ -381,7 +464,7 @@ def main():
     h2d += len(g.materials) * 72 + (g.sky_map.nbytes if g.sky_map is not None else 0)
     d2h = W_RES * H_RES * 5 * 8
     e2e_rays, e2e_t = 0, 0.0
-    for k in range(e2e_steps):
+    for k in range(e2e_steps + 1):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         sc = ks.Scene(ctx, g.desc)
@@ -389,6 +472,8 @@ def main():
         sc.render(cam, params)
         st = sc.stats()
         sc.close()
+        if k == 0:
+            continue  # untimed warm-up step
         e2e_t += time.perf_counter() - t0
         e2e_rays += st.extension_rays + st.shadow_rays
     if pg:
@@ -408,9 +493,13 @@ def main():
         cpu = {"value": r["rays"] / r["seconds"] / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "port",
                "sample": r["sample"] + "; oracle restatement of small_pt over the reference cuda/sbvh.cu traversal"}
 
-    ttr = None
+    ttr = c4 = c5 = None
     if rank == 0 and world == 1 and not args.no_ttr:
         ttr = time_to_relmse(ks, ctx, torch, not args.no_cpu_baseline)
+    if rank == 0 and world == 1 and not args.no_c4:
+        c4 = batched_leg(ks, ctx, torch, max(1, args.c4_spp_div))
+    if rank == 0 and world == 1 and not args.no_c5:
+        c5 = instanced_leg(ks, ctx, torch, max(1, args.c5_spp))
 
     if rank == 0:
         line = {
@@ -430,6 +519,8 @@ def main():
             "gpu_launches": sum(s.kernel_launches for s in stats),
             "clocks": clk,
             "time_to_relmse": ttr,
+            "batched": c4,
+            "instanced": c5,
         }
         print(json.dumps(line), flush=True)
     scene.close()

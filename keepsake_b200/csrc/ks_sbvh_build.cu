@@ -866,8 +866,10 @@ struct RangeOut
     float bound[6] = {0, 0, 0, 0, 0, 0};
 };
 
+// `done` (may be null) is recorded on the stream after the last build kernel, before the scratch
+// buffers are released.
 static ks_status build_range(ks_context *ctx, const float *verts, const uint32_t *indices, uint32_t tri_begin,
-                             uint32_t n_tris, const Params &p, RangeOut &out)
+                             uint32_t n_tris, const Params &p, RangeOut &out, cudaEvent_t done = nullptr)
 {
     cudaStream_t st = ctx->stream;
 
@@ -1020,6 +1022,8 @@ static ks_status build_range(ks_context *ctx, const float *verts, const uint32_t
     k_prim_tris<<<grid_for(pool_used, 256), 256, 0, st>>>(out.prims.ptr, pool_used, verts, indices,
                                                           out.prim_tris.ptr);
     KS_CUDA_TRY(ctx, cudaGetLastError());
+    if (done)
+        KS_CUDA_TRY(ctx, cudaEventRecord(done, st));
     RefNode root_node;
     KS_CUDA_TRY(ctx, cudaMemcpyAsync(&root_node, out.ref_nodes.ptr, sizeof(RefNode), cudaMemcpyDeviceToHost, st));
     KS_CUDA_TRY(ctx, cudaStreamSynchronize(st));
@@ -1272,9 +1276,11 @@ ks_status build_sbvh(ks_scene *scene, const ks_sbvh_options &o, float *build_ms)
     ks_status s = KS_OK;
     if (scene->n_instances > 0) {
         s = build_instanced(scene, p);
+        if (s == KS_OK)
+            cudaEventRecord(ev1, st);
     } else {
         RangeOut r;
-        s = build_range(ctx, scene->verts.ptr, scene->indices.ptr, 0, scene->n_tris, p, r);
+        s = build_range(ctx, scene->verts.ptr, scene->indices.ptr, 0, scene->n_tris, p, r, ev1);
         if (s == KS_OK) {
             scene->ref_nodes.swap(r.ref_nodes);
             scene->prims.swap(r.prims);
@@ -1289,7 +1295,6 @@ ks_status build_sbvh(ks_scene *scene, const ks_sbvh_options &o, float *build_ms)
         }
     }
     float ms = 0;
-    cudaEventRecord(ev1, st);
     cudaEventSynchronize(ev1);
     cudaEventElapsedTime(&ms, ev0, ev1);
     cudaEventDestroy(ev0);
