@@ -56,6 +56,9 @@ def parse():
     ap.add_argument("--no-c4", action="store_true", help="skip the batched multi-scene leg")
     ap.add_argument("--c4-spp-div", type=int, default=8, help="divides the spp of every batched job")
     ap.add_argument("--no-c5", action="store_true", help="skip the instanced-scene leg")
+    ap.add_argument("--profile-guided", action="store_true",
+                    help="profiling case only: one guided render of the glossy occluded scene at --res x "
+                         "(--res * 9 / 16), --spp samples (default 16), then exit")
     ap.add_argument("--c5-spp", type=int, default=16)
     # reduced frames of the same scene, for profiling captures only (not a bench line)
     ap.add_argument("--spp", type=int, default=None)
@@ -395,6 +398,27 @@ def main():
     import keepsake_b200 as ks
 
     ctx = ks.Context(local_rank)
+    if args.profile_guided:
+        W = args.res or 512
+        H = W * 9 // 16
+        gg = ks.Generated("icosphere", 0, level=8, sky=(2048, 1024), resolution=(W, H), roughness=(0.02, 0.2),
+                          occluder=True)
+        sc = ks.Scene(ctx, gg.desc, keepalive=gg)
+        sc.build_bvh()
+        lo, hi = gg.bound
+        guide = ks.Guide(ctx, list(lo - 0.05) + list(hi + 0.05), seed=1)
+        pp = ks.SmallPTParams.make(render_width=W, render_height=H, spp=args.spp or 16, bounces=BOUNCES,
+                                   spp_prog_interval=1)
+        opts = ks.GuideRenderOptions.make(train_passes=1 << 20, train_batch=1 << 16, max_records=1 << 17)
+        acc = torch.zeros((H, W, 3), dtype=torch.float64, device="cuda")
+        wts = torch.zeros((H, W, 2), dtype=torch.float64, device="cuda")
+        cam = ks.camera_perspective(gg.camera_to_world, gg.vfov, gg.aspect)
+        sc.render_guided_device(cam, pp, guide, opts, acc.data_ptr(), wts.data_ptr())
+        print(json.dumps({"profile_case": "guided", "resolution": [W, H], "stats": sc.stats().as_dict()}))
+        guide.close()
+        sc.close()
+        ctx.close()
+        return 0
     g = make_generated(ks)
     cam = ks.camera_perspective(g.camera_to_world, g.vfov, g.aspect)
     # replicas: each rank renders the full frame with its own sampler seed
