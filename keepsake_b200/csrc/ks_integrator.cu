@@ -65,6 +65,30 @@ struct ShadowBuf
 
 constexpr uint32_t kTermBit = 0x80000000u;
 
+// Minimum resident CTAs per SM asked of the compiler (a register cap) for the hit-shading and the
+// persistent traversal kernels.  Both are latency bound: at 10 CTAs of 128 (48 registers, a few
+// hundred bytes of spills) the shading kernel runs about 1.25x faster than at its natural 113
+// registers (4 CTAs); the traversal kernels gain a little at 8 (64 registers).
+#ifndef KS_SHADE_MIN_BLOCKS
+#define KS_SHADE_MIN_BLOCKS 10
+#endif
+#ifndef KS_TRAV_MIN_BLOCKS
+#define KS_TRAV_MIN_BLOCKS 8
+#endif
+// Persistent traversal with dynamic ray fetch (1) or one thread per ray (0) for flat scenes.
+#ifndef KS_PERSISTENT_TRAV
+#define KS_PERSISTENT_TRAV 1
+#endif
+constexpr bool kPersistentTraversal = KS_PERSISTENT_TRAV != 0;
+// Path slots of a single-frame wavefront (log2).
+#ifndef KS_WAVE_LOG2
+#define KS_WAVE_LOG2 22
+#endif
+
+// Per-iteration counters: paths continuing, shadow rays, hit queue, miss queue, extension-ray
+// fetch, shadow-ray fetch.
+constexpr uint32_t kCounters = 6;
+
 // ---- batched rendering: many (scene, camera, params) jobs in one wavefront --------------------
 // A path's job id rides in bits 21..30 of its pixel word (per-job frames of at most 2^21 pixels,
 // up to 1024 jobs); the scene view, render parameters and accumulators of a job are read from
@@ -147,14 +171,20 @@ KS_D void reortho(f3 &t, f3 &b, f3 &n)
     b = bb;
 }
 
+// Hit point from the barycentrics of vertices 1 and 2 (geometry.cpp:68-163).
+KS_D f3 hit_point(f3 p0, f3 p1, f3 p2, float u, float v)
+{
+    float w0 = 1.0f - u - v;
+    return w0 * p0 + u * p1 + v * p2;
+}
+
 KS_D ShadeFrame make_frame(f3 p0, f3 p1, f3 p2, float u, float v, f3 ray_dir, bool twosided)
 {
     ShadeFrame f;
     f3 rd = normalize(ray_dir);
     f3 wo_object = -rd;
     f3 ng = normalize(cross(p1 - p0, p2 - p0));
-    float w0 = 1.0f - u - v;
-    f.p = w0 * p0 + u * p1 + v * p2;
+    f.p = hit_point(p0, p1, p2, u, v);
     f3 dpdu = p1 - p0;
     f3 b = normalize(cross(ng, dpdu));
     f3 t = normalize(cross(b, ng));
@@ -328,7 +358,8 @@ __global__ void k_batch_prep(BatchState *st, uint32_t *counters, uint32_t capaci
     s.issued += n_new;
     s.count = alive + n_new;
     s.ext_rays += s.count;
-    counters[0] = counters[1] = counters[2] = counters[3] = 0;
+    for (uint32_t k = 0; k < kCounters; ++k)
+        counters[k] = 0;
 }
 
 // Batched iteration tail: counts the shadow rays and decides whether another iteration is
@@ -418,22 +449,117 @@ __global__ void __launch_bounds__(128) k_extend(const __grid_constant__ SceneVie
     flush_counts(tc, work);
 }
 
-// Sobol samples of one bounce for every path in the hit queue (whose bounce is below the limit):
-// light selection (dimension d), light uv (d+1, d+2), BSDF lobe (d+3), BSDF direction (d+4,
-// d+5) and Russian roulette (d+6), exactly as sample_with_nee + trace() draw them
-// (nee.cpp:28-34, material.cpp:157-158, small_pt.cpp:168-174).  Integer-only and uniform across
-// the warp, so it runs at full occupancy instead of inside the divergent shading kernel.
-// samples[2 * i] = (light, light u, light v, lobe), samples[2 * i + 1] = (wi u, wi v, roulette, -)
+// ---- persistent traversal with dynamic ray fetch (flat scenes) --------------------------------
+// One thread per ray leaves a warp running until its longest ray ends (about 5 of 32 lanes stay
+// busy on average).  k_extend_pt and k_shadow_pt keep the lanes busy instead (warp_fetch and
+// trav_step, ks_traverse.cuh).  The grid is one wave of resident CTAs; the fetch counters restart
+// every iteration.
+
+// Closest hit of every queued ray into hits[i] (slot ~0u: miss); k_build_queues then sorts the
+// paths into the hit and miss queues in index order, so that shading reads the path state in
+// order.  kBatch: paths of many jobs, the count read from the batch state.
 template <bool kBatch = false>
-__global__ void __launch_bounds__(128) k_sample(const __grid_constant__ RenderParams rp_in, PathBuf cur,
-                                                const uint32_t *queue, const uint32_t *queue_count, float4 *samples,
-                                                BatchView bv)
+__global__ void __launch_bounds__(128, KS_TRAV_MIN_BLOCKS) k_extend_pt(const __grid_constant__ SceneView sv_in, PathBuf pb, uint32_t count,
+                                                   float4 *hits, uint32_t *fetch, int *overflow,
+                                                   unsigned long long *work, BatchView bv)
+{
+    if constexpr (kBatch)
+        count = bv.state->count;
+    TravCount tc;
+    uint4 stack[kStackDepth];
+    TravState s;
+    const TravNode *nodes = sv_in.nodes;
+    const float4 *tris = sv_in.prim_tris;
+    uint32_t ray = ~0u;
+    bool drained = false;
+    int of = 0;
+    while (true) {
+        const uint32_t id = warp_fetch(fetch, count, ray == ~0u, drained);
+        if (id != ~0u) {
+            const uint32_t job = kBatch ? (bits(pb.beta_pix[id].w) >> kJobShift) : 0u;
+            const SceneView &sv = job_of<kBatch>(sv_in, bv.views, job);
+            nodes = sv.nodes;
+            tris = sv.prim_tris;
+            float4 a = pb.o_pdf[id], b = pb.d_info[id];
+            RayQuery q;
+            q.o = mk(a.x, a.y, a.z);
+            q.d = mk(b.x, b.y, b.z);
+            q.tmin = 0.0f;
+            q.tmax = kInf;
+            if (trav_begin(s, q, sv.root_ref, sv.root_count, sv.bmin, sv.bmax))
+                ray = id;
+            else
+                hits[id] = make_float4(0, 0, 0, fbits(~0u));
+        }
+        if (__ballot_sync(0xffffffffu, ray != ~0u) == 0) {
+            if (drained)
+                break;
+            continue;
+        }
+        while (true) {
+            if (ray != ~0u && trav_step<false>(nodes, tris, s, stack, 2, of, &tc)) {
+                hits[ray] = s.hit.tri != ~0u ? make_float4(s.hit.t, s.hit.b1, s.hit.b2, fbits(s.hit.slot))
+                                             : make_float4(0, 0, 0, fbits(~0u));
+                ray = ~0u;
+            }
+            const int n_idle = __popc(__ballot_sync(0xffffffffu, ray == ~0u));
+            if (n_idle == 32 || (!drained && n_idle >= KS_TRAV_REFILL))
+                break;
+        }
+    }
+    if (of)
+        atomicOr(overflow, 1);
+    flush_counts(tc, work);
+}
+
+// Hit and miss queues from the per-ray results of k_extend_pt, one warp-aggregated append per
+// kind (queue order follows the path index, warp by warp).
+template <bool kBatch = false>
+__global__ void __launch_bounds__(256) k_build_queues(const float4 *hits, uint32_t count, uint32_t *hit_queue,
+                                                      uint32_t *miss_queue, uint32_t *queue_counts, BatchView bv)
+{
+    if constexpr (kBatch)
+        count = bv.state->count;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t *slot = reinterpret_cast<const uint32_t *>(hits) + 3;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += stride) {
+        const uint32_t i = base + threadIdx.x;
+        const bool valid = i < count;
+        const bool is_hit = valid && slot[4 * (size_t)i] != ~0u;
+        const uint32_t jh = warp_append(queue_counts, is_hit);
+        const uint32_t jm = warp_append(queue_counts + 1, valid && !is_hit);
+        if (valid) {
+            if (is_hit)
+                hit_queue[jh] = i;
+            else
+                miss_queue[jm] = i;
+        }
+    }
+}
+
+// Sobol samples and the NEE light sample of one bounce for every path in the hit queue (whose
+// bounce is below the limit).  Sobol dimensions: light selection (d), light uv (d+1, d+2), BSDF
+// lobe (d+3), BSDF direction (d+4, d+5) and Russian roulette (d+6), exactly as sample_with_nee +
+// trace() draw them (nee.cpp:28-34, material.cpp:157-158, small_pt.cpp:168-174).  The light is
+// selected and sampled here too (next_event_estimate, nee.cpp:28-40), so the shading kernel keeps
+// only the BSDF work: this kernel runs at full occupancy and SIMT efficiency, and the sky's
+// binary searches no longer sit in the large shading kernel.
+// samples[4 i + 0] = (lobe, wi u, wi v, roulette)
+// samples[4 i + 1] = (light direction, light distance)
+// samples[4 i + 2] = (Le / pdf of the light sample (Le_beta), pdf of the direction)
+// samples[4 i + 3] = (light selection probability, -, -, -)
+template <bool kBatch = false>
+__global__ void __launch_bounds__(128) k_sample(const __grid_constant__ SceneView sv_in,
+                                                const __grid_constant__ RenderParams rp_in, PathBuf cur,
+                                                const float4 *hits, const uint32_t *hit_inst, const uint32_t *queue,
+                                                const uint32_t *queue_count, float4 *samples, BatchView bv)
 {
     const uint32_t count = *queue_count;
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x) {
         uint32_t i = queue[q];
         uint32_t pix = bits(cur.beta_pix[i].w), smp = bits(cur.L_smp[i].w);
-        const RenderParams &rp = job_of<kBatch>(rp_in, bv.params, pix >> kJobShift);
+        const uint32_t job = kBatch ? (pix >> kJobShift) : 0u;
+        const RenderParams &rp = job_of<kBatch>(rp_in, bv.params, job);
         if constexpr (kBatch)
             pix &= kPixMask;
         uint32_t info = bits(cur.d_info[i].w);
@@ -441,17 +567,51 @@ __global__ void __launch_bounds__(128) k_sample(const __grid_constant__ RenderPa
         if (bounce == rp.bounces)
             continue;
         int dim = (int)(info >> 16);
-        SobolSampler s = SobolSampler::start(pix % (uint32_t)rp.W, pix / (uint32_t)rp.W, smp, rp.log2_spp,
-                                             rp.n_digits, (uint32_t)rp.seed, dim);
-        float a = s.next();
-        float b, c;
-        s.next2d(b, c);
-        float d = s.next();
-        float e, f;
-        s.next2d(e, f);
-        float g = s.next();
-        samples[2 * (size_t)i] = make_float4(a, b, c, d);
-        samples[2 * (size_t)i + 1] = make_float4(e, f, g, 0.0f);
+        SobolSampler smp_s = SobolSampler::start(pix % (uint32_t)rp.W, pix / (uint32_t)rp.W, smp, rp.log2_spp,
+                                                 rp.n_digits, (uint32_t)rp.seed, dim);
+        float ul = smp_s.next();
+        float u0, u1;
+        smp_s.next2d(u0, u1);
+        float u_lobe = smp_s.next();
+        float b0, b1;
+        smp_s.next2d(b0, b1);
+        float u_rr = smp_s.next();
+        // next_event_estimate: light selection and the light's sample (nee.cpp:28-40)
+        const SceneView &sv = job_of<kBatch>(sv_in, bv.views, job);
+        uint32_t light = cdf_find(sv.power_cdf, sv.light_count, clamp_u(ul));
+        float pr_light = sv.power_cdf[light + 1] - sv.power_cdf[light];
+        f3 wi = mk(0, 0, 0);
+        float wi_dist = 0.0f, pdf_wi_light = 0.0f;
+        f3 Le_beta;
+        if (light < sv.n_nonmesh) {
+            Le_beta = sky_sample(sv, u0, u1, wi, wi_dist, pdf_wi_light);
+        } else {
+            // the shading point as the hit record computes it (make_frame)
+            const float4 h = hits[i];
+            const float4 *pt = sv.prim_tris + 3 * (size_t)bits(h.w);
+            float4 v0 = __ldg(pt), v1 = __ldg(pt + 1), v2 = __ldg(pt + 2);
+            f3 p0 = mk(v0.x, v0.y, v0.z), p1 = mk(v1.x, v1.y, v1.z), p2 = mk(v2.x, v2.y, v2.z);
+            if (sv.inst.n) {
+                const uint32_t inst = hit_inst[i];
+                float m[12];
+#pragma unroll
+                for (int e = 0; e < 12; ++e)
+                    m[e] = __ldg(&sv.inst.xf[12 * (size_t)inst + e]);
+                p0 = xf_point(m, p0);
+                p1 = xf_point(m, p1);
+                p2 = xf_point(m, p2);
+            }
+            const f3 p = hit_point(p0, p1, p2, h.y, h.z);
+            uint32_t k = light - sv.n_nonmesh;
+            const float4 *mv = sv.ml_verts + 3 * (size_t)k;
+            float4 a0 = __ldg(mv), a1 = __ldg(mv + 1), a2 = __ldg(mv + 2);
+            TriVerts tv{mk(a0.x, a0.y, a0.z), mk(a1.x, a1.y, a1.z), mk(a2.x, a2.y, a2.z)};
+            Le_beta = mesh_light_sample(sv, k, tv, p, u0, u1, wi, wi_dist, pdf_wi_light);
+        }
+        samples[4 * (size_t)i] = make_float4(u_lobe, b0, b1, u_rr);
+        samples[4 * (size_t)i + 1] = make_float4(wi.x, wi.y, wi.z, wi_dist);
+        samples[4 * (size_t)i + 2] = make_float4(Le_beta.x, Le_beta.y, Le_beta.z, pdf_wi_light);
+        samples[4 * (size_t)i + 3] = make_float4(pr_light, 0.0f, 0.0f, 0.0f);
     }
 }
 
@@ -466,7 +626,7 @@ __global__ void __launch_bounds__(128) k_sample(const __grid_constant__ RenderPa
 // the direction if both keep seeing the BSDF pdf.
 // kBatch: paths of many jobs; the view, parameters and accumulators of a path's job come from bv.
 template <bool kMiss, bool kGuided, bool kBatch = false>
-__global__ void __launch_bounds__(128) k_shade(const __grid_constant__ SceneView sv_in,
+__global__ void __launch_bounds__(128, KS_SHADE_MIN_BLOCKS) k_shade(const __grid_constant__ SceneView sv_in,
                                                const __grid_constant__ RenderParams rp_in, PathBuf cur, PathBuf nxt,
                                                const float4 *hits, const uint32_t *hit_inst,
                                                const float4 *samples, const uint32_t *queue,
@@ -584,30 +744,14 @@ __global__ void __launch_bounds__(128) k_shade(const __grid_constant__ SceneView
                 } else {
                     f3 wo = -normalize(rd);
                     Principled bsdf{make_closure(mat)};
-                    // this bounce's Sobol values, drawn by k_sample
-                    const float4 sa = samples[2 * (size_t)i], sc = samples[2 * (size_t)i + 1];
-                    // next_event_estimate (nee.cpp:11-57)
-                    float ul = sa.x;
-                    uint32_t light = cdf_find(sv.power_cdf, sv.light_count, clamp_u(ul));
-                    float pr_light = sv.power_cdf[light + 1] - sv.power_cdf[light];
-                    float u0 = sa.y, u1 = sa.z;
-                    f3 wi = mk(0, 0, 0);
-                    float wi_dist = 0.0f, pdf_wi_light = 0.0f;
-                    f3 Le_beta;
-                    if (light < sv.n_nonmesh) {
-                        Le_beta = sky_sample(sv, u0, u1, wi, wi_dist, pdf_wi_light);
-                    } else {
-                        uint32_t k = light - sv.n_nonmesh;
-                        TriVerts tv{mk(0, 0, 0), mk(0, 0, 0), mk(0, 0, 0)};
-                        {
-                            const float4 *mv = sv.ml_verts + 3 * (size_t)k;
-                            float4 a0 = __ldg(mv), a1 = __ldg(mv + 1), a2 = __ldg(mv + 2);
-                            tv.v0 = mk(a0.x, a0.y, a0.z);
-                            tv.v1 = mk(a1.x, a1.y, a1.z);
-                            tv.v2 = mk(a2.x, a2.y, a2.z);
-                        }
-                        Le_beta = mesh_light_sample(sv, k, tv, it.p, u0, u1, wi, wi_dist, pdf_wi_light);
-                    }
+                    // this bounce's Sobol values and light sample, drawn by k_sample
+                    const float4 sa = samples[4 * (size_t)i], sl = samples[4 * (size_t)i + 1];
+                    const float4 se = samples[4 * (size_t)i + 2];
+                    const float pr_light = samples[4 * (size_t)i + 3].x;
+                    // next_event_estimate (nee.cpp:11-57): the light sample's BSDF term and MIS
+                    const f3 wi = mk(sl.x, sl.y, sl.z);
+                    const float wi_dist = sl.w, pdf_wi_light = se.w;
+                    const f3 Le_beta = mk(se.x, se.y, se.z);
                     if (!is_zero(Le_beta) && pdf_wi_light > 0.0f) {
                         f3 wo_l = sh_to_local(it, wo), wi_l = sh_to_local(it, wi);
                         f3 f;
@@ -626,8 +770,8 @@ __global__ void __launch_bounds__(128) k_shade(const __grid_constant__ SceneView
                     }
                     // BSDF sampling (material.cpp:155-166)
                     f3 wo_local = sh_to_local(it, wo);
-                    float u_lobe = sa.w;
-                    float b0 = sc.x, b1 = sc.y;
+                    float u_lobe = sa.x;
+                    float b0 = sa.y, b1 = sa.z;
                     int next_dim = dim + 6;
                     f3 wi_local;
                     float pdf_wi = 0.0f;
@@ -675,7 +819,7 @@ __global__ void __launch_bounds__(128) k_shade(const __grid_constant__ SceneView
                             float q = 1.0f - max3(nbeta);
                             q = q < 0.0f ? 0.0f : q;
                             next_dim = dim + 7;
-                            if (sc.z < q)
+                            if (sa.w < q)
                                 finish = true;
                             else
                                 nbeta /= 1.0f - q;
@@ -805,6 +949,89 @@ __global__ void __launch_bounds__(128) k_shadow(const __grid_constant__ SceneVie
     flush_counts(tc, work);
 }
 
+// Completion of shadow ray i: records, then the contribution goes to the continuing path or, for a
+// path that ended this bounce, the path is accumulated.
+template <bool kBatch>
+KS_D void shadow_done(const ShadowBuf &sb, uint32_t i, bool occ, PathBuf nxt, double *accum_in, double *weights_in,
+                      const GuideView &gv, const BatchView &bv)
+{
+    const float4 c = sb.contrib[i];
+    const uint32_t target = bits(sb.d_target[i].w);
+    const uint32_t job = kBatch ? bits(c.w) : 0u;
+    if (gv.rec_cap && !occ && bits(c.w) != kNoRecord)
+        record_add(gv, bits(c.w), mk(c.x, c.y, c.z));
+    if (target & kTermBit) {
+        double *accum = kBatch ? bv.accum[job] : accum_in;
+        double *weights = kBatch ? bv.weights[job] : weights_in;
+        float4 l = sb.L_term[i];
+        f3 L = mk(l.x, l.y, l.z);
+        if (!occ)
+            L += mk(c.x, c.y, c.z);
+        accumulate(accum, weights, kBatch ? (target & kPixMask) : (target & ~kTermBit), L);
+    } else if (!occ) {
+        float4 l = nxt.L_smp[target];
+        l.x += c.x;
+        l.y += c.y;
+        l.z += c.z;
+        nxt.L_smp[target] = l;
+    }
+}
+
+// Any-hit traversal of the NEE shadow rays with dynamic ray fetch (flat scenes); each ray is
+// finished by shadow_done as soon as its traversal ends.
+template <bool kBatch = false>
+__global__ void __launch_bounds__(128, KS_TRAV_MIN_BLOCKS) k_shadow_pt(const __grid_constant__ SceneView sv_in, ShadowBuf sb,
+                                                   const uint32_t *shadow_count, uint32_t *fetch, PathBuf nxt,
+                                                   double *accum_in, double *weights_in, int *overflow,
+                                                   unsigned long long *work, GuideView gv, BatchView bv)
+{
+    const uint32_t count = *shadow_count;
+    TravCount tc;
+    uint4 stack[kStackDepth];
+    TravState s;
+    const TravNode *nodes = sv_in.nodes;
+    const float4 *tris = sv_in.prim_tris;
+    uint32_t ray = ~0u;
+    bool drained = false;
+    int of = 0;
+    while (true) {
+        const uint32_t id = warp_fetch(fetch, count, ray == ~0u, drained);
+        if (id != ~0u) {
+            const uint32_t job = kBatch ? bits(sb.contrib[id].w) : 0u;
+            const SceneView &sv = job_of<kBatch>(sv_in, bv.views, job);
+            nodes = sv.nodes;
+            tris = sv.prim_tris;
+            float4 a = sb.o_tmax[id], b = sb.d_target[id];
+            RayQuery q;
+            q.o = mk(a.x, a.y, a.z);
+            q.d = mk(b.x, b.y, b.z);
+            q.tmin = 0.0f;
+            q.tmax = a.w;
+            if (trav_begin(s, q, sv.root_ref, sv.root_count, sv.bmin, sv.bmax))
+                ray = id;
+            else
+                shadow_done<kBatch>(sb, id, false, nxt, accum_in, weights_in, gv, bv);
+        }
+        if (__ballot_sync(0xffffffffu, ray != ~0u) == 0) {
+            if (drained)
+                break;
+            continue;
+        }
+        while (true) {
+            if (ray != ~0u && trav_step<true>(nodes, tris, s, stack, 2, of, &tc)) {
+                shadow_done<kBatch>(sb, ray, s.hit.tri != ~0u, nxt, accum_in, weights_in, gv, bv);
+                ray = ~0u;
+            }
+            const int n_idle = __popc(__ballot_sync(0xffffffffu, ray == ~0u));
+            if (n_idle == 32 || (!drained && n_idle >= KS_TRAV_REFILL))
+                break;
+        }
+    }
+    if (of)
+        atomicOr(overflow, 1);
+    flush_counts(tc, work);
+}
+
 // Relative MSE of the composited image (RenderTarget2::composite_and_save_to_exr,
 // render_target.cpp:181-205) against a reference: sum over pixels and channels of
 // (x - r)^2 / (r^2 + eps), accumulated in FP64 (one atomic per warp).
@@ -835,14 +1062,24 @@ __global__ void k_rel_mse(const double *accum, const double *weights, const doub
 
 using namespace ksb;
 
+// One wave of resident CTAs of a persistent kernel.
+template <class Kernel>
+static unsigned resident_grid(Kernel kernel, int block, int sm_count)
+{
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    return (unsigned)per_sm * (unsigned)sm_count;
+}
+
 struct RenderWork
 {
     DevBuf<float4> state[2][4];
     DevBuf<float4> hits;
     DevBuf<uint32_t> hit_inst; // instanced scenes: instance of each hit
-    DevBuf<float4> samples; // 2 per path slot
+    DevBuf<float4> samples; // 4 per path slot
     DevBuf<float4> shadow[4];
-    DevBuf<uint32_t> counters; // [next, shadow, hit queue, miss queue]
+    DevBuf<uint32_t> counters; // [next, shadow, hit queue, miss queue, extension fetch, shadow fetch]
     DevBuf<uint32_t> queue[2]; // hit / miss path indices
     DevBuf<int> overflow;
     uint32_t capacity = 0;
@@ -919,19 +1156,19 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
     const uint32_t n_pix = (uint32_t)rp.cw * (uint32_t)rp.ch;
     const uint64_t max_interval = (uint64_t)n_pix * (uint64_t)std::min(in->spp, in->spp_prog_interval);
     RenderWork w;
-    w.capacity = (uint32_t)std::min<uint64_t>(max_interval, 1u << 22);
+    w.capacity = (uint32_t)std::min<uint64_t>(max_interval, 1u << KS_WAVE_LOG2);
     for (int b = 0; b < 2; ++b)
         for (int f = 0; f < 4; ++f)
             KS_CUDA_TRY(ctx, w.state[b][f].alloc(w.capacity));
     KS_CUDA_TRY(ctx, w.hits.alloc(w.capacity));
     if (scene->n_instances)
         KS_CUDA_TRY(ctx, w.hit_inst.alloc(w.capacity));
-    KS_CUDA_TRY(ctx, w.samples.alloc(2 * (size_t)w.capacity));
+    KS_CUDA_TRY(ctx, w.samples.alloc(4 * (size_t)w.capacity));
     KS_CUDA_TRY(ctx, w.queue[0].alloc(w.capacity));
     KS_CUDA_TRY(ctx, w.queue[1].alloc(w.capacity));
     for (int f = 0; f < 4; ++f)
         KS_CUDA_TRY(ctx, w.shadow[f].alloc(w.capacity));
-    KS_CUDA_TRY(ctx, w.counters.alloc(4));
+    KS_CUDA_TRY(ctx, w.counters.alloc(kCounters));
     KS_CUDA_TRY(ctx, w.overflow.alloc(1));
     DevBuf<unsigned long long> work; // ext nodes, ext tris, shadow nodes, shadow tris
     KS_CUDA_TRY(ctx, work.alloc(4));
@@ -989,6 +1226,8 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
     cudaEventRecord(t_begin, st);
     ks_render_stats stats{};
     const unsigned max_grid = (unsigned)ctx->sm_count * 16;
+    const unsigned ext_grid = resident_grid(k_extend_pt<false>, 128, ctx->sm_count);
+    const unsigned shadow_grid = resident_grid(k_shadow_pt<false>, 128, ctx->sm_count);
     int cur = 0;
     cudaError_t err = cudaSuccess;
     std::vector<double> cb_acc, cb_w;
@@ -1020,16 +1259,25 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
             issued += n_new;
             uint32_t count = cur_count + n_new;
             stats.extension_rays += count;
-            // counters: [0] next paths, [1] shadow rays, [2] hit queue, [3] miss queue
-            cudaMemsetAsync(w.counters.ptr, 0, sizeof(uint32_t) * 4, st);
+            // counters: [0] next paths, [1] shadow rays, [2] hit queue, [3] miss queue, [4], [5] ray fetch
+            cudaMemsetAsync(w.counters.ptr, 0, sizeof(uint32_t) * kCounters, st);
             unsigned grid = std::min<unsigned>((count + 127) / 128, max_grid);
             cudaEventRecord(ev[1], st);
             if (scene->n_instances)
                 k_extend<true><<<grid, 128, 0, st>>>(sv, pb[cur], count, w.hits.ptr, w.hit_inst.ptr, w.queue[0].ptr,
                                                      w.queue[1].ptr, w.counters.ptr + 2, w.overflow.ptr, work.ptr, BatchView{});
-            else
+            else if (!kPersistentTraversal)
                 k_extend<false><<<grid, 128, 0, st>>>(sv, pb[cur], count, w.hits.ptr, nullptr, w.queue[0].ptr,
-                                                      w.queue[1].ptr, w.counters.ptr + 2, w.overflow.ptr, work.ptr, BatchView{});
+                                                      w.queue[1].ptr, w.counters.ptr + 2, w.overflow.ptr, work.ptr,
+                                                      BatchView{});
+            else {
+                k_extend_pt<false><<<std::min(grid, ext_grid), 128, 0, st>>>(sv, pb[cur], count, w.hits.ptr,
+                                                                             w.counters.ptr + 4, w.overflow.ptr,
+                                                                             work.ptr, BatchView{});
+                k_build_queues<false><<<std::min((count + 255) / 256, max_grid), 256, 0, st>>>(
+                    w.hits.ptr, count, w.queue[0].ptr, w.queue[1].ptr, w.counters.ptr + 2, BatchView{});
+                stats.kernel_launches++;
+            }
             cudaEventRecord(ev[2], st);
             if (guide && gv.active) {
                 ks_status gs = guide_impl::infer_paths(guide, w.queue[0].ptr, w.counters.ptr + 2, pb[cur].o_pdf,
@@ -1042,7 +1290,8 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
                 stats.kernel_launches++;
             }
             cudaEventRecord(ev[5], st);
-            k_sample<<<grid, 128, 0, st>>>(rp, pb[cur], w.queue[0].ptr, w.counters.ptr + 2, w.samples.ptr, BatchView{});
+            k_sample<<<grid, 128, 0, st>>>(sv, rp, pb[cur], w.hits.ptr, w.hit_inst.ptr, w.queue[0].ptr,
+                                           w.counters.ptr + 2, w.samples.ptr, BatchView{});
             if (guide) {
                 k_shade<false, true><<<grid, 128, 0, st>>>(sv, rp, pb[cur], pb[1 - cur], w.hits.ptr, w.hit_inst.ptr, w.samples.ptr,
                                                            w.queue[0].ptr, w.counters.ptr + 2, w.counters.ptr, sb,
@@ -1064,9 +1313,13 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
             if (scene->n_instances)
                 k_shadow<true><<<grid, 128, 0, st>>>(sv, sb, w.counters.ptr + 1, pb[1 - cur], d_accum, d_weights,
                                                      w.overflow.ptr, work.ptr + 2, gv, BatchView{});
-            else
+            else if (!kPersistentTraversal)
                 k_shadow<false><<<grid, 128, 0, st>>>(sv, sb, w.counters.ptr + 1, pb[1 - cur], d_accum, d_weights,
                                                       w.overflow.ptr, work.ptr + 2, gv, BatchView{});
+            else
+                k_shadow_pt<false><<<std::min(grid, shadow_grid), 128, 0, st>>>(sv, sb, w.counters.ptr + 1, w.counters.ptr + 5,
+                                                                pb[1 - cur], d_accum, d_weights, w.overflow.ptr,
+                                                                work.ptr + 2, gv, BatchView{});
             cudaEventRecord(ev[4], st);
             stats.kernel_launches += 5;
             cudaMemcpyAsync(h_counts, w.counters.ptr, sizeof(uint32_t) * 2, cudaMemcpyDeviceToHost, st);
@@ -1184,6 +1437,7 @@ struct BatchWork
     DevBuf<double *> accum, weights;
     DevBuf<unsigned long long> path_begin;
     DevBuf<BatchState> state_dev;
+    unsigned ext_grid = 0, shadow_grid = 0; // one wave of resident CTAs of the traversal kernels
 };
 
 // Validates the jobs and fills the per-job tables; returns the total path count in *total.
@@ -1246,17 +1500,19 @@ static void batch_iteration(ks_context *ctx, BatchWork &w, const BatchView &bv, 
     const GuideView gv{};
     k_batch_prep<<<1, 32, 0, st>>>(bv.state, cnt, capacity);
     k_raygen_batch<<<(unsigned)ctx->sm_count * 8, 256, 0, st>>>(bv, pb[cur]);
-    k_extend<false, true><<<grid, 128, 0, st>>>(SceneView{}, pb[cur], 0u, w.hits.ptr, nullptr, w.queue[0].ptr,
-                                                w.queue[1].ptr, cnt + 2, w.overflow.ptr, w.work.ptr, bv);
-    k_sample<true><<<grid, 128, 0, st>>>(RenderParams{}, pb[cur], w.queue[0].ptr, cnt + 2, w.samples.ptr, bv);
+    k_extend_pt<true><<<w.ext_grid, 128, 0, st>>>(SceneView{}, pb[cur], 0u, w.hits.ptr, cnt + 4, w.overflow.ptr,
+                                                w.work.ptr, bv);
+    k_build_queues<true><<<grid, 256, 0, st>>>(w.hits.ptr, 0u, w.queue[0].ptr, w.queue[1].ptr, cnt + 2, bv);
+    k_sample<true><<<grid, 128, 0, st>>>(SceneView{}, RenderParams{}, pb[cur], w.hits.ptr, nullptr, w.queue[0].ptr,
+                                         cnt + 2, w.samples.ptr, bv);
     k_shade<false, false, true><<<grid, 128, 0, st>>>(SceneView{}, RenderParams{}, pb[cur], pb[1 - cur], w.hits.ptr,
                                                       nullptr, w.samples.ptr, w.queue[0].ptr, cnt + 2, cnt, sb,
                                                       cnt + 1, nullptr, nullptr, gv, bv);
     k_shade<true, false, true><<<grid, 128, 0, st>>>(SceneView{}, RenderParams{}, pb[cur], pb[1 - cur], w.hits.ptr,
                                                      nullptr, w.samples.ptr, w.queue[1].ptr, cnt + 3, cnt, sb,
                                                      cnt + 1, nullptr, nullptr, gv, bv);
-    k_shadow<false, true><<<grid, 128, 0, st>>>(SceneView{}, sb, cnt + 1, pb[1 - cur], nullptr, nullptr,
-                                                w.overflow.ptr, w.work.ptr + 2, gv, bv);
+    k_shadow_pt<true><<<w.shadow_grid, 128, 0, st>>>(SceneView{}, sb, cnt + 1, cnt + 5, pb[1 - cur], nullptr, nullptr,
+                                                   w.overflow.ptr, w.work.ptr + 2, gv, bv);
     k_batch_advance<<<1, 32, 0, st>>>(bv.state, cnt, handle, use_graph);
 }
 
@@ -1274,16 +1530,18 @@ static ks_status batch_render(ks_context *ctx, const ks_batch_job *jobs, uint32_
         (uint32_t)std::max<unsigned long long>(1, std::min<unsigned long long>(o.capacity ? o.capacity : 1u << 22,
                                                                                total));
     const unsigned grid = (unsigned)ctx->sm_count * (o.grid_per_sm ? std::min(o.grid_per_sm, 64u) : 16u);
+    w.ext_grid = resident_grid(k_extend_pt<true>, 128, ctx->sm_count);
+    w.shadow_grid = resident_grid(k_shadow_pt<true>, 128, ctx->sm_count);
     for (int b = 0; b < 2; ++b)
         for (int f = 0; f < 4; ++f)
             KS_CUDA_TRY(ctx, w.state[b][f].alloc(capacity));
     KS_CUDA_TRY(ctx, w.hits.alloc(capacity));
-    KS_CUDA_TRY(ctx, w.samples.alloc(2 * (size_t)capacity));
+    KS_CUDA_TRY(ctx, w.samples.alloc(4 * (size_t)capacity));
     for (auto &q : w.queue)
         KS_CUDA_TRY(ctx, q.alloc(capacity));
     for (auto &f : w.shadow)
         KS_CUDA_TRY(ctx, f.alloc(capacity));
-    KS_CUDA_TRY(ctx, w.counters.alloc(4));
+    KS_CUDA_TRY(ctx, w.counters.alloc(kCounters));
     KS_CUDA_TRY(ctx, w.overflow.alloc(1));
     KS_CUDA_TRY(ctx, w.work.alloc(4));
     KS_CUDA_TRY(ctx, w.state_dev.alloc(1));
@@ -1293,7 +1551,7 @@ static ks_status batch_render(ks_context *ctx, const ks_batch_job *jobs, uint32_
     init.max_iterations = (uint32_t)std::min<unsigned long long>((total / capacity + 2) * (max_bounces + 2) + 64,
                                                                   0x7fffffffull);
     KS_CUDA_TRY(ctx, cudaMemcpyAsync(w.state_dev.ptr, &init, sizeof(init), cudaMemcpyHostToDevice, st));
-    KS_CUDA_TRY(ctx, cudaMemsetAsync(w.counters.ptr, 0, sizeof(uint32_t) * 4, st));
+    KS_CUDA_TRY(ctx, cudaMemsetAsync(w.counters.ptr, 0, sizeof(uint32_t) * kCounters, st));
     KS_CUDA_TRY(ctx, cudaMemsetAsync(w.overflow.ptr, 0, sizeof(int), st));
     KS_CUDA_TRY(ctx, cudaMemsetAsync(w.work.ptr, 0, sizeof(unsigned long long) * 4, st));
     BatchView bv{w.views.ptr, w.params.ptr, w.accum.ptr, w.weights.ptr, w.path_begin.ptr, n, w.state_dev.ptr};

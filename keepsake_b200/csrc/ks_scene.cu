@@ -60,6 +60,68 @@ __global__ void trace_kernel(const TravNode *nodes, const float4 *tris, uint32_t
         atomicOr(overflow_flag, 1);
 }
 
+// ks_trace_rays for flat scenes: the same queries as trace_kernel, traversed by trav_step with
+// dynamic ray fetch (each ray makes the same tests as traverse(): same triangle, t and barycentrics).
+__global__ void __launch_bounds__(128) trace_kernel_pt(const TravNode *nodes, const float4 *tris, uint32_t root_ref,
+                                                       uint32_t root_count, float bx0, float by0, float bz0, float bx1,
+                                                       float by1, float bz1, const float *rays, uint32_t n, int any_hit,
+                                                       int culling, uint32_t *tri_out, float *t_out, float *bary_out,
+                                                       int *overflow_flag, uint32_t *fetch)
+{
+    const float bmin[3] = {bx0, by0, bz0}, bmax[3] = {bx1, by1, bz1};
+    uint4 stack[kStackDepth];
+    TravState s;
+    uint32_t ray = ~0u;
+    bool drained = false;
+    int overflow = 0;
+    auto finish = [&](uint32_t i, const Hit &h) {
+        if (any_hit) {
+            tri_out[i] = h.tri != ~0u ? 1u : 0u;
+            return;
+        }
+        tri_out[i] = h.tri;
+        t_out[i] = h.tri != ~0u ? h.t : -kInf;
+        bary_out[3 * i + 0] = h.tri != ~0u ? h.b0 : 0.0f;
+        bary_out[3 * i + 1] = h.tri != ~0u ? h.b1 : 0.0f;
+        bary_out[3 * i + 2] = h.tri != ~0u ? h.b2 : 0.0f;
+    };
+    while (true) {
+        const uint32_t id = warp_fetch(fetch, n, ray == ~0u, drained);
+        if (id != ~0u) {
+            const float *r = rays + 8 * (size_t)id;
+            RayQuery q;
+            q.o = mk(r[0], r[1], r[2]);
+            q.tmin = r[3];
+            q.d = mk(r[4], r[5], r[6]);
+            q.tmax = r[7];
+            if (trav_begin(s, q, root_ref, root_count, bmin, bmax))
+                ray = id;
+            else
+                finish(id, s.hit);
+        }
+        if (__ballot_sync(0xffffffffu, ray != ~0u) == 0) {
+            if (drained)
+                break;
+            continue;
+        }
+        while (true) {
+            if (ray != ~0u) {
+                const bool done = any_hit ? trav_step<true>(nodes, tris, s, stack, culling, overflow, nullptr)
+                                          : trav_step<false>(nodes, tris, s, stack, culling, overflow, nullptr);
+                if (done) {
+                    finish(ray, s.hit);
+                    ray = ~0u;
+                }
+            }
+            const int n_idle = __popc(__ballot_sync(0xffffffffu, ray == ~0u));
+            if (n_idle == 32 || (!drained && n_idle >= KS_TRAV_REFILL))
+                break;
+        }
+    }
+    if (overflow)
+        atomicOr(overflow_flag, 1);
+}
+
 bool valid_material(const ks_material_desc &m)
 {
     auto finite = [](float x) { return x == x && x < 3.0e38f && x > -3.0e38f; };
@@ -354,7 +416,7 @@ ks_status ks_trace_rays(ks_scene *scene, const float *rays, uint32_t n, int any_
         return KS_OK;
     KS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
     DevBuf<float> d_rays, d_t, d_bary;
-    DevBuf<uint32_t> d_tri;
+    DevBuf<uint32_t> d_tri, d_fetch;
     DevBuf<int> d_flag;
     KS_CUDA_TRY(ctx, d_rays.alloc((size_t)n * 8));
     KS_CUDA_TRY(ctx, d_tri.alloc(n));
@@ -365,10 +427,22 @@ ks_status ks_trace_rays(ks_scene *scene, const float *rays, uint32_t n, int any_
     KS_CUDA_TRY(ctx, cudaMemcpyAsync(d_rays.ptr, rays, d_rays.bytes(), cudaMemcpyHostToDevice, st));
     KS_CUDA_TRY(ctx, cudaMemsetAsync(d_flag.ptr, 0, sizeof(int), st));
     const float *b = scene->scene_bound;
-    trace_kernel<<<(n + 127) / 128, 128, 0, st>>>(scene->trav_nodes.ptr, scene->prim_tris.ptr, scene->root_ref,
-                                                   scene->root_count, b[0], b[1], b[2], b[3], b[4], b[5], d_rays.ptr, n,
-                                                   any_hit, culling, d_tri.ptr, d_t.ptr, d_bary.ptr, d_flag.ptr,
-                                                   make_view(scene).inst);
+    if (scene->n_instances) {
+        trace_kernel<<<(n + 127) / 128, 128, 0, st>>>(scene->trav_nodes.ptr, scene->prim_tris.ptr, scene->root_ref,
+                                                       scene->root_count, b[0], b[1], b[2], b[3], b[4], b[5],
+                                                       d_rays.ptr, n, any_hit, culling, d_tri.ptr, d_t.ptr,
+                                                       d_bary.ptr, d_flag.ptr, make_view(scene).inst);
+    } else {
+        KS_CUDA_TRY(ctx, d_fetch.alloc(1));
+        KS_CUDA_TRY(ctx, cudaMemsetAsync(d_fetch.ptr, 0, sizeof(uint32_t), st));
+        int per_sm = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_kernel_pt, 128, 0);
+        const unsigned grid = std::min<unsigned>((n + 127) / 128, (unsigned)std::max(per_sm, 1) * ctx->sm_count);
+        trace_kernel_pt<<<grid, 128, 0, st>>>(scene->trav_nodes.ptr, scene->prim_tris.ptr, scene->root_ref,
+                                              scene->root_count, b[0], b[1], b[2], b[3], b[4], b[5], d_rays.ptr, n,
+                                              any_hit, culling, d_tri.ptr, d_t.ptr, d_bary.ptr, d_flag.ptr,
+                                              d_fetch.ptr);
+    }
     KS_CUDA_TRY(ctx, cudaGetLastError());
     int overflow = 0;
     KS_CUDA_TRY(ctx, cudaMemcpyAsync(tri_idx, d_tri.ptr, d_tri.bytes(), cudaMemcpyDeviceToHost, st));

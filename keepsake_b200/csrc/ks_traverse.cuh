@@ -123,39 +123,27 @@ KS_D bool isect_tri(const RayQuery &ray, const TriHelper &h, f3 v0, f3 v1, f3 v2
 KS_D bool slab(const RayQuery &ray, const BoxHelper &h, const float bmin[3], const float bmax[3], float &t0,
                float &t1)
 {
+    // every value is computed and the early outs become one condition: the same results without
+    // data-dependent branches
     float tmin = (h.neg[0] ? bmax[0] : bmin[0]) - ray.o.x;
-    if (tmin != 0.0f)
-        tmin *= h.inv.x;
+    tmin = tmin != 0.0f ? tmin * h.inv.x : tmin;
     float tmax = (h.neg[0] ? bmin[0] : bmax[0]) - ray.o.x;
-    if (tmax != 0.0f)
-        tmax *= h.inv.x;
+    tmax = tmax != 0.0f ? tmax * h.inv.x : tmax;
     float tymin = (h.neg[1] ? bmax[1] : bmin[1]) - ray.o.y;
-    if (tymin != 0.0f)
-        tymin *= h.inv.y;
+    tymin = tymin != 0.0f ? tymin * h.inv.y : tymin;
     float tymax = (h.neg[1] ? bmin[1] : bmax[1]) - ray.o.y;
-    if (tymax != 0.0f)
-        tymax *= h.inv.y;
-    if (tmin > tymax || tymin > tmax)
-        return false;
-    if (tymin > tmin)
-        tmin = tymin;
-    if (tymax < tmax)
-        tmax = tymax;
+    tymax = tymax != 0.0f ? tymax * h.inv.y : tymax;
+    const bool miss_y = tmin > tymax || tymin > tmax;
+    tmin = tymin > tmin ? tymin : tmin;
+    tmax = tymax < tmax ? tymax : tmax;
     float tzmin = (h.neg[2] ? bmax[2] : bmin[2]) - ray.o.z;
-    if (tzmin != 0.0f)
-        tzmin *= h.inv.z;
+    tzmin = tzmin != 0.0f ? tzmin * h.inv.z : tzmin;
     float tzmax = (h.neg[2] ? bmin[2] : bmax[2]) - ray.o.z;
-    if (tzmax != 0.0f)
-        tzmax *= h.inv.z;
-    if (tmin > tzmax || tzmin > tmax)
-        return false;
-    if (tzmin > tmin)
-        tmin = tzmin;
-    if (tzmax < tmax)
-        tmax = tzmax;
-    t0 = tmin;
-    t1 = tmax;
-    return true;
+    tzmax = tzmax != 0.0f ? tzmax * h.inv.z : tzmax;
+    const bool miss_z = tmin > tzmax || tzmin > tmax;
+    t0 = tzmin > tmin ? tzmin : tmin;
+    t1 = tzmax < tmax ? tzmax : tmax;
+    return !miss_y && !miss_z;
 }
 
 enum class Culling : int
@@ -205,9 +193,7 @@ KS_D bool traverse(const TravNode *__restrict__ nodes, const float4 *__restrict_
     hit.tri = ~0u;
     const TriHelper th = make_tri_helper(ray.d);
     const BoxHelper bh = make_box_helper(ray.d);
-    uint32_t st_ref[kStackDepth];
-    uint32_t st_cnt[kStackDepth];
-    float st_t[kStackDepth];
+    uint4 stack[kStackDepth]; // (ref, count, entry t bits, -): one 16-byte access per push or pop
     int sp = 0;
     // the root's own box (cuda/sbvh.cu:520-527)
     float t0, t1;
@@ -266,10 +252,7 @@ KS_D bool traverse(const TravNode *__restrict__ nodes, const float4 *__restrict_
                         overflow = 1;
                         return !kAnyHit && hit.tri != ~0u;
                     }
-                    st_ref[sp] = far_ref;
-                    st_cnt[sp] = far_cnt;
-                    st_t[sp] = far_t;
-                    ++sp;
+                    stack[sp++] = make_uint4(far_ref, far_cnt, __float_as_uint(far_t), 0u);
                 }
                 ref = near_ref;
                 cnt = near_cnt;
@@ -284,10 +267,10 @@ KS_D bool traverse(const TravNode *__restrict__ nodes, const float4 *__restrict_
         // pop, re-checking the entry time against the current tmax
         bool found = false;
         while (sp > 0) {
-            --sp;
-            if (st_t[sp] < ray.tmax) {
-                ref = st_ref[sp];
-                cnt = st_cnt[sp];
+            const uint4 e = stack[--sp];
+            if (__uint_as_float(e.z) < ray.tmax) {
+                ref = e.x;
+                cnt = e.y;
                 found = true;
                 break;
             }
@@ -296,6 +279,166 @@ KS_D bool traverse(const TravNode *__restrict__ nodes, const float4 *__restrict_
             break;
     }
     return hit.tri != ~0u;
+}
+
+// ---- resumable traversal (persistent warps with dynamic ray fetch) ---------------------------
+// The same traversal as traverse(), cut into steps so that a warp can hand finished lanes a new
+// ray and keep its lanes busy: trav_begin does the root test, every trav_step visits the current
+// node (an interior node, or a leaf and its triangles) and then descends or pops, exactly as one
+// pass of traverse()'s loop.  Each ray therefore makes the same sequence of box and triangle tests
+// (same hits, same distances); only the interleaving of rays changes.  The stack lives in the
+// caller's array.
+struct TravState
+{
+    RayQuery ray;
+    TriHelper th;
+    BoxHelper bh;
+    uint32_t ref, cnt;
+    int sp;
+    Hit hit;
+};
+
+// Returns false when the ray misses the root box (the traversal is then over, without a hit).
+KS_D bool trav_begin(TravState &s, const RayQuery &ray, uint32_t root_ref, uint32_t root_count,
+                     const float root_bmin[3], const float root_bmax[3])
+{
+    s.hit.tri = ~0u;
+    s.ray = ray;
+    s.th = make_tri_helper(ray.d);
+    s.bh = make_box_helper(ray.d);
+    s.sp = 0;
+    s.ref = root_ref;
+    s.cnt = root_count;
+    float t0, t1;
+    return slab(s.ray, s.bh, root_bmin, root_bmax, t0, t1) && t0 < s.ray.tmax && t1 > s.ray.tmin;
+}
+
+// Interior node test of trav_step: descends to the near child (pushing the far one when both are
+// hit) and returns 1, returns 0 when neither child is hit, and -1 with the overflow flag set when
+// the stack is full (the caller then ends the ray).
+KS_D int trav_interior(const TravNode *__restrict__ nodes, TravState &s, uint4 *stack, int &overflow,
+                        TravCount *count)
+{
+    const TravNode *n = nodes + s.ref;
+    if (count)
+        count->nodes++;
+    float4 A = __ldg(&n->a), B = __ldg(&n->b), C = __ldg(&n->c);
+    uint4 D = __ldg(&n->d);
+    float lmin[3] = {A.x, A.y, A.z}, lmax[3] = {A.w, B.x, B.y};
+    float rmin[3] = {B.z, B.w, C.x}, rmax[3] = {C.y, C.z, C.w};
+    float lt0, lt1, rt0, rt1;
+    bool lok = slab(s.ray, s.bh, lmin, lmax, lt0, lt1) && lt1 > s.ray.tmin && lt0 < s.ray.tmax;
+    bool rok = slab(s.ray, s.bh, rmin, rmax, rt0, rt1) && rt1 > s.ray.tmin && rt0 < s.ray.tmax;
+    uint32_t axis = D.z >> 30;
+    uint32_t lcnt = D.z & 0x3fffffffu, rcnt = D.w;
+    bool right_first = s.bh.neg[axis] != 0;
+    uint32_t near_ref = right_first ? D.y : D.x, far_ref = right_first ? D.x : D.y;
+    uint32_t near_cnt = right_first ? rcnt : lcnt, far_cnt = right_first ? lcnt : rcnt;
+    bool near_ok = right_first ? rok : lok, far_ok = right_first ? lok : rok;
+    float far_t = right_first ? lt0 : rt0;
+    if (near_ok && far_ok) {
+        if (s.sp >= kStackDepth) {
+            overflow = 1;
+            return -1;
+        }
+        stack[s.sp++] = make_uint4(far_ref, far_cnt, __float_as_uint(far_t), 0u);
+    }
+    if (!near_ok && !far_ok)
+        return 0;
+    s.ref = near_ok ? near_ref : far_ref;
+    s.cnt = near_ok ? near_cnt : far_cnt;
+    return 1;
+}
+
+// Pops the next node whose entry time is below the current tmax; false when the stack is empty.
+KS_D bool trav_pop(TravState &s, const uint4 *stack)
+{
+    while (s.sp > 0) {
+        const uint4 e = stack[--s.sp];
+        if (__uint_as_float(e.z) < s.ray.tmax) {
+            s.ref = e.x;
+            s.cnt = e.y;
+            return true;
+        }
+    }
+    return false;
+}
+
+// Leaf triangles of trav_step; true when an any-hit query found an occluder.
+template <bool kAnyHit>
+KS_D bool trav_leaf(const float4 *__restrict__ tris, TravState &s, int culling, TravCount *count)
+{
+    const uint32_t first = s.ref & ~kLeafBit;
+    for (uint32_t k = 0; k < s.cnt; ++k) {
+        if (count)
+            count->tris++;
+        const float4 *p = tris + 3 * (size_t)(first + k);
+        float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2);
+        f3 v0 = mk(a.x, a.y, a.z), v1 = mk(b.x, b.y, b.z), v2 = mk(c.x, c.y, c.z);
+        if (cull_tri(s.ray, v0, v1, v2, culling))
+            continue;
+        float t, b0, b1, b2;
+        if (isect_tri(s.ray, s.th, v0, v1, v2, t, b0, b1, b2)) {
+            if (kAnyHit) {
+                s.hit.tri = __float_as_uint(a.w);
+                return true;
+            }
+            if (t < s.ray.tmax) {
+                s.ray.tmax = t;
+                s.hit.tri = __float_as_uint(a.w);
+                s.hit.slot = first + k;
+                s.hit.t = t;
+                s.hit.b0 = b0;
+                s.hit.b1 = b1;
+                s.hit.b2 = b2;
+            }
+        }
+    }
+    return false;
+}
+
+// One step; returns true when the traversal of the ray is over (any-hit: found an occluder).
+// A step visits one node (an interior node or a leaf), then descends or pops.
+template <bool kAnyHit>
+KS_D bool trav_step(const TravNode *__restrict__ nodes, const float4 *__restrict__ tris, TravState &s,
+                    uint4 *stack, int culling, int &overflow, TravCount *count)
+{
+    if (s.ref & kLeafBit) {
+        if (trav_leaf<kAnyHit>(tris, s, culling, count))
+            return true;
+    } else {
+        const int r = trav_interior(nodes, s, stack, overflow, count);
+        if (r != 0)
+            return r < 0;
+    }
+    return !trav_pop(s, stack);
+}
+
+// Dynamic ray fetch for trav_step: each warp takes rays from a global counter and hands every lane
+// that finished a new ray once at least KS_TRAV_REFILL lanes are idle, so a warp no longer runs
+// until its longest ray ends with most lanes masked off.
+#ifndef KS_TRAV_REFILL
+#define KS_TRAV_REFILL 12
+#endif
+
+// Hands the idle lanes of the warp rays [base, base + popc(idle)) in lane order; every lane calls
+// it.  Returns this lane's ray (or ~0u) and sets drained once the counter has passed count.
+KS_D uint32_t warp_fetch(uint32_t *fetch, uint32_t count, bool idle, bool &drained)
+{
+    const uint32_t mask = __ballot_sync(0xffffffffu, idle);
+    if (drained || mask == 0)
+        return ~0u;
+    const uint32_t lane = threadIdx.x & 31;
+    uint32_t base = 0;
+    if (lane == (uint32_t)(__ffs(mask) - 1))
+        base = atomicAdd(fetch, (uint32_t)__popc(mask));
+    base = __shfl_sync(0xffffffffu, base, __ffs(mask) - 1);
+    if (base + (uint32_t)__popc(mask) >= count)
+        drained = true;
+    if (!idle)
+        return ~0u;
+    const uint32_t id = base + __popc(mask & ((1u << lane) - 1u));
+    return id < count ? id : ~0u;
 }
 
 // ---- two-level traversal (instances) --------------------------------------------------------
@@ -325,9 +468,7 @@ KS_D bool traverse_instances(const TravNode *__restrict__ nodes, const float4 *_
     hit.tri = ~0u;
     inst = 0;
     const BoxHelper bh = make_box_helper(ray.d);
-    uint32_t st_ref[kTlasStackDepth];
-    uint32_t st_cnt[kTlasStackDepth];
-    float st_t[kTlasStackDepth];
+    uint4 stack[kTlasStackDepth];
     int sp = 0;
     float t0, t1;
     if (!slab(ray, bh, iv.bmin, iv.bmax, t0, t1) || !(t0 < ray.tmax && t1 > ray.tmin))
@@ -392,10 +533,7 @@ KS_D bool traverse_instances(const TravNode *__restrict__ nodes, const float4 *_
                         overflow = 1;
                         return !kAnyHit && hit.tri != ~0u;
                     }
-                    st_ref[sp] = far_ref;
-                    st_cnt[sp] = far_cnt;
-                    st_t[sp] = far_t;
-                    ++sp;
+                    stack[sp++] = make_uint4(far_ref, far_cnt, __float_as_uint(far_t), 0u);
                 }
                 ref = near_ref;
                 cnt = near_cnt;
@@ -409,10 +547,10 @@ KS_D bool traverse_instances(const TravNode *__restrict__ nodes, const float4 *_
         }
         bool found = false;
         while (sp > 0) {
-            --sp;
-            if (st_t[sp] < ray.tmax) {
-                ref = st_ref[sp];
-                cnt = st_cnt[sp];
+            const uint4 e = stack[--sp];
+            if (__uint_as_float(e.z) < ray.tmax) {
+                ref = e.x;
+                cnt = e.y;
                 found = true;
                 break;
             }
