@@ -1,8 +1,9 @@
 // Device-side scalar/vector helpers for the B200 small_pt path.
 //
-// Every translation unit of the product is compiled with -fmad=false and IEEE division/sqrt, so a
-// float expression here rounds exactly like the same expression in the reference's x86-64 SSE host
-// build.  Where the reference relies on a fused multiply-add (ksc::difference_of_products,
+// The translation units of the bit-exact parts (sampler, camera rays, SBVH build and traversal) are
+// compiled with -fmad=false and IEEE division/sqrt, so a float expression there rounds exactly like
+// the same expression in the reference's x86-64 SSE host build; the shading unit (ks_shade.cu) uses
+// fast math and is checked statistically.  Where the reference relies on a fused multiply-add (ksc::difference_of_products,
 // cuda/math.cuh:189-195) it is written out with fmaf() explicitly.
 #pragma once
 #include <cstdint>

@@ -105,13 +105,12 @@ __global__ void __launch_bounds__(128) trace_kernel_pt(const TravNode *nodes, co
             continue;
         }
         while (true) {
-            if (ray != ~0u) {
-                const bool done = any_hit ? trav_step<true>(nodes, tris, s, stack, culling, overflow, nullptr)
-                                          : trav_step<false>(nodes, tris, s, stack, culling, overflow, nullptr);
-                if (done) {
-                    finish(ray, s.hit);
-                    ray = ~0u;
-                }
+            const bool done =
+                any_hit ? trav_warp_step<true>(nodes, tris, s, stack, culling, overflow, nullptr, ray != ~0u)
+                        : trav_warp_step<false>(nodes, tris, s, stack, culling, overflow, nullptr, ray != ~0u);
+            if (done) {
+                finish(ray, s.hit);
+                ray = ~0u;
             }
             const int n_idle = __popc(__ballot_sync(0xffffffffu, ray == ~0u));
             if (n_idle == 32 || (!drained && n_idle >= KS_TRAV_REFILL))

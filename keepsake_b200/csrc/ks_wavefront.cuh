@@ -1,0 +1,234 @@
+// Types and device helpers shared by the wavefront kernels of ks_integrator.cu (ray generation,
+// traversal, batching, host loop) and ks_shade.cu (sampling and shading, compiled with fast
+// division and square root), plus the host launchers of the shading kernels.
+#pragma once
+#include "ks_guide_view.cuh"
+#include "ks_lights.cuh"
+
+namespace ksb
+{
+namespace wave
+{
+
+struct RenderParams
+{
+    int W, H, cx, cy, cw, ch;
+    int spp, seed, log2_spp, n_digits;
+    int bounces, include_background;
+    float clamp_direct, clamp_indirect;
+    float filter_r;
+    float cam_pos[3];
+    float p2w[16];
+};
+
+// Path state, structure of arrays, one float4 per field (16-byte vector loads/stores).
+struct PathBuf
+{
+    float4 *o_pdf;    // ray origin, pdf_wi_bsdf of the previous bounce
+    float4 *d_info;   // ray direction, (sobol dimension << 16 | bounce)
+    float4 *beta_pix; // throughput, pixel index
+    float4 *L_smp;    // radiance so far, sample index
+    uint32_t *rec;    // guided renders: training record of the path (kNoRecord: none); else null
+};
+
+struct ShadowBuf
+{
+    float4 *o_tmax;   // origin, tmax
+    float4 *d_target; // direction, target (next-queue slot, or kTermBit | pixel)
+    float4 *contrib;  // beta * clamped Ld
+    float4 *L_term;   // radiance of a path that ended this bounce
+};
+
+constexpr uint32_t kTermBit = 0x80000000u;
+
+// ---- batched rendering: many (scene, camera, params) jobs in one wavefront --------------------
+// A path's job id rides in bits 21..30 of its pixel word (per-job frames of at most 2^21 pixels,
+// up to 1024 jobs); the scene view, render parameters and accumulators of a job are read from
+// device arrays.  The iteration's counts live on the device (BatchState), so the loop needs no
+// host round trip and runs as a CUDA graph with a device-side while condition.
+constexpr uint32_t kJobShift = 21;
+constexpr uint32_t kPixMask = (1u << kJobShift) - 1u;
+constexpr uint32_t kMaxJobs = 1024;
+
+struct BatchState
+{
+    unsigned long long total, issued, first_path; // paths of all jobs, paths issued, first of this refill
+    unsigned long long ext_rays, shadow_rays;     // work counters
+    uint32_t cur_count, n_new, count, base_slot;  // paths alive, refilled, traced this iteration
+    uint32_t iterations, max_iterations, error;
+};
+
+struct BatchView
+{
+    const SceneView *views;       // per job
+    const RenderParams *params;   // per job
+    double *const *accum;         // per job: W * H * 3
+    double *const *weights;       // per job: W * H * 2
+    const unsigned long long *path_begin; // n_jobs + 1: first global path index of each job
+    uint32_t n_jobs;
+    BatchState *state;
+};
+
+template <bool kBatch, class T>
+KS_D const T &job_of(const T &single, const T *table, uint32_t job)
+{
+    if constexpr (kBatch)
+        return table[job];
+    else
+        return single;
+}
+
+KS_D uint32_t bits(float f) { return __float_as_uint(f); }
+KS_D float fbits(uint32_t u) { return __uint_as_float(u); }
+
+// One atomic per warp; every lane of the warp must call this.
+KS_D uint32_t warp_append(uint32_t *counter, bool pred)
+{
+    uint32_t mask = __ballot_sync(0xffffffffu, pred);
+    if (mask == 0)
+        return 0;
+    uint32_t lane = threadIdx.x & 31;
+    int leader = __ffs(mask) - 1;
+    uint32_t base = 0;
+    if ((int)lane == leader)
+        base = atomicAdd(counter, (uint32_t)__popc(mask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    return base + __popc(mask & ((1u << lane) - 1u));
+}
+
+KS_D void accumulate(double *accum, double *weights, uint32_t pix, f3 L)
+{
+    atomicAdd(&weights[2 * (size_t)pix], 1.0);
+    atomicAdd(&accum[3 * (size_t)pix + 0], (double)L.x);
+    atomicAdd(&accum[3 * (size_t)pix + 1], (double)L.y);
+    atomicAdd(&accum[3 * (size_t)pix + 2], (double)L.z);
+}
+
+// ---- hit record (geometry.cpp:68-163 + transform_it with the identity instance) ----------------
+struct ShadeFrame
+{
+    f3 p;
+    f3 t, b, n;    // geometric frame (after re-orthonormalisation)
+    f3 st, sb, sn; // shading frame (flat shading: same as the geometric one)
+};
+
+KS_D void reortho(f3 &t, f3 &b, f3 &n)
+{
+    // Transform::frame (maths.h:989-996) with identity: t' = normalize(t),
+    // b' = normalize(b - dot(b, t') t'), n' = normalize(cross(t', b'))
+    f3 tt = normalize(t);
+    f3 bb = normalize(b - dot(b, tt) * tt);
+    n = normalize(cross(tt, bb));
+    t = tt;
+    b = bb;
+}
+
+// Hit point from the barycentrics of vertices 1 and 2 (geometry.cpp:68-163).
+KS_D f3 hit_point(f3 p0, f3 p1, f3 p2, float u, float v)
+{
+    float w0 = 1.0f - u - v;
+    return w0 * p0 + u * p1 + v * p2;
+}
+
+KS_D ShadeFrame make_frame(f3 p0, f3 p1, f3 p2, float u, float v, f3 ray_dir, bool twosided)
+{
+    ShadeFrame f;
+    f3 rd = normalize(ray_dir);
+    f3 wo_object = -rd;
+    f3 ng = normalize(cross(p1 - p0, p2 - p0));
+    f.p = hit_point(p0, p1, p2, u, v);
+    f3 dpdu = p1 - p0;
+    f3 b = normalize(cross(ng, dpdu));
+    f3 t = normalize(cross(b, ng));
+    if (twosided && dot(wo_object, ng) < 0.0f) {
+        ng = -ng;
+        t = -t;
+    }
+    f3 ft = t, fb = b, fn = ng;
+    reortho(ft, fb, fn);
+    f.t = ft;
+    f.b = fb;
+    f.n = fn;
+    // flat shading: sh_frame = frame (geometry.cpp:139-141), re-orthonormalised identically
+    f.st = ft;
+    f.sb = fb;
+    f.sn = fn;
+    return f;
+}
+
+KS_D f3 sh_to_local(const ShadeFrame &f, f3 w)
+{
+    bool hw = dot(f.n, w) >= 0.0f;
+    f3 l = mk(dot(f.st, w), dot(f.sb, w), dot(f.sn, w));
+    bool hl = l.z >= 0.0f;
+    if (hw != hl)
+        l.z *= -1.0f;
+    return l;
+}
+
+KS_D f3 sh_to_world(const ShadeFrame &f, f3 l)
+{
+    bool hl = l.z >= 0.0f;
+    f3 w = f.st * l.x + f.sb * l.y + f.sn * l.z;
+    bool hw = dot(f.n, w) >= 0.0f;
+    if (hl != hw)
+        w = w - 2.0f * dot(f.n, w) * f.n;
+    return w;
+}
+
+// offset_ray (ray.h:66-81)
+KS_D f3 offset_ray(f3 p, f3 n)
+{
+    const float origin = 1.0f / 32.0f, float_scale = 1.0f / 65536.0f, int_scale = 256.0f;
+    int ox = (int)(int_scale * n.x), oy = (int)(int_scale * n.y), oz = (int)(int_scale * n.z);
+    f3 pi = mk(__int_as_float(__float_as_int(p.x) + ((p.x < 0) ? -ox : ox)),
+               __int_as_float(__float_as_int(p.y) + ((p.y < 0) ? -oy : oy)),
+               __int_as_float(__float_as_int(p.z) + ((p.z < 0) ? -oz : oz)));
+    return mk(fabsf(p.x) < origin ? p.x + float_scale * n.x : pi.x,
+              fabsf(p.y) < origin ? p.y + float_scale * n.y : pi.y,
+              fabsf(p.z) < origin ? p.z + float_scale * n.z : pi.z);
+}
+
+// spawn_ray<OffsetType::NextBounce> origin (ray.h:89-96)
+KS_D f3 spawn_origin(f3 p, f3 dir, f3 n) { return offset_ray(p, dot(dir, n) > 0.0f ? n : -n); }
+
+KS_D float power_heur(float pf, float pg)
+{
+    float f2 = pf * pf, g2 = pg * pg;
+    return f2 / (f2 + g2);
+}
+
+KS_D f3 clamp_contrib(f3 v, int bounce_for_direct, const RenderParams &rp, bool is_nee)
+{
+    // trace(): NEE uses bounce==0 -> clamp_direct, bounce>=1 -> clamp_indirect (small_pt.cpp:153-157);
+    // unidirectional hits use bounce==1 -> direct, bounce>=2 -> indirect (:97-103, :128-133).
+    int b = bounce_for_direct;
+    if (is_nee) {
+        if (b == 0 && rp.clamp_direct > 0.0f)
+            return cwise_min(v, rp.clamp_direct);
+        if (b >= 1 && rp.clamp_indirect > 0.0f)
+            return cwise_min(v, rp.clamp_indirect);
+        return v;
+    }
+    if (b == 1 && rp.clamp_direct > 0.0f)
+        return cwise_min(v, rp.clamp_direct);
+    if (b >= 2 && rp.clamp_indirect > 0.0f)
+        return cwise_min(v, rp.clamp_indirect);
+    return v;
+}
+
+// ---- shading launchers (ks_shade.cu) ----------------------------------------------------------
+// k_sample: Sobol values and the NEE light sample of every path in the hit queue.
+void launch_sample(bool batch, unsigned grid, cudaStream_t st, const SceneView &sv, const RenderParams &rp,
+                   PathBuf cur, const float4 *hits, const uint32_t *hit_inst, const uint32_t *queue,
+                   const uint32_t *queue_count, float4 *samples, const BatchView &bv);
+// k_shade: hit (miss = false) or miss shading of the paths in a queue; guided and batched
+// renders are not combined.
+void launch_shade(bool miss, bool guided, bool batch, unsigned grid, cudaStream_t st, const SceneView &sv,
+                  const RenderParams &rp, PathBuf cur, PathBuf nxt, const float4 *hits, const uint32_t *hit_inst,
+                  const float4 *samples, const uint32_t *queue, const uint32_t *queue_count, uint32_t *next_count,
+                  ShadowBuf sb, uint32_t *shadow_count, double *accum, double *weights, const GuideView &gv,
+                  const BatchView &bv);
+
+} // namespace wave
+} // namespace ksb
