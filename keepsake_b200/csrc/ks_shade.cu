@@ -20,10 +20,10 @@ namespace
 using namespace wave;
 
 // Minimum resident CTAs per SM asked of the compiler (a register cap) for the shading kernel: it is
-// latency bound, and at 10 CTAs of 128 (48 registers, a few hundred bytes of spills) it runs about
-// 1.25x faster than at its natural 113 registers (4 CTAs).
+// latency bound, and at 8 CTAs of 128 (64 registers, a few dozen bytes of spills) it runs about
+// 1.25x faster than at its natural register count (about 110: 4 CTAs).
 #ifndef KS_SHADE_MIN_BLOCKS
-#define KS_SHADE_MIN_BLOCKS 10
+#define KS_SHADE_MIN_BLOCKS 8
 #endif
 
 // Sobol samples and the NEE light sample of one bounce for every path in the hit queue (whose
