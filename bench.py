@@ -349,7 +349,7 @@ def measured_peaks():
 
 def profile_traffic():
     """DRAM bytes per closest-hit query from the committed ncu summary (None if absent)."""
-    p = os.path.join(ROOT, "profiles", "k_extend_icosphere_l8.md")
+    p = os.path.join(ROOT, "profiles", "k_extend_pt_icosphere_l8.md")
     if not os.path.exists(p):
         return None
     for line in open(p):
