@@ -252,7 +252,7 @@ __global__ void __launch_bounds__(128, KS_TRAV_MIN_BLOCKS) k_extend_pt(const __g
     if constexpr (kBatch)
         count = bv.state->count;
     TravCount tc;
-    uint4 stack[kStackDepth];
+    KS_TRAV_STACK(stack);
     TravState s;
     const TravNode *nodes = sv_in.nodes;
     const float4 *tris = sv_in.prim_tris;
@@ -413,7 +413,7 @@ __global__ void __launch_bounds__(128, KS_TRAV_MIN_BLOCKS) k_shadow_pt(const __g
 {
     const uint32_t count = *shadow_count;
     TravCount tc;
-    uint4 stack[kStackDepth];
+    KS_TRAV_STACK(stack);
     TravState s;
     const TravNode *nodes = sv_in.nodes;
     const float4 *tris = sv_in.prim_tris;

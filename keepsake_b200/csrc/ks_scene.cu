@@ -69,7 +69,7 @@ __global__ void __launch_bounds__(128) trace_kernel_pt(const TravNode *nodes, co
                                                        int *overflow_flag, uint32_t *fetch)
 {
     const float bmin[3] = {bx0, by0, bz0}, bmax[3] = {bx1, by1, bz1};
-    uint4 stack[kStackDepth];
+    KS_TRAV_STACK(stack);
     TravState s;
     uint32_t ray = ~0u;
     bool drained = false;
