@@ -298,8 +298,8 @@ __global__ void __launch_bounds__(128, KS_TRAV_MIN_BLOCKS) k_extend_pt(const __g
     flush_counts(tc, work);
 }
 
-// Hit and miss queues from the per-ray results of k_extend_pt, one warp-aggregated append per
-// kind (queue order follows the path index, warp by warp).
+// Hit and miss queues from the per-ray results of k_extend_pt, one CTA-aggregated append per
+// kind (queue order follows the path index within each CTA's tile).
 template <bool kBatch = false>
 __global__ void __launch_bounds__(256) k_build_queues(const float4 *hits, uint32_t count, uint32_t *hit_queue,
                                                       uint32_t *miss_queue, uint32_t *queue_counts, BatchView bv)
@@ -312,8 +312,8 @@ __global__ void __launch_bounds__(256) k_build_queues(const float4 *hits, uint32
         const uint32_t i = base + threadIdx.x;
         const bool valid = i < count;
         const bool is_hit = valid && slot[4 * (size_t)i] != ~0u;
-        const uint32_t jh = warp_append(queue_counts, is_hit);
-        const uint32_t jm = warp_append(queue_counts + 1, valid && !is_hit);
+        uint32_t jh, jm;
+        block_append2(queue_counts, is_hit, queue_counts + 1, valid && !is_hit, jh, jm);
         if (valid) {
             if (is_hit)
                 hit_queue[jh] = i;

@@ -337,8 +337,8 @@ __global__ void __launch_bounds__(128, KS_SHADE_MIN_BLOCKS) k_shade(const __grid
                 }
             }
         }
-        uint32_t jc = warp_append(next_count, cont);
-        uint32_t js = warp_append(shadow_count, shadow);
+        uint32_t jc, js;
+        block_append2(next_count, cont, shadow_count, shadow, jc, js);
         const uint32_t sh_rec = rec; // the shadow ray of this vertex feeds the path's earlier record
         if constexpr (kGuided) {
             uint32_t jr = warp_append(gv.rec_count, want_rec);

@@ -96,6 +96,48 @@ KS_D uint32_t warp_append(uint32_t *counter, bool pred)
     return base + __popc(mask & ((1u << lane) - 1u));
 }
 
+// Appends to two queues with one atomic per CTA and queue instead of one per warp (the queue
+// counters are single addresses that every CTA hits, and same-address atomics serialise in L2).
+// Slots follow the CTA's threads in order.  Every thread of the CTA must call it (it synchronises
+// the CTA); blockDim.x is a multiple of 32.
+KS_D void block_append2(uint32_t *c0, bool p0, uint32_t *c1, bool p1, uint32_t &j0, uint32_t &j1)
+{
+    __shared__ uint32_t s_off[2][32];
+    __shared__ uint32_t s_base[2];
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, n_warps = blockDim.x >> 5;
+    const uint32_t m0 = __ballot_sync(0xffffffffu, p0), m1 = __ballot_sync(0xffffffffu, p1);
+    if (lane == 0) {
+        s_off[0][warp] = __popc(m0);
+        s_off[1][warp] = __popc(m1);
+    }
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t a = lane < n_warps ? s_off[0][lane] : 0u, b = lane < n_warps ? s_off[1][lane] : 0u;
+        uint32_t sa = a, sb = b; // inclusive prefix sums over the warps
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t ta = __shfl_up_sync(0xffffffffu, sa, o), tb = __shfl_up_sync(0xffffffffu, sb, o);
+            if ((int)lane >= o) {
+                sa += ta;
+                sb += tb;
+            }
+        }
+        const uint32_t na = __shfl_sync(0xffffffffu, sa, 31), nb = __shfl_sync(0xffffffffu, sb, 31);
+        if (lane == 0) {
+            s_base[0] = na ? atomicAdd(c0, na) : 0u;
+            s_base[1] = nb ? atomicAdd(c1, nb) : 0u;
+        }
+        if (lane < n_warps) {
+            s_off[0][lane] = sa - a;
+            s_off[1][lane] = sb - b;
+        }
+    }
+    __syncthreads();
+    const uint32_t below = (1u << lane) - 1u;
+    j0 = s_base[0] + s_off[0][warp] + __popc(m0 & below);
+    j1 = s_base[1] + s_off[1][warp] + __popc(m1 & below);
+    __syncthreads(); // the next call reuses the shared arrays
+}
+
 KS_D void accumulate(double *accum, double *weights, uint32_t pix, f3 L)
 {
     atomicAdd(&weights[2 * (size_t)pix], 1.0);
