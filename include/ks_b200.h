@@ -159,6 +159,15 @@ ks_status ks_sbvh_export(const ks_scene *scene, float *node_bounds, uint32_t *no
 ks_status ks_trace_rays(ks_scene *scene, const float *rays, uint32_t n, int any_hit, int culling, uint32_t *tri_idx,
                         float *t, float *bary);
 
+/* The same queries through the renderer's traversal: a 4-wide view of the same SBVH (each node
+ * with its interior children replaced by theirs, boxes tested with the same slab test), nearest
+ * slot first.  It reaches the same leaves, so the result equals ks_trace_rays' except where two
+ * triangles are hit at exactly the same distance (the visiting order then picks one of them).
+ * Flat scenes only (instanced scenes: KS_ERR_UNSUPPORTED).  Replaces the same reference calls as
+ * ks_trace_rays (cuda/sbvh.cu:512-603); exists to test the rendering traversal. */
+ks_status ks_trace_rays_wide(ks_scene *scene, const float *rays, uint32_t n, int any_hit, int culling,
+                             uint32_t *tri_idx, float *t, float *bary);
+
 /* ks_trace_rays without any device allocation.  No counterpart in the reference: it exists for
  * callers that may not allocate device memory (a host application that owns the device-memory
  * budget through its own allocator, or a frame loop that forbids cudaMalloc/cudaFree).  Rays and

@@ -194,6 +194,7 @@ _sig("ks_scene_build_bvh", [_vp, ctypes.POINTER(SBVHOptions), ctypes.POINTER(_f3
 _sig("ks_sbvh_counts", [_vp, ctypes.POINTER(_u32), ctypes.POINTER(_u32)])
 _sig("ks_sbvh_export", [_vp, _vp, _vp, _vp, _vp, _vp])
 _sig("ks_trace_rays", [_vp, _vp, _u32, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp])
+_sig("ks_trace_rays_wide", [_vp, _vp, _u32, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp])
 _sig("ks_camera_perspective", [ctypes.POINTER(_f32), _f32, _f32, ctypes.POINTER(CameraDesc)])
 _sig("ks_procedural_scene", [ctypes.c_char_p, ctypes.c_uint64, ctypes.POINTER(ProceduralOptions),
                              ctypes.POINTER(_vp)])
@@ -410,14 +411,15 @@ class Scene:
                        "ks_sbvh_export")
         return dict(bounds=bounds, axis=axis, right=right, prim_offset=off, prims=prims)
 
-    def trace(self, rays, any_hit=False, culling=2):
+    def trace(self, rays, any_hit=False, culling=2, wide=False):
+        """ks_trace_rays (wide=True: ks_trace_rays_wide, the renderer's 4-wide traversal)."""
         rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
         n = len(rays)
         tri = np.empty(n, np.uint32)
         t = np.empty(n, np.float32)
         bary = np.empty((n, 3), np.float32)
-        self.ctx.check(lib.ks_trace_rays(self.handle, ptr(rays), n, int(any_hit), culling, ptr(tri), ptr(t),
-                                         ptr(bary)), "ks_trace_rays")
+        fn, name = (lib.ks_trace_rays_wide, "ks_trace_rays_wide") if wide else (lib.ks_trace_rays, "ks_trace_rays")
+        self.ctx.check(fn(self.handle, ptr(rays), n, int(any_hit), culling, ptr(tri), ptr(t), ptr(bary)), name)
         return (tri.astype(bool), None, None) if any_hit else (tri, t, bary)
 
     def render(self, camera: CameraDesc, params: SmallPTParams, callback=None):

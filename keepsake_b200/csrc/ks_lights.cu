@@ -180,6 +180,7 @@ SceneView make_view(const ks_scene *s)
     v.ml_verts = s->ml_verts.ptr;
     v.inst_light_base = s->inst_light_base.ptr;
     v.nodes = s->trav_nodes.ptr;
+    v.wide = s->wide_nodes.ptr;
     v.prim_tris = s->prim_tris.ptr;
     v.verts = s->verts.ptr;
     v.indices = s->indices.ptr;

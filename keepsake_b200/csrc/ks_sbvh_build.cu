@@ -1038,6 +1038,57 @@ static ks_status build_range(ks_context *ctx, const float *verts, const uint32_t
 }
 
 // BLAS concatenation: interior refs move by the node base, leaf refs by the slot base.
+// Wide node i from interior node i: its leaf children as they are, its interior children replaced
+// by their two children (boxes and refs read from the child's node).
+__global__ void k_widen(const TravNode *nodes, uint32_t n, WideNode *wide)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    float lo[3][4], hi[3][4];
+    uint32_t ref[4], cnt[4];
+    for (int k = 0; k < 4; ++k) {
+        for (int a = 0; a < 3; ++a) {
+            lo[a][k] = __int_as_float(0x7f800000);  // +inf
+            hi[a][k] = __int_as_float(0xff800000);  // -inf
+        }
+        ref[k] = kLeafBit;
+        cnt[k] = 0;
+    }
+    int m = 0;
+    auto put = [&](const TravNode &nd, int side) {
+        const float4 A = nd.a, B = nd.b, C = nd.c;
+        const float l0[3] = {A.x, A.y, A.z}, h0[3] = {A.w, B.x, B.y};
+        const float l1[3] = {B.z, B.w, C.x}, h1[3] = {C.y, C.z, C.w};
+        for (int a = 0; a < 3; ++a) {
+            lo[a][m] = side ? l1[a] : l0[a];
+            hi[a][m] = side ? h1[a] : h0[a];
+        }
+        ref[m] = side ? nd.d.y : nd.d.x;
+        cnt[m] = side ? nd.d.w : (nd.d.z & 0x3fffffffu);
+        ++m;
+    };
+    const TravNode nd = nodes[i];
+    for (int side = 0; side < 2; ++side) {
+        const uint32_t r = side ? nd.d.y : nd.d.x;
+        if (r & kLeafBit) {
+            put(nd, side);
+        } else {
+            const TravNode c = nodes[r];
+            put(c, 0);
+            put(c, 1);
+        }
+    }
+    WideNode w;
+    for (int a = 0; a < 3; ++a) {
+        w.lo[a] = make_float4(lo[a][0], lo[a][1], lo[a][2], lo[a][3]);
+        w.hi[a] = make_float4(hi[a][0], hi[a][1], hi[a][2], hi[a][3]);
+    }
+    w.ref = make_uint4(ref[0], ref[1], ref[2], ref[3]);
+    w.cnt = make_uint4(cnt[0], cnt[1], cnt[2], cnt[3]);
+    wide[i] = w;
+}
+
 __global__ void k_offset_trav(const TravNode *src, uint32_t n, uint32_t node_base, uint32_t slot_base, TravNode *dst)
 {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1269,9 +1320,12 @@ ks_status build_sbvh(ks_scene *scene, const ks_sbvh_options &o, float *build_ms)
         return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_build_bvh: bucket_count must be >= 2");
     if (scene->n_tris == 0)
         return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_build_bvh: scene has no triangles");
-    cudaEvent_t ev0, ev1;
+    cudaEvent_t ev0, ev1, ev2, ev3;
     KS_CUDA_TRY(ctx, cudaEventCreate(&ev0));
     KS_CUDA_TRY(ctx, cudaEventCreate(&ev1));
+    KS_CUDA_TRY(ctx, cudaEventCreate(&ev2));
+    KS_CUDA_TRY(ctx, cudaEventCreate(&ev3));
+    bool widened = false;
     KS_CUDA_TRY(ctx, cudaEventRecord(ev0, st));
     ks_status s = KS_OK;
     if (scene->n_instances > 0) {
@@ -1292,13 +1346,31 @@ ks_status build_sbvh(ks_scene *scene, const ks_sbvh_options &o, float *build_ms)
             scene->n_trav = r.n_trav;
             scene->root_count = r.n_prims;
             scene->root_ref = r.n_trav > 0 ? 0u : kLeafBit;
+            // the renderer's 4-wide view of the tree (timed with the build)
+            if (scene->wide_nodes.alloc(r.n_trav > 0 ? r.n_trav : 1) != cudaSuccess) {
+                s = fail(ctx, KS_ERR_OUT_OF_MEMORY, "ks_scene_build_bvh: wide nodes");
+            } else if (r.n_trav > 0) {
+                cudaEventRecord(ev2, st);
+                k_widen<<<grid_for(r.n_trav, 256), 256, 0, st>>>(scene->trav_nodes.ptr, r.n_trav,
+                                                                  scene->wide_nodes.ptr);
+                cudaEventRecord(ev3, st);
+                widened = true;
+            }
         }
     }
     float ms = 0;
     cudaEventSynchronize(ev1);
     cudaEventElapsedTime(&ms, ev0, ev1);
+    if (widened) {
+        float mw = 0;
+        cudaEventSynchronize(ev3);
+        cudaEventElapsedTime(&mw, ev2, ev3);
+        ms += mw;
+    }
     cudaEventDestroy(ev0);
     cudaEventDestroy(ev1);
+    cudaEventDestroy(ev2);
+    cudaEventDestroy(ev3);
     if (s != KS_OK)
         return s;
     if (build_ms)

@@ -61,8 +61,10 @@ __global__ void trace_kernel(const TravNode *nodes, const float4 *tris, uint32_t
 }
 
 // ks_trace_rays for flat scenes: the same queries as trace_kernel, traversed by trav_step with
-// dynamic ray fetch (each ray makes the same tests as traverse(): same triangle, t and barycentrics).
-__global__ void __launch_bounds__(128) trace_kernel_pt(const TravNode *nodes, const float4 *tris, uint32_t root_ref,
+// dynamic ray fetch.  Node = TravNode: each ray makes the same tests as traverse() (same triangle, t
+// and barycentrics); Node = WideNode (ks_trace_rays_wide): the renderer's 4-wide traversal.
+template <class Node>
+__global__ void __launch_bounds__(128) trace_kernel_pt(const Node *nodes, const float4 *tris, uint32_t root_ref,
                                                        uint32_t root_count, float bx0, float by0, float bz0, float bx1,
                                                        float by1, float bz1, const float *rays, uint32_t n, int any_hit,
                                                        int culling, uint32_t *tri_out, float *t_out, float *bary_out,
@@ -403,14 +405,19 @@ ks_status ks_sbvh_export(const ks_scene *scene, float *node_bounds, uint32_t *no
     return KS_OK;
 }
 
-ks_status ks_trace_rays(ks_scene *scene, const float *rays, uint32_t n, int any_hit, int culling, uint32_t *tri_idx,
-                        float *t, float *bary)
+} // extern "C"
+
+// ks_trace_rays and ks_trace_rays_wide (wide: the renderer's 4-wide traversal, flat scenes only).
+static ks_status trace_rays_impl(ks_scene *scene, const float *rays, uint32_t n, int any_hit, int culling,
+                                 uint32_t *tri_idx, float *t, float *bary, bool wide, const char *name)
 {
     if (!scene || !rays || !tri_idx || (!any_hit && (!t || !bary)) || culling < 0 || culling > 2)
-        return fail(scene ? scene->ctx : nullptr, KS_ERR_INVALID_ARGUMENT, "ks_trace_rays: bad argument");
+        return fail(scene ? scene->ctx : nullptr, KS_ERR_INVALID_ARGUMENT, std::string(name) + ": bad argument");
     ks_context *ctx = scene->ctx;
     if (!scene->bvh_built)
-        return fail(ctx, KS_ERR_NOT_BUILT, "ks_trace_rays: call ks_scene_build_bvh first");
+        return fail(ctx, KS_ERR_NOT_BUILT, std::string(name) + ": call ks_scene_build_bvh first");
+    if (wide && scene->n_instances)
+        return fail(ctx, KS_ERR_UNSUPPORTED, std::string(name) + ": instanced scenes have no 4-wide view");
     if (n == 0)
         return KS_OK;
     KS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
@@ -435,12 +442,21 @@ ks_status ks_trace_rays(ks_scene *scene, const float *rays, uint32_t n, int any_
         KS_CUDA_TRY(ctx, d_fetch.alloc(1));
         KS_CUDA_TRY(ctx, cudaMemsetAsync(d_fetch.ptr, 0, sizeof(uint32_t), st));
         int per_sm = 1;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_kernel_pt, 128, 0);
+        if (wide)
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_kernel_pt<WideNode>, 128, 0);
+        else
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_kernel_pt<TravNode>, 128, 0);
         const unsigned grid = std::min<unsigned>((n + 127) / 128, (unsigned)std::max(per_sm, 1) * ctx->sm_count);
-        trace_kernel_pt<<<grid, 128, 0, st>>>(scene->trav_nodes.ptr, scene->prim_tris.ptr, scene->root_ref,
-                                              scene->root_count, b[0], b[1], b[2], b[3], b[4], b[5], d_rays.ptr, n,
-                                              any_hit, culling, d_tri.ptr, d_t.ptr, d_bary.ptr, d_flag.ptr,
-                                              d_fetch.ptr);
+        if (wide)
+            trace_kernel_pt<<<grid, 128, 0, st>>>(scene->wide_nodes.ptr, scene->prim_tris.ptr, scene->root_ref,
+                                                  scene->root_count, b[0], b[1], b[2], b[3], b[4], b[5], d_rays.ptr,
+                                                  n, any_hit, culling, d_tri.ptr, d_t.ptr, d_bary.ptr, d_flag.ptr,
+                                                  d_fetch.ptr);
+        else
+            trace_kernel_pt<<<grid, 128, 0, st>>>(scene->trav_nodes.ptr, scene->prim_tris.ptr, scene->root_ref,
+                                                  scene->root_count, b[0], b[1], b[2], b[3], b[4], b[5], d_rays.ptr,
+                                                  n, any_hit, culling, d_tri.ptr, d_t.ptr, d_bary.ptr, d_flag.ptr,
+                                                  d_fetch.ptr);
     }
     KS_CUDA_TRY(ctx, cudaGetLastError());
     int overflow = 0;
@@ -452,8 +468,22 @@ ks_status ks_trace_rays(ks_scene *scene, const float *rays, uint32_t n, int any_
     KS_CUDA_TRY(ctx, cudaMemcpyAsync(&overflow, d_flag.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
     KS_CUDA_TRY(ctx, cudaStreamSynchronize(st));
     if (overflow)
-        return fail(ctx, KS_ERR_QUEUE_OVERFLOW, "ks_trace_rays: traversal stack depth exceeded");
+        return fail(ctx, KS_ERR_QUEUE_OVERFLOW, std::string(name) + ": traversal stack depth exceeded");
     return KS_OK;
+}
+
+extern "C" {
+
+ks_status ks_trace_rays(ks_scene *scene, const float *rays, uint32_t n, int any_hit, int culling, uint32_t *tri_idx,
+                        float *t, float *bary)
+{
+    return trace_rays_impl(scene, rays, n, any_hit, culling, tri_idx, t, bary, false, "ks_trace_rays");
+}
+
+ks_status ks_trace_rays_wide(ks_scene *scene, const float *rays, uint32_t n, int any_hit, int culling,
+                             uint32_t *tri_idx, float *t, float *bary)
+{
+    return trace_rays_impl(scene, rays, n, any_hit, culling, tri_idx, t, bary, true, "ks_trace_rays_wide");
 }
 
 } // extern "C"

@@ -29,6 +29,20 @@ struct TravNode
 };
 constexpr uint32_t kLeafBit = 0x80000000u;
 
+// 4-wide view of the same SBVH, read by the renderer's traversal kernels: wide node i holds the
+// children of interior node i, each interior child replaced by its own two children (2 to 4 slots).
+// Slot boxes are the SBVH's boxes of those nodes; unused slots hold an empty box (lo +inf, hi -inf),
+// which the slab test always rejects.  Indexed like the TravNode array (entries of nodes at odd
+// depth are written but never read), so child refs need no renumbering.
+struct WideNode
+{
+    float4 lo[3]; // per axis: the 4 slots' lower bounds
+    float4 hi[3]; // per axis: the 4 slots' upper bounds
+    uint4 ref;    // child refs (kLeafBit: leaf, first primitive slot)
+    uint4 cnt;    // primitive counts of leaf children
+};
+static_assert(sizeof(WideNode) == 128, "one 128-byte line per wide node");
+
 // Device copy of one material (constant principled fields + emission).
 struct MaterialGPU
 {
@@ -72,6 +86,7 @@ struct ks_scene
     uint32_t n_nodes = 0, n_prims = 0;
     // traversal layout
     ksb::DevBuf<ksb::TravNode> trav_nodes;
+    ksb::DevBuf<ksb::WideNode> wide_nodes; // flat scenes: the 4-wide view of trav_nodes
     ksb::DevBuf<float4> prim_tris; // 3 float4 per primitive slot: v0 (+tri index bits in w), v1, v2
     uint32_t n_trav = 0;
     uint32_t root_ref = 0;   // ref of the root (leaf bit when the whole tree is one leaf)

@@ -307,11 +307,14 @@ constexpr int kTravBlock = 128;
 #ifndef KS_SMEM_STACK
 #define KS_SMEM_STACK 8
 #endif
+// Capacity: the binary traversal pushes at most one entry per level and stops at kStackDepth; the
+// 4-wide one pushes up to three per wide level and stops at kWideStackDepth.
+constexpr int kWideStackDepth = 96;
 constexpr int kSmemStack = KS_SMEM_STACK < kStackDepth ? KS_SMEM_STACK : kStackDepth;
 struct TravStack
 {
     uint4 *sm; // this thread's column of the block's shared array: entry i at sm[i * kTravBlock]
-    uint4 loc[kStackDepth - kSmemStack > 0 ? kStackDepth - kSmemStack : 1];
+    uint4 loc[kWideStackDepth - kSmemStack];
     KS_D void set(int i, uint4 e)
     {
         if (i < kSmemStack)
@@ -380,6 +383,143 @@ KS_D int trav_interior(const TravNode *__restrict__ nodes, TravState &s, TravSta
     return 1;
 }
 
+// Interior step of the 4-wide view (WideNode): the slots' boxes are tested with the same slab test,
+// the ray descends into the nearest hit slot (smallest entry time, then lowest slot) and the other
+// hit slots are pushed farthest first, each with its entry time (re-checked against tmax when
+// popped, as in trav_interior).  Any-hit queries skip the ordering.  Returns 1 / 0 / -1 like
+// trav_interior.  The set of leaves a closest-hit ray can reach is that of the binary tree (a
+// slot's slab interval lies inside its parent's: same operations, monotone rounding), so the
+// closest hit is the binary traversal's up to the order of exact ties.
+template <bool kAnyHit>
+KS_D int trav_wide(const WideNode *__restrict__ wide, TravState &s, TravStack &stack, int &overflow,
+                   TravCount *count)
+{
+    const WideNode *n = wide + s.ref;
+    if (count)
+        count->nodes += 2; // 128 bytes: two 64-byte node units
+    const float4 lx = __ldg(&n->lo[0]), ly = __ldg(&n->lo[1]), lz = __ldg(&n->lo[2]);
+    const float4 hx = __ldg(&n->hi[0]), hy = __ldg(&n->hi[1]), hz = __ldg(&n->hi[2]);
+    const uint4 ref = __ldg(&n->ref), cnt = __ldg(&n->cnt);
+    const float blo[3][4] = {{lx.x, lx.y, lx.z, lx.w}, {ly.x, ly.y, ly.z, ly.w}, {lz.x, lz.y, lz.z, lz.w}};
+    const float bhi[3][4] = {{hx.x, hx.y, hx.z, hx.w}, {hy.x, hy.y, hy.z, hy.w}, {hz.x, hz.y, hz.z, hz.w}};
+    const uint32_t refs[4] = {ref.x, ref.y, ref.z, ref.w}, cnts[4] = {cnt.x, cnt.y, cnt.z, cnt.w};
+    float t0[4];
+    bool ok[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float bmin[3] = {blo[0][k], blo[1][k], blo[2][k]}, bmax[3] = {bhi[0][k], bhi[1][k], bhi[2][k]};
+        float a, b;
+        ok[k] = slab(s.ray, s.bh, bmin, bmax, a, b) && b > s.ray.tmin && a < s.ray.tmax;
+        t0[k] = a;
+    }
+    int n_hit = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        n_hit += ok[k] ? 1 : 0;
+    if (n_hit == 0)
+        return 0;
+    if (s.sp + n_hit - 1 > kWideStackDepth) {
+        overflow = 1;
+        return -1;
+    }
+    if constexpr (kAnyHit) {
+        bool first = true;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (!ok[k])
+                continue;
+            if (first) {
+                s.ref = refs[k];
+                s.cnt = cnts[k];
+                first = false;
+            } else {
+                stack.set(s.sp++, make_uint4(refs[k], cnts[k], __float_as_uint(t0[k]), 0u));
+            }
+        }
+    } else if (n_hit <= 2) {
+        // one or two slots hit (the common cases): nearest first, the other pushed
+        int a = -1, b = -1;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (!ok[k])
+                continue;
+            if (a < 0)
+                a = k;
+            else
+                b = k;
+        }
+        float ta = 0.0f, tb = 0.0f;
+        uint32_t ra = 0, ca = 0, rb = 0, cb = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (k == a) {
+                ta = t0[k];
+                ra = refs[k];
+                ca = cnts[k];
+            }
+            if (k == b) {
+                tb = t0[k];
+                rb = refs[k];
+                cb = cnts[k];
+            }
+        }
+        if (b >= 0 && tb < ta) { // strictly nearer (ties keep the lower slot first)
+            const float tt = ta;
+            ta = tb;
+            tb = tt;
+            const uint32_t r2 = ra, c2 = ca;
+            ra = rb;
+            ca = cb;
+            rb = r2;
+            cb = c2;
+        }
+        if (b >= 0)
+            stack.set(s.sp++, make_uint4(rb, cb, __float_as_uint(tb), 0u));
+        s.ref = ra;
+        s.cnt = ca;
+    } else {
+        // rank of each hit slot by (entry time, slot index); rank 0 is visited next
+        int rank[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            int r = 0;
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if (j != k && ok[j] && (t0[j] < t0[k] || (t0[j] == t0[k] && j < k)))
+                    ++r;
+            rank[k] = ok[k] ? r : -1;
+        }
+        for (int r = n_hit - 1; r >= 0; --r) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                if (rank[k] != r)
+                    continue;
+                if (r == 0) {
+                    s.ref = refs[k];
+                    s.cnt = cnts[k];
+                } else {
+                    stack.set(s.sp++, make_uint4(refs[k], cnts[k], __float_as_uint(t0[k]), 0u));
+                }
+            }
+        }
+    }
+    return 1;
+}
+
+// Interior step for either tree layout.
+template <bool kAnyHit>
+KS_D int trav_node(const TravNode *__restrict__ nodes, TravState &s, TravStack &stack, int &overflow,
+                   TravCount *count)
+{
+    return trav_interior(nodes, s, stack, overflow, count);
+}
+template <bool kAnyHit>
+KS_D int trav_node(const WideNode *__restrict__ nodes, TravState &s, TravStack &stack, int &overflow,
+                   TravCount *count)
+{
+    return trav_wide<kAnyHit>(nodes, s, stack, overflow, count);
+}
+
 // Pops the next node whose entry time is below the current tmax; false when the stack is empty.
 KS_D bool trav_pop(TravState &s, const TravStack &stack)
 {
@@ -429,15 +569,15 @@ KS_D bool trav_leaf(const float4 *__restrict__ tris, TravState &s, int culling, 
 
 // One step; returns true when the traversal of the ray is over (any-hit: found an occluder).
 // A step visits one node (an interior node or a leaf), then descends or pops.
-template <bool kAnyHit>
-KS_D bool trav_step(const TravNode *__restrict__ nodes, const float4 *__restrict__ tris, TravState &s,
+template <bool kAnyHit, class Node>
+KS_D bool trav_step(const Node *__restrict__ nodes, const float4 *__restrict__ tris, TravState &s,
                     TravStack &stack, int culling, int &overflow, TravCount *count)
 {
     if (s.ref & kLeafBit) {
         if (trav_leaf<kAnyHit>(tris, s, culling, count))
             return true;
     } else {
-        const int r = trav_interior(nodes, s, stack, overflow, count);
+        const int r = trav_node<kAnyHit>(nodes, s, stack, overflow, count);
         if (r != 0)
             return r < 0;
     }
@@ -455,8 +595,8 @@ KS_D bool trav_step(const TravNode *__restrict__ nodes, const float4 *__restrict
 #ifndef KS_LEAF_BATCH
 #define KS_LEAF_BATCH 8
 #endif
-template <bool kAnyHit>
-KS_D bool trav_warp_step(const TravNode *__restrict__ nodes, const float4 *__restrict__ tris, TravState &s,
+template <bool kAnyHit, class Node>
+KS_D bool trav_warp_step(const Node *__restrict__ nodes, const float4 *__restrict__ tris, TravState &s,
                          TravStack &stack, int culling, int &overflow, TravCount *count, bool busy)
 {
     if constexpr (kAnyHit || KS_LEAF_BATCH == 0) {
@@ -473,7 +613,7 @@ KS_D bool trav_warp_step(const TravNode *__restrict__ nodes, const float4 *__res
         }
         if (!busy || at_leaf)
             return false;
-        const int r = trav_interior(nodes, s, stack, overflow, count);
+        const int r = trav_node<false>(nodes, s, stack, overflow, count);
         if (r != 0)
             return r < 0;
         return !trav_pop(s, stack);

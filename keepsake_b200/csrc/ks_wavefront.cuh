@@ -259,6 +259,20 @@ KS_D f3 clamp_contrib(f3 v, int bounce_for_direct, const RenderParams &rp, bool 
     return v;
 }
 
+// The tree a kernel traverses: the SBVH nodes or their 4-wide view.
+template <class Node>
+KS_D const Node *tree_of(const SceneView &sv);
+template <>
+KS_D const TravNode *tree_of<TravNode>(const SceneView &sv)
+{
+    return sv.nodes;
+}
+template <>
+KS_D const WideNode *tree_of<WideNode>(const SceneView &sv)
+{
+    return sv.wide;
+}
+
 // ---- shading launchers (ks_shade.cu) ----------------------------------------------------------
 // k_sample: Sobol values and the NEE light sample of every path in the hit queue.
 void launch_sample(bool batch, unsigned grid, cudaStream_t st, const SceneView &sv, const RenderParams &rp,

@@ -93,7 +93,7 @@ def test_builder_topology_icosphere(ctx, level):
     _check_build(ctx, v, i)
 
 
-def _check_trace(scene, ref, rays, max_tie_frac=0.0):
+def _check_trace(scene, ref, rays, max_tie_frac=0.0, wide=False):
     """Hit ids, distances and barycentrics must match bit for bit.  The one documented exception
     is a near tie: triangles hit at the same or a few-ulp-apart t (duplicate or coplanar
     overlapping triangles, a shared edge or vertex).  The order of the triangles inside a leaf
@@ -101,8 +101,10 @@ def _check_trace(scene, ref, rays, max_tie_frac=0.0):
     reproduce (leaf contents are identical as multisets); with a near tie that order decides
     which triangle is accepted first, and because the triangle test compares T against
     tmax * det in scaled form, it can also decide whether a triangle of a later leaf passes.
-    For such rays the distances must agree within 8 ulp."""
-    tri, t, bary = scene.trace(rays)
+    For such rays the distances must agree within 8 ulp.  wide: the renderer's 4-wide traversal
+    (ks_trace_rays_wide), whose visiting order differs from the reference's, so exact ties may
+    resolve to the other triangle as well."""
+    tri, t, bary = scene.trace(rays, wide=wide)
     rtri, rt, rbary = ref.intersect(rays)
     hit = rtri != 0xFFFFFFFF
     assert np.array_equal(tri != 0xFFFFFFFF, hit), "hit/miss differs"
@@ -114,7 +116,7 @@ def _check_trace(scene, ref, rays, max_tie_frac=0.0):
     if tie.any():
         ulps = np.abs(t[tie].view(np.int32).astype(np.int64) - rt[tie].view(np.int32).astype(np.int64))
         assert ulps.max() <= 8, f"tie distances differ by {ulps.max()} ulp"
-    occ, _, _ = scene.trace(rays, any_hit=True)
+    occ, _, _ = scene.trace(rays, any_hit=True, wide=wide)
     rocc, _, _ = ref.intersect(rays, any_hit=True)
     assert np.array_equal(occ, rocc), "occlusion results differ"
     return hit.mean()
@@ -162,3 +164,51 @@ def test_trace_icosphere_bit_exact(ctx):
     frac = _check_trace(s, ref, scenes.rays_at_triangles(v, i, 200000, seed=8), max_tie_frac=0.02)
     assert frac > 0.5
     _check_trace(s, ref, scenes.random_rays(v, 200000, seed=9, inside=False), max_tie_frac=1e-4)
+
+
+@pytest.mark.gpu
+def test_trace_wide_matches_reference(ctx):
+    """The renderer's 4-wide traversal against the reference SBVH queries: same hits and occlusion,
+    identical ids, distances and barycentrics except at exact ties."""
+    v, i = scenes.soup(5000, seed=7)
+    s, ref = _check_build(ctx, v, i)
+    _check_trace(s, ref, scenes.random_rays(v, 20000, seed=1), wide=True)
+    _check_trace(s, ref, scenes.random_rays(v, 20000, seed=2, inside=False), wide=True)
+    _check_trace(s, ref, scenes.rays_at_triangles(v, i, 20000, seed=3), max_tie_frac=1e-3, wide=True)
+    _check_trace(s, ref, scenes.random_rays(v, 20000, seed=4, tmax=0.7), wide=True)
+    # 12 identical triangles: every ray that hits them is an exact tie, which either traversal
+    # order may resolve to any of the 12 (distances still within 8 ulp)
+    v, i = scenes.degenerate_soup(1)
+    s, ref = _check_build(ctx, v, i)
+    _check_trace(s, ref, scenes.rays_at_triangles(v, i, 20000, seed=5), max_tie_frac=1.0, wide=True)
+
+
+@pytest.mark.gpu
+def test_trace_wide_icosphere(ctx):
+    import keepsake_b200 as ks
+    g = ks.Generated("icosphere", 0, level=8)
+    v, i = g.flat_geometry()
+    s, ref = _check_build(ctx, v, i)
+    frac = _check_trace(s, ref, scenes.rays_at_triangles(v, i, 200000, seed=8), max_tie_frac=0.02, wide=True)
+    assert frac > 0.5
+    _check_trace(s, ref, scenes.random_rays(v, 200000, seed=9, inside=False), max_tie_frac=1e-4, wide=True)
+    for culling in (0, 1):
+        rays = scenes.rays_at_triangles(v, i, 20000, seed=6)
+        a, _, _ = s.trace(rays, culling=culling, wide=True)
+        b, _, _ = s.trace(rays, culling=culling)
+        assert (a != b).mean() <= 0.02
+
+
+@pytest.mark.gpu
+def test_trace_wide_rejects_instanced(ctx):
+    import keepsake_b200 as ks
+    g = ks.Generated("instanced", 1, sky=(64, 32), resolution=(32, 32), prototypes=2, instances=3, frequency=4,
+                     emitters=1)
+    s = ks.Scene(ctx, g.desc)
+    s.build_bvh()
+    rays = np.zeros((4, 8), np.float32)
+    rays[:, 4] = 1.0
+    rays[:, 7] = 1e30
+    with pytest.raises(RuntimeError, match="4-wide"):
+        s.trace(rays, wide=True)
+    s.close()
