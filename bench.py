@@ -81,6 +81,7 @@ def make_generated(ks):
 
 
 TTR_W, TTR_H, TTR_TARGET, TTR_REF_SPP, TTR_MAX_SPP = 1920, 1080, 1e-2, 2048, 1024
+TTR_PRETRAIN_PASSES = 192
 
 
 def time_to_relmse(ks, ctx, torch, with_cpu, guide_options=None, guide_params=None):
@@ -106,7 +107,7 @@ def time_to_relmse(ks, ctx, torch, with_cpu, guide_options=None, guide_params=No
     fg = torch.where(w0[:, None] == 0, torch.zeros_like(acc), acc / torch.clamp(w0[:, None], min=1e-300))
     ref = (w[:, None] * fg).contiguous()
 
-    def run(guide, max_passes=None):
+    def run(guide, max_passes=None, frozen=False):
         acc.zero_()
         wts.zero_()
         torch.cuda.synchronize()
@@ -130,6 +131,8 @@ def time_to_relmse(ks, ctx, torch, with_cpu, guide_options=None, guide_params=No
         if guide is not None:
             kw = dict(train_passes=1 << 20, train_batch=1 << 18, max_records=1 << 20)
             kw.update(guide_options or {})
+            if frozen:
+                kw.update(train_passes=0, guide_from_pass=0)
             opts = ks.GuideRenderOptions.make(**kw)
         sc.render_device_progress(cam, p, acc.data_ptr(), wts.data_ptr(), cb, guide=guide, options=opts)
         s = sc.stats()
@@ -159,6 +162,20 @@ def time_to_relmse(ks, ctx, torch, with_cpu, guide_options=None, guide_params=No
     gp.update(guide_params or {})
     guide = ks.Guide(ctx, bound, **gp)
     guided = run(guide)
+    # the same guide trained further (untimed), then frozen: what a trained proposal gains per
+    # sample once its training is paid for (e.g. by an earlier frame of the same scene)
+    t0 = time.perf_counter()
+    acc.zero_()
+    wts.zero_()
+    pt = ks.SmallPTParams.make(render_width=TTR_W, render_height=TTR_H, spp=TTR_PRETRAIN_PASSES, bounces=BOUNCES,
+                               rng_seed=11, spp_prog_interval=1)
+    sc.render_device_progress(cam, pt, acc.data_ptr(), wts.data_ptr(), lambda spp: False, guide=guide,
+                              options=ks.GuideRenderOptions.make(train_passes=1 << 20, train_batch=1 << 18,
+                                                                 max_records=1 << 20))
+    torch.cuda.synchronize()
+    pre_s = time.perf_counter() - t0
+    frozen = run(guide, frozen=True)
+    frozen.update(pretrain_passes=TTR_PRETRAIN_PASSES + (guided["last"]["spp"] or 0), pretrain_seconds=pre_s)
     guide.close()
     res = {"target_rel_mse": TTR_TARGET, "eps": 1e-2,
            "workload": f"icosphere_l8 glossy (roughness U[0.02,0.2]) behind an occluder slab, {TTR_W}x{TTR_H}, "
@@ -167,7 +184,7 @@ def time_to_relmse(ks, ctx, torch, with_cpu, guide_options=None, guide_params=No
                      "minus the time spent in the per-pass error evaluation; device_seconds: the library's "
                      "CUDA-event time of the same render call",
            "reference": {"spp": TTR_REF_SPP, "seed": 1000, "seconds": ref_s},
-           "plain": plain, "guided": guided}
+           "plain": plain, "guided": guided, "guided_pretrained": frozen}
     if with_cpu and plain["spp"]:
         threads = os.cpu_count() or 1
         sys.path.insert(0, os.path.join(ROOT, "tests"))
