@@ -68,10 +68,12 @@ void ks_context_destroy(ks_context *ctx)
     if (!ctx)
         return;
     cudaSetDevice(ctx->device);
-    if (ctx->stream) {
+    if (ctx->stream)
         cudaStreamSynchronize(ctx->stream);
+    ctx->render_cache.reset();
+    ctx->build_cache.reset();
+    if (ctx->stream)
         cudaStreamDestroy(ctx->stream);
-    }
     delete ctx;
 }
 

@@ -523,6 +523,48 @@ struct RenderWork
     uint32_t capacity = 0;
 };
 
+// Buffers of the single-job renders kept by the context between calls: allocating and freeing the
+// wavefront state (about 1.3 GB at 4 M path slots) and the accumulators took tens of milliseconds
+// per render.  A render that starts while the cache is in use (from a progress callback) uses
+// buffers of its own.
+struct RenderCache
+{
+    RenderWork work;
+    bool work_busy = false;
+    DevBuf<double> accum, weights; // the host-buffer entry's device accumulators
+    double *staging = nullptr;     // pinned host copy of them
+    size_t staging_n = 0;
+    bool host_busy = false;
+    ~RenderCache()
+    {
+        if (staging)
+            cudaFreeHost(staging);
+    }
+};
+
+static RenderCache &render_cache(ks_context *ctx)
+{
+    if (!ctx->render_cache)
+        ctx->render_cache = std::make_shared<RenderCache>();
+    return *static_cast<RenderCache *>(ctx->render_cache.get());
+}
+
+// Marks a cached buffer set in use for a scope.
+struct CacheLease
+{
+    bool *flag;
+    explicit CacheLease(bool *f) : flag(f)
+    {
+        if (flag)
+            *flag = true;
+    }
+    ~CacheLease()
+    {
+        if (flag)
+            *flag = false;
+    }
+};
+
 // RenderParams of one render (SmallPTInput fields + camera); false for an empty crop window.
 static bool fill_params(const ks_camera_desc *cam, const ks_small_pt_params *in, RenderParams &rp)
 {
@@ -593,21 +635,24 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
     SceneView sv = make_view(scene);
     const uint32_t n_pix = (uint32_t)rp.cw * (uint32_t)rp.ch;
     const uint64_t max_interval = (uint64_t)n_pix * (uint64_t)std::min(in->spp, in->spp_prog_interval);
-    RenderWork w;
+    RenderCache &rc = render_cache(ctx);
+    RenderWork own;
+    RenderWork &w = rc.work_busy ? own : rc.work;
+    CacheLease lease(rc.work_busy ? nullptr : &rc.work_busy);
     w.capacity = (uint32_t)std::min<uint64_t>(max_interval, 1u << KS_WAVE_LOG2);
     for (int b = 0; b < 2; ++b)
         for (int f = 0; f < 4; ++f)
-            KS_CUDA_TRY(ctx, w.state[b][f].alloc(w.capacity));
-    KS_CUDA_TRY(ctx, w.hits.alloc(w.capacity));
+            KS_CUDA_TRY(ctx, w.state[b][f].reserve(w.capacity));
+    KS_CUDA_TRY(ctx, w.hits.reserve(w.capacity));
     if (scene->n_instances)
-        KS_CUDA_TRY(ctx, w.hit_inst.alloc(w.capacity));
-    KS_CUDA_TRY(ctx, w.samples.alloc(4 * (size_t)w.capacity));
-    KS_CUDA_TRY(ctx, w.queue[0].alloc(w.capacity));
-    KS_CUDA_TRY(ctx, w.queue[1].alloc(w.capacity));
+        KS_CUDA_TRY(ctx, w.hit_inst.reserve(w.capacity));
+    KS_CUDA_TRY(ctx, w.samples.reserve(4 * (size_t)w.capacity));
+    KS_CUDA_TRY(ctx, w.queue[0].reserve(w.capacity));
+    KS_CUDA_TRY(ctx, w.queue[1].reserve(w.capacity));
     for (int f = 0; f < 4; ++f)
-        KS_CUDA_TRY(ctx, w.shadow[f].alloc(w.capacity));
-    KS_CUDA_TRY(ctx, w.counters.alloc(kCounters));
-    KS_CUDA_TRY(ctx, w.overflow.alloc(1));
+        KS_CUDA_TRY(ctx, w.shadow[f].reserve(w.capacity));
+    KS_CUDA_TRY(ctx, w.counters.reserve(kCounters));
+    KS_CUDA_TRY(ctx, w.overflow.reserve(1));
     DevBuf<unsigned long long> work; // ext nodes, ext tris, shadow nodes, shadow tris
     KS_CUDA_TRY(ctx, work.alloc(4));
     KS_CUDA_TRY(ctx, cudaMemsetAsync(work.ptr, 0, 4 * sizeof(unsigned long long), st));
@@ -1100,22 +1145,42 @@ static ks_status render_host(ks_scene *scene, const ks_camera_desc *camera, cons
         return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_small_pt_render: bad resolution");
     size_t na = (size_t)params->render_width * params->render_height * 3;
     size_t nw = (size_t)params->render_width * params->render_height * 2;
-    DevBuf<double> da, dw;
-    KS_CUDA_TRY(ctx, da.alloc(na));
-    KS_CUDA_TRY(ctx, dw.alloc(nw));
+    RenderCache &rc = render_cache(ctx);
+    DevBuf<double> own_a, own_w;
+    const bool cached = !rc.host_busy;
+    CacheLease lease(cached ? &rc.host_busy : nullptr);
+    DevBuf<double> &da = cached ? rc.accum : own_a, &dw = cached ? rc.weights : own_w;
+    KS_CUDA_TRY(ctx, da.reserve(na));
+    KS_CUDA_TRY(ctx, dw.reserve(nw));
     KS_CUDA_TRY(ctx, cudaMemsetAsync(da.ptr, 0, na * sizeof(double), ctx->stream));
     KS_CUDA_TRY(ctx, cudaMemsetAsync(dw.ptr, 0, nw * sizeof(double), ctx->stream));
     ks_status s = render_impl(scene, camera, params, cb, user, da.ptr, dw.ptr, accum_rgb, weights, guide, gopt);
     if (s != KS_OK)
         return s;
-    std::vector<double> ha(na), hw(nw);
-    KS_CUDA_TRY(ctx, cudaMemcpyAsync(ha.data(), da.ptr, na * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    KS_CUDA_TRY(ctx, cudaMemcpyAsync(hw.data(), dw.ptr, nw * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    // through pinned staging (pageable copies run at a fraction of the link's speed)
+    std::vector<double> own_h;
+    double *h = nullptr;
+    if (cached) {
+        if (rc.staging_n < na + nw) {
+            if (rc.staging)
+                cudaFreeHost(rc.staging);
+            rc.staging = nullptr;
+            rc.staging_n = 0;
+            KS_CUDA_TRY(ctx, cudaMallocHost((void **)&rc.staging, (na + nw) * sizeof(double)));
+            rc.staging_n = na + nw;
+        }
+        h = rc.staging;
+    } else {
+        own_h.resize(na + nw);
+        h = own_h.data();
+    }
+    KS_CUDA_TRY(ctx, cudaMemcpyAsync(h, da.ptr, na * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    KS_CUDA_TRY(ctx, cudaMemcpyAsync(h + na, dw.ptr, nw * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     KS_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     for (size_t k = 0; k < na; ++k)
-        accum_rgb[k] += ha[k];
+        accum_rgb[k] += h[k];
     for (size_t k = 0; k < nw; ++k)
-        weights[k] += hw[k];
+        weights[k] += h[na + k];
     return KS_OK;
 }
 

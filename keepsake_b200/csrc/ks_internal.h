@@ -4,6 +4,7 @@
 #include "../../include/ks_b200.h"
 
 #include <cuda_runtime.h>
+#include <memory>
 #include <string>
 
 struct ks_context
@@ -12,6 +13,9 @@ struct ks_context
     cudaStream_t stream = nullptr;
     std::string last_error;
     int sm_count = 148;
+    // buffers the renders and the SBVH builder keep between calls (owned by ks_integrator.cu and
+    // ks_sbvh_build.cu; freed at destroy)
+    std::shared_ptr<void> render_cache, build_cache;
 };
 
 namespace ksb

@@ -308,7 +308,7 @@ ks_status build_lights(ks_scene *s)
         sky_power_mean = (Phi[0] + Phi[1] + Phi[2]) / 3.0f;
     }
     // ---- mesh lights (host: constant emission, a few triangles) ----
-    std::vector<float> h_verts(3 * (size_t)s->n_verts);
+    std::vector<float> h_verts;
     std::vector<uint32_t> h_idx;
     std::vector<uint32_t> ml_tri;
     std::vector<float> ml_area, ml_importance;
@@ -321,6 +321,7 @@ ks_status build_lights(ks_scene *s)
     std::vector<int32_t> tri_light;
     if (any_emission) {
         h_idx.resize(3 * (size_t)s->n_tris);
+        h_verts.resize(3 * (size_t)s->n_verts);
         KS_CUDA_TRY(ctx, cudaMemcpy(h_verts.data(), s->verts.ptr, s->verts.bytes(), cudaMemcpyDeviceToHost));
         KS_CUDA_TRY(ctx, cudaMemcpy(h_idx.data(), s->indices.ptr, s->indices.bytes(), cudaMemcpyDeviceToHost));
         tri_light.assign(s->n_tris, -1);

@@ -868,30 +868,55 @@ struct RangeOut
 
 // `done` (may be null) is recorded on the stream after the last build kernel, before the scratch
 // buffers are released.
-static ks_status build_range(ks_context *ctx, const float *verts, const uint32_t *indices, uint32_t tri_begin,
-                             uint32_t n_tris, const Params &p, RangeOut &out, cudaEvent_t done = nullptr)
+// Scratch of build_range, kept by the context between builds: growing these buffers level by level
+// costs a few hundred allocations per build (each replaced buffer's cudaFree waits for the
+// device), so a context reuses them; they grow to the largest tree built on it and are freed with
+// the context.
+struct BuildScratch
 {
-    cudaStream_t st = ctx->stream;
-
     DevBuf<BRef> refs_a, refs_b;
     DevBuf<LevelNode> nodes_a, nodes_b;
     DevBuf<Item> items;
     DevBuf<NodeInfo> info;
     DevBuf<uint32_t> bnd, obj, sp, item_cnt, item_off, cl, cr, cp, sl, sr, spool, split_flag, split_scan, pool, flag;
+    DevBuf<uint32_t> interior_flag, interior_scan;
     DevBuf<BuildRec> recs;
     ScanScratch scan;
+};
+
+static BuildScratch &build_scratch(ks_context *ctx)
+{
+    if (!ctx->build_cache)
+        ctx->build_cache = std::make_shared<BuildScratch>();
+    return *static_cast<BuildScratch *>(ctx->build_cache.get());
+}
+
+static ks_status build_range(ks_context *ctx, const float *verts, const uint32_t *indices, uint32_t tri_begin,
+                             uint32_t n_tris, const Params &p, RangeOut &out, cudaEvent_t done = nullptr)
+{
+    cudaStream_t st = ctx->stream;
+    BuildScratch &bs = build_scratch(ctx);
+    auto &refs_a = bs.refs_a, &refs_b = bs.refs_b;
+    auto &nodes_a = bs.nodes_a, &nodes_b = bs.nodes_b;
+    auto &items = bs.items;
+    auto &info = bs.info;
+    auto &bnd = bs.bnd, &obj = bs.obj, &sp = bs.sp, &item_cnt = bs.item_cnt, &item_off = bs.item_off;
+    auto &cl = bs.cl, &cr = bs.cr, &cp = bs.cp, &sl = bs.sl, &sr = bs.sr, &spool = bs.spool;
+    auto &split_flag = bs.split_flag, &split_scan = bs.split_scan, &pool = bs.pool, &flag = bs.flag;
+    auto &recs = bs.recs;
+    auto &scan = bs.scan;
 
     size_t ref_cap = (size_t)n_tris * 2 + 1024;
-    KS_CUDA_TRY(ctx, refs_a.alloc(ref_cap));
-    KS_CUDA_TRY(ctx, refs_b.alloc(ref_cap));
-    KS_CUDA_TRY(ctx, pool.alloc(ref_cap));
+    KS_CUDA_TRY(ctx, refs_a.reserve(ref_cap));
+    KS_CUDA_TRY(ctx, refs_b.reserve(ref_cap));
+    KS_CUDA_TRY(ctx, pool.reserve(ref_cap));
     size_t rec_cap = (size_t)n_tris * 4 + 1024;
-    KS_CUDA_TRY(ctx, recs.alloc(rec_cap));
-    KS_CUDA_TRY(ctx, flag.alloc(1));
+    KS_CUDA_TRY(ctx, recs.reserve(rec_cap));
+    KS_CUDA_TRY(ctx, flag.reserve(1));
 
     k_init_refs<<<grid_for(n_tris, 256), 256, 0, st>>>(verts, indices, tri_begin, n_tris, refs_a.ptr);
     LevelNode root{0, n_tris, 0, 0};
-    KS_CUDA_TRY(ctx, nodes_a.alloc(1));
+    KS_CUDA_TRY(ctx, nodes_a.reserve(1));
     KS_CUDA_TRY(ctx, cudaMemcpyAsync(nodes_a.ptr, &root, sizeof(root), cudaMemcpyHostToDevice, st));
 
     uint32_t n_active = 1, n_refs = n_tris, build_base = 0, pool_used = 0;
@@ -1007,9 +1032,9 @@ static ks_status build_range(ks_context *ctx, const float *verts, const uint32_t
     }
     KS_CUDA_TRY(ctx, out.ref_nodes.alloc(n_nodes));
     KS_CUDA_TRY(ctx, out.prims.alloc(pool_used));
-    DevBuf<uint32_t> interior_flag, interior_scan;
-    KS_CUDA_TRY(ctx, interior_flag.alloc(n_nodes));
-    KS_CUDA_TRY(ctx, interior_scan.alloc(n_nodes + 1));
+    auto &interior_flag = bs.interior_flag, &interior_scan = bs.interior_scan;
+    KS_CUDA_TRY(ctx, interior_flag.reserve(n_nodes));
+    KS_CUDA_TRY(ctx, interior_scan.reserve(n_nodes + 1));
     k_emit<<<grid_for(n_nodes, 256), 256, 0, st>>>(recs.ptr, n_nodes, pool.ptr, out.ref_nodes.ptr, out.prims.ptr,
                                                    interior_flag.ptr);
     KS_CUDA_TRY(ctx, exclusive_scan(interior_flag.ptr, interior_scan.ptr, n_nodes, scan, st));
