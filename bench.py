@@ -505,18 +505,25 @@ def main():
     h2d += len(g.materials) * 72 + (g.sky_map.nbytes if g.sky_map is not None else 0)
     d2h = W_RES * H_RES * 5 * 8
     e2e_rays, e2e_t = 0, 0.0
+    e2e_parts = []
     for k in range(e2e_steps + 1):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         sc = ks.Scene(ctx, g.desc)
+        t1 = time.perf_counter()
         sc.build_bvh()
+        t2 = time.perf_counter()
         sc.render(cam, params)
+        t3 = time.perf_counter()
         st = sc.stats()
         sc.close()
+        t4 = time.perf_counter()
         if k == 0:
             continue  # untimed warm-up step
-        e2e_t += time.perf_counter() - t0
+        e2e_t += t4 - t0
         e2e_rays += st.extension_rays + st.shadow_rays
+        e2e_parts.append({"scene_create": t1 - t0, "build": t2 - t1, "render": t3 - t2, "render_device": st.ms_total / 1e3,
+                          "destroy": t4 - t3})
     if pg:
         t = torch.tensor([e2e_t], dtype=torch.float64, device="cuda")
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
@@ -525,7 +532,9 @@ def main():
         pg.all_reduce(r)
         e2e_rays = int(r.item())
     e2e = {"value": e2e_rays / e2e_t / 1e6 if e2e_t > 0 else None, "unit": "Mrays/s", "h2d_bytes_per_step": h2d,
-           "d2h_bytes_per_step": d2h, "steps": e2e_steps, "timing": "host wall clock around synchronous C-ABI calls"}
+           "d2h_bytes_per_step": d2h, "steps": e2e_steps, "timing": "host wall clock around synchronous C-ABI calls",
+           "step_seconds": {key: statistics.median(p[key] for p in e2e_parts) for key in e2e_parts[0]} if e2e_parts
+           else None}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
