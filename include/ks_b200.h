@@ -162,11 +162,12 @@ ks_status ks_sbvh_export(const ks_scene *scene, float *node_bounds, uint32_t *no
 ks_status ks_trace_rays(ks_scene *scene, const float *rays, uint32_t n, int any_hit, int culling, uint32_t *tri_idx,
                         float *t, float *bary);
 
-/* The same queries through the renderer's traversal: a 4-wide view of the same SBVH (each node
- * with its interior children replaced by theirs, boxes tested with the same slab test), nearest
- * slot first.  It reaches the same leaves, so the result equals ks_trace_rays' except where two
- * triangles are hit at exactly the same distance (the visiting order then picks one of them).
- * Flat scenes only (instanced scenes: KS_ERR_UNSUPPORTED).  Replaces the same reference calls as
+/* The same queries through the renderer's traversal kernels.  Flat scenes: a 4-wide view of the
+ * same SBVH (each node with its interior children replaced by theirs, boxes tested with the same
+ * slab test), nearest slot first; it reaches the same leaves, so the result equals
+ * ks_trace_rays' except where two triangles are hit at exactly the same distance (the visiting
+ * order then picks one of them).  Instanced scenes: the persistent two-level traversal, the same
+ * tests per ray as ks_trace_rays (identical results).  Replaces the same reference calls as
  * ks_trace_rays (cuda/sbvh.cu:512-603); exists to test the rendering traversal. */
 ks_status ks_trace_rays_wide(ks_scene *scene, const float *rays, uint32_t n, int any_hit, int culling,
                              uint32_t *tri_idx, float *t, float *bary);

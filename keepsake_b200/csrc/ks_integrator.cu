@@ -470,6 +470,108 @@ __global__ void __launch_bounds__(128, KS_TRAV_MIN_BLOCKS) k_shadow_pt(const __g
     flush_counts(tc, work);
 }
 
+// ---- persistent two-level traversal (instanced scenes) ----------------------------------------
+#ifndef KS_INST_MIN_BLOCKS
+#define KS_INST_MIN_BLOCKS 1
+#endif
+// The same warp-level ray fetch as k_extend_pt / k_shadow_pt over inst_step (ks_traverse.cuh):
+// each ray makes the tests of traverse_instances, in resumable steps.
+__global__ void __launch_bounds__(128, KS_INST_MIN_BLOCKS) k_extend_inst_pt(const __grid_constant__ SceneView sv, PathBuf pb,
+                                                        uint32_t count, float4 *hits, uint32_t *hit_inst,
+                                                        uint32_t *fetch, int *overflow, unsigned long long *work)
+{
+    TravCount tc;
+    KS_TRAV_STACK(stack);
+    InstTravState s;
+    uint4 tstack[kTlasStackDepth];
+    uint32_t ray = ~0u;
+    bool drained = false;
+    int of = 0;
+    while (true) {
+        const uint32_t id = warp_fetch(fetch, count, ray == ~0u, drained);
+        if (id != ~0u) {
+            float4 a = pb.o_pdf[id], b = pb.d_info[id];
+            RayQuery q;
+            q.o = mk(a.x, a.y, a.z);
+            q.d = mk(b.x, b.y, b.z);
+            q.tmin = 0.0f;
+            q.tmax = kInf;
+            if (inst_begin(s, sv.inst, q)) {
+                ray = id;
+            } else {
+                hits[id] = make_float4(0, 0, 0, fbits(~0u));
+                hit_inst[id] = 0;
+            }
+        }
+        if (__ballot_sync(0xffffffffu, ray != ~0u) == 0) {
+            if (drained)
+                break;
+            continue;
+        }
+        while (true) {
+            if (ray != ~0u && inst_step<false>(sv.nodes, sv.prim_tris, sv.inst, s, tstack, stack, 2, of, &tc)) {
+                hits[ray] = s.hit.tri != ~0u ? make_float4(s.hit.t, s.hit.b1, s.hit.b2, fbits(s.hit.slot))
+                                             : make_float4(0, 0, 0, fbits(~0u));
+                hit_inst[ray] = s.hit_inst;
+                ray = ~0u;
+            }
+            const int n_idle = __popc(__ballot_sync(0xffffffffu, ray == ~0u));
+            if (n_idle == 32 || (!drained && n_idle >= KS_TRAV_REFILL))
+                break;
+        }
+    }
+    if (of)
+        atomicOr(overflow, 1);
+    flush_counts(tc, work);
+}
+
+__global__ void __launch_bounds__(128, KS_INST_MIN_BLOCKS) k_shadow_inst_pt(const __grid_constant__ SceneView sv, ShadowBuf sb,
+                                                        const uint32_t *shadow_count, uint32_t *fetch, PathBuf nxt,
+                                                        double *accum, double *weights, int *overflow,
+                                                        unsigned long long *work, GuideView gv)
+{
+    const uint32_t count = *shadow_count;
+    TravCount tc;
+    KS_TRAV_STACK(stack);
+    InstTravState s;
+    uint4 tstack[kTlasStackDepth];
+    uint32_t ray = ~0u;
+    bool drained = false;
+    int of = 0;
+    while (true) {
+        const uint32_t id = warp_fetch(fetch, count, ray == ~0u, drained);
+        if (id != ~0u) {
+            float4 a = sb.o_tmax[id], b = sb.d_target[id];
+            RayQuery q;
+            q.o = mk(a.x, a.y, a.z);
+            q.d = mk(b.x, b.y, b.z);
+            q.tmin = 0.0f;
+            q.tmax = a.w;
+            if (inst_begin(s, sv.inst, q))
+                ray = id;
+            else
+                shadow_done<false>(sb, id, false, nxt, accum, weights, gv, BatchView{});
+        }
+        if (__ballot_sync(0xffffffffu, ray != ~0u) == 0) {
+            if (drained)
+                break;
+            continue;
+        }
+        while (true) {
+            if (ray != ~0u && inst_step<true>(sv.nodes, sv.prim_tris, sv.inst, s, tstack, stack, 2, of, &tc)) {
+                shadow_done<false>(sb, ray, s.hit.tri != ~0u, nxt, accum, weights, gv, BatchView{});
+                ray = ~0u;
+            }
+            const int n_idle = __popc(__ballot_sync(0xffffffffu, ray == ~0u));
+            if (n_idle == 32 || (!drained && n_idle >= KS_TRAV_REFILL))
+                break;
+        }
+    }
+    if (of)
+        atomicOr(overflow, 1);
+    flush_counts(tc, work);
+}
+
 // Relative MSE of the composited image (RenderTarget2::composite_and_save_to_exr,
 // render_target.cpp:181-205) against a reference: sum over pixels and channels of
 // (x - r)^2 / (r^2 + eps), accumulated in FP64 (one atomic per warp).
@@ -711,6 +813,8 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
     const unsigned max_grid = (unsigned)ctx->sm_count * 16;
     const unsigned ext_grid = resident_grid(k_extend_pt<false>, 128, ctx->sm_count);
     const unsigned shadow_grid = resident_grid(k_shadow_pt<false>, 128, ctx->sm_count);
+    const unsigned inst_ext_grid = resident_grid(k_extend_inst_pt, 128, ctx->sm_count);
+    const unsigned inst_shadow_grid = resident_grid(k_shadow_inst_pt, 128, ctx->sm_count);
     int cur = 0;
     cudaError_t err = cudaSuccess;
     std::vector<double> cb_acc, cb_w;
@@ -746,10 +850,19 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
             cudaMemsetAsync(w.counters.ptr, 0, sizeof(uint32_t) * kCounters, st);
             unsigned grid = std::min<unsigned>((count + 127) / 128, max_grid);
             cudaEventRecord(ev[1], st);
-            if (scene->n_instances)
-                k_extend<true><<<grid, 128, 0, st>>>(sv, pb[cur], count, w.hits.ptr, w.hit_inst.ptr, w.queue[0].ptr,
-                                                     w.queue[1].ptr, w.counters.ptr + 2, w.overflow.ptr, work.ptr, BatchView{});
-            else if (!kPersistentTraversal)
+            if (scene->n_instances) {
+                if (kPersistentTraversal) {
+                    k_extend_inst_pt<<<std::min(grid, inst_ext_grid), 128, 0, st>>>(
+                        sv, pb[cur], count, w.hits.ptr, w.hit_inst.ptr, w.counters.ptr + 4, w.overflow.ptr, work.ptr);
+                    k_build_queues<false><<<std::min((count + 255) / 256, max_grid), 256, 0, st>>>(
+                        w.hits.ptr, count, w.queue[0].ptr, w.queue[1].ptr, w.counters.ptr + 2, BatchView{});
+                    stats.kernel_launches++;
+                } else {
+                    k_extend<true><<<grid, 128, 0, st>>>(sv, pb[cur], count, w.hits.ptr, w.hit_inst.ptr,
+                                                         w.queue[0].ptr, w.queue[1].ptr, w.counters.ptr + 2,
+                                                         w.overflow.ptr, work.ptr, BatchView{});
+                }
+            } else if (!kPersistentTraversal)
                 k_extend<false><<<grid, 128, 0, st>>>(sv, pb[cur], count, w.hits.ptr, nullptr, w.queue[0].ptr,
                                                       w.queue[1].ptr, w.counters.ptr + 2, w.overflow.ptr, work.ptr,
                                                       BatchView{});
@@ -780,10 +893,15 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
                              w.hit_inst.ptr, w.samples.ptr, w.queue[miss].ptr, w.counters.ptr + 2 + miss,
                              w.counters.ptr, sb, w.counters.ptr + 1, d_accum, d_weights, gv, BatchView{});
             cudaEventRecord(ev[3], st);
-            if (scene->n_instances)
-                k_shadow<true><<<grid, 128, 0, st>>>(sv, sb, w.counters.ptr + 1, pb[1 - cur], d_accum, d_weights,
-                                                     w.overflow.ptr, work.ptr + 2, gv, BatchView{});
-            else if (!kPersistentTraversal)
+            if (scene->n_instances) {
+                if (kPersistentTraversal)
+                    k_shadow_inst_pt<<<std::min(grid, inst_shadow_grid), 128, 0, st>>>(
+                        sv, sb, w.counters.ptr + 1, w.counters.ptr + 5, pb[1 - cur], d_accum, d_weights,
+                        w.overflow.ptr, work.ptr + 2, gv);
+                else
+                    k_shadow<true><<<grid, 128, 0, st>>>(sv, sb, w.counters.ptr + 1, pb[1 - cur], d_accum, d_weights,
+                                                         w.overflow.ptr, work.ptr + 2, gv, BatchView{});
+            } else if (!kPersistentTraversal)
                 k_shadow<false><<<grid, 128, 0, st>>>(sv, sb, w.counters.ptr + 1, pb[1 - cur], d_accum, d_weights,
                                                       w.overflow.ptr, work.ptr + 2, gv, BatchView{});
             else

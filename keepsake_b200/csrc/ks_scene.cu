@@ -123,6 +123,68 @@ __global__ void __launch_bounds__(128) trace_kernel_pt(const Node *nodes, const 
         atomicOr(overflow_flag, 1);
 }
 
+// ks_trace_rays_wide for instanced scenes: the renderer's persistent two-level traversal
+// (inst_step), the same tests per ray as trace_kernel's traverse_instances.
+__global__ void __launch_bounds__(128) trace_inst_kernel_pt(const TravNode *nodes, const float4 *tris,
+                                                            InstanceView iv, const float *rays, uint32_t n,
+                                                            int any_hit, int culling, uint32_t *tri_out,
+                                                            float *t_out, float *bary_out, int *overflow_flag,
+                                                            uint32_t *fetch)
+{
+    KS_TRAV_STACK(stack);
+    InstTravState s;
+    uint4 tstack[kTlasStackDepth];
+    uint32_t ray = ~0u;
+    bool drained = false;
+    int overflow = 0;
+    auto finish = [&](uint32_t i, const Hit &h) {
+        if (any_hit) {
+            tri_out[i] = h.tri != ~0u ? 1u : 0u;
+            return;
+        }
+        tri_out[i] = h.tri;
+        t_out[i] = h.tri != ~0u ? h.t : -kInf;
+        bary_out[3 * i + 0] = h.tri != ~0u ? h.b0 : 0.0f;
+        bary_out[3 * i + 1] = h.tri != ~0u ? h.b1 : 0.0f;
+        bary_out[3 * i + 2] = h.tri != ~0u ? h.b2 : 0.0f;
+    };
+    while (true) {
+        const uint32_t id = warp_fetch(fetch, n, ray == ~0u, drained);
+        if (id != ~0u) {
+            const float *r = rays + 8 * (size_t)id;
+            RayQuery q;
+            q.o = mk(r[0], r[1], r[2]);
+            q.tmin = r[3];
+            q.d = mk(r[4], r[5], r[6]);
+            q.tmax = r[7];
+            if (inst_begin(s, iv, q))
+                ray = id;
+            else
+                finish(id, s.hit);
+        }
+        if (__ballot_sync(0xffffffffu, ray != ~0u) == 0) {
+            if (drained)
+                break;
+            continue;
+        }
+        while (true) {
+            if (ray != ~0u) {
+                const bool done = any_hit ? inst_step<true>(nodes, tris, iv, s, tstack, stack, culling, overflow, nullptr)
+                                          : inst_step<false>(nodes, tris, iv, s, tstack, stack, culling, overflow, nullptr);
+                if (done) {
+                    finish(ray, s.hit);
+                    ray = ~0u;
+                }
+            }
+            const int n_idle = __popc(__ballot_sync(0xffffffffu, ray == ~0u));
+            if (n_idle == 32 || (!drained && n_idle >= KS_TRAV_REFILL))
+                break;
+        }
+    }
+    if (overflow)
+        atomicOr(overflow_flag, 1);
+}
+
 bool valid_material(const ks_material_desc &m)
 {
     auto finite = [](float x) { return x == x && x < 3.0e38f && x > -3.0e38f; };
@@ -407,7 +469,8 @@ ks_status ks_sbvh_export(const ks_scene *scene, float *node_bounds, uint32_t *no
 
 } // extern "C"
 
-// ks_trace_rays and ks_trace_rays_wide (wide: the renderer's 4-wide traversal, flat scenes only).
+// ks_trace_rays and ks_trace_rays_wide (wide: the renderer's traversal kernels: the 4-wide view for
+// flat scenes, the persistent two-level traversal for instanced ones).
 static ks_status trace_rays_impl(ks_scene *scene, const float *rays, uint32_t n, int any_hit, int culling,
                                  uint32_t *tri_idx, float *t, float *bary, bool wide, const char *name)
 {
@@ -416,8 +479,6 @@ static ks_status trace_rays_impl(ks_scene *scene, const float *rays, uint32_t n,
     ks_context *ctx = scene->ctx;
     if (!scene->bvh_built)
         return fail(ctx, KS_ERR_NOT_BUILT, std::string(name) + ": call ks_scene_build_bvh first");
-    if (wide && scene->n_instances)
-        return fail(ctx, KS_ERR_UNSUPPORTED, std::string(name) + ": instanced scenes have no 4-wide view");
     if (n == 0)
         return KS_OK;
     KS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
@@ -433,7 +494,16 @@ static ks_status trace_rays_impl(ks_scene *scene, const float *rays, uint32_t n,
     KS_CUDA_TRY(ctx, cudaMemcpyAsync(d_rays.ptr, rays, d_rays.bytes(), cudaMemcpyHostToDevice, st));
     KS_CUDA_TRY(ctx, cudaMemsetAsync(d_flag.ptr, 0, sizeof(int), st));
     const float *b = scene->scene_bound;
-    if (scene->n_instances) {
+    if (scene->n_instances && wide) {
+        KS_CUDA_TRY(ctx, d_fetch.alloc(1));
+        KS_CUDA_TRY(ctx, cudaMemsetAsync(d_fetch.ptr, 0, sizeof(uint32_t), st));
+        int per_sm = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_inst_kernel_pt, 128, 0);
+        const unsigned grid = std::min<unsigned>((n + 127) / 128, (unsigned)std::max(per_sm, 1) * ctx->sm_count);
+        trace_inst_kernel_pt<<<grid, 128, 0, st>>>(scene->trav_nodes.ptr, scene->prim_tris.ptr, make_view(scene).inst,
+                                                   d_rays.ptr, n, any_hit, culling, d_tri.ptr, d_t.ptr, d_bary.ptr,
+                                                   d_flag.ptr, d_fetch.ptr);
+    } else if (scene->n_instances) {
         trace_kernel<<<(n + 127) / 128, 128, 0, st>>>(scene->trav_nodes.ptr, scene->prim_tris.ptr, scene->root_ref,
                                                        scene->root_count, b[0], b[1], b[2], b[3], b[4], b[5],
                                                        d_rays.ptr, n, any_hit, culling, d_tri.ptr, d_t.ptr,

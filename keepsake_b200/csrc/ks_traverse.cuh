@@ -767,4 +767,146 @@ KS_D bool traverse_instances(const TravNode *__restrict__ nodes, const float4 *_
     return hit.tri != ~0u;
 }
 
+
+// ---- resumable two-level traversal (persistent kernels, instanced scenes) -------------------
+// traverse_instances cut into steps: a step visits one TLAS node, starts the BLAS traversal of
+// the next instance of a TLAS leaf, or advances that BLAS traversal by one trav_step.  Each ray
+// makes the same TLAS and BLAS tests as traverse_instances, so hits, distances and instances are
+// identical; only the interleaving of rays changes.  The BLAS stack is the caller's TravStack, the
+// TLAS stack (kTlasStackDepth entries) a separate caller array, so that the scalar state can stay
+// in registers.
+struct InstTravState
+{
+    RayQuery ray;       // world-space ray; tmax shrinks with the hits found
+    BoxHelper bh;       // of the world-space ray (TLAS boxes)
+    uint32_t ref, cnt;  // current TLAS node
+    uint32_t item;      // next instance of the current TLAS leaf
+    int sp;             // TLAS stack size
+    bool in_blas;       // a BLAS traversal is running in blas
+    uint32_t inst;      // its instance
+    TravState blas;
+    Hit hit;            // best hit so far
+    uint32_t hit_inst;  // its instance
+};
+
+// False when the ray misses the TLAS root box.
+KS_D bool inst_begin(InstTravState &s, const InstanceView &iv, const RayQuery &ray)
+{
+    s.hit.tri = ~0u;
+    s.hit_inst = 0;
+    s.ray = ray;
+    s.bh = make_box_helper(ray.d);
+    s.sp = 0;
+    s.item = 0;
+    s.in_blas = false;
+    s.ref = iv.root_ref;
+    s.cnt = iv.root_count;
+    float t0, t1;
+    return slab(s.ray, s.bh, iv.bmin, iv.bmax, t0, t1) && t0 < s.ray.tmax && t1 > s.ray.tmin;
+}
+
+// TLAS pop with the tmax re-check; false when the TLAS stack is empty (the ray is done).
+KS_D bool inst_pop(InstTravState &s, const uint4 *tstack)
+{
+    while (s.sp > 0) {
+        const uint4 e = tstack[--s.sp];
+        if (__uint_as_float(e.z) < s.ray.tmax) {
+            s.ref = e.x;
+            s.cnt = e.y;
+            s.item = 0;
+            return true;
+        }
+    }
+    return false;
+}
+
+// One step; true when the ray's traversal is over (any-hit: an occluder was found).
+template <bool kAnyHit>
+KS_D bool inst_step(const TravNode *__restrict__ nodes, const float4 *__restrict__ tris, const InstanceView &iv,
+                    InstTravState &s, uint4 *tstack, TravStack &blas_stack, int culling, int &overflow,
+                    TravCount *count)
+{
+    if (s.in_blas) {
+        if (!trav_step<kAnyHit>(nodes, tris, s.blas, blas_stack, culling, overflow, count))
+            return false;
+        s.in_blas = false;
+        const Hit &h = s.blas.hit;
+        if (h.tri != ~0u) {
+            if (kAnyHit) {
+                s.hit.tri = h.tri;
+                s.hit_inst = s.inst;
+                return true;
+            }
+            if (h.t < s.ray.tmax) {
+                s.ray.tmax = h.t;
+                s.hit = h;
+                s.hit_inst = s.inst;
+            }
+        }
+        ++s.item;
+        return false;
+    }
+    if (s.ref & kLeafBit) {
+        if (s.item < s.cnt) {
+            // the next instance of the leaf: the ray in object space, then its prototype's BLAS
+            const uint32_t id = __ldg(&iv.items[(s.ref & ~kLeafBit) + s.item]);
+            const float *m = iv.inv + 12 * (size_t)id;
+            float mi[12];
+#pragma unroll
+            for (int e = 0; e < 12; ++e)
+                mi[e] = __ldg(&m[e]);
+            RayQuery q;
+            q.o = xf_point(mi, s.ray.o);
+            q.d = xf_dir(mi, s.ray.d);
+            q.tmin = s.ray.tmin;
+            q.tmax = s.ray.tmax;
+            const uint32_t pr = __ldg(&iv.proto[id]);
+            const uint4 r = __ldg(&iv.proto_root[pr]);
+            float pb[6];
+#pragma unroll
+            for (int e = 0; e < 6; ++e)
+                pb[e] = __ldg(&iv.proto_bound[6 * (size_t)pr + e]);
+            if (trav_begin(s.blas, q, r.x, r.y, pb, pb + 3)) {
+                s.in_blas = true;
+                s.inst = id;
+            } else {
+                ++s.item;
+            }
+            return false;
+        }
+        return !inst_pop(s, tstack);
+    }
+    const TravNode *n = iv.tlas + s.ref;
+    if (count)
+        count->nodes++;
+    float4 A = __ldg(&n->a), B = __ldg(&n->b), C = __ldg(&n->c);
+    uint4 D = __ldg(&n->d);
+    float lmin[3] = {A.x, A.y, A.z}, lmax[3] = {A.w, B.x, B.y};
+    float rmin[3] = {B.z, B.w, C.x}, rmax[3] = {C.y, C.z, C.w};
+    float lt0, lt1, rt0, rt1;
+    bool lok = slab(s.ray, s.bh, lmin, lmax, lt0, lt1) && lt1 > s.ray.tmin && lt0 < s.ray.tmax;
+    bool rok = slab(s.ray, s.bh, rmin, rmax, rt0, rt1) && rt1 > s.ray.tmin && rt0 < s.ray.tmax;
+    uint32_t axis = D.z >> 30;
+    uint32_t lcnt = D.z & 0x3fffffffu, rcnt = D.w;
+    bool right_first = s.bh.neg[axis] != 0;
+    uint32_t near_ref = right_first ? D.y : D.x, far_ref = right_first ? D.x : D.y;
+    uint32_t near_cnt = right_first ? rcnt : lcnt, far_cnt = right_first ? lcnt : rcnt;
+    bool near_ok = right_first ? rok : lok, far_ok = right_first ? lok : rok;
+    float far_t = right_first ? lt0 : rt0;
+    if (near_ok && far_ok) {
+        if (s.sp >= kTlasStackDepth) {
+            overflow = 1;
+            return true;
+        }
+        tstack[s.sp++] = make_uint4(far_ref, far_cnt, __float_as_uint(far_t), 0u);
+    }
+    if (near_ok || far_ok) {
+        s.ref = near_ok ? near_ref : far_ref;
+        s.cnt = near_ok ? near_cnt : far_cnt;
+        s.item = 0;
+        return false;
+    }
+    return !inst_pop(s, tstack);
+}
+
 } // namespace ksb

@@ -200,15 +200,31 @@ def test_trace_wide_icosphere(ctx):
 
 
 @pytest.mark.gpu
-def test_trace_wide_rejects_instanced(ctx):
+def test_trace_wide_instanced_identical(ctx):
+    """Instanced scenes: the renderer's persistent two-level traversal makes the same tests per ray
+    as the one-thread-per-ray kernel of ks_trace_rays, so ids, distances, barycentrics and
+    occlusion are identical."""
     import keepsake_b200 as ks
-    g = ks.Generated("instanced", 1, sky=(64, 32), resolution=(32, 32), prototypes=2, instances=3, frequency=4,
-                     emitters=1)
+    g = ks.Generated("instanced", 5, sky=(64, 32), resolution=(32, 32), prototypes=4, instances=24, frequency=6,
+                     emitters=8)
     s = ks.Scene(ctx, g.desc)
     s.build_bvh()
-    rays = np.zeros((4, 8), np.float32)
-    rays[:, 4] = 1.0
-    rays[:, 7] = 1e30
-    with pytest.raises(RuntimeError, match="4-wide"):
-        s.trace(rays, wide=True)
+    base, vs, ids = 0, [], []
+    for mv, mi, _ in g.flattened():
+        vs.append(np.asarray(mv, np.float32))
+        ids.append(np.asarray(mi, np.int64) + base)
+        base += len(mv)
+    v, i = np.concatenate(vs), np.concatenate(ids)
+    for rays in (scenes.random_rays(v, 50000, seed=21), scenes.random_rays(v, 50000, seed=22, inside=False),
+                 scenes.rays_at_triangles(v, i, 50000, seed=23)):
+        a, ta, ba = s.trace(rays, wide=True)
+        b, tb, bb = s.trace(rays)
+        assert np.array_equal(a, b)
+        hit = b != 0xFFFFFFFF
+        assert hit.mean() > 0.05
+        assert np.array_equal(ta[hit].view(np.uint32), tb[hit].view(np.uint32))
+        assert np.array_equal(ba[hit].view(np.uint32), bb[hit].view(np.uint32))
+        oa, _, _ = s.trace(rays, any_hit=True, wide=True)
+        ob, _, _ = s.trace(rays, any_hit=True)
+        assert np.array_equal(oa, ob)
     s.close()
