@@ -166,8 +166,9 @@ ks_status ks_trace_rays(ks_scene *scene, const float *rays, uint32_t n, int any_
  * same SBVH (each node with its interior children replaced by theirs, boxes tested with the same
  * slab test), nearest slot first; it reaches the same leaves, so the result equals
  * ks_trace_rays' except where two triangles are hit at exactly the same distance (the visiting
- * order then picks one of them).  Instanced scenes: the persistent two-level traversal, the same
- * tests per ray as ks_trace_rays (identical results).  Replaces the same reference calls as
+ * order then picks one of them).  Instanced scenes: the persistent two-level traversal over the
+ * TLAS and the 4-wide view of the BLAS nodes, the same except at exact ties.  Replaces the same
+ * reference calls as
  * ks_trace_rays (cuda/sbvh.cu:512-603); exists to test the rendering traversal. */
 ks_status ks_trace_rays_wide(ks_scene *scene, const float *rays, uint32_t n, int any_hit, int culling,
                              uint32_t *tri_idx, float *t, float *bary);

@@ -474,6 +474,11 @@ __global__ void __launch_bounds__(128, KS_TRAV_MIN_BLOCKS) k_shadow_pt(const __g
 #ifndef KS_INST_MIN_BLOCKS
 #define KS_INST_MIN_BLOCKS 1
 #endif
+// BLAS layout of the instanced kernels: the SBVH nodes (0) or their 4-wide view (1).
+#ifndef KS_WIDE_INST
+#define KS_WIDE_INST 1
+#endif
+using InstNode = std::conditional_t<KS_WIDE_INST != 0, WideNode, TravNode>;
 // The same warp-level ray fetch as k_extend_pt / k_shadow_pt over inst_step (ks_traverse.cuh):
 // each ray makes the tests of traverse_instances, in resumable steps.
 __global__ void __launch_bounds__(128, KS_INST_MIN_BLOCKS) k_extend_inst_pt(const __grid_constant__ SceneView sv, PathBuf pb,
@@ -509,7 +514,8 @@ __global__ void __launch_bounds__(128, KS_INST_MIN_BLOCKS) k_extend_inst_pt(cons
             continue;
         }
         while (true) {
-            if (ray != ~0u && inst_step<false>(sv.nodes, sv.prim_tris, sv.inst, s, tstack, stack, 2, of, &tc)) {
+            if (ray != ~0u &&
+                inst_step<false>(tree_of<InstNode>(sv), sv.prim_tris, sv.inst, s, tstack, stack, 2, of, &tc)) {
                 hits[ray] = s.hit.tri != ~0u ? make_float4(s.hit.t, s.hit.b1, s.hit.b2, fbits(s.hit.slot))
                                              : make_float4(0, 0, 0, fbits(~0u));
                 hit_inst[ray] = s.hit_inst;
@@ -558,7 +564,8 @@ __global__ void __launch_bounds__(128, KS_INST_MIN_BLOCKS) k_shadow_inst_pt(cons
             continue;
         }
         while (true) {
-            if (ray != ~0u && inst_step<true>(sv.nodes, sv.prim_tris, sv.inst, s, tstack, stack, 2, of, &tc)) {
+            if (ray != ~0u &&
+                inst_step<true>(tree_of<InstNode>(sv), sv.prim_tris, sv.inst, s, tstack, stack, 2, of, &tc)) {
                 shadow_done<false>(sb, ray, s.hit.tri != ~0u, nxt, accum, weights, gv, BatchView{});
                 ray = ~0u;
             }

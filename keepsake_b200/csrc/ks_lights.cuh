@@ -18,7 +18,7 @@ struct SceneView
 {
     InstanceView inst; // instances (inst.n == 0: flat scene)
     const TravNode *nodes;
-    const WideNode *wide; // flat scenes: 4-wide view of nodes (null for instanced scenes)
+    const WideNode *wide; // 4-wide view of nodes (instanced scenes: of the concatenated BLAS nodes)
     const float4 *prim_tris;
     const float *verts;      // global vertex positions (3 floats each)
     const uint32_t *indices; // global triangle vertex ids (3 each)

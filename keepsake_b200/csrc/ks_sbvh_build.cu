@@ -1273,6 +1273,10 @@ static ks_status build_instanced(ks_scene *scene, const Params &p)
         slot_base += r.n_prims;
     }
     KS_CUDA_TRY(ctx, cudaGetLastError());
+    // the renderer's 4-wide view of the concatenated BLAS nodes (their refs are already global)
+    KS_CUDA_TRY(ctx, scene->wide_nodes.alloc(total_trav > 0 ? total_trav : 1));
+    if (total_trav > 0)
+        k_widen<<<grid_for(total_trav, 256), 256, 0, st>>>(scene->trav_nodes.ptr, total_trav, scene->wide_nodes.ptr);
     // instance boxes: the 8 corners of the prototype box, transformed, padded by a relative epsilon
     TlasBuilder tb;
     for (uint32_t i = 0; i < scene->n_instances; ++i) {

@@ -124,8 +124,8 @@ __global__ void __launch_bounds__(128) trace_kernel_pt(const Node *nodes, const 
 }
 
 // ks_trace_rays_wide for instanced scenes: the renderer's persistent two-level traversal
-// (inst_step), the same tests per ray as trace_kernel's traverse_instances.
-__global__ void __launch_bounds__(128) trace_inst_kernel_pt(const TravNode *nodes, const float4 *tris,
+// (inst_step over the 4-wide view of the BLAS nodes).
+__global__ void __launch_bounds__(128) trace_inst_kernel_pt(const WideNode *nodes, const float4 *tris,
                                                             InstanceView iv, const float *rays, uint32_t n,
                                                             int any_hit, int culling, uint32_t *tri_out,
                                                             float *t_out, float *bary_out, int *overflow_flag,
@@ -500,7 +500,7 @@ static ks_status trace_rays_impl(ks_scene *scene, const float *rays, uint32_t n,
         int per_sm = 1;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_inst_kernel_pt, 128, 0);
         const unsigned grid = std::min<unsigned>((n + 127) / 128, (unsigned)std::max(per_sm, 1) * ctx->sm_count);
-        trace_inst_kernel_pt<<<grid, 128, 0, st>>>(scene->trav_nodes.ptr, scene->prim_tris.ptr, make_view(scene).inst,
+        trace_inst_kernel_pt<<<grid, 128, 0, st>>>(scene->wide_nodes.ptr, scene->prim_tris.ptr, make_view(scene).inst,
                                                    d_rays.ptr, n, any_hit, culling, d_tri.ptr, d_t.ptr, d_bary.ptr,
                                                    d_flag.ptr, d_fetch.ptr);
     } else if (scene->n_instances) {

@@ -86,7 +86,7 @@ struct ks_scene
     uint32_t n_nodes = 0, n_prims = 0;
     // traversal layout
     ksb::DevBuf<ksb::TravNode> trav_nodes;
-    ksb::DevBuf<ksb::WideNode> wide_nodes; // flat scenes: the 4-wide view of trav_nodes
+    ksb::DevBuf<ksb::WideNode> wide_nodes; // the 4-wide view of trav_nodes
     ksb::DevBuf<float4> prim_tris; // 3 float4 per primitive slot: v0 (+tri index bits in w), v1, v2
     uint32_t n_trav = 0;
     uint32_t root_ref = 0;   // ref of the root (leaf bit when the whole tree is one leaf)

@@ -770,9 +770,10 @@ KS_D bool traverse_instances(const TravNode *__restrict__ nodes, const float4 *_
 
 // ---- resumable two-level traversal (persistent kernels, instanced scenes) -------------------
 // traverse_instances cut into steps: a step visits one TLAS node, starts the BLAS traversal of
-// the next instance of a TLAS leaf, or advances that BLAS traversal by one trav_step.  Each ray
-// makes the same TLAS and BLAS tests as traverse_instances, so hits, distances and instances are
-// identical; only the interleaving of rays changes.  The BLAS stack is the caller's TravStack, the
+// the next instance of a TLAS leaf, or advances that BLAS traversal by one trav_step.  With the
+// BLAS in its binary layout (Node = TravNode) each ray makes the same TLAS and BLAS tests as
+// traverse_instances (identical hits, distances and instances); with the 4-wide view (WideNode)
+// the BLAS visiting order differs, which only matters for exact ties.  The BLAS stack is the caller's TravStack, the
 // TLAS stack (kTlasStackDepth entries) a separate caller array, so that the scalar state can stay
 // in registers.
 struct InstTravState
@@ -821,8 +822,8 @@ KS_D bool inst_pop(InstTravState &s, const uint4 *tstack)
 }
 
 // One step; true when the ray's traversal is over (any-hit: an occluder was found).
-template <bool kAnyHit>
-KS_D bool inst_step(const TravNode *__restrict__ nodes, const float4 *__restrict__ tris, const InstanceView &iv,
+template <bool kAnyHit, class Node>
+KS_D bool inst_step(const Node *__restrict__ nodes, const float4 *__restrict__ tris, const InstanceView &iv,
                     InstTravState &s, uint4 *tstack, TravStack &blas_stack, int culling, int &overflow,
                     TravCount *count)
 {
