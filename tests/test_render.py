@@ -3,8 +3,8 @@ small_pt.cpp / nee.cpp / material.cpp / principled_bsdf.cpp / light.cpp over the
 
 Two checks per scene:
   * same seed, same spp: the GPU runs the same estimator on the same Sobol samples, so the
-    images agree up to the last-ulp differences of CUDA's transcendental functions against the
-    host libm (a handful of paths diverge at an edge or a roulette threshold).  Hit/miss weights
+    images agree up to the last-ulp differences of the shading unit's fast-math functions against
+    the host libm (a handful of paths diverge at an edge or a roulette threshold).  Hit/miss weights
     must agree exactly.
   * convergence: the GPU image at N spp has the same relative MSE against a 16x higher-spp FP64
     oracle image as the oracle's own N-spp image (same estimator, same error).
@@ -178,3 +178,54 @@ def test_device_progress_and_rel_mse(ctx):
     img = composite(acc.cpu().numpy().reshape(H, W, 3), wts.cpu().numpy().reshape(H, W, 2))
     assert abs(e_dev - rel_mse(img, ref)) <= 1e-12 * max(1.0, rel_mse(img, ref))
     s.close()
+
+
+@pytest.mark.gpu
+def test_context_keeps_buffers_across_calls():
+    """A context keeps its render buffers and SBVH-build scratch between calls.  Renders that grow
+    and shrink the wavefront, and scenes built after larger ones, must come out as on a fresh
+    context: identical hit/miss weights and trees, images equal up to FP64 summation order."""
+    import keepsake_b200 as ks
+    small_c = CASES["box_room"]
+    big_c = dict(small_c, W=256, H=256, spp=4)
+
+    def render(c, context):
+        g, cam, p = make_case(c)
+        s = ks.Scene(context, g.desc)
+        s.build_bvh()
+        out = s.render(cam, p)
+        s.close()
+        return out
+
+    def tree(level, context):
+        g = ks.Generated("icosphere", 0, level=level)
+        s = ks.Scene(context, g.desc)
+        s.build_bvh()
+        t = s.export_sbvh()
+        s.close()
+        return t
+
+    a = ks.Context(0)
+    try:
+        render(small_c, a)
+        render(big_c, a)
+        acc_a, w_a = render(small_c, a)
+        tree(6, a)
+        t_a = tree(4, a)
+    finally:
+        a.close()
+    b = ks.Context(0)
+    try:
+        acc_b, w_b = render(small_c, b)
+        t_b = tree(4, b)
+    finally:
+        b.close()
+    assert np.array_equal(w_a, w_b)
+    assert rel_mse(composite(acc_a, w_a), composite(acc_b, w_b)) < 1e-12
+    for k in ("bounds", "axis", "right", "prim_offset"):
+        assert np.array_equal(t_a[k], t_b[k]), k
+    # primitives: the same multiset per leaf (their order inside a leaf is not part of the contract)
+    ends = np.append(t_b["prim_offset"][1:], len(t_b["prims"]))
+    for n in np.nonzero(t_b["right"] == 0)[0]:
+        lo, hi = t_b["prim_offset"][n], ends[n]
+        assert np.array_equal(np.sort(t_a["prims"][lo:hi]), np.sort(t_b["prims"][lo:hi]))
