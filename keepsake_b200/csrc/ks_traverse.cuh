@@ -595,25 +595,30 @@ KS_D bool trav_step(const Node *__restrict__ nodes, const float4 *__restrict__ t
 #ifndef KS_LEAF_BATCH
 #define KS_LEAF_BATCH 8
 #endif
+#ifndef KS_LEAF_BATCH_ANY
+#define KS_LEAF_BATCH_ANY 0
+#endif
 template <bool kAnyHit, class Node>
 KS_D bool trav_warp_step(const Node *__restrict__ nodes, const float4 *__restrict__ tris, TravState &s,
                          TravStack &stack, int culling, int &overflow, TravCount *count, bool busy)
 {
-    if constexpr (kAnyHit || KS_LEAF_BATCH == 0) {
+    constexpr int kBatch = kAnyHit ? KS_LEAF_BATCH_ANY : KS_LEAF_BATCH;
+    if constexpr (kBatch == 0) {
         return busy && trav_step<kAnyHit>(nodes, tris, s, stack, culling, overflow, count);
     } else {
         const bool at_leaf = busy && (s.ref & kLeafBit);
         const uint32_t leaves = __ballot_sync(0xffffffffu, at_leaf);
         const uint32_t inner = __ballot_sync(0xffffffffu, busy && !at_leaf);
-        if (__popc(leaves) >= KS_LEAF_BATCH || inner == 0) {
+        if (__popc(leaves) >= kBatch || inner == 0) {
             if (!at_leaf)
                 return false;
-            trav_leaf<false>(tris, s, culling, count);
+            if (trav_leaf<kAnyHit>(tris, s, culling, count))
+                return true;
             return !trav_pop(s, stack);
         }
         if (!busy || at_leaf)
             return false;
-        const int r = trav_node<false>(nodes, s, stack, overflow, count);
+        const int r = trav_node<kAnyHit>(nodes, s, stack, overflow, count);
         if (r != 0)
             return r < 0;
         return !trav_pop(s, stack);
