@@ -271,6 +271,17 @@ def instanced_leg(ks, ctx, torch, spp):
     wts.zero_()
     s.render_device(cam, p, acc.data_ptr(), wts.data_ptr())
     st = s.stats()
+    # the same frame guided (the C5 configuration): 1 spp passes, the guide trained online
+    lo, hi = g.bound
+    guide = ks.Guide(ctx, list(lo - 0.05) + list(hi + 0.05), seed=1)
+    pg = ks.SmallPTParams.make(render_width=3840, render_height=2160, spp=spp, bounces=16, spp_prog_interval=1)
+    acc.zero_()
+    wts.zero_()
+    s.render_guided_device(cam, pg, guide, ks.GuideRenderOptions.make(train_passes=1 << 20, train_batch=1 << 18,
+                                                                      max_records=1 << 20),
+                           acc.data_ptr(), wts.data_ptr())
+    sg = s.stats()
+    guide.close()
     s.close()
     flat = sum(len(g.meshes[first + k]["indices"]) for proto, _ in g.instances
                for first, n in [g.prototypes[proto]] for k in range(n))
@@ -278,7 +289,11 @@ def instanced_leg(ks, ctx, torch, spp):
                         f"3840x2160, {spp} spp, depth 16",
             "unique_triangles": g.n_triangles, "instanced_triangles": flat, "bvh_build_ms": build_ms,
             "ms": st.ms_total, "mrays_per_s": (st.extension_rays + st.shadow_rays) / st.ms_total / 1e3,
-            "mpaths_per_s": st.paths / st.ms_total / 1e3}
+            "mpaths_per_s": st.paths / st.ms_total / 1e3,
+            "guided": {"ms": sg.ms_total, "mrays_per_s": (sg.extension_rays + sg.shadow_rays) / sg.ms_total / 1e3,
+                       "mpaths_per_s": sg.paths / sg.ms_total / 1e3, "passes": spp,
+                       "train_steps": sg.guide_train_steps, "ms_guide_infer": sg.ms_guide_infer,
+                       "ms_guide_train": sg.ms_guide_train}}
 
 
 def cpu_crop_params(ks, crop=CPU_CROP):
