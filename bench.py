@@ -170,8 +170,9 @@ def time_to_relmse(ks, ctx, torch, with_cpu, guide_options=None, guide_params=No
     pt = ks.SmallPTParams.make(render_width=TTR_W, render_height=TTR_H, spp=TTR_PRETRAIN_PASSES, bounces=BOUNCES,
                                rng_seed=11, spp_prog_interval=1)
     sc.render_device_progress(cam, pt, acc.data_ptr(), wts.data_ptr(), lambda spp: False, guide=guide,
-                              options=ks.GuideRenderOptions.make(train_passes=1 << 20, train_batch=1 << 18,
-                                                                 max_records=1 << 20))
+                              options=ks.GuideRenderOptions.make(**{**dict(train_passes=1 << 20, train_batch=1 << 18,
+                                                                              max_records=1 << 20),
+                                                                   **(guide_options or {})}))
     torch.cuda.synchronize()
     pre_s = time.perf_counter() - t0
     frozen = run(guide, frozen=True)

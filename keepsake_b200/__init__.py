@@ -520,7 +520,7 @@ _sig("ks_guide_gradients", [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _u32, ctypes.c_in
 
 class GuideRenderOptions(ctypes.Structure):
     _fields_ = [("guide_from_pass", _i32), ("train_passes", _i32),
-                ("max_records", _u32), ("train_batch", _u32), ("record_bounces", _i32)]
+                ("max_records", _u32), ("train_batch", _u32), ("record_bounces", _i32), ("min_roughness", _f32)]
 
     @staticmethod
     def make(**kw):

@@ -587,7 +587,7 @@ ks_context *context_of(const ks_guide *g) { return g->ctx; }
 
 ks_status infer_paths(ks_guide *g, const uint32_t *queue, const uint32_t *queue_count, const float4 *o_pdf,
                       const float4 *d_info, const float4 *hits, const float4 *prim_tris, const uint32_t *hit_inst,
-                      const float *inst_xf, float4 *lobes, uint32_t cap)
+                      const float *inst_xf, float4 *lobes, uint32_t cap, uint32_t max_rows)
 {
     if (!g->packed) {
         ks_status s = pack(g);
@@ -610,7 +610,11 @@ ks_status infer_paths(ks_guide *g, const uint32_t *queue, const uint32_t *queue_
     a.cap = cap;
     a.alpha_max = g->params.alpha_max;
     a.err = g->err.ptr;
-    k_guide_paths<<<g->ctx->sm_count * kPathCtasPerSm, kThreads, kPathSmem, g->ctx->stream>>>(a);
+    // one CTA per 128-row tile up to one wave of resident CTAs (each CTA loads the 39 KB weight
+    // image and takes TMEM once, so the late bounces' few rows should not start a full wave)
+    const uint32_t tiles = (max_rows + kThreads - 1) / kThreads;
+    const uint32_t grid = std::max(1u, std::min(tiles, (uint32_t)g->ctx->sm_count * kPathCtasPerSm));
+    k_guide_paths<<<grid, kThreads, kPathSmem, g->ctx->stream>>>(a);
     KS_CUDA_TRY(g->ctx, cudaGetLastError());
     return KS_OK;
 }

@@ -36,6 +36,7 @@ struct GuideView
     uint32_t rec_cap;       // 0 = no capture
     uint32_t rec_threshold; // a path records when the low 16 bits of its hash are below this
     uint32_t rec_bounces;   // the recorded bounce is drawn from [0, rec_bounces)
+    float min_roughness;    // vertices below this roughness are not guided (alpha 0) and not recorded
 };
 
 // Selection probability alpha of the guide at path slot i.

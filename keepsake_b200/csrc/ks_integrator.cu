@@ -579,6 +579,40 @@ __global__ void __launch_bounds__(128, KS_INST_MIN_BLOCKS) k_shadow_inst_pt(cons
     flush_counts(tc, work);
 }
 
+// Guided renders: the hit paths the guide is evaluated for (those that sample a direction at this
+// vertex, with a material at least min_roughness rough) go to gqueue; the others get selection
+// probability 0 (their two weight vectors zeroed), so the shading samples their BSDF only.
+__global__ void __launch_bounds__(128) k_guide_filter(const __grid_constant__ SceneView sv, int bounces,
+                                                      float min_roughness, PathBuf cur, const float4 *hits,
+                                                      const uint32_t *queue, const uint32_t *queue_count,
+                                                      uint32_t *gqueue, uint32_t *gcount, float4 *lobes,
+                                                      uint32_t cap)
+{
+    const uint32_t count = *queue_count;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += stride) {
+        const uint32_t q = base + threadIdx.x;
+        bool use = false;
+        uint32_t i = 0;
+        if (q < count) {
+            i = queue[q];
+            const int bounce = (int)(bits(cur.d_info[i].w) & 0xffffu);
+            if (bounce < bounces) {
+                const uint32_t tri = bits(__ldg(&sv.prim_tris[3 * (size_t)bits(hits[i].w)]).w);
+                const uint32_t mesh = __ldg(&sv.tri_mesh[tri]);
+                use = sv.materials[__ldg(&sv.mesh_material[mesh])].roughness >= min_roughness;
+            }
+            if (!use) {
+                lobes[(size_t)8 * cap + i] = make_float4(0, 0, 0, 0);
+                lobes[(size_t)9 * cap + i] = make_float4(0, 0, 0, 0);
+            }
+        }
+        const uint32_t j = warp_append(gcount, use);
+        if (use)
+            gqueue[j] = i;
+    }
+}
+
 // Relative MSE of the composited image (RenderTarget2::composite_and_save_to_exr,
 // render_target.cpp:181-205) against a reference: sum over pixels and channels of
 // (x - r)^2 / (r^2 + eps), accumulated in FP64 (one atomic per warp).
@@ -712,6 +746,7 @@ static bool fill_params(const ks_camera_desc *cam, const ks_small_pt_params *in,
 struct GuideWork
 {
     DevBuf<float4> lobes;
+    DevBuf<uint32_t> gqueue, gcount; // hit paths the guide is evaluated for
     DevBuf<uint32_t> rec[2];
     DevBuf<float4> rec_f4[5]; // pos, wo, wi, ibeta, normal
     DevBuf<float> rec_t;
@@ -780,7 +815,11 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
             go.max_records = 1u << 19;
         if (go.record_bounces <= 0)
             go.record_bounces = 6;
+        if (!(go.min_roughness >= 0.0f))
+            return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_small_pt_render_guided: negative or NaN min_roughness");
         KS_CUDA_TRY(ctx, gw.lobes.alloc((size_t)kGuideLobeVecs * w.capacity));
+        KS_CUDA_TRY(ctx, gw.gqueue.alloc(w.capacity));
+        KS_CUDA_TRY(ctx, gw.gcount.alloc(1));
         for (int b = 0; b < 2; ++b) {
             KS_CUDA_TRY(ctx, gw.rec[b].alloc(w.capacity));
             pb[b].rec = gw.rec[b].ptr;
@@ -802,6 +841,7 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
         gv.rec_t = gw.rec_t.ptr;
         gv.rec_count = gw.rec_count.ptr;
         gv.rec_bounces = (uint32_t)std::max(1, std::min(go.record_bounces, in->bounces));
+        gv.min_roughness = go.min_roughness;
         // about twice max_records candidates per pass; paths that end early record nothing
         const double per_pass = (double)n_pix * std::min(in->spp, in->spp_prog_interval);
         gv.rec_threshold = (uint32_t)std::min(65536.0, std::ceil(65536.0 * 2.0 * go.max_records / per_pass));
@@ -883,9 +923,15 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
             }
             cudaEventRecord(ev[2], st);
             if (guide && gv.active) {
-                ks_status gs = guide_impl::infer_paths(guide, w.queue[0].ptr, w.counters.ptr + 2, pb[cur].o_pdf,
+                // the guide only at vertices that sample a direction with a rough enough BSDF
+                cudaMemsetAsync(gw.gcount.ptr, 0, sizeof(uint32_t), st);
+                k_guide_filter<<<grid, 128, 0, st>>>(sv, rp.bounces, gv.min_roughness, pb[cur], w.hits.ptr,
+                                                     w.queue[0].ptr, w.counters.ptr + 2, gw.gqueue.ptr,
+                                                     gw.gcount.ptr, gw.lobes.ptr, w.capacity);
+                stats.kernel_launches++;
+                ks_status gs = guide_impl::infer_paths(guide, gw.gqueue.ptr, gw.gcount.ptr, pb[cur].o_pdf,
                                                        pb[cur].d_info, w.hits.ptr, sv.prim_tris, w.hit_inst.ptr,
-                                                       sv.inst.xf, gw.lobes.ptr, w.capacity);
+                                                       sv.inst.xf, gw.lobes.ptr, w.capacity, count);
                 if (gs != KS_OK) {
                     err = cudaErrorLaunchFailure;
                     break;
@@ -1324,6 +1370,7 @@ void ks_guide_render_options_default(ks_guide_render_options *o)
     o->max_records = 1u << 19;
     o->train_batch = 1u << 18;
     o->record_bounces = 6;
+    o->min_roughness = 0.3f;
 }
 
 ks_status ks_small_pt_render_guided(ks_scene *scene, const ks_camera_desc *camera, const ks_small_pt_params *params,

@@ -286,7 +286,9 @@ __global__ void __launch_bounds__(128, KS_SHADE_MIN_BLOCKS) k_shade(const __grid
                         }
                         // throughput over the density the direction was drawn from; the MIS weights
                         // with the lights keep the BSDF pdf (pdf_wi), as in the unguided estimator
-                        const float pdf_mix = is_zero(fcos) ? 0.0f : guide_pdf(gv, i, wnext) + (1.0f - al) * p_b;
+                        // (alpha 0: a vertex the guide skipped; its mixture slots hold nothing)
+                        const float q_al = al > 0.0f ? guide_pdf(gv, i, wnext) : 0.0f;
+                        const float pdf_mix = is_zero(fcos) ? 0.0f : q_al + (1.0f - al) * p_b;
                         sbeta = pdf_mix > 0.0f ? fcos / pdf_mix : mk(0, 0, 0);
                         pdf_wi = p_b;
                         p_bsdf = p_b;
@@ -318,7 +320,7 @@ __global__ void __launch_bounds__(128, KS_SHADE_MIN_BLOCKS) k_shade(const __grid
                             n_beta = nbeta;
                             n_info = ((uint32_t)next_dim << 16) | (uint32_t)(bounce + 1);
                             if constexpr (kGuided) {
-                                if (gv.rec_cap && rec == kNoRecord) {
+                                if (gv.rec_cap && rec == kNoRecord && mat.roughness >= gv.min_roughness) {
                                     uint32_t hh = path_hash(pix, smp);
                                     if ((hh & 0xffffu) < gv.rec_threshold && (uint32_t)bounce == (hh >> 16) % gv.rec_bounces) {
                                         want_rec = true;

@@ -111,4 +111,6 @@ def test_guided_render_rejects_bad_options(ctx, setup):
     guide = ks.Guide(ctx, bound)
     with pytest.raises(ks.KsError):
         sc.render_guided(cam, _params(8, 1), guide, ks.GuideRenderOptions.make(train_passes=-1))
+    with pytest.raises(ks.KsError):
+        sc.render_guided(cam, _params(8, 1), guide, ks.GuideRenderOptions.make(min_roughness=-1.0))
     guide.close()
