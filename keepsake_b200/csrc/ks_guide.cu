@@ -132,8 +132,22 @@ __device__ __forceinline__ bool wait_mma(uint64_t *bar, uint32_t &phase, int *ct
 __device__ __forceinline__ uint32_t mlp_prologue(const uint8_t *w_image, uint8_t *sw, uint64_t *bar,
                                                  uint32_t *tmem_slot, int *cta_err, uint32_t cols)
 {
-    for (uint32_t i = threadIdx.x; i < kWImage / 16; i += kThreads)
-        reinterpret_cast<uint4 *>(sw)[i] = reinterpret_cast<const uint4 *>(w_image)[i];
+    // the weight image into shared memory, kCopyBatch loads in flight per thread (a load-store loop
+    // waits for each load: about 20 round trips per thread, most of a small launch's time)
+    constexpr uint32_t kCopyBatch = 10, kVecs = kWImage / 16;
+    const uint4 *src = reinterpret_cast<const uint4 *>(w_image);
+    uint4 *dst = reinterpret_cast<uint4 *>(sw);
+    for (uint32_t base = threadIdx.x; base < kVecs; base += kThreads * kCopyBatch) {
+        uint4 v[kCopyBatch];
+#pragma unroll
+        for (uint32_t c = 0; c < kCopyBatch; ++c)
+            if (base + c * kThreads < kVecs)
+                v[c] = __ldg(&src[base + c * kThreads]);
+#pragma unroll
+        for (uint32_t c = 0; c < kCopyBatch; ++c)
+            if (base + c * kThreads < kVecs)
+                dst[base + c * kThreads] = v[c];
+    }
     if (threadIdx.x == 0) {
         tc::mbar_init(bar, 1);
         *cta_err = 0;
