@@ -147,7 +147,16 @@ def time_to_relmse(ks, ctx, torch, with_cpu, guide_options=None, guide_params=No
         out["mpaths_per_s"] = s.paths / (s.ms_total / 1e3) / 1e6 if s.ms_total > 0 else None
         if guide is not None:
             out.update(train_steps=s.guide_train_steps, records=s.guide_records,
-                       ms_guide_infer=s.ms_guide_infer, ms_guide_train=s.ms_guide_train, ms_total=s.ms_total)
+                       ms_guide_infer=s.ms_guide_infer, ms_guide_train=s.ms_guide_train, ms_total=s.ms_total,
+                       guide_rows=s.guide_rows)
+            if s.ms_guide_infer > 0:
+                # guide inference against the dense BF16 tensor peak: 2 x (4 x 64 x 64 + 48 x 64) FLOPs per
+                # row evaluated (the tcgen05 GEMMs)
+                tflops = s.guide_rows * GUIDE_FLOPS_PER_ROW / (s.ms_guide_infer / 1e3) / 1e12
+                peak, kind = measured_bf16_peak()
+                out["guide_inference_roofline"] = {"bound": "tensor", "achieved": tflops, "peak": peak,
+                                                   "unit": "TFLOP/s", "frac": tflops / peak, "peak_source": kind,
+                                                   "rows": s.guide_rows}
         return out
 
     lo, hi = g.bound
@@ -372,6 +381,18 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+GUIDE_FLOPS_PER_ROW = 2 * (4 * 64 * 64 + 48 * 64)
+
+
+def measured_bf16_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        if "bf16_tflops" in d:
+            return d["bf16_tflops"], "measured"
+    return 1590.0, "fallback"
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -578,6 +599,9 @@ def main():
                        "l2": "inputs larger than L2 (BVH + triangles + sky > 126 MB)",
                        "bvh_build_ms": build_ms},
             "mpaths_per_s": paths / (dev_ms / 1e3) / 1e6,
+            # the two query kinds separately, over the same device time
+            "mrays_per_s_extension": sum(s.extension_rays for s in stats) / (dev_ms / 1e3) / 1e6,
+            "mrays_per_s_shadow": sum(s.shadow_rays for s in stats) / (dev_ms / 1e3) / 1e6,
             "wall_ms_per_step": 1000.0 * wall / args.steps,
             "roofline": roofline,
             "cpu_baseline": cpu,

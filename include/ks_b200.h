@@ -262,6 +262,7 @@ typedef struct ks_render_stats {
     float ms_guide_train;    /* guided renders: training (forward, backward, Adam), summed */
     uint64_t guide_records;  /* guided renders: training samples captured */
     uint32_t guide_train_steps; /* guided renders: Adam steps taken */
+    uint64_t guide_rows;     /* guided renders: path vertices the guide network was evaluated for */
 } ks_render_stats;
 
 ks_status ks_render_stats_last(const ks_scene *scene, ks_render_stats *out);

@@ -210,7 +210,7 @@ class RenderStats(ctypes.Structure):
                 ("ms_shade", _f32), ("ms_shadow", _f32), ("ext_nodes", ctypes.c_uint64),
                 ("ext_tris", ctypes.c_uint64), ("shadow_nodes", ctypes.c_uint64), ("shadow_tris", ctypes.c_uint64),
                 ("ms_guide_infer", _f32), ("ms_guide_train", _f32), ("guide_records", ctypes.c_uint64),
-                ("guide_train_steps", _u32)]
+                ("guide_train_steps", _u32), ("guide_rows", ctypes.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -848,7 +848,8 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
     }
     ShadowBuf sb{w.shadow[0].ptr, w.shadow[1].ptr, w.shadow[2].ptr, w.shadow[3].ptr};
     uint32_t *h_counts = nullptr;
-    KS_CUDA_TRY(ctx, cudaMallocHost((void **)&h_counts, sizeof(uint32_t) * 2));
+    KS_CUDA_TRY(ctx, cudaMallocHost((void **)&h_counts, sizeof(uint32_t) * 3));
+    h_counts[2] = 0;
     cudaEvent_t ev[6];
     for (auto &e : ev)
         cudaEventCreate(&e);
@@ -964,6 +965,8 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
             cudaEventRecord(ev[4], st);
             stats.kernel_launches += 5;
             cudaMemcpyAsync(h_counts, w.counters.ptr, sizeof(uint32_t) * 2, cudaMemcpyDeviceToHost, st);
+            if (guide && gv.active)
+                cudaMemcpyAsync(h_counts + 2, gw.gcount.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
             err = cudaStreamSynchronize(st);
             if (err != cudaSuccess)
                 break;
@@ -980,6 +983,8 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
             cudaEventElapsedTime(&ms, ev[3], ev[4]);
             stats.ms_shadow += ms;
             stats.shadow_rays += h_counts[1];
+            if (guide && gv.active)
+                stats.guide_rows += h_counts[2];
             stats.iterations++;
             cur_count = h_counts[0];
             cur = 1 - cur;
