@@ -514,8 +514,8 @@ __global__ void __launch_bounds__(128, KS_INST_MIN_BLOCKS) k_extend_inst_pt(cons
             continue;
         }
         while (true) {
-            if (ray != ~0u &&
-                inst_step<false>(tree_of<InstNode>(sv), sv.prim_tris, sv.inst, s, tstack, stack, 2, of, &tc)) {
+            if (inst_warp_step<false>(tree_of<InstNode>(sv), sv.prim_tris, sv.inst, s, tstack, stack, 2, of, &tc,
+                                      ray != ~0u)) {
                 hits[ray] = s.hit.tri != ~0u ? make_float4(s.hit.t, s.hit.b1, s.hit.b2, fbits(s.hit.slot))
                                              : make_float4(0, 0, 0, fbits(~0u));
                 hit_inst[ray] = s.hit_inst;

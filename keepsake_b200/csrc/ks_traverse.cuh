@@ -915,4 +915,26 @@ KS_D bool inst_step(const Node *__restrict__ nodes, const float4 *__restrict__ t
     return !inst_pop(s, tstack);
 }
 
+// Warp-wide step of the two-level traversal (every lane calls it; busy: the lane holds a ray).
+// Closest-hit queries batch their BLAS leaf tests like trav_warp_step: a lane whose BLAS node is
+// a leaf waits until KS_LEAF_BATCH lanes (or all busy lanes) are at one.  Each ray's own sequence
+// of tests is that of inst_step.
+template <bool kAnyHit, class Node>
+KS_D bool inst_warp_step(const Node *__restrict__ nodes, const float4 *__restrict__ tris, const InstanceView &iv,
+                         InstTravState &s, uint4 *tstack, TravStack &blas_stack, int culling, int &overflow,
+                         TravCount *count, bool busy)
+{
+    if constexpr (kAnyHit || KS_LEAF_BATCH == 0) {
+        return busy && inst_step<kAnyHit>(nodes, tris, iv, s, tstack, blas_stack, culling, overflow, count);
+    } else {
+        const bool at_leaf = busy && s.in_blas && (s.blas.ref & kLeafBit);
+        const uint32_t leaves = __ballot_sync(0xffffffffu, at_leaf);
+        const uint32_t others = __ballot_sync(0xffffffffu, busy && !at_leaf);
+        const bool leaf_phase = __popc(leaves) >= KS_LEAF_BATCH || others == 0;
+        if (leaf_phase ? !at_leaf : (!busy || at_leaf))
+            return false;
+        return inst_step<false>(nodes, tris, iv, s, tstack, blas_stack, culling, overflow, count);
+    }
+}
+
 } // namespace ksb
