@@ -171,9 +171,27 @@ __device__ __forceinline__ void mlp_epilogue(uint32_t tmem, uint32_t cols)
 
 // Input encoding of this thread's row into X_0^T: 16 hash-grid levels x 2 features, then 16 SH
 // coefficients of wo and 16 of the normal.  Invalid rows are zero.
+// Hash-grid gathers with an L2 evict-last policy: the 64 MB table is read by every inference and
+// training launch, while the wavefront streams gigabytes of path state through L2 in between;
+// the hint keeps the table's lines ahead of those streams.
+__device__ __forceinline__ uint64_t l2_keep_policy()
+{
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+
+__device__ __forceinline__ float2 ld_grid(const float2 *ptr, uint64_t pol)
+{
+    float2 v;
+    asm volatile("ld.global.nc.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;" : "=f"(v.x), "=f"(v.y) : "l"(ptr), "l"(pol));
+    return v;
+}
+
 __device__ __forceinline__ void encode_row(const GridParams &gp, const float *grid, bool valid, f3 pn, f3 wo,
                                            f3 nrm, uint8_t *x0)
 {
+    const uint64_t pol = l2_keep_policy();
     const uint32_t tid = threadIdx.x;
     for (int l = 0; l < kLevels; ++l) {
         float f0 = 0.0f, f1 = 0.0f;
@@ -183,7 +201,7 @@ __device__ __forceinline__ void encode_row(const GridParams &gp, const float *gr
             const float2 *tab = reinterpret_cast<const float2 *>(grid) + (size_t)l * kTableSize;
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
-                float2 e = __ldg(&tab[c.idx[k]]);
+                float2 e = ld_grid(&tab[c.idx[k]], pol);
                 f0 += c.w[k] * e.x;
                 f1 += c.w[k] * e.y;
             }
