@@ -75,6 +75,24 @@ def test_guided_render_bsdf_only_passes_match_plain(ctx, setup):
     assert rel_mse(img, plain) < 1e-10
 
 
+@pytest.mark.gpu
+def test_guided_render_roughness_filter(ctx, setup):
+    """min_roughness above every material: the guide is evaluated for no vertex (alpha 0
+    everywhere), the render samples the BSDF only and comes out as the plain one up to the
+    rounding of dividing by the one-sample MIS density; min_roughness 0 evaluates the guide at
+    every vertex that samples a direction, 0.3 (the default) only at the rough ground and slab."""
+    g, sc, cam, bound, ref = setup
+    img, st = _guided(ctx, sc, cam, bound, 64, 5, min_roughness=2.0)
+    assert st.guide_rows == 0 and st.guide_records == 0
+    plain = composite(*sc.render(cam, _params(64, 5)))
+    assert rel_mse(img, plain) < 1e-6
+    _, st_all = _guided(ctx, sc, cam, bound, 16, 6, min_roughness=0.0)
+    _, st_def = _guided(ctx, sc, cam, bound, 16, 6)
+    assert 0 < st_def.guide_rows < st_all.guide_rows
+    # every vertex that samples a direction (bounce below the limit) on a hit, after the first pass
+    assert st_all.guide_rows <= st_all.extension_rays
+
+
 def _pass_images(render):
     """Per-pass images (differences of the progress callback's running totals)."""
     imgs, prev = [], [None, None]
