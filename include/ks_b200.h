@@ -337,7 +337,8 @@ typedef struct ks_guide_render_options {
     int32_t train_passes;    /* passes that capture records and train afterwards */
     uint32_t max_records;    /* records captured per pass (0 -> 2^19) */
     uint32_t train_batch;    /* records per Adam step (0 -> 2^18) */
-    int32_t record_bounces;  /* the recorded vertex is drawn from bounces [0, record_bounces) (0 -> 6) */
+    int32_t record_bounces;  /* the recorded vertex is drawn from bounces [0, record_bounces) (0 -> 6);
+                                the guide samples directions at those bounces only */
     float min_roughness;     /* vertices whose material roughness is below this sample the BSDF only:
                                 no network inference there and no training records (default 0.3; 0
                                 guides every vertex).  A narrow BSDF lobe is already sampled well by

@@ -579,10 +579,11 @@ __global__ void __launch_bounds__(128, KS_INST_MIN_BLOCKS) k_shadow_inst_pt(cons
     flush_counts(tc, work);
 }
 
-// Guided renders: the hit paths the guide is evaluated for (those that sample a direction at this
-// vertex, with a material at least min_roughness rough) go to gqueue; the others get selection
-// probability 0 (their two weight vectors zeroed), so the shading samples their BSDF only.
-__global__ void __launch_bounds__(128) k_guide_filter(const __grid_constant__ SceneView sv, int bounces,
+// Guided renders: the hit paths the guide is evaluated for (those that sample a direction at a
+// bounce below guided_bounces, the bounces its training records come from, with a material at
+// least min_roughness rough) go to gqueue; the others get selection probability 0 (their two
+// weight vectors zeroed), so the shading samples their BSDF only.
+__global__ void __launch_bounds__(128) k_guide_filter(const __grid_constant__ SceneView sv, int guided_bounces,
                                                       float min_roughness, PathBuf cur, const float4 *hits,
                                                       const uint32_t *queue, const uint32_t *queue_count,
                                                       uint32_t *gqueue, uint32_t *gcount, float4 *lobes,
@@ -597,7 +598,7 @@ __global__ void __launch_bounds__(128) k_guide_filter(const __grid_constant__ Sc
         if (q < count) {
             i = queue[q];
             const int bounce = (int)(bits(cur.d_info[i].w) & 0xffffu);
-            if (bounce < bounces) {
+            if (bounce < guided_bounces) {
                 const uint32_t tri = bits(__ldg(&sv.prim_tris[3 * (size_t)bits(hits[i].w)]).w);
                 const uint32_t mesh = __ldg(&sv.tri_mesh[tri]);
                 use = sv.materials[__ldg(&sv.mesh_material[mesh])].roughness >= min_roughness;
@@ -926,7 +927,8 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
             if (guide && gv.active) {
                 // the guide only at vertices that sample a direction with a rough enough BSDF
                 cudaMemsetAsync(gw.gcount.ptr, 0, sizeof(uint32_t), st);
-                k_guide_filter<<<grid, 128, 0, st>>>(sv, rp.bounces, gv.min_roughness, pb[cur], w.hits.ptr,
+                k_guide_filter<<<grid, 128, 0, st>>>(sv, std::min<int>(rp.bounces, (int)gv.rec_bounces),
+                                                     gv.min_roughness, pb[cur], w.hits.ptr,
                                                      w.queue[0].ptr, w.counters.ptr + 2, gw.gqueue.ptr,
                                                      gw.gcount.ptr, gw.lobes.ptr, w.capacity);
                 stats.kernel_launches++;
