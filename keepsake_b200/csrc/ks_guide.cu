@@ -423,9 +423,15 @@ struct PathArgs
     float alpha_max;
     int *err;
 };
-constexpr uint32_t kPathSmemX0 = kWImage, kPathSmemX1 = kPathSmemX0 + 16384u, kPathSmemBar = kPathSmemX1 + 16384u;
+// One activation buffer: layer l's output overwrites its input, which every thread writes only after
+// the MMAs that read it have completed (the mbarrier wait in mlp_forward).  52 KB per CTA lets 4 CTAs
+// (4 tiles in flight, 256 of the 512 TMEM columns) share an SM.
+constexpr uint32_t kPathSmemX0 = kWImage, kPathSmemBar = kPathSmemX0 + 16384u;
 constexpr uint32_t kPathSmem = kPathSmemBar + 64;
-constexpr int kPathCtasPerSm = 3;
+#ifndef KS_GUIDE_PATH_CTAS
+#define KS_GUIDE_PATH_CTAS 4
+#endif
+constexpr int kPathCtasPerSm = KS_GUIDE_PATH_CTAS;
 
 __global__ void __launch_bounds__(kThreads, kPathCtasPerSm) k_guide_paths(PathArgs a)
 {
@@ -437,7 +443,7 @@ __global__ void __launch_bounds__(kThreads, kPathCtasPerSm) k_guide_paths(PathAr
     const uint32_t tmem = mlp_prologue(a.w_image, sw, bar, tmem_slot, cta_err, 64u);
     uint8_t *xb[kLayers];
     for (int l = 0; l < kLayers; ++l)
-        xb[l] = smem + ((l & 1) ? kPathSmemX1 : kPathSmemX0);
+        xb[l] = smem + kPathSmemX0;
     uint32_t phase = 0;
     const uint32_t count = *a.queue_count;
     const uint32_t n_tiles = (count + kThreads - 1) / kThreads;
