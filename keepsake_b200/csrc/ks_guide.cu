@@ -625,12 +625,14 @@ ks_context *context_of(const ks_guide *g) { return g->ctx; }
 
 ks_status infer_paths(ks_guide *g, const uint32_t *queue, const uint32_t *queue_count, const float4 *o_pdf,
                       const float4 *d_info, const float4 *hits, const float4 *prim_tris, const uint32_t *hit_inst,
-                      const float *inst_xf, float4 *lobes, uint32_t cap, uint32_t max_rows)
+                      const float *inst_xf, float4 *lobes, uint32_t cap, uint32_t max_rows, cudaStream_t stream)
 {
+    if (!stream)
+        stream = g->ctx->stream;
     if (!g->packed) {
-        ks_status s = pack(g);
-        if (s != KS_OK)
-            return s;
+        k_pack<<<(kWeights + 255) / 256, 256, 0, stream>>>(g->w.ptr, g->w_image.ptr);
+        KS_CUDA_TRY(g->ctx, cudaGetLastError());
+        g->packed = true;
     }
     PathArgs a{};
     a.gp = g->gp;
@@ -652,7 +654,7 @@ ks_status infer_paths(ks_guide *g, const uint32_t *queue, const uint32_t *queue_
     // image and takes TMEM once, so the late bounces' few rows should not start a full wave)
     const uint32_t tiles = (max_rows + kThreads - 1) / kThreads;
     const uint32_t grid = std::max(1u, std::min(tiles, (uint32_t)g->ctx->sm_count * kPathCtasPerSm));
-    k_guide_paths<<<grid, kThreads, kPathSmem, g->ctx->stream>>>(a);
+    k_guide_paths<<<grid, kThreads, kPathSmem, stream>>>(a);
     KS_CUDA_TRY(g->ctx, cudaGetLastError());
     return KS_OK;
 }

@@ -679,10 +679,13 @@ struct RenderCache
     double *staging = nullptr;     // pinned host copy of them
     size_t staging_n = 0;
     bool host_busy = false;
+    cudaStream_t aux = nullptr;    // guided renders: the guide runs here beside sampling and miss shading
     ~RenderCache()
     {
         if (staging)
             cudaFreeHost(staging);
+        if (aux)
+            cudaStreamDestroy(aux);
     }
 };
 
@@ -851,6 +854,19 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
     uint32_t *h_counts = nullptr;
     KS_CUDA_TRY(ctx, cudaMallocHost((void **)&h_counts, sizeof(uint32_t) * 3));
     h_counts[2] = 0;
+    // guided renders: the guide's filter and inference run on a second stream, overlapping the
+    // sampling and the miss shading, and join before the hit shading
+    cudaStream_t aux = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_g0 = nullptr, ev_g1 = nullptr;
+    if (guide) {
+        if (!rc.aux)
+            KS_CUDA_TRY(ctx, cudaStreamCreateWithFlags(&rc.aux, cudaStreamNonBlocking));
+        aux = rc.aux;
+        cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming);
+        cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming);
+        cudaEventCreate(&ev_g0);
+        cudaEventCreate(&ev_g1);
+    }
     cudaEvent_t ev[6];
     for (auto &e : ev)
         cudaEventCreate(&e);
@@ -924,18 +940,25 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
                 stats.kernel_launches++;
             }
             cudaEventRecord(ev[2], st);
-            if (guide && gv.active) {
+            const bool guiding = guide && gv.active;
+            if (guiding) {
                 // the guide only at vertices that sample a direction with a rough enough BSDF
-                cudaMemsetAsync(gw.gcount.ptr, 0, sizeof(uint32_t), st);
-                k_guide_filter<<<grid, 128, 0, st>>>(sv, std::min<int>(rp.bounces, (int)gv.rec_bounces),
-                                                     gv.min_roughness, pb[cur], w.hits.ptr,
-                                                     w.queue[0].ptr, w.counters.ptr + 2, gw.gqueue.ptr,
-                                                     gw.gcount.ptr, gw.lobes.ptr, w.capacity);
+                cudaEventRecord(ev_fork, st);
+                cudaStreamWaitEvent(aux, ev_fork, 0);
+                cudaEventRecord(ev_g0, aux);
+                cudaMemsetAsync(gw.gcount.ptr, 0, sizeof(uint32_t), aux);
+                k_guide_filter<<<grid, 128, 0, aux>>>(sv, std::min<int>(rp.bounces, (int)gv.rec_bounces),
+                                                      gv.min_roughness, pb[cur], w.hits.ptr,
+                                                      w.queue[0].ptr, w.counters.ptr + 2, gw.gqueue.ptr,
+                                                      gw.gcount.ptr, gw.lobes.ptr, w.capacity);
                 stats.kernel_launches++;
                 ks_status gs = guide_impl::infer_paths(guide, gw.gqueue.ptr, gw.gcount.ptr, pb[cur].o_pdf,
                                                        pb[cur].d_info, w.hits.ptr, sv.prim_tris, w.hit_inst.ptr,
-                                                       sv.inst.xf, gw.lobes.ptr, w.capacity, count);
+                                                       sv.inst.xf, gw.lobes.ptr, w.capacity, count, aux);
+                cudaEventRecord(ev_g1, aux);
+                cudaEventRecord(ev_join, aux);
                 if (gs != KS_OK) {
+                    cudaStreamWaitEvent(st, ev_join, 0);
                     err = cudaErrorLaunchFailure;
                     break;
                 }
@@ -944,10 +967,14 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
             cudaEventRecord(ev[5], st);
             launch_sample(false, grid, st, sv, rp, pb[cur], w.hits.ptr, w.hit_inst.ptr, w.queue[0].ptr,
                           w.counters.ptr + 2, w.samples.ptr, BatchView{});
-            for (int miss = 0; miss < 2; ++miss)
+            // misses first (they do not read the guide), then the hits once the guide has joined
+            for (int miss = 1; miss >= 0; --miss) {
+                if (!miss && guiding)
+                    cudaStreamWaitEvent(st, ev_join, 0);
                 launch_shade(miss != 0, guide != nullptr, false, grid, st, sv, rp, pb[cur], pb[1 - cur], w.hits.ptr,
                              w.hit_inst.ptr, w.samples.ptr, w.queue[miss].ptr, w.counters.ptr + 2 + miss,
                              w.counters.ptr, sb, w.counters.ptr + 1, d_accum, d_weights, gv, BatchView{});
+            }
             cudaEventRecord(ev[3], st);
             if (scene->n_instances) {
                 if (kPersistentTraversal)
@@ -978,8 +1005,10 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
             stats.ms_shade += ms;
             cudaEventElapsedTime(&ms, ev[1], ev[2]);
             stats.ms_extend += ms;
-            cudaEventElapsedTime(&ms, ev[2], ev[5]);
-            stats.ms_guide_infer += ms;
+            if (guiding) {
+                cudaEventElapsedTime(&ms, ev_g0, ev_g1);
+                stats.ms_guide_infer += ms;
+            }
             cudaEventElapsedTime(&ms, ev[5], ev[3]);
             stats.ms_shade += ms;
             cudaEventElapsedTime(&ms, ev[3], ev[4]);
@@ -1047,6 +1076,9 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
     cudaEventElapsedTime(&stats.ms_total, t_begin, t_end);
     for (auto &e : ev)
         cudaEventDestroy(e);
+    for (cudaEvent_t e : {ev_fork, ev_join, ev_g0, ev_g1})
+        if (e)
+            cudaEventDestroy(e);
     cudaEventDestroy(t_begin);
     cudaEventDestroy(t_end);
     int overflow = 0;
