@@ -72,6 +72,16 @@ def parse():
     return a
 
 
+def reduce_ranks(pg, torch, seconds, counts, device):
+    """Whole-job aggregation over the ranks (replicas): the slowest rank's time (max) and the sums
+    of the work counts.  Every rank calls it, in the same order."""
+    t = torch.tensor([seconds], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    r = torch.tensor(counts, dtype=torch.float64, device=device)
+    pg.all_reduce(r)
+    return float(t.item()), [int(x) for x in r.tolist()]
+
+
 def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
 
@@ -509,12 +519,7 @@ def main():
     rays = sum(s.extension_rays + s.shadow_rays for s in stats)
     paths = sum(s.paths for s in stats)
     if pg:
-        t = torch.tensor([dev_ms], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        dev_ms = float(t.item())
-        r = torch.tensor([rays, paths], dtype=torch.float64, device="cuda")
-        pg.all_reduce(r)
-        rays, paths = int(r[0].item()), int(r[1].item())
+        dev_ms, (rays, paths) = reduce_ranks(pg, torch, dev_ms, [rays, paths], "cuda")
     value = rays / (dev_ms / 1e3) / 1e6
 
     # roofline of the dominant kernel (closest-hit traversal); algorithmic bytes per query:
@@ -562,12 +567,7 @@ def main():
         e2e_parts.append({"scene_create": t1 - t0, "build": t2 - t1, "render": t3 - t2, "render_device": st.ms_total / 1e3,
                           "destroy": t4 - t3})
     if pg:
-        t = torch.tensor([e2e_t], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_t = float(t.item())
-        r = torch.tensor([e2e_rays], dtype=torch.float64, device="cuda")
-        pg.all_reduce(r)
-        e2e_rays = int(r.item())
+        e2e_t, (e2e_rays,) = reduce_ranks(pg, torch, e2e_t, [e2e_rays], "cuda")
     e2e = {"value": e2e_rays / e2e_t / 1e6 if e2e_t > 0 else None, "unit": "Mrays/s", "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": d2h, "steps": e2e_steps, "timing": "host wall clock around synchronous C-ABI calls",
            "step_seconds": {key: statistics.median(p[key] for p in e2e_parts) for key in e2e_parts[0]} if e2e_parts
