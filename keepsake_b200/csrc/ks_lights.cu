@@ -3,8 +3,9 @@
 //
 //   SkyLight::SkyLight (light.cpp:19-49): lum = sin(theta) * luminance, threshold at the mean,
 //     DistribTable2D of the thresholded values.  The conditional CDFs are float prefix sums in
-//     index order, exactly as DistribTable (distrib.cpp:9-29): one GPU thread per row keeps the
-//     reference's summation order, so the table is bit-identical to a sequential host build.
+//     index order, exactly as DistribTable (distrib.cpp:9-29): one GPU thread per row runs the
+//     row's sum in the reference's order over tiles staged in shared memory, so the table is
+//     bit-identical to a sequential host build.
 //     The mean is a double sum (rows in order) - the reference uses an unordered float atomic.
 //   SkyLight::power (light.cpp:136-159): float row sums in column order (one thread per row),
 //     rows added in order in double.
@@ -22,84 +23,148 @@ namespace ksb
 namespace
 {
 
-__global__ void k_sky_rows(const float4 *map, int w, int h, const float *row_sin, float *lum, double *row_sum)
+// The per-row sums below keep the reference's summation order (one running sum per row, columns in
+// order); the rows' texels are staged through shared memory in tiles of kTileRows x kTileCols so
+// that the loads are coalesced and many rows progress at once.
+constexpr int kTileRows = 32, kTileCols = 64, kTileThreads = 256;
+
+// RGB (3 floats per texel) -> float4 texels.
+__global__ void k_sky_unpack(const float *rgb, size_t n, float4 *map)
 {
-    int y = blockIdx.x * blockDim.x + threadIdx.x;
-    if (y >= h)
-        return;
-    float st = row_sin[y];
-    double s = 0.0;
-    for (int x = 0; x < w; ++x) {
-        float4 c = map[(size_t)y * w + x];
-        float l = st * luminance(mk(c.x, c.y, c.z));
-        lum[(size_t)y * w + x] = l;
-        s += l;
-    }
-    row_sum[y] = s;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        map[i] = make_float4(rgb[3 * i], rgb[3 * i + 1], rgb[3 * i + 2], 0.0f);
 }
 
-// DistribTable(f, n) per row with f = max(lum - average, 0) (distrib.cpp:9-29).
-__global__ void k_sky_cond(const float *lum, int w, int h, float average, float *cond, float *acc, int threshold)
+// lum = sin(theta) * luminance per texel, and its double row sums in column order.
+__global__ void __launch_bounds__(kTileThreads) k_sky_rows(const float4 *map, int w, int h, const float *row_sin,
+                                                           float *lum, double *row_sum)
 {
-    int y = blockIdx.x * blockDim.x + threadIdx.x;
-    if (y >= h)
-        return;
-    float *cdf = cond + (size_t)y * (w + 1);
-    const float *f = lum + (size_t)y * w;
-    cdf[0] = 0.0f;
-    float invn = 1.0f / (float)w;
-    for (int i = 1; i < w + 1; ++i) {
-        float v = f[i - 1];
-        if (threshold) {
-            v = v - average;
-            v = v < 0.0f ? 0.0f : v; // std::max(lum - average, 0.0f)
+    __shared__ float tile[kTileRows][kTileCols + 1];
+    const int y0 = blockIdx.x * kTileRows, r0 = threadIdx.x;
+    double s = 0.0;
+    for (int x0 = 0; x0 < w; x0 += kTileCols) {
+        for (int k = threadIdx.x; k < kTileRows * kTileCols; k += kTileThreads) {
+            const int r = k / kTileCols, c = k % kTileCols, y = y0 + r, x = x0 + c;
+            float l = 0.0f;
+            if (y < h && x < w) {
+                float4 t = map[(size_t)y * w + x];
+                l = row_sin[y] * luminance(mk(t.x, t.y, t.z));
+                lum[(size_t)y * w + x] = l;
+            }
+            tile[r][c] = l;
         }
-        cdf[i] = cdf[i - 1] + v * invn;
+        __syncthreads();
+        if (r0 < kTileRows && y0 + r0 < h)
+            for (int c = 0; c < kTileCols && x0 + c < w; ++c)
+                s += tile[r0][c];
+        __syncthreads();
     }
-    float a = cdf[w];
-    acc[y] = a;
-    if (a == 0.0f) {
-        for (int i = 0; i < w + 1; ++i)
-            cdf[i] = (float)i / (float)w;
-    } else {
-        float inva = 1.0f / a;
-        for (int i = 0; i < w + 1; ++i)
-            cdf[i] *= inva;
+    if (r0 < kTileRows && y0 + r0 < h)
+        row_sum[y0 + r0] = s;
+}
+
+// DistribTable(f, n) per row with f = max(lum - average, 0) (distrib.cpp:9-29): the float prefix
+// sums in column order, then the normalisation.
+__global__ void __launch_bounds__(kTileThreads) k_sky_cond(const float *lum, int w, int h, float average,
+                                                           float *cond, float *acc, int threshold)
+{
+    __shared__ float tile[kTileRows][kTileCols + 1];
+    __shared__ float total[kTileRows];
+    const int y0 = blockIdx.x * kTileRows, r0 = threadIdx.x;
+    const float invn = 1.0f / (float)w;
+    float prev = 0.0f;
+    for (int x0 = 0; x0 < w; x0 += kTileCols) {
+        for (int k = threadIdx.x; k < kTileRows * kTileCols; k += kTileThreads) {
+            const int r = k / kTileCols, c = k % kTileCols, y = y0 + r, x = x0 + c;
+            tile[r][c] = (y < h && x < w) ? lum[(size_t)y * w + x] : 0.0f;
+        }
+        __syncthreads();
+        if (r0 < kTileRows && y0 + r0 < h)
+            for (int c = 0; c < kTileCols && x0 + c < w; ++c) {
+                float v = tile[r0][c];
+                if (threshold) {
+                    v = v - average;
+                    v = v < 0.0f ? 0.0f : v; // std::max(lum - average, 0.0f)
+                }
+                prev = prev + v * invn;
+                tile[r0][c] = prev; // cdf[x0 + c + 1]
+            }
+        __syncthreads();
+        for (int k = threadIdx.x; k < kTileRows * kTileCols; k += kTileThreads) {
+            const int r = k / kTileCols, c = k % kTileCols, y = y0 + r, x = x0 + c;
+            if (y < h && x < w)
+                cond[(size_t)y * (w + 1) + x + 1] = tile[r][c];
+        }
+        __syncthreads();
     }
-    cdf[w] = 1.0f;
+    if (r0 < kTileRows && y0 + r0 < h) {
+        cond[(size_t)(y0 + r0) * (w + 1)] = 0.0f;
+        acc[y0 + r0] = prev;
+        total[r0] = prev;
+    }
+    __syncthreads();
+    // normalisation, every entry independently
+    for (int r = 0; r < kTileRows && y0 + r < h; ++r) {
+        float *cdf = cond + (size_t)(y0 + r) * (w + 1);
+        const float a = total[r];
+        const float inva = a == 0.0f ? 0.0f : 1.0f / a;
+        for (int i = threadIdx.x; i < w + 1; i += kTileThreads) {
+            if (i == w)
+                cdf[i] = 1.0f;
+            else if (a == 0.0f)
+                cdf[i] = (float)i / (float)w;
+            else
+                cdf[i] *= inva;
+        }
+    }
 }
 
 // Row sums of SkyLight::power (light.cpp:140-153); eval() through the same device code as shading.
-__global__ void k_sky_power_rows(SceneView s, double *row_sums)
+// Each texel's term is computed by its own thread; the float row sums run in column order.
+__global__ void __launch_bounds__(kTileThreads) k_sky_power_rows(SceneView s, double *row_sums)
 {
-    int row = blockIdx.x * blockDim.x + threadIdx.x;
-    if (row >= s.sky_h)
-        return;
-    float theta = (row + 0.5f) / (float)s.sky_h * kPi;
-    float sin_theta = sinf(theta);
+    __shared__ float tile[3][kTileRows][kTileCols + 1];
+    const int y0 = blockIdx.x * kTileRows, r0 = threadIdx.x;
     f3 rs = mk(0, 0, 0);
-    for (int col = 0; col < s.sky_w; ++col) {
-        float phi = (col + 0.5f) / (float)s.sky_w * kTwoPi;
-        float ct = cosf(theta), st = sinf(theta), cp = cosf(phi), sp = sinf(phi);
-        f3 dir = mk(cp * st, sp * st, ct); // to_cartesian (z up), as the reference does here
-        rs += sky_eval(s, dir) * sin_theta;
+    for (int x0 = 0; x0 < s.sky_w; x0 += kTileCols) {
+        for (int k = threadIdx.x; k < kTileRows * kTileCols; k += kTileThreads) {
+            const int r = k / kTileCols, c = k % kTileCols, row = y0 + r, col = x0 + c;
+            f3 v = mk(0, 0, 0);
+            if (row < s.sky_h && col < s.sky_w) {
+                float theta = (row + 0.5f) / (float)s.sky_h * kPi;
+                float sin_theta = sinf(theta);
+                float phi = (col + 0.5f) / (float)s.sky_w * kTwoPi;
+                float ct = cosf(theta), st = sinf(theta), cp = cosf(phi), sp = sinf(phi);
+                f3 dir = mk(cp * st, sp * st, ct); // to_cartesian (z up), as the reference does here
+                v = sky_eval(s, dir) * sin_theta;
+            }
+            tile[0][r][c] = v.x;
+            tile[1][r][c] = v.y;
+            tile[2][r][c] = v.z;
+        }
+        __syncthreads();
+        if (r0 < kTileRows && y0 + r0 < s.sky_h)
+            for (int c = 0; c < kTileCols && x0 + c < s.sky_w; ++c)
+                rs += mk(tile[0][r0][c], tile[1][r0][c], tile[2][r0][c]);
+        __syncthreads();
     }
-    row_sums[3 * row + 0] = rs.x;
-    row_sums[3 * row + 1] = rs.y;
-    row_sums[3 * row + 2] = rs.z;
+    if (r0 < kTileRows && y0 + r0 < s.sky_h) {
+        const int row = y0 + r0;
+        row_sums[3 * row + 0] = rs.x;
+        row_sums[3 * row + 1] = rs.y;
+        row_sums[3 * row + 2] = rs.z;
+    }
 }
 
-// Guide tables (see cdf_find_guided): one thread per CDF row.
+// Guide tables (see cdf_find_guided): one thread per (row, entry).
 __global__ void k_guide(const float *cdf, uint32_t n, uint32_t rows, uint32_t *guide)
 {
-    uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= rows)
+    const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (t >= (size_t)rows * kGuide)
         return;
+    const uint32_t r = (uint32_t)(t / kGuide), k = (uint32_t)(t % kGuide);
     const float *c = cdf + (size_t)r * (n + 1);
-    for (uint32_t k = 0; k < kGuide; ++k) {
-        float t = (float)k / (float)kGuide;
-        guide[(size_t)r * kGuide + k] = cdf_find(c, n, t);
-    }
+    guide[t] = cdf_find(c, n, (float)k / (float)kGuide);
 }
 
 // DistribTable on the host, identical to distrib.cpp:9-29.
@@ -227,16 +292,11 @@ ks_status build_lights(ks_scene *s)
     if (sd.kind == 1 || sd.kind == 2) {
         s->n_nonmesh = 1;
         int w, h;
-        std::vector<float4> map;
         if (sd.kind == 1) {
             w = h = 1;
-            map = {make_float4(sd.ambient[0], sd.ambient[1], sd.ambient[2], 0.0f)};
         } else {
             w = (int)sd.width;
             h = (int)sd.height;
-            map.resize((size_t)w * h);
-            for (size_t i = 0; i < map.size(); ++i)
-                map[i] = make_float4(s->h_sky_map[3 * i], s->h_sky_map[3 * i + 1], s->h_sky_map[3 * i + 2], 0.0f);
             float m4[16], inv4[16];
             std::memcpy(m4, sd.to_world, sizeof(m4));
             if (!invert4(m4, inv4))
@@ -249,8 +309,16 @@ ks_status build_lights(ks_scene *s)
         }
         s->sky_w = w;
         s->sky_h = h;
-        KS_CUDA_TRY(ctx, s->sky_map.alloc(map.size()));
-        KS_CUDA_TRY(ctx, cudaMemcpyAsync(s->sky_map.ptr, map.data(), s->sky_map.bytes(), cudaMemcpyHostToDevice, st));
+        KS_CUDA_TRY(ctx, s->sky_map.alloc((size_t)w * h));
+        if (sd.kind == 1) {
+            const float4 amb = make_float4(sd.ambient[0], sd.ambient[1], sd.ambient[2], 0.0f);
+            KS_CUDA_TRY(ctx, cudaMemcpyAsync(s->sky_map.ptr, &amb, sizeof(amb), cudaMemcpyHostToDevice, st));
+            KS_CUDA_TRY(ctx, cudaStreamSynchronize(st)); // amb lives on this stack frame
+        } else {
+            // the map was uploaded as RGB at ks_scene_create
+            k_sky_unpack<<<(unsigned)std::min<size_t>(((size_t)w * h + 255) / 256, 4096), 256, 0, st>>>(
+                s->sky_rgb.ptr, (size_t)w * h, s->sky_map.ptr);
+        }
         KS_CUDA_TRY(ctx, s->sky_cond.alloc((size_t)h * (w + 1)));
         DevBuf<float> lum, acc, row_sin;
         DevBuf<double> row_sum;
@@ -265,7 +333,8 @@ ks_status build_lights(ks_scene *s)
         if (sd.kind == 1)
             h_sin[0] = 1.0f; // the ambient constructor uses plain luminance (light.cpp:52-57)
         KS_CUDA_TRY(ctx, cudaMemcpyAsync(row_sin.ptr, h_sin.data(), sizeof(float) * h, cudaMemcpyHostToDevice, st));
-        k_sky_rows<<<(h + 127) / 128, 128, 0, st>>>(s->sky_map.ptr, w, h, row_sin.ptr, lum.ptr, row_sum.ptr);
+        const unsigned row_tiles = (unsigned)((h + kTileRows - 1) / kTileRows);
+        k_sky_rows<<<row_tiles, kTileThreads, 0, st>>>(s->sky_map.ptr, w, h, row_sin.ptr, lum.ptr, row_sum.ptr);
         std::vector<double> h_rows(h);
         KS_CUDA_TRY(ctx, cudaMemcpyAsync(h_rows.data(), row_sum.ptr, sizeof(double) * h, cudaMemcpyDeviceToHost, st));
         KS_CUDA_TRY(ctx, cudaStreamSynchronize(st));
@@ -273,7 +342,7 @@ ks_status build_lights(ks_scene *s)
         for (int y = 0; y < h; ++y)
             lum_sum += h_rows[y];
         float average = (float)lum_sum / (size_t)((size_t)w * h);
-        k_sky_cond<<<(h + 127) / 128, 128, 0, st>>>(lum.ptr, w, h, average, s->sky_cond.ptr, acc.ptr,
+        k_sky_cond<<<row_tiles, kTileThreads, 0, st>>>(lum.ptr, w, h, average, s->sky_cond.ptr, acc.ptr,
                                                     sd.kind == 2 ? 1 : 0);
         std::vector<float> h_acc(h);
         KS_CUDA_TRY(ctx, cudaMemcpyAsync(h_acc.data(), acc.ptr, sizeof(float) * h, cudaMemcpyDeviceToHost, st));
@@ -284,11 +353,12 @@ ks_status build_lights(ks_scene *s)
                                          cudaMemcpyHostToDevice, st));
         KS_CUDA_TRY(ctx, s->sky_cond_guide.alloc((size_t)h * kGuide));
         KS_CUDA_TRY(ctx, s->sky_margin_guide.alloc(kGuide));
-        k_guide<<<(h + 127) / 128, 128, 0, st>>>(s->sky_cond.ptr, (uint32_t)w, (uint32_t)h, s->sky_cond_guide.ptr);
-        k_guide<<<1, 32, 0, st>>>(s->sky_margin.ptr, (uint32_t)h, 1u, s->sky_margin_guide.ptr);
+        k_guide<<<(unsigned)(((size_t)h * kGuide + 255) / 256), 256, 0, st>>>(s->sky_cond.ptr, (uint32_t)w,
+                                                                               (uint32_t)h, s->sky_cond_guide.ptr);
+        k_guide<<<(kGuide + 255) / 256, 256, 0, st>>>(s->sky_margin.ptr, (uint32_t)h, 1u, s->sky_margin_guide.ptr);
         // power (light.cpp:136-159)
         SceneView v = make_view(s);
-        k_sky_power_rows<<<(h + 127) / 128, 128, 0, st>>>(v, row_sum.ptr);
+        k_sky_power_rows<<<row_tiles, kTileThreads, 0, st>>>(v, row_sum.ptr);
         std::vector<double> h_pr(3 * h);
         KS_CUDA_TRY(ctx, cudaMemcpyAsync(h_pr.data(), row_sum.ptr, sizeof(double) * 3 * h, cudaMemcpyDeviceToHost, st));
         KS_CUDA_TRY(ctx, cudaStreamSynchronize(st));

@@ -339,8 +339,6 @@ ks_status ks_scene_create(ks_context *ctx, const ks_scene_desc *desc, ks_scene *
         return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_create: bad sky description");
     }
     s->sky_desc = sd;
-    if (sd.kind == 2)
-        s->h_sky_map.assign(sd.map_rgb, sd.map_rgb + 3 * (size_t)sd.width * sd.height);
     s->sky_desc.map_rgb = nullptr;
     std::vector<MaterialGPU> mats(desc->n_materials);
     for (uint32_t k = 0; k < desc->n_materials; ++k) {
@@ -387,6 +385,12 @@ ks_status ks_scene_create(ks_context *ctx, const ks_scene_desc *desc, ks_scene *
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(s->tri_mesh.ptr, tri_mesh.data(), s->tri_mesh.bytes(), cudaMemcpyHostToDevice,
                             ctx->stream);
+    if (e == cudaSuccess && sd.kind == 2) {
+        const size_t n = 3 * (size_t)sd.width * sd.height;
+        e = s->sky_rgb.alloc(n);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(s->sky_rgb.ptr, sd.map_rgb, sizeof(float) * n, cudaMemcpyHostToDevice, ctx->stream);
+    }
     if (e == cudaSuccess)
         e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) {
