@@ -3,11 +3,13 @@
 // SmallPT::run / trace (small_pt.cpp:15-178) restructured as a streaming wavefront:
 //
 //   raygen  -> new camera paths fill the free queue slots (sample-major over the crop window),
-//   extend  -> closest-hit SBVH traversal, one thread per ray (ks_traverse.cuh),
-//   shade   -> miss/sky MIS, emitter MIS, NEE light sample + BSDF eval (Material::sample_with_nee,
+//   extend  -> closest-hit traversal of the SBVH's 4-wide view by persistent warps that fetch rays
+//              from a counter (ks_traverse.cuh), then hit and miss queues in path order,
+//   sample  -> the bounce's Sobol values and the NEE light sample (ks_shade.cu),
+//   shade   -> miss/sky MIS, emitter MIS, BSDF eval of the light sample (Material::sample_with_nee,
 //              material.cpp:101-167; next_event_estimate, nee.cpp:11-57), BSDF sample, Russian
-//              roulette; surviving paths and shadow rays are appended to compacted SoA queues
-//              with one atomic per warp (ballot + popc),
+//              roulette (ks_shade.cu); surviving paths and shadow rays are appended to compacted
+//              SoA queues (ballot + popc within a warp, one atomic per CTA),
 //   shadow  -> any-hit traversal of the NEE shadow rays; unoccluded contributions are added to the
 //              path (or, for a path that ended this bounce, the path is accumulated).
 //
