@@ -63,10 +63,15 @@ typedef struct ks_mesh_desc {
     uint32_t n_vertices;
     const uint32_t *indices;     /* 3 per triangle */
     uint32_t n_triangles;
-    const float *vertex_normals; /* optional, 3 per vertex; NULL = flat shading */
+    const float *vertex_normals; /* optional, 3 per vertex (object space); the shading frame
+                                    follows the interpolated normal when use_smooth_normal != 0
+                                    (geometry.cpp:139-156); NULL = flat shading */
     uint32_t material;           /* index into ks_scene_desc.materials */
     int32_t twosided;            /* MeshData::twosided (geometry.h:84); reference default 1 */
     int32_t use_smooth_normal;   /* MeshData::use_smooth_normal (geometry.h:85) */
+    const float *texcoords;      /* optional, 2 per vertex (MeshData::texcoords); when given, the
+                                    frame's tangent is dP/du of this parameterisation
+                                    (geometry.cpp:94-116); NULL = dP/du of the barycentrics */
 } ks_mesh_desc;
 
 /* PrincipledBSDF with constant shader fields (principled_bsdf.cpp:707-733) plus the

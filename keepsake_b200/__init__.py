@@ -119,7 +119,8 @@ class Context:
 # ---------------------------------------------------------------------------------------------
 class MeshDesc(ctypes.Structure):
     _fields_ = [("vertices", _vp), ("n_vertices", _u32), ("indices", _vp), ("n_triangles", _u32),
-                ("vertex_normals", _vp), ("material", _u32), ("twosided", _i32), ("use_smooth_normal", _i32)]
+                ("vertex_normals", _vp), ("material", _u32), ("twosided", _i32), ("use_smooth_normal", _i32),
+                ("texcoords", _vp)]
 
 
 class MaterialDesc(ctypes.Structure):
@@ -332,11 +333,15 @@ class Generated:
 
 
 def scene_desc(meshes, materials, sky=None):
-    """A SceneDesc over Python arrays: meshes = [(vertices [V,3], indices [T,3], material)],
-    materials = [MaterialDesc].  Returns (desc, keepalive)."""
+    """A SceneDesc over Python arrays: meshes = [(vertices [V,3], indices [T,3], material[, extra])]
+    with the optional dict `extra` holding "normals" [V,3], "texcoords" [V,2], "twosided" (default
+    1) and "smooth" (use_smooth_normal, default 1); materials = [MaterialDesc].  Returns
+    (desc, keepalive)."""
     keep = []
     md = (MeshDesc * len(meshes))()
-    for k, (v, idx, mat) in enumerate(meshes):
+    for k, mesh in enumerate(meshes):
+        v, idx, mat = mesh[:3]
+        extra = mesh[3] if len(mesh) > 3 else {}
         v = np.ascontiguousarray(v, np.float32)
         idx = np.ascontiguousarray(idx, np.uint32)
         keep += [v, idx]
@@ -345,8 +350,13 @@ def scene_desc(meshes, materials, sky=None):
         md[k].indices = idx.ctypes.data
         md[k].n_triangles = len(idx)
         md[k].material = mat
-        md[k].twosided = 1
-        md[k].use_smooth_normal = 1
+        md[k].twosided = int(extra.get("twosided", 1))
+        md[k].use_smooth_normal = int(extra.get("smooth", 1))
+        for key, field, width in (("normals", "vertex_normals", 3), ("texcoords", "texcoords", 2)):
+            if extra.get(key) is not None:
+                a = np.ascontiguousarray(extra[key], np.float32).reshape(len(v), width)
+                keep.append(a)
+                setattr(md[k], field, a.ctypes.data)
     mats = (MaterialDesc * len(materials))(*materials)
     keep += [md, mats]
     d = SceneDesc()
@@ -372,7 +382,7 @@ def triangle_soup_desc(vertices, indices, material=None):
     """Builds a one-mesh SceneDesc over numpy arrays; returns (desc, keepalive)."""
     v = np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1, 3)
     i = np.ascontiguousarray(indices, dtype=np.uint32).reshape(-1, 3)
-    mesh = MeshDesc(ptr(v), len(v), ptr(i), len(i), None, 0, 1, 1)
+    mesh = MeshDesc(ptr(v), len(v), ptr(i), len(i), None, 0, 1, 1, None)
     mat = material or MaterialDesc((0.8, 0.8, 0.8), 1.0, 0.0, 1.5, 0.5, 0.0, 0.0, 0.5, (0, 0, 0), 0, 0, (0, 0, 0))
     meshes = (MeshDesc * 1)(mesh)
     mats = (MaterialDesc * 1)(mat)

@@ -783,6 +783,7 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
         return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_small_pt_render: empty crop window");
 
     SceneView sv = make_view(scene);
+    const bool attribs = sv.normals != nullptr || sv.texcoords != nullptr;
     const uint32_t n_pix = (uint32_t)rp.cw * (uint32_t)rp.ch;
     const uint64_t max_interval = (uint64_t)n_pix * (uint64_t)std::min(in->spp, in->spp_prog_interval);
     RenderCache &rc = render_cache(ctx);
@@ -973,7 +974,7 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
             for (int miss = 1; miss >= 0; --miss) {
                 if (!miss && guiding)
                     cudaStreamWaitEvent(st, ev_join, 0);
-                launch_shade(miss != 0, guide != nullptr, false, grid, st, sv, rp, pb[cur], pb[1 - cur], w.hits.ptr,
+                launch_shade(miss != 0, guide != nullptr, false, attribs, grid, st, sv, rp, pb[cur], pb[1 - cur], w.hits.ptr,
                              w.hit_inst.ptr, w.samples.ptr, w.queue[miss].ptr, w.counters.ptr + 2 + miss,
                              w.counters.ptr, sb, w.counters.ptr + 1, d_accum, d_weights, gv, BatchView{});
             }
@@ -1120,6 +1121,7 @@ struct BatchWork
     DevBuf<unsigned long long> path_begin;
     DevBuf<BatchState> state_dev;
     unsigned ext_grid = 0, shadow_grid = 0; // one wave of resident CTAs of the traversal kernels
+    bool attribs = false;                   // some job's scene has vertex normals or texcoords
 };
 
 // Validates the jobs and fills the per-job tables; returns the total path count in *total.
@@ -1133,6 +1135,7 @@ static ks_status batch_tables(ks_context *ctx, const ks_batch_job *jobs, uint32_
     std::vector<double *> acc(n), wts(n);
     std::vector<unsigned long long> begin(n + 1, 0);
     *max_bounces = 0;
+    w.attribs = false;
     for (uint32_t j = 0; j < n; ++j) {
         const ks_batch_job &jb = jobs[j];
         const ks_small_pt_params &in = jb.params;
@@ -1152,6 +1155,7 @@ static ks_status batch_tables(ks_context *ctx, const ks_batch_job *jobs, uint32_
         if (!fill_params(&jb.camera, &in, params[j]))
             return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_batch_render_device: empty crop window");
         views[j] = make_view(jb.scene);
+        w.attribs |= views[j].normals != nullptr || views[j].texcoords != nullptr;
         acc[j] = jb.accum_rgb_device;
         wts[j] = jb.weights_device;
         begin[j + 1] = begin[j] + (unsigned long long)params[j].cw * params[j].ch * (unsigned long long)in.spp;
@@ -1188,7 +1192,7 @@ static void batch_iteration(ks_context *ctx, BatchWork &w, const BatchView &bv, 
     launch_sample(true, grid, st, SceneView{}, RenderParams{}, pb[cur], w.hits.ptr, nullptr, w.queue[0].ptr, cnt + 2,
                   w.samples.ptr, bv);
     for (int miss = 0; miss < 2; ++miss)
-        launch_shade(miss != 0, false, true, grid, st, SceneView{}, RenderParams{}, pb[cur], pb[1 - cur], w.hits.ptr,
+        launch_shade(miss != 0, false, true, w.attribs, grid, st, SceneView{}, RenderParams{}, pb[cur], pb[1 - cur], w.hits.ptr,
                      nullptr, w.samples.ptr, w.queue[miss].ptr, cnt + 2 + miss, cnt, sb, cnt + 1, nullptr, nullptr,
                      gv, bv);
     k_shadow_pt<true><<<w.shadow_grid, 128, 0, st>>>(SceneView{}, sb, cnt + 1, cnt + 5, pb[1 - cur], nullptr, nullptr,

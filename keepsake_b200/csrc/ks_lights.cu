@@ -257,7 +257,9 @@ SceneView make_view(const ks_scene *s)
     }
     v.tri_mesh = s->tri_mesh.ptr;
     v.mesh_material = s->mesh_material.ptr;
-    v.mesh_twosided = s->mesh_twosided.ptr;
+    v.mesh_flags = s->mesh_flags.ptr;
+    v.normals = s->normals.ptr;
+    v.texcoords = s->texcoords.ptr;
     v.materials = s->materials.ptr;
     v.light_count = s->light_count;
     v.n_nonmesh = s->n_nonmesh;

@@ -26,7 +26,9 @@ struct SceneView
     float bmin[3], bmax[3];
     const uint32_t *tri_mesh;
     const uint32_t *mesh_material;
-    const int *mesh_twosided;
+    const int *mesh_flags;   // per mesh: kMeshTwosided | kMeshSmooth | kMeshTexcoords
+    const float *normals;    // global vertex normals (3 floats each; null when no mesh shades smooth)
+    const float *texcoords;  // global texture coordinates (2 floats each; null when no mesh has them)
     const MaterialGPU *materials;
     // lights
     uint32_t light_count;

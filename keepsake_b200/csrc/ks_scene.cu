@@ -308,6 +308,14 @@ ks_status ks_scene_create(ks_context *ctx, const ks_scene_desc *desc, ks_scene *
     s->n_verts = (uint32_t)n_verts;
     std::vector<float> verts(3 * n_verts);
     std::vector<uint32_t> idx(3 * n_tris), tri_mesh(n_tris);
+    // per-vertex shading attributes: only meshes that shade smooth contribute normals (a mesh with
+    // use_smooth_normal off or no vertex normals shades flat, geometry.cpp:139-141)
+    bool any_smooth = false, any_uv = false;
+    for (uint32_t m = 0; m < desc->n_meshes; ++m) {
+        any_smooth |= desc->meshes[m].use_smooth_normal && desc->meshes[m].vertex_normals;
+        any_uv |= desc->meshes[m].texcoords != nullptr;
+    }
+    std::vector<float> normals(any_smooth ? 3 * n_verts : 0), texcoords(any_uv ? 2 * n_verts : 0);
     uint64_t vo = 0, to = 0;
     for (uint32_t m = 0; m < desc->n_meshes; ++m) {
         const ks_mesh_desc &md = desc->meshes[m];
@@ -316,9 +324,18 @@ ks_status ks_scene_create(ks_context *ctx, const ks_scene_desc *desc, ks_scene *
             idx[3 * to + k] = (uint32_t)(md.indices[k] + vo);
         for (uint64_t k = 0; k < md.n_triangles; ++k)
             tri_mesh[to + k] = m;
+        int flags = md.twosided ? kMeshTwosided : 0;
+        if (md.use_smooth_normal && md.vertex_normals) {
+            flags |= kMeshSmooth;
+            std::memcpy(&normals[3 * vo], md.vertex_normals, sizeof(float) * 3 * md.n_vertices);
+        }
+        if (md.texcoords) {
+            flags |= kMeshTexcoords;
+            std::memcpy(&texcoords[2 * vo], md.texcoords, sizeof(float) * 2 * md.n_vertices);
+        }
         s->host.mesh_tri_offset.push_back((uint32_t)to);
         s->host.mesh_material.push_back(md.material);
-        s->host.mesh_twosided.push_back(md.twosided);
+        s->host.mesh_flags.push_back(flags);
         vo += md.n_vertices;
         to += md.n_triangles;
     }
@@ -363,15 +380,27 @@ ks_status ks_scene_create(ks_context *ctx, const ks_scene_desc *desc, ks_scene *
     if (e == cudaSuccess)
         e = s->mesh_material.alloc(s->host.mesh_material.size());
     if (e == cudaSuccess)
-        e = s->mesh_twosided.alloc(s->host.mesh_twosided.size());
+        e = s->mesh_flags.alloc(s->host.mesh_flags.size());
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(s->materials.ptr, mats.data(), s->materials.bytes(), cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(s->mesh_material.ptr, s->host.mesh_material.data(), s->mesh_material.bytes(),
                             cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess)
-        e = cudaMemcpyAsync(s->mesh_twosided.ptr, s->host.mesh_twosided.data(), s->mesh_twosided.bytes(),
+        e = cudaMemcpyAsync(s->mesh_flags.ptr, s->host.mesh_flags.data(), s->mesh_flags.bytes(),
                             cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess && any_smooth) {
+        e = s->normals.alloc(normals.size());
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(s->normals.ptr, normals.data(), s->normals.bytes(), cudaMemcpyHostToDevice,
+                                ctx->stream);
+    }
+    if (e == cudaSuccess && any_uv) {
+        e = s->texcoords.alloc(texcoords.size());
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(s->texcoords.ptr, texcoords.data(), s->texcoords.bytes(), cudaMemcpyHostToDevice,
+                                ctx->stream);
+    }
     if (e == cudaSuccess)
         e = s->verts.alloc(verts.size());
     if (e == cudaSuccess)

@@ -43,6 +43,15 @@ struct WideNode
 };
 static_assert(sizeof(WideNode) == 128, "one 128-byte line per wide node");
 
+// Per-mesh shading flags (MeshData::twosided; use_smooth_normal with vertex normals given;
+// texcoords given).
+enum : int
+{
+    kMeshTwosided = 1,
+    kMeshSmooth = 2,
+    kMeshTexcoords = 4
+};
+
 // Device copy of one material (constant principled fields + emission).
 struct MaterialGPU
 {
@@ -58,7 +67,7 @@ struct SceneHost
 {
     std::vector<uint32_t> mesh_tri_offset; // first global triangle of each mesh (+ total at the end)
     std::vector<uint32_t> mesh_material;
-    std::vector<int> mesh_twosided;
+    std::vector<int> mesh_flags; // kMeshTwosided | kMeshSmooth | kMeshTexcoords (ks_wavefront.cuh)
     std::vector<ks_material_desc> materials;
     // instancing (empty: flat scene)
     std::vector<uint32_t> proto_tri_begin, proto_tri_end; // global triangle range of each prototype
@@ -96,7 +105,10 @@ struct ks_scene
     // materials (device copies of the per-mesh tables)
     ksb::DevBuf<ksb::MaterialGPU> materials;
     ksb::DevBuf<uint32_t> mesh_material;
-    ksb::DevBuf<int> mesh_twosided;
+    ksb::DevBuf<int> mesh_flags;
+    // per-vertex shading attributes, indexed like verts (allocated only when some mesh has them)
+    ksb::DevBuf<float> normals;   // 3 per vertex: MeshData::vertex_normals of smooth-shaded meshes
+    ksb::DevBuf<float> texcoords; // 2 per vertex: MeshData::texcoords
     // lights (PowerLightSampler over [sky] + mesh-light triangles)
     bool lights_built = false;
     uint32_t light_count = 0, n_nonmesh = 0;

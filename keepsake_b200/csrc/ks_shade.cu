@@ -114,7 +114,8 @@ __global__ void __launch_bounds__(128) k_sample(const __grid_constant__ SceneVie
 // probability that its emitter-hit weight includes, and the two only stay the same functions of
 // the direction if both keep seeing the BSDF pdf.
 // kBatch: paths of many jobs; the view, parameters and accumulators of a path's job come from bv.
-template <bool kMiss, bool kGuided, bool kBatch = false>
+// kAttribs: meshes may carry vertex normals (smooth shading frames) and texcoords (tangents).
+template <bool kMiss, bool kGuided, bool kBatch = false, bool kAttribs = false>
 __global__ void __launch_bounds__(128, KS_SHADE_MIN_BLOCKS) k_shade(const __grid_constant__ SceneView sv_in,
                                                const __grid_constant__ RenderParams rp_in, PathBuf cur, PathBuf nxt,
                                                const float4 *hits, const uint32_t *hit_inst,
@@ -187,10 +188,10 @@ __global__ void __launch_bounds__(128, KS_SHADE_MIN_BLOCKS) k_shade(const __grid
                 uint32_t tri = bits(v0.w);
                 f3 p0 = mk(v0.x, v0.y, v0.z), p1 = mk(v1.x, v1.y, v1.z), p2 = mk(v2.x, v2.y, v2.z);
                 uint32_t inst = 0;
+                float m[12];
                 if (sv.inst.n) {
                     // instanced: the hit triangle in world space (transform_it, ray.h:166-183)
                     inst = hit_inst[i];
-                    float m[12];
 #pragma unroll
                     for (int e = 0; e < 12; ++e)
                         m[e] = __ldg(&sv.inst.xf[12 * (size_t)inst + e]);
@@ -200,7 +201,8 @@ __global__ void __launch_bounds__(128, KS_SHADE_MIN_BLOCKS) k_shade(const __grid
                 }
                 uint32_t mesh = __ldg(&sv.tri_mesh[tri]);
                 const MaterialGPU &mat = sv.materials[__ldg(&sv.mesh_material[mesh])];
-                ShadeFrame it = make_frame(p0, p1, p2, h.y, h.z, rd, __ldg(&sv.mesh_twosided[mesh]) != 0);
+                ShadeFrame it = hit_frame<kAttribs>(sv, tri, __ldg(&sv.mesh_flags[mesh]), p0, p1, p2, h.y, h.z, rd,
+                                          sv.inst.n ? m : nullptr);
                 // emitter hit (small_pt.cpp:112-138)
                 if (mat.has_emission && sv.tri_light) {
                     int32_t light = __ldg(&sv.tri_light[tri]);
@@ -403,27 +405,33 @@ void launch_sample(bool batch, unsigned grid, cudaStream_t st, const SceneView &
         k_sample<false><<<grid, 128, 0, st>>>(sv, rp, cur, hits, hit_inst, queue, queue_count, samples, bv);
 }
 
-void launch_shade(bool miss, bool guided, bool batch, unsigned grid, cudaStream_t st, const SceneView &sv,
-                  const RenderParams &rp, PathBuf cur, PathBuf nxt, const float4 *hits, const uint32_t *hit_inst,
-                  const float4 *samples, const uint32_t *queue, const uint32_t *queue_count, uint32_t *next_count,
-                  ShadowBuf sb, uint32_t *shadow_count, double *accum, double *weights, const GuideView &gv,
-                  const BatchView &bv)
+void launch_shade(bool miss, bool guided, bool batch, bool attribs, unsigned grid, cudaStream_t st,
+                  const SceneView &sv, const RenderParams &rp, PathBuf cur, PathBuf nxt, const float4 *hits,
+                  const uint32_t *hit_inst, const float4 *samples, const uint32_t *queue, const uint32_t *queue_count,
+                  uint32_t *next_count, ShadowBuf sb, uint32_t *shadow_count, double *accum, double *weights,
+                  const GuideView &gv, const BatchView &bv)
 {
 #define KS_SHADE_ARGS                                                                                              \
     sv, rp, cur, nxt, hits, hit_inst, samples, queue, queue_count, next_count, sb, shadow_count, accum, weights, gv, bv
     if (batch) {
         if (miss)
             k_shade<true, false, true><<<grid, 128, 0, st>>>(KS_SHADE_ARGS);
+        else if (attribs)
+            k_shade<false, false, true, true><<<grid, 128, 0, st>>>(KS_SHADE_ARGS);
         else
             k_shade<false, false, true><<<grid, 128, 0, st>>>(KS_SHADE_ARGS);
     } else if (guided) {
         if (miss)
             k_shade<true, true><<<grid, 128, 0, st>>>(KS_SHADE_ARGS);
+        else if (attribs)
+            k_shade<false, true, false, true><<<grid, 128, 0, st>>>(KS_SHADE_ARGS);
         else
             k_shade<false, true><<<grid, 128, 0, st>>>(KS_SHADE_ARGS);
     } else {
         if (miss)
             k_shade<true, false><<<grid, 128, 0, st>>>(KS_SHADE_ARGS);
+        else if (attribs)
+            k_shade<false, false, false, true><<<grid, 128, 0, st>>>(KS_SHADE_ARGS);
         else
             k_shade<false, false><<<grid, 128, 0, st>>>(KS_SHADE_ARGS);
     }

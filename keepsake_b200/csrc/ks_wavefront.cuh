@@ -172,18 +172,37 @@ KS_D f3 hit_point(f3 p0, f3 p1, f3 p2, float u, float v)
     return w0 * p0 + u * p1 + v * p2;
 }
 
-KS_D ShadeFrame make_frame(f3 p0, f3 p1, f3 p2, float u, float v, f3 ray_dir, bool twosided)
+// dP/du from the triangle's texture coordinates (geometry.cpp:94-116); the positional dP/du
+// (p1 - p0) when the uv parameterisation is degenerate.
+KS_D f3 uv_dpdu(f3 p0, f3 p1, f3 p2, float2 t0, float2 t1, float2 t2, f3 dpdu)
+{
+    const float du02 = t0.x - t2.x, dv02 = t0.y - t2.y;
+    const float du12 = t1.x - t2.x, dv12 = t1.y - t2.y;
+    const float det = du02 * dv12 - dv02 * du12;
+    if (!(fabsf(det) < 1e-8f)) {
+        const float inv = 1.0f / det;
+        dpdu = (dv12 * (p0 - p2) - dv02 * (p1 - p2)) * inv;
+    }
+    return dpdu;
+}
+
+// compute_intersection (geometry.cpp:68-163) for a hit at barycentrics (u, v) of the triangle
+// (p0, p1, p2), all in the space the frame is built in.  `dpdu` is p1 - p0 or the uv-derived
+// tangent.  Smooth shading: `vn` is the interpolated vertex normal carried into that space (the
+// zero vector for flat shading); a non-finite normal falls back to the geometric frame.
+KS_D ShadeFrame make_frame(f3 p0, f3 p1, f3 p2, float u, float v, f3 ray_dir, bool twosided, f3 dpdu, bool smooth,
+                           f3 vn)
 {
     ShadeFrame f;
     f3 rd = normalize(ray_dir);
     f3 wo_object = -rd;
     f3 ng = normalize(cross(p1 - p0, p2 - p0));
     f.p = hit_point(p0, p1, p2, u, v);
-    f3 dpdu = p1 - p0;
     f3 b = normalize(cross(ng, dpdu));
     f3 t = normalize(cross(b, ng));
     if (twosided && dot(wo_object, ng) < 0.0f) {
         ng = -ng;
+        dpdu = -dpdu;
         t = -t;
     }
     f3 ft = t, fb = b, fn = ng;
@@ -191,11 +210,77 @@ KS_D ShadeFrame make_frame(f3 p0, f3 p1, f3 p2, float u, float v, f3 ray_dir, bo
     f.t = ft;
     f.b = fb;
     f.n = fn;
+    if (smooth) {
+        vn = normalize(vn);
+        if (isfinite(vn.x) && isfinite(vn.y) && isfinite(vn.z)) {
+            // the vertex normal on the side of the face normal, the frame re-orthogonalised
+            // around it (geometry.cpp:142-155)
+            if (dot(vn, ng) < 0.0f)
+                vn = -vn;
+            f3 vb = normalize(cross(vn, dpdu));
+            f3 vt = normalize(cross(vb, vn));
+            reortho(vt, vb, vn);
+            f.st = vt;
+            f.sb = vb;
+            f.sn = vn;
+            return f;
+        }
+    }
     // flat shading: sh_frame = frame (geometry.cpp:139-141), re-orthonormalised identically
     f.st = ft;
     f.sb = fb;
     f.sn = fn;
     return f;
+}
+
+// The per-vertex attributes of a hit: dP/du (from texcoords) and the interpolated vertex normal.
+// Instanced hits pass the world-space vertices and the instance's object-to-world rows `m` (12
+// floats); the vertex normal goes to world space through the cofactor matrix of m, which is what
+// the reference's Transform::frame makes of a frame built around it in object space
+// (maths.h:989-996).
+struct HitAttribs
+{
+    f3 dpdu, vn;
+};
+KS_D HitAttribs hit_attribs(const SceneView &sv, uint32_t tri, int flags, f3 p0, f3 p1, f3 p2,
+                                               float u, float v, const float *m)
+{
+    HitAttribs a{p1 - p0, mk(0.0f, 0.0f, 0.0f)};
+    const uint32_t i0 = __ldg(&sv.indices[3 * (size_t)tri]), i1 = __ldg(&sv.indices[3 * (size_t)tri + 1]),
+                   i2 = __ldg(&sv.indices[3 * (size_t)tri + 2]);
+    if (flags & kMeshTexcoords) {
+        const float2 *tc = reinterpret_cast<const float2 *>(sv.texcoords);
+        a.dpdu = uv_dpdu(p0, p1, p2, __ldg(&tc[i0]), __ldg(&tc[i1]), __ldg(&tc[i2]), a.dpdu);
+    }
+    if (flags & kMeshSmooth) {
+        auto ld = [&](uint32_t k) {
+            return mk(__ldg(&sv.normals[3 * (size_t)k]), __ldg(&sv.normals[3 * (size_t)k + 1]),
+                      __ldg(&sv.normals[3 * (size_t)k + 2]));
+        };
+        // rtcInterpolate0 of the vertex-normal buffer: (1 - u - v) n0 + u n1 + v n2
+        a.vn = hit_point(ld(i0), ld(i1), ld(i2), u, v);
+        if (m) {
+            const f3 c0 = mk(m[0], m[4], m[8]), c1 = mk(m[1], m[5], m[9]), c2 = mk(m[2], m[6], m[10]);
+            a.vn = a.vn.x * cross(c1, c2) + a.vn.y * cross(c2, c0) + a.vn.z * cross(c0, c1);
+        }
+    }
+    return a;
+}
+
+// The hit's frames from the scene's per-mesh flags and per-vertex attributes.  kAttribs = false
+// (no mesh of the scene has vertex normals or texcoords) compiles to the flat-shading frame only:
+// a separate shading frame keeps three more values live through the BSDF code.
+template <bool kAttribs>
+KS_D ShadeFrame hit_frame(const SceneView &sv, uint32_t tri, int flags, f3 p0, f3 p1, f3 p2, float u, float v,
+                          f3 ray_dir, const float *m)
+{
+    HitAttribs a{p1 - p0, mk(0.0f, 0.0f, 0.0f)};
+    if (!kAttribs)
+        flags &= kMeshTwosided;
+    else if (flags & (kMeshSmooth | kMeshTexcoords))
+        a = hit_attribs(sv, tri, flags, p0, p1, p2, u, v, m);
+    return make_frame(p0, p1, p2, u, v, ray_dir, (flags & kMeshTwosided) != 0, a.dpdu, (flags & kMeshSmooth) != 0,
+                      a.vn);
 }
 
 KS_D f3 sh_to_local(const ShadeFrame &f, f3 w)
@@ -279,8 +364,9 @@ void launch_sample(bool batch, unsigned grid, cudaStream_t st, const SceneView &
                    PathBuf cur, const float4 *hits, const uint32_t *hit_inst, const uint32_t *queue,
                    const uint32_t *queue_count, float4 *samples, const BatchView &bv);
 // k_shade: hit (miss = false) or miss shading of the paths in a queue; guided and batched
-// renders are not combined.
-void launch_shade(bool miss, bool guided, bool batch, unsigned grid, cudaStream_t st, const SceneView &sv,
+// renders are not combined.  attribs: some mesh of the scene (of a job) has vertex normals or
+// texcoords.
+void launch_shade(bool miss, bool guided, bool batch, bool attribs, unsigned grid, cudaStream_t st, const SceneView &sv,
                   const RenderParams &rp, PathBuf cur, PathBuf nxt, const float4 *hits, const uint32_t *hit_inst,
                   const float4 *samples, const uint32_t *queue, const uint32_t *queue_count, uint32_t *next_count,
                   ShadowBuf sb, uint32_t *shadow_count, double *accum, double *weights, const GuideView &gv,

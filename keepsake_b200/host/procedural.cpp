@@ -508,6 +508,7 @@ void GeneratedScene::finalize()
         d.indices = meshes[i].indices.data();
         d.n_triangles = (uint32_t)meshes[i].indices.size() / 3;
         d.vertex_normals = nullptr;
+        d.texcoords = nullptr;
         d.material = meshes[i].material;
         d.twosided = 1;
         d.use_smooth_normal = 1;

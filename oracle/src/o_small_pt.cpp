@@ -5,7 +5,7 @@
 //   Material::sample_with_nee     material.cpp:101-167 (no subsurface)
 //   Camera::spawn_ray             camera.cpp:129-170 (perspective, no ray differentials: the
 //                                 constant shader fields never read them)
-//   MeshGeometry::compute_intersection  geometry.cpp:68-163 (no texcoords, flat shading)
+//   MeshGeometry::compute_intersection  geometry.cpp:68-163 (texcoord tangents, smooth normals)
 //   transform_it / Transform::frame      ray.h:166-183, maths.h:989-996
 //   SkyLight                      light.cpp:19-159 (in-memory lat-long map instead of a file)
 //   MeshLightShared / MeshTriLight light.cpp:307-628 (constant emission: uniform importance)
@@ -301,7 +301,9 @@ struct Scene
     std::vector<uint32_t> tri_mesh;
     std::vector<uint32_t> mesh_tri_off;
     std::vector<uint32_t> mesh_material;
-    std::vector<int> mesh_twosided;
+    std::vector<int> mesh_twosided, mesh_smooth, mesh_uv;
+    std::vector<float> normals;   // 3 per vertex (zeros for meshes without)
+    std::vector<float> texcoords; // 2 per vertex (zeros for meshes without)
     std::vector<ks_material_desc> materials;
     void *bvh = nullptr;
     float bound[6];
@@ -374,9 +376,23 @@ inline Intersection make_intersection(const Scene &s, uint32_t tri, float t, flo
     float w0 = 1.0f - u - v;
     it.p = w0 * p0 + u * p1 + v * p2;
     V3 dpdu = p1 - p0;
+    const uint32_t mesh = s.tri_mesh[tri];
+    const uint32_t i0 = s.idx[3 * tri], i1 = s.idx[3 * tri + 1], i2 = s.idx[3 * tri + 2];
+    if (s.mesh_uv[mesh]) {
+        // dP/du of the texture parameterisation (geometry.cpp:94-116)
+        const float *tc = s.texcoords.data();
+        float du02 = tc[2 * i0] - tc[2 * i2], dv02 = tc[2 * i0 + 1] - tc[2 * i2 + 1];
+        float du12 = tc[2 * i1] - tc[2 * i2], dv12 = tc[2 * i1 + 1] - tc[2 * i2 + 1];
+        V3 dp02 = p0 - p2, dp12 = p1 - p2;
+        float det = du02 * dv12 - dv02 * du12;
+        if (!(std::abs(det) < 1e-8f)) {
+            float inv = 1.0f / det;
+            dpdu = (dv12 * dp02 - dv02 * dp12) * inv;
+        }
+    }
     V3 b = normalized(cross(ng, dpdu));
     V3 tt = normalized(cross(b, ng));
-    if (s.mesh_twosided[s.tri_mesh[tri]]) {
+    if (s.mesh_twosided[mesh]) {
         if (dot(wo_object, ng) < 0.0f) {
             ng = -ng;
             dpdu = -dpdu;
@@ -387,6 +403,20 @@ inline Intersection make_intersection(const Scene &s, uint32_t tri, float t, flo
     it.frame.b = b;
     it.frame.n = ng;
     it.sh_frame = it.frame;
+    if (s.mesh_smooth[mesh]) {
+        // interpolated vertex normal; a non-finite one keeps the face frame (geometry.cpp:139-156)
+        auto nrm = [&](uint32_t k) { return V3(s.normals[3 * k], s.normals[3 * k + 1], s.normals[3 * k + 2]); };
+        V3 vn = normalized(w0 * nrm(i0) + u * nrm(i1) + v * nrm(i2));
+        if (std::isfinite(vn.x) && std::isfinite(vn.y) && std::isfinite(vn.z)) {
+            if (dot(vn, it.frame.n) < 0.0f)
+                vn = -vn;
+            V3 vb = normalized(cross(vn, dpdu));
+            V3 vt = normalized(cross(vb, vn));
+            it.sh_frame.t = vt;
+            it.sh_frame.b = vb;
+            it.sh_frame.n = vn;
+        }
+    }
     // transform_it with the identity instance transform
     it.frame = identity_transform_frame(it.frame);
     it.sh_frame = identity_transform_frame(it.sh_frame);
@@ -641,6 +671,16 @@ Scene *create_scene(const ks_scene_desc *d, const ks_sbvh_options *opts)
         s->tri_mesh.insert(s->tri_mesh.end(), md.n_triangles, m);
         s->mesh_material.push_back(md.material);
         s->mesh_twosided.push_back(md.twosided);
+        s->mesh_smooth.push_back(md.use_smooth_normal && md.vertex_normals ? 1 : 0);
+        s->mesh_uv.push_back(md.texcoords ? 1 : 0);
+        if (md.use_smooth_normal && md.vertex_normals)
+            s->normals.insert(s->normals.end(), md.vertex_normals, md.vertex_normals + 3 * md.n_vertices);
+        else
+            s->normals.insert(s->normals.end(), 3 * (size_t)md.n_vertices, 0.0f);
+        if (md.texcoords)
+            s->texcoords.insert(s->texcoords.end(), md.texcoords, md.texcoords + 2 * md.n_vertices);
+        else
+            s->texcoords.insert(s->texcoords.end(), 2 * (size_t)md.n_vertices, 0.0f);
         vo += md.n_vertices;
     }
     s->mesh_tri_off.push_back((uint32_t)s->tri_mesh.size());
