@@ -384,9 +384,13 @@ ks_status ks_small_pt_render_guided_device(ks_scene *scene, const ks_camera_desc
  * "small_pt" and "small_pt_b200" (same keys as small_pt.cpp:180-241, plus `emission` on a
  * material).  Runs every [[task]] of config_text in order; asset paths are relative to
  * asset_root_dir (NULL = current directory); outputs go to output_dir/<task_dir or task_N>/
- * (config.toml and small_pt_spp<N>.pfm per spp interval).  Supported assets: [bsdf.X] of type
- * principled_bsdf with constant fields, [material.X] {bsdf, emission}, [mesh_asset.X] of type
- * "obj" (path), "inline" (geometry list) or "procedural" (kind box_room | icosphere).  Returns
+ * (config.toml and small_pt_spp<N>.exr per spp interval).  Also registered: "convert_mesh_asset"
+ * (mesh_asset.cpp:301-311: the listed mesh assets as <name>.bin binary mesh assets).  Supported
+ * assets: [bsdf.X] of type principled_bsdf with constant fields, [material.X] {bsdf, emission},
+ * [mesh_asset.X] with a `path` and `format` "obj" (positions, texcoords, normals; twosided,
+ * use_smooth_normal) or "bin" (keepsake's binary mesh asset), optional `to_world`
+ * (create_mesh_asset, mesh_asset.cpp:243-266), or of `type` "inline" (geometry list) or
+ * "procedural" (kind box_room | icosphere); sky maps from .exr, .hdr or .pfm files.  Returns
  * KS_ERR_PARSE, KS_ERR_IO or KS_ERR_UNSUPPORTED with a message in ks_config_last_error().
  * C++ hosts can use the ConfigTask-shaped API of ks_b200_task.hpp instead.
  * ------------------------------------------------------------------------------------------- */
@@ -397,6 +401,23 @@ const char *ks_config_last_error(void);
  * The document, normalised (keys sorted, nested tables inline), is written to normalised
  * (NUL-terminated, truncated to capacity; may be NULL) and its length to *length (may be NULL). */
 ks_status ks_config_parse(const char *config_text, char *normalised, size_t capacity, size_t *length);
+
+/* ---------------------------------------------------------------------------------------------
+ * Image files of the small_pt task (save_to_exr / load_from_exr, image_util.cpp:71-190; the
+ * Radiance .hdr maps SkyLight reads through stb_image, light.cpp:19-31).
+ * ------------------------------------------------------------------------------------------- */
+/* Writes width x height pixels of `channels` (1-4) interleaved floats, rows top first, as an
+ * OpenEXR scanline file with save_to_exr's channel names (R, G, B, A), FP32 (half = 0) or FP16
+ * (half = 1, rounded to nearest even), ZIP-compressed.  KS_ERR_INVALID_ARGUMENT, KS_ERR_IO. */
+ks_status ks_image_save_exr(const char *path, const float *pixels, int32_t width, int32_t height,
+                            int32_t channels, int32_t half);
+/* Reads the RGB pixels of an .exr (NONE, RLE, ZIPS or ZIP compression; R, G, B channels or a
+ * single one), .hdr (RGBE) or .pfm file, by extension, into a buffer the library allocates
+ * (width * height * 3 floats, rows top first; release it with ks_image_free).  KS_ERR_IO, or
+ * KS_ERR_UNSUPPORTED for a variant of the format this reader does not handle; the message is in
+ * ks_config_last_error(). */
+ks_status ks_image_load_rgb(const char *path, float **pixels, int32_t *width, int32_t *height);
+void ks_image_free(float *pixels);
 
 /* ---------------------------------------------------------------------------------------------
  * Batched rendering: many (scene, camera, parameters) jobs in one wavefront.  The paths of all

@@ -9,8 +9,14 @@
  *   reading the same keys (object, material, sky, backdrop, bounces, clamp_direct,
  *   clamp_indirect, render_width, render_height, crop_*, spp, scale_ray_diff, rng_seed,
  *   spp_prog_interval, camera) plus the `emission` key of a material.  After every spp interval
- *   the composited image is written to TASK_DIR/small_pt_spp<N>.pfm (the reference writes EXR
- *   through tinyexr, which this build does not have).
+ *   the composited image is written to TASK_DIR/small_pt_spp<N>.exr (OpenEXR, FP32 RGB; ZIP
+ *   compression where the reference's tinyexr call asks for PIZ: both lossless).  Sky maps are
+ *   read from .exr, .hdr (and .pfm) files.
+ *   "convert_mesh_asset": each mesh asset of `assets` written to TASK_DIR/<name>.bin in keepsake's
+ *   binary mesh asset format (mesh_asset.cpp:180-240, 301-311).
+ * Mesh assets: `path` + `format` "obj" (twosided, default false; use_smooth_normal, default true;
+ * positions, texcoords and normals) or "bin", with an optional `to_world` transform
+ * (create_mesh_asset, mesh_asset.cpp:243-266).
  * Errors throw std::runtime_error (the reference asserts); the C entry point ks_config_run in
  * ks_b200.h returns a status instead.
  */
@@ -57,6 +63,7 @@ using ConfigTask = std::function<void(const ConfigArgs &args, const std::filesys
 
 // The GPU small_pt task.  Device: KS_B200_DEVICE environment variable, else 0.
 void small_pt_b200(const ConfigArgs &args, const std::filesystem::path &task_dir, int task_id);
+void convert_mesh_asset(const ConfigArgs &args, const std::filesystem::path &task_dir, int task_id);
 
 struct ConfigServiceImpl;
 

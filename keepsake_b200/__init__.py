@@ -672,6 +672,36 @@ def read_pfm(path):
     return data.reshape(h, w, 3)[::-1].astype(np.float32)
 
 
+_sig("ks_image_save_exr", [ctypes.c_char_p, _vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32])
+_sig("ks_image_load_rgb", [ctypes.c_char_p, ctypes.POINTER(ctypes.POINTER(_f32)), ctypes.POINTER(ctypes.c_int32),
+                           ctypes.POINTER(ctypes.c_int32)])
+_sig("ks_image_free", [ctypes.POINTER(_f32)], None)
+
+
+def save_exr(path, pixels, half=False):
+    """float array [H, W, C] (C = 1..4, R G B A) -> OpenEXR file (ks_image_save_exr)."""
+    a = np.ascontiguousarray(pixels, np.float32)
+    if a.ndim == 2:
+        a = a[:, :, None]
+    h, w, c = a.shape
+    st = lib.ks_image_save_exr(str(path).encode(), a.ctypes.data, w, h, c, int(half))
+    if st != KS_OK:
+        raise KsError(st, lib.ks_config_last_error().decode())
+
+
+def load_image(path) -> np.ndarray:
+    """RGB pixels of an .exr, .hdr or .pfm file -> float32 [H, W, 3] (ks_image_load_rgb)."""
+    buf = ctypes.POINTER(_f32)()
+    w, h = ctypes.c_int32(), ctypes.c_int32()
+    st = lib.ks_image_load_rgb(str(path).encode(), ctypes.byref(buf), ctypes.byref(w), ctypes.byref(h))
+    if st != KS_OK:
+        raise KsError(st, lib.ks_config_last_error().decode())
+    try:
+        return np.ctypeslib.as_array(buf, shape=(h.value, w.value, 3)).copy()
+    finally:
+        lib.ks_image_free(buf)
+
+
 # ---------------------------------------------------------------------------------------------
 # Batched rendering (ks_batch_*)
 # ---------------------------------------------------------------------------------------------

@@ -10,8 +10,13 @@
 //   create_sky_light                   light.cpp:257-275
 //   create_camera / look_at            camera.cpp:12-31,172-205
 //   load_transform_field               config.cpp:204-260
+//   create_mesh_asset                  mesh_asset.cpp:243-266 (obj / bin formats, to_world)
+//   convert_mesh_asset task            mesh_asset.cpp:301-311
+//   composite_and_save_to_exr          render_target.cpp:181-208 (interval images)
 #include "../../include/ks_b200.h"
 #include "../../include/ks_b200_task.hpp"
+#include "image_io.h"
+#include "mesh_io.h"
 #include "procedural.h"
 #include "toml.h"
 
@@ -56,6 +61,10 @@ struct Geometry
 {
     std::vector<float> vertices;
     std::vector<uint32_t> indices;
+    std::vector<float> normals;   // 3 per vertex or empty
+    std::vector<float> texcoords; // 2 per vertex or empty
+    bool twosided = true;
+    bool use_smooth_normal = true;
     int own_material = -1; // index into MeshAsset::materials (procedural assets)
 };
 
@@ -310,63 +319,19 @@ ConfigArgs args_of(ConfigServiceImpl *svc, const Value *node, const std::string 
     return ConfigArgs(a);
 }
 
-// Wavefront OBJ: v lines and polygonal f lines (fan-triangulated; v, v/t, v//n, v/t/n and
-// negative indices); every o / g statement starts a new geometry.
-void load_obj(const fs::path &path, MeshAsset &out)
+// MeshData (mesh files) to the task's geometries.
+void add_meshes(std::vector<ksb::mesh::MeshData> &&meshes, MeshAsset &out)
 {
-    std::ifstream f(path);
-    if (!f)
-        throw IoError("cannot open " + path.string());
-    std::vector<float> pos;
-    Geometry cur;
-    std::map<uint32_t, uint32_t> remap;
-    auto flush = [&]() {
-        if (!cur.indices.empty())
-            out.geometries.push_back(std::move(cur));
-        cur = Geometry();
-        remap.clear();
-    };
-    std::string line;
-    int ln = 0;
-    while (std::getline(f, line)) {
-        ++ln;
-        std::istringstream ss(line);
-        std::string tag;
-        ss >> tag;
-        if (tag == "v") {
-            float x, y, z;
-            if (!(ss >> x >> y >> z))
-                throw ParseError(path.string() + ":" + std::to_string(ln) + ": bad vertex");
-            pos.insert(pos.end(), {x, y, z});
-        } else if (tag == "o" || tag == "g") {
-            flush();
-        } else if (tag == "f") {
-            std::vector<uint32_t> poly;
-            std::string tok;
-            while (ss >> tok) {
-                long idx = std::strtol(tok.c_str(), nullptr, 10);
-                long nv = (long)pos.size() / 3;
-                long v = idx < 0 ? nv + idx : idx - 1;
-                if (idx == 0 || v < 0 || v >= nv)
-                    throw ParseError(path.string() + ":" + std::to_string(ln) + ": bad face index");
-                auto it = remap.find((uint32_t)v);
-                uint32_t local;
-                if (it == remap.end()) {
-                    local = (uint32_t)cur.vertices.size() / 3;
-                    cur.vertices.insert(cur.vertices.end(), {pos[3 * v], pos[3 * v + 1], pos[3 * v + 2]});
-                    remap[(uint32_t)v] = local;
-                } else {
-                    local = it->second;
-                }
-                poly.push_back(local);
-            }
-            for (size_t k = 2; k < poly.size(); ++k)
-                cur.indices.insert(cur.indices.end(), {poly[0], poly[k - 1], poly[k]});
-        }
+    for (auto &md : meshes) {
+        Geometry g;
+        g.vertices = std::move(md.vertices);
+        g.indices = std::move(md.indices);
+        g.normals = std::move(md.normals);
+        g.texcoords = std::move(md.texcoords);
+        g.twosided = md.twosided;
+        g.use_smooth_normal = md.use_smooth_normal;
+        out.geometries.push_back(std::move(g));
     }
-    flush();
-    if (out.geometries.empty())
-        throw ParseError(path.string() + ": no faces");
 }
 
 void flat_numbers(const Value &v, std::vector<double> &out, const std::string &what)
@@ -391,8 +356,51 @@ std::shared_ptr<MeshAsset> ConfigServiceImpl::mesh_asset(const std::string &path
         throw ParseError("config: unknown mesh asset '" + path + "'");
     ConfigArgs a = args_of(this, node, path);
     auto m = std::make_shared<MeshAsset>();
-    std::string type = a.load_string("type", a.contains("path") ? "obj" : "inline");
-    if (type == "procedural") {
+    // a mesh file (create_mesh_asset: "format" obj | bin), or an extension "type" of this build
+    std::string type = a.contains("type") ? a.load_string("type") : a.contains("path") ? "file" : "inline";
+    if (type == "obj" || type == "bin") // the file types spelled as "type"
+        type = "file";
+    if (type == "file") {
+        const std::string fmt = a.contains("format") ? a.load_string("format")
+                                : a.contains("type") ? a.load_string("type")
+                                                     : "obj";
+        const fs::path file = a.load_path("path");
+        try {
+            if (fmt == "obj") {
+                if (a.load_bool("load_materials", false))
+                    throw StatusError(KS_ERR_UNSUPPORTED, "config: load_materials (MTL Lambertian materials) is not "
+                                                          "supported; give the task a material list");
+                add_meshes(ksb::mesh::load_obj(file, a.load_bool("twosided", false),
+                                               a.load_bool("use_smooth_normal", true)),
+                           *m);
+            } else if (fmt == "bin") {
+                add_meshes(ksb::mesh::load_binary(file), *m);
+            } else {
+                throw StatusError(KS_ERR_UNSUPPORTED, "config: unsupported mesh asset format '" + fmt + "'");
+            }
+        } catch (const ksb::mesh::Error &e) {
+            throw IoError(e.what());
+        }
+        if (a.contains("to_world")) {
+            // MeshData::transform (geometry.cpp:15-32) of every mesh of the asset
+            float xf[16];
+            a.load_transform("to_world", xf);
+            std::vector<ksb::mesh::MeshData> tmp(m->geometries.size());
+            for (size_t k = 0; k < tmp.size(); ++k) {
+                tmp[k].vertices = std::move(m->geometries[k].vertices);
+                tmp[k].normals = std::move(m->geometries[k].normals);
+            }
+            try {
+                ksb::mesh::transform(tmp, xf);
+            } catch (const ksb::mesh::Error &e) {
+                throw ParseError(std::string("config: ") + e.what());
+            }
+            for (size_t k = 0; k < tmp.size(); ++k) {
+                m->geometries[k].vertices = std::move(tmp[k].vertices);
+                m->geometries[k].normals = std::move(tmp[k].normals);
+            }
+        }
+    } else if (type == "procedural") {
         // seeded synthetic scene (extension): kind "box_room" | "icosphere"
         ksb::ProceduralOptions o;
         o.level = a.load_integer("level", o.level);
@@ -423,8 +431,6 @@ std::shared_ptr<MeshAsset> ConfigServiceImpl::mesh_asset(const std::string &path
         m->sky_map = std::move(g.sky_map);
         m->sky = g.sky;
         m->sky.map_rgb = nullptr;
-    } else if (type == "obj") {
-        load_obj(a.load_path("path"), *m);
     } else if (type == "inline") {
         // extension for small scenes written in the file: geometry = [{vertices = [...], indices = [...]}]
         ConfigArgs list = a["geometry"];
@@ -559,54 +565,16 @@ void look_at(const float pos[3], const float target[3], float up[3], float m[16]
     std::memcpy(m, mm, sizeof(mm));
 }
 
-// Portable float map (little-endian RGB, bottom row first).
-void write_pfm(const fs::path &path, int w, int h, const std::vector<float> &rgb)
-{
-    std::ofstream f(path, std::ios::binary);
-    if (!f)
-        throw IoError("cannot write " + path.string());
-    f << "PF\n" << w << " " << h << "\n-1.0\n";
-    for (int y = h - 1; y >= 0; --y)
-        f.write(reinterpret_cast<const char *>(rgb.data() + (size_t)y * w * 3), sizeof(float) * 3 * w);
-    if (!f)
-        throw IoError("cannot write " + path.string());
-}
-
-std::vector<float> read_pfm(const fs::path &path, uint32_t &w, uint32_t &h)
-{
-    std::ifstream f(path, std::ios::binary);
-    if (!f)
-        throw IoError("cannot open " + path.string());
-    std::string magic;
-    double scale;
-    f >> magic >> w >> h >> scale;
-    f.get();
-    if (magic != "PF" || !f || w == 0 || h == 0)
-        throw IoError(path.string() + ": not an RGB PFM file");
-    std::vector<float> top_first((size_t)w * h * 3), rows((size_t)w * h * 3);
-    f.read(reinterpret_cast<char *>(rows.data()), sizeof(float) * rows.size());
-    if (!f)
-        throw IoError(path.string() + ": truncated");
-    if (scale > 0.0)
-        for (float &v : rows) {
-            uint32_t u;
-            std::memcpy(&u, &v, 4);
-            u = __builtin_bswap32(u);
-            std::memcpy(&v, &u, 4);
-        }
-    for (uint32_t y = 0; y < h; ++y)
-        std::memcpy(&top_first[(size_t)y * w * 3], &rows[(size_t)(h - 1 - y) * w * 3], sizeof(float) * 3 * w);
-    return top_first;
-}
-
 struct TaskOutput
 {
     fs::path dir;
     int w, h;
     float backdrop[3];
+    std::string error; // the first failed image write (reported after the render returns)
 };
 
-// RenderTarget2::composite_and_save_to_exr (render_target.cpp:181-205), written as PFM
+// RenderTarget2::composite_and_save_to_exr (render_target.cpp:181-208): the composite of each
+// progressive interval as small_pt_spp<N>.exr (FP32 RGB)
 void save_interval(int spp, const double *accum, const double *weights, void *user)
 {
     auto *o = static_cast<TaskOutput *>(user);
@@ -620,8 +588,13 @@ void save_interval(int spp, const double *accum, const double *weights, void *us
         }
     }
     char name[64];
-    std::snprintf(name, sizeof(name), "small_pt_spp%d.pfm", spp);
-    write_pfm(o->dir / name, o->w, o->h, rgb);
+    std::snprintf(name, sizeof(name), "small_pt_spp%d.exr", spp);
+    try {
+        ksb::image::write_exr(o->dir / name, rgb.data(), o->w, o->h, 3, false);
+    } catch (const ksb::image::Error &e) {
+        if (o->error.empty())
+            o->error = e.what();
+    }
 }
 
 struct ContextGuard
@@ -675,8 +648,15 @@ void small_pt_b200(const ConfigArgs &args, const fs::path &task_dir, int task_id
     std::vector<ks_mesh_desc> meshes(asset->geometries.size());
     for (size_t g = 0; g < meshes.size(); ++g) {
         const Geometry &geo = asset->geometries[g];
-        meshes[g] = ks_mesh_desc{geo.vertices.data(), (uint32_t)(geo.vertices.size() / 3), geo.indices.data(),
-                                 (uint32_t)(geo.indices.size() / 3), nullptr, geom_mat[g], 1, 1};
+        meshes[g] = ks_mesh_desc{geo.vertices.data(),
+                                 (uint32_t)(geo.vertices.size() / 3),
+                                 geo.indices.data(),
+                                 (uint32_t)(geo.indices.size() / 3),
+                                 geo.normals.empty() ? nullptr : geo.normals.data(),
+                                 geom_mat[g],
+                                 geo.twosided ? 1 : 0,
+                                 geo.use_smooth_normal ? 1 : 0,
+                                 geo.texcoords.empty() ? nullptr : geo.texcoords.data()};
     }
     ks_scene_desc desc{};
     desc.meshes = meshes.data();
@@ -703,11 +683,18 @@ void small_pt_b200(const ConfigArgs &args, const fs::path &task_dir, int task_id
                 sky_map = src->sky_map;
                 desc.sky = src->sky;
             } else {
+                // SkyLight reads .hdr and .exr maps (light.cpp:19-31); .pfm is an extension
                 fs::path p = s.load_path("map");
-                if (p.extension() != ".pfm")
-                    throw StatusError(KS_ERR_UNSUPPORTED, "config: sky maps are read from PFM files (" + p.string() +
-                                                              ")");
-                sky_map = read_pfm(p, desc.sky.width, desc.sky.height);
+                int w = 0, h = 0;
+                try {
+                    sky_map = ksb::image::read_rgb(p, w, h);
+                } catch (const ksb::image::Error &e) {
+                    if (e.unsupported)
+                        throw StatusError(KS_ERR_UNSUPPORTED, std::string("config: sky map: ") + e.what());
+                    throw IoError(e.what());
+                }
+                desc.sky.width = (uint32_t)w;
+                desc.sky.height = (uint32_t)h;
                 desc.sky.kind = 2;
                 std::memcpy(desc.sky.to_world, id, sizeof(id));
             }
@@ -788,6 +775,37 @@ void small_pt_b200(const ConfigArgs &args, const fs::path &task_dir, int task_id
         out.backdrop[0] = out.backdrop[1] = out.backdrop[2] = 0.0f;
     check(ks_small_pt_render(g.scene, &cam, &p, save_interval, &out, accum.data(), weights.data()), g.ctx,
           "ks_small_pt_render");
+    if (!out.error.empty())
+        throw IoError(out.error);
+}
+
+// convert_mesh_asset (mesh_asset.cpp:301-311): each listed mesh asset written as a binary mesh
+// asset named after the last component of its asset path, <name>.bin, in the task directory.
+void convert_mesh_asset(const ConfigArgs &args, const fs::path &task_dir, int task_id)
+{
+    (void)task_id;
+    ConfigServiceImpl *svc = args.internal->service;
+    ConfigArgs list = args["assets"];
+    for (int i = 0; i < list.array_size(); ++i) {
+        const std::string asset_path = list.load_string(i);
+        std::shared_ptr<MeshAsset> asset = svc->mesh_asset(asset_path);
+        std::vector<ksb::mesh::MeshData> meshes(asset->geometries.size());
+        for (size_t k = 0; k < meshes.size(); ++k) {
+            const Geometry &g = asset->geometries[k];
+            meshes[k].vertices = g.vertices;
+            meshes[k].indices = g.indices;
+            meshes[k].normals = g.normals;
+            meshes[k].texcoords = g.texcoords;
+            meshes[k].twosided = g.twosided;
+            meshes[k].use_smooth_normal = g.use_smooth_normal;
+        }
+        const std::string name = asset_path.substr(asset_path.rfind('.') + 1);
+        try {
+            ksb::mesh::write_binary(task_dir / (name + ".bin"), meshes);
+        } catch (const ksb::mesh::Error &e) {
+            throw IoError(e.what());
+        }
+    }
 }
 
 // ---- ConfigService ----------------------------------------------------------------------------
@@ -795,6 +813,7 @@ ConfigService::ConfigService() : impl(std::make_unique<ConfigServiceImpl>())
 {
     register_task("small_pt", small_pt_b200);
     register_task("small_pt_b200", small_pt_b200);
+    register_task("convert_mesh_asset", convert_mesh_asset);
 }
 ConfigService::~ConfigService() = default;
 
@@ -929,5 +948,52 @@ ks_status ks_config_parse(const char *config_text, char *normalised, size_t capa
         return KS_ERR_PARSE;
     }
 }
+
+ks_status ks_image_save_exr(const char *path, const float *pixels, int32_t width, int32_t height, int32_t channels,
+                            int32_t half)
+{
+    g_config_error.clear();
+    if (!path || !pixels || width <= 0 || height <= 0 || channels < 1 || channels > 4) {
+        g_config_error = "ks_image_save_exr: bad argument";
+        return KS_ERR_INVALID_ARGUMENT;
+    }
+    try {
+        ksb::image::write_exr(path, pixels, width, height, channels, half != 0);
+        return KS_OK;
+    } catch (const std::exception &e) {
+        g_config_error = e.what();
+        return KS_ERR_IO;
+    }
+}
+
+ks_status ks_image_load_rgb(const char *path, float **pixels, int32_t *width, int32_t *height)
+{
+    g_config_error.clear();
+    if (!path || !pixels || !width || !height) {
+        g_config_error = "ks_image_load_rgb: null argument";
+        return KS_ERR_INVALID_ARGUMENT;
+    }
+    *pixels = nullptr;
+    try {
+        int w = 0, h = 0;
+        std::vector<float> rgb = ksb::image::read_rgb(path, w, h);
+        float *out = static_cast<float *>(std::malloc(sizeof(float) * rgb.size()));
+        if (!out)
+            return KS_ERR_OUT_OF_MEMORY;
+        std::memcpy(out, rgb.data(), sizeof(float) * rgb.size());
+        *pixels = out;
+        *width = w;
+        *height = h;
+        return KS_OK;
+    } catch (const ksb::image::Error &e) {
+        g_config_error = e.what();
+        return e.unsupported ? KS_ERR_UNSUPPORTED : KS_ERR_IO;
+    } catch (const std::exception &e) {
+        g_config_error = e.what();
+        return KS_ERR_IO;
+    }
+}
+
+void ks_image_free(float *pixels) { std::free(pixels); }
 
 } // extern "C"

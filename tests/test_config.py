@@ -30,6 +30,7 @@ geometry = [
 
 [mesh_asset.obj_pair]
 path = "pair.obj"
+twosided = true
 
 [[task]]
 type = "small_pt_b200"
@@ -126,9 +127,9 @@ def test_config_inline_and_obj_match(tmp_path):
     ks.config_run(DOC, str(tmp_path / "out"), str(tmp_path))
     for d in ("inline", "obj"):
         for spp in (4, 8):
-            assert (tmp_path / "out" / d / f"small_pt_spp{spp}.pfm").exists()
-    a = ks.read_pfm(tmp_path / "out" / "inline" / "small_pt_spp8.pfm")
-    b = ks.read_pfm(tmp_path / "out" / "obj" / "small_pt_spp8.pfm")
+            assert (tmp_path / "out" / d / f"small_pt_spp{spp}.exr").exists()
+    a = ks.load_image(tmp_path / "out" / "inline" / "small_pt_spp8.exr")
+    b = ks.load_image(tmp_path / "out" / "obj" / "small_pt_spp8.exr")
     assert a.shape == (32, 48, 3) and a.mean() > 0.0
     assert np.array_equal(a, b)
     merged = (tmp_path / "out" / "obj" / "config.toml").read_text()
@@ -162,7 +163,7 @@ rng_seed = 3
 camera = {{ type = "perspective", to_world = {{ matrix_rm = {c2w} }}, vfov = {deg!r}, aspect = {aspect!r} }}
 """
     ks.config_run(doc, str(tmp_path))
-    img = ks.read_pfm(tmp_path / "task_0" / "small_pt_spp16.pfm")
+    img = ks.load_image(tmp_path / "task_0" / "small_pt_spp16.exr")
     vfov = np.float32(deg) / np.float32(180.0) * np.float32(np.pi)
     cam = ks.camera_perspective(np.array(c2w, np.float32), float(vfov), aspect)
     s = ks.Scene(ctx, g.desc)

@@ -211,3 +211,104 @@ def test_instanced_smooth_spheres_match_flattened(ctx):
     fs.close()
     assert a.mean() > 0.0
     assert rel_mse(a, b) < SAME_SEED_RELMSE, rel_mse(a, b)
+
+
+def _obj_text(meshes):
+    """Wavefront OBJ of [(vertices, indices, normals or None, texcoords or None)], one `o` per mesh,
+    a corner's vt / vn the ones of its vertex (floats printed to round-trip exactly)."""
+    out, vb, tb, nb = [], 1, 1, 1
+    for k, (v, idx, n, t) in enumerate(meshes):
+        out.append(f"o mesh{k}")
+        out += ["v %.9g %.9g %.9g" % tuple(map(float, p)) for p in v]
+        if t is not None:
+            out += ["vt %.9g %.9g" % tuple(map(float, p)) for p in t]
+        if n is not None:
+            out += ["vn %.9g %.9g %.9g" % tuple(map(float, p)) for p in n]
+        for tri in idx.astype(np.int64):
+            corners = []
+            for i in tri:
+                c = str(i + vb)
+                if t is not None or n is not None:
+                    c += "/" + (str(i + tb) if t is not None else "")
+                if n is not None:
+                    c += "/" + str(i + nb)
+                corners.append(c)
+            out.append("f " + " ".join(corners))
+        vb += len(v)
+        tb += 0 if t is None else len(t)
+        nb += 0 if n is None else len(n)
+    return "\n".join(out) + "\n"
+
+
+@pytest.mark.gpu
+def test_obj_normals_and_texcoords_through_config_task(ctx, tmp_path):
+    """An OBJ mesh asset with vt / vn lines, rendered by the TOML small_pt task, equals the C-ABI
+    render of the same meshes with the same normals and texcoords (bit-exact image)."""
+    import keepsake_b200 as ks
+    ground = (np.array([[-2, 0, -2], [2, 0, -2], [2, 0, 2], [-2, 0, 2]], np.float32),
+              np.array([[0, 2, 1], [0, 3, 2]], np.uint32), None, None)
+    s1 = uv_sphere((-0.5, 0.3, 0.55), 0.3)
+    s2 = uv_sphere((0.4, 0.25, 0.0), 0.25, nu=12, nv=6)
+    s1 = (s1[0], s1[1], s1[2], s1[3])
+    s2 = (s2[0], s2[1], None, s2[3])  # texcoords only: flat shading, uv tangents
+    (tmp_path / "spheres.obj").write_text(_obj_text([ground, s1, s2]))
+    c2w = [1.0, 0.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.6, 0.0, 0.0, 1.0, 3.0, 0.0, 0.0, 0.0, 1.0]
+    doc = f"""
+[bsdf.white]
+type = "principled_bsdf"
+
+[bsdf.gold]
+type = "principled_bsdf"
+basecolor = {{ type = "constant", value = [0.95, 0.7, 0.35] }}
+roughness = {{ type = "constant", value = 0.2 }}
+metallic = {{ type = "constant", value = 1.0 }}
+
+[bsdf.blue]
+type = "principled_bsdf"
+basecolor = {{ type = "constant", value = [0.3, 0.6, 0.8] }}
+
+[material.white]
+bsdf = "bsdf.white"
+[material.gold]
+bsdf = "bsdf.gold"
+[material.blue]
+bsdf = "bsdf.blue"
+
+[mesh_asset.spheres]
+path = "spheres.obj"
+twosided = true
+
+[[task]]
+type = "small_pt"
+object = "mesh_asset.spheres"
+material = [["material.white", "material.gold", "material.blue"]]
+sky = {{ ambient = [0.6, 0.7, 0.9] }}
+bounces = 6
+render_width = 48
+render_height = 48
+spp = 8
+spp_prog_interval = 8
+rng_seed = 2
+camera = {{ type = "perspective", to_world = {{ matrix_rm = {c2w} }}, vfov = 40.0, aspect = 1.0 }}
+"""
+    ks.config_run(doc, str(tmp_path / "out"), str(tmp_path))
+    img = ks.load_image(tmp_path / "out" / "task_0" / "small_pt_spp8.exr")
+    mats = [_material((0.8, 0.8, 0.8), 1.0, 0.0), _material((0.95, 0.7, 0.35), 0.2, 1.0),
+            _material((0.3, 0.6, 0.8), 1.0, 0.0)]
+    meshes = [(v, i, k, dict(twosided=1, normals=n, texcoords=t)) for k, (v, i, n, t) in enumerate([ground, s1, s2])]
+    sky = ks.SkyDesc()
+    sky.kind = 1
+    sky.ambient[:] = [0.6, 0.7, 0.9]
+    sky.to_world[:] = [1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1]
+    sky.transform_y_up = 1
+    sky.strength = 1.0
+    d, keep = ks.scene_desc(meshes, mats, sky)
+    s = ks.Scene(ctx, d, keepalive=keep)
+    s.build_bvh()
+    vfov = np.float32(40.0) / np.float32(180.0) * np.float32(np.pi)
+    cam = ks.camera_perspective(np.array(c2w, np.float32), float(vfov), 1.0)
+    p = ks.SmallPTParams.make(render_width=48, render_height=48, spp=8, bounces=6, spp_prog_interval=8, rng_seed=2)
+    ref = composite(*s.render(cam, p)).astype(np.float32)
+    s.close()
+    assert img.mean() > 0.0
+    assert np.array_equal(img, ref)
