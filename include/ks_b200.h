@@ -395,7 +395,8 @@ ks_status ks_small_pt_render_guided_device(ks_scene *scene, const ks_camera_desc
  * C++ hosts can use the ConfigTask-shaped API of ks_b200_task.hpp instead.
  * ------------------------------------------------------------------------------------------- */
 ks_status ks_config_run(const char *config_text, const char *asset_root_dir, const char *output_dir);
-/* Message of the last failing ks_config_run / ks_config_parse on this thread ("" if none). */
+/* Message of the last failing host-side call on this thread (ks_config_run, ks_config_parse, the
+ * image and asset loaders; "" if none). */
 const char *ks_config_last_error(void);
 /* Parses config_text without running anything: KS_OK or KS_ERR_PARSE (message with the line).
  * The document, normalised (keys sorted, nested tables inline), is written to normalised
@@ -491,6 +492,17 @@ const ks_scene_desc *ks_generated_scene_desc(const ks_generated *g);
 /* Camera-to-world (row-major 4x4), vertical fov (radians) and aspect of the generated view. */
 ks_status ks_generated_camera(const ks_generated *g, float camera_to_world[16], float *vfov, float *aspect);
 void ks_generated_destroy(ks_generated *g);
+/* A glTF 2.0 compound mesh asset (.gltf or .glb; CompoundMeshAsset::load_from_gltf,
+ * mesh_asset.cpp:551-1091) as a scene description: each glTF mesh a prototype (its primitives
+ * the meshes, with normals and texcoords; twosided), each node with a mesh of the default scene
+ * an instance under the node's world transform.  load_materials: each primitive's
+ * metallic-roughness material as a principled material with constant fields (emission from
+ * emissiveFactor x KHR_materials_emissive_strength, ior, specular, transmission extensions);
+ * otherwise every mesh has material 0 and the description no materials (the caller supplies
+ * them).  No camera (ks_generated_camera returns the default view).  KS_ERR_IO, or
+ * KS_ERR_UNSUPPORTED for textures, non-opaque alpha, sparse accessors, non-triangle primitives;
+ * the message is in ks_config_last_error(). */
+ks_status ks_compound_asset_load(const char *path, int32_t load_materials, ks_generated **out);
 
 #ifdef __cplusplus
 }

@@ -202,6 +202,7 @@ _sig("ks_procedural_scene", [ctypes.c_char_p, ctypes.c_uint64, ctypes.POINTER(Pr
 _sig("ks_generated_scene_desc", [_vp], ctypes.POINTER(SceneDesc))
 _sig("ks_generated_camera", [_vp, ctypes.POINTER(_f32), ctypes.POINTER(_f32), ctypes.POINTER(_f32)])
 _sig("ks_generated_destroy", [_vp], None)
+_sig("ks_compound_asset_load", [ctypes.c_char_p, ctypes.c_int32, ctypes.POINTER(_vp)])
 _sig("ks_small_pt_params_default", [ctypes.POINTER(SmallPTParams)], None)
 
 
@@ -247,6 +248,20 @@ class Generated:
         st = lib.ks_procedural_scene(kind.encode(), seed, ctypes.byref(o), ctypes.byref(h))
         if st != KS_OK:
             raise KsError(st, "ks_procedural_scene")
+        self._adopt(h)
+
+    @classmethod
+    def load_compound(cls, path, load_materials=True):
+        """A glTF compound mesh asset as a scene description (ks_compound_asset_load)."""
+        h = _vp()
+        st = lib.ks_compound_asset_load(str(path).encode(), int(load_materials), ctypes.byref(h))
+        if st != KS_OK:
+            raise KsError(st, lib.ks_config_last_error().decode())
+        g = cls.__new__(cls)
+        g._adopt(h)
+        return g
+
+    def _adopt(self, h):
         self.handle = h
         self.desc = lib.ks_generated_scene_desc(h)
         d = self.desc.contents
@@ -256,7 +271,11 @@ class Generated:
             self.meshes.append(dict(
                 vertices=_arr(md.vertices, 3 * md.n_vertices, np.float32).reshape(-1, 3),
                 indices=_arr(md.indices, 3 * md.n_triangles, np.uint32).reshape(-1, 3),
-                material=md.material, twosided=md.twosided))
+                normals=(_arr(md.vertex_normals, 3 * md.n_vertices, np.float32).reshape(-1, 3)
+                         if md.vertex_normals else None),
+                texcoords=(_arr(md.texcoords, 2 * md.n_vertices, np.float32).reshape(-1, 2)
+                           if md.texcoords else None),
+                material=md.material, twosided=md.twosided, smooth=md.use_smooth_normal))
         self.materials = [d.materials[k] for k in range(d.n_materials)]
         c2w = (_f32 * 16)()
         vfov, aspect = _f32(), _f32()

@@ -1,10 +1,18 @@
-// Host-only C-ABI entry points: camera matrices and procedural scenes.
+// Host-only C-ABI entry points: camera matrices, procedural scenes and loaded compound assets.
 #include "../../include/ks_b200.h"
+#include "gltf.h"
 #include "procedural.h"
 
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <new>
+#include <string>
+
+namespace ksb
+{
+void set_host_error(const std::string &msg); // task.cpp
+}
 
 namespace
 {
@@ -158,6 +166,53 @@ ks_status ks_generated_camera(const ks_generated *g, float camera_to_world[16], 
 }
 
 void ks_generated_destroy(ks_generated *g) { delete g; }
+
+ks_status ks_compound_asset_load(const char *path, int32_t load_materials, ks_generated **out)
+{
+    if (!path || !out)
+        return KS_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    auto g = std::make_unique<ks_generated>();
+    ksb::GeneratedScene &sc = g->scene;
+    try {
+        ksb::gltf::Compound c = ksb::gltf::load(path, load_materials != 0);
+        if (c.instances.empty())
+            throw ksb::gltf::Error(std::string(path) + ": the default scene instances no mesh");
+        for (const auto &p : c.prototypes) {
+            sc.prototypes.push_back({(uint32_t)sc.meshes.size(), (uint32_t)p.meshes.size()});
+            for (size_t k = 0; k < p.meshes.size(); ++k) {
+                const ksb::mesh::MeshData &md = p.meshes[k];
+                ksb::GeneratedMesh gm;
+                gm.vertices = md.vertices;
+                gm.indices = md.indices;
+                gm.normals = md.normals;
+                gm.texcoords = md.texcoords;
+                gm.twosided = md.twosided ? 1 : 0;
+                gm.use_smooth_normal = md.use_smooth_normal ? 1 : 0;
+                if (load_materials) {
+                    gm.material = (uint32_t)sc.materials.size();
+                    sc.materials.push_back(p.materials[k]);
+                }
+                sc.meshes.push_back(std::move(gm));
+            }
+        }
+        for (const auto &i : c.instances) {
+            ks_instance_desc d{};
+            d.prototype = i.prototype;
+            std::memcpy(d.to_world, i.to_world, sizeof(d.to_world));
+            sc.instances.push_back(d);
+        }
+    } catch (const ksb::gltf::Error &e) {
+        ksb::set_host_error(e.what());
+        return e.unsupported ? KS_ERR_UNSUPPORTED : KS_ERR_IO;
+    } catch (const std::exception &e) {
+        ksb::set_host_error(e.what());
+        return KS_ERR_IO;
+    }
+    sc.finalize();
+    *out = g.release();
+    return KS_OK;
+}
 
 void ks_small_pt_params_default(ks_small_pt_params *p)
 {

@@ -1,0 +1,770 @@
+// glTF 2.0 compound mesh assets: a JSON reader, the .glb container, buffers / buffer views /
+// accessors, meshes and primitives, the node hierarchy and constant metallic-roughness
+// materials, following the glTF 2.0 specification and the reference's use of it
+// (CompoundMeshAsset::load_from_gltf, mesh_asset.cpp:551-1091).
+#include "gltf.h"
+
+#include <algorithm>
+#include <array>
+#include <cctype>
+#include <cmath>
+#include <cstring>
+#include <fstream>
+#include <utility>
+
+namespace fs = std::filesystem;
+
+namespace ksb
+{
+namespace gltf
+{
+
+namespace
+{
+
+// ---- JSON --------------------------------------------------------------------------------------
+struct Json
+{
+    enum Kind
+    {
+        Null,
+        Bool,
+        Number,
+        String,
+        Array,
+        Object
+    } kind = Null;
+    bool b = false;
+    double num = 0.0;
+    std::string str;
+    std::vector<Json> arr;
+    std::vector<std::pair<std::string, Json>> obj;
+
+    const Json *get(const std::string &key) const
+    {
+        if (kind != Object)
+            return nullptr;
+        for (const auto &kv : obj)
+            if (kv.first == key)
+                return &kv.second;
+        return nullptr;
+    }
+    double number(const std::string &key, double dflt) const
+    {
+        const Json *v = get(key);
+        if (!v)
+            return dflt;
+        if (v->kind != Number)
+            throw Error("glTF: '" + key + "' is not a number");
+        return v->num;
+    }
+    long integer(const std::string &key, long dflt) const
+    {
+        const double d = number(key, (double)dflt);
+        if (d != std::floor(d))
+            throw Error("glTF: '" + key + "' is not an integer");
+        return (long)d;
+    }
+    std::string string(const std::string &key, const std::string &dflt) const
+    {
+        const Json *v = get(key);
+        if (!v)
+            return dflt;
+        if (v->kind != String)
+            throw Error("glTF: '" + key + "' is not a string");
+        return v->str;
+    }
+    const std::vector<Json> &array(const std::string &key) const
+    {
+        static const std::vector<Json> empty;
+        const Json *v = get(key);
+        if (!v)
+            return empty;
+        if (v->kind != Array)
+            throw Error("glTF: '" + key + "' is not an array");
+        return v->arr;
+    }
+    // numbers of an array member (empty when absent)
+    std::vector<double> numbers(const std::string &key) const
+    {
+        std::vector<double> out;
+        for (const Json &e : array(key)) {
+            if (e.kind != Number)
+                throw Error("glTF: '" + key + "' holds a non-number");
+            out.push_back(e.num);
+        }
+        return out;
+    }
+};
+
+struct JsonParser
+{
+    const char *p, *end;
+    int depth = 0;
+
+    [[noreturn]] void fail(const std::string &what) { throw Error("glTF: JSON " + what); }
+    void ws()
+    {
+        while (p < end && (*p == ' ' || *p == '\t' || *p == '\n' || *p == '\r'))
+            ++p;
+    }
+    bool lit(const char *s)
+    {
+        const size_t n = std::strlen(s);
+        if ((size_t)(end - p) >= n && std::memcmp(p, s, n) == 0) {
+            p += n;
+            return true;
+        }
+        return false;
+    }
+    static void utf8(std::string &out, uint32_t cp)
+    {
+        if (cp < 0x80) {
+            out += (char)cp;
+        } else if (cp < 0x800) {
+            out += (char)(0xc0 | (cp >> 6));
+            out += (char)(0x80 | (cp & 0x3f));
+        } else if (cp < 0x10000) {
+            out += (char)(0xe0 | (cp >> 12));
+            out += (char)(0x80 | ((cp >> 6) & 0x3f));
+            out += (char)(0x80 | (cp & 0x3f));
+        } else {
+            out += (char)(0xf0 | (cp >> 18));
+            out += (char)(0x80 | ((cp >> 12) & 0x3f));
+            out += (char)(0x80 | ((cp >> 6) & 0x3f));
+            out += (char)(0x80 | (cp & 0x3f));
+        }
+    }
+    uint32_t hex4()
+    {
+        if (end - p < 4)
+            fail("truncated \\u escape");
+        uint32_t v = 0;
+        for (int i = 0; i < 4; ++i) {
+            const char c = *p++;
+            v <<= 4;
+            if (c >= '0' && c <= '9')
+                v |= (uint32_t)(c - '0');
+            else if (c >= 'a' && c <= 'f')
+                v |= (uint32_t)(c - 'a' + 10);
+            else if (c >= 'A' && c <= 'F')
+                v |= (uint32_t)(c - 'A' + 10);
+            else
+                fail("bad \\u escape");
+        }
+        return v;
+    }
+    std::string string()
+    {
+        if (p >= end || *p != '"')
+            fail("expected a string");
+        ++p;
+        std::string s;
+        for (;;) {
+            if (p >= end)
+                fail("unterminated string");
+            const char c = *p++;
+            if (c == '"')
+                return s;
+            if (c != '\\') {
+                s += c;
+                continue;
+            }
+            if (p >= end)
+                fail("unterminated escape");
+            const char e = *p++;
+            switch (e) {
+            case '"':
+            case '\\':
+            case '/':
+                s += e;
+                break;
+            case 'b':
+                s += '\b';
+                break;
+            case 'f':
+                s += '\f';
+                break;
+            case 'n':
+                s += '\n';
+                break;
+            case 'r':
+                s += '\r';
+                break;
+            case 't':
+                s += '\t';
+                break;
+            case 'u': {
+                uint32_t cp = hex4();
+                if (cp >= 0xd800 && cp < 0xdc00 && end - p >= 6 && p[0] == '\\' && p[1] == 'u') {
+                    p += 2;
+                    const uint32_t lo = hex4();
+                    if (lo >= 0xdc00 && lo < 0xe000)
+                        cp = 0x10000 + ((cp - 0xd800) << 10) + (lo - 0xdc00);
+                }
+                utf8(s, cp);
+                break;
+            }
+            default:
+                fail("bad escape");
+            }
+        }
+    }
+    Json value()
+    {
+        if (++depth > 256)
+            fail("nested too deeply");
+        ws();
+        if (p >= end)
+            fail("unexpected end");
+        Json v;
+        if (*p == '{') {
+            ++p;
+            v.kind = Json::Object;
+            ws();
+            if (p < end && *p == '}') {
+                ++p;
+            } else {
+                for (;;) {
+                    ws();
+                    std::string k = string();
+                    ws();
+                    if (p >= end || *p != ':')
+                        fail("expected ':'");
+                    ++p;
+                    v.obj.emplace_back(std::move(k), value());
+                    ws();
+                    if (p < end && *p == ',') {
+                        ++p;
+                        continue;
+                    }
+                    if (p < end && *p == '}') {
+                        ++p;
+                        break;
+                    }
+                    fail("expected ',' or '}'");
+                }
+            }
+        } else if (*p == '[') {
+            ++p;
+            v.kind = Json::Array;
+            ws();
+            if (p < end && *p == ']') {
+                ++p;
+            } else {
+                for (;;) {
+                    v.arr.push_back(value());
+                    ws();
+                    if (p < end && *p == ',') {
+                        ++p;
+                        continue;
+                    }
+                    if (p < end && *p == ']') {
+                        ++p;
+                        break;
+                    }
+                    fail("expected ',' or ']'");
+                }
+            }
+        } else if (*p == '"') {
+            v.kind = Json::String;
+            v.str = string();
+        } else if (lit("true")) {
+            v.kind = Json::Bool;
+            v.b = true;
+        } else if (lit("false")) {
+            v.kind = Json::Bool;
+        } else if (lit("null")) {
+            v.kind = Json::Null;
+        } else {
+            const std::string tok(p, (size_t)std::min<ptrdiff_t>(end - p, 64));
+            char *stop = nullptr;
+            v.num = std::strtod(tok.c_str(), &stop);
+            if (stop == tok.c_str())
+                fail("unexpected character");
+            v.kind = Json::Number;
+            p += stop - tok.c_str();
+        }
+        --depth;
+        return v;
+    }
+};
+
+Json parse_json(const std::string &text)
+{
+    JsonParser jp{text.data(), text.data() + text.size()};
+    Json v = jp.value();
+    jp.ws();
+    if (jp.p != jp.end)
+        jp.fail("trailing characters");
+    return v;
+}
+
+// ---- files and buffers -------------------------------------------------------------------------
+std::string read_all(const fs::path &path)
+{
+    std::ifstream f(path, std::ios::binary);
+    if (!f)
+        throw Error("cannot open " + path.string());
+    return std::string((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+}
+
+std::string base64_decode(const std::string &s, size_t from)
+{
+    auto val = [](char c) -> int {
+        if (c >= 'A' && c <= 'Z')
+            return c - 'A';
+        if (c >= 'a' && c <= 'z')
+            return c - 'a' + 26;
+        if (c >= '0' && c <= '9')
+            return c - '0' + 52;
+        if (c == '+' || c == '-')
+            return 62;
+        if (c == '/' || c == '_')
+            return 63;
+        return -1;
+    };
+    std::string out;
+    uint32_t acc = 0;
+    int bits = 0;
+    for (size_t i = from; i < s.size(); ++i) {
+        const char c = s[i];
+        if (c == '=')
+            break;
+        const int v = val(c);
+        if (v < 0)
+            throw Error("glTF: bad base64 data URI");
+        acc = (acc << 6) | (uint32_t)v;
+        bits += 6;
+        if (bits >= 8) {
+            bits -= 8;
+            out += (char)((acc >> bits) & 0xff);
+        }
+    }
+    return out;
+}
+
+std::string uri_decode(const std::string &u)
+{
+    std::string out;
+    for (size_t i = 0; i < u.size(); ++i) {
+        if (u[i] == '%' && i + 2 < u.size() && std::isxdigit((unsigned char)u[i + 1]) &&
+            std::isxdigit((unsigned char)u[i + 2])) {
+            out += (char)std::stoi(u.substr(i + 1, 2), nullptr, 16);
+            i += 2;
+        } else {
+            out += u[i];
+        }
+    }
+    return out;
+}
+
+uint32_t le32(const std::string &s, size_t at)
+{
+    uint32_t v;
+    std::memcpy(&v, s.data() + at, 4);
+    return v;
+}
+
+struct Model
+{
+    Json doc;
+    std::vector<std::string> buffers;
+};
+
+Model load_model(const fs::path &path)
+{
+    Model m;
+    const std::string file = read_all(path);
+    std::string glb_bin;
+    bool have_bin = false;
+    if (file.size() >= 12 && le32(file, 0) == 0x46546c67u) { // "glTF": binary container
+        if (le32(file, 4) != 2)
+            throw Error(path.string() + ": glb version " + std::to_string(le32(file, 4)) + " is not supported", true);
+        const size_t length = std::min<size_t>(le32(file, 8), file.size());
+        size_t at = 12;
+        bool have_json = false;
+        while (at + 8 <= length) {
+            const uint32_t n = le32(file, at), type = le32(file, at + 4);
+            if (at + 8 + (size_t)n > length)
+                throw Error(path.string() + ": truncated glb chunk");
+            if (type == 0x4e4f534au && !have_json) { // JSON
+                m.doc = parse_json(file.substr(at + 8, n));
+                have_json = true;
+            } else if (type == 0x004e4942u && !have_bin) { // BIN
+                glb_bin = file.substr(at + 8, n);
+                have_bin = true;
+            }
+            at += 8 + (size_t)((n + 3) & ~3u);
+        }
+        if (!have_json)
+            throw Error(path.string() + ": glb without a JSON chunk");
+    } else {
+        m.doc = parse_json(file);
+    }
+    if (m.doc.kind != Json::Object)
+        throw Error(path.string() + ": not a glTF document");
+    const Json *asset = m.doc.get("asset");
+    const std::string version = asset ? asset->string("version", "") : "";
+    if (version.empty() || version[0] != '2')
+        throw Error(path.string() + ": glTF version '" + version + "' is not supported (2.x)", true);
+    const auto &bufs = m.doc.array("buffers");
+    for (size_t i = 0; i < bufs.size(); ++i) {
+        const Json &b = bufs[i];
+        const size_t len = (size_t)b.integer("byteLength", 0);
+        std::string data;
+        const Json *uri = b.get("uri");
+        if (!uri) {
+            if (i != 0 || !have_bin)
+                throw Error(path.string() + ": buffer " + std::to_string(i) + " has no data");
+            data = glb_bin;
+        } else {
+            const std::string u = b.string("uri", "");
+            if (u.rfind("data:", 0) == 0) {
+                const size_t comma = u.find(',');
+                if (comma == std::string::npos || u.substr(0, comma).find(";base64") == std::string::npos)
+                    throw Error(path.string() + ": only base64 data URIs are supported", true);
+                data = base64_decode(u, comma + 1);
+            } else {
+                data = read_all(path.parent_path() / uri_decode(u));
+            }
+        }
+        if (data.size() < len)
+            throw Error(path.string() + ": buffer " + std::to_string(i) + " is shorter than its byteLength");
+        m.buffers.push_back(std::move(data));
+    }
+    return m;
+}
+
+// ---- accessors ---------------------------------------------------------------------------------
+int component_bytes(long type)
+{
+    switch (type) {
+    case 5120:
+    case 5121:
+        return 1;
+    case 5122:
+    case 5123:
+        return 2;
+    case 5125:
+    case 5126:
+        return 4;
+    default:
+        throw Error("glTF: unknown accessor componentType " + std::to_string(type));
+    }
+}
+
+int type_components(const std::string &t)
+{
+    if (t == "SCALAR")
+        return 1;
+    if (t == "VEC2")
+        return 2;
+    if (t == "VEC3")
+        return 3;
+    if (t == "VEC4" || t == "MAT2")
+        return 4;
+    if (t == "MAT3")
+        return 9;
+    if (t == "MAT4")
+        return 16;
+    throw Error("glTF: unknown accessor type '" + t + "'");
+}
+
+// copy_accessor_to_linear (mesh_asset.cpp:312-329): the accessor's elements, packed.  An
+// accessor without a buffer view is all zeros (glTF 2.0, 3.6.2.3).
+std::string accessor_bytes(const Model &m, long index, long want_component, const std::string &want_type,
+                           size_t &count)
+{
+    const auto &accs = m.doc.array("accessors");
+    if (index < 0 || index >= (long)accs.size())
+        throw Error("glTF: accessor index out of range");
+    const Json &a = accs[(size_t)index];
+    if (a.get("sparse"))
+        throw Error("glTF: sparse accessors are not supported", true);
+    const long ct = a.integer("componentType", -1);
+    const std::string type = a.string("type", "");
+    if (ct != want_component || type != want_type)
+        throw Error("glTF: accessor " + std::to_string(index) + " is not of component type " +
+                        std::to_string(want_component) + " and type " + want_type,
+                    true);
+    const long cnt = a.integer("count", -1);
+    if (cnt < 0)
+        throw Error("glTF: accessor without a count");
+    count = (size_t)cnt;
+    const size_t elem = (size_t)component_bytes(ct) * (size_t)type_components(type);
+    std::string out(count * elem, '\0');
+    if (!a.get("bufferView"))
+        return out;
+    const auto &views = m.doc.array("bufferViews");
+    const long vi = a.integer("bufferView", -1);
+    if (vi < 0 || vi >= (long)views.size())
+        throw Error("glTF: buffer view index out of range");
+    const Json &v = views[(size_t)vi];
+    const long bi = v.integer("buffer", -1);
+    if (bi < 0 || bi >= (long)m.buffers.size())
+        throw Error("glTF: buffer index out of range");
+    const std::string &buf = m.buffers[(size_t)bi];
+    const size_t view_off = (size_t)v.integer("byteOffset", 0), view_len = (size_t)v.integer("byteLength", 0);
+    const size_t stride = v.get("byteStride") ? (size_t)v.integer("byteStride", 0) : elem;
+    const size_t off = (size_t)a.integer("byteOffset", 0);
+    if (view_off + view_len > buf.size() || stride < elem ||
+        (count > 0 && off + stride * (count - 1) + elem > view_len))
+        throw Error("glTF: accessor " + std::to_string(index) + " reaches past its buffer view");
+    for (size_t i = 0; i < count; ++i)
+        std::memcpy(&out[i * elem], buf.data() + view_off + off + i * stride, elem);
+    return out;
+}
+
+std::vector<float> floats(const Model &m, long index, const std::string &type, size_t &count)
+{
+    const std::string b = accessor_bytes(m, index, 5126, type, count);
+    std::vector<float> out(b.size() / 4);
+    std::memcpy(out.data(), b.data(), b.size());
+    return out;
+}
+
+std::vector<uint32_t> indices(const Model &m, long index)
+{
+    const auto &accs = m.doc.array("accessors");
+    if (index < 0 || index >= (long)accs.size())
+        throw Error("glTF: primitive without indices (non-indexed primitives are not supported)", true);
+    const long ct = accs[(size_t)index].integer("componentType", -1);
+    if (ct != 5125 && ct != 5123)
+        throw Error("glTF: index component type " + std::to_string(ct) + " is not supported", true);
+    size_t count = 0;
+    const std::string b = accessor_bytes(m, index, ct, "SCALAR", count);
+    std::vector<uint32_t> out(count);
+    for (size_t i = 0; i < count; ++i) {
+        if (ct == 5125) {
+            std::memcpy(&out[i], &b[4 * i], 4);
+        } else {
+            uint16_t s;
+            std::memcpy(&s, &b[2 * i], 2);
+            out[i] = s;
+        }
+    }
+    if (count % 3)
+        throw Error("glTF: index count is not a multiple of 3");
+    return out;
+}
+
+// ---- materials ---------------------------------------------------------------------------------
+bool has_texture(const Json *o, const char *key) { return o && o->get(key); }
+
+// The metallic-roughness material as a principled BSDF with constant fields (mesh_asset.cpp:672-
+// 940): basecolor, roughness, metallic; emissive = KHR_materials_emissive_strength x
+// emissiveFactor, an emitter when both are positive; ior (KHR_materials_ior, 1.5); specular_r0_mul
+// (KHR_materials_specular: specularFactor x mean(specularColorFactor), 0.5 without it);
+// specular_trans (KHR_materials_transmission, which also makes the mesh one-sided); no diffuse
+// transmission; GGX.
+ks_material_desc material(const Json &src, const std::string &where, bool &twosided)
+{
+    ks_material_desc d{};
+    const Json *pbr = src.get("pbrMetallicRoughness");
+    if (has_texture(pbr, "baseColorTexture") || has_texture(pbr, "metallicRoughnessTexture") ||
+        src.get("emissiveTexture") || src.get("normalTexture"))
+        throw Error(where + ": textured materials are not supported (constant fields only)", true);
+    if (src.string("alphaMode", "OPAQUE") != "OPAQUE")
+        throw Error(where + ": alpha modes other than OPAQUE (opacity maps) are not supported", true);
+    std::vector<double> bc = pbr ? pbr->numbers("baseColorFactor") : std::vector<double>{};
+    if (bc.empty())
+        bc = {1.0, 1.0, 1.0, 1.0};
+    if (bc.size() != 4)
+        throw Error(where + ": baseColorFactor needs 4 numbers");
+    for (int c = 0; c < 3; ++c)
+        d.basecolor[c] = (float)bc[c];
+    d.roughness = pbr ? (float)pbr->number("roughnessFactor", 1.0) : 1.0f;
+    d.metallic = pbr ? (float)pbr->number("metallicFactor", 1.0) : 1.0f;
+    const Json *ext = src.get("extensions");
+    auto extension = [&](const char *name) { return ext ? ext->get(name) : nullptr; };
+    float strength = 1.0f;
+    if (const Json *e = extension("KHR_materials_emissive_strength"))
+        strength = (float)e->number("emissiveStrength", 1.0);
+    std::vector<double> ef = src.numbers("emissiveFactor");
+    if (ef.empty())
+        ef = {0.0, 0.0, 0.0};
+    if (ef.size() != 3)
+        throw Error(where + ": emissiveFactor needs 3 numbers");
+    for (int c = 0; c < 3; ++c)
+        d.emissive[c] = strength * (float)ef[c];
+    if (strength > 0.0f && (ef[0] > 0.0 || ef[1] > 0.0 || ef[2] > 0.0)) {
+        d.has_emission = 1;
+        for (int c = 0; c < 3; ++c)
+            d.emission[c] = d.emissive[c];
+    }
+    d.ior = 1.5f;
+    if (const Json *e = extension("KHR_materials_ior"))
+        d.ior = (float)e->number("ior", 1.5);
+    d.specular_r0_mul = 0.5f;
+    if (const Json *e = extension("KHR_materials_specular")) {
+        if (e->get("specularTexture") || e->get("specularColorTexture"))
+            throw Error(where + ": textured specular is not supported", true);
+        const std::vector<double> scf = e->numbers("specularColorFactor");
+        if (e->get("specularFactor") || !scf.empty()) {
+            float sf = (float)e->number("specularFactor", 1.0);
+            if (scf.size() == 3)
+                sf *= (float)((scf[0] + scf[1] + scf[2]) / 3.0);
+            d.specular_r0_mul = sf;
+        }
+    }
+    if (const Json *e = extension("KHR_materials_transmission")) {
+        if (e->get("transmissionTexture"))
+            throw Error(where + ": textured transmission is not supported", true);
+        twosided = false;
+        d.specular_trans = (float)e->number("transmissionFactor", 0.0);
+    }
+    d.diffuse_trans = 0.0f;
+    d.diffuse_trans_fwd = 0.0f;
+    d.microfacet = 0;
+    return d;
+}
+
+// ---- node transforms ---------------------------------------------------------------------------
+using Mat4 = std::array<double, 16>; // row-major
+
+Mat4 mul(const Mat4 &a, const Mat4 &b)
+{
+    Mat4 c{};
+    for (int r = 0; r < 4; ++r)
+        for (int k = 0; k < 4; ++k)
+            for (int j = 0; j < 4; ++j)
+                c[4 * r + j] += a[4 * r + k] * b[4 * k + j];
+    return c;
+}
+
+// A node's local transform: its column-major `matrix`, else T * R * S of its translation,
+// rotation (x, y, z, w) and scale (traverse_gltf_scene_graph, mesh_asset.cpp:466-498).
+Mat4 local_transform(const Json &node)
+{
+    const std::vector<double> mat = node.numbers("matrix");
+    Mat4 m{};
+    if (!mat.empty()) {
+        if (mat.size() != 16)
+            throw Error("glTF: node matrix needs 16 numbers");
+        for (int r = 0; r < 4; ++r)
+            for (int c = 0; c < 4; ++c)
+                m[4 * r + c] = mat[4 * c + r];
+        return m;
+    }
+    std::vector<double> s = node.numbers("scale"), q = node.numbers("rotation"), t = node.numbers("translation");
+    if (s.empty())
+        s = {1, 1, 1};
+    if (q.empty())
+        q = {0, 0, 0, 1};
+    if (t.empty())
+        t = {0, 0, 0};
+    if (s.size() != 3 || q.size() != 4 || t.size() != 3)
+        throw Error("glTF: bad node scale / rotation / translation");
+    // rotation matrix of the quaternion (taken as given, like Eigen's toRotationMatrix)
+    const double x = q[0], y = q[1], z = q[2], w = q[3];
+    const double R[9] = {1 - 2 * (y * y + z * z), 2 * (x * y - w * z),     2 * (x * z + w * y),
+                         2 * (x * y + w * z),     1 - 2 * (x * x + z * z), 2 * (y * z - w * x),
+                         2 * (x * z - w * y),     2 * (y * z + w * x),     1 - 2 * (x * x + y * y)};
+    for (int r = 0; r < 3; ++r) {
+        for (int c = 0; c < 3; ++c)
+            m[4 * r + c] = R[3 * r + c] * s[c];
+        m[4 * r + 3] = t[r];
+    }
+    m[15] = 1.0;
+    return m;
+}
+
+} // namespace
+
+Compound load(const fs::path &path, bool load_materials)
+{
+    Model m = load_model(path);
+    Compound out;
+    const auto &meshes = m.doc.array("meshes");
+    const auto &mats = m.doc.array("materials");
+    for (size_t i = 0; i < meshes.size(); ++i) {
+        Prototype proto;
+        const auto &prims = meshes[i].array("primitives");
+        for (size_t j = 0; j < prims.size(); ++j) {
+            const Json &pr = prims[j];
+            const std::string where = path.string() + ": mesh " + std::to_string(i) + " primitive " + std::to_string(j);
+            if (pr.integer("mode", 4) != 4)
+                throw Error(where + ": only triangle primitives are supported", true);
+            const Json *attrs = pr.get("attributes");
+            if (!attrs || !attrs->get("POSITION"))
+                throw Error(where + ": primitive without positions");
+            mesh::MeshData md;
+            size_t nv = 0, n = 0;
+            md.vertices = floats(m, attrs->integer("POSITION", -1), "VEC3", nv);
+            md.indices = indices(m, pr.integer("indices", -1));
+            for (uint32_t k : md.indices)
+                if (k >= nv)
+                    throw Error(where + ": vertex index out of range");
+            if (attrs->get("NORMAL")) {
+                md.normals = floats(m, attrs->integer("NORMAL", -1), "VEC3", n);
+                if (n != nv)
+                    throw Error(where + ": NORMAL count differs from POSITION count");
+            }
+            if (attrs->get("TEXCOORD_0")) {
+                md.texcoords = floats(m, attrs->integer("TEXCOORD_0", -1), "VEC2", n);
+                if (n != nv)
+                    throw Error(where + ": TEXCOORD_0 count differs from POSITION count");
+            }
+            md.twosided = true;
+            md.use_smooth_normal = true;
+            md.name = meshes[i].string("name", "");
+            if (load_materials) {
+                const long mi = pr.integer("material", -1);
+                if (mi < 0 || mi >= (long)mats.size())
+                    throw Error(where + ": primitive without a material", true);
+                proto.materials.push_back(material(mats[(size_t)mi], where, md.twosided));
+            }
+            proto.meshes.push_back(std::move(md));
+        }
+        if (proto.meshes.empty())
+            throw Error(path.string() + ": mesh " + std::to_string(i) + " has no primitives");
+        out.prototypes.push_back(std::move(proto));
+    }
+    // the default scene's node trees, depth first, world = parent x local
+    const auto &nodes = m.doc.array("nodes");
+    const auto &scenes = m.doc.array("scenes");
+    if (scenes.empty())
+        return out;
+    const long si = m.doc.integer("scene", 0);
+    if (si < 0 || si >= (long)scenes.size())
+        throw Error(path.string() + ": scene index out of range");
+    std::vector<int> on_path(nodes.size(), 0);
+    auto dfs = [&](long ni, const Mat4 &parent, auto &self) -> void {
+        if (ni < 0 || ni >= (long)nodes.size())
+            throw Error(path.string() + ": node index out of range");
+        if (on_path[(size_t)ni])
+            throw Error(path.string() + ": the node graph has a cycle");
+        on_path[(size_t)ni] = 1;
+        const Json &node = nodes[(size_t)ni];
+        const Mat4 world = mul(parent, local_transform(node));
+        if (node.get("mesh")) {
+            const long mi = node.integer("mesh", -1);
+            if (mi < 0 || mi >= (long)out.prototypes.size())
+                throw Error(path.string() + ": node mesh index out of range");
+            Instance inst;
+            inst.prototype = (uint32_t)mi;
+            for (int r = 0; r < 3; ++r)
+                for (int c = 0; c < 4; ++c)
+                    inst.to_world[4 * r + c] = (float)world[4 * r + c];
+            out.instances.push_back(inst);
+        }
+        for (const Json &c : node.array("children")) {
+            if (c.kind != Json::Number)
+                throw Error(path.string() + ": bad child index");
+            self((long)c.num, world, self);
+        }
+        on_path[(size_t)ni] = 0;
+    };
+    Mat4 id{};
+    id[0] = id[5] = id[10] = id[15] = 1.0;
+    for (const Json &root : scenes[(size_t)si].array("nodes")) {
+        if (root.kind != Json::Number)
+            throw Error(path.string() + ": bad scene node index");
+        dfs((long)root.num, id, dfs);
+    }
+    return out;
+}
+
+} // namespace gltf
+} // namespace ksb

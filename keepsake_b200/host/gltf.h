@@ -1,0 +1,53 @@
+// glTF 2.0 compound mesh assets (CompoundMeshAsset::load_from_gltf, mesh_asset.cpp:551-1091;
+// create_compound_mesh_asset, mesh_asset.cpp:1114-1132): each glTF mesh a prototype whose
+// primitives are its meshes, each node with a mesh an instance under the node's world transform
+// (traverse_gltf_scene_graph, mesh_asset.cpp:466-520), and, with load_materials, the
+// primitives' metallic-roughness materials as principled BSDFs with constant fields.
+//
+// .gltf (JSON, buffers in files next to it or in base64 data URIs) and .glb (binary container).
+// Not handled, each an error marked unsupported: textures (textured shader fields), alpha modes
+// other than OPAQUE (opacity maps), sparse accessors, non-triangle primitives, index types other
+// than unsigned short / unsigned int (the reference asserts on those too).  Animations are not
+// read (camera and transform animation are outside the small_pt path).
+#pragma once
+#include "../../include/ks_b200.h"
+#include "mesh_io.h"
+
+#include <filesystem>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace ksb
+{
+namespace gltf
+{
+
+struct Error : std::runtime_error
+{
+    bool unsupported;
+    Error(const std::string &what, bool unsupported = false) : std::runtime_error(what), unsupported(unsupported) {}
+};
+
+struct Prototype
+{
+    std::vector<mesh::MeshData> meshes;        // one per primitive
+    std::vector<ks_material_desc> materials;   // one per primitive (load_materials), else empty
+};
+
+struct Instance
+{
+    uint32_t prototype;
+    float to_world[12]; // row-major 3x4
+};
+
+struct Compound
+{
+    std::vector<Prototype> prototypes;
+    std::vector<Instance> instances;
+};
+
+Compound load(const std::filesystem::path &path, bool load_materials);
+
+} // namespace gltf
+} // namespace ksb

@@ -507,11 +507,11 @@ void GeneratedScene::finalize()
         d.n_vertices = (uint32_t)meshes[i].vertices.size() / 3;
         d.indices = meshes[i].indices.data();
         d.n_triangles = (uint32_t)meshes[i].indices.size() / 3;
-        d.vertex_normals = nullptr;
-        d.texcoords = nullptr;
+        d.vertex_normals = meshes[i].normals.empty() ? nullptr : meshes[i].normals.data();
+        d.texcoords = meshes[i].texcoords.empty() ? nullptr : meshes[i].texcoords.data();
         d.material = meshes[i].material;
-        d.twosided = 1;
-        d.use_smooth_normal = 1;
+        d.twosided = meshes[i].twosided;
+        d.use_smooth_normal = meshes[i].use_smooth_normal;
     }
     desc.meshes = mesh_descs.data();
     desc.n_meshes = (uint32_t)mesh_descs.size();

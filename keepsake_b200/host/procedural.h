@@ -33,6 +33,10 @@ struct GeneratedMesh
     std::vector<float> vertices;
     std::vector<uint32_t> indices;
     uint32_t material = 0;
+    std::vector<float> normals;   // 3 per vertex or empty (loaded assets)
+    std::vector<float> texcoords; // 2 per vertex or empty
+    int twosided = 1;
+    int use_smooth_normal = 1;
 };
 
 struct GeneratedScene

@@ -11,10 +11,12 @@
 //   create_camera / look_at            camera.cpp:12-31,172-205
 //   load_transform_field               config.cpp:204-260
 //   create_mesh_asset                  mesh_asset.cpp:243-266 (obj / bin formats, to_world)
+//   create_compound_mesh_asset         mesh_asset.cpp:1114-1132 (glTF: prototypes + instances)
 //   convert_mesh_asset task            mesh_asset.cpp:301-311
 //   composite_and_save_to_exr          render_target.cpp:181-208 (interval images)
 #include "../../include/ks_b200.h"
 #include "../../include/ks_b200_task.hpp"
+#include "gltf.h"
 #include "image_io.h"
 #include "mesh_io.h"
 #include "procedural.h"
@@ -74,6 +76,9 @@ struct MeshAsset
     std::vector<ks_material_desc> materials; // procedural assets bring their own
     std::vector<float> sky_map;              // procedural assets: their sky
     ks_sky_desc sky{};
+    // compound (glTF) assets: prototypes as runs of geometries, and their instances
+    std::vector<ks_prototype_desc> prototypes;
+    std::vector<ks_instance_desc> instances;
 };
 
 } // namespace
@@ -89,6 +94,7 @@ struct ConfigServiceImpl
 
     const Value *find_asset(const std::string &path) const;
     std::shared_ptr<MeshAsset> mesh_asset(const std::string &path);
+    std::shared_ptr<MeshAsset> compound_asset(const std::string &path);
     ks_material_desc material(const std::string &path);
 };
 
@@ -458,6 +464,56 @@ std::shared_ptr<MeshAsset> ConfigServiceImpl::mesh_asset(const std::string &path
     return m;
 }
 
+// create_compound_mesh_asset (mesh_asset.cpp:1114-1132): a glTF file ("format" glb | gltf) as
+// prototypes (its meshes) and instances (its nodes), with its materials when load_materials.
+std::shared_ptr<MeshAsset> ConfigServiceImpl::compound_asset(const std::string &path)
+{
+    auto it = meshes.find(path);
+    if (it != meshes.end())
+        return it->second;
+    const Value *node = find_asset(path);
+    if (!node || path.rfind("compound_mesh_asset.", 0) != 0)
+        throw ParseError("config: unknown compound mesh asset '" + path + "'");
+    ConfigArgs a = args_of(this, node, path);
+    const std::string fmt = a.load_string("format", "glb");
+    if (fmt != "glb" && fmt != "gltf")
+        throw StatusError(KS_ERR_UNSUPPORTED, "config: unsupported compound mesh asset format '" + fmt + "'");
+    if (a.load_string("bsdf_type", "principled_bsdf") != "principled_bsdf")
+        throw StatusError(KS_ERR_UNSUPPORTED, "config: only principled_bsdf materials are supported");
+    const bool load_materials = a.load_bool("load_materials", false);
+    ksb::gltf::Compound c;
+    try {
+        c = ksb::gltf::load(a.load_path("path"), load_materials);
+    } catch (const ksb::gltf::Error &e) {
+        if (e.unsupported)
+            throw StatusError(KS_ERR_UNSUPPORTED, std::string("config: ") + e.what());
+        throw IoError(e.what());
+    }
+    if (c.instances.empty())
+        throw ParseError("config: compound mesh asset '" + path + "' instances no mesh");
+    auto m = std::make_shared<MeshAsset>();
+    for (auto &p : c.prototypes) {
+        m->prototypes.push_back({(uint32_t)m->geometries.size(), (uint32_t)p.meshes.size()});
+        for (size_t k = 0; k < p.meshes.size(); ++k) {
+            std::vector<ksb::mesh::MeshData> one(1);
+            one[0] = std::move(p.meshes[k]);
+            add_meshes(std::move(one), *m);
+            if (load_materials) {
+                m->geometries.back().own_material = (int)m->materials.size();
+                m->materials.push_back(p.materials[k]);
+            }
+        }
+    }
+    for (const auto &i : c.instances) {
+        ks_instance_desc d{};
+        d.prototype = i.prototype;
+        std::memcpy(d.to_world, i.to_world, sizeof(d.to_world));
+        m->instances.push_back(d);
+    }
+    meshes[path] = m;
+    return m;
+}
+
 ks_material_desc ConfigServiceImpl::material(const std::string &path)
 {
     auto it = materials.find(path);
@@ -617,25 +673,34 @@ void small_pt_b200(const ConfigArgs &args, const fs::path &task_dir, int task_id
     (void)task_id;
     ConfigServiceImpl *svc = args.internal->service;
     // ---- scene (create_scene, scene.cpp:345-365) ----
-    if (args.contains("compound_object"))
-        throw StatusError(KS_ERR_UNSUPPORTED, "config: compound_object is not supported");
-    std::shared_ptr<MeshAsset> asset = svc->mesh_asset(args.load_string("object"));
+    const bool compound = !args.contains("object") && args.contains("compound_object");
+    std::shared_ptr<MeshAsset> asset = compound ? svc->compound_asset(args.load_string("compound_object"))
+                                                : svc->mesh_asset(args.load_string("object"));
+    // subscenes: one per mesh asset, one per prototype of a compound asset
+    std::vector<ks_prototype_desc> subscenes = asset->prototypes;
+    if (!compound)
+        subscenes = {ks_prototype_desc{0, (uint32_t)asset->geometries.size()}};
     std::vector<ks_material_desc> mats;
     std::vector<uint32_t> geom_mat(asset->geometries.size());
     if (args.contains("material")) {
-        // one list per subscene (one subscene per mesh asset), one material per geometry
+        // assign_material_list (mesh_asset.cpp:286-299): one list per subscene, one material per
+        // geometry
         ConfigArgs lists = args["material"];
-        if (lists.array_size() != 1 || lists[0].array_size() != (int)asset->geometries.size())
+        if (lists.array_size() != (int)subscenes.size())
             throw ParseError("config: material list mismatch dimension");
         std::map<std::string, uint32_t> index;
-        for (int g = 0; g < (int)asset->geometries.size(); ++g) {
-            std::string name = lists[0].load_string(g);
-            auto it = index.find(name);
-            if (it == index.end()) {
-                it = index.emplace(name, (uint32_t)mats.size()).first;
-                mats.push_back(svc->material(name));
+        for (int sub = 0; sub < (int)subscenes.size(); ++sub) {
+            if (lists[sub].array_size() != (int)subscenes[sub].n_meshes)
+                throw ParseError("config: material list mismatch dimension");
+            for (int k = 0; k < (int)subscenes[sub].n_meshes; ++k) {
+                std::string name = lists[sub].load_string(k);
+                auto it = index.find(name);
+                if (it == index.end()) {
+                    it = index.emplace(name, (uint32_t)mats.size()).first;
+                    mats.push_back(svc->material(name));
+                }
+                geom_mat[subscenes[sub].first_mesh + k] = it->second;
             }
-            geom_mat[g] = it->second;
         }
     } else {
         for (size_t g = 0; g < asset->geometries.size(); ++g) {
@@ -663,6 +728,12 @@ void small_pt_b200(const ConfigArgs &args, const fs::path &task_dir, int task_id
     desc.n_meshes = (uint32_t)meshes.size();
     desc.materials = mats.data();
     desc.n_materials = (uint32_t)mats.size();
+    if (compound) {
+        desc.prototypes = asset->prototypes.data();
+        desc.n_prototypes = (uint32_t)asset->prototypes.size();
+        desc.instances = asset->instances.data();
+        desc.n_instances = (uint32_t)asset->instances.size();
+    }
     // ---- sky (create_sky_light, light.cpp:257-275) ----
     std::vector<float> sky_map;
     if (args.contains("sky")) {
@@ -891,6 +962,12 @@ namespace
 {
 thread_local std::string g_config_error;
 }
+
+namespace ksb
+{
+// The message ks_config_last_error() returns, for the other host-side entry points.
+void set_host_error(const std::string &msg) { g_config_error = msg; }
+} // namespace ksb
 
 extern "C" {
 
