@@ -390,7 +390,8 @@ ks_status ks_small_pt_render_guided_device(ks_scene *scene, const ks_camera_desc
  * [mesh_asset.X] with a `path` and `format` "obj" (positions, texcoords, normals; twosided,
  * use_smooth_normal) or "bin" (keepsake's binary mesh asset), optional `to_world`
  * (create_mesh_asset, mesh_asset.cpp:243-266), or of `type` "inline" (geometry list) or
- * "procedural" (kind box_room | icosphere); sky maps from .exr, .hdr or .pfm files.  Returns
+ * "procedural" (kind box_room | icosphere); [compound_mesh_asset.X] glTF files for the task's
+ * `compound_object` (see ks_compound_asset_load); sky maps from .exr, .hdr or .pfm files.  Returns
  * KS_ERR_PARSE, KS_ERR_IO or KS_ERR_UNSUPPORTED with a message in ks_config_last_error().
  * C++ hosts can use the ConfigTask-shaped API of ks_b200_task.hpp instead.
  * ------------------------------------------------------------------------------------------- */

@@ -16,7 +16,10 @@
  *   binary mesh asset format (mesh_asset.cpp:180-240, 301-311).
  * Mesh assets: `path` + `format` "obj" (twosided, default false; use_smooth_normal, default true;
  * positions, texcoords and normals) or "bin", with an optional `to_world` transform
- * (create_mesh_asset, mesh_asset.cpp:243-266).
+ * (create_mesh_asset, mesh_asset.cpp:243-266).  Compound mesh assets
+ * ([compound_mesh_asset.NAME], the task's `compound_object`): a glTF 2.0 file (`format` "glb" or
+ * "gltf"; `load_materials` for its constant metallic-roughness materials), prototypes per glTF
+ * mesh and instances per node (create_compound_mesh_asset, mesh_asset.cpp:1114-1132).
  * Errors throw std::runtime_error (the reference asserts); the C entry point ks_config_run in
  * ks_b200.h returns a status instead.
  */
