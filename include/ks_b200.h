@@ -226,7 +226,13 @@ typedef struct ks_small_pt_params {
     float clamp_direct;   /* default 0 (off) */
     float clamp_indirect; /* default 10 */
     int32_t spp_prog_interval; /* default 32 */
-    float pixel_filter_width;  /* box filter width (BoxPixelFilter, render_target.h:108-125); default 1 */
+    float pixel_filter_width;  /* filter width; default 1 (box).  The task's defaults for the
+                                  Gaussian and Blackman-Harris filters are 3 (render_target.cpp:28-44) */
+    int32_t pixel_filter;      /* 0 box (BoxPixelFilter), 1 Gaussian, 2 Blackman-Harris
+                                  (render_target.h:108-180): camera samples are drawn from the
+                                  filter's tabulated distribution (PixelFilterSampleTable,
+                                  render_target.h:79-106) with weight 1; default 0 */
+    float pixel_filter_sigma;  /* Gaussian sigma; default 0.5 */
 } ks_small_pt_params;
 
 /* Fills the defaults of SmallPTInput (small_pt.h:17-39) and the task (small_pt.cpp:224-241). */

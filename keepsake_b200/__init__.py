@@ -169,7 +169,7 @@ class SmallPTParams(ctypes.Structure):
                 ("render_height", _i32), ("crop_start_x", _i32), ("crop_start_y", _i32), ("crop_width", _i32),
                 ("crop_height", _i32), ("spp", _i32), ("rng_seed", _i32), ("scale_ray_diff", _i32),
                 ("clamp_direct", _f32), ("clamp_indirect", _f32), ("spp_prog_interval", _i32),
-                ("pixel_filter_width", _f32)]
+                ("pixel_filter_width", _f32), ("pixel_filter", _i32), ("pixel_filter_sigma", _f32)]
 
     @classmethod
     def make(cls, **kw):

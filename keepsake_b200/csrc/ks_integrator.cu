@@ -24,6 +24,7 @@
 #include "ks_wavefront.cuh"
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <type_traits>
 #include <vector>
@@ -68,8 +69,10 @@ constexpr uint32_t kCounters = 6;
 
 // ---- kernels --------------------------------------------------------------------------------
 
-// Camera sample s of pixel (px, py) into path slot `slot`: Sobol box-filter offset, ray through
-// the projection (Camera::spawn_ray, camera.cpp:129-170; film position small_pt.cpp:50-54).
+// Camera sample s of pixel (px, py) into path slot `slot`: Sobol pixel-filter offset (box: uniform
+// over [-r, r]^2; Gaussian / Blackman-Harris: PixelFilterSampleTable::sample, render_target.h:94-101,
+// through the tabulated DistribTable2D's sample_linear, distrib.cpp:74-86), ray through the
+// projection (Camera::spawn_ray, camera.cpp:129-170; film position small_pt.cpp:50-54).
 // pix_word is the pixel index (with the job id in its upper bits for batched renders).
 KS_D void camera_path(const RenderParams &rp, int px, int py, int s, uint32_t pix_word, PathBuf &pb, uint32_t slot)
 {
@@ -79,6 +82,14 @@ KS_D void camera_path(const RenderParams &rp, int px, int py, int s, uint32_t pi
     if (rp.spp != 1) {
         float u0, u1;
         smp.next2d(u0, u1);
+        if (rp.filter_n) {
+            const uint32_t n = rp.filter_n;
+            float pdf_m, pdf_c;
+            uint32_t vi, ui;
+            const float vs = distrib_sample_linear(rp.filter_cdf + (size_t)n * (n + 1), n, u1, pdf_m, vi);
+            u0 = distrib_sample_linear(rp.filter_cdf + (size_t)vi * (n + 1), n, u0, pdf_c, ui);
+            u1 = vs;
+        }
         offx = (1.0f - u0) * -rp.filter_r + u0 * rp.filter_r;
         offy = (1.0f - u1) * -rp.filter_r + u1 * rp.filter_r;
     }
@@ -666,6 +677,7 @@ struct RenderWork
     DevBuf<uint32_t> counters; // [next, shadow, hit queue, miss queue, extension fetch, shadow fetch]
     DevBuf<uint32_t> queue[2]; // hit / miss path indices
     DevBuf<int> overflow;
+    DevBuf<float> filter; // the pixel filter's sample table (Gaussian / Blackman-Harris)
     uint32_t capacity = 0;
 };
 
@@ -715,6 +727,84 @@ struct CacheLease
 };
 
 // RenderParams of one render (SmallPTInput fields + camera); false for an empty crop window.
+// DistribTable (distrib.cpp:9-30): the normalised CDF of n values, appended to `out`; returns
+// their integral (acc).
+static float append_cdf(const float *f, uint32_t n, std::vector<float> &out)
+{
+    const size_t base = out.size();
+    out.resize(base + n + 1);
+    float *cdf = &out[base];
+    cdf[0] = 0;
+    const float invn = 1.0f / (float)n;
+    for (uint32_t i = 1; i < n + 1; ++i)
+        cdf[i] = cdf[i - 1] + f[i - 1] * invn;
+    const float acc = cdf[n];
+    if (acc == 0.0f) {
+        for (uint32_t i = 0; i < n + 1; ++i)
+            cdf[i] = (float)i / (float)n;
+    } else {
+        const float invacc = 1.0f / acc;
+        for (uint32_t i = 0; i < n + 1; ++i)
+            cdf[i] *= invacc;
+    }
+    cdf[n] = 1.0f;
+    return acc;
+}
+
+// PixelFilterSampleTable (render_target.h:79-92) of a Gaussian (1) or Blackman-Harris (2) filter of
+// radius r: the filter at the centres of an n x n grid over [-r, r]^2, n = ceil(32 r), as a
+// DistribTable2D (distrib.cpp:61-72): the n conditional CDFs (n + 1 floats each), then the
+// marginal one.  The filters as GaussianPixelFilter / BlackmanHarrisPixelFilter evaluate them
+// (render_target.h:127-180, gaussian() maths.h:1070-1073), in float.
+static std::vector<float> filter_table(int type, float r, float sigma, uint32_t &n_out)
+{
+    constexpr float pi = 3.14159265359f, two_pi = 6.28318530718f;
+    auto gaussian = [&](float x) {
+        return 1.0f / std::sqrt(two_pi * sigma * sigma) * std::exp(-((x - 0.0f) * (x - 0.0f)) / (2.0f * sigma * sigma));
+    };
+    const float threshold = type == 1 ? gaussian(r) : 0.0f;
+    auto eval = [&](float x, float y) {
+        if (x < -r || x > r || y < -r || y > r)
+            return 0.0f;
+        if (type == 1)
+            return (gaussian(x) - threshold) * (gaussian(y) - threshold);
+        constexpr float a0 = 0.35875f, a1 = 0.48829f, a2 = 0.14128f, a3 = 0.01168f;
+        const float tx = (x + r) / (2.0f * r);
+        const float fx = a0 - a1 * std::cos(2.0f * pi * tx) + a2 * std::cos(4.0f * pi * tx) - a3 * std::cos(6.0f * pi * tx);
+        const float ty = (y + r) / (2.0f * r);
+        const float fy = a0 - a1 * std::cos(2.0f * pi * ty) + a2 * std::cos(4.0f * pi * ty) - a3 * std::cos(6.0f * pi * ty);
+        return fx * fy;
+    };
+    const uint32_t n = (uint32_t)(int)std::ceil(32 * r);
+    std::vector<float> f((size_t)n * n);
+    for (uint32_t y = 0; y < n; ++y)
+        for (uint32_t x = 0; x < n; ++x)
+            f[(size_t)y * n + x] = eval(std::lerp(-r, r, (x + 0.5f) / n), std::lerp(-r, r, (y + 0.5f) / n));
+    std::vector<float> out, margin(n);
+    out.reserve((size_t)(n + 1) * (n + 1));
+    for (uint32_t y = 0; y < n; ++y)
+        margin[y] = append_cdf(&f[(size_t)y * n], n, out);
+    append_cdf(margin.data(), n, out);
+    n_out = n;
+    return out;
+}
+
+// The pixel filter of the parameters: false for bad values (unknown type, width <= 0, a table
+// of more than 256 x 256 cells, a Gaussian sigma <= 0).
+static bool pixel_filter_table(const ks_small_pt_params *in, std::vector<float> &table, uint32_t &n)
+{
+    table.clear();
+    n = 0;
+    const float width = in->pixel_filter_width > 0.0f ? in->pixel_filter_width : 1.0f;
+    if (in->pixel_filter == 0)
+        return true;
+    if (in->pixel_filter < 0 || in->pixel_filter > 2 || !(width <= 16.0f) ||
+        (in->pixel_filter == 1 && !(in->pixel_filter_sigma > 0.0f)))
+        return false;
+    table = filter_table(in->pixel_filter, 0.5f * width, in->pixel_filter_sigma, n);
+    return true;
+}
+
 static bool fill_params(const ks_camera_desc *cam, const ks_small_pt_params *in, RenderParams &rp)
 {
     const int W = in->render_width, H = in->render_height;
@@ -781,6 +871,9 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
     RenderParams rp{};
     if (!fill_params(cam, in, rp))
         return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_small_pt_render: empty crop window");
+    std::vector<float> ftab;
+    if (!pixel_filter_table(in, ftab, rp.filter_n))
+        return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_small_pt_render: bad pixel filter");
 
     SceneView sv = make_view(scene);
     const bool attribs = sv.normals != nullptr || sv.texcoords != nullptr;
@@ -798,6 +891,12 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
     if (scene->n_instances)
         KS_CUDA_TRY(ctx, w.hit_inst.reserve(w.capacity));
     KS_CUDA_TRY(ctx, w.samples.reserve(4 * (size_t)w.capacity));
+    if (rp.filter_n) {
+        KS_CUDA_TRY(ctx, w.filter.reserve(ftab.size()));
+        KS_CUDA_TRY(ctx, cudaMemcpyAsync(w.filter.ptr, ftab.data(), sizeof(float) * ftab.size(),
+                                         cudaMemcpyHostToDevice, st));
+        rp.filter_cdf = w.filter.ptr;
+    }
     KS_CUDA_TRY(ctx, w.queue[0].reserve(w.capacity));
     KS_CUDA_TRY(ctx, w.queue[1].reserve(w.capacity));
     for (int f = 0; f < 4; ++f)
@@ -1120,6 +1219,7 @@ struct BatchWork
     DevBuf<double *> accum, weights;
     DevBuf<unsigned long long> path_begin;
     DevBuf<BatchState> state_dev;
+    DevBuf<float> filters; // the jobs' pixel-filter sample tables, concatenated
     unsigned ext_grid = 0, shadow_grid = 0; // one wave of resident CTAs of the traversal kernels
     bool attribs = false;                   // some job's scene has vertex normals or texcoords
 };
@@ -1134,6 +1234,8 @@ static ks_status batch_tables(ks_context *ctx, const ks_batch_job *jobs, uint32_
     std::vector<RenderParams> params(n);
     std::vector<double *> acc(n), wts(n);
     std::vector<unsigned long long> begin(n + 1, 0);
+    std::vector<float> filter_host;
+    std::vector<size_t> filter_off(n, 0);
     *max_bounces = 0;
     w.attribs = false;
     for (uint32_t j = 0; j < n; ++j) {
@@ -1154,6 +1256,12 @@ static ks_status batch_tables(ks_context *ctx, const ks_batch_job *jobs, uint32_
                                                           ": bad resolution (at most 2^21 pixels), spp or bounces");
         if (!fill_params(&jb.camera, &in, params[j]))
             return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_batch_render_device: empty crop window");
+        std::vector<float> ftab;
+        if (!pixel_filter_table(&in, ftab, params[j].filter_n))
+            return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_batch_render_device: job " + std::to_string(j) +
+                                                          ": bad pixel filter");
+        filter_off[j] = filter_host.size();
+        filter_host.insert(filter_host.end(), ftab.begin(), ftab.end());
         views[j] = make_view(jb.scene);
         w.attribs |= views[j].normals != nullptr || views[j].texcoords != nullptr;
         acc[j] = jb.accum_rgb_device;
@@ -1163,6 +1271,14 @@ static ks_status batch_tables(ks_context *ctx, const ks_batch_job *jobs, uint32_
     }
     *total = begin[n];
     cudaStream_t st = ctx->stream;
+    if (!filter_host.empty()) {
+        KS_CUDA_TRY(ctx, w.filters.alloc(filter_host.size()));
+        KS_CUDA_TRY(ctx, cudaMemcpyAsync(w.filters.ptr, filter_host.data(), sizeof(float) * filter_host.size(),
+                                         cudaMemcpyHostToDevice, ctx->stream));
+        for (uint32_t j = 0; j < n; ++j)
+            if (params[j].filter_n)
+                params[j].filter_cdf = w.filters.ptr + filter_off[j];
+    }
     KS_CUDA_TRY(ctx, w.views.alloc(n));
     KS_CUDA_TRY(ctx, w.params.alloc(n));
     KS_CUDA_TRY(ctx, w.accum.alloc(n));

@@ -17,6 +17,9 @@ struct RenderParams
     int bounces, include_background;
     float clamp_direct, clamp_indirect;
     float filter_r;
+    const float *filter_cdf; // Gaussian / Blackman-Harris: filter_n conditional CDFs (filter_n + 1
+                             // each), then the marginal CDF; null for the box filter
+    uint32_t filter_n;
     float cam_pos[3];
     float p2w[16];
 };

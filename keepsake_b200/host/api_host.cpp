@@ -230,6 +230,8 @@ void ks_small_pt_params_default(ks_small_pt_params *p)
     p->clamp_indirect = 10.0f;
     p->spp_prog_interval = 32;
     p->pixel_filter_width = 1.0f;
+    p->pixel_filter = 0;
+    p->pixel_filter_sigma = 0.5f;
 }
 
 } // extern "C"

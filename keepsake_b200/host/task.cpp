@@ -803,10 +803,22 @@ void small_pt_b200(const ConfigArgs &args, const fs::path &task_dir, int task_id
     p.rng_seed = args.load_integer("rng_seed", 0);
     p.spp_prog_interval = args.load_integer("spp_prog_interval", 32);
     if (args.contains("pixel_filter")) {
+        // create_pixel_filter (render_target.cpp:28-44)
         ConfigArgs f = args["pixel_filter"];
-        if (f.load_string("type") != "box")
-            throw StatusError(KS_ERR_UNSUPPORTED, "config: only the box pixel filter is supported");
-        p.pixel_filter_width = f.load_float("width", 1.0f);
+        const std::string type = f.load_string("type");
+        if (type == "box") {
+            p.pixel_filter = 0;
+            p.pixel_filter_width = f.load_float("width", 1.0f);
+        } else if (type == "gaussian") {
+            p.pixel_filter = 1;
+            p.pixel_filter_width = f.load_float("width", 3.0f);
+            p.pixel_filter_sigma = f.load_float("sigma", 0.5f);
+        } else if (type == "blackman_harris") {
+            p.pixel_filter = 2;
+            p.pixel_filter_width = f.load_float("width", 3.0f);
+        } else {
+            throw ParseError("config: invalid pixel filter type [" + type + "]");
+        }
     }
     // ---- camera (create_camera, camera.cpp:172-205) ----
     ConfigArgs c = args["camera"];

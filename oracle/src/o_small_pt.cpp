@@ -5,6 +5,7 @@
 //   Material::sample_with_nee     material.cpp:101-167 (no subsurface)
 //   Camera::spawn_ray             camera.cpp:129-170 (perspective, no ray differentials: the
 //                                 constant shader fields never read them)
+//   pixel filters                 render_target.h:79-180 (box, Gaussian, Blackman-Harris)
 //   MeshGeometry::compute_intersection  geometry.cpp:68-163 (texcoord tangents, smooth normals)
 //   transform_it / Transform::frame      ray.h:166-183, maths.h:989-996
 //   SkyLight                      light.cpp:19-159 (in-memory lat-long map instead of a file)
@@ -118,6 +119,54 @@ struct DistribTable2D
         int x = std::clamp(int(p0 * (cond[0].cdf.size() - 1)), 0, (int)cond[0].cdf.size() - 2);
         int y = std::clamp(int(p1 * cond.size()), 0, (int)cond.size() - 1);
         return margin.pdf(y) * cond[y].pdf(x);
+    }
+};
+
+// GaussianPixelFilter / BlackmanHarrisPixelFilter::eval (render_target.h:127-180; gaussian(),
+// maths.h:1070-1073) tabulated as PixelFilterSampleTable (render_target.h:79-106): n = ceil(32 r)
+// cells per side over [-r, r]^2, sampled through DistribTable2D::sample_linear.
+struct PixelFilterTable
+{
+    float r = 0.5f;
+    uint32_t n = 0;
+    DistribTable2D distrib;
+    PixelFilterTable(int type, float width, float sigma) : r(0.5f * width)
+    {
+        if (type == 0)
+            return;
+        const float pi = 3.14159265359f, two_pi = 6.28318530718f;
+        auto gaussian = [&](float x, float mu) {
+            return 1.0f / std::sqrt(two_pi * sigma * sigma) * std::exp(-((x - mu) * (x - mu)) / (2.0f * sigma * sigma));
+        };
+        const float threshold = gaussian(r, 0.0f);
+        auto eval = [&](float x, float y) {
+            if (x < -r || x > r || y < -r || y > r)
+                return 0.0f;
+            if (type == 1)
+                return (gaussian(x, 0.0f) - threshold) * (gaussian(y, 0.0f) - threshold);
+            const float a0 = 0.35875f, a1 = 0.48829f, a2 = 0.14128f, a3 = 0.01168f;
+            float tx = (x + r) / (2.0f * r);
+            float fx = a0 - a1 * std::cos(2.0f * pi * tx) + a2 * std::cos(4.0f * pi * tx) - a3 * std::cos(6.0f * pi * tx);
+            float ty = (y + r) / (2.0f * r);
+            float fy = a0 - a1 * std::cos(2.0f * pi * ty) + a2 * std::cos(4.0f * pi * ty) - a3 * std::cos(6.0f * pi * ty);
+            return fx * fy;
+        };
+        n = (uint32_t)(int)std::ceil(32 * r);
+        std::vector<float> f((size_t)n * n);
+        for (uint32_t y = 0; y < n; ++y)
+            for (uint32_t x = 0; x < n; ++x)
+                f[(size_t)y * n + x] = eval(std::lerp(-r, r, (x + 0.5f) / n), std::lerp(-r, r, (y + 0.5f) / n));
+        distrib = DistribTable2D(f.data(), n, n);
+    }
+    // PixelFilterSampleTable::sample / BoxPixelFilter::sample: lerp(-r, r, .) = (1 - t) * -r + t * r
+    void sample(float u0, float u1, float &offx, float &offy) const
+    {
+        if (n) {
+            float pdf;
+            distrib.sample_linear(u0, u1, pdf, u0, u1);
+        }
+        offx = (1.0f - u0) * -r + u0 * r;
+        offy = (1.0f - u1) * -r + u1 * r;
     }
 };
 
@@ -871,7 +920,7 @@ int oracle_render(void *sp, const ks_camera_desc *cam, const ks_small_pt_params 
     const int tiles_x = (cw + 3) / 4, tiles_y = (ch + 3) / 4;
     std::atomic<int> next_tile{0};
     std::atomic<uint64_t> n_ext{0}, n_shadow{0};
-    const float r = 0.5f * in->pixel_filter_width;
+    const PixelFilterTable filter(in->pixel_filter, in->pixel_filter_width, in->pixel_filter_sigma);
     auto worker = [&]() {
         Tracer tr{s, *in, {}};
         while (true) {
@@ -889,9 +938,7 @@ int oracle_render(void *sp, const ks_camera_desc *cam, const ks_small_pt_params 
                         if (in->spp != 1) {
                             float u0, u1;
                             sampler.sobol.next2d(u0, u1);
-                            // BoxPixelFilter::sample: lerp(-r, r, u) = (1 - u) * -r + u * r
-                            offx = (1.0f - u0) * -r + u0 * r;
-                            offy = (1.0f - u1) * -r + u1 * r;
+                            filter.sample(u0, u1, offx, offy);
                         }
                         float fx = ((px + 0.5f) + offx) / (float)W;
                         float fy = ((py + 0.5f) + offy) / (float)H;

@@ -27,6 +27,13 @@ CASES = {
     "box_room_backdrop": dict(kind="box_room", W=48, H=48, spp=8, bounces=4, clamp_indirect=0.0,
                               backdrop=(0.2, 0.3, 0.4)),
     "box_room_spp1": dict(kind="box_room", W=64, H=64, spp=1, bounces=8, clamp_indirect=0.0),
+    # pixel filters (render_target.h:108-180): camera offsets from the tabulated filter
+    "box_room_gaussian": dict(kind="box_room", W=48, H=48, spp=16, bounces=8, clamp_indirect=0.0,
+                              filter=(1, 3.0, 0.5)),
+    "box_room_blackman_harris": dict(kind="box_room", W=48, H=48, spp=16, bounces=8, clamp_indirect=0.0,
+                                     filter=(2, 2.0, 0.5)),
+    "box_room_box_wide": dict(kind="box_room", W=48, H=48, spp=8, bounces=8, clamp_indirect=0.0,
+                              filter=(0, 2.5, 0.5)),
     "icosphere_sky": dict(kind="icosphere", level=5, sky=(256, 128), W=64, H=64, spp=16, bounces=12),
     "icosphere_glossy_occluder": dict(kind="icosphere", level=5, sky=(256, 128), W=64, H=48, spp=8, bounces=12,
                                       roughness=(0.02, 0.2), occluder=True),
@@ -49,6 +56,8 @@ def make_case(c):
                   crop_height=c["crop"][3])
     if "backdrop" in c:
         kw.update(include_background=0, backdrop=c["backdrop"])
+    if "filter" in c:
+        kw.update(pixel_filter=c["filter"][0], pixel_filter_width=c["filter"][1], pixel_filter_sigma=c["filter"][2])
     return g, cam, ks.SmallPTParams.make(**kw)
 
 
@@ -61,6 +70,22 @@ def test_oracle_render_deterministic_and_weighted(oracle):
     assert (w1.sum(-1) == p.spp).all()
     assert np.isfinite(a1).all() and (a1 >= 0).all()
     assert c1[0] > 0 and c1[1] > 0
+
+
+def test_oracle_pixel_filters(oracle):
+    """Same samples through the box, Gaussian and Blackman-Harris filters: identical weights,
+    different camera offsets (different images), the same flux within the noise."""
+    imgs = {}
+    for name in ("box_room", "box_room_gaussian", "box_room_blackman_harris"):
+        c = dict(CASES[name], W=32, H=32, spp=16)
+        g, cam, p = make_case(c)
+        a, w, _ = oracle.scene(g.desc).render(cam, p, threads=4)
+        imgs[name] = (composite(a, w), w)
+    box, gau, bh = (imgs[k] for k in ("box_room", "box_room_gaussian", "box_room_blackman_harris"))
+    assert np.array_equal(box[1], gau[1]) or (box[1].sum(-1) == gau[1].sum(-1)).all()
+    for img, _ in (gau, bh):
+        assert rel_mse(img, box[0]) > 1e-4
+        assert abs(img.mean() / box[0].mean() - 1.0) < 0.05
 
 
 def test_oracle_converges(oracle):
@@ -151,6 +176,13 @@ def test_render_errors(ctx):
     with pytest.raises(ks.KsError) as e:
         s.render(cam, p)
     assert e.value.status == 1
+    p.spp = 4
+    for bad in (dict(pixel_filter=3), dict(pixel_filter=1, pixel_filter_sigma=0.0),
+                dict(pixel_filter=2, pixel_filter_width=40.0)):
+        q = ks.SmallPTParams.make(render_width=16, render_height=16, spp=4, bounces=2, **bad)
+        with pytest.raises(ks.KsError) as e:
+            s.render(cam, q)
+        assert e.value.status == 1
 
 
 @pytest.mark.gpu
