@@ -511,6 +511,22 @@ void ks_generated_destroy(ks_generated *g);
  * the message is in ks_config_last_error(). */
 ks_status ks_compound_asset_load(const char *path, int32_t load_materials, ks_generated **out);
 
+/* Camera animation (CameraAnimation, camera.h:44-61; create_camera_animation, camera.cpp:276-465):
+ * the translation and rotation keys of the perspective camera `camera_name` in a .glb file
+ * (found depth first in the default scene), optionally turned from y-up to z-up.  Frames: one per
+ * translation key; eval: translation interpolated linearly, rotation spherically
+ * (CameraAnimation::eval, camera.cpp:207-255), as a camera-to-world matrix (row-major) plus the
+ * camera's vfov (radians) and aspect, ready for ks_camera_perspective.  The small_pt task renders
+ * frame i at duration * (i + 0.5) / frames (small_pt.cpp:243-296). */
+typedef struct ks_camera_animation ks_camera_animation;
+ks_status ks_camera_animation_load(const char *path, const char *camera_name, int32_t convert_y_up_to_z_up,
+                                   ks_camera_animation **out);
+uint32_t ks_camera_animation_frames(const ks_camera_animation *a);
+float ks_camera_animation_duration(const ks_camera_animation *a);
+ks_status ks_camera_animation_eval(const ks_camera_animation *a, float time, float camera_to_world[16], float *vfov,
+                                   float *aspect);
+void ks_camera_animation_destroy(ks_camera_animation *a);
+
 #ifdef __cplusplus
 }
 #endif

@@ -203,6 +203,49 @@ _sig("ks_generated_scene_desc", [_vp], ctypes.POINTER(SceneDesc))
 _sig("ks_generated_camera", [_vp, ctypes.POINTER(_f32), ctypes.POINTER(_f32), ctypes.POINTER(_f32)])
 _sig("ks_generated_destroy", [_vp], None)
 _sig("ks_compound_asset_load", [ctypes.c_char_p, ctypes.c_int32, ctypes.POINTER(_vp)])
+_sig("ks_camera_animation_load", [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int32, ctypes.POINTER(_vp)])
+_sig("ks_camera_animation_frames", [_vp], ctypes.c_uint32)
+_sig("ks_camera_animation_duration", [_vp], _f32)
+_sig("ks_camera_animation_eval", [_vp, _f32, ctypes.POINTER(_f32), ctypes.POINTER(_f32), ctypes.POINTER(_f32)])
+_sig("ks_camera_animation_destroy", [_vp], None)
+
+
+class CameraAnimation:
+    """A glTF camera animation (ks_camera_animation_*)."""
+
+    def __init__(self, path, camera_name, convert_y_up_to_z_up=False):
+        h = _vp()
+        st = lib.ks_camera_animation_load(str(path).encode(), camera_name.encode(), int(convert_y_up_to_z_up),
+                                          ctypes.byref(h))
+        if st != KS_OK:
+            raise KsError(st, lib.ks_config_last_error().decode())
+        self.handle = h
+        self.frames = lib.ks_camera_animation_frames(h)
+        self.duration = lib.ks_camera_animation_duration(h)
+
+    def eval(self, time):
+        """(camera_to_world [4, 4] row-major, vfov radians, aspect) at `time`."""
+        m = (_f32 * 16)()
+        vfov, aspect = _f32(), _f32()
+        st = lib.ks_camera_animation_eval(self.handle, time, m, ctypes.byref(vfov), ctypes.byref(aspect))
+        if st != KS_OK:
+            raise KsError(st, "ks_camera_animation_eval")
+        return np.array(m[:], np.float32).reshape(4, 4), vfov.value, aspect.value
+
+    def frame_time(self, frame):
+        """The time the small_pt task renders frame `frame` at: duration x (frame + 0.5) / frames."""
+        return float(np.float32(self.duration) * (np.float32(frame) + np.float32(0.5)) / np.float32(self.frames))
+
+    def close(self):
+        if self.handle:
+            lib.ks_camera_animation_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 _sig("ks_small_pt_params_default", [ctypes.POINTER(SmallPTParams)], None)
 
 

@@ -79,6 +79,11 @@ struct ks_generated
     ksb::GeneratedScene scene;
 };
 
+struct ks_camera_animation
+{
+    ksb::gltf::CameraAnimation anim;
+};
+
 extern "C" {
 
 ks_status ks_camera_perspective(const float camera_to_world[16], float vfov, float aspect, ks_camera_desc *out)
@@ -166,6 +171,43 @@ ks_status ks_generated_camera(const ks_generated *g, float camera_to_world[16], 
 }
 
 void ks_generated_destroy(ks_generated *g) { delete g; }
+
+ks_status ks_camera_animation_load(const char *path, const char *camera_name, int32_t convert_y_up_to_z_up,
+                                   ks_camera_animation **out)
+{
+    if (!path || !camera_name || !out)
+        return KS_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    try {
+        auto a = std::make_unique<ks_camera_animation>();
+        a->anim = ksb::gltf::load_camera_animation(path, camera_name, convert_y_up_to_z_up != 0);
+        *out = a.release();
+        return KS_OK;
+    } catch (const ksb::gltf::Error &e) {
+        ksb::set_host_error(e.what());
+        return e.unsupported ? KS_ERR_UNSUPPORTED : KS_ERR_IO;
+    } catch (const std::exception &e) {
+        ksb::set_host_error(e.what());
+        return KS_ERR_IO;
+    }
+}
+
+uint32_t ks_camera_animation_frames(const ks_camera_animation *a) { return a ? a->anim.n_frames() : 0; }
+
+float ks_camera_animation_duration(const ks_camera_animation *a) { return a ? a->anim.duration() : 0.0f; }
+
+ks_status ks_camera_animation_eval(const ks_camera_animation *a, float time, float camera_to_world[16], float *vfov,
+                                   float *aspect)
+{
+    if (!a || !camera_to_world || !vfov || !aspect)
+        return KS_ERR_INVALID_ARGUMENT;
+    a->anim.eval(time, camera_to_world);
+    *vfov = a->anim.vfov;
+    *aspect = a->anim.aspect;
+    return KS_OK;
+}
+
+void ks_camera_animation_destroy(ks_camera_animation *a) { delete a; }
 
 ks_status ks_compound_asset_load(const char *path, int32_t load_materials, ks_generated **out)
 {

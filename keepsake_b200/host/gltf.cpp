@@ -768,3 +768,185 @@ Compound load(const fs::path &path, bool load_materials)
 
 } // namespace gltf
 } // namespace ksb
+
+namespace ksb
+{
+namespace gltf
+{
+
+namespace
+{
+
+// Shortest-arc spherical interpolation of unit quaternions (x, y, z, w) (Shoemake), with the
+// linear blend near parallel quaternions, as Eigen's QuaternionBase::slerp does it.
+void slerp(const float *a, const float *b, float t, float *out)
+{
+    const float d = a[0] * b[0] + a[1] * b[1] + a[2] * b[2] + a[3] * b[3];
+    const float ad = std::fabs(d);
+    float s0, s1;
+    if (ad >= 1.0f - 1e-5f) {
+        s0 = 1.0f - t;
+        s1 = t;
+    } else {
+        const float theta = std::acos(ad), st = std::sin(theta);
+        s0 = std::sin((1.0f - t) * theta) / st;
+        s1 = std::sin(t * theta) / st;
+    }
+    if (d < 0.0f)
+        s1 = -s1;
+    for (int k = 0; k < 4; ++k)
+        out[k] = s0 * a[k] + s1 * b[k];
+}
+
+// The interpolation interval of `time` among ascending keys (CameraAnimation::eval): the first
+// key above time and the one before it, or the last two; delta clamped to [0, 1] (0 when both
+// keys coincide, where the reference divides zero by zero).
+void interval(const std::vector<float> &keys, float time, int &left, int &right, float &delta)
+{
+    const auto it = std::upper_bound(keys.begin(), keys.end(), time);
+    if (it != keys.end()) {
+        right = (int)(it - keys.begin());
+        left = std::max(right - 1, 0);
+    } else {
+        right = (int)keys.size() - 1;
+        left = std::max(right - 1, 0);
+    }
+    const float t0 = keys[(size_t)left], t1 = keys[(size_t)right];
+    delta = t1 == t0 ? 0.0f : std::clamp((time - t0) / (t1 - t0), 0.0f, 1.0f);
+}
+
+} // namespace
+
+void CameraAnimation::eval(float time, float m[16]) const
+{
+    int l, r;
+    float dt;
+    float t[3] = {0, 0, 0}, q[4] = {0, 0, 0, 1};
+    if (!translation_keys.empty()) {
+        interval(translation_keys, time, l, r, dt);
+        for (int k = 0; k < 3; ++k)
+            t[k] = (1.0f - dt) * translation_values[3 * (size_t)l + k] + dt * translation_values[3 * (size_t)r + k];
+    }
+    if (!rotation_keys.empty()) {
+        interval(rotation_keys, time, l, r, dt);
+        slerp(&rotation_values[4 * (size_t)l], &rotation_values[4 * (size_t)r], dt, q);
+    }
+    const float x = q[0], y = q[1], z = q[2], w = q[3];
+    const float R[9] = {1 - 2 * (y * y + z * z), 2 * (x * y - w * z),     2 * (x * z + w * y),
+                        2 * (x * y + w * z),     1 - 2 * (x * x + z * z), 2 * (y * z - w * x),
+                        2 * (x * z - w * y),     2 * (y * z + w * x),     1 - 2 * (x * x + y * y)};
+    for (int row = 0; row < 3; ++row) {
+        for (int c = 0; c < 3; ++c)
+            m[4 * row + c] = R[3 * row + c];
+        m[4 * row + 3] = t[row];
+    }
+    m[12] = m[13] = m[14] = 0.0f;
+    m[15] = 1.0f;
+}
+
+CameraAnimation load_camera_animation(const fs::path &path, const std::string &name, bool y_up_to_z_up)
+{
+    Model m = load_model(path);
+    const auto &nodes = m.doc.array("nodes");
+    const auto &cameras = m.doc.array("cameras");
+    const auto &scenes = m.doc.array("scenes");
+    const long si = m.doc.integer("scene", 0);
+    if (si < 0 || si >= (long)scenes.size())
+        throw Error(path.string() + ": no default scene");
+    std::vector<int> seen(nodes.size(), 0);
+    auto find = [&](long ni, auto &self) -> long {
+        if (ni < 0 || ni >= (long)nodes.size() || seen[(size_t)ni]++)
+            throw Error(path.string() + ": bad node graph");
+        const Json &node = nodes[(size_t)ni];
+        const long ci = node.integer("camera", -1);
+        if (ci >= 0 && ci < (long)cameras.size() && cameras[(size_t)ci].string("name", "") == name)
+            return ni;
+        for (const Json &c : node.array("children")) {
+            const long r = self(c.kind == Json::Number ? (long)c.num : -1, self);
+            if (r >= 0)
+                return r;
+        }
+        return -1;
+    };
+    long cam_node = -1;
+    for (const Json &root : scenes[(size_t)si].array("nodes")) {
+        cam_node = find(root.kind == Json::Number ? (long)root.num : -1, find);
+        if (cam_node >= 0)
+            break;
+    }
+    if (cam_node < 0)
+        throw Error(path.string() + ": no camera node named [" + name + "]");
+    const Json &cam = cameras[(size_t)nodes[(size_t)cam_node].integer("camera", -1)];
+    CameraAnimation a;
+    if (cam.string("type", "") != "perspective")
+        throw Error(path.string() + ": camera [" + name + "] is not a perspective camera", true);
+    const Json *persp = cam.get("perspective");
+    if (!persp)
+        throw Error(path.string() + ": camera [" + name + "] without perspective parameters");
+    a.vfov = (float)persp->number("yfov", 0.0);
+    a.aspect = (float)persp->number("aspectRatio", 0.0);
+    long t_in = -1, t_out = -1, r_in = -1, r_out = -1;
+    for (const Json &anim : m.doc.array("animations")) {
+        long ts = -1, rs = -1;
+        for (const Json &ch : anim.array("channels")) {
+            const Json *target = ch.get("target");
+            if (!target || target->integer("node", -1) != cam_node)
+                continue;
+            const std::string what = target->string("path", "");
+            if (what == "translation")
+                ts = ch.integer("sampler", -1);
+            else if (what == "rotation")
+                rs = ch.integer("sampler", -1);
+        }
+        const auto &samplers = anim.array("samplers");
+        auto io = [&](long s, long &in, long &out) {
+            if (s < 0 || s >= (long)samplers.size())
+                throw Error(path.string() + ": animation sampler index out of range");
+            in = samplers[(size_t)s].integer("input", -1);
+            out = samplers[(size_t)s].integer("output", -1);
+        };
+        if (ts >= 0)
+            io(ts, t_in, t_out);
+        if (rs >= 0)
+            io(rs, r_in, r_out);
+        if (ts >= 0 && rs >= 0)
+            break;
+    }
+    if (t_in < 0)
+        throw Error(path.string() + ": no translation animation for the camera [" + name + "]", r_in >= 0);
+    size_t n = 0, n2 = 0;
+    a.translation_keys = floats(m, t_in, "SCALAR", n);
+    a.translation_values = floats(m, t_out, "VEC3", n2);
+    if (n == 0 || n2 != n)
+        throw Error(path.string() + ": translation keys and values differ in count");
+    if (r_in >= 0) {
+        a.rotation_keys = floats(m, r_in, "SCALAR", n);
+        a.rotation_values = floats(m, r_out, "VEC4", n2);
+        if (n == 0 || n2 != n)
+            throw Error(path.string() + ": rotation keys and values differ in count");
+    }
+    if (!std::is_sorted(a.translation_keys.begin(), a.translation_keys.end()) ||
+        !std::is_sorted(a.rotation_keys.begin(), a.rotation_keys.end()))
+        throw Error(path.string() + ": animation keys are not in ascending order");
+    if (y_up_to_z_up) {
+        for (size_t i = 0; i + 2 < a.translation_values.size(); i += 3) {
+            const float y = a.translation_values[i + 1], z = a.translation_values[i + 2];
+            a.translation_values[i + 1] = -z;
+            a.translation_values[i + 2] = y;
+        }
+        // r * q with r the quarter turn about x of convert_yup_to_zup: (sin 45, 0, 0, cos 45)
+        const float s = std::sqrt(0.5f);
+        for (size_t i = 0; i + 3 < a.rotation_values.size(); i += 4) {
+            const float qx = a.rotation_values[i], qy = a.rotation_values[i + 1], qz = a.rotation_values[i + 2],
+                        qw = a.rotation_values[i + 3];
+            a.rotation_values[i] = s * qw + s * qx;
+            a.rotation_values[i + 1] = s * qy - s * qz;
+            a.rotation_values[i + 2] = s * qz + s * qy;
+            a.rotation_values[i + 3] = s * qw - s * qx;
+        }
+    }
+    return a;
+}
+
+} // namespace gltf
+} // namespace ksb

@@ -49,5 +49,25 @@ struct Compound
 
 Compound load(const std::filesystem::path &path, bool load_materials);
 
+// CameraAnimation (camera.h:44-61, camera.cpp:207-465): the translation and rotation keys of a
+// named perspective camera's node in a .glb file, evaluated with linear interpolation of the
+// translation and spherical interpolation of the rotation (CameraAnimation::eval).
+struct CameraAnimation
+{
+    float vfov = 0.0f, aspect = 1.0f;
+    std::vector<float> translation_keys, translation_values; // 3 values per key
+    std::vector<float> rotation_keys, rotation_values;       // x, y, z, w per key
+    uint32_t n_frames() const { return (uint32_t)translation_keys.size(); }
+    float duration() const { return translation_keys.empty() ? 0.0f : translation_keys.back(); }
+    // camera-to-world (row-major 4x4) at `time`
+    void eval(float time, float camera_to_world[16]) const;
+};
+
+// create_camera_animation (camera.cpp:276-465): camera `name` found depth first in the default
+// scene; the first animation that drives its node's translation or rotation (the search stops at
+// one that drives both); convert_y_up_to_z_up turns the keys by convert_yup_to_zup (maths.h:916-927).
+CameraAnimation load_camera_animation(const std::filesystem::path &path, const std::string &name,
+                                      bool convert_y_up_to_z_up);
+
 } // namespace gltf
 } // namespace ksb

@@ -95,6 +95,8 @@ struct ConfigServiceImpl
     const Value *find_asset(const std::string &path) const;
     std::shared_ptr<MeshAsset> mesh_asset(const std::string &path);
     std::shared_ptr<MeshAsset> compound_asset(const std::string &path);
+    std::shared_ptr<ksb::gltf::CameraAnimation> camera_animation(const std::string &path);
+    std::map<std::string, std::shared_ptr<ksb::gltf::CameraAnimation>> animations;
     ks_material_desc material(const std::string &path);
 };
 
@@ -514,6 +516,29 @@ std::shared_ptr<MeshAsset> ConfigServiceImpl::compound_asset(const std::string &
     return m;
 }
 
+// create_camera_animation (camera.cpp:276-465): keys path, camera_name, convert_y_up_to_z_up.
+std::shared_ptr<ksb::gltf::CameraAnimation> ConfigServiceImpl::camera_animation(const std::string &path)
+{
+    auto it = animations.find(path);
+    if (it != animations.end())
+        return it->second;
+    const Value *node = find_asset(path);
+    if (!node || path.rfind("camera_animation.", 0) != 0)
+        throw ParseError("config: unknown camera animation '" + path + "'");
+    ConfigArgs a = args_of(this, node, path);
+    std::shared_ptr<ksb::gltf::CameraAnimation> anim;
+    try {
+        anim = std::make_shared<ksb::gltf::CameraAnimation>(ksb::gltf::load_camera_animation(
+            a.load_path("path"), a.load_string("camera_name"), a.load_bool("convert_y_up_to_z_up", false)));
+    } catch (const ksb::gltf::Error &e) {
+        if (e.unsupported)
+            throw StatusError(KS_ERR_UNSUPPORTED, std::string("config: ") + e.what());
+        throw IoError(e.what());
+    }
+    animations[path] = anim;
+    return anim;
+}
+
 ks_material_desc ConfigServiceImpl::material(const std::string &path)
 {
     auto it = materials.find(path);
@@ -626,7 +651,8 @@ struct TaskOutput
     fs::path dir;
     int w, h;
     float backdrop[3];
-    std::string error; // the first failed image write (reported after the render returns)
+    std::string error;   // the first failed image write (reported after the render returns)
+    std::string postfix; // "_<frame>" of animated renders (composite_and_save_to_exr's path_postfix)
 };
 
 // RenderTarget2::composite_and_save_to_exr (render_target.cpp:181-208): the composite of each
@@ -643,8 +669,8 @@ void save_interval(int spp, const double *accum, const double *weights, void *us
             rgb[3 * i + c] = (float)((1.0 - a) * o->backdrop[c] + a * fg);
         }
     }
-    char name[64];
-    std::snprintf(name, sizeof(name), "small_pt_spp%d.exr", spp);
+    char name[96];
+    std::snprintf(name, sizeof(name), "small_pt_spp%d%s.exr", spp, o->postfix.c_str());
     try {
         ksb::image::write_exr(o->dir / name, rgb.data(), o->w, o->h, 3, false);
     } catch (const ksb::image::Error &e) {
@@ -778,8 +804,6 @@ void small_pt_b200(const ConfigArgs &args, const fs::path &task_dir, int task_id
     }
     if (args.contains("light"))
         throw StatusError(KS_ERR_UNSUPPORTED, "config: point / directional lights are not supported");
-    if (args.contains("camera_animation"))
-        throw StatusError(KS_ERR_UNSUPPORTED, "config: camera_animation is not supported");
     // ---- parameters (small_pt.cpp:224-241) ----
     ks_small_pt_params p;
     ks_small_pt_params_default(&p);
@@ -820,29 +844,40 @@ void small_pt_b200(const ConfigArgs &args, const fs::path &task_dir, int task_id
             throw ParseError("config: invalid pixel filter type [" + type + "]");
         }
     }
-    // ---- camera (create_camera, camera.cpp:172-205) ----
-    ConfigArgs c = args["camera"];
-    float c2w[16];
-    if (c.contains("to_world")) {
-        c.load_transform("to_world", c2w);
+    // ---- camera (create_camera, camera.cpp:172-205), or the frames of a camera_animation
+    // (small_pt.cpp:243-296: frame i at duration x (i + 0.5) / frames) ----
+    ks_camera_desc cam{};
+    std::shared_ptr<ksb::gltf::CameraAnimation> anim;
+    uint32_t n_frames = 1, frame_start = 0, frame_end = 1;
+    if (args.contains("camera_animation")) {
+        anim = svc->camera_animation(args.load_string("camera_animation"));
+        n_frames = anim->n_frames();
+        frame_start = (uint32_t)args.load_integer("camera_animation_offset", 0);
+        const uint32_t count = (uint32_t)args.load_integer("camera_animation_count", 0);
+        frame_end = count == 0 ? n_frames : frame_start + count;
     } else {
-        float pos[3], target[3], up[3];
-        c.load_vec3("pos", pos);
-        c.load_vec3("target", target);
-        c.load_vec3("up", up);
-        look_at(pos, target, up, c2w);
+        ConfigArgs c = args["camera"];
+        float c2w[16];
+        if (c.contains("to_world")) {
+            c.load_transform("to_world", c2w);
+        } else {
+            float pos[3], target[3], up[3];
+            c.load_vec3("pos", pos);
+            c.load_vec3("target", target);
+            c.load_vec3("up", up);
+            look_at(pos, target, up, c2w);
+        }
+        if (c.load_string("type") != "perspective")
+            throw StatusError(KS_ERR_UNSUPPORTED, "config: only the perspective camera is supported");
+        float aspect = c.load_float("aspect");
+        float vfov;
+        if (c.contains("vfov"))
+            vfov = c.load_float("vfov") / 180.0f * 3.14159265358979323846f;
+        else
+            vfov = 2.0f * std::atan((1.0f / aspect) * std::tan(0.5f * (c.load_float("hfov") / 180.0f *
+                                                                        3.14159265358979323846f)));
+        check(ks_camera_perspective(c2w, vfov, aspect, &cam), nullptr, "camera");
     }
-    if (c.load_string("type") != "perspective")
-        throw StatusError(KS_ERR_UNSUPPORTED, "config: only the perspective camera is supported");
-    float aspect = c.load_float("aspect");
-    float vfov;
-    if (c.contains("vfov"))
-        vfov = c.load_float("vfov") / 180.0f * 3.14159265358979323846f;
-    else
-        vfov = 2.0f * std::atan((1.0f / aspect) * std::tan(0.5f * (c.load_float("hfov") / 180.0f *
-                                                                    3.14159265358979323846f)));
-    ks_camera_desc cam;
-    check(ks_camera_perspective(c2w, vfov, aspect, &cam), nullptr, "camera");
     // ---- render ----
     int device = 0;
     if (const char *e = std::getenv("KS_B200_DEVICE"))
@@ -851,15 +886,27 @@ void small_pt_b200(const ConfigArgs &args, const fs::path &task_dir, int task_id
     check(ks_context_create(device, &g.ctx), nullptr, "ks_context_create");
     check(ks_scene_create(g.ctx, &desc, &g.scene), g.ctx, "ks_scene_create");
     check(ks_scene_build_bvh(g.scene, nullptr, nullptr), g.ctx, "ks_scene_build_bvh");
-    std::vector<double> accum((size_t)p.render_width * p.render_height * 3, 0.0);
-    std::vector<double> weights((size_t)p.render_width * p.render_height * 2, 0.0);
     TaskOutput out{task_dir, p.render_width, p.render_height, {p.backdrop[0], p.backdrop[1], p.backdrop[2]}};
     if (p.include_background)
         out.backdrop[0] = out.backdrop[1] = out.backdrop[2] = 0.0f;
-    check(ks_small_pt_render(g.scene, &cam, &p, save_interval, &out, accum.data(), weights.data()), g.ctx,
-          "ks_small_pt_render");
-    if (!out.error.empty())
-        throw IoError(out.error);
+    for (uint32_t frame = frame_start; frame < frame_end; ++frame) {
+        if (anim) {
+            float m[16];
+            anim->eval(anim->duration() * ((float)frame + 0.5f) / (float)n_frames, m);
+            check(ks_camera_perspective(m, anim->vfov, anim->aspect, &cam), nullptr, "camera animation");
+        }
+        char postfix[16] = "";
+        if (n_frames > 1)
+            std::snprintf(postfix, sizeof(postfix), "_%06u", frame);
+        out.postfix = postfix;
+        // a fresh render target per frame (SmallPT::run)
+        std::vector<double> accum((size_t)p.render_width * p.render_height * 3, 0.0);
+        std::vector<double> weights((size_t)p.render_width * p.render_height * 2, 0.0);
+        check(ks_small_pt_render(g.scene, &cam, &p, save_interval, &out, accum.data(), weights.data()), g.ctx,
+              "ks_small_pt_render");
+        if (!out.error.empty())
+            throw IoError(out.error);
+    }
 }
 
 // convert_mesh_asset (mesh_asset.cpp:301-311): each listed mesh asset written as a binary mesh

@@ -250,3 +250,154 @@ camera = {{ type = "perspective", to_world = {{ matrix_rm = {c2w} }}, vfov = 60.
     s.close()
     assert img.mean() > 0.0
     assert np.array_equal(img, ref)
+
+
+# ---- camera animation ----------------------------------------------------------------------
+T_KEYS = np.array([0.0, 1.0, 2.5], np.float32)
+T_VALS = np.array([[0, 1, 8], [1, 1, 7], [2, 2, 5]], np.float32)
+R_KEYS = np.array([0.0, 2.5], np.float32)
+R_VALS = np.array([[0, 0, 0, 1], [0, np.sin(0.3), 0, np.cos(0.3)]], np.float32)  # x y z w
+
+
+def _anim_document(camera_type="perspective", with_anim=True):
+    parts = [T_KEYS.tobytes(), T_VALS.tobytes(), R_KEYS.tobytes(), R_VALS.tobytes()]
+    offs = np.cumsum([0] + [len(p) for p in parts])
+    buf = b"".join(parts)
+    views = [dict(buffer=0, byteOffset=int(offs[i]), byteLength=len(parts[i])) for i in range(4)]
+    accs = [dict(bufferView=0, componentType=5126, count=3, type="SCALAR"),
+            dict(bufferView=1, componentType=5126, count=3, type="VEC3"),
+            dict(bufferView=2, componentType=5126, count=2, type="SCALAR"),
+            dict(bufferView=3, componentType=5126, count=2, type="VEC4")]
+    cam = dict(name="shot", type=camera_type)
+    if camera_type == "perspective":
+        cam["perspective"] = dict(yfov=0.8, aspectRatio=1.5, znear=0.1)
+    else:
+        cam["orthographic"] = dict(xmag=1, ymag=1, znear=0.1, zfar=10)
+    doc = dict(asset=dict(version="2.0"), buffers=[dict(byteLength=len(buf))], bufferViews=views, accessors=accs,
+               cameras=[dict(name="other", type="perspective", perspective=dict(yfov=1.0, aspectRatio=1.0,
+                                                                                 znear=0.1)), cam],
+               nodes=[dict(children=[1, 2]), dict(camera=0), dict(camera=1, translation=[9, 9, 9])],
+               scenes=[dict(nodes=[0])])
+    if with_anim:
+        doc["animations"] = [dict(channels=[dict(sampler=0, target=dict(node=2, path="translation")),
+                                            dict(sampler=1, target=dict(node=2, path="rotation"))],
+                                  samplers=[dict(input=0, output=1), dict(input=2, output=3)])]
+    return doc, buf
+
+
+def _slerp(a, b, t):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    d = float(a @ b)
+    if d < 0:
+        b, d = -b, -d
+    if d > 1 - 1e-7:
+        q = (1 - t) * a + t * b
+    else:
+        th = np.arccos(d)
+        q = (np.sin((1 - t) * th) * a + np.sin(t * th) * b) / np.sin(th)
+    return q / np.linalg.norm(q)
+
+
+def _expected_camera(time, yup=False):
+    def seg(keys, t):
+        i = int(np.searchsorted(keys, t, side="right"))
+        r = min(i, len(keys) - 1)
+        lo = max(r - 1, 0)
+        if keys[r] == keys[lo]:
+            return lo, r, 0.0
+        return lo, r, float(np.clip((t - keys[lo]) / (keys[r] - keys[lo]), 0, 1))
+    lo, r, d = seg(T_KEYS, time)
+    t = (1 - d) * T_VALS[lo].astype(np.float64) + d * T_VALS[r]
+    lo, r, d = seg(R_KEYS, time)
+    q = _slerp(R_VALS[lo], R_VALS[r], d)
+    if yup:
+        t = np.array([t[0], -t[2], t[1]])
+        s = np.sqrt(0.5)
+        rq = np.array([s, 0, 0, s])  # x y z w
+        x1, y1, z1, w1 = rq
+        x2, y2, z2, w2 = q
+        q = np.array([w1 * x2 + x1 * w2 + y1 * z2 - z1 * y2, w1 * y2 - x1 * z2 + y1 * w2 + z1 * x2,
+                      w1 * z2 + x1 * y2 - y1 * x2 + z1 * w2, w1 * w2 - x1 * x2 - y1 * y2 - z1 * z2])
+    m = np.eye(4)
+    m[:3, :3] = _quat_matrix(q)
+    m[:3, 3] = t
+    return m
+
+
+@pytest.mark.parametrize("yup", [False, True])
+def test_camera_animation(tmp_path, yup):
+    ks = _ks()
+    f = tmp_path / "cam.glb"
+    write_glb(f, *_anim_document())
+    a = ks.CameraAnimation(f, "shot", convert_y_up_to_z_up=yup)
+    assert a.frames == 3 and np.isclose(a.duration, 2.5)
+    for time in (-1.0, 0.0, 0.4, 1.0, 1.7, 2.5, 3.0, a.frame_time(0), a.frame_time(2)):
+        m, vfov, aspect = a.eval(time)
+        assert np.isclose(vfov, 0.8) and np.isclose(aspect, 1.5)
+        assert np.allclose(m, _expected_camera(time, yup), atol=2e-6), (time, m, _expected_camera(time, yup))
+    assert np.isclose(a.frame_time(1), 2.5 * 1.5 / 3)
+    a.close()
+
+
+def test_camera_animation_errors(tmp_path):
+    ks = _ks()
+    f = tmp_path / "cam.glb"
+    write_glb(f, *_anim_document())
+    with pytest.raises(ks.KsError) as e:
+        ks.CameraAnimation(f, "nobody")
+    assert e.value.status == 9 and "nobody" in str(e.value)
+    write_glb(f, *_anim_document(camera_type="orthographic"))
+    with pytest.raises(ks.KsError) as e:
+        ks.CameraAnimation(f, "shot")
+    assert e.value.status == 7
+    write_glb(f, *_anim_document(with_anim=False))
+    with pytest.raises(ks.KsError) as e:
+        ks.CameraAnimation(f, "shot")
+    assert e.value.status == 9 and "animation" in str(e.value)
+
+
+@pytest.mark.gpu
+def test_camera_animation_through_config_task(ctx, tmp_path):
+    """small_pt with camera_animation renders the requested frames (offset 1, count 2) to
+    small_pt_spp<N>_<frame>.exr, each equal to the C-ABI render from the animation's camera at
+    duration x (frame + 0.5) / frames."""
+    from imaging import composite
+    ks = _ks()
+    write_glb(tmp_path / "cam.glb", *_anim_document())
+    g = ks.Generated("box_room", 0)
+    doc = """
+[camera_animation.walk]
+path = "cam.glb"
+camera_name = "shot"
+convert_y_up_to_z_up = false
+
+[mesh_asset.room]
+type = "procedural"
+kind = "box_room"
+seed = 0
+
+[[task]]
+type = "small_pt"
+object = "mesh_asset.room"
+camera_animation = "camera_animation.walk"
+camera_animation_offset = 1
+camera_animation_count = 2
+bounces = 4
+render_width = 24
+render_height = 16
+spp = 4
+spp_prog_interval = 4
+"""
+    ks.config_run(doc, str(tmp_path / "out"), str(tmp_path))
+    anim = ks.CameraAnimation(tmp_path / "cam.glb", "shot")
+    s = ks.Scene(ctx, g.desc, keepalive=g)
+    s.build_bvh()
+    for frame in (1, 2):
+        img = ks.load_image(tmp_path / "out" / "task_0" / f"small_pt_spp4_{frame:06d}.exr")
+        m, vfov, aspect = anim.eval(anim.frame_time(frame))
+        cam = ks.camera_perspective(m, vfov, aspect)
+        p = ks.SmallPTParams.make(render_width=24, render_height=16, spp=4, bounces=4, spp_prog_interval=4)
+        ref = composite(*s.render(cam, p)).astype(np.float32)
+        assert np.array_equal(img, ref), frame
+    assert not (tmp_path / "out" / "task_0" / "small_pt_spp4_000000.exr").exists()
+    s.close()
