@@ -118,6 +118,16 @@ typedef struct ks_instance_desc {
     float to_world[12];
 } ks_instance_desc;
 
+/* Point and directional lights (PointLight / DirectionalLight, light.h:91-123, light.cpp:208-240;
+ * create_point_light / create_directional_light, light.cpp:285-305): delta lights, sampled by
+ * next-event estimation only (MIS weight 1, nee.cpp:45-48), ordered after the sky in the light
+ * list of PowerLightSampler with powers 4 pi I and L pi r^2 (r: half the scene box diagonal). */
+typedef struct ks_light_desc {
+    int32_t type;    /* 0 point, 1 directional */
+    float color[3];  /* I (point intensity) or L (directional radiance) */
+    float vec[3];    /* point: position; directional: unit direction toward the light */
+} ks_light_desc;
+
 typedef struct ks_scene_desc {
     const ks_mesh_desc *meshes;
     uint32_t n_meshes;
@@ -129,6 +139,8 @@ typedef struct ks_scene_desc {
     uint32_t n_prototypes;
     const ks_instance_desc *instances;
     uint32_t n_instances;
+    const ks_light_desc *lights; /* the task's `light` list (small_pt.cpp:186-199); may be NULL */
+    uint32_t n_lights;
 } ks_scene_desc;
 
 /* SBVHBuildOption (cuda/sbvh.cuh:9-16); clamped like SBVH::build (cuda/sbvh.cu:411-414). */

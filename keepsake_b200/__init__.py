@@ -143,11 +143,16 @@ class InstanceDesc(ctypes.Structure):
     _fields_ = [("prototype", _u32), ("to_world", _f32 * 12)]
 
 
+class LightDesc(ctypes.Structure):
+    _fields_ = [("type", _i32), ("color", _f32 * 3), ("vec", _f32 * 3)]
+
+
 class SceneDesc(ctypes.Structure):
     _fields_ = [("meshes", ctypes.POINTER(MeshDesc)), ("n_meshes", _u32),
                 ("materials", ctypes.POINTER(MaterialDesc)), ("n_materials", _u32), ("sky", SkyDesc),
                 ("prototypes", ctypes.POINTER(PrototypeDesc)), ("n_prototypes", _u32),
-                ("instances", ctypes.POINTER(InstanceDesc)), ("n_instances", _u32)]
+                ("instances", ctypes.POINTER(InstanceDesc)), ("n_instances", _u32),
+                ("lights", ctypes.POINTER(LightDesc)), ("n_lights", _u32)]
 
 
 class SBVHOptions(ctypes.Structure):

@@ -263,6 +263,8 @@ SceneView make_view(const ks_scene *s)
     v.materials = s->materials.ptr;
     v.light_count = s->light_count;
     v.n_nonmesh = s->n_nonmesh;
+    v.n_sky = (s->sky_desc.kind == 1 || s->sky_desc.kind == 2) ? 1u : 0u;
+    v.punctual = s->punctual.ptr;
     v.power_cdf = s->power_cdf.ptr;
     v.tri_light = s->tri_light.ptr;
     v.ml_tri = s->ml_tri.ptr;
@@ -386,6 +388,18 @@ ks_status build_lights(ks_scene *s)
     std::vector<float> ml_area, ml_importance;
     std::vector<float4> ml_em, ml_verts;
     std::vector<int32_t> inst_light_base;
+    // ---- point and directional lights: after the sky, before the mesh lights ----
+    s->n_nonmesh += (uint32_t)s->lights.size();
+    if (!s->lights.empty()) {
+        std::vector<float4> pl;
+        for (const ks_light_desc &l : s->lights) {
+            pl.push_back(make_float4(l.vec[0], l.vec[1], l.vec[2], (float)l.type));
+            pl.push_back(make_float4(l.color[0], l.color[1], l.color[2], 0.0f));
+        }
+        KS_CUDA_TRY(ctx, s->punctual.alloc(pl.size()));
+        KS_CUDA_TRY(ctx, cudaMemcpyAsync(s->punctual.ptr, pl.data(), sizeof(float4) * pl.size(),
+                                         cudaMemcpyHostToDevice, st));
+    }
     bool any_emission = false;
     for (size_t m = 0; m + 1 < s->host.mesh_tri_offset.size(); ++m)
         if (s->host.materials[s->host.mesh_material[m]].has_emission)
@@ -505,8 +519,23 @@ ks_status build_lights(ks_scene *s)
     s->light_count = count;
     s->h_powers.assign(count, 0.0f);
     uint32_t flat = 0;
-    if (s->n_nonmesh)
+    if (s->n_nonmesh > s->lights.size())
         s->h_powers[flat++] = sky_power_mean;
+    for (const ks_light_desc &l : s->lights) {
+        // PointLight::power = 4 pi I; DirectionalLight::power = L pi r^2 (light.cpp:218-240); mean
+        float p[3];
+        if (l.type == 0) {
+            for (int c = 0; c < 3; ++c)
+                p[c] = 4.0f * 3.14159265359f * l.color[c];
+        } else {
+            const float ex = s->scene_bound[3] - s->scene_bound[0], ey = s->scene_bound[4] - s->scene_bound[1],
+                        ez = s->scene_bound[5] - s->scene_bound[2];
+            const float r = 0.5f * std::sqrt(ex * ex + ey * ey + ez * ez);
+            for (int c = 0; c < 3; ++c)
+                p[c] = l.color[c] * 3.14159265359f * (r * r);
+        }
+        s->h_powers[flat++] = (p[0] + p[1] + p[2]) / 3.0f;
+    }
     for (size_t k = 0; k < ml_tri.size(); ++k) {
         float pw = ml_importance[k];
         s->h_powers[flat] = (pw + pw + pw) / 3.0f;

@@ -32,7 +32,9 @@ struct SceneView
     const MaterialGPU *materials;
     // lights
     uint32_t light_count;
-    uint32_t n_nonmesh; // 1 when a sky light exists (it is light 0)
+    uint32_t n_nonmesh; // the sky (light 0, when there is one) and the point / directional lights
+    uint32_t n_sky;     // 1 when a sky light exists
+    const float4 *punctual; // per point / directional light: (vec, type), (color, 0)
     const float *power_cdf;   // light_count + 1
     const int32_t *tri_light; // per triangle: flat light index or -1 (nullptr if no emitters)
     const uint32_t *ml_tri;   // per mesh-light triangle (flat index - n_nonmesh): global triangle

@@ -356,6 +356,21 @@ ks_status ks_scene_create(ks_context *ctx, const ks_scene_desc *desc, ks_scene *
         return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_create: bad sky description");
     }
     s->sky_desc = sd;
+    if (desc->n_lights && !desc->lights) {
+        delete s;
+        return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_create: n_lights without lights");
+    }
+    for (uint32_t k = 0; k < desc->n_lights; ++k) {
+        const ks_light_desc &l = desc->lights[k];
+        bool ok = l.type == 0 || l.type == 1;
+        for (int c = 0; c < 3; ++c)
+            ok = ok && std::isfinite(l.color[c]) && std::isfinite(l.vec[c]);
+        if (!ok) {
+            delete s;
+            return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_create: bad light " + std::to_string(k));
+        }
+        s->lights.push_back(l);
+    }
     s->sky_desc.map_rgb = nullptr;
     std::vector<MaterialGPU> mats(desc->n_materials);
     for (uint32_t k = 0; k < desc->n_materials; ++k) {

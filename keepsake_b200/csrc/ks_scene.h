@@ -120,6 +120,8 @@ struct ks_scene
     ksb::DevBuf<float4> ml_emission;
     // sky
     ks_sky_desc sky_desc{};
+    std::vector<ks_light_desc> lights; // point / directional lights, after the sky in the light list
+    ksb::DevBuf<float4> punctual;      // per light: (vec, type), (color, 0)
     ksb::DevBuf<float> sky_rgb;   // kind 2: the map as given (3 floats per texel), for the light build
     float sky_l2w[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, sky_w2l[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
     ksb::DevBuf<float4> sky_map;

@@ -36,7 +36,7 @@ using namespace wave;
 // samples[4 i + 0] = (lobe, wi u, wi v, roulette)
 // samples[4 i + 1] = (light direction, light distance)
 // samples[4 i + 2] = (Le / pdf of the light sample (Le_beta), pdf of the direction)
-// samples[4 i + 3] = (light selection probability, -, -, -)
+// samples[4 i + 3] = (light selection probability, 1 for a delta light, -, -)
 template <bool kBatch = false>
 __global__ void __launch_bounds__(128) k_sample(const __grid_constant__ SceneView sv_in,
                                                 const __grid_constant__ RenderParams rp_in, PathBuf cur,
@@ -72,8 +72,46 @@ __global__ void __launch_bounds__(128) k_sample(const __grid_constant__ SceneVie
         f3 wi = mk(0, 0, 0);
         float wi_dist = 0.0f, pdf_wi_light = 0.0f;
         f3 Le_beta;
-        if (light < sv.n_nonmesh) {
+        float delta_light = 0.0f;
+        if (light < sv.n_sky) {
             Le_beta = sky_sample(sv, u0, u1, wi, wi_dist, pdf_wi_light);
+        } else if (light < sv.n_nonmesh) {
+            // PointLight / DirectionalLight::sample (light.cpp:208-236): a delta light, weight 1
+            delta_light = 1.0f;
+            const float4 a = __ldg(&sv.punctual[2 * (size_t)(light - sv.n_sky)]);
+            const float4 c = __ldg(&sv.punctual[2 * (size_t)(light - sv.n_sky) + 1]);
+            pdf_wi_light = 1.0f;
+            if (a.w == 0.0f) {
+                const float4 h = hits[i];
+                const float4 *pt = sv.prim_tris + 3 * (size_t)bits(h.w);
+                float4 v0 = __ldg(pt), v1 = __ldg(pt + 1), v2 = __ldg(pt + 2);
+                f3 p0 = mk(v0.x, v0.y, v0.z), p1 = mk(v1.x, v1.y, v1.z), p2 = mk(v2.x, v2.y, v2.z);
+                if (sv.inst.n) {
+                    const uint32_t inst = hit_inst[i];
+                    float m[12];
+#pragma unroll
+                    for (int e = 0; e < 12; ++e)
+                        m[e] = __ldg(&sv.inst.xf[12 * (size_t)inst + e]);
+                    p0 = xf_point(m, p0);
+                    p1 = xf_point(m, p1);
+                    p2 = xf_point(m, p2);
+                }
+                wi = mk(a.x, a.y, a.z) - hit_point(p0, p1, p2, h.y, h.z);
+                const float l2 = dot(wi, wi);
+                if (l2 == 0.0f) {
+                    Le_beta = mk(0, 0, 0);
+                    pdf_wi_light = 0.0f;
+                } else {
+                    const float l = sqrtf(l2);
+                    wi = mk(wi.x / l, wi.y / l, wi.z / l);
+                    wi_dist = l;
+                    Le_beta = mk(c.x / l2, c.y / l2, c.z / l2);
+                }
+            } else {
+                wi = mk(a.x, a.y, a.z);
+                wi_dist = kInf;
+                Le_beta = mk(c.x, c.y, c.z);
+            }
         } else {
             // the shading point as the hit record computes it (make_frame)
             const float4 h = hits[i];
@@ -100,7 +138,7 @@ __global__ void __launch_bounds__(128) k_sample(const __grid_constant__ SceneVie
         samples[4 * (size_t)i] = make_float4(u_lobe, b0, b1, u_rr);
         samples[4 * (size_t)i + 1] = make_float4(wi.x, wi.y, wi.z, wi_dist);
         samples[4 * (size_t)i + 2] = make_float4(Le_beta.x, Le_beta.y, Le_beta.z, pdf_wi_light);
-        samples[4 * (size_t)i + 3] = make_float4(pr_light, 0.0f, 0.0f, 0.0f);
+        samples[4 * (size_t)i + 3] = make_float4(pr_light, delta_light, 0.0f, 0.0f);
     }
 }
 
@@ -238,7 +276,8 @@ __global__ void __launch_bounds__(128, KS_SHADE_MIN_BLOCKS) k_shade(const __grid
                     // this bounce's Sobol values and light sample, drawn by k_sample
                     const float4 sa = samples[4 * (size_t)i], sl = samples[4 * (size_t)i + 1];
                     const float4 se = samples[4 * (size_t)i + 2];
-                    const float pr_light = samples[4 * (size_t)i + 3].x;
+                    const float4 s3 = samples[4 * (size_t)i + 3];
+                    const float pr_light = s3.x;
                     // next_event_estimate (nee.cpp:11-57): the light sample's BSDF term and MIS
                     const f3 wi = mk(sl.x, sl.y, sl.z);
                     const float wi_dist = sl.w, pdf_wi_light = se.w;
@@ -249,7 +288,8 @@ __global__ void __launch_bounds__(128, KS_SHADE_MIN_BLOCKS) k_shade(const __grid
                         float pdf_b;
                         bsdf.eval_and_pdf(wo_l, wi_l, f, pdf_b);
                         if (!is_zero(f) && pdf_b > 0.0f) {
-                            float mis = power_heur(pdf_wi_light, pdf_b);
+                            // delta lights: weight 1 (nee.cpp:45-48)
+                            float mis = s3.y != 0.0f ? 1.0f : power_heur(pdf_wi_light, pdf_b);
                             f3 Ld = Le_beta * f * mis / pr_light;
                             Ld = clamp_contrib(Ld, bounce, rp, true);
                             shadow = true;

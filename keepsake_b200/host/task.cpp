@@ -802,8 +802,41 @@ void small_pt_b200(const ConfigArgs &args, const fs::path &task_dir, int task_id
             desc.sky.strength = s.load_float("strength", 1.0f);
         }
     }
-    if (args.contains("light"))
-        throw StatusError(KS_ERR_UNSUPPORTED, "config: point / directional lights are not supported");
+    // ---- lights (create_light, light.cpp:243-305): point and directional ----
+    std::vector<ks_light_desc> lights;
+    if (args.contains("light")) {
+        ConfigArgs list = args["light"];
+        for (int i = 0; i < list.array_size(); ++i) {
+            ConfigArgs l = list[i];
+            const std::string type = l.load_string("type");
+            ks_light_desc d{};
+            if (type == "point") {
+                d.type = 0;
+                if (l.contains("I")) {
+                    l.load_vec3("I", d.color);
+                } else {
+                    float c[3];
+                    l.load_vec3("color", c);
+                    const float power = l.load_float("power");
+                    for (int k = 0; k < 3; ++k)
+                        d.color[k] = c[k] * power / (4.0f * 3.14159265359f);
+                }
+                l.load_vec3("pos", d.vec);
+            } else if (type == "directional") {
+                d.type = 1;
+                l.load_vec3("L", d.color);
+                l.load_vec3("dir", d.vec);
+                const float n = std::sqrt(d.vec[0] * d.vec[0] + d.vec[1] * d.vec[1] + d.vec[2] * d.vec[2]);
+                for (int k = 0; k < 3; ++k)
+                    d.vec[k] /= n;
+            } else {
+                throw StatusError(KS_ERR_UNSUPPORTED, "config: light type '" + type + "' is not supported");
+            }
+            lights.push_back(d);
+        }
+    }
+    desc.lights = lights.empty() ? nullptr : lights.data();
+    desc.n_lights = (uint32_t)lights.size();
     // ---- parameters (small_pt.cpp:224-241) ----
     ks_small_pt_params p;
     ks_small_pt_params_default(&p);

@@ -360,6 +360,7 @@ struct Scene
     std::vector<MeshLight> mesh_lights;
     std::vector<int32_t> tri_light; // global triangle -> flat light index, -1 if none
     std::vector<uint32_t> index_psum;
+    std::vector<ks_light_desc> lights; // point / directional lights, after the sky
     DistribTable power_distrib;
     uint32_t light_count = 0;
     std::vector<float> powers;
@@ -579,9 +580,32 @@ struct Tracer
         V3 wi;
         float wi_dist = 0.0f, pdf_wi_light = 0.0f;
         V3 Le_beta;
-        uint32_t n_nonmesh = s.index_psum[1];
-        if (light < n_nonmesh) {
+        uint32_t n_nonmesh = s.index_psum[1], n_sky = s.sky ? 1u : 0u;
+        bool delta_light = false;
+        if (light < n_sky) {
             Le_beta = s.sky->sample(u0, u1, wi, wi_dist, pdf_wi_light);
+        } else if (light < n_nonmesh) {
+            // PointLight / DirectionalLight::sample (light.cpp:208-236)
+            const ks_light_desc &l = s.lights[light - n_sky];
+            delta_light = true;
+            pdf_wi_light = 1.0f;
+            if (l.type == 0) {
+                wi = V3(l.vec[0], l.vec[1], l.vec[2]) - hit.p;
+                float l2 = dot(wi, wi);
+                if (l2 == 0.0f) {
+                    Le_beta = V3(0.0f, 0.0f, 0.0f);
+                    pdf_wi_light = 0.0f;
+                } else {
+                    float len = std::sqrt(l2);
+                    wi = wi / len;
+                    wi_dist = len;
+                    Le_beta = V3(l.color[0] / l2, l.color[1] / l2, l.color[2] / l2);
+                }
+            } else {
+                wi = V3(l.vec[0], l.vec[1], l.vec[2]);
+                wi_dist = std::numeric_limits<float>::infinity();
+                Le_beta = V3(l.color[0], l.color[1], l.color[2]);
+            }
         } else {
             Le_beta = mesh_light_sample(s, light, hit.p, u0, u1, wi, wi_dist, pdf_wi_light);
         }
@@ -596,7 +620,7 @@ struct Tracer
                 V3 o = spawn_origin(hit.p, wi, hit.frame.n);
                 cnt.shadow++;
                 if (!occluded(s, o, wi, wi_dist)) {
-                    float mis_weight = power_heur(pdf_wi_light, pdf_wi_bsdf);
+                    float mis_weight = delta_light ? 1.0f : power_heur(pdf_wi_light, pdf_wi_bsdf);
                     beta_nee += Le_beta * f * mis_weight / pr_light;
                 }
             }
@@ -829,7 +853,9 @@ Scene *create_scene(const ks_scene_desc *d, const ks_sbvh_options *opts)
         s->mesh_lights.push_back(std::move(ml));
     }
     // PowerLightSampler::build (light.cpp:636-672)
-    uint32_t n_nonmesh = s->sky ? 1u : 0u;
+    if (d->n_lights)
+        s->lights.assign(d->lights, d->lights + d->n_lights);
+    uint32_t n_nonmesh = (s->sky ? 1u : 0u) + (uint32_t)s->lights.size();
     s->index_psum.assign(1 + s->mesh_lights.size() + 1, 0);
     uint32_t sum = 0;
     for (uint32_t i = 0; i < (uint32_t)s->index_psum.size(); ++i) {
@@ -844,6 +870,20 @@ Scene *create_scene(const ks_scene_desc *d, const ks_sbvh_options *opts)
     if (s->sky) {
         V3 P = s->sky->power(s->bound);
         s->powers[flat++] = (P.x + P.y + P.z) / 3.0f;
+    }
+    for (const ks_light_desc &l : s->lights) {
+        // PointLight::power 4 pi I, DirectionalLight::power L pi r^2 (light.cpp:218-240)
+        float P[3];
+        if (l.type == 0) {
+            for (int c = 0; c < 3; ++c)
+                P[c] = 4.0f * pi * l.color[c];
+        } else {
+            float ex = s->bound[3] - s->bound[0], ey = s->bound[4] - s->bound[1], ez = s->bound[5] - s->bound[2];
+            float r = 0.5f * std::sqrt(ex * ex + ey * ey + ez * ez);
+            for (int c = 0; c < 3; ++c)
+                P[c] = l.color[c] * pi * (r * r);
+        }
+        s->powers[flat++] = (P[0] + P[1] + P[2]) / 3.0f;
     }
     for (const MeshLight &ml : s->mesh_lights)
         for (uint32_t j = 0; j < ml.prim_ids.size(); ++j) {

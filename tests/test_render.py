@@ -34,6 +34,11 @@ CASES = {
                                      filter=(2, 2.0, 0.5)),
     "box_room_box_wide": dict(kind="box_room", W=48, H=48, spp=8, bounces=8, clamp_indirect=0.0,
                               filter=(0, 2.5, 0.5)),
+    # point and directional lights (light.cpp:208-240): delta lights after the sky in the light list
+    "box_room_point_light": dict(kind="box_room", W=48, H=48, spp=16, bounces=8, clamp_indirect=0.0,
+                                 lights=[(0, (3.0, 2.5, 2.0), (0.3, 1.6, 0.4))]),
+    "icosphere_directional": dict(kind="icosphere", level=4, sky=(128, 64), W=48, H=48, spp=8, bounces=8,
+                                  lights=[(1, (2.0, 1.8, 1.5), (0.3, 0.9, 0.3)), (0, (5.0, 5.0, 5.0), (0.0, 3.0, 2.0))]),
     "icosphere_sky": dict(kind="icosphere", level=5, sky=(256, 128), W=64, H=64, spp=16, bounces=12),
     "icosphere_glossy_occluder": dict(kind="icosphere", level=5, sky=(256, 128), W=64, H=48, spp=8, bounces=12,
                                       roughness=(0.02, 0.2), occluder=True),
@@ -58,6 +63,19 @@ def make_case(c):
         kw.update(include_background=0, backdrop=c["backdrop"])
     if "filter" in c:
         kw.update(pixel_filter=c["filter"][0], pixel_filter_width=c["filter"][1], pixel_filter_sigma=c["filter"][2])
+    if "lights" in c:
+        arr = (ks.LightDesc * len(c["lights"]))()
+        for k, (t, col, v) in enumerate(c["lights"]):
+            v = np.asarray(v, np.float64)
+            if t == 1:
+                v = v / np.linalg.norm(v)
+            arr[k].type = t
+            arr[k].color[:] = col
+            arr[k].vec[:] = [float(x) for x in np.float32(v)]
+        d = g.desc.contents
+        d.lights = arr
+        d.n_lights = len(c["lights"])
+        g._lights = arr  # keeps the array alive with the scene description
     return g, cam, ks.SmallPTParams.make(**kw)
 
 
@@ -86,6 +104,20 @@ def test_oracle_pixel_filters(oracle):
     for img, _ in (gau, bh):
         assert rel_mse(img, box[0]) > 1e-4
         assert abs(img.mean() / box[0].mean() - 1.0) < 0.05
+
+
+def test_oracle_delta_lights(oracle):
+    """A point light adds light to the box room (same samples, same weights, a brighter image);
+    its NEE contribution falls off with the square of the distance."""
+    base, cam, p = make_case(CASES["box_room"])
+    lit, _, _ = make_case(dict(CASES["box_room_point_light"], W=64, H=64, spp=16))
+    a0, w0, c0 = oracle.scene(base.desc).render(cam, p, threads=4)
+    a1, w1, c1 = oracle.scene(lit.desc).render(cam, p, threads=4)
+    assert np.array_equal(w0, w1)
+    assert composite(a1, w1).mean() > 1.05 * composite(a0, w0).mean()
+    powers = oracle.scene(lit.desc).light_table()[0]
+    # [emitter triangles..., point light]: the point light comes first (no sky), 4 pi I
+    assert np.isclose(powers[0], 4.0 * np.float32(3.14159265359) * (3.0 + 2.5 + 2.0) / 3.0, rtol=1e-6)
 
 
 def test_oracle_converges(oracle):
