@@ -86,7 +86,7 @@ typedef struct ks_material_desc {
     float diffuse_trans;
     float diffuse_trans_fwd;
     float emissive[3];
-    int32_t microfacet;   /* 0 = GGX, 1 = Beckmann */
+    int32_t microfacet;   /* 0 = GGX (1 = Beckmann: KS_ERR_UNSUPPORTED at ks_scene_create) */
     int32_t has_emission; /* Material::emission != nullptr */
     float emission[3];
 } ks_material_desc;

@@ -299,6 +299,10 @@ ks_status ks_scene_create(ks_context *ctx, const ks_scene_desc *desc, ks_scene *
     for (uint32_t k = 0; k < desc->n_materials; ++k)
         if (!valid_material(desc->materials[k]))
             return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_create: non-finite material field");
+    for (uint32_t k = 0; k < desc->n_materials; ++k)
+        if (desc->materials[k].microfacet != 0)
+            return fail(ctx, KS_ERR_UNSUPPORTED, "ks_scene_create: only the GGX microfacet distribution is supported "
+                                                 "(material " + std::to_string(k) + ")");
     KS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
     ks_scene *s = new (std::nothrow) ks_scene();
     if (!s)

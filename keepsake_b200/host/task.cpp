@@ -591,7 +591,9 @@ ks_material_desc ConfigServiceImpl::material(const std::string &path)
     field("diffuse_trans_fwd", 1, &d.diffuse_trans_fwd, &half);
     field("emissive", 3, d.emissive, z3);
     std::string mf = b.load_string("microfacet", "ggx");
-    d.microfacet = mf == "beckmann" ? 1 : 0;
+    if (mf != "ggx")
+        throw StatusError(KS_ERR_UNSUPPORTED, "config: microfacet '" + mf + "' is not supported (ggx)");
+    d.microfacet = 0;
     if (a.contains("emission")) {
         a.load_vec3("emission", d.emission);
         d.has_emission = 1;

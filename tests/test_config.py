@@ -111,6 +111,10 @@ def test_task_errors_before_any_device_work(tmp_path):
     with pytest.raises(ks.KsError) as e:
         ks.config_run(DOC.replace("spp = 8\n", ""), str(tmp_path))
     assert e.value.status == 8 and "spp" in str(e.value)
+    with pytest.raises(ks.KsError) as e:  # the Beckmann distribution is not built: an error, not GGX
+        ks.config_run(DOC.replace('type = "principled_bsdf"', 'type = "principled_bsdf"\nmicrofacet = "beckmann"'),
+                      str(tmp_path))
+    assert e.value.status == 7 and "beckmann" in str(e.value)
     with pytest.raises(ks.KsError) as e:
         ks.config_run(DOC.replace('"material.white", "material.lamp"', '"material.white"'), str(tmp_path))
     assert "mismatch" in str(e.value)
