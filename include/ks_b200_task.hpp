@@ -6,10 +6,12 @@
  * output directory (ConfigServiceInternal::run_all_tasks, config.cpp:262-312).  Tasks are
  * functions with keepsake's ConfigTask signature (config.h:119).  Registered:
  *   "small_pt" and "small_pt_b200": small_pt (small_pt.cpp:180-300) on the GPU through the C ABI,
- *   reading the same keys (object, material, sky, backdrop, bounces, clamp_direct,
+ *   reading the same keys (object or compound_object, material, sky, light (point,
+ *   directional), pixel_filter (box, gaussian, blackman_harris), backdrop, bounces, clamp_direct,
  *   clamp_indirect, render_width, render_height, crop_*, spp, scale_ray_diff, rng_seed,
- *   spp_prog_interval, camera) plus the `emission` key of a material.  After every spp interval
- *   the composited image is written to TASK_DIR/small_pt_spp<N>.exr (OpenEXR, FP32 RGB; ZIP
+ *   spp_prog_interval, camera or camera_animation with camera_animation_offset / _count) plus
+ *   the `emission` key of a material.  After every spp interval the composited image is written
+ *   to TASK_DIR/small_pt_spp<N>[_<frame>].exr (OpenEXR, FP32 RGB; ZIP
  *   compression where the reference's tinyexr call asks for PIZ: both lossless).  Sky maps are
  *   read from .exr, .hdr (and .pfm) files.
  *   "convert_mesh_asset": each mesh asset of `assets` written to TASK_DIR/<name>.bin in keepsake's
