@@ -212,7 +212,14 @@ typedef struct ks_camera_desc {
     float camera_to_world[16];
     float proj_to_camera[16];
     float proj_to_world[16];
+    int32_t orthographic; /* 1: rays start on the film plane and share the view direction */
 } ks_camera_desc;
+
+/* Orthographic camera (Camera's orthographic constructor with rev_orthographic, camera.cpp:72-
+ * 114): film window [left, right] x [bottom, top] and the clip range in camera space; rays start
+ * at the film point and run along -z of camera_to_world (Camera::spawn_ray, camera.cpp:155-160). */
+ks_status ks_camera_orthographic(const float camera_to_world[16], float left, float right, float bottom, float top,
+                                 float near_clip, float far_clip, ks_camera_desc *out);
 
 /* Perspective camera from a camera-to-world matrix (row-major 4x4), vertical field of view in
  * radians and aspect ratio: Camera::Camera(to_world, vfov, aspect) (camera.cpp:85-92). */

@@ -160,7 +160,8 @@ class SBVHOptions(ctypes.Structure):
 
 
 class CameraDesc(ctypes.Structure):
-    _fields_ = [("camera_to_world", _f32 * 16), ("proj_to_camera", _f32 * 16), ("proj_to_world", _f32 * 16)]
+    _fields_ = [("camera_to_world", _f32 * 16), ("proj_to_camera", _f32 * 16), ("proj_to_world", _f32 * 16),
+                ("orthographic", _i32)]
 
 
 class ProceduralOptions(ctypes.Structure):
@@ -202,6 +203,7 @@ _sig("ks_sbvh_export", [_vp, _vp, _vp, _vp, _vp, _vp])
 _sig("ks_trace_rays", [_vp, _vp, _u32, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp])
 _sig("ks_trace_rays_wide", [_vp, _vp, _u32, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp])
 _sig("ks_camera_perspective", [ctypes.POINTER(_f32), _f32, _f32, ctypes.POINTER(CameraDesc)])
+_sig("ks_camera_orthographic", [ctypes.POINTER(_f32), _f32, _f32, _f32, _f32, _f32, _f32, ctypes.POINTER(CameraDesc)])
 _sig("ks_procedural_scene", [ctypes.c_char_p, ctypes.c_uint64, ctypes.POINTER(ProceduralOptions),
                              ctypes.POINTER(_vp)])
 _sig("ks_generated_scene_desc", [_vp], ctypes.POINTER(SceneDesc))
@@ -442,6 +444,15 @@ def camera_perspective(camera_to_world, vfov, aspect) -> CameraDesc:
     st = lib.ks_camera_perspective(m, vfov, aspect, ctypes.byref(c))
     if st != KS_OK:
         raise KsError(st, "ks_camera_perspective")
+    return c
+
+
+def camera_orthographic(camera_to_world, left, right, bottom, top, near_clip, far_clip) -> CameraDesc:
+    c = CameraDesc()
+    m = (_f32 * 16)(*[float(x) for x in np.asarray(camera_to_world).reshape(16)])
+    st = lib.ks_camera_orthographic(m, left, right, bottom, top, near_clip, far_clip, ctypes.byref(c))
+    if st != KS_OK:
+        raise KsError(st, "ks_camera_orthographic")
     return c
 
 

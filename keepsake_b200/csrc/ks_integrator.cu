@@ -102,7 +102,13 @@ KS_D void camera_path(const RenderParams &rp, int px, int py, int s, uint32_t pi
         o[r] = m[4 * r + 0] * ndc.x + m[4 * r + 1] * ndc.y + m[4 * r + 2] * ndc.z + m[4 * r + 3] * 1.0f;
     f3 wp = mk(o[0] / o[3], o[1] / o[3], o[2] / o[3]);
     f3 cp = mk(rp.cam_pos[0], rp.cam_pos[1], rp.cam_pos[2]);
-    f3 dir = normalize(wp - cp);
+    f3 dir;
+    if (rp.ortho) {
+        cp = wp;
+        dir = mk(rp.cam_dir[0], rp.cam_dir[1], rp.cam_dir[2]);
+    } else {
+        dir = normalize(wp - cp);
+    }
     pb.o_pdf[slot] = make_float4(cp.x, cp.y, cp.z, 0.0f);
     pb.d_info[slot] = make_float4(dir.x, dir.y, dir.z, fbits(((uint32_t)smp.dimension << 16) | 0u));
     pb.beta_pix[slot] = make_float4(1.0f, 1.0f, 1.0f, fbits(pix_word));
@@ -831,6 +837,15 @@ static bool fill_params(const ks_camera_desc *cam, const ks_small_pt_params *in,
     rp.clamp_direct = in->clamp_direct;
     rp.clamp_indirect = in->clamp_indirect;
     rp.filter_r = 0.5f * (in->pixel_filter_width > 0.0f ? in->pixel_filter_width : 1.0f);
+    rp.ortho = cam->orthographic ? 1 : 0;
+    {
+        // Camera::direction: -(column 2 of camera_to_world).normalized()
+        const float x = cam->camera_to_world[2], y = cam->camera_to_world[6], z = cam->camera_to_world[10];
+        const float n = std::sqrt(x * x + y * y + z * z);
+        rp.cam_dir[0] = -(x / n);
+        rp.cam_dir[1] = -(y / n);
+        rp.cam_dir[2] = -(z / n);
+    }
     rp.cam_pos[0] = cam->camera_to_world[3];
     rp.cam_pos[1] = cam->camera_to_world[7];
     rp.cam_pos[2] = cam->camera_to_world[11];

@@ -20,6 +20,8 @@ struct RenderParams
     const float *filter_cdf; // Gaussian / Blackman-Harris: filter_n conditional CDFs (filter_n + 1
                              // each), then the marginal CDF; null for the box filter
     uint32_t filter_n;
+    int ortho;          // orthographic camera: origin on the film plane, direction cam_dir
+    float cam_dir[3];   // -z of camera_to_world, normalised (Camera::direction, camera.h:24-27)
     float cam_pos[3];
     float p2w[16];
 };

@@ -109,6 +109,36 @@ ks_status ks_camera_perspective(const float camera_to_world[16], float vfov, flo
     std::memcpy(out->camera_to_world, camera_to_world, sizeof(float) * 16);
     store(p2c, out->proj_to_camera);
     store(p2w, out->proj_to_world);
+    out->orthographic = 0;
+    return KS_OK;
+}
+
+ks_status ks_camera_orthographic(const float camera_to_world[16], float left, float right, float bottom, float top,
+                                 float near_clip, float far_clip, ks_camera_desc *out)
+{
+    if (!camera_to_world || !out || !(right != left) || !(top != bottom) || !(far_clip != near_clip))
+        return KS_ERR_INVALID_ARGUMENT;
+    double c2w[4][4], w2c[4][4], proj[4][4] = {}, p2c[4][4], p2w[4][4], w2p[4][4];
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c)
+            c2w[r][c] = camera_to_world[4 * r + c];
+    if (!invert4(c2w, w2c))
+        return KS_ERR_INVALID_ARGUMENT;
+    // rev_orthographic (camera.cpp:72-83), built in float like the reference, then promoted
+    proj[0][0] = 2.0f / (right - left);
+    proj[0][3] = -(right + left) / (right - left);
+    proj[1][1] = 2.0f / (bottom - top);
+    proj[1][3] = -(top + bottom) / (bottom - top);
+    proj[2][2] = 1.0f / (far_clip - near_clip);
+    proj[2][3] = far_clip / (far_clip - near_clip);
+    proj[3][3] = 1.0f;
+    mul4(proj, w2c, w2p);
+    if (!invert4(proj, p2c) || !invert4(w2p, p2w))
+        return KS_ERR_INVALID_ARGUMENT;
+    std::memcpy(out->camera_to_world, camera_to_world, sizeof(float) * 16);
+    store(p2c, out->proj_to_camera);
+    store(p2w, out->proj_to_world);
+    out->orthographic = 1;
     return KS_OK;
 }
 

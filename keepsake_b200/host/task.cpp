@@ -902,8 +902,15 @@ void small_pt_b200(const ConfigArgs &args, const fs::path &task_dir, int task_id
             c.load_vec3("up", up);
             look_at(pos, target, up, c2w);
         }
-        if (c.load_string("type") != "perspective")
-            throw StatusError(KS_ERR_UNSUPPORTED, "config: only the perspective camera is supported");
+        const std::string ctype = c.load_string("type");
+        if (ctype == "orthographic") {
+            check(ks_camera_orthographic(c2w, c.load_float("left"), c.load_float("right"), c.load_float("bottom"),
+                                         c.load_float("top"), c.load_float("near_clip"), c.load_float("far_clip"),
+                                         &cam),
+                  nullptr, "camera");
+        } else if (ctype != "perspective") {
+            throw StatusError(KS_ERR_UNSUPPORTED, "config: camera type '" + ctype + "' is not supported");
+        } else {
         float aspect = c.load_float("aspect");
         float vfov;
         if (c.contains("vfov"))
@@ -912,6 +919,7 @@ void small_pt_b200(const ConfigArgs &args, const fs::path &task_dir, int task_id
             vfov = 2.0f * std::atan((1.0f / aspect) * std::tan(0.5f * (c.load_float("hfov") / 180.0f *
                                                                         3.14159265358979323846f)));
         check(ks_camera_perspective(c2w, vfov, aspect, &cam), nullptr, "camera");
+        }
     }
     // ---- render ----
     int device = 0;

@@ -561,7 +561,10 @@ struct Counters
 struct Camera
 {
     float c2w[16], p2w[16];
+    bool ortho = false;
     V3 position() const { return V3(c2w[3], c2w[7], c2w[11]); }
+    // Camera::direction (camera.h:24-27)
+    V3 direction() const { return -normalized(V3(c2w[2], c2w[6], c2w[10])); }
 };
 
 struct Tracer
@@ -957,6 +960,7 @@ int oracle_render(void *sp, const ks_camera_desc *cam, const ks_small_pt_params 
     Camera camera;
     std::memcpy(camera.c2w, cam->camera_to_world, sizeof(float) * 16);
     std::memcpy(camera.p2w, cam->proj_to_world, sizeof(float) * 16);
+    camera.ortho = cam->orthographic != 0;
     const int tiles_x = (cw + 3) / 4, tiles_y = (ch + 3) / 4;
     std::atomic<int> next_tile{0};
     std::atomic<uint64_t> n_ext{0}, n_shadow{0};
@@ -985,7 +989,13 @@ int oracle_render(void *sp, const ks_camera_desc *cam, const ks_small_pt_params 
                         V3 ndc(fx * 2.0f - 1.0f, fy * 2.0f - 1.0f, 1.0f);
                         V3 cp = camera.position();
                         V3 world_pos = point_hdiv(camera.p2w, ndc);
-                        V3 dir = normalized(world_pos - cp);
+                        V3 dir;
+                        if (camera.ortho) { // Camera::spawn_ray, orthographic (camera.cpp:155-160)
+                            cp = world_pos;
+                            dir = camera.direction();
+                        } else {
+                            dir = normalized(world_pos - cp);
+                        }
                         V3 L;
                         bool hit = tr.trace(cp, dir, sampler.sobol, L);
                         if (hit) {

@@ -34,6 +34,9 @@ CASES = {
                                      filter=(2, 2.0, 0.5)),
     "box_room_box_wide": dict(kind="box_room", W=48, H=48, spp=8, bounces=8, clamp_indirect=0.0,
                               filter=(0, 2.5, 0.5)),
+    # orthographic camera (camera.cpp:72-114, 155-160): left, right, bottom, top, near, far
+    "box_room_orthographic": dict(kind="box_room", W=48, H=48, spp=8, bounces=8, clamp_indirect=0.0,
+                                  ortho=(-1.1, 1.1, -1.1, 1.1, 0.1, 10.0)),
     # point and directional lights (light.cpp:208-240): delta lights after the sky in the light list
     "box_room_point_light": dict(kind="box_room", W=48, H=48, spp=16, bounces=8, clamp_indirect=0.0,
                                  lights=[(0, (3.0, 2.5, 2.0), (0.3, 1.6, 0.4))]),
@@ -53,6 +56,8 @@ def make_case(c):
         g = ks.Generated("icosphere", 0, level=c["level"], sky=c["sky"], resolution=(c["W"], c["H"]),
                          roughness=c.get("roughness", (0.05, 1.0)), occluder=c.get("occluder", False))
     cam = ks.camera_perspective(g.camera_to_world, g.vfov, g.aspect)
+    if "ortho" in c:
+        cam = ks.camera_orthographic(g.camera_to_world, *c["ortho"])
     kw = dict(render_width=c["W"], render_height=c["H"], spp=c["spp"], bounces=c["bounces"])
     if "clamp_indirect" in c:
         kw["clamp_indirect"] = c["clamp_indirect"]
@@ -104,6 +109,26 @@ def test_oracle_pixel_filters(oracle):
     for img, _ in (gau, bh):
         assert rel_mse(img, box[0]) > 1e-4
         assert abs(img.mean() / box[0].mean() - 1.0) < 0.05
+
+
+def test_oracle_orthographic_camera(oracle):
+    """Orthographic rays start on the film plane and share one direction (-z): through a 6 x 6
+    window in front of the open box room (2 x 2 cross-section, no sky), the columns and rows whose
+    rays all pass beside the room stay black and the ones looking into it are lit."""
+    import keepsake_b200 as ks
+    g, cam, p = make_case(dict(CASES["box_room_orthographic"], W=16, H=16, spp=4,
+                               ortho=(-3.0, 3.0, -3.0, 3.0, 0.1, 10.0)))
+    assert cam.orthographic == 1
+    a, w, _ = oracle.scene(g.desc).render(cam, p, threads=4)
+    img = composite(a, w).mean(-1)
+    assert np.isfinite(img).all()
+    # film x = -3 + (i + 0.5 +- 0.5) * 0.375: columns 0-3 and 12-15 lie entirely outside |x| <= 1
+    assert not img[:, :4].any() and not img[:, 12:].any()
+    assert (img[6:10, 6:10] > 0).all()
+    persp = ks.camera_perspective(g.camera_to_world, g.vfov, g.aspect)
+    assert persp.orthographic == 0
+    with pytest.raises(ks.KsError):
+        ks.camera_orthographic(g.camera_to_world, 1.0, 1.0, -1.0, 1.0, 0.1, 10.0)
 
 
 def test_oracle_delta_lights(oracle):
