@@ -43,6 +43,30 @@ const char *ks_status_string(ks_status s);
 /* Detail message of the last failing call on this context ("" if none). */
 const char *ks_last_error(const ks_context *ctx);
 
+/* Failure-detection limits of a context, for tests of the error paths (the reference aborts on its
+ * failures instead: ASSERT, cuda_check, the Embree error handler).  Each limit ends a loop that
+ * would otherwise run longer with a status code, and the context stays usable afterwards.  0
+ * keeps the library's own bound.
+ *   sbvh_max_levels:          SBVH build levels (own bound 4096) -> KS_ERR_WATCHDOG from
+ *                             ks_scene_build_bvh, the scene stays unbuilt;
+ *   wavefront_max_iterations: wavefront iterations per spp interval of a render, and per batch
+ *                             (own bound: (paths / path slots + 2) x (bounces + 2) + 64) ->
+ *                             KS_ERR_WATCHDOG from the render.
+ * ks_context_set_limits(ctx, NULL) restores the defaults. */
+typedef struct ks_context_limits {
+    uint32_t sbvh_max_levels;
+    uint32_t wavefront_max_iterations;
+} ks_context_limits;
+ks_status ks_context_set_limits(ks_context *ctx, const ks_context_limits *limits);
+
+/* The bounded mbarrier wait of the tensor-core kernels (the guide network's MMA completion wait)
+ * run on its own: one CTA initialises an mbarrier for one arrival, arrives on it when `arrive` is
+ * nonzero, and waits for its phase with at most max_polls try_wait polls.  KS_OK when the phase
+ * completed, KS_ERR_WATCHDOG when the polls ran out (nothing arrives when arrive = 0; no
+ * asynchronous operation is in flight, so the kernel returns cleanly).  No reference counterpart:
+ * it tests the timeout path that keeps a lost completion from hanging the GPU. */
+ks_status ks_mbarrier_wait_probe(ks_context *ctx, uint32_t max_polls, int arrive);
+
 /* Sobol parity hook.  For every pixel (x0..x0+nx-1, y0..y0+ny-1), sample index s0..s0+ns-1 and
  * dimension d in 0..nd-1 it starts a PTRenderSampler(full_res, pixel, spp, s, seed) at dimension d
  * (sobol.h:235-241 + start_pixel :140) and writes three floats:
@@ -74,8 +98,15 @@ typedef struct ks_mesh_desc {
                                     (geometry.cpp:94-116); NULL = dP/du of the barycentrics */
 } ks_mesh_desc;
 
-/* PrincipledBSDF with constant shader fields (principled_bsdf.cpp:707-733) plus the
- * Material::emission field (material.h:45), which the TOML task reads from an `emission` key. */
+/* A material's BSDF with constant shader fields plus the Material::emission field
+ * (material.h:45), which the TOML task reads from an `emission` key.  bsdf selects the reference
+ * type (create_bsdf, bsdf.cpp:50-62):
+ *   0 PrincipledBSDF (principled_bsdf.cpp:707-733): every field below but `specular`;
+ *   1 PrincipledBRDF (principled_bsdf.cpp:227-244): basecolor, roughness, metallic, specular,
+ *     microfacet;
+ *   2 Lambertian (bsdf.cpp:43-48): albedo = basecolor.
+ * Zero-initialise the descriptor before filling it: the fields after `emission` were added later
+ * and zero selects PrincipledBSDF; out-of-range enums are KS_ERR_INVALID_ARGUMENT. */
 typedef struct ks_material_desc {
     float basecolor[3];
     float roughness;
@@ -86,9 +117,11 @@ typedef struct ks_material_desc {
     float diffuse_trans;
     float diffuse_trans_fwd;
     float emissive[3];
-    int32_t microfacet;   /* 0 = GGX (1 = Beckmann: KS_ERR_UNSUPPORTED at ks_scene_create) */
+    int32_t microfacet;   /* 0 GGX, 1 Beckmann (microfacet.h:20-257) */
     int32_t has_emission; /* Material::emission != nullptr */
     float emission[3];
+    int32_t bsdf;         /* 0 principled_bsdf, 1 principled_brdf, 2 lambertian */
+    float specular;       /* principled_brdf: specular, clamped to [0, 1] and scaled by 0.08 */
 } ks_material_desc;
 
 /* SkyLight (light.h:34-58): ambient colour or a lat-long RGB map. */
@@ -195,13 +228,28 @@ ks_status ks_trace_rays_wide(ks_scene *scene, const float *rays, uint32_t n, int
  * budget through its own allocator, or a frame loop that forbids cudaMalloc/cudaFree).  Rays and
  * results are staged in one static device array of the library (KS_TRACE_NOALLOC_MAX_RAYS rays,
  * 3.4 MB, resident on every GPU that loads the library until the process exits); larger n is
- * rejected with KS_ERR_INVALID_ARGUMENT.  The first call on a device looks up that array's
- * device address (cudaGetSymbolAddress): make that first call before any stream capture.  All
- * calls share the array, so calls that overlap on the GPU (two contexts on one device, two
- * threads) race; serialise them. */
+ * rejected with KS_ERR_INVALID_ARGUMENT.  Each call returns once the results are in the caller's
+ * host arrays.  The first call on a device looks up that array's device address
+ * (cudaGetSymbolAddress) and keeps it for the life of the process: make that first call before
+ * any stream capture begins, and do not reset the device (cudaDeviceReset) between calls, which
+ * would leave the kept address stale.  All calls share the array, so calls that overlap on the
+ * GPU (two contexts on one device, two threads) race; serialise them. */
 #define KS_TRACE_NOALLOC_MAX_RAYS 65536
 ks_status ks_trace_rays_noalloc(ks_scene *scene, const float *rays, uint32_t n, int any_hit, int culling,
                                 uint32_t *tri_idx, float *t, float *bary);
+
+/* BSDF parity hooks: the renderer's own device BSDF code (the shading unit's arithmetic) over
+ * host batches of directions in the local shading frame (z = shading normal).
+ * ks_bsdf_eval: per pair (wo, wi) the cosine-weighted value f cos(theta_i) (3 floats) and the
+ * pdf of sampling wi (BSDF::eval_and_pdf, bsdf.h:14-22; PrincipledBSDF::eval_and_pdf,
+ * principled_bsdf.cpp:297-307).  ks_bsdf_sample: per (wo, u) with u = (u_lobe, u_wi.x, u_wi.y) the
+ * sampled wi, the throughput weight f cos / pdf (3 floats) and the pdf (BSDF::sample, bsdf.h:18-21;
+ * PrincipledBSDF::sample, principled_bsdf.cpp:326-393); wi = 0, weight 0 and pdf 0 where the
+ * reference returns no sample.  Arrays hold 3 floats per entry (pdf: 1), host memory, n <= 2^26. */
+ks_status ks_bsdf_eval(ks_context *ctx, const ks_material_desc *material, const float *wo, const float *wi,
+                       uint32_t n, float *f, float *pdf);
+ks_status ks_bsdf_sample(ks_context *ctx, const ks_material_desc *material, const float *wo, const float *u,
+                         uint32_t n, float *wi, float *weight, float *pdf);
 
 /* ---------------------------------------------------------------------------------------------
  * Camera.  The render consumes the matrices of a reference `Camera` (camera.cpp:85-94):
@@ -212,7 +260,10 @@ typedef struct ks_camera_desc {
     float camera_to_world[16];
     float proj_to_camera[16];
     float proj_to_world[16];
-    int32_t orthographic; /* 1: rays start on the film plane and share the view direction */
+    int32_t orthographic; /* 1: rays start on the film plane and share the view direction; 0:
+                             perspective.  Fill descriptors with ks_camera_perspective /
+                             ks_camera_orthographic (or zero-initialise them): any other value is
+                             KS_ERR_INVALID_ARGUMENT at render time. */
 } ks_camera_desc;
 
 /* Orthographic camera (Camera's orthographic constructor with rev_orthographic, camera.cpp:72-

@@ -107,6 +107,38 @@ class Context:
                    "ks_image_rel_mse_device")
         return float(out[0])
 
+    def set_limits(self, sbvh_max_levels=0, wavefront_max_iterations=0):
+        """ks_context_set_limits: failure-detection limits (0 = the library's own bound)."""
+        lim = ContextLimits(sbvh_max_levels, wavefront_max_iterations)
+        self.check(lib.ks_context_set_limits(self.handle, ctypes.byref(lim)), "ks_context_set_limits")
+
+    def mbarrier_probe(self, max_polls, arrive) -> int:
+        """ks_mbarrier_wait_probe: the status (KS_OK or KS_ERR_WATCHDOG) of a bounded mbarrier wait."""
+        return lib.ks_mbarrier_wait_probe(self.handle, max_polls, int(arrive))
+
+    def bsdf_eval(self, material, wo, wi):
+        """ks_bsdf_eval: (f cos [n, 3], pdf [n]) of the device BSDF code for local directions."""
+        wo = np.ascontiguousarray(wo, np.float32)
+        wi = np.ascontiguousarray(wi, np.float32)
+        n = len(wo)
+        f = np.empty((n, 3), np.float32)
+        pdf = np.empty(n, np.float32)
+        self.check(lib.ks_bsdf_eval(self.handle, ctypes.byref(material), ptr(wo), ptr(wi), n, ptr(f), ptr(pdf)),
+                   "ks_bsdf_eval")
+        return f, pdf
+
+    def bsdf_sample(self, material, wo, u):
+        """ks_bsdf_sample: (wi [n, 3], weight f cos / pdf [n, 3], pdf [n]) for u = (u_lobe, u0, u1)."""
+        wo = np.ascontiguousarray(wo, np.float32)
+        u = np.ascontiguousarray(u, np.float32)
+        n = len(wo)
+        wi = np.empty((n, 3), np.float32)
+        beta = np.empty((n, 3), np.float32)
+        pdf = np.empty(n, np.float32)
+        self.check(lib.ks_bsdf_sample(self.handle, ctypes.byref(material), ptr(wo), ptr(u), n, ptr(wi), ptr(beta),
+                                      ptr(pdf)), "ks_bsdf_sample")
+        return wi, beta, pdf
+
     def sobol_points(self, full_w, full_h, spp, seed, x0, y0, nx, ny, s0, ns, nd) -> np.ndarray:
         out = np.empty((ny, nx, ns, nd, 3), dtype=np.float32)
         st = lib.ks_sobol_points(self.handle, full_w, full_h, spp, seed, x0, y0, nx, ny, s0, ns, nd, ptr(out))
@@ -127,7 +159,7 @@ class MaterialDesc(ctypes.Structure):
     _fields_ = [("basecolor", _f32 * 3), ("roughness", _f32), ("metallic", _f32), ("ior", _f32),
                 ("specular_r0_mul", _f32), ("specular_trans", _f32), ("diffuse_trans", _f32),
                 ("diffuse_trans_fwd", _f32), ("emissive", _f32 * 3), ("microfacet", _i32),
-                ("has_emission", _i32), ("emission", _f32 * 3)]
+                ("has_emission", _i32), ("emission", _f32 * 3), ("bsdf", _i32), ("specular", _f32)]
 
 
 class SkyDesc(ctypes.Structure):
@@ -153,6 +185,10 @@ class SceneDesc(ctypes.Structure):
                 ("prototypes", ctypes.POINTER(PrototypeDesc)), ("n_prototypes", _u32),
                 ("instances", ctypes.POINTER(InstanceDesc)), ("n_instances", _u32),
                 ("lights", ctypes.POINTER(LightDesc)), ("n_lights", _u32)]
+
+
+class ContextLimits(ctypes.Structure):
+    _fields_ = [("sbvh_max_levels", _u32), ("wavefront_max_iterations", _u32)]
 
 
 class SBVHOptions(ctypes.Structure):
@@ -196,6 +232,10 @@ def _sig(name, args, res=ctypes.c_int):
 
 
 _sig("ks_scene_create", [_vp, ctypes.POINTER(SceneDesc), ctypes.POINTER(_vp)])
+_sig("ks_bsdf_eval", [_vp, ctypes.POINTER(MaterialDesc), _vp, _vp, _u32, _vp, _vp])
+_sig("ks_context_set_limits", [_vp, ctypes.POINTER(ContextLimits)])
+_sig("ks_mbarrier_wait_probe", [_vp, _u32, ctypes.c_int])
+_sig("ks_bsdf_sample", [_vp, ctypes.POINTER(MaterialDesc), _vp, _vp, _u32, _vp, _vp, _vp])
 _sig("ks_scene_destroy", [_vp], None)
 _sig("ks_scene_build_bvh", [_vp, ctypes.POINTER(SBVHOptions), ctypes.POINTER(_f32)])
 _sig("ks_sbvh_counts", [_vp, ctypes.POINTER(_u32), ctypes.POINTER(_u32)])

@@ -79,6 +79,14 @@ void ks_context_destroy(ks_context *ctx)
 
 const char *ks_last_error(const ks_context *ctx) { return ctx ? ctx->last_error.c_str() : ""; }
 
+ks_status ks_context_set_limits(ks_context *ctx, const ks_context_limits *limits)
+{
+    if (!ctx)
+        return KS_ERR_INVALID_ARGUMENT;
+    ctx->limits = limits ? *limits : ks_context_limits{};
+    return KS_OK;
+}
+
 } // extern "C"
 
 namespace

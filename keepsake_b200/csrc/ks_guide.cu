@@ -683,12 +683,44 @@ ks_status train_rows(ks_guide *g, uint32_t n, const float4 *pos, const float4 *w
 
 ks_status status(ks_guide *g) { return check_err(g); }
 
+// The bounded completion wait of wait_mma on its own: one mbarrier for one arrival, which one
+// thread makes when `arrive` is set; every thread then polls the phase at most max_polls times.
+__global__ void k_mbarrier_probe(uint32_t max_polls, int arrive, int *timed_out)
+{
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0)
+        tc::mbar_init(&bar, 1);
+    __syncthreads();
+    if (arrive && threadIdx.x == 0)
+        tc::mbar_arrive(&bar);
+    if (!tc::mbar_wait_bounded(&bar, 0, max_polls))
+        atomicOr(timed_out, 1);
+}
+
 } // namespace guide_impl
 } // namespace ksb
 
 using namespace ksb::guide_impl;
 
 extern "C" {
+
+ks_status ks_mbarrier_wait_probe(ks_context *ctx, uint32_t max_polls, int arrive)
+{
+    if (!ctx || max_polls == 0)
+        return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_mbarrier_wait_probe: null context or zero polls");
+    KS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    DevBuf<int> flag;
+    KS_CUDA_TRY(ctx, flag.alloc(1));
+    KS_CUDA_TRY(ctx, cudaMemsetAsync(flag.ptr, 0, sizeof(int), ctx->stream));
+    k_mbarrier_probe<<<1, 64, 0, ctx->stream>>>(max_polls, arrive, flag.ptr);
+    KS_CUDA_TRY(ctx, cudaGetLastError());
+    int timed_out = 0;
+    KS_CUDA_TRY(ctx, cudaMemcpyAsync(&timed_out, flag.ptr, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    KS_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (timed_out)
+        return fail(ctx, KS_ERR_WATCHDOG, "ks_mbarrier_wait_probe: the bounded wait ran out of polls");
+    return KS_OK;
+}
 
 ks_status ks_guide_create(ks_context *ctx, const ks_guide_params *params, ks_guide **out)
 {

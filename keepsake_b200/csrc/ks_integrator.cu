@@ -884,6 +884,9 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
     if ((uint64_t)W * H >= (1ull << 31))
         return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_small_pt_render: resolution too large");
     RenderParams rp{};
+    if (cam->orthographic != 0 && cam->orthographic != 1)
+        return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_small_pt_render: camera.orthographic must be 0 or 1 (fill the "
+                                                  "descriptor with ks_camera_perspective / ks_camera_orthographic)");
     if (!fill_params(cam, in, rp))
         return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_small_pt_render: empty crop window");
     std::vector<float> ftab;
@@ -891,7 +894,7 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
         return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_small_pt_render: bad pixel filter");
 
     SceneView sv = make_view(scene);
-    const bool attribs = sv.normals != nullptr || sv.texcoords != nullptr;
+    const int variant = sv.shade_variant;
     const uint32_t n_pix = (uint32_t)rp.cw * (uint32_t)rp.ch;
     const uint64_t max_interval = (uint64_t)n_pix * (uint64_t)std::min(in->spp, in->spp_prog_interval);
     RenderCache &rc = render_cache(ctx);
@@ -1011,7 +1014,9 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
         uint64_t total = (uint64_t)n_pix * (uint64_t)batch, issued = 0;
         uint32_t cur_count = 0;
         // every path ends after at most bounces + 1 extension rays
-        const uint64_t watchdog = (total / w.capacity + 2) * (uint64_t)(in->bounces + 2) + 64;
+        uint64_t watchdog = (total / w.capacity + 2) * (uint64_t)(in->bounces + 2) + 64;
+        if (ctx->limits.wavefront_max_iterations)
+            watchdog = std::min<uint64_t>(watchdog, ctx->limits.wavefront_max_iterations);
         uint64_t it_interval = 0;
         while ((issued < total || cur_count > 0) && err == cudaSuccess) {
             if (++it_interval > watchdog) {
@@ -1088,7 +1093,7 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
             for (int miss = 1; miss >= 0; --miss) {
                 if (!miss && guiding)
                     cudaStreamWaitEvent(st, ev_join, 0);
-                launch_shade(miss != 0, guide != nullptr, false, attribs, grid, st, sv, rp, pb[cur], pb[1 - cur], w.hits.ptr,
+                launch_shade(miss != 0, guide != nullptr, false, variant, grid, st, sv, rp, pb[cur], pb[1 - cur], w.hits.ptr,
                              w.hit_inst.ptr, w.samples.ptr, w.queue[miss].ptr, w.counters.ptr + 2 + miss,
                              w.counters.ptr, sb, w.counters.ptr + 1, d_accum, d_weights, gv, BatchView{});
             }
@@ -1236,7 +1241,7 @@ struct BatchWork
     DevBuf<BatchState> state_dev;
     DevBuf<float> filters; // the jobs' pixel-filter sample tables, concatenated
     unsigned ext_grid = 0, shadow_grid = 0; // one wave of resident CTAs of the traversal kernels
-    bool attribs = false;                   // some job's scene has vertex normals or texcoords
+    int variant = kShadePlain;              // the shading kernel variant of the most demanding job
 };
 
 // Validates the jobs and fills the per-job tables; returns the total path count in *total.
@@ -1252,7 +1257,7 @@ static ks_status batch_tables(ks_context *ctx, const ks_batch_job *jobs, uint32_
     std::vector<float> filter_host;
     std::vector<size_t> filter_off(n, 0);
     *max_bounces = 0;
-    w.attribs = false;
+    w.variant = kShadePlain;
     for (uint32_t j = 0; j < n; ++j) {
         const ks_batch_job &jb = jobs[j];
         const ks_small_pt_params &in = jb.params;
@@ -1269,6 +1274,9 @@ static ks_status batch_tables(ks_context *ctx, const ks_batch_job *jobs, uint32_
             (uint64_t)in.render_width * in.render_height > (1ull << kJobShift))
             return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_batch_render_device: job " + std::to_string(j) +
                                                           ": bad resolution (at most 2^21 pixels), spp or bounces");
+        if (jb.camera.orthographic != 0 && jb.camera.orthographic != 1)
+            return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_batch_render_device: job " + std::to_string(j) +
+                                                          ": camera.orthographic must be 0 or 1");
         if (!fill_params(&jb.camera, &in, params[j]))
             return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_batch_render_device: empty crop window");
         std::vector<float> ftab;
@@ -1278,7 +1286,7 @@ static ks_status batch_tables(ks_context *ctx, const ks_batch_job *jobs, uint32_
         filter_off[j] = filter_host.size();
         filter_host.insert(filter_host.end(), ftab.begin(), ftab.end());
         views[j] = make_view(jb.scene);
-        w.attribs |= views[j].normals != nullptr || views[j].texcoords != nullptr;
+        w.variant = std::max(w.variant, views[j].shade_variant);
         acc[j] = jb.accum_rgb_device;
         wts[j] = jb.weights_device;
         begin[j + 1] = begin[j] + (unsigned long long)params[j].cw * params[j].ch * (unsigned long long)in.spp;
@@ -1323,7 +1331,7 @@ static void batch_iteration(ks_context *ctx, BatchWork &w, const BatchView &bv, 
     launch_sample(true, grid, st, SceneView{}, RenderParams{}, pb[cur], w.hits.ptr, nullptr, w.queue[0].ptr, cnt + 2,
                   w.samples.ptr, bv);
     for (int miss = 0; miss < 2; ++miss)
-        launch_shade(miss != 0, false, true, w.attribs, grid, st, SceneView{}, RenderParams{}, pb[cur], pb[1 - cur], w.hits.ptr,
+        launch_shade(miss != 0, false, true, w.variant, grid, st, SceneView{}, RenderParams{}, pb[cur], pb[1 - cur], w.hits.ptr,
                      nullptr, w.samples.ptr, w.queue[miss].ptr, cnt + 2 + miss, cnt, sb, cnt + 1, nullptr, nullptr,
                      gv, bv);
     k_shadow_pt<true><<<w.shadow_grid, 128, 0, st>>>(SceneView{}, sb, cnt + 1, cnt + 5, pb[1 - cur], nullptr, nullptr,
@@ -1365,6 +1373,8 @@ static ks_status batch_render(ks_context *ctx, const ks_batch_job *jobs, uint32_
     // every path ends after at most bounces + 1 extension rays
     init.max_iterations = (uint32_t)std::min<unsigned long long>((total / capacity + 2) * (max_bounces + 2) + 64,
                                                                   0x7fffffffull);
+    if (ctx->limits.wavefront_max_iterations)
+        init.max_iterations = std::min(init.max_iterations, ctx->limits.wavefront_max_iterations);
     KS_CUDA_TRY(ctx, cudaMemcpyAsync(w.state_dev.ptr, &init, sizeof(init), cudaMemcpyHostToDevice, st));
     KS_CUDA_TRY(ctx, cudaMemsetAsync(w.counters.ptr, 0, sizeof(uint32_t) * kCounters, st));
     KS_CUDA_TRY(ctx, cudaMemsetAsync(w.overflow.ptr, 0, sizeof(int), st));

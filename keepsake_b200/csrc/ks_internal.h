@@ -16,6 +16,8 @@ struct ks_context
     // buffers the renders and the SBVH builder keep between calls (owned by ks_integrator.cu and
     // ks_sbvh_build.cu; freed at destroy)
     std::shared_ptr<void> render_cache, build_cache;
+    // failure-detection limits (ks_context_set_limits; 0 = the library's own bound)
+    ks_context_limits limits{};
 };
 
 namespace ksb

@@ -261,6 +261,9 @@ SceneView make_view(const ks_scene *s)
     v.normals = s->normals.ptr;
     v.texcoords = s->texcoords.ptr;
     v.materials = s->materials.ptr;
+    v.shade_variant = s->ext_materials ? kShadeGeneral
+                      : (s->normals.ptr != nullptr || s->texcoords.ptr != nullptr) ? kShadeAttribs
+                                                                                     : kShadePlain;
     v.light_count = s->light_count;
     v.n_nonmesh = s->n_nonmesh;
     v.n_sky = (s->sky_desc.kind == 1 || s->sky_desc.kind == 2) ? 1u : 0u;

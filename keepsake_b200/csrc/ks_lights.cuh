@@ -14,6 +14,13 @@ namespace ksb
 {
 
 // Flat, read-only view of everything the shading kernels read (passed by value).
+enum : int
+{
+    kShadePlain = 0,
+    kShadeAttribs = 1,
+    kShadeGeneral = 2
+};
+
 struct SceneView
 {
     InstanceView inst; // instances (inst.n == 0: flat scene)
@@ -30,6 +37,9 @@ struct SceneView
     const float *normals;    // global vertex normals (3 floats each; null when no mesh shades smooth)
     const float *texcoords;  // global texture coordinates (2 floats each; null when no mesh has them)
     const MaterialGPU *materials;
+    // the shading kernel variant the scene needs: kShadePlain; kShadeAttribs for vertex normals or
+    // texcoords; kShadeGeneral for a material other than the GGX PrincipledBSDF
+    int shade_variant;
     // lights
     uint32_t light_count;
     uint32_t n_nonmesh; // the sky (light 0, when there is one) and the point / directional lights

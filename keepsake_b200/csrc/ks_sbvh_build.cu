@@ -1015,7 +1015,7 @@ static ks_status build_range(ks_context *ctx, const float *verts, const uint32_t
         std::swap(cur_buf, nxt_buf);
         std::swap(cur_nodes, nxt_nodes);
         ++level;
-        if (level > 4096)
+        if ((uint32_t)level > (ctx->limits.sbvh_max_levels ? ctx->limits.sbvh_max_levels : 4096u))
             return fail(ctx, KS_ERR_WATCHDOG, "sbvh build: level limit reached");
     }
     (void)n_refs;

@@ -192,10 +192,37 @@ bool valid_material(const ks_material_desc &m)
         if (!finite(m.basecolor[c]) || !finite(m.emission[c]))
             return false;
     return finite(m.roughness) && finite(m.metallic) && finite(m.ior) && finite(m.specular_r0_mul) &&
-           finite(m.specular_trans) && finite(m.diffuse_trans) && finite(m.diffuse_trans_fwd);
+           finite(m.specular_trans) && finite(m.diffuse_trans) && finite(m.diffuse_trans_fwd) &&
+           finite(m.specular);
 }
 
 } // namespace
+
+// The device copy of a material; false for a non-finite field or an enum out of range.
+bool ksb::material_to_gpu(const ks_material_desc &m, MaterialGPU &g)
+{
+    if (!valid_material(m) || m.microfacet < 0 || m.microfacet > 1 || m.bsdf < 0 || m.bsdf > 2 ||
+        m.has_emission < 0 || m.has_emission > 1)
+        return false;
+    g = MaterialGPU{};
+    for (int c = 0; c < 3; ++c) {
+        g.basecolor[c] = m.basecolor[c];
+        g.emission[c] = m.emission[c];
+    }
+    g.roughness = m.roughness;
+    g.metallic = m.metallic;
+    g.ior = m.ior;
+    g.specular_r0_mul = m.specular_r0_mul;
+    g.specular_trans = m.specular_trans;
+    g.diffuse_trans = m.diffuse_trans;
+    g.diffuse_trans_fwd = m.diffuse_trans_fwd;
+    g.microfacet = m.microfacet;
+    g.bsdf = m.bsdf;
+    g.specular = m.specular;
+    g.has_emission = m.has_emission;
+    g.mesh_light = -1;
+    return true;
+}
 
 extern "C" {
 
@@ -296,13 +323,14 @@ ks_status ks_scene_create(ks_context *ctx, const ks_scene_desc *desc, ks_scene *
     }
     if (n_tris >= (1ull << 30) || n_verts >= (1ull << 31))
         return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_create: scene too large");
-    for (uint32_t k = 0; k < desc->n_materials; ++k)
-        if (!valid_material(desc->materials[k]))
-            return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_create: non-finite material field");
-    for (uint32_t k = 0; k < desc->n_materials; ++k)
-        if (desc->materials[k].microfacet != 0)
-            return fail(ctx, KS_ERR_UNSUPPORTED, "ks_scene_create: only the GGX microfacet distribution is supported "
-                                                 "(material " + std::to_string(k) + ")");
+    for (uint32_t k = 0; k < desc->n_materials; ++k) {
+        MaterialGPU g;
+        if (!material_to_gpu(desc->materials[k], g))
+            return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_create: material " + std::to_string(k) +
+                                                          ": a non-finite field, or microfacet, bsdf or "
+                                                          "has_emission out of range (zero-initialise the "
+                                                          "descriptor)");
+    }
     KS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
     ks_scene *s = new (std::nothrow) ks_scene();
     if (!s)
@@ -379,21 +407,8 @@ ks_status ks_scene_create(ks_context *ctx, const ks_scene_desc *desc, ks_scene *
     std::vector<MaterialGPU> mats(desc->n_materials);
     for (uint32_t k = 0; k < desc->n_materials; ++k) {
         const ks_material_desc &m = desc->materials[k];
-        MaterialGPU &g = mats[k];
-        for (int c = 0; c < 3; ++c) {
-            g.basecolor[c] = m.basecolor[c];
-            g.emission[c] = m.emission[c];
-        }
-        g.roughness = m.roughness;
-        g.metallic = m.metallic;
-        g.ior = m.ior;
-        g.specular_r0_mul = m.specular_r0_mul;
-        g.specular_trans = m.specular_trans;
-        g.diffuse_trans = m.diffuse_trans;
-        g.diffuse_trans_fwd = m.diffuse_trans_fwd;
-        g.microfacet = m.microfacet;
-        g.has_emission = m.has_emission;
-        g.mesh_light = -1;
+        material_to_gpu(m, mats[k]);
+        s->ext_materials |= m.bsdf != 0 || m.microfacet != 0;
     }
     cudaError_t e = s->materials.alloc(mats.size());
     if (e == cudaSuccess)

@@ -57,10 +57,12 @@ struct MaterialGPU
 {
     float basecolor[3];
     float roughness, metallic, ior, specular_r0_mul, specular_trans, diffuse_trans, diffuse_trans_fwd;
-    int microfacet;
+    int microfacet; // 0 GGX, 1 Beckmann
     int has_emission;
     float emission[3];
     int mesh_light; // index of the MeshLightShared for emissive meshes, -1 otherwise
+    int bsdf;       // 0 PrincipledBSDF, 1 PrincipledBRDF, 2 Lambertian (albedo = basecolor)
+    float specular; // PrincipledBRDF's specular field
 };
 
 struct SceneHost
@@ -106,6 +108,7 @@ struct ks_scene
     ksb::DevBuf<ksb::MaterialGPU> materials;
     ksb::DevBuf<uint32_t> mesh_material;
     ksb::DevBuf<int> mesh_flags;
+    bool ext_materials = false; // some material is not a GGX PrincipledBSDF
     // per-vertex shading attributes, indexed like verts (allocated only when some mesh has them)
     ksb::DevBuf<float> normals;   // 3 per vertex: MeshData::vertex_normals of smooth-shaded meshes
     ksb::DevBuf<float> texcoords; // 2 per vertex: MeshData::texcoords
@@ -144,6 +147,7 @@ struct ks_scene
 
 namespace ksb
 {
+bool material_to_gpu(const ks_material_desc &m, MaterialGPU &g);
 ks_status build_sbvh(ks_scene *scene, const ks_sbvh_options &opts, float *build_ms);
 ks_status build_lights(ks_scene *scene);
 }

@@ -13,6 +13,8 @@
 #include "ks_sampler.cuh"
 #include "ks_wavefront.cuh"
 
+#include <type_traits>
+
 namespace ksb
 {
 namespace
@@ -152,8 +154,11 @@ __global__ void __launch_bounds__(128) k_sample(const __grid_constant__ SceneVie
 // probability that its emitter-hit weight includes, and the two only stay the same functions of
 // the direction if both keep seeing the BSDF pdf.
 // kBatch: paths of many jobs; the view, parameters and accumulators of a path's job come from bv.
-// kAttribs: meshes may carry vertex normals (smooth shading frames) and texcoords (tangents).
-template <bool kMiss, bool kGuided, bool kBatch = false, bool kAttribs = false>
+// kVariant (kShadePlain, kShadeAttribs, kShadeGeneral): kShadeAttribs lets meshes carry vertex
+// normals (smooth shading frames) and texcoords (tangents); kShadeGeneral also takes materials of
+// any BSDF kind (AnyBsdf).  The plain variant's materials are all GGX PrincipledBSDFs, whose code
+// alone keeps the kernel's register budget; each variant keeps the spills of its own features.
+template <bool kMiss, bool kGuided, bool kBatch = false, int kVariant = kShadePlain>
 __global__ void __launch_bounds__(128, KS_SHADE_MIN_BLOCKS) k_shade(const __grid_constant__ SceneView sv_in,
                                                const __grid_constant__ RenderParams rp_in, PathBuf cur, PathBuf nxt,
                                                const float4 *hits, const uint32_t *hit_inst,
@@ -239,7 +244,7 @@ __global__ void __launch_bounds__(128, KS_SHADE_MIN_BLOCKS) k_shade(const __grid
                 }
                 uint32_t mesh = __ldg(&sv.tri_mesh[tri]);
                 const MaterialGPU &mat = sv.materials[__ldg(&sv.mesh_material[mesh])];
-                ShadeFrame it = hit_frame<kAttribs>(sv, tri, __ldg(&sv.mesh_flags[mesh]), p0, p1, p2, h.y, h.z, rd,
+                ShadeFrame it = hit_frame<(kVariant >= kShadeAttribs)>(sv, tri, __ldg(&sv.mesh_flags[mesh]), p0, p1, p2, h.y, h.z, rd,
                                           sv.inst.n ? m : nullptr);
                 // emitter hit (small_pt.cpp:112-138)
                 if (mat.has_emission && sv.tri_light) {
@@ -272,7 +277,7 @@ __global__ void __launch_bounds__(128, KS_SHADE_MIN_BLOCKS) k_shade(const __grid
                     finish = true;
                 } else {
                     f3 wo = -normalize(rd);
-                    Principled bsdf{make_closure(mat)};
+                    const std::conditional_t<kVariant == kShadeGeneral, AnyBsdf, Principled> bsdf{make_closure(mat)};
                     // this bounce's Sobol values and light sample, drawn by k_sample
                     const float4 sa = samples[4 * (size_t)i], sl = samples[4 * (size_t)i + 1];
                     const float4 se = samples[4 * (size_t)i + 2];
@@ -430,6 +435,76 @@ __global__ void __launch_bounds__(128, KS_SHADE_MIN_BLOCKS) k_shade(const __grid
     }
 }
 
+// BSDF parity hooks: the shading kernels' BSDF code (AnyBsdf, compiled in this fast-math unit)
+// on batches of local directions.
+__global__ void k_bsdf_eval(const MaterialGPU m, const float *wo, const float *wi, uint32_t n, float *f, float *pdf)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const AnyBsdf b{make_closure(m)};
+    f3 fv;
+    float p;
+    b.eval_and_pdf(mk(wo[3 * i], wo[3 * i + 1], wo[3 * i + 2]), mk(wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]), fv, p);
+    f[3 * i] = fv.x;
+    f[3 * i + 1] = fv.y;
+    f[3 * i + 2] = fv.z;
+    pdf[i] = p;
+}
+
+__global__ void k_bsdf_sample(const MaterialGPU m, const float *wo, const float *u, uint32_t n, float *wi,
+                              float *beta, float *pdf)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const AnyBsdf b{make_closure(m)};
+    f3 w = mk(0, 0, 0);
+    float p = 0.0f;
+    const f3 bt = b.sample(mk(wo[3 * i], wo[3 * i + 1], wo[3 * i + 2]), w, u[3 * i], u[3 * i + 1], u[3 * i + 2], p);
+    wi[3 * i] = w.x;
+    wi[3 * i + 1] = w.y;
+    wi[3 * i + 2] = w.z;
+    beta[3 * i] = bt.x;
+    beta[3 * i + 1] = bt.y;
+    beta[3 * i + 2] = bt.z;
+    pdf[i] = p;
+}
+
+// Runs one of the hooks over host arrays of n entries: two inputs of 3 floats each, outputs of 3
+// floats (out3a, and out3b when sampling) and of one float, copied back.
+template <class Launch>
+ks_status bsdf_hook(ks_context *ctx, const ks_material_desc *mat, uint32_t n, const float *in0, const float *in1,
+                    float *out3a, float *out3b, bool sampling, float *out1, Launch launch, const char *what)
+{
+    if (!ctx || !mat || (n && (!in0 || !in1 || !out3a || !out1 || (sampling && !out3b))))
+        return fail(ctx, KS_ERR_INVALID_ARGUMENT, std::string(what) + ": null argument");
+    if (n > (1u << 26))
+        return fail(ctx, KS_ERR_INVALID_ARGUMENT, std::string(what) + ": at most 2^26 entries per call");
+    if (n == 0)
+        return KS_OK;
+    MaterialGPU g;
+    if (!material_to_gpu(*mat, g))
+        return fail(ctx, KS_ERR_INVALID_ARGUMENT, std::string(what) + ": invalid material");
+    KS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    const size_t v3 = 3 * (size_t)n * sizeof(float);
+    DevBuf<float> buf;
+    KS_CUDA_TRY(ctx, buf.alloc(3 * 3 * (size_t)n + 3 * (size_t)n + n));
+    float *d_in0 = buf.ptr, *d_in1 = d_in0 + 3 * (size_t)n, *d_a = d_in1 + 3 * (size_t)n, *d_b = d_a + 3 * (size_t)n,
+          *d_p = d_b + 3 * (size_t)n;
+    cudaStream_t st = ctx->stream;
+    KS_CUDA_TRY(ctx, cudaMemcpyAsync(d_in0, in0, v3, cudaMemcpyHostToDevice, st));
+    KS_CUDA_TRY(ctx, cudaMemcpyAsync(d_in1, in1, v3, cudaMemcpyHostToDevice, st));
+    launch((n + 127) / 128, st, g, d_in0, d_in1, d_a, d_b, d_p);
+    KS_CUDA_TRY(ctx, cudaGetLastError());
+    KS_CUDA_TRY(ctx, cudaMemcpyAsync(out3a, d_a, v3, cudaMemcpyDeviceToHost, st));
+    if (sampling)
+        KS_CUDA_TRY(ctx, cudaMemcpyAsync(out3b, d_b, v3, cudaMemcpyDeviceToHost, st));
+    KS_CUDA_TRY(ctx, cudaMemcpyAsync(out1, d_p, n * sizeof(float), cudaMemcpyDeviceToHost, st));
+    KS_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    return KS_OK;
+}
+
 } // namespace
 
 namespace wave
@@ -445,7 +520,7 @@ void launch_sample(bool batch, unsigned grid, cudaStream_t st, const SceneView &
         k_sample<false><<<grid, 128, 0, st>>>(sv, rp, cur, hits, hit_inst, queue, queue_count, samples, bv);
 }
 
-void launch_shade(bool miss, bool guided, bool batch, bool attribs, unsigned grid, cudaStream_t st,
+void launch_shade(bool miss, bool guided, bool batch, int variant, unsigned grid, cudaStream_t st,
                   const SceneView &sv, const RenderParams &rp, PathBuf cur, PathBuf nxt, const float4 *hits,
                   const uint32_t *hit_inst, const float4 *samples, const uint32_t *queue, const uint32_t *queue_count,
                   uint32_t *next_count, ShadowBuf sb, uint32_t *shadow_count, double *accum, double *weights,
@@ -453,30 +528,60 @@ void launch_shade(bool miss, bool guided, bool batch, bool attribs, unsigned gri
 {
 #define KS_SHADE_ARGS                                                                                              \
     sv, rp, cur, nxt, hits, hit_inst, samples, queue, queue_count, next_count, sb, shadow_count, accum, weights, gv, bv
+#define KS_SHADE_HIT(G, B)                                                                                         \
+    do {                                                                                                           \
+        if (variant == kShadeGeneral)                                                                             \
+            k_shade<false, G, B, kShadeGeneral><<<grid, 128, 0, st>>>(KS_SHADE_ARGS);                              \
+        else if (variant == kShadeAttribs)                                                                        \
+            k_shade<false, G, B, kShadeAttribs><<<grid, 128, 0, st>>>(KS_SHADE_ARGS);                              \
+        else                                                                                                       \
+            k_shade<false, G, B, kShadePlain><<<grid, 128, 0, st>>>(KS_SHADE_ARGS);                                \
+    } while (0)
     if (batch) {
         if (miss)
             k_shade<true, false, true><<<grid, 128, 0, st>>>(KS_SHADE_ARGS);
-        else if (attribs)
-            k_shade<false, false, true, true><<<grid, 128, 0, st>>>(KS_SHADE_ARGS);
         else
-            k_shade<false, false, true><<<grid, 128, 0, st>>>(KS_SHADE_ARGS);
+            KS_SHADE_HIT(false, true);
     } else if (guided) {
         if (miss)
             k_shade<true, true><<<grid, 128, 0, st>>>(KS_SHADE_ARGS);
-        else if (attribs)
-            k_shade<false, true, false, true><<<grid, 128, 0, st>>>(KS_SHADE_ARGS);
         else
-            k_shade<false, true><<<grid, 128, 0, st>>>(KS_SHADE_ARGS);
+            KS_SHADE_HIT(true, false);
     } else {
         if (miss)
             k_shade<true, false><<<grid, 128, 0, st>>>(KS_SHADE_ARGS);
-        else if (attribs)
-            k_shade<false, false, false, true><<<grid, 128, 0, st>>>(KS_SHADE_ARGS);
         else
-            k_shade<false, false><<<grid, 128, 0, st>>>(KS_SHADE_ARGS);
+            KS_SHADE_HIT(false, false);
     }
+#undef KS_SHADE_HIT
 #undef KS_SHADE_ARGS
 }
 
 } // namespace wave
 } // namespace ksb
+
+extern "C" {
+
+ks_status ks_bsdf_eval(ks_context *ctx, const ks_material_desc *mat, const float *wo, const float *wi, uint32_t n,
+                       float *f, float *pdf)
+{
+    using namespace ksb;
+    return bsdf_hook(ctx, mat, n, wo, wi, f, nullptr, false, pdf,
+                     [n](unsigned grid, cudaStream_t st, const MaterialGPU &g, const float *a, const float *b,
+                         float *oa, float *, float *op) { k_bsdf_eval<<<grid, 128, 0, st>>>(g, a, b, n, oa, op); },
+                     "ks_bsdf_eval");
+}
+
+ks_status ks_bsdf_sample(ks_context *ctx, const ks_material_desc *mat, const float *wo, const float *u, uint32_t n,
+                         float *wi, float *beta, float *pdf)
+{
+    using namespace ksb;
+    return bsdf_hook(ctx, mat, n, wo, u, wi, beta, true, pdf,
+                     [n](unsigned grid, cudaStream_t st, const MaterialGPU &g, const float *a, const float *b,
+                         float *oa, float *ob, float *op) {
+                         k_bsdf_sample<<<grid, 128, 0, st>>>(g, a, b, n, oa, ob, op);
+                     },
+                     "ks_bsdf_sample");
+}
+
+} // extern "C"

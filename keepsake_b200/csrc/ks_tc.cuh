@@ -100,6 +100,15 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t phase)
     return done != 0;
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("{\n\t"
+                 ".reg .b64 state;\n\t"
+                 "mbarrier.arrive.shared::cta.b64 state, [%0];\n\t"
+                 "}" ::"r"(smem_addr(bar))
+                 : "memory");
+}
+
 // Waits for `phase` of the mbarrier with an iteration limit; returns false (and the caller sets
 // its error flag and stops) if the limit is reached.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t phase, uint32_t max_iter = 1u << 22)

@@ -369,9 +369,9 @@ void launch_sample(bool batch, unsigned grid, cudaStream_t st, const SceneView &
                    PathBuf cur, const float4 *hits, const uint32_t *hit_inst, const uint32_t *queue,
                    const uint32_t *queue_count, float4 *samples, const BatchView &bv);
 // k_shade: hit (miss = false) or miss shading of the paths in a queue; guided and batched
-// renders are not combined.  attribs: some mesh of the scene (of a job) has vertex normals or
-// texcoords.
-void launch_shade(bool miss, bool guided, bool batch, bool attribs, unsigned grid, cudaStream_t st, const SceneView &sv,
+// renders are not combined.  variant: the shading kernel's feature set (kShadePlain,
+// kShadeAttribs, kShadeGeneral) that the scene (of every job) needs, SceneView::shade_variant.
+void launch_shade(bool miss, bool guided, bool batch, int variant, unsigned grid, cudaStream_t st, const SceneView &sv,
                   const RenderParams &rp, PathBuf cur, PathBuf nxt, const float4 *hits, const uint32_t *hit_inst,
                   const float4 *samples, const uint32_t *queue, const uint32_t *queue_count, uint32_t *next_count,
                   ShadowBuf sb, uint32_t *shadow_count, double *accum, double *weights, const GuideView &gv,

@@ -554,8 +554,10 @@ ks_material_desc ConfigServiceImpl::material(const std::string &path)
         throw ParseError("config: unknown bsdf '" + bsdf_path + "'");
     ConfigArgs b = args_of(this, bnode, bsdf_path);
     std::string type = b.load_string("type");
-    if (type != "principled_bsdf")
-        throw StatusError(KS_ERR_UNSUPPORTED, "config: bsdf type '" + type + "' is not supported (principled_bsdf)");
+    // create_bsdf (bsdf.cpp:50-62)
+    if (type != "principled_bsdf" && type != "principled_brdf" && type != "lambertian")
+        throw StatusError(KS_ERR_UNSUPPORTED, "config: bsdf type '" + type +
+                                                  "' is not supported (principled_bsdf, principled_brdf, lambertian)");
     if (a.contains("subsurface") || a.contains("normal_map"))
         throw StatusError(KS_ERR_UNSUPPORTED, "config: subsurface and normal maps are not supported");
     ks_material_desc d{};
@@ -581,19 +583,42 @@ ks_material_desc ConfigServiceImpl::material(const std::string &path)
             vec_n(*val, n, out, key);
     };
     const float c08[3] = {0.8f, 0.8f, 0.8f}, one = 1.0f, zero = 0.0f, ior = 1.5f, half = 0.5f, z3[3] = {0, 0, 0};
-    field("basecolor", 3, d.basecolor, c08);
-    field("roughness", 1, &d.roughness, &one);
-    field("metallic", 1, &d.metallic, &zero);
-    field("ior", 1, &d.ior, &ior);
-    field("specular_r0_mul", 1, &d.specular_r0_mul, &half);
-    field("specular_trans", 1, &d.specular_trans, &zero);
-    field("diffuse_trans", 1, &d.diffuse_trans, &zero);
-    field("diffuse_trans_fwd", 1, &d.diffuse_trans_fwd, &half);
-    field("emissive", 3, d.emissive, z3);
-    std::string mf = b.load_string("microfacet", "ggx");
-    if (mf != "ggx")
-        throw StatusError(KS_ERR_UNSUPPORTED, "config: microfacet '" + mf + "' is not supported (ggx)");
-    d.microfacet = 0;
+    // the PrincipledBSDF defaults of the fields a BSDF type does not read
+    d.roughness = one;
+    d.ior = ior;
+    d.specular_r0_mul = half;
+    d.diffuse_trans_fwd = half;
+    if (type == "lambertian") {
+        // create_lambertian (bsdf.cpp:43-48): albedo
+        d.bsdf = 2;
+        field("albedo", 3, d.basecolor, c08);
+    } else if (type == "principled_brdf") {
+        // create_principled_brdf (principled_bsdf.cpp:227-244)
+        d.bsdf = 1;
+        field("basecolor", 3, d.basecolor, c08);
+        field("roughness", 1, &d.roughness, &one);
+        field("metallic", 1, &d.metallic, &zero);
+        field("specular", 1, &d.specular, &half);
+    } else {
+        field("basecolor", 3, d.basecolor, c08);
+        field("roughness", 1, &d.roughness, &one);
+        field("metallic", 1, &d.metallic, &zero);
+        field("ior", 1, &d.ior, &ior);
+        field("specular_r0_mul", 1, &d.specular_r0_mul, &half);
+        field("specular_trans", 1, &d.specular_trans, &zero);
+        field("diffuse_trans", 1, &d.diffuse_trans, &zero);
+        field("diffuse_trans_fwd", 1, &d.diffuse_trans_fwd, &half);
+        field("emissive", 3, d.emissive, z3);
+    }
+    if (type != "lambertian") {
+        std::string mf = b.load_string("microfacet", "ggx");
+        if (mf == "ggx")
+            d.microfacet = 0;
+        else if (mf == "beckmann")
+            d.microfacet = 1;
+        else
+            throw StatusError(KS_ERR_UNSUPPORTED, "config: microfacet '" + mf + "' is not supported (ggx, beckmann)");
+    }
     if (a.contains("emission")) {
         a.load_vec3("emission", d.emission);
         d.has_emission = 1;

@@ -7,6 +7,7 @@
 //   * closest-hit and any-hit queries ksc::SBVH::intersect / intersectBool (cuda/sbvh.cu:512-603)
 // so that tests can pin the CUDA builder's topology and the CUDA traversal's hit IDs
 // against the reference itself.
+#include "ray_tri.cuh"
 #include "sbvh.cuh"
 
 #include <cstdint>
@@ -134,6 +135,24 @@ uint32_t ksref_sbvh_intersect1(void *handle, const float *r, int any_hit, float 
         bary[2] = rec.coord.z;
     }
     return rec.tri_idx;
+}
+
+// The reference's own watertight ray/triangle test (cuda/ray_tri.cuh:46-97, through the query of
+// cuda/sbvh.cu with culling off) of triangle tri[i] against ray i over the ray's [tmin, tmax]:
+// hit[i] = 1 and t[i] = its distance on a hit, else hit[i] = 0.  Used to prove a hit-id
+// difference a tie: the other triangle is a candidate of the reference at (nearly) the same t.
+void ksref_tri_test(void *handle, const float *rays, const uint32_t *tri, uint32_t n, float *t, uint32_t *hit)
+{
+    auto *h = (RefHandle *)handle;
+    for (uint32_t i = 0; i < n; ++i) {
+        const float *r = rays + 8 * (size_t)i;
+        ksc::Ray ray(ksc::vec3(r[0], r[1], r[2]), ksc::vec3(r[4], r[5], r[6]), r[3], r[7]);
+        ksc::RayTriHelper help(ray);
+        auto v = h->bvh.tri_verts(tri[i]);
+        ksc::RayTriIsect isect;
+        hit[i] = ksc::isect_ray_tri(ray, help, v[0], v[1], v[2], &isect) ? 1u : 0u;
+        t[i] = hit[i] ? isect.tHit : 0.0f;
+    }
 }
 
 // Root bounds (min xyz, max xyz).

@@ -1,8 +1,10 @@
-// ORACLE (test infrastructure only).  Restatement of keepsake's PrincipledBSDF with constant
-// shader fields and the GGX microfacet distribution.
+// ORACLE (test infrastructure only).  Restatement of keepsake's BSDFs with constant shader fields:
+// PrincipledBSDF and PrincipledBRDF with the GGX or Beckmann microfacet distribution, Lambertian.
 //
-// Follows: principled_bsdf.cpp:246-705 (closure, eval, sample, pdf, lobe weights, per-lobe
-// functions), microfacet.h:20-147 (GGX D, lambda, G1, G2 with std::beta, VNDF sample),
+// Follows: principled_bsdf.cpp:246-705 (PrincipledBSDF: closure, eval, sample, pdf, lobe weights,
+// per-lobe functions), principled_bsdf.cpp:11-225 (PrincipledBRDF), bsdf.cpp:13-41 (Lambertian),
+// microfacet.h:20-147 (GGX D, lambda, G1, G2 with std::beta, VNDF sample), microfacet.h:155-318
+// (Beckmann, BeckmannSample11, BeckmannSample), maths.h:598-627 (erfinv),
 // fresnel.h:9-37, bsdf.h:47-52 + bsdf.cpp:64-92 (Henyey-Greenstein), rng.h:243-265
 // (sample_disk, sample_cosine_hemisphere), rng.h:399-434 (sample_small_distrib),
 // maths.h:1037-1049 (reflect, refract), maths.h:813-821 (orthonormal_basis).
@@ -20,6 +22,8 @@ struct Closure
     V3 basecolor;
     float roughness, ax, ay, metallic, ior, specular_r0_mul, specular_trans, diffuse_trans, diffuse_trans_fwd;
     int microfacet;
+    int bsdf;       // 0 PrincipledBSDF, 1 PrincipledBRDF, 2 Lambertian
+    float specular; // PrincipledBRDF: clamp(specular, 0, 1) * 0.08 (principled_bsdf.cpp:22-23)
 };
 
 inline Closure eval_closure(const ks_material_desc &m)
@@ -38,6 +42,8 @@ inline Closure eval_closure(const ks_material_desc &m)
     c.diffuse_trans = std::clamp(m.diffuse_trans, 0.0f, 1.0f);
     c.diffuse_trans_fwd = std::clamp(m.diffuse_trans_fwd, 0.0f, 1.0f);
     c.microfacet = m.microfacet;
+    c.bsdf = m.bsdf;
+    c.specular = std::clamp(m.specular, 0.0f, 1.0f) * 0.08f;
     return c;
 }
 
@@ -101,6 +107,153 @@ struct GGX
         t2 = (1.0f - s) * std::sqrt(1.0f - t1 * t1) + s * t2;
         V3 Nh = t1 * T1 + t2 * T2 + std::sqrt(std::max(0.0f, 1.0f - t1 * t1 - t2 * t2)) * Vh;
         return normalized(V3(alpha_x * Nh.x, alpha_y * Nh.y, std::max(0.0f, Nh.z)));
+    }
+};
+
+// ---- erfinv (maths.h:598-627) -----------------------------------------------------------------
+inline float erfinv(float x)
+{
+    float w, p;
+    x = std::clamp(x, -.99999f, .99999f);
+    w = -std::log((1 - x) * (1 + x));
+    if (w < 5) {
+        w = w - 2.5f;
+        p = 2.81022636e-08f;
+        p = 3.43273939e-07f + p * w;
+        p = -3.5233877e-06f + p * w;
+        p = -4.39150654e-06f + p * w;
+        p = 0.00021858087f + p * w;
+        p = -0.00125372503f + p * w;
+        p = -0.00417768164f + p * w;
+        p = 0.246640727f + p * w;
+        p = 1.50140941f + p * w;
+    } else {
+        w = std::sqrt(w) - 3;
+        p = -0.000200214257f;
+        p = 0.000100950558f + p * w;
+        p = 0.00134934322f + p * w;
+        p = -0.00367342844f + p * w;
+        p = 0.00573950773f + p * w;
+        p = -0.0076224613f + p * w;
+        p = 0.00943887047f + p * w;
+        p = 1.00167406f + p * w;
+        p = 2.83297682f + p * w;
+    }
+    return p * x;
+}
+
+// ---- Beckmann (microfacet.h:155-318) -----------------------------------------------------------
+inline void beckmann_sample11(float cos_theta_i, float U1, float U2, float *slope_x, float *slope_y)
+{
+    if (cos_theta_i > .9999) {
+        float r = std::sqrt(-std::log(1.0f - U1));
+        float sin_phi = std::sin(2 * pi * U2);
+        float cos_phi = std::cos(2 * pi * U2);
+        *slope_x = r * cos_phi;
+        *slope_y = r * sin_phi;
+        return;
+    }
+    float sin_theta_i = std::sqrt(std::max((float)0, (float)1 - cos_theta_i * cos_theta_i));
+    float tan_theta_i = sin_theta_i / cos_theta_i;
+    float cot_theta_i = 1 / tan_theta_i;
+    float a = -1, c = std::erf(cot_theta_i);
+    float sample_x = std::max(U1, (float)1e-6f);
+    float theta_i = std::acos(cos_theta_i);
+    float fit = 1 + theta_i * (-0.876f + theta_i * (0.4265f - 0.0594f * theta_i));
+    float b = c - (1 + c) * std::pow(1 - sample_x, fit);
+    static const float sqrt_pi_inv = 1.f / std::sqrt(pi);
+    float normalization = 1 / (1 + c + sqrt_pi_inv * tan_theta_i * std::exp(-cot_theta_i * cot_theta_i));
+    int it = 0;
+    while (++it < 10) {
+        if (!(b >= a && b <= c))
+            b = 0.5f * (a + c);
+        float inv_erf = erfinv(b);
+        float value = normalization * (1 + b + sqrt_pi_inv * tan_theta_i * std::exp(-inv_erf * inv_erf)) - sample_x;
+        float derivative = normalization * (1 - inv_erf * tan_theta_i);
+        if (std::abs(value) < 1e-5f)
+            break;
+        if (value > 0)
+            c = b;
+        else
+            a = b;
+        b -= value / derivative;
+    }
+    *slope_x = erfinv(b);
+    *slope_y = erfinv(2.0f * std::max(U2, (float)1e-6f) - 1.0f);
+}
+
+struct Beckmann
+{
+    static constexpr float min_alpha = 1e-3f;
+    float alpha_x, alpha_y;
+    Beckmann(float ax, float ay)
+        : alpha_x(std::clamp(ax, min_alpha, 1.0f)), alpha_y(std::clamp(ay, min_alpha, 1.0f))
+    {
+    }
+    float D(V3 wm) const
+    {
+        float cos_theta2 = sqr(wm.z);
+        float sin_theta2 = std::max(1.0f - cos_theta2, 0.0f);
+        float tan_theta2 = sin_theta2 / cos_theta2;
+        if (std::isinf(tan_theta2))
+            return 0.0f;
+        float cos_theta4 = sqr(cos_theta2);
+        float sin_theta = std::sqrt(sin_theta2);
+        float cos_phi = (sin_theta == 0) ? 1 : std::clamp(wm.x / sin_theta, -1.0f, 1.0f);
+        float cos_phi2 = sqr(cos_phi);
+        float sin_phi = (sin_theta == 0) ? 0 : std::clamp(wm.y / sin_theta, -1.0f, 1.0f);
+        float sin_phi2 = sqr(sin_phi);
+        return std::exp(-tan_theta2 * (cos_phi2 / sqr(alpha_x) + sin_phi2 / sqr(alpha_y))) /
+               (pi * alpha_x * alpha_y * cos_theta4);
+    }
+    float lambda(V3 w) const
+    {
+        float cos_theta2 = sqr(w.z);
+        float sin_theta2 = std::max(1.0f - cos_theta2, 0.0f);
+        float sin_theta = std::sqrt(sin_theta2);
+        float tan_theta = sin_theta / w.z;
+        float abs_tan_theta = std::abs(tan_theta);
+        if (std::isinf(abs_tan_theta))
+            return 0.;
+        float cos_phi = (sin_theta == 0) ? 1 : std::clamp(w.x / sin_theta, -1.0f, 1.0f);
+        float cos_phi2 = sqr(cos_phi);
+        float sin_phi = (sin_theta == 0) ? 0 : std::clamp(w.y / sin_theta, -1.0f, 1.0f);
+        float sin_phi2 = sqr(sin_phi);
+        float alpha = std::sqrt(cos_phi2 * sqr(alpha_x) + sin_phi2 * sqr(alpha_y));
+        float a = 1 / (alpha * abs_tan_theta);
+        if (a >= 1.6f)
+            return 0;
+        return (1 - 1.259f * a + 0.396f * a * a) / (3.535f * a + 2.181f * a * a);
+    }
+    float G1(V3 w) const { return 1.0f / (1.0f + lambda(w)); }
+    float G2(V3 wo, V3 wi) const
+    {
+        if (wo.z * wi.z >= 0.0f)
+            return 1.0f / (1.0f + lambda(wo) + lambda(wi));
+        return (float)std::beta(1.0f + lambda(wo), 1.0f + lambda(wi));
+    }
+    V3 sample(V3 wo, float u0, float u1) const
+    {
+        bool flip = wo.z < 0;
+        V3 wi = flip ? -wo : wo;
+        // BeckmannSample (microfacet.h:217-245)
+        V3 stretched = normalized(V3(alpha_x * wi.x, alpha_y * wi.y, wi.z));
+        float slope_x, slope_y;
+        beckmann_sample11(stretched.z, u0, u1, &slope_x, &slope_y);
+        float cos_theta2 = sqr(stretched.z);
+        float sin_theta2 = std::max(1.0f - cos_theta2, 0.0f);
+        float sin_theta = std::sqrt(sin_theta2);
+        float cos_phi = (sin_theta == 0) ? 1 : std::clamp(stretched.x / sin_theta, -1.0f, 1.0f);
+        float sin_phi = (sin_theta == 0) ? 0 : std::clamp(stretched.y / sin_theta, -1.0f, 1.0f);
+        float tmp = cos_phi * slope_x - sin_phi * slope_y;
+        slope_y = sin_phi * slope_x + cos_phi * slope_y;
+        slope_x = tmp;
+        slope_x = alpha_x * slope_x;
+        slope_y = alpha_y * slope_y;
+        V3 wh = normalized(V3(-slope_x, -slope_y, 1.f));
+        if (flip)
+            wh = -wh;
+        return wh;
     }
 };
 
@@ -230,10 +383,11 @@ inline int sample_small_distrib4(const float *data, float u, float *u_remap)
 }
 
 // ---- PrincipledBSDF::internal (principled_bsdf.cpp:320-705) ---------------------------------
-struct Principled
+template <class MF>
+struct PrincipledT
 {
     Closure c;
-    GGX mf() const { return GGX(c.ax, c.ay); }
+    MF mf() const { return MF(c.ax, c.ay); }
 
     V3 eval_diffuse(V3 wo, V3 wi) const
     {
@@ -299,7 +453,9 @@ struct Principled
         } else {
             float denom = sqr(dot(wo, wh) + eta * dot(wi, wh));
             float specular = D * G * (1.0f - Fr) * dot(wo, wh) * dot(wi, wh) / (denom * wo.z);
-            f = std::abs(specular);
+            // wi = -wo through ior 1 makes wo + eta wi vanish: 0 / 0, which the reference asserts
+            // against (principled_bsdf.cpp:500); no transmission is counted there
+            f = denom == 0.0f ? 0.0f : std::abs(specular);
         }
         V3 out(f, f, f);
         out *= lobe_weight;
@@ -359,7 +515,7 @@ struct Principled
         } else {
             float denom = sqr(dot(wo, wh) + eta * dot(wi, wh));
             float jacobian = eta * eta * std::abs(dot(wi, wh)) / denom;
-            pdf = D * G1 * std::abs(dot(wo, wh)) / std::abs(wo.z) * jacobian;
+            pdf = denom == 0.0f ? 0.0f : D * G1 * std::abs(dot(wo, wh)) / std::abs(wo.z) * jacobian;
             pdf *= Fr_refr / (Fr_refl + Fr_refr);
         }
         return pdf;
@@ -529,6 +685,203 @@ struct Principled
         }
         pdf = p[0] * w[0] + p[1] * w[1] + p[2] * w[2] + p[3] * w[3];
         return eval(wo, wi) / pdf;
+    }
+};
+
+using Principled = PrincipledT<GGX>;
+
+// ---- PrincipledBRDF::internal (principled_bsdf.cpp:61-225) -----------------------------------
+template <class MF>
+struct PrincipledBrdfT
+{
+    Closure c;
+    MF mf() const { return MF(c.ax, c.ay); }
+    V3 eval_diffuse(V3, V3 wi) const
+    {
+        float lobe_weight = (1.0f - c.metallic);
+        if (lobe_weight == 0.0f)
+            return V3();
+        return lobe_weight * c.basecolor * inv_pi * wi.z;
+    }
+    V3 eval_specular(V3 wo, V3 wi) const
+    {
+        V3 wh = normalized(wo + wi);
+        float D = mf().D(wh);
+        float G = mf().G2(wo, wi);
+        V3 R0 = lerp3(V3(c.specular, c.specular, c.specular), c.basecolor, c.metallic);
+        V3 Fr = lerp3(R0, V3(1, 1, 1), fresnel_schlick(dot(wo, wh)));
+        return D * G * Fr / (4.0f * wo.z);
+    }
+    void lobe_sample_weights(V3 wo, float w[2]) const
+    {
+        float lum_basecolor = luminance(c.basecolor);
+        float lum_R0 = std::lerp(c.specular, lum_basecolor, c.metallic);
+        float weight_diffuse = wo.z > 0.0f ? (1.0f - c.metallic) * lum_basecolor * inv_pi : 0.0f;
+        float weight_specular = wo.z > 0.0f ? std::lerp(lum_R0, 1.0f, fresnel_schlick(wo.z)) : 0.0f;
+        float sum = weight_diffuse + weight_specular;
+        if (sum == 0.0f) {
+            w[0] = w[1] = 0.0f;
+            return;
+        }
+        float inv_sum = 1.0f / sum;
+        w[0] = weight_diffuse * inv_sum;
+        w[1] = weight_specular * inv_sum;
+    }
+    float pdf_diffuse(V3, V3 wi) const { return wi.z * inv_pi; }
+    float pdf_specular(V3 wo, V3 wi) const
+    {
+        V3 wh = normalized(wo + wi);
+        float D = mf().D(wh);
+        float G1 = mf().G1(wo);
+        return D * G1 / (4.0f * std::abs(wo.z));
+    }
+    V3 eval(V3 wo, V3 wi) const
+    {
+        if (wo.z == 0.0f || wi.z == 0.0f)
+            return V3();
+        V3 f;
+        if (wo.z > 0.0f && wi.z > 0.0f) {
+            f += eval_diffuse(wo, wi);
+            f += eval_specular(wo, wi);
+        }
+        return f;
+    }
+    float pdf(V3 wo, V3 wi) const
+    {
+        if (wo.z == 0.0f || wi.z == 0.0f)
+            return 0.0f;
+        float w[2];
+        lobe_sample_weights(wo, w);
+        if (w[0] == 0.0f && w[1] == 0.0f)
+            return 0.0f;
+        if (wo.z <= 0.0f || wi.z <= 0.0f)
+            return 0.0f;
+        float p[2] = {0.0f, 0.0f};
+        if (wo.z > 0.0f && wi.z > 0.0f) {
+            p[0] = pdf_diffuse(wo, wi);
+            p[1] = pdf_specular(wo, wi);
+        }
+        return p[0] * w[0] + p[1] * w[1];
+    }
+    void eval_and_pdf(V3 wo, V3 wi, V3 &f, float &p) const
+    {
+        f = eval(wo, wi);
+        if (is_zero(f)) {
+            p = 0.0f;
+            return;
+        }
+        p = pdf(wo, wi);
+    }
+    V3 sample_specular(V3 wo, float u0, float u1, float &pdf) const
+    {
+        if (wo.z == 0.0f) {
+            pdf = 0.0f;
+            return V3();
+        }
+        V3 wh = mf().sample(sgn(wo.z) * wo, u0, u1);
+        V3 wi = reflect(wo, wh);
+        if (wo.z * wi.z < 0.0f) {
+            pdf = 0.0f;
+            return V3();
+        }
+        float D = mf().D(wh);
+        float G1 = mf().G1(wo);
+        pdf = D * G1 / (4.0f * std::abs(wo.z));
+        return wi;
+    }
+    V3 sample(V3 wo, V3 &wi, float u_lobe, float u0, float u1, float &pdf) const
+    {
+        if (wo.z == 0.0f) {
+            pdf = 0.0f;
+            return V3();
+        }
+        float w[2];
+        lobe_sample_weights(wo, w);
+        if (w[0] == 0.0f && w[1] == 0.0f) {
+            pdf = 0.0f;
+            return V3();
+        }
+        // sample_small_distrib over the two weights (rng.h:399-432)
+        float w4[4] = {w[0], w[1], 0.0f, 0.0f};
+        int lobe = sample_small_distrib4(w4, u_lobe, nullptr);
+        float p[2] = {0.0f, 0.0f};
+        if (lobe == 0) {
+            wi = sample_cosine_hemisphere(u0, u1);
+            p[0] = wi.z * inv_pi;
+            if (is_zero(wi) || p[0] == 0.0f) {
+                pdf = 0.0f;
+                return V3();
+            }
+            if (wo.z > 0.0f && wi.z > 0.0f)
+                p[1] = pdf_specular(wo, wi);
+        } else {
+            wi = sample_specular(wo, u0, u1, p[1]);
+            if (is_zero(wi)) {
+                pdf = 0.0f;
+                return V3();
+            }
+            if (wo.z > 0.0f && wi.z > 0.0f)
+                p[0] = pdf_diffuse(wo, wi);
+        }
+        pdf = p[0] * w[0] + p[1] * w[1];
+        return eval(wo, wi) / pdf;
+    }
+};
+
+// ---- Lambertian (bsdf.cpp:13-41) -------------------------------------------------------------
+struct Lambertian
+{
+    Closure c;
+    V3 eval(V3 wo, V3 wi) const
+    {
+        if (wo.z <= 0.0f || wi.z <= 0.0f)
+            return V3();
+        return inv_pi * c.basecolor * wi.z;
+    }
+    float pdf(V3 wo, V3 wi) const
+    {
+        if (wo.z <= 0.0f || wi.z <= 0.0f)
+            return 0.0f;
+        return wi.z * inv_pi;
+    }
+    // BSDF::eval_and_pdf (bsdf.cpp:8-11)
+    void eval_and_pdf(V3 wo, V3 wi, V3 &f, float &p) const
+    {
+        f = eval(wo, wi);
+        p = pdf(wo, wi);
+    }
+    V3 sample(V3 wo, V3 &wi, float, float u0, float u1, float &pdf) const
+    {
+        if (wo.z <= 0.0f) {
+            pdf = 0.0f;
+            return V3();
+        }
+        wi = sample_cosine_hemisphere(u0, u1);
+        pdf = wi.z * inv_pi;
+        return c.basecolor;
+    }
+};
+
+// A material's BSDF (Material::bsdf, material.h:39), by type and microfacet distribution.
+struct Bsdf
+{
+    Closure c;
+    template <class F>
+    auto visit(F &&fn) const
+    {
+        if (c.bsdf == 2)
+            return fn(Lambertian{c});
+        if (c.bsdf == 1)
+            return c.microfacet == 1 ? fn(PrincipledBrdfT<Beckmann>{c}) : fn(PrincipledBrdfT<GGX>{c});
+        return c.microfacet == 1 ? fn(PrincipledT<Beckmann>{c}) : fn(PrincipledT<GGX>{c});
+    }
+    void eval_and_pdf(V3 wo, V3 wi, V3 &f, float &p) const
+    {
+        visit([&](const auto &b) { b.eval_and_pdf(wo, wi, f, p); return 0; });
+    }
+    V3 sample(V3 wo, V3 &wi, float u_lobe, float u0, float u1, float &pdf) const
+    {
+        return visit([&](const auto &b) { return b.sample(wo, wi, u_lobe, u0, u1, pdf); });
     }
 };
 

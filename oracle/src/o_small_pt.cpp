@@ -574,7 +574,7 @@ struct Tracer
     Counters cnt;
 
     // next_event_estimate (nee.cpp:11-57)
-    V3 nee(const Principled &bsdf, const Intersection &hit, V3 wo, OwenScrambledSobol02Morton &sobol)
+    V3 nee(const Bsdf &bsdf, const Intersection &hit, V3 wo, OwenScrambledSobol02Morton &sobol)
     {
         float pr_light;
         uint32_t light = s.power_distrib.sample(sobol.next(), pr_light);
@@ -698,7 +698,7 @@ struct Tracer
             if (bounce == in.bounces)
                 break;
             V3 wo = -normalized(rd);
-            Principled bsdf{eval_closure(mat)};
+            Bsdf bsdf{eval_closure(mat)};
             // Material::sample_with_nee (material.cpp:101-167)
             V3 Ld = nee(bsdf, it, wo, sobol);
             V3 wo_local = it.sh_to_local(wo);
@@ -1030,7 +1030,7 @@ int oracle_render(void *sp, const ks_camera_desc *cam, const ks_small_pt_params 
 void oracle_bsdf_eval(const ks_material_desc *mat, const float *wo, const float *wi, uint32_t n, float *f,
                       float *pdf)
 {
-    Principled b{eval_closure(*mat)};
+    Bsdf b{eval_closure(*mat)};
     for (uint32_t i = 0; i < n; ++i) {
         V3 o(wo[3 * i], wo[3 * i + 1], wo[3 * i + 2]), w(wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]);
         V3 fv;
@@ -1046,7 +1046,7 @@ void oracle_bsdf_eval(const ks_material_desc *mat, const float *wo, const float 
 void oracle_bsdf_sample(const ks_material_desc *mat, const float *wo, const float *u, uint32_t n, float *wi,
                         float *beta, float *pdf)
 {
-    Principled b{eval_closure(*mat)};
+    Bsdf b{eval_closure(*mat)};
     for (uint32_t i = 0; i < n; ++i) {
         V3 o(wo[3 * i], wo[3 * i + 1], wo[3 * i + 2]);
         V3 w;

@@ -26,7 +26,9 @@ def sobol_matrices(ref_root):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <reference source tree>")
+    ref = sys.argv[1]
     here = os.path.dirname(os.path.abspath(__file__))
     with open(os.path.join(here, "sobol_matrices.json"), "w") as f:
         json.dump(sobol_matrices(ref), f, indent=0)

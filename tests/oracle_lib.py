@@ -126,6 +126,8 @@ class RefSBVH:
         L.ksref_sbvh_export.argtypes = [_vp] * 6
         L.ksref_sbvh_intersect.argtypes = [_vp, _vp, _u32, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, ctypes.c_int]
         L.ksref_sbvh_destroy.argtypes = [_vp]
+        L.ksref_tri_test.argtypes = [_vp, _vp, _vp, _u32, _vp, _vp]
+        L.ksref_tri_test.restype = None
 
     def build(self, verts, idx, max_prims=4, buckets=12, trav_weight=1.0, alpha=1e-5):
         verts = np.ascontiguousarray(verts, dtype=np.float32).reshape(-1, 3)
@@ -158,6 +160,16 @@ class RefTree:
         self.owner.lib.ksref_sbvh_intersect(self.h, P(rays), n, int(any_hit), culling, P(tri), P(t), P(bary),
                                             threads)
         return (tri.astype(bool), None, None) if any_hit else (tri, t, bary)
+
+    def tri_test(self, rays, tri):
+        """The reference's watertight test of triangle tri[i] against ray i: (hit [n] bool, t [n])."""
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+        tri = np.ascontiguousarray(tri, dtype=np.uint32)
+        n = len(rays)
+        t = np.zeros(n, np.float32)
+        hit = np.zeros(n, np.uint32)
+        self.owner.lib.ksref_tri_test(self.h, P(rays), P(tri), n, P(t), P(hit))
+        return hit.astype(bool), t
 
     def __del__(self):
         try:

@@ -70,3 +70,28 @@ def rays_at_triangles(verts, idx, n, seed=0):
     r[:, 4:7] = d
     r[:, 7] = np.inf
     return r
+
+
+def deep_chain(n=250, k0=-125):
+    """Triangles across the x axis at x = 2^k, k = k0 .. k0 + n - 1 (each spanning y, z in [-1, 1]).
+    Built with 2 SAH buckets, every split peels the farthest triangle off the rest, so the SBVH is
+    about n / 2 levels deep and a ray along +x through all of them meets both children at every
+    level: deeper than a 64-entry traversal stack."""
+    v = []
+    for k in range(k0, k0 + n):
+        x = np.float32(2.0) ** k
+        v += [[x, -1, -1], [x, 1, -1], [x, 0, 1]]
+    v = np.array(v, np.float32)
+    return v, np.arange(len(v), dtype=np.uint32).reshape(-1, 3)
+
+
+def sbvh_depth(right):
+    """Levels of a flattened SBVH (DFS order: left child i + 1, right child right[i], 0 = leaf)."""
+    best, stack = 0, [(0, 1)]
+    while stack:
+        i, d = stack.pop()
+        best = max(best, d)
+        if right[i] != 0:
+            stack.append((i + 1, d + 1))
+            stack.append((int(right[i]), d + 1))
+    return best

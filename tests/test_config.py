@@ -104,17 +104,17 @@ def test_task_errors_before_any_device_work(tmp_path):
     with pytest.raises(ks.KsError) as e:
         ks.config_run('[[task]]\ntype = "gpu_small_pt"\n', str(tmp_path))
     assert e.value.status == 7
-    doc = DOC.replace('type = "principled_bsdf"', 'type = "lambertian"')
+    doc = DOC.replace('type = "principled_bsdf"', 'type = "oren_nayar"')
     with pytest.raises(ks.KsError) as e:
         ks.config_run(doc, str(tmp_path))
-    assert e.value.status == 7 and "lambertian" in str(e.value)
+    assert e.value.status == 7 and "oren_nayar" in str(e.value)
     with pytest.raises(ks.KsError) as e:
         ks.config_run(DOC.replace("spp = 8\n", ""), str(tmp_path))
     assert e.value.status == 8 and "spp" in str(e.value)
-    with pytest.raises(ks.KsError) as e:  # the Beckmann distribution is not built: an error, not GGX
-        ks.config_run(DOC.replace('type = "principled_bsdf"', 'type = "principled_bsdf"\nmicrofacet = "beckmann"'),
+    with pytest.raises(ks.KsError) as e:  # an unknown distribution is an error, not GGX
+        ks.config_run(DOC.replace('type = "principled_bsdf"', 'type = "principled_bsdf"\nmicrofacet = "phong"'),
                       str(tmp_path))
-    assert e.value.status == 7 and "beckmann" in str(e.value)
+    assert e.value.status == 7 and "phong" in str(e.value)
     with pytest.raises(ks.KsError) as e:
         ks.config_run(DOC.replace('"material.white", "material.lamp"', '"material.white"'), str(tmp_path))
     assert "mismatch" in str(e.value)
@@ -176,4 +176,94 @@ camera = {{ type = "perspective", to_world = {{ matrix_rm = {c2w} }}, vfov = {de
                               spp_prog_interval=8, rng_seed=3)
     ref = composite(*s.render(cam, p)).astype(np.float32)
     s.close()
+    assert np.array_equal(img, ref)
+
+
+@pytest.mark.gpu
+def test_config_bsdf_types_equal_c_abi(ctx, tmp_path):
+    """principled_brdf (Beckmann), lambertian and a Beckmann principled_bsdf through the TOML task
+    (create_bsdf, bsdf.cpp:50-62) equal the same materials through the C ABI."""
+    ks = _ks()
+    c2w = [1.0, 0.0, 0.0, 0.0, 0.0, 0.9578, 0.2873, 1.8, 0.0, -0.2873, 0.9578, 3.0, 0.0, 0.0, 0.0, 1.0]
+    doc = f"""
+[bsdf.floor]
+type = "principled_brdf"
+basecolor = {{ type = "constant", value = [0.6, 0.5, 0.4] }}
+roughness = {{ type = "constant", value = 0.4 }}
+metallic = {{ type = "constant", value = 0.2 }}
+specular = {{ type = "constant", value = 0.7 }}
+microfacet = "beckmann"
+
+[bsdf.lamp]
+type = "lambertian"
+albedo = {{ type = "constant", value = [0.3, 0.3, 0.3] }}
+
+[bsdf.box]
+type = "principled_bsdf"
+basecolor = {{ type = "constant", value = [0.2, 0.7, 0.3] }}
+roughness = {{ type = "constant", value = 0.3 }}
+microfacet = "beckmann"
+
+[material.floor]
+bsdf = "bsdf.floor"
+
+[material.lamp]
+bsdf = "bsdf.lamp"
+emission = [17.0, 12.0, 4.0]
+
+[material.box]
+bsdf = "bsdf.box"
+
+[mesh_asset.trio]
+type = "inline"
+geometry = [
+  {{ vertices = [[-1, 0, -1], [1, 0, -1], [1, 0, 1], [-1, 0, 1]], indices = [[0, 2, 1], [0, 3, 2]] }},
+  {{ vertices = [[-0.3, 1.5, -0.3], [0.3, 1.5, -0.3], [0.3, 1.5, 0.3], [-0.3, 1.5, 0.3]], indices = [[0, 1, 2], [0, 2, 3]] }},
+  {{ vertices = [[-0.2, 0.0, 0.0], [0.2, 0.0, 0.0], [0.0, 0.5, 0.1]], indices = [[0, 1, 2]] }},
+]
+
+[[task]]
+type = "small_pt_b200"
+object = "mesh_asset.trio"
+material = [["material.floor", "material.lamp", "material.box"]]
+sky = {{ ambient = [0.1, 0.2, 0.3] }}
+bounces = 4
+clamp_indirect = 0.0
+render_width = 48
+render_height = 32
+spp = 8
+spp_prog_interval = 8
+camera = {{ type = "perspective", to_world = {{ matrix_rm = {c2w} }}, vfov = 45.0, aspect = 1.5 }}
+"""
+    ks.config_run(doc, str(tmp_path))
+    img = ks.load_image(tmp_path / "task_0" / "small_pt_spp8.exr")
+
+    def mat(**kw):
+        m = ks.MaterialDesc()
+        m.basecolor[:] = kw.pop("basecolor")
+        m.roughness, m.ior, m.specular_r0_mul, m.diffuse_trans_fwd = 1.0, 1.5, 0.5, 0.5
+        for k, v in kw.items():
+            setattr(m, k, v)
+        return m
+    mats = [mat(basecolor=(0.6, 0.5, 0.4), roughness=0.4, metallic=0.2, specular=0.7, bsdf=1, microfacet=1),
+            mat(basecolor=(0.3, 0.3, 0.3), bsdf=2, has_emission=1),
+            mat(basecolor=(0.2, 0.7, 0.3), roughness=0.3, microfacet=1)]
+    mats[1].emission[:] = (17.0, 12.0, 4.0)
+    meshes = [(np.array([[-1, 0, -1], [1, 0, -1], [1, 0, 1], [-1, 0, 1]], np.float32), np.array([[0, 2, 1], [0, 3, 2]]), 0),
+              (np.array([[-0.3, 1.5, -0.3], [0.3, 1.5, -0.3], [0.3, 1.5, 0.3], [-0.3, 1.5, 0.3]], np.float32),
+               np.array([[0, 1, 2], [0, 2, 3]]), 1),
+              (np.array([[-0.2, 0, 0], [0.2, 0, 0], [0, 0.5, 0.1]], np.float32), np.array([[0, 1, 2]]), 2)]
+    sky = ks.SkyDesc()
+    sky.kind = 1
+    sky.ambient[:] = (0.1, 0.2, 0.3)
+    desc, keep = ks.scene_desc(meshes, mats, sky)
+    s = ks.Scene(ctx, desc, keep)
+    s.build_bvh()
+    vfov = np.float32(45.0) / np.float32(180.0) * np.float32(np.pi)
+    cam = ks.camera_perspective(np.array(c2w, np.float32), float(vfov), 1.5)
+    p = ks.SmallPTParams.make(render_width=48, render_height=32, spp=8, bounces=4, clamp_indirect=0.0,
+                              spp_prog_interval=8)
+    ref = composite(*s.render(cam, p)).astype(np.float32)
+    s.close()
+    assert ref.mean() > 0.0
     assert np.array_equal(img, ref)

@@ -45,7 +45,35 @@ CASES = {
     "icosphere_sky": dict(kind="icosphere", level=5, sky=(256, 128), W=64, H=64, spp=16, bounces=12),
     "icosphere_glossy_occluder": dict(kind="icosphere", level=5, sky=(256, 128), W=64, H=48, spp=8, bounces=12,
                                       roughness=(0.02, 0.2), occluder=True),
+    # transmission (principled_bsdf.cpp:423-516): the two boxes as one-sided glass (rough, ior 1.5
+    # and 4), refracting in and out through the inside branch of the BSDF (wo below the surface)
+    "box_room_glass": dict(kind="box_room", W=48, H=48, spp=16, bounces=8, clamp_indirect=0.0, one_sided=(5, 6),
+                           materials={5: dict(specular_trans=1.0, roughness=0.15, ior=1.5),
+                                      6: dict(specular_trans=1.0, roughness=0.4, ior=4.0, metallic=0.0)}),
+    # diffuse transmission: cosine (fwd 0) and forward Henyey-Greenstein (fwd 0.7) lobes
+    "box_room_diffuse_transmission": dict(kind="box_room", W=48, H=48, spp=16, bounces=8, clamp_indirect=0.0,
+                                          one_sided=(5, 6),
+                                          materials={5: dict(diffuse_trans=1.0, diffuse_trans_fwd=0.0),
+                                                     6: dict(diffuse_trans=0.5, diffuse_trans_fwd=0.7,
+                                                             specular_trans=0.3, roughness=0.5)}),
+    # the Beckmann distribution (microfacet.h:155-318) on every sphere patch
+    "icosphere_beckmann": dict(kind="icosphere", level=4, sky=(128, 64), W=48, H=48, spp=8, bounces=8,
+                               roughness=(0.05, 0.6), patch_materials=dict(microfacet=1)),
+    # PrincipledBRDF (GGX, Beckmann) boxes and Lambertian walls (principled_bsdf.cpp:11-225,
+    # bsdf.cpp:13-41)
+    "box_room_brdf_lambertian": dict(kind="box_room", W=48, H=48, spp=16, bounces=8, clamp_indirect=0.0,
+                                     materials={0: dict(bsdf=2), 2: dict(bsdf=2), 3: dict(bsdf=2),
+                                                5: dict(bsdf=1, roughness=0.3, metallic=0.5, specular=0.7),
+                                                6: dict(bsdf=1, microfacet=1, roughness=0.4, specular=0.5)}),
 }
+
+
+def set_fields(m, fields):
+    for k, v in fields.items():
+        if k == "basecolor":
+            m.basecolor[:] = v
+        else:
+            setattr(m, k, v)
 
 
 def make_case(c):
@@ -68,6 +96,14 @@ def make_case(c):
         kw.update(include_background=0, backdrop=c["backdrop"])
     if "filter" in c:
         kw.update(pixel_filter=c["filter"][0], pixel_filter_width=c["filter"][1], pixel_filter_sigma=c["filter"][2])
+    d = g.desc.contents
+    for k, fields in c.get("materials", {}).items():
+        set_fields(d.materials[k], fields)
+    if "patch_materials" in c:  # every material but the ground's (the last)
+        for k in range(d.n_materials - 1):
+            set_fields(d.materials[k], c["patch_materials"])
+    for k in c.get("one_sided", ()):
+        d.meshes[k].twosided = 0
     if "lights" in c:
         arr = (ks.LightDesc * len(c["lights"]))()
         for k, (t, col, v) in enumerate(c["lights"]):
@@ -345,3 +381,18 @@ def test_full_frame_same_seed_matches_oracle(ctx, oracle):
     assert (rel > 1e-2).mean() < 0.01
     assert abs(st.extension_rays - int(ocnt[0])) <= 0.01 * ocnt[0]
     assert abs(st.shadow_rays - int(ocnt[1])) <= 0.01 * ocnt[1]
+
+
+def test_oracle_material_cases_render(oracle):
+    """The transmission, Beckmann, PrincipledBRDF and Lambertian cases render finite images with
+    the same hit/miss weights as the plain scene and differ from it where the materials changed."""
+    for name, base in (("box_room_glass", "box_room"), ("box_room_diffuse_transmission", "box_room"),
+                       ("box_room_brdf_lambertian", "box_room")):
+        c = dict(CASES[name], W=24, H=24, spp=8)
+        g, cam, p = make_case(c)
+        a, w, cnt = oracle.scene(g.desc).render(cam, p, threads=4)
+        g0, cam0, p0 = make_case(dict(CASES[base], W=24, H=24, spp=8, clamp_indirect=0.0))
+        a0, w0, _ = oracle.scene(g0.desc).render(cam0, p0, threads=4)
+        assert np.isfinite(a).all() and (a >= 0).all(), name
+        assert np.array_equal(w.sum(-1), w0.sum(-1)), name
+        assert rel_mse(composite(a, w), composite(a0, w0)) > 1e-3, name

@@ -10,6 +10,8 @@ import pytest
 
 import scenes
 
+KS_ERR_QUEUE_OVERFLOW = 4
+
 
 def _noalloc(ks, scene, rays, any_hit=0, culling=2):
     lib = ks.lib
@@ -61,3 +63,66 @@ def test_noalloc_rejects_oversized_batch(ctx):
     st, _, _, _ = _noalloc(ks, s, rays)
     assert st == 1  # KS_ERR_INVALID_ARGUMENT
     assert b"65536" in ks.lib.ks_last_error(ctx.handle)
+
+
+@pytest.mark.gpu
+def test_noalloc_matches_reference_sbvh_and_culling(ctx):
+    """Against the reference's own SBVH queries (cuda/sbvh.cu:512-603, compiled from the reference
+    tree): identical hit ids, distances and barycentrics except proven ties, for every culling mode;
+    an empty batch is a no-op."""
+    import keepsake_b200 as ks
+    import oracle_lib
+    from test_sbvh import check_ties
+    v, i = scenes.soup(3000, seed=31)
+    desc, keep = ks.triangle_soup_desc(v, i)
+    s = ks.Scene(ctx, desc, keep)
+    s.build_bvh()
+    ref = oracle_lib.ref_sbvh().build(v, i)
+    rays = scenes.rays_at_triangles(v, i, 20000, seed=32)
+    for culling in (0, 1, 2):
+        st, tri, t, bary = _noalloc(ks, s, rays, culling=culling)
+        assert st == 0
+        rtri, rt, rbary = ref.intersect(rays, culling=culling)
+        hit = rtri != 0xFFFFFFFF
+        assert np.array_equal(tri != 0xFFFFFFFF, hit)
+        tie = tri != rtri
+        assert tie.mean() <= 1e-3
+        same = hit & ~tie
+        assert np.array_equal(t[same].view(np.uint32), rt[same].view(np.uint32))
+        assert np.array_equal(bary[same].view(np.uint32), rbary[same].view(np.uint32))
+        if tie.any():
+            check_ties(ref, rays[tie], tri[tie], t[tie], rtri[tie], rt[tie], np.nonzero(tie)[0])
+        st, occ, _, _ = _noalloc(ks, s, rays, any_hit=1, culling=culling)
+        assert st == 0
+        rocc, _, _ = ref.intersect(rays, any_hit=True, culling=culling)
+        assert np.array_equal(occ.astype(bool), rocc)
+    st, tri, _, _ = _noalloc(ks, s, rays[:0])
+    assert st == 0 and len(tri) == 0
+    s.close()
+
+
+@pytest.mark.gpu
+def test_noalloc_overflow_then_next_call_succeeds(ctx):
+    """A tree deeper than the traversal stack makes a call fail with KS_ERR_QUEUE_OVERFLOW (the
+    overflow flag lives in the shared array); the next call on an ordinary scene clears the flag
+    and returns ks_trace_rays's results."""
+    import keepsake_b200 as ks
+    from test_failures import chain_rays, chain_scene
+    desc, keep = chain_scene(ks)
+    deep = ks.Scene(ctx, desc, keep)
+    deep.build_bvh(buckets=2)
+    st, _, _, _ = _noalloc(ks, deep, chain_rays())
+    assert st == KS_ERR_QUEUE_OVERFLOW
+    deep.close()
+    g = ks.Generated("box_room", 0)
+    s = ks.Scene(ctx, g.desc)
+    s.build_bvh()
+    v, i = g.flat_geometry()
+    rays = scenes.random_rays(v, 4000, seed=33)
+    st, tri, t, _ = _noalloc(ks, s, rays)
+    assert st == 0, ks.lib.ks_last_error(ctx.handle)
+    rtri, rt, _ = s.trace(rays)
+    assert np.array_equal(tri, rtri)
+    hit = rtri != 0xFFFFFFFF
+    assert np.array_equal(t[hit].view(np.uint32), rt[hit].view(np.uint32))
+    s.close()
