@@ -13,18 +13,28 @@ queries) over the K timed steps, device time from CUDA events on the library's s
 ranks.  e2e = the same metric through the host-buffer C ABI (scene upload, GPU SBVH build,
 render, FP64 image download every step).
 
-time_to_relmse: the glossy scene behind an occluder (the same icosphere made glossy-heavy,
-roughness U[0.02,0.2], with an opaque slab between it and the sun) at 1920x1080, depth 12.  A
-2048-spp plain render with its own seed is the reference; plain and guided progressive renders
-(1 spp per pass, guide trained online: batches of 2^18 records, Adam lr 1e-2) run until the
-relative MSE (eps 1e-2, reduced in FP64 on the GPU after each pass, outside the timed region)
-reaches 1e-2.  The host CPU runs the same estimator on the same Sobol samples as the plain GPU
-render, so it reaches the same error at the same spp: its time is that spp count over its
-measured paths/s on the same frame.
+Roofline of the closest-hit traversal kernel: algorithmic bytes per query as the CPU oracle counts
+them on the same frame (32 B per SBVH node whose bound the reference traversal tests, 48 B per
+triangle tested, 48 B of ray and hit I/O), over the kernel's CUDA-event time; beside it the
+kernel's own fetch count (128 B per 4-wide node, 48 B per triangle).
 
---impl reference runs the CPU implementation of the path on the host cores (the oracle's
-restatement of small_pt over the reference's own SBVH traversal), each step a bounded crop of the
-same frame.
+time_to_relmse: the glossy scene behind an occluder (the same icosphere made glossy-heavy,
+roughness U[0.02,0.2], with an opaque slab between it and the sun) at 1920x1080, depth 12.  The
+reference is eight 64x64 crop windows rendered by the CPU oracle at 2048 spp (its own seed) and
+accumulated in FP64; plain and guided progressive GPU renders (1 spp per pass, guide trained
+online: batches of 2^18 records, Adam lr 1e-2) run until the relative MSE on those crops (eps 1e-2,
+reduced in FP64 on the GPU after each pass, outside the timed region) reaches 1e-2, and the CPU
+oracle renders the full frame progressively (4 spp per chunk, same sample sequence) to the same
+error, timed.
+
+Side configurations, each once per run: the box room (256x256, 64 spp, depth 8) on the GPU and
+on the CPU oracle; 64 batched scenes at their full spp (one CUDA-graph launch, autotuned); the
+instanced scene (400 instances, 3840x2160, 1024 spp, depth 16) plain and guided.
+
+--impl reference runs the CPU implementation of the path on all host cores (the oracle's
+restatement of small_pt over the reference's own SBVH traversal, with the scene, camera and
+parameters made by the oracle library, without loading the CUDA library) on the same frame and
+configuration, each step one 16-spp interval of the 256-spp render of the full frame.
 """
 import argparse
 import json
@@ -40,8 +50,9 @@ sys.path.insert(0, ROOT)
 
 WORKLOAD = "icosphere_l8_1310722tris_1024x1024_256spp_depth12_sky2048x1024"
 W_RES, H_RES, SPP, BOUNCES = 1024, 1024, 256, 12
-# CPU sample: a centred crop of the same frame at the full 256 spp
-CPU_CROP = 128
+# CPU sample: one interval of the frame's samples per step (the full frame, CPU_SPP of the SPP
+# samples per pixel, the next interval each step, as SmallPT::run renders its spp intervals)
+CPU_SPP = 16
 
 
 def parse():
@@ -54,12 +65,13 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ttr", action="store_true", help="skip the time-to-relMSE leg")
     ap.add_argument("--no-c4", action="store_true", help="skip the batched multi-scene leg")
-    ap.add_argument("--c4-spp-div", type=int, default=8, help="divides the spp of every batched job")
+    ap.add_argument("--c4-spp-div", type=int, default=1, help="divides the spp of every batched job")
+    ap.add_argument("--no-c1", action="store_true", help="skip the box-room leg")
     ap.add_argument("--no-c5", action="store_true", help="skip the instanced-scene leg")
     ap.add_argument("--profile-guided", action="store_true",
                     help="profiling case only: one guided render of the glossy occluded scene at --res x "
                          "(--res * 9 / 16), --spp samples (default 16), then exit")
-    ap.add_argument("--c5-spp", type=int, default=16)
+    ap.add_argument("--c5-spp", type=int, default=1024)
     # reduced frames of the same scene, for profiling captures only (not a bench line)
     ap.add_argument("--spp", type=int, default=None)
     ap.add_argument("--res", type=int, default=None)
@@ -92,43 +104,95 @@ def make_generated(ks):
 
 TTR_W, TTR_H, TTR_TARGET, TTR_REF_SPP, TTR_MAX_SPP = 1920, 1080, 1e-2, 2048, 1024
 TTR_PRETRAIN_PASSES = 192
+# the reference crops: eight 64x64 windows on a 4 x 2 grid over the frame (crop_* semantics of
+# small_pt.cpp:25-34), rendered by the CPU oracle at TTR_REF_SPP with their own seed
+TTR_CROP = 64
+TTR_CROPS = [(int((i + 0.5) * TTR_W / 4) - TTR_CROP // 2, int((j + 0.5) * TTR_H / 2) - TTR_CROP // 2)
+             for j in range(2) for i in range(4)]
+TTR_REF_SEED, TTR_SEED = 1000, 7
+# the CPU arm renders the full frame in chunks of this many samples per pixel, timed
+TTR_CPU_CHUNK = 4
+TTR_CPU_MAX_SECONDS = 120.0
+
+
+def oracle_module():
+    """tests/oracle_lib (the CPU oracle's binding); used by the CPU legs of this file only."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib
+    return oracle_lib
+
+
+def crop_pixels(W):
+    """Frame pixel indices of the reference crops, crop by crop, row-major inside each."""
+    import numpy as np
+    idx = []
+    for x0, y0 in TTR_CROPS:
+        ys, xs = np.mgrid[y0:y0 + TTR_CROP, x0:x0 + TTR_CROP]
+        idx.append((ys * W + xs).reshape(-1))
+    return np.concatenate(idx)
 
 
 def time_to_relmse(ks, ctx, torch, with_cpu, guide_options=None, guide_params=None):
-    """Seconds (and spp) for plain and guided renders to reach relMSE 1e-2 on the glossy
-    occluded scene; the CPU estimate from the oracle's paths/s on the same frame."""
+    """Seconds (and spp) for plain and guided GPU renders, and for the CPU oracle, to reach relMSE
+    1e-2 against FP64 CPU reference crops of the glossy occluded scene."""
+    import numpy as np
     g = ks.Generated("icosphere", 0, level=8, sky=(2048, 1024), resolution=(TTR_W, TTR_H), roughness=(0.02, 0.2),
                      occluder=True)
     sc = ks.Scene(ctx, g.desc)
     sc.build_bvh()
     cam = ks.camera_perspective(g.camera_to_world, g.vfov, g.aspect)
     n = TTR_W * TTR_H
+    idx_np = crop_pixels(TTR_W)
+    n_crop = len(idx_np)
+    res = {"target_rel_mse": TTR_TARGET, "eps": 1e-2,
+           "workload": f"icosphere_l8 glossy (roughness U[0.02,0.2]) behind an occluder slab, {TTR_W}x{TTR_H}, "
+                       f"depth {BOUNCES}, 1 spp per GPU pass",
+           "timing": "seconds: host wall clock of the render call up to the pass that reached the target, "
+                     "minus the time spent in the per-pass error evaluation; device_seconds: the library's "
+                     "CUDA-event time of the same render call; cpu: wall clock of the oracle's chunks"}
+    # ---- FP64 reference crops from the CPU oracle (the reference's estimator over its SBVH) ----
+    ol = oracle_module()
+    orc = ol.load()
+    osc = orc.scene(g.desc)
+    threads = os.cpu_count() or 1
+    ref_img = np.zeros((n_crop, 3), np.float64)
+    t0 = time.perf_counter()
+    ref_paths = 0
+    for k, (x0, y0) in enumerate(TTR_CROPS):
+        pr = ks.SmallPTParams.make(render_width=TTR_W, render_height=TTR_H, spp=TTR_REF_SPP, bounces=BOUNCES,
+                                   rng_seed=TTR_REF_SEED, crop_start_x=x0, crop_start_y=y0, crop_width=TTR_CROP,
+                                   crop_height=TTR_CROP)
+        a, w, _ = osc.render(cam, pr, threads=threads)
+        from imaging import composite
+        img = composite(a, w)[y0:y0 + TTR_CROP, x0:x0 + TTR_CROP].reshape(-1, 3)
+        ref_img[k * TTR_CROP * TTR_CROP:(k + 1) * TTR_CROP * TTR_CROP] = img
+        ref_paths += TTR_CROP * TTR_CROP * TTR_REF_SPP
+    ref_s = time.perf_counter() - t0
+    res["reference"] = {"kind": "CPU oracle, FP64 accumulation", "crops": [[x, y, TTR_CROP, TTR_CROP] for x, y in TTR_CROPS],
+                        "spp": TTR_REF_SPP, "seed": TTR_REF_SEED, "paths": ref_paths, "seconds": ref_s,
+                        "cores": threads}
+    idx = torch.as_tensor(idx_np, device="cuda")
+    ref = torch.as_tensor(ref_img, device="cuda").contiguous()
     acc = torch.zeros((n, 3), dtype=torch.float64, device="cuda")
     wts = torch.zeros((n, 2), dtype=torch.float64, device="cuda")
-    pr = ks.SmallPTParams.make(render_width=TTR_W, render_height=TTR_H, spp=TTR_REF_SPP, bounces=BOUNCES,
-                               rng_seed=1000, spp_prog_interval=256)
-    t0 = time.perf_counter()
-    sc.render_device(cam, pr, acc.data_ptr(), wts.data_ptr())
-    torch.cuda.synchronize()
-    ref_s = time.perf_counter() - t0
-    w0, w1 = wts[:, 0], wts[:, 1]
-    w_sum = (w0 + w1).to(torch.int64).to(torch.float64)
-    w = torch.where(w_sum == 0, torch.zeros_like(w_sum), w0 / torch.clamp(w_sum, min=1))
-    fg = torch.where(w0[:, None] == 0, torch.zeros_like(acc), acc / torch.clamp(w0[:, None], min=1e-300))
-    ref = (w[:, None] * fg).contiguous()
+
+    def crop_error():
+        a = acc.index_select(0, idx).contiguous()
+        w = wts.index_select(0, idx).contiguous()
+        return ctx.rel_mse_device(a.data_ptr(), w.data_ptr(), ref.data_ptr(), n_crop, 1e-2)
 
     def run(guide, max_passes=None, frozen=False):
         acc.zero_()
         wts.zero_()
         torch.cuda.synchronize()
         p = ks.SmallPTParams.make(render_width=TTR_W, render_height=TTR_H, spp=TTR_MAX_SPP, bounces=BOUNCES,
-                                  rng_seed=7, spp_prog_interval=1)
+                                  rng_seed=TTR_SEED, spp_prog_interval=1)
         st = {"cb": 0.0, "hit": None, "last": None, "passes": []}
         t_start = time.perf_counter()
 
         def cb(spp):
             t_in = time.perf_counter()
-            e = ctx.rel_mse_device(acc.data_ptr(), wts.data_ptr(), ref.data_ptr(), n, 1e-2)
+            e = crop_error()
             render_s = (t_in - t_start) - st["cb"]
             st["last"] = (spp, render_s, e)
             st["passes"].append(render_s)
@@ -197,30 +261,72 @@ def time_to_relmse(ks, ctx, torch, with_cpu, guide_options=None, guide_params=No
     frozen = run(guide, frozen=True)
     frozen.update(pretrain_passes=TTR_PRETRAIN_PASSES + (guided["last"]["spp"] or 0), pretrain_seconds=pre_s)
     guide.close()
-    res = {"target_rel_mse": TTR_TARGET, "eps": 1e-2,
-           "workload": f"icosphere_l8 glossy (roughness U[0.02,0.2]) behind an occluder slab, {TTR_W}x{TTR_H}, "
-                       f"depth {BOUNCES}, 1 spp per pass",
-           "timing": "seconds: host wall clock of the render call up to the pass that reached the target, "
-                     "minus the time spent in the per-pass error evaluation; device_seconds: the library's "
-                     "CUDA-event time of the same render call",
-           "reference": {"spp": TTR_REF_SPP, "seed": 1000, "seconds": ref_s},
-           "plain": plain, "guided": guided, "guided_pretrained": frozen}
-    if with_cpu and plain["spp"]:
-        threads = os.cpu_count() or 1
-        sys.path.insert(0, os.path.join(ROOT, "tests"))
-        import oracle_lib
-        orc = oracle_lib.load()
-        osc = orc.scene(g.desc)
-        pc = ks.SmallPTParams.make(render_width=TTR_W, render_height=TTR_H, spp=1, bounces=BOUNCES, rng_seed=7)
-        t0 = time.perf_counter()
-        _, _, cnt = osc.render(cam, pc, threads=threads)
-        cpu_s = time.perf_counter() - t0
-        pps = n / cpu_s
-        res["cpu"] = {"seconds_est": plain["spp"] * n / pps, "spp": plain["spp"], "paths_per_s": pps,
-                      "cores": threads, "kind": "port",
-                      "sample": f"full {TTR_W}x{TTR_H} frame at 1 spp ({n} paths, {int(cnt[0]) + int(cnt[1])} rays)"}
+    res.update(plain=plain, guided=guided, guided_pretrained=frozen)
+    if with_cpu:
+        # the CPU oracle renders the same full frame with the same sample sequence (spp intervals of
+        # the TTR_MAX_SPP sequence, as the GPU's 1-spp passes), timed, until its error on the crops
+        # reaches the target
+        from imaging import composite, rel_mse
+        pc = ks.SmallPTParams.make(render_width=TTR_W, render_height=TTR_H, spp=TTR_MAX_SPP, bounces=BOUNCES,
+                                   rng_seed=TTR_SEED)
+        a = np.zeros((TTR_H, TTR_W, 3), np.float64)
+        w = np.zeros((TTR_H, TTR_W, 2), np.float64)
+        cpu_s, spp, err, rays, paths = 0.0, 0, None, 0, 0
+        while spp < TTR_MAX_SPP and cpu_s < TTR_CPU_MAX_SECONDS:
+            t0 = time.perf_counter()
+            _, _, cnt, _ = osc.render_range(cam, pc, spp, spp + TTR_CPU_CHUNK, threads=threads, accum=a, weights=w)
+            cpu_s += time.perf_counter() - t0
+            spp += TTR_CPU_CHUNK
+            rays += int(cnt[0]) + int(cnt[1])
+            paths += n * TTR_CPU_CHUNK
+            img = composite(a.reshape(-1, 3)[idx_np], w.reshape(-1, 2)[idx_np])
+            err = rel_mse(img, ref_img)
+            if err <= TTR_TARGET:
+                break
+        res["cpu"] = {"seconds": cpu_s if err is not None and err <= TTR_TARGET else None, "spp": spp,
+                      "rel_mse": err, "seconds_run": cpu_s, "cores": threads, "kind": "port",
+                      "mpaths_per_s": paths / cpu_s / 1e6, "mrays_per_s": rays / cpu_s / 1e6,
+                      "sample": f"the full {TTR_W}x{TTR_H} frame, {TTR_CPU_CHUNK} spp per chunk, error on the "
+                                f"reference crops after each chunk (outside the timing)"}
     sc.close()
     return res
+
+
+def box_room_leg(ks, ctx, torch, with_cpu):
+    """The box room (5 wall quads, 2 rotated boxes, a rectangular light; 256x256, 64 spp, depth 8):
+    device-timed GPU render and, on the host cores, the CPU oracle on the same full frame."""
+    g = ks.Generated("box_room", 0)
+    s = ks.Scene(ctx, g.desc)
+    s.build_bvh()
+    cam = ks.camera_perspective(g.camera_to_world, g.vfov, g.aspect)
+    p = ks.SmallPTParams.make(render_width=256, render_height=256, spp=64, bounces=8, clamp_indirect=0.0)
+    acc = torch.zeros((256, 256, 3), dtype=torch.float64, device="cuda")
+    wts = torch.zeros((256, 256, 2), dtype=torch.float64, device="cuda")
+    for _ in range(3):
+        s.render_device(cam, p, acc.data_ptr(), wts.data_ptr())
+    runs = []
+    for _ in range(5):
+        acc.zero_()
+        wts.zero_()
+        s.render_device(cam, p, acc.data_ptr(), wts.data_ptr())
+        runs.append(s.stats())
+    ms = statistics.median(r.ms_total for r in runs)
+    st = runs[0]
+    out = {"workload": "box_room: 5 wall quads + 2 rotated boxes + 1 area light (36 triangles), 256x256, 64 spp, "
+                       "depth 8, clamp_indirect 0",
+           "gpu": {"ms": ms, "mrays_per_s": (st.extension_rays + st.shadow_rays) / ms / 1e3,
+                   "mpaths_per_s": st.paths / ms / 1e3, "timing": "median of 5 renders, CUDA events"}}
+    if with_cpu:
+        orc = oracle_module().load()
+        threads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        _, _, cnt = orc.scene(g.desc).render(cam, p, threads=threads)
+        cpu_s = time.perf_counter() - t0
+        out["cpu"] = {"seconds": cpu_s, "mrays_per_s": (int(cnt[0]) + int(cnt[1])) / cpu_s / 1e6,
+                      "mpaths_per_s": 256 * 256 * 64 / cpu_s / 1e6, "cores": threads, "kind": "port",
+                      "sample": "the whole frame"}
+    s.close()
+    return out
 
 
 def batched_leg(ks, ctx, torch, spp_div):
@@ -316,33 +422,49 @@ def instanced_leg(ks, ctx, torch, spp):
                        "ms_guide_train": sg.ms_guide_train}}
 
 
-def cpu_crop_params(ks, crop=CPU_CROP):
-    x0 = (W_RES - crop) // 2
-    return ks.SmallPTParams.make(render_width=W_RES, render_height=H_RES, spp=SPP, bounces=BOUNCES,
-                                 crop_start_x=x0, crop_start_y=x0, crop_width=crop, crop_height=crop)
+def cpu_sample_range(step):
+    """Sample indices [s0, s1) of the CPU sample of step `step`: consecutive CPU_SPP-sample intervals
+    of the SPP samples per pixel, wrapping around."""
+    s0 = (step * CPU_SPP) % SPP
+    return s0, s0 + CPU_SPP
 
 
-def run_cpu(ks, g, steps, warmup, threads):
-    """The oracle (CPU restatement over the reference SBVH) on a bounded crop; returns stats."""
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    import oracle_lib
-    orc = oracle_lib.load()
-    cam = ks.camera_perspective(g.camera_to_world, g.vfov, g.aspect)
+def run_cpu(orc, desc, camera, params, steps, warmup, threads):
+    """The oracle (CPU restatement of small_pt over the reference SBVH) on the full frame, one
+    CPU_SPP-sample interval per step; returns the timed totals."""
     t0 = time.perf_counter()
-    sc = orc.scene(g.desc)
+    sc = orc.scene(desc)
     setup_s = time.perf_counter() - t0
-    p = cpu_crop_params(ks)
     times, rays = [], []
     for k in range(warmup + steps):
+        s0, s1 = cpu_sample_range(k)
         t0 = time.perf_counter()
-        _, _, cnt = sc.render(cam, p, threads=threads)
+        _, _, cnt, _ = sc.render_range(camera, params, s0, s1, threads=threads)
         dt = time.perf_counter() - t0
         if k >= warmup:
             times.append(dt)
             rays.append(int(cnt[0]) + int(cnt[1]))
-    return dict(seconds=sum(times), rays=sum(rays), steps=steps, setup_s=setup_s,
-                sample=f"{CPU_CROP}x{CPU_CROP} centre crop of the {W_RES}x{H_RES} frame at {SPP} spp, depth "
-                       f"{BOUNCES} ({CPU_CROP * CPU_CROP * SPP} paths per step)")
+    return dict(seconds=sum(times), rays=sum(rays), steps=steps, setup_s=setup_s, scene=sc,
+                sample=f"the full {W_RES}x{H_RES} frame, samples [{CPU_SPP} k, {CPU_SPP} (k + 1)) of its {SPP} "
+                       f"per pixel in step k ({W_RES * H_RES * CPU_SPP} paths per step), depth {BOUNCES}")
+
+
+def oracle_work(sc, camera, params, threads, n_spp=2):
+    """Per-query work of the frame's ray queries as the restatement of the reference traversal
+    counts it (nodes whose bound is tested, triangles tested), over n_spp samples per pixel of the
+    full frame; checked against the reference's own queries on every ray."""
+    _, _, cnt, wk = sc.render_range(camera, params, 0, n_spp, threads=threads, count_work=True)
+    ext, sh = int(cnt[0]), int(cnt[1])
+    return {"ext_queries": ext, "ext_nodes_per_query": wk["ext_nodes"] / ext, "ext_tris_per_query": wk["ext_tris"] / ext,
+            "shadow_queries": sh, "shadow_nodes_per_query": wk["shadow_nodes"] / max(sh, 1),
+            "shadow_tris_per_query": wk["shadow_tris"] / max(sh, 1), "mismatches": wk["mismatches"],
+            "sample": f"the full {W_RES}x{H_RES} frame at samples [0, {n_spp}) of {SPP}"}
+
+
+def bench_config(world):
+    """The workload description both arms print (identical for the same N)."""
+    return {"workload": WORKLOAD, "triangles": 1310722, "resolution": [W_RES, H_RES], "spp": SPP, "depth": BOUNCES,
+            "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (BVH + triangles + sky > 126 MB)"}
 
 
 class ClockSampler:
@@ -412,31 +534,33 @@ def measured_peaks():
 
 
 def profile_traffic():
-    """DRAM bytes per closest-hit query from the committed ncu summary (None if absent)."""
-    p = os.path.join(ROOT, "profiles", "k_extend_pt_icosphere_l8.md")
+    """DRAM bytes per closest-hit query of the traversal kernel, from the committed ncu summary's
+    data file (None if absent)."""
+    p = os.path.join(ROOT, "profiles", "k_extend_pt_icosphere_l8.json")
     if not os.path.exists(p):
         return None
-    for line in open(p):
-        if line.startswith("dram_bytes_per_query:"):
-            return float(line.split(":")[1])
-    return None
+    return json.load(open(p)).get("dram_bytes_per_query")
 
 
 def reference_arm(args):
+    """The CPU implementation of the path on all host cores, through the oracle only (scene,
+    camera and parameters from the oracle library; the CUDA library is not loaded)."""
     rank, local_rank, world = dist_env()
     if rank != 0:
         return 0
-    import keepsake_b200 as ks
-    g = make_generated(ks)
+    ol = oracle_module()
+    orc = ol.load()
+    g = orc.generate("icosphere", 0, level=8, sky=(2048, 1024), resolution=(W_RES, H_RES))
+    params = orc.params(render_width=W_RES, render_height=H_RES, spp=SPP, bounces=BOUNCES, rng_seed=0)
     threads = os.cpu_count() or 1
-    r = run_cpu(ks, g, args.steps, args.warmup, threads)
+    r = run_cpu(orc, g.desc, g.camera, params, args.steps, args.warmup, threads)
     v = r["rays"] / r["seconds"] / 1e6
     line = {
         "impl": "reference", "metric": "Mrays/s (closest-hit + shadow queries), small_pt on the icosphere frame",
         "value": v, "unit": "Mrays/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 * r["seconds"] / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
-        "config": {"workload": WORKLOAD, "sample": r["sample"]},
+        "config": bench_config(args.gpus),
         "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": threads, "kind": "port", "sample": r["sample"]},
         "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -522,24 +646,52 @@ def main():
         dev_ms, (rays, paths) = reduce_ranks(pg, torch, dev_ms, [rays, paths], "cuda")
     value = rays / (dev_ms / 1e3) / 1e6
 
-    # roofline of the dominant kernel (closest-hit traversal); algorithmic bytes per query:
-    # 64 B per interior node fetched + 48 B per triangle tested + 32 B ray read + 16 B hit write
+    # the CPU baseline leg: the oracle on a bounded sample of the same frame (rank 0 at N = 1), and
+    # the oracle's count of the frame's per-query work for the roofline
+    cpu = owork = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        orc = oracle_module().load()
+        threads = os.cpu_count() or 1
+        r = run_cpu(orc, g.desc, cam, params, 1, 0, threads)
+        cpu = {"value": r["rays"] / r["seconds"] / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "port",
+               "sample": r["sample"] + "; oracle restatement of small_pt over the reference cuda/sbvh.cu traversal"}
+        owork = oracle_work(r["scene"], cam, params, threads)
+
+    # roofline of the dominant kernel (closest-hit traversal).  Algorithmic bytes per query as the
+    # oracle counts them on this frame: 32 B per node whose bound the reference traversal tests +
+    # 48 B per triangle tested + 32 B ray read + 16 B hit write; beside it the kernel's own count:
+    # 64 B per half of each 128-B 4-wide node fetched + 48 B per triangle tested + 48 B ray/hit I/O.
     ext_ms = sum(s.ms_extend for s in stats)
     shade_ms = sum(s.ms_shade for s in stats)
     shadow_ms = sum(s.ms_shadow for s in stats)
     ext_q = sum(s.extension_rays for s in stats)
-    ext_bytes = sum(s.ext_nodes * 64 + s.ext_tris * 48 for s in stats) + ext_q * (32 + 16)
+    kernel_bytes = sum(s.ext_nodes * 64 + s.ext_tris * 48 for s in stats) + ext_q * (32 + 16)
     launches = sum(s.iterations for s in stats)
     peak, peak_kind = measured_peaks()
-    achieved = ext_bytes / (ext_ms / 1e3) / 1e9
+    achieved_kernel = kernel_bytes / (ext_ms / 1e3) / 1e9
     tpq = profile_traffic()
-    roofline = {"kernel": "k_extend (closest-hit SBVH traversal)", "bound": "hbm", "achieved": achieved,
-                "peak": peak, "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+    roofline = {"kernel": "k_extend_pt (closest-hit SBVH traversal)", "bound": "hbm", "peak": peak,
+                "peak_source": peak_kind, "unit": "GB/s",
                 "traffic": (tpq * ext_q / launches) if tpq else None,
-                "algorithmic_bytes_per_launch": ext_bytes / launches,
-                "nodes_per_query": sum(s.ext_nodes for s in stats) / ext_q,
-                "tris_per_query": sum(s.ext_tris for s in stats) / ext_q,
+                "traffic_source": "profiles/k_extend_pt_icosphere_l8.json (ncu DRAM bytes per query x queries per "
+                                  "launch)" if tpq else None,
+                "achieved_kernel_counted": achieved_kernel, "frac_kernel_counted": achieved_kernel / peak,
+                "kernel_bytes_per_launch": kernel_bytes / launches,
+                "kernel_wide_nodes_per_query": sum(s.ext_nodes for s in stats) / 2 / ext_q,
+                "kernel_tris_per_query": sum(s.ext_tris for s in stats) / ext_q,
                 "share": {"extend": ext_ms / dev_ms, "shade_raygen": shade_ms / dev_ms, "shadow": shadow_ms / dev_ms}}
+    if owork:
+        bpq = 32.0 * owork["ext_nodes_per_query"] + 48.0 * owork["ext_tris_per_query"] + 48.0
+        achieved = ext_q * bpq / (ext_ms / 1e3) / 1e9
+        roofline.update(achieved=achieved, frac=achieved / peak, algorithmic_bytes_per_query=bpq,
+                        algorithmic_bytes_per_launch=ext_q * bpq / launches,
+                        bytes_model="32 B x nodes + 48 B x triangles tested by the reference traversal (counted "
+                                    "by the oracle on the same frame) + 48 B of ray and hit I/O",
+                        oracle_counts=owork)
+    else:
+        roofline.update(achieved=achieved_kernel, frac=achieved_kernel / peak,
+                        algorithmic_bytes_per_launch=kernel_bytes / launches,
+                        bytes_model="the kernel's own fetch count (no CPU leg in this run)")
 
     # ---- end to end through the host-buffer C ABI ----
     e2e_steps = args.e2e_steps if args.e2e_steps is not None else args.steps
@@ -573,14 +725,9 @@ def main():
            "step_seconds": {key: statistics.median(p[key] for p in e2e_parts) for key in e2e_parts[0]} if e2e_parts
            else None}
 
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        threads = os.cpu_count() or 1
-        r = run_cpu(ks, g, 1, 0, threads)
-        cpu = {"value": r["rays"] / r["seconds"] / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "port",
-               "sample": r["sample"] + "; oracle restatement of small_pt over the reference cuda/sbvh.cu traversal"}
-
-    ttr = c4 = c5 = None
+    ttr = c1 = c4 = c5 = None
+    if rank == 0 and world == 1 and not args.no_c1:
+        c1 = box_room_leg(ks, ctx, torch, not args.no_cpu_baseline)
     if rank == 0 and world == 1 and not args.no_ttr:
         ttr = time_to_relmse(ks, ctx, torch, not args.no_cpu_baseline)
     if rank == 0 and world == 1 and not args.no_c4:
@@ -594,10 +741,8 @@ def main():
             "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded procedural scene)",
-            "config": {"workload": WORKLOAD, "triangles": g.n_triangles, "resolution": [W_RES, H_RES], "spp": SPP,
-                       "depth": BOUNCES, "parallelism": f"replicas{world}",
-                       "l2": "inputs larger than L2 (BVH + triangles + sky > 126 MB)",
-                       "bvh_build_ms": build_ms},
+            "config": bench_config(world),
+            "bvh_build_ms": build_ms,
             "mpaths_per_s": paths / (dev_ms / 1e3) / 1e6,
             # the two query kinds separately, over the same device time
             "mrays_per_s_extension": sum(s.extension_rays for s in stats) / (dev_ms / 1e3) / 1e6,
@@ -609,6 +754,7 @@ def main():
             "gpu_launches": sum(s.kernel_launches for s in stats),
             "clocks": clk,
             "time_to_relmse": ttr,
+            "box_room": c1,
             "batched": c4,
             "instanced": c5,
         }

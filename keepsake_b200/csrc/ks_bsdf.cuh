@@ -393,7 +393,9 @@ struct PrincipledT
     {
         float R0 = sqr((1.0f - c.ior) / (1.0f + c.ior));
         float schlick = fresnel_schlick(wo_dot_wh);
-        return std_lerp(c.specular_r0_mul * R0, 1.0f, schlick) / std_lerp(R0, 1.0f, schlick);
+        // ior 1 (R0 = 0) at wo = wh: 0 / 0 in the reference; the ratio's limit there is 1
+        const float den = std_lerp(R0, 1.0f, schlick);
+        return den == 0.0f ? 1.0f : std_lerp(c.specular_r0_mul * R0, 1.0f, schlick) / den;
     }
     KS_D f3 eval_dielectric_specular(f3 wo, f3 wi) const
     {
@@ -579,6 +581,10 @@ struct PrincipledT
                 return mk(0, 0, 0);
             }
             float denom = sqr(dot(wo, wh) + eta * dot(wi, wh));
+            if (denom == 0.0f) { // wi = -wo through ior 1: no density (the reference asserts, :668)
+                pdf = 0.0f;
+                return mk(0, 0, 0);
+            }
             float jac = eta * eta * fabsf(dot(wi, wh)) / denom;
             pdf = D * G1 * fabsf(dot(wo, wh)) / fabsf(wo.z) * jac;
             pdf *= Fr_refr / (Fr_refl + Fr_refr);

@@ -128,7 +128,7 @@ extern "C" ks_status ks_sobol_points(ks_context *ctx, uint32_t full_width, uint3
     uint64_t total = (uint64_t)nx * ny * ns * nd;
     if (total == 0)
         return KS_OK;
-    KS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    KS_CUDA_TRY(ctx, enter_device(ctx));
     int log2_spp, n_digits;
     sobol_setup((int)spp, (int)full_width, (int)full_height, log2_spp, n_digits);
     DevBuf<float> d_out;

@@ -708,7 +708,7 @@ ks_status ks_mbarrier_wait_probe(ks_context *ctx, uint32_t max_polls, int arrive
 {
     if (!ctx || max_polls == 0)
         return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_mbarrier_wait_probe: null context or zero polls");
-    KS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    KS_CUDA_TRY(ctx, enter_device(ctx));
     DevBuf<int> flag;
     KS_CUDA_TRY(ctx, flag.alloc(1));
     KS_CUDA_TRY(ctx, cudaMemsetAsync(flag.ptr, 0, sizeof(int), ctx->stream));
@@ -731,7 +731,7 @@ ks_status ks_guide_create(ks_context *ctx, const ks_guide_params *params, ks_gui
     for (int k = 0; k < 3; ++k)
         if (!(b[3 + k] > b[k]))
             return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_guide_create: empty bound");
-    KS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    KS_CUDA_TRY(ctx, enter_device(ctx));
     ks_guide *g = new (std::nothrow) ks_guide();
     if (!g)
         return fail(ctx, KS_ERR_OUT_OF_MEMORY, "ks_guide_create");
@@ -832,7 +832,7 @@ ks_status ks_guide_last_loss(ks_guide *g, double *loss)
 {
     if (!g || !loss)
         return KS_ERR_INVALID_ARGUMENT;
-    KS_CUDA_TRY(g->ctx, cudaSetDevice(g->ctx->device));
+    KS_CUDA_TRY(g->ctx, enter_device(g->ctx));
     KS_CUDA_TRY(g->ctx, cudaStreamSynchronize(g->ctx->stream));
     KS_CUDA_TRY(g->ctx, cudaMemcpy(loss, g->loss.ptr, sizeof(double), cudaMemcpyDeviceToHost));
     return KS_OK;
@@ -842,7 +842,7 @@ ks_status ks_guide_get_weights(ks_guide *g, float *mlp_weights, float *grid)
 {
     if (!g)
         return KS_ERR_INVALID_ARGUMENT;
-    KS_CUDA_TRY(g->ctx, cudaSetDevice(g->ctx->device));
+    KS_CUDA_TRY(g->ctx, enter_device(g->ctx));
     if (mlp_weights)
         KS_CUDA_TRY(g->ctx, cudaMemcpy(mlp_weights, g->w.ptr, g->w.bytes(), cudaMemcpyDeviceToHost));
     if (grid)
@@ -854,7 +854,7 @@ ks_status ks_guide_set_weights(ks_guide *g, const float *mlp_weights, const floa
 {
     if (!g)
         return KS_ERR_INVALID_ARGUMENT;
-    KS_CUDA_TRY(g->ctx, cudaSetDevice(g->ctx->device));
+    KS_CUDA_TRY(g->ctx, enter_device(g->ctx));
     if (mlp_weights)
         KS_CUDA_TRY(g->ctx, cudaMemcpy(g->w.ptr, mlp_weights, g->w.bytes(), cudaMemcpyHostToDevice));
     if (grid)
@@ -869,7 +869,7 @@ ks_status ks_guide_infer(ks_guide *g, const float *pos, const float *wo, const f
     if (!g || !pos || !wo || !normal || !raw_out)
         return KS_ERR_INVALID_ARGUMENT;
     ks_context *ctx = g->ctx;
-    KS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    KS_CUDA_TRY(ctx, enter_device(ctx));
     if (n == 0)
         return KS_OK;
     DevBuf<float> dp, dw, dn, dout;
@@ -895,7 +895,7 @@ ks_status ks_guide_gradients(ks_guide *g, const float *pos, const float *wo, con
     if (!g || !pos || !wo || !normal || !wi || !target)
         return KS_ERR_INVALID_ARGUMENT;
     ks_context *ctx = g->ctx;
-    KS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    KS_CUDA_TRY(ctx, enter_device(ctx));
     cudaStream_t st = ctx->stream;
     DevBuf<float> dp, dwo, dn, dwi, dt, dpb;
     KS_CUDA_TRY(ctx, dn.alloc(3 * (size_t)n + 3));

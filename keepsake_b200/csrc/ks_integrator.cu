@@ -1486,7 +1486,7 @@ ks_status ks_small_pt_render_device(ks_scene *scene, const ks_camera_desc *camer
 {
     if (!scene || !camera || !params || !accum_rgb_device || !weights_device)
         return fail(scene ? scene->ctx : nullptr, KS_ERR_INVALID_ARGUMENT, "ks_small_pt_render_device: null");
-    KS_CUDA_TRY(scene->ctx, cudaSetDevice(scene->ctx->device));
+    KS_CUDA_TRY(scene->ctx, enter_device(scene->ctx));
     return render_impl(scene, camera, params, nullptr, nullptr, accum_rgb_device, weights_device, nullptr, nullptr);
 }
 
@@ -1497,7 +1497,7 @@ static ks_status render_host(ks_scene *scene, const ks_camera_desc *camera, cons
     if (!scene || !camera || !params || !accum_rgb || !weights)
         return fail(scene ? scene->ctx : nullptr, KS_ERR_INVALID_ARGUMENT, "ks_small_pt_render: null");
     ks_context *ctx = scene->ctx;
-    KS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    KS_CUDA_TRY(ctx, enter_device(ctx));
     if (params->render_width <= 0 || params->render_height <= 0)
         return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_small_pt_render: bad resolution");
     size_t na = (size_t)params->render_width * params->render_height * 3;
@@ -1575,7 +1575,7 @@ ks_status ks_small_pt_render_guided_device(ks_scene *scene, const ks_camera_desc
 {
     if (!scene || !camera || !params || !guide || !options || !accum_rgb_device || !weights_device)
         return fail(scene ? scene->ctx : nullptr, KS_ERR_INVALID_ARGUMENT, "ks_small_pt_render_guided_device: null");
-    KS_CUDA_TRY(scene->ctx, cudaSetDevice(scene->ctx->device));
+    KS_CUDA_TRY(scene->ctx, enter_device(scene->ctx));
     return render_impl(scene, camera, params, nullptr, nullptr, accum_rgb_device, weights_device, nullptr, nullptr,
                        guide, options);
 }
@@ -1588,7 +1588,7 @@ ks_status ks_small_pt_render_device_progress(ks_scene *scene, const ks_camera_de
     if (!scene || !camera || !params || !progress || !accum_rgb_device || !weights_device || (guide && !options))
         return fail(scene ? scene->ctx : nullptr, KS_ERR_INVALID_ARGUMENT,
                     "ks_small_pt_render_device_progress: null argument");
-    KS_CUDA_TRY(scene->ctx, cudaSetDevice(scene->ctx->device));
+    KS_CUDA_TRY(scene->ctx, enter_device(scene->ctx));
     return render_impl(scene, camera, params, nullptr, nullptr, accum_rgb_device, weights_device, nullptr, nullptr,
                        guide, guide ? options : nullptr, progress, user);
 }
@@ -1599,7 +1599,7 @@ ks_status ks_image_rel_mse_device(ks_context *ctx, const double *accum_rgb_devic
 {
     if (!ctx || !accum_rgb_device || !weights_device || !reference_rgb_device || !rel_mse)
         return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_image_rel_mse_device: null argument");
-    KS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    KS_CUDA_TRY(ctx, enter_device(ctx));
     *rel_mse = 0.0;
     if (n_pixels == 0)
         return KS_OK;
@@ -1632,7 +1632,7 @@ ks_status ks_batch_render_device(ks_context *ctx, const ks_batch_job *jobs, uint
 {
     if (!ctx)
         return KS_ERR_INVALID_ARGUMENT;
-    KS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    KS_CUDA_TRY(ctx, enter_device(ctx));
     ks_batch_options o{0, 0, 1};
     if (options)
         o = *options;
@@ -1644,7 +1644,7 @@ ks_status ks_batch_autotune(ks_context *ctx, const ks_batch_job *jobs, uint32_t 
 {
     if (!ctx || !jobs || !best || n_jobs == 0)
         return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_batch_autotune: null argument");
-    KS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    KS_CUDA_TRY(ctx, enter_device(ctx));
     // sample: up to 8 evenly spaced jobs at no more than 4 spp, into scratch images
     const uint32_t m = std::min<uint32_t>(n_jobs, 8);
     std::vector<ks_batch_job> sample(m);

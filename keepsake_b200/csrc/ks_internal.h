@@ -31,6 +31,18 @@ inline ks_status fail(ks_context *ctx, ks_status s, const std::string &msg)
     return s;
 }
 
+// Makes the context's device current at the start of an entry point and clears a launch error
+// left in the thread's CUDA state by earlier code (another library, or a call that already
+// reported its failure), so that the checks after this call's launches see only its own errors.
+// Errors that poison the context (a fault) are sticky and still surface.
+inline cudaError_t enter_device(const ks_context *ctx)
+{
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e == cudaSuccess)
+        cudaGetLastError();
+    return e;
+}
+
 inline ks_status cuda_fail(ks_context *ctx, cudaError_t e, const char *what)
 {
     return fail(ctx, e == cudaErrorMemoryAllocation ? KS_ERR_OUT_OF_MEMORY : KS_ERR_CUDA,

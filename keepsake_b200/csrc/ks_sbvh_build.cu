@@ -1388,13 +1388,20 @@ ks_status build_sbvh(ks_scene *scene, const ks_sbvh_options &o, float *build_ms)
         }
     }
     float ms = 0;
-    cudaEventSynchronize(ev1);
-    cudaEventElapsedTime(&ms, ev0, ev1);
-    if (widened) {
-        float mw = 0;
-        cudaEventSynchronize(ev3);
-        cudaEventElapsedTime(&mw, ev2, ev3);
-        ms += mw;
+    if (s == KS_OK) {
+        cudaEventSynchronize(ev1);
+        cudaEventElapsedTime(&ms, ev0, ev1);
+        if (widened) {
+            float mw = 0;
+            cudaEventSynchronize(ev3);
+            cudaEventElapsedTime(&mw, ev2, ev3);
+            ms += mw;
+        }
+    } else {
+        // a build that stopped early leaves its work on the stream: let it finish before the
+        // scratch is reused, and keep no error of it for the next call
+        cudaStreamSynchronize(st);
+        cudaGetLastError();
     }
     cudaEventDestroy(ev0);
     cudaEventDestroy(ev1);

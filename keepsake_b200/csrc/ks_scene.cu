@@ -331,7 +331,7 @@ ks_status ks_scene_create(ks_context *ctx, const ks_scene_desc *desc, ks_scene *
                                                           "has_emission out of range (zero-initialise the "
                                                           "descriptor)");
     }
-    KS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    KS_CUDA_TRY(ctx, enter_device(ctx));
     ks_scene *s = new (std::nothrow) ks_scene();
     if (!s)
         return fail(ctx, KS_ERR_OUT_OF_MEMORY, "ks_scene_create");
@@ -480,7 +480,7 @@ ks_status ks_scene_build_bvh(ks_scene *scene, const ks_sbvh_options *opts, float
     ks_sbvh_options o{4, 12, 1.0f, 1e-5f};
     if (opts)
         o = *opts;
-    KS_CUDA_TRY(scene->ctx, cudaSetDevice(scene->ctx->device));
+    KS_CUDA_TRY(scene->ctx, enter_device(scene->ctx));
     scene->bvh_built = false;
     scene->lights_built = false;
     ks_status st = build_sbvh(scene, o, build_ms);
@@ -511,7 +511,7 @@ ks_status ks_sbvh_export(const ks_scene *scene, float *node_bounds, uint32_t *no
         return fail(ctx, KS_ERR_NOT_BUILT, "ks_sbvh_export: call ks_scene_build_bvh first");
     if (scene->n_instances)
         return fail(ctx, KS_ERR_UNSUPPORTED, "ks_sbvh_export: instanced scenes have one SBVH per prototype");
-    KS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    KS_CUDA_TRY(ctx, enter_device(ctx));
     std::vector<RefNode> nodes(scene->n_nodes);
     KS_CUDA_TRY(ctx, cudaMemcpy(nodes.data(), scene->ref_nodes.ptr, sizeof(RefNode) * nodes.size(),
                                 cudaMemcpyDeviceToHost));
@@ -548,7 +548,7 @@ static ks_status trace_rays_impl(ks_scene *scene, const float *rays, uint32_t n,
         return fail(ctx, KS_ERR_NOT_BUILT, std::string(name) + ": call ks_scene_build_bvh first");
     if (n == 0)
         return KS_OK;
-    KS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    KS_CUDA_TRY(ctx, enter_device(ctx));
     DevBuf<float> d_rays, d_t, d_bary;
     DevBuf<uint32_t> d_tri, d_fetch;
     DevBuf<int> d_flag;

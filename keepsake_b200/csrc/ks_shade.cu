@@ -486,7 +486,7 @@ ks_status bsdf_hook(ks_context *ctx, const ks_material_desc *mat, uint32_t n, co
     MaterialGPU g;
     if (!material_to_gpu(*mat, g))
         return fail(ctx, KS_ERR_INVALID_ARGUMENT, std::string(what) + ": invalid material");
-    KS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    KS_CUDA_TRY(ctx, enter_device(ctx));
     const size_t v3 = 3 * (size_t)n * sizeof(float);
     DevBuf<float> buf;
     KS_CUDA_TRY(ctx, buf.alloc(3 * 3 * (size_t)n + 3 * (size_t)n + n));

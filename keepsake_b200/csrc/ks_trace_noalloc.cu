@@ -102,7 +102,7 @@ extern "C" ks_status ks_trace_rays_noalloc(ks_scene *scene, const float *rays, u
         return KS_OK;
     if (ctx->device < 0 || ctx->device >= kMaxDevices)
         return fail(ctx, KS_ERR_UNSUPPORTED, "ks_trace_rays_noalloc: device index too large");
-    KS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    KS_CUDA_TRY(ctx, enter_device(ctx));
     NoAllocScratch *s = nullptr;
     KS_CUDA_TRY(ctx, noalloc_scratch(ctx->device, &s));
     cudaStream_t st = ctx->stream;

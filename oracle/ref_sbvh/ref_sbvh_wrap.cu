@@ -137,6 +137,96 @@ uint32_t ksref_sbvh_intersect1(void *handle, const float *r, int any_hit, float 
     return rec.tri_idx;
 }
 
+// SBVH::intersect / intersectBool (cuda/sbvh.cu:512-603) restated over the reference's own node and
+// primitive arrays, with the same bound and triangle tests (isect_ray_aabb with RayBoundHelper,
+// cuda/aabb.cuh:155-252; the culling check and isect_ray_tri of IsectQuery, cuda/sbvh.cu:485-504)
+// in the same order, counting the work of the query: counts[0] += nodes whose bound is tested,
+// counts[1] += triangles tested.  These are the algorithmic units of a query (32-byte nodes,
+// triangles of three vertices + an index triple).  The stack holds 64 entries like the reference's;
+// a deeper push ends the query and sets counts[2].  Returns what ksref_sbvh_intersect1 returns.
+uint32_t ksref_sbvh_intersect1_counted(void *handle, const float *r, int any_hit, int culling, float *t, float *bary,
+                                       uint64_t *counts)
+{
+    auto *h = (RefHandle *)handle;
+    const ksc::SBVH &b = h->bvh;
+    ksc::Ray ray(ksc::vec3(r[0], r[1], r[2]), ksc::vec3(r[4], r[5], r[6]), r[3], r[7]);
+    const ksc::RayBoundHelper rb(ray);
+    const ksc::RayTriHelper rt(ray);
+    const ksc::SBVHCulling cull = (ksc::SBVHCulling)culling;
+    auto tri_test = [&](uint32_t tri, ksc::RayTriIsect *isect) {
+        auto v = b.tri_verts(tri);
+        float check = ksc::dot(ray.dir, ksc::cross(v[1] - v[0], v[2] - v[1]));
+        if (check >= 0.0f && cull == ksc::SBVHCulling::CullBackface)
+            return false;
+        if (check <= 0.0f && cull == ksc::SBVHCulling::CullFrontFace)
+            return false;
+        return ksc::isect_ray_tri(ray, rt, v[0], v[1], v[2], isect);
+    };
+    uint32_t stack_node[64], stack_cnt[64];
+    int sp = 0;
+    uint32_t node_i = 0, cnt = (uint32_t)b.primitives.size, result = ~0u;
+    float thit = 0.0f;
+    ksc::vec3 coord(0.0f);
+    while (true) {
+        const ksc::SBVHNode &node = b.nodes[node_i];
+        ++counts[0];
+        bool pop = false;
+        if (!ksc::isect_ray_aabb(ray, node.bound, rb)) {
+            pop = true;
+        } else if (node.is_leaf()) {
+            for (uint32_t i = 0; i < cnt; ++i) {
+                const uint32_t tri = b.primitives[i + node.primOffset].shapeIndex;
+                ++counts[1];
+                ksc::RayTriIsect isect;
+                if (any_hit) {
+                    if (tri_test(tri, nullptr))
+                        return 1u;
+                } else if (tri_test(tri, &isect) && isect.tHit < ray.tmax) {
+                    ray.tmax = isect.tHit;
+                    thit = isect.tHit;
+                    coord = isect.coord;
+                    result = tri;
+                }
+            }
+            pop = true;
+        } else {
+            const uint32_t right = node.rightChildOffset;
+            const uint32_t left_cnt = b.nodes[right].primOffset - node.primOffset, right_cnt = cnt - left_cnt;
+            if (sp == 64) {
+                counts[2] = 1;
+                break;
+            }
+            if (rb.dir_is_neg[node.splitAxis]) {
+                stack_node[sp] = node_i + 1;
+                stack_cnt[sp++] = left_cnt;
+                node_i = right;
+                cnt = right_cnt;
+            } else {
+                stack_node[sp] = right;
+                stack_cnt[sp++] = right_cnt;
+                node_i = node_i + 1;
+                cnt = left_cnt;
+            }
+        }
+        if (pop) {
+            if (sp == 0)
+                break;
+            --sp;
+            node_i = stack_node[sp];
+            cnt = stack_cnt[sp];
+        }
+    }
+    if (any_hit)
+        return 0u;
+    if (result != ~0u) {
+        *t = thit;
+        bary[0] = coord.x;
+        bary[1] = coord.y;
+        bary[2] = coord.z;
+    }
+    return result;
+}
+
 // The reference's own watertight ray/triangle test (cuda/ray_tri.cuh:46-97, through the query of
 // cuda/sbvh.cu with culling off) of triangle tri[i] against ray i over the ray's [tmin, tmax]:
 // hit[i] = 1 and t[i] = its distance on a hit, else hit[i] = 0.  Used to prove a hit-id

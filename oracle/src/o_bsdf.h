@@ -424,7 +424,10 @@ struct PrincipledT
     {
         float R0 = sqr((1.0f - c.ior) / (1.0f + c.ior));
         float schlick = fresnel_schlick(wo_dot_wh);
-        return std::lerp(c.specular_r0_mul * R0, 1.0f, schlick) / std::lerp(R0, 1.0f, schlick);
+        // ior 1 (R0 = 0) at wo = wh: 0 / 0 in the reference (principled_bsdf.cpp:508-513); the
+        // ratio's limit there is 1
+        const float den = std::lerp(R0, 1.0f, schlick);
+        return den == 0.0f ? 1.0f : std::lerp(c.specular_r0_mul * R0, 1.0f, schlick) / den;
     }
     V3 eval_dielectric_specular(V3 wo, V3 wi) const
     {
@@ -613,6 +616,10 @@ struct PrincipledT
                 return V3();
             }
             float denom = sqr(dot(wo, wh) + eta * dot(wi, wh));
+            if (denom == 0.0f) { // wi = -wo through ior 1: no density (the reference asserts a finite pdf)
+                pdf = 0.0f;
+                return V3();
+            }
             float jacobian = eta * eta * std::abs(dot(wi, wh)) / denom;
             pdf = D * G1 * std::abs(dot(wo, wh)) / std::abs(wo.z) * jacobian;
             pdf *= Fr_refr / (Fr_refl + Fr_refr);

@@ -27,6 +27,7 @@
 #include <atomic>
 #include <cstdint>
 #include <memory>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -34,6 +35,7 @@ extern "C" {
 int ksref_sbvh_build(const float *, uint32_t, const uint32_t *, uint32_t, uint32_t, uint32_t, float, float, void **,
                      uint32_t *, uint32_t *);
 uint32_t ksref_sbvh_intersect1(void *, const float *, int, float *, float *);
+uint32_t ksref_sbvh_intersect1_counted(void *, const float *, int, int, float *, float *, uint64_t *);
 void ksref_sbvh_bound(void *, float *);
 void ksref_sbvh_destroy(void *);
 }
@@ -473,16 +475,35 @@ inline Intersection make_intersection(const Scene &s, uint32_t tri, float t, flo
     return it;
 }
 
-inline bool intersect(const Scene &s, V3 o, V3 d, float tmax, uint32_t &tri, float &t, float bary[3])
+// Work of the ray queries, counted by the restatement of the reference traversal (nodes whose
+// bound is tested, triangles tested), and the queries where that restatement's answer differed
+// from the reference's own SBVH::intersect / intersectBool (none expected).
+struct Work
+{
+    uint64_t ext[3] = {0, 0, 0}, shadow[3] = {0, 0, 0}; // nodes, triangles, stack overflows
+    uint64_t mismatches = 0;
+};
+
+inline bool intersect(const Scene &s, V3 o, V3 d, float tmax, uint32_t &tri, float &t, float bary[3],
+                      Work *work = nullptr)
 {
     float r[8] = {o.x, o.y, o.z, 0.0f, d.x, d.y, d.z, tmax};
     tri = ksref_sbvh_intersect1(s.bvh, r, 0, &t, bary);
+    if (work) {
+        float t2 = 0.0f, b2[3] = {0, 0, 0};
+        uint32_t tri2 = ksref_sbvh_intersect1_counted(s.bvh, r, 0, 2, &t2, b2, work->ext);
+        if (tri2 != tri || (tri != ~0u && std::memcmp(&t2, &t, sizeof(float)) != 0))
+            ++work->mismatches;
+    }
     return tri != ~0u;
 }
-inline bool occluded(const Scene &s, V3 o, V3 d, float tmax)
+inline bool occluded(const Scene &s, V3 o, V3 d, float tmax, Work *work = nullptr)
 {
     float r[8] = {o.x, o.y, o.z, 0.0f, d.x, d.y, d.z, tmax};
-    return ksref_sbvh_intersect1(s.bvh, r, 1, nullptr, nullptr) != 0;
+    const bool occ = ksref_sbvh_intersect1(s.bvh, r, 1, nullptr, nullptr) != 0;
+    if (work && (ksref_sbvh_intersect1_counted(s.bvh, r, 1, 2, nullptr, nullptr, work->shadow) != 0) != occ)
+        ++work->mismatches;
+    return occ;
 }
 
 // spawn_ray<OffsetType::NextBounce> (ray.h:89-96): returns the offset origin
@@ -572,6 +593,7 @@ struct Tracer
     const Scene &s;
     const ks_small_pt_params &in;
     Counters cnt;
+    Work *work = nullptr; // counts the queries' nodes and triangles when set
 
     // next_event_estimate (nee.cpp:11-57)
     V3 nee(const Bsdf &bsdf, const Intersection &hit, V3 wo, OwenScrambledSobol02Morton &sobol)
@@ -622,7 +644,7 @@ struct Tracer
             if (!is_zero(f) && pdf_wi_bsdf > 0.0f) {
                 V3 o = spawn_origin(hit.p, wi, hit.frame.n);
                 cnt.shadow++;
-                if (!occluded(s, o, wi, wi_dist)) {
+                if (!occluded(s, o, wi, wi_dist, work)) {
                     float mis_weight = delta_light ? 1.0f : power_heur(pdf_wi_light, pdf_wi_bsdf);
                     beta_nee += Le_beta * f * mis_weight / pr_light;
                 }
@@ -640,7 +662,7 @@ struct Tracer
             uint32_t tri;
             float t, bary[3];
             cnt.extension++;
-            bool isect_geom = intersect(s, ro, rd, inf, tri, t, bary);
+            bool isect_geom = intersect(s, ro, rd, inf, tri, t, bary, work);
             if (!isect_geom) {
                 if (s.sky) {
                     uint32_t light_index = 0;
@@ -942,12 +964,28 @@ int oracle_sky_tables(void *sp, float *cond, float *margin)
     return 0;
 }
 
+int oracle_render_range(void *sp, const ks_camera_desc *cam, const ks_small_pt_params *in, int s_begin, int s_end,
+                        double *accum, double *weights, int n_threads, uint64_t *counts, uint64_t *work_out);
+
 // SmallPT::run (small_pt.cpp:15-70) on n_threads host threads over 4x4 pixel tiles
 // (parallel.h:93-113).  accum: W*H*3 doubles, weights: W*H*2 doubles (both zero-initialised by
 // the caller and accumulated into).  counts[0..1] receive extension and shadow ray counts.
 int oracle_render(void *sp, const ks_camera_desc *cam, const ks_small_pt_params *in, double *accum, double *weights,
                   int n_threads, uint64_t *counts)
 {
+    return oracle_render_range(sp, cam, in, 0, in->spp, accum, weights, n_threads, counts, nullptr);
+}
+
+// The same render restricted to the sample indices [s_begin, s_end) of the in->spp samples per
+// pixel (one spp interval of SmallPT::run, small_pt.cpp:56-66, or any bounded part of the frame's
+// samples).  work_out (7 values, may be NULL): the extension queries' nodes, triangles and stack
+// overflows, the shadow queries' nodes, triangles and overflows, counted by the restatement of the
+// reference traversal, then the number of queries where it disagreed with the reference's own.
+int oracle_render_range(void *sp, const ks_camera_desc *cam, const ks_small_pt_params *in, int s_begin, int s_end,
+                        double *accum, double *weights, int n_threads, uint64_t *counts, uint64_t *work_out)
+{
+    if (s_begin < 0 || s_end > in->spp || s_begin > s_end)
+        return 1;
     Scene &s = *(Scene *)sp;
     const int W = in->render_width, H = in->render_height;
     int cx = 0, cy = 0, cw = W, ch = H;
@@ -964,9 +1002,14 @@ int oracle_render(void *sp, const ks_camera_desc *cam, const ks_small_pt_params 
     const int tiles_x = (cw + 3) / 4, tiles_y = (ch + 3) / 4;
     std::atomic<int> next_tile{0};
     std::atomic<uint64_t> n_ext{0}, n_shadow{0};
+    std::mutex work_mutex;
+    Work work_total;
     const PixelFilterTable filter(in->pixel_filter, in->pixel_filter_width, in->pixel_filter_sigma);
     auto worker = [&]() {
         Tracer tr{s, *in, {}};
+        Work work;
+        if (work_out)
+            tr.work = &work;
         while (true) {
             int tile = next_tile.fetch_add(1);
             if (tile >= tiles_x * tiles_y)
@@ -976,7 +1019,7 @@ int oracle_render(void *sp, const ks_camera_desc *cam, const ks_small_pt_params 
                 for (int ox = tx * 4; ox < std::min(cw, tx * 4 + 4); ++ox) {
                     int px = cx + ox, py = cy + oy;
                     size_t pix = (size_t)py * W + px;
-                    for (int smp = 0; smp < in->spp; ++smp) {
+                    for (int smp = s_begin; smp < s_end; ++smp) {
                         PTRenderSampler sampler(W, H, px, py, in->spp, smp, in->rng_seed);
                         float offx = 0.0f, offy = 0.0f;
                         if (in->spp != 1) {
@@ -1012,6 +1055,12 @@ int oracle_render(void *sp, const ks_camera_desc *cam, const ks_small_pt_params 
         }
         n_ext += tr.cnt.extension;
         n_shadow += tr.cnt.shadow;
+        std::lock_guard<std::mutex> lock(work_mutex);
+        for (int k = 0; k < 3; ++k) {
+            work_total.ext[k] += work.ext[k];
+            work_total.shadow[k] += work.shadow[k];
+        }
+        work_total.mismatches += work.mismatches;
     };
     int nt = std::max(1, n_threads);
     std::vector<std::thread> pool;
@@ -1022,6 +1071,13 @@ int oracle_render(void *sp, const ks_camera_desc *cam, const ks_small_pt_params 
     if (counts) {
         counts[0] = n_ext.load();
         counts[1] = n_shadow.load();
+    }
+    if (work_out) {
+        for (int k = 0; k < 3; ++k) {
+            work_out[k] = work_total.ext[k];
+            work_out[3 + k] = work_total.shadow[k];
+        }
+        work_out[6] = work_total.mismatches;
     }
     return 0;
 }

@@ -20,6 +20,24 @@ def P(a):
     return None if a is None else ctypes.c_void_p(a.ctypes.data)
 
 
+# Mirrors of include/ks_b200.h's camera and render-parameter structs, so that CPU-only callers of
+# the oracle (bench.py's reference arm) need not load the CUDA library.
+class CameraDesc(ctypes.Structure):
+    _fields_ = [("camera_to_world", ctypes.c_float * 16), ("proj_to_camera", ctypes.c_float * 16),
+                ("proj_to_world", ctypes.c_float * 16), ("orthographic", ctypes.c_int32)]
+
+
+class SmallPTParams(ctypes.Structure):
+    _fields_ = [("include_background", ctypes.c_int32), ("backdrop", ctypes.c_float * 3),
+                ("bounces", ctypes.c_int32), ("render_width", ctypes.c_int32), ("render_height", ctypes.c_int32),
+                ("crop_start_x", ctypes.c_int32), ("crop_start_y", ctypes.c_int32), ("crop_width", ctypes.c_int32),
+                ("crop_height", ctypes.c_int32), ("spp", ctypes.c_int32), ("rng_seed", ctypes.c_int32),
+                ("scale_ray_diff", ctypes.c_int32), ("clamp_direct", ctypes.c_float),
+                ("clamp_indirect", ctypes.c_float), ("spp_prog_interval", ctypes.c_int32),
+                ("pixel_filter_width", ctypes.c_float), ("pixel_filter", ctypes.c_int32),
+                ("pixel_filter_sigma", ctypes.c_float)]
+
+
 class Oracle:
     def __init__(self):
         self.lib = ctypes.CDLL(ORACLE_SO)
@@ -37,10 +55,42 @@ class Oracle:
         L.oracle_light_table.restype = _u32
         L.oracle_sky_tables.argtypes = [_vp, _vp, _vp]
         L.oracle_render.argtypes = [_vp, _vp, _vp, _vp, _vp, ctypes.c_int, _vp]
+        L.oracle_render_range.argtypes = [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, ctypes.c_int, _vp, _vp]
+        L.oracle_render_range.restype = ctypes.c_int
         L.oracle_bsdf_eval.argtypes = [_vp, _vp, _vp, _u32, _vp, _vp]
         L.oracle_bsdf_eval.restype = None
         L.oracle_bsdf_sample.argtypes = [_vp, _vp, _vp, _u32, _vp, _vp, _vp]
         L.oracle_bsdf_sample.restype = None
+        L.oracle_generate.argtypes = [ctypes.c_char_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_float, ctypes.c_float,
+                                      ctypes.c_int, _u32, _u32, _u32, _u32]
+        L.oracle_generate.restype = _vp
+        L.oracle_generated_desc.argtypes = [_vp]
+        L.oracle_generated_desc.restype = _vp
+        L.oracle_generated_camera.argtypes = [_vp, _vp, _vp, _vp]
+        L.oracle_generated_camera.restype = None
+        L.oracle_generated_destroy.argtypes = [_vp]
+        L.oracle_generated_destroy.restype = None
+        L.oracle_camera_perspective.argtypes = [_vp, ctypes.c_float, ctypes.c_float, _vp]
+        L.oracle_camera_perspective.restype = ctypes.c_int
+        L.oracle_params_default.argtypes = [_vp]
+        L.oracle_params_default.restype = None
+
+    def generate(self, kind, seed=0, level=8, roughness=(0.05, 1.0), occluder=False, sky=(2048, 1024),
+                 resolution=(1024, 1024)):
+        """A seeded synthetic scene (the library's generator, compiled into the oracle library) with
+        its camera: (OracleGenerated, CameraDesc)."""
+        return OracleGenerated(self, kind, seed, level, roughness, occluder, sky, resolution)
+
+    def params(self, **kw):
+        """SmallPTParams with the small_pt task's defaults, then the given fields."""
+        p = SmallPTParams()
+        self.lib.oracle_params_default(ctypes.byref(p))
+        for k, v in kw.items():
+            if k == "backdrop":
+                p.backdrop[:] = v
+            else:
+                setattr(p, k, v)
+        return p
 
     def scene(self, desc, keepalive=None):
         return OracleScene(self, desc, keepalive)
@@ -81,7 +131,12 @@ class OracleScene:
     def __init__(self, oracle, desc, keepalive=None):
         self.o = oracle
         self._keep = keepalive
-        dp = ctypes.cast(desc, _vp) if isinstance(desc, ctypes._Pointer) else ctypes.cast(ctypes.pointer(desc), _vp)
+        if isinstance(desc, (int, _vp)):
+            dp = desc
+        elif isinstance(desc, ctypes._Pointer):
+            dp = ctypes.cast(desc, _vp)
+        else:
+            dp = ctypes.cast(ctypes.pointer(desc), _vp)
         self.h = oracle.lib.oracle_scene_create(dp, None)
         assert self.h, "oracle_scene_create failed"
 
@@ -108,9 +163,54 @@ class OracleScene:
                                  threads, P(counts))
         return accum, weights, counts
 
+    def render_range(self, camera, params, s_begin, s_end, threads=None, count_work=False, accum=None,
+                     weights=None):
+        """Samples [s_begin, s_end) of the params.spp samples per pixel, accumulated into accum /
+        weights (fresh zero arrays when None).  Returns (accum, weights, counts, work): counts =
+        (extension, shadow) queries; work (count_work) = dict of the queries' nodes and triangles
+        counted by the restatement of the reference traversal, and its disagreements with the
+        reference's own queries."""
+        W, H = params.render_width, params.render_height
+        if accum is None:
+            accum = np.zeros((H, W, 3), np.float64)
+        if weights is None:
+            weights = np.zeros((H, W, 2), np.float64)
+        counts = np.zeros(2, np.uint64)
+        work = np.zeros(7, np.uint64) if count_work else None
+        threads = threads or os.cpu_count() or 1
+        st = self.o.lib.oracle_render_range(self.h, ctypes.byref(camera), ctypes.byref(params), s_begin, s_end,
+                                            P(accum), P(weights), threads, P(counts), P(work))
+        assert st == 0, "oracle_render_range: bad sample range"
+        wd = None
+        if count_work:
+            wd = dict(ext_nodes=int(work[0]), ext_tris=int(work[1]), ext_overflows=int(work[2]),
+                      shadow_nodes=int(work[3]), shadow_tris=int(work[4]), shadow_overflows=int(work[5]),
+                      mismatches=int(work[6]))
+        return accum, weights, counts, wd
+
     def __del__(self):
         try:
             self.o.lib.oracle_scene_destroy(self.h)
+        except Exception:
+            pass
+
+
+class OracleGenerated:
+    def __init__(self, oracle, kind, seed, level, roughness, occluder, sky, resolution):
+        self.o = oracle
+        self.h = oracle.lib.oracle_generate(kind.encode(), seed, level, roughness[0], roughness[1], int(occluder),
+                                            sky[0], sky[1], resolution[0], resolution[1])
+        assert self.h, f"oracle_generate({kind}) failed"
+        self.desc = oracle.lib.oracle_generated_desc(self.h)
+        c2w = (ctypes.c_float * 16)()
+        vfov, aspect = ctypes.c_float(), ctypes.c_float()
+        oracle.lib.oracle_generated_camera(self.h, c2w, ctypes.byref(vfov), ctypes.byref(aspect))
+        self.camera = CameraDesc()
+        assert oracle.lib.oracle_camera_perspective(c2w, vfov.value, aspect.value, ctypes.byref(self.camera)) == 0
+
+    def __del__(self):
+        try:
+            self.o.lib.oracle_generated_destroy(self.h)
         except Exception:
             pass
 

@@ -47,9 +47,10 @@ def chain_rays(n=256):
 
 
 def chain_camera(ks):
-    # look_at from (-1, 0.05, 0.05) toward +x, up +y: columns right (0, 0, 1), up, back (-1, 0, 0), pos
-    c2w = np.array([[0, 0, -1, -1.0], [0, 1, 0, 0.05], [1, 0, 0, 0.05], [0, 0, 0, 1]], np.float32)
-    return ks.camera_perspective(c2w, 0.2, 1.0)
+    # orthographic, from x = -1 toward +x (up +y; columns right (0, 0, 1), up, back (-1, 0, 0), pos):
+    # every camera ray runs parallel to the chain's axis and meets both children at every level
+    c2w = np.array([[0, 0, -1, -1.0], [0, 1, 0, 0.0], [1, 0, 0, 0.0], [0, 0, 0, 1]], np.float32)
+    return ks.camera_orthographic(c2w, -0.2, 0.2, -0.2, 0.2, 0.1, 10.0)
 
 
 def test_deep_chain_outgrows_the_stack(oracle):

@@ -396,3 +396,25 @@ def test_oracle_material_cases_render(oracle):
         assert np.isfinite(a).all() and (a >= 0).all(), name
         assert np.array_equal(w.sum(-1), w0.sum(-1)), name
         assert rel_mse(composite(a, w), composite(a0, w0)) > 1e-3, name
+
+
+def test_oracle_sample_ranges_and_work_counts(oracle):
+    """Rendering the samples of a frame in two ranges adds up to the whole render bit for bit, and
+    the counted restatement of the reference traversal (the roofline's algorithmic units: nodes
+    whose bound is tested, triangles tested) answers every query exactly as the reference's own
+    SBVH::intersect / intersectBool."""
+    import keepsake_b200 as ks
+    g = ks.Generated("icosphere", 0, level=5, sky=(128, 64), resolution=(32, 32))
+    cam = ks.camera_perspective(g.camera_to_world, g.vfov, g.aspect)
+    p = ks.SmallPTParams.make(render_width=32, render_height=32, spp=8, bounces=8)
+    sc = oracle.scene(g.desc)
+    a, w, c = sc.render(cam, p, threads=4)
+    a1, w1, c1, k1 = sc.render_range(cam, p, 0, 3, threads=4, count_work=True)
+    a1, w1, c2, k2 = sc.render_range(cam, p, 3, 8, threads=3, count_work=True, accum=a1, weights=w1)
+    assert np.array_equal(a, a1) and np.array_equal(w, w1)
+    assert np.array_equal(c, c1 + c2)
+    for k in (k1, k2):
+        assert k["mismatches"] == 0 and k["ext_overflows"] == 0 and k["shadow_overflows"] == 0
+        assert k["ext_nodes"] > 0 and k["ext_tris"] > 0 and k["shadow_nodes"] > 0
+    # every closest-hit query tests the root at least
+    assert k1["ext_nodes"] >= c1[0]
