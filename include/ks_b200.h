@@ -124,15 +124,20 @@ typedef struct ks_material_desc {
     float specular;       /* principled_brdf: specular, clamped to [0, 1] and scaled by 0.08 */
 } ks_material_desc;
 
-/* SkyLight (light.h:34-58): ambient colour or a lat-long RGB map. */
+/* The sky light: SkyLight (light.h:34-58), an ambient colour or a lat-long RGB map, or
+ * EqualAreaSkyLight (light.h:60-86, light.cpp:161-206), a square map in the equal-area octahedral
+ * parameterisation of the sphere sampled through an alias table over its texels' luminance (its
+ * sample / pdf / eval as the reference's GPU path defines them, gpu/shaders/light.slang:92-186;
+ * the reference's CPU path leaves them unimplemented). */
 typedef struct ks_sky_desc {
-    int32_t kind;         /* 0 none, 1 ambient, 2 lat-long map */
+    int32_t kind;         /* 0 none, 1 ambient, 2 lat-long map, 3 equal-area map */
     float ambient[3];
-    const float *map_rgb; /* width*height*3 floats, row 0 = theta 0 (light.cpp:33-40) */
+    const float *map_rgb; /* width*height*3 floats; lat-long: row 0 = theta 0 (light.cpp:33-40);
+                             equal-area: width = height, a power of two, at most 16384 */
     uint32_t width;
     uint32_t height;
-    float to_world[16];   /* row-major 4x4 light-to-world */
-    int32_t transform_y_up;
+    float to_world[16];   /* row-major 4x4 light-to-world (equal-area: its 3x3 part, a rotation) */
+    int32_t transform_y_up; /* lat-long maps only */
     float strength;
 } ks_sky_desc;
 

@@ -266,7 +266,7 @@ SceneView make_view(const ks_scene *s)
                                                                                      : kShadePlain;
     v.light_count = s->light_count;
     v.n_nonmesh = s->n_nonmesh;
-    v.n_sky = (s->sky_desc.kind == 1 || s->sky_desc.kind == 2) ? 1u : 0u;
+    v.n_sky = (s->sky_desc.kind >= 1 && s->sky_desc.kind <= 3) ? 1u : 0u;
     v.punctual = s->punctual.ptr;
     v.power_cdf = s->power_cdf.ptr;
     v.tri_light = s->tri_light.ptr;
@@ -279,13 +279,70 @@ SceneView make_view(const ks_scene *s)
     std::memcpy(v.sky_l2w, s->sky_l2w, sizeof(v.sky_l2w));
     std::memcpy(v.sky_w2l, s->sky_w2l, sizeof(v.sky_w2l));
     v.sky_y_up = s->sky_desc.kind == 2 ? s->sky_desc.transform_y_up : 1;
-    v.sky_strength = s->sky_desc.kind == 2 ? s->sky_desc.strength : 1.0f;
+    v.sky_strength = s->sky_desc.kind >= 2 ? s->sky_desc.strength : 1.0f;
+    v.sky_alias = s->sky_alias.ptr;
     v.sky_map = s->sky_map.ptr;
     v.sky_cond = s->sky_cond.ptr;
     v.sky_margin = s->sky_margin.ptr;
     v.sky_cond_guide = s->sky_cond_guide.ptr;
     v.sky_margin_guide = s->sky_margin_guide.ptr;
     return v;
+}
+
+// AliasTable::AliasTable (distrib.cpp:109-165): the weights normalised by their double sum, then
+// Vose's pairing of under- and over-full bins from two work lists used as stacks.  Bins hold
+// (q, p, alias as bits, 0).  False when no weight is positive.
+bool alias_table(const std::vector<float> &weights, std::vector<float4> &bins)
+{
+    const size_t n = weights.size();
+    double sum = 0.0;
+    for (float w : weights)
+        sum += w;
+    if (!(sum > 0.0))
+        return false;
+    std::vector<float> q(n, 0.0f), p(n);
+    std::vector<uint32_t> alias(n, 0);
+    for (size_t i = 0; i < n; ++i)
+        p[i] = (float)(weights[i] / sum);
+    struct Outcome
+    {
+        float p_hat;
+        size_t index;
+    };
+    std::vector<Outcome> under, over;
+    for (size_t i = 0; i < n; ++i) {
+        const float p_hat = p[i] * n;
+        (p_hat < 1 ? under : over).push_back(Outcome{p_hat, i});
+    }
+    while (!under.empty() && !over.empty()) {
+        const Outcome un = under.back(), ov = over.back();
+        under.pop_back();
+        over.pop_back();
+        q[un.index] = un.p_hat;
+        alias[un.index] = (uint32_t)ov.index;
+        const float excess = un.p_hat + ov.p_hat - 1;
+        (excess < 1 ? under : over).push_back(Outcome{excess, ov.index});
+    }
+    while (!over.empty()) {
+        const Outcome ov = over.back();
+        over.pop_back();
+        q[ov.index] = 1;
+        alias[ov.index] = 0xffffffffu;
+    }
+    while (!under.empty()) {
+        const Outcome un = under.back();
+        under.pop_back();
+        q[un.index] = 1;
+        alias[un.index] = 0xffffffffu;
+    }
+    bins.resize(n);
+    for (size_t i = 0; i < n; ++i) {
+        const uint32_t a = alias[i] == 0xffffffffu ? (uint32_t)i : alias[i]; // q = 1: never taken
+        float a_bits;
+        std::memcpy(&a_bits, &a, sizeof(a_bits));
+        bins[i] = make_float4(q[i], p[i], a_bits, 0.0f);
+    }
+    return true;
 }
 
 ks_status build_lights(ks_scene *s)
@@ -375,6 +432,55 @@ ks_status build_lights(ks_scene *s)
                 sum[c] += (double)(float)h_pr[3 * y + c];
         float Phi[3] = {(float)sum[0], (float)sum[1], (float)sum[2]};
         float scale = (pi / h) * (6.28318530718f / w);
+        float ex = s->scene_bound[3] - s->scene_bound[0], ey = s->scene_bound[4] - s->scene_bound[1],
+              ez = s->scene_bound[5] - s->scene_bound[2];
+        float radius = 0.5f * std::sqrt(ex * ex + ey * ey + ez * ez);
+        for (int c = 0; c < 3; ++c) {
+            Phi[c] *= scale;
+            Phi[c] *= pi * (radius * radius);
+        }
+        sky_power_mean = (Phi[0] + Phi[1] + Phi[2]) / 3.0f;
+    }
+    if (sd.kind == 3) {
+        // EqualAreaSkyLight (light.cpp:161-206): the map, an alias table over its texels'
+        // luminance, and unit_power * pi r^2 as its power
+        s->n_nonmesh = 1;
+        const int res = (int)sd.width;
+        const size_t n = (size_t)res * res;
+        s->sky_w = s->sky_h = res;
+        // a rotation: the light-to-world 3x3 of to_world and its transpose (light.slang:104, 153)
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) {
+                s->sky_l2w[3 * r + c] = sd.to_world[4 * r + c];
+                s->sky_w2l[3 * c + r] = sd.to_world[4 * r + c];
+            }
+        KS_CUDA_TRY(ctx, s->sky_map.alloc(n));
+        k_sky_unpack<<<(unsigned)std::min<size_t>((n + 255) / 256, 4096), 256, 0, st>>>(s->sky_rgb.ptr, n,
+                                                                                          s->sky_map.ptr);
+        const std::vector<float> &t = s->sky_host;
+        std::vector<float> lum(n);
+        for (size_t i = 0; i < n; ++i)
+            lum[i] = 0.212671f * t[3 * i] + 0.715160f * t[3 * i + 1] + 0.072169f * t[3 * i + 2];
+        std::vector<float4> bins;
+        if (!alias_table(lum, bins))
+            return fail(ctx, KS_ERR_INVALID_ARGUMENT, "equal-area sky: the map has no positive luminance");
+        KS_CUDA_TRY(ctx, s->sky_alias.alloc(n));
+        KS_CUDA_TRY(ctx, cudaMemcpyAsync(s->sky_alias.ptr, bins.data(), sizeof(float4) * n, cudaMemcpyHostToDevice,
+                                         st));
+        KS_CUDA_TRY(ctx, cudaStreamSynchronize(st)); // bins lives on this stack frame
+        // unit_power (light.cpp:182-198): row sums in float, rows summed in a fixed order
+        double sum[3] = {0, 0, 0};
+        for (int row = 0; row < res; ++row) {
+            float rs[3] = {0, 0, 0};
+            for (int col = 0; col < res; ++col)
+                for (int c = 0; c < 3; ++c)
+                    rs[c] += t[3 * ((size_t)row * res + col) + c];
+            for (int c = 0; c < 3; ++c)
+                sum[c] += rs[c];
+        }
+        const float pi = 3.14159265359f;
+        float Phi[3] = {(float)sum[0], (float)sum[1], (float)sum[2]};
+        const float scale = (4 * pi) / (float)(res * res);
         float ex = s->scene_bound[3] - s->scene_bound[0], ey = s->scene_bound[4] - s->scene_bound[1],
               ez = s->scene_bound[5] - s->scene_bound[2];
         float radius = 0.5f * std::sqrt(ex * ex + ey * ey + ez * ez);

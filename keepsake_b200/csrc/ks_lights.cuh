@@ -53,7 +53,7 @@ struct SceneView
     const float4 *ml_verts;         // 3 per mesh-light triangle: world-space vertices
     const int32_t *inst_light_base; // instanced scenes: flat light index of each instance's first mesh light
     // sky
-    int sky_kind; // 0 none, 1 ambient, 2 map
+    int sky_kind; // 0 none, 1 ambient, 2 lat-long map, 3 equal-area map (sky_w = sky_h = res)
     int sky_w, sky_h;
     float sky_l2w[9], sky_w2l[9];
     int sky_y_up;
@@ -63,6 +63,7 @@ struct SceneView
     const float *sky_margin; // sky_h + 1
     const uint32_t *sky_cond_guide;   // sky_h rows of kGuide
     const uint32_t *sky_margin_guide; // kGuide
+    const float4 *sky_alias;          // equal-area map: res^2 alias-table bins (q, p, alias bits, 0)
 };
 
 // ---- distribution tables ----------------------------------------------------------------------
@@ -187,7 +188,7 @@ KS_D f3 sky_texel(const SceneView &s, int u, int v)
     return mk(c.x, c.y, c.z);
 }
 
-KS_D f3 sky_eval(const SceneView &s, f3 wi)
+KS_D f3 latlong_sky_eval(const SceneView &s, f3 wi)
 {
     f3 wl = mat3_apply(s.sky_w2l, wi);
     float phi, theta;
@@ -206,7 +207,7 @@ KS_D f3 sky_eval(const SceneView &s, f3 wi)
     return L;
 }
 
-KS_D f3 sky_sample(const SceneView &s, float u0, float u1, f3 &wi, float &wi_dist, float &pdf)
+KS_D f3 latlong_sky_sample(const SceneView &s, float u0, float u1, f3 &wi, float &wi_dist, float &pdf)
 {
     float pdf_m, pdf_c;
     uint32_t vi, ui;
@@ -228,10 +229,10 @@ KS_D f3 sky_sample(const SceneView &s, float u0, float u1, f3 &wi, float &wi_dis
     }
     wi = mat3_apply(s.sky_l2w, wl);
     wi_dist = kInf;
-    return sky_eval(s, wi) / pdf;
+    return latlong_sky_eval(s, wi) / pdf;
 }
 
-KS_D float sky_pdf(const SceneView &s, f3 wi)
+KS_D float latlong_sky_pdf(const SceneView &s, f3 wi)
 {
     f3 wl = mat3_apply(s.sky_w2l, wi);
     float phi, theta;
@@ -248,6 +249,194 @@ KS_D float sky_pdf(const SceneView &s, f3 wi)
               distrib_pdf(s.sky_cond + (size_t)y * (s.sky_w + 1), (uint32_t)s.sky_w, (uint32_t)x);
     p /= (2.0f * kPi * kPi * sin_theta);
     return p;
+}
+
+// ---- equal-area sky (EqualAreaSkyLight: light.cpp:161-206; sample / pdf / eval as the
+// reference's GPU path defines them, gpu/shaders/light.slang:92-186) ------------------------------
+// The map is a res x res square in the equal-area octahedral parameterisation of the sphere; a
+// direction is drawn by an alias table over the texels' luminance, then uniformly inside the texel
+// (the second uniform split into two by bit de-interleaving), so the density is constant per texel.
+
+// equal_area_square_to_sphere (gpu/shaders/common.slang:245-265; pbrt-v4's mapping)
+KS_D f3 ea_square_to_sphere(float px, float py)
+{
+    float u = 2 * px - 1, v = 2 * py - 1;
+    float up = fabsf(u), vp = fabsf(v);
+    float signed_distance = 1 - (up + vp);
+    float d = fabsf(signed_distance);
+    float r = 1 - d;
+    float phi = (r == 0 ? 1 : (vp - up) / r + 1) * kPi / 4;
+    float z = copysignf(1 - sqr(r), signed_distance);
+    float cos_phi = copysignf(cosf(phi), u);
+    float sin_phi = copysignf(sinf(phi), v);
+    float s2 = 2 - sqr(r);
+    float st = r * sqrtf(s2 > 0.0f ? s2 : 0.0f);
+    return mk(cos_phi * st, sin_phi * st, z);
+}
+
+// equal_area_sphere_to_square (gpu/shaders/common.slang:267-322): Clarberg's inverse with a 6th
+// degree minimax polynomial for atan(x) 2 / pi, evaluated with fused multiply-adds
+KS_D void ea_sphere_to_square(f3 dir, float &ou, float &ov)
+{
+    float x = fabsf(dir.x), y = fabsf(dir.y), z = fabsf(dir.z);
+    float r2 = 1 - z;
+    float r = sqrtf(r2 > 0.0f ? r2 : 0.0f);
+    float a = fmaxf(x, y), b = fminf(x, y);
+    b = a == 0 ? 0 : b / a;
+    const float t1 = 0.406758566246788489601959989e-5f, t2 = 0.636226545274016134946890922156f,
+                t3 = 0.61572017898280213493197203466e-2f, t4 = -0.247333733281268944196501420480f,
+                t5 = 0.881770664775316294736387951347e-1f, t6 = 0.419038818029165735901852432784e-1f,
+                t7 = -0.251390972343483509333252996350e-1f;
+    float phi = fmaf(t7, b, t6);
+    phi = fmaf(phi, b, t5);
+    phi = fmaf(phi, b, t4);
+    phi = fmaf(phi, b, t3);
+    phi = fmaf(phi, b, t2);
+    phi = fmaf(phi, b, t1);
+    if (x < y)
+        phi = 1 - phi;
+    float v = phi * r;
+    float u = r - v;
+    if (dir.z < 0) {
+        const float t = u;
+        u = 1 - v;
+        v = 1 - t;
+    }
+    u = copysignf(u, dir.x);
+    v = copysignf(v, dir.y);
+    ou = 0.5f * (u + 1);
+    ov = 0.5f * (v + 1);
+}
+
+// equal_area_bilerp (gpu/shaders/common.slang:350-395): the four texels around uv with bilinear
+// weights, folded across the square's edges the way the octahedral parameterisation wraps
+KS_D void ea_bilerp(float ux, float uy, int N, int ix[4], int iy[4], float w[4])
+{
+    float x = ux * N - 0.5f, y = uy * N - 0.5f;
+    int x0 = (int)floorf(x), y0 = (int)floorf(y);
+    float tx = x - x0, ty = y - y0;
+    int x1 = x0 + 1, y1 = y0 + 1;
+    x0 = x0 < 0 ? 0 : (x0 > N - 1 ? N - 1 : x0);
+    y0 = y0 < 0 ? 0 : (y0 > N - 1 ? N - 1 : y0);
+    x1 = x1 < 0 ? 0 : (x1 > N - 1 ? N - 1 : x1);
+    y1 = y1 < 0 ? 0 : (y1 > N - 1 ? N - 1 : y1);
+    w[0] = (1.0f - tx) * (1.0f - ty);
+    w[1] = tx * (1.0f - ty);
+    w[2] = (1.0f - tx) * ty;
+    w[3] = tx * ty;
+    const int xs[4] = {x0, x1, x0, x1}, ys[4] = {y0, y0, y1, y1}, m = N - 1;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const bool mirror = ((xs[k] ^ ys[k]) & N) != 0;
+        const int a = xs[k] & m, b = ys[k] & m;
+        ix[k] = mirror ? m - a : a;
+        iy[k] = mirror ? m - b : b;
+    }
+}
+
+// demux_float (gpu/shaders/common.slang:569-576): the even and odd bits of f's 32-bit fixed-point
+// form, each as a 16-bit fraction
+KS_D uint32_t compact_1_by_1(uint32_t x)
+{
+    x &= 0x55555555u;
+    x = (x ^ (x >> 1)) & 0x33333333u;
+    x = (x ^ (x >> 2)) & 0x0f0f0f0fu;
+    x = (x ^ (x >> 4)) & 0x00ff00ffu;
+    x = (x ^ (x >> 8)) & 0x0000ffffu;
+    return x;
+}
+
+KS_D void demux_float(float f, float &a, float &b)
+{
+    const uint32_t v = (uint32_t)(f * 4294967296.0f);
+    a = (float)compact_1_by_1(v) / 65536.0f;
+    b = (float)compact_1_by_1(v >> 1) / 65536.0f;
+}
+
+// EqualAreaSkyLight::eval(p_square) (light.slang:160-178): texels read at their centres
+KS_D f3 ea_sky_eval_square(const SceneView &s, float px, float py)
+{
+    int ix[4], iy[4];
+    float w[4];
+    ea_bilerp(px, py, s.sky_w, ix, iy, w);
+    f3 L = mk(0, 0, 0);
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        L += w[k] * sky_texel(s, ix[k], iy[k]);
+    L *= s.sky_strength;
+    return L;
+}
+
+KS_D f3 ea_sky_eval(const SceneView &s, f3 wi)
+{
+    const f3 wl = mat3_apply(s.sky_w2l, wi); // the transposed rotation (light.slang:153-156)
+    float px, py;
+    ea_sphere_to_square(wl, px, py);
+    return ea_sky_eval_square(s, px, py);
+}
+
+// AliasTable::sample (distrib.cpp:167-193; gpu/shaders/alias_table.slang): bins (q, p, alias, -)
+KS_D uint32_t alias_sample(const float4 *bins, uint32_t n, float u, float &pmf)
+{
+    const float un = u * (float)n;
+    uint32_t offset = (uint32_t)floorf(un);
+    offset = offset < n - 1 ? offset : n - 1;
+    float up = un - (float)offset;
+    up = up < kOneMinusEps ? up : kOneMinusEps;
+    const float4 b = __ldg(&bins[offset]);
+    if (up < b.x) {
+        pmf = b.y;
+        return offset;
+    }
+    const uint32_t alias = __float_as_uint(b.z);
+    pmf = __ldg(&bins[alias]).y;
+    return alias;
+}
+
+// EqualAreaSkyLight::sample (light.slang:114-135)
+KS_D f3 ea_sky_sample(const SceneView &s, float u0, float u1, f3 &wi, float &wi_dist, float &pdf)
+{
+    const uint32_t res = (uint32_t)s.sky_w;
+    float pmf;
+    const uint32_t index = alias_sample(s.sky_alias, res * res, u0, pmf);
+    const uint32_t iy = index / res, ix = index % res;
+    float dx, dy;
+    demux_float(u1, dx, dy);
+    const float px = ((float)ix + dx) / (float)res, py = ((float)iy + dy) / (float)res;
+    pdf = pmf * (float)(res * res) / (4.0f * kPi);
+    wi = mat3_apply(s.sky_l2w, ea_square_to_sphere(px, py));
+    wi_dist = kInf;
+    if (pdf == 0.0f)
+        return mk(0, 0, 0);
+    return ea_sky_eval_square(s, px, py) / pdf;
+}
+
+// EqualAreaSkyLight::pdf (light.slang:138-150)
+KS_D float ea_sky_pdf(const SceneView &s, f3 wi)
+{
+    const int res = s.sky_w;
+    const f3 wl = mat3_apply(s.sky_w2l, wi);
+    float px, py;
+    ea_sphere_to_square(wl, px, py);
+    int iy = (int)floorf(py * res), ix = (int)floorf(px * res);
+    iy = iy < 0 ? 0 : (iy > res - 1 ? res - 1 : iy);
+    ix = ix < 0 ? 0 : (ix > res - 1 ? res - 1 : ix);
+    return __ldg(&s.sky_alias[(size_t)iy * res + ix]).y * (float)(res * res) / (4.0f * kPi);
+}
+
+// The scene's sky light, lat-long (SkyLight) or equal-area (EqualAreaSkyLight).
+KS_D f3 sky_eval(const SceneView &s, f3 wi)
+{
+    return s.sky_kind == 3 ? ea_sky_eval(s, wi) : latlong_sky_eval(s, wi);
+}
+KS_D f3 sky_sample(const SceneView &s, float u0, float u1, f3 &wi, float &wi_dist, float &pdf)
+{
+    return s.sky_kind == 3 ? ea_sky_sample(s, u0, u1, wi, wi_dist, pdf)
+                           : latlong_sky_sample(s, u0, u1, wi, wi_dist, pdf);
+}
+KS_D float sky_pdf(const SceneView &s, f3 wi)
+{
+    return s.sky_kind == 3 ? ea_sky_pdf(s, wi) : latlong_sky_pdf(s, wi);
 }
 
 // ---- mesh lights ----------------------------------------------------------------------------

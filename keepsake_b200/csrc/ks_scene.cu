@@ -383,10 +383,14 @@ ks_status ks_scene_create(ks_context *ctx, const ks_scene_desc *desc, ks_scene *
     }
     // sky
     const ks_sky_desc &sd = desc->sky;
-    if (sd.kind < 0 || sd.kind > 2 || (sd.kind == 2 && (!sd.map_rgb || sd.width == 0 || sd.height == 0))) {
+    if (sd.kind < 0 || sd.kind > 3 || (sd.kind >= 2 && (!sd.map_rgb || sd.width == 0 || sd.height == 0)) ||
+        (sd.kind == 3 && (sd.width != sd.height || (sd.width & (sd.width - 1)) != 0 || sd.width > (1u << 14)))) {
         delete s;
-        return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_create: bad sky description");
+        return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_create: bad sky description (an equal-area map is a "
+                                                  "square of a power-of-two side, at most 16384)");
     }
+    if (sd.kind == 3) // the alias table over the texels is built on the host
+        s->sky_host.assign(sd.map_rgb, sd.map_rgb + 3 * (size_t)sd.width * sd.height);
     s->sky_desc = sd;
     if (desc->n_lights && !desc->lights) {
         delete s;
@@ -448,7 +452,7 @@ ks_status ks_scene_create(ks_context *ctx, const ks_scene_desc *desc, ks_scene *
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(s->tri_mesh.ptr, tri_mesh.data(), s->tri_mesh.bytes(), cudaMemcpyHostToDevice,
                             ctx->stream);
-    if (e == cudaSuccess && sd.kind == 2) {
+    if (e == cudaSuccess && (sd.kind == 2 || sd.kind == 3)) {
         const size_t n = 3 * (size_t)sd.width * sd.height;
         e = s->sky_rgb.alloc(n);
         if (e == cudaSuccess)

@@ -125,7 +125,9 @@ struct ks_scene
     ks_sky_desc sky_desc{};
     std::vector<ks_light_desc> lights; // point / directional lights, after the sky in the light list
     ksb::DevBuf<float4> punctual;      // per light: (vec, type), (color, 0)
-    ksb::DevBuf<float> sky_rgb;   // kind 2: the map as given (3 floats per texel), for the light build
+    ksb::DevBuf<float> sky_rgb;   // kinds 2, 3: the map as given (3 floats per texel), for the light build
+    std::vector<float> sky_host;  // kind 3: the equal-area map on the host, for its alias table
+    ksb::DevBuf<float4> sky_alias; // kind 3: alias-table bins (q, p, alias bits, 0) over the texels
     float sky_l2w[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, sky_w2l[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
     ksb::DevBuf<float4> sky_map;
     ksb::DevBuf<float> sky_cond, sky_margin;

@@ -856,6 +856,47 @@ void small_pt_b200(const ConfigArgs &args, const fs::path &task_dir, int task_id
                 const float n = std::sqrt(d.vec[0] * d.vec[0] + d.vec[1] * d.vec[1] + d.vec[2] * d.vec[2]);
                 for (int k = 0; k < 3; ++k)
                     d.vec[k] /= n;
+            } else if (type == "equal_area_sky") {
+                // create_equal_area_sky_light (light.cpp:274-283): an .exr / .hdr map of a square
+                // equal-area parameterisation, a quaternion to_world (x, y, z, w) and a strength.
+                // The scene's one sky slot takes it (first in the light list).
+                if (desc.sky.kind != 0)
+                    throw StatusError(KS_ERR_UNSUPPORTED, "config: an equal_area_sky light with a sky: the "
+                                                          "library renders one sky light");
+                fs::path path = l.load_path("map");
+                int w = 0, h = 0;
+                try {
+                    sky_map = ksb::image::read_rgb(path, w, h);
+                } catch (const ksb::image::Error &e) {
+                    if (e.unsupported)
+                        throw StatusError(KS_ERR_UNSUPPORTED, std::string("config: sky map: ") + e.what());
+                    throw IoError(e.what());
+                }
+                if (w != h)
+                    throw ParseError("config: the equal-area map must be square (light.cpp:178)");
+                float q[4] = {0, 0, 0, 1};
+                if (l.contains("to_world"))
+                    vec_n(child(*l.internal, "to_world"), 4, q, "to_world");
+                // Eigen's quaternion from its coefficients (x, y, z, w), as a rotation matrix
+                const double n2 = (double)q[0] * q[0] + (double)q[1] * q[1] + (double)q[2] * q[2] + (double)q[3] * q[3];
+                const double x = q[0] / std::sqrt(n2), y = q[1] / std::sqrt(n2), z = q[2] / std::sqrt(n2),
+                             qw = q[3] / std::sqrt(n2);
+                const double r[9] = {1 - 2 * (y * y + z * z), 2 * (x * y - z * qw),     2 * (x * z + y * qw),
+                                     2 * (x * y + z * qw),     1 - 2 * (x * x + z * z), 2 * (y * z - x * qw),
+                                     2 * (x * z - y * qw),     2 * (y * z + x * qw),     1 - 2 * (x * x + y * y)};
+                float m[16] = {0};
+                for (int a = 0; a < 3; ++a)
+                    for (int b = 0; b < 3; ++b)
+                        m[4 * a + b] = (float)r[3 * a + b];
+                m[15] = 1.0f;
+                desc.sky.kind = 3;
+                desc.sky.map_rgb = sky_map.data();
+                desc.sky.width = (uint32_t)w;
+                desc.sky.height = (uint32_t)h;
+                std::memcpy(desc.sky.to_world, m, sizeof(m));
+                desc.sky.transform_y_up = 0;
+                desc.sky.strength = l.load_float("strength", 1.0f);
+                continue;
             } else {
                 throw StatusError(KS_ERR_UNSUPPORTED, "config: light type '" + type + "' is not supported");
             }

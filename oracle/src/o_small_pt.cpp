@@ -28,6 +28,7 @@
 #include <cstdint>
 #include <memory>
 #include <mutex>
+#include <numeric>
 #include <thread>
 #include <vector>
 
@@ -173,9 +174,168 @@ struct PixelFilterTable
 };
 
 // ---- SkyLight -----------------------------------------------------------------------------------
+// ---- EqualAreaSkyLight (light.cpp:161-206; its sample / pdf / eval are defined by the reference's
+// GPU path, gpu/shaders/light.slang:92-186, which this restates) ---------------------------------
+// equal_area_square_to_sphere (gpu/shaders/common.slang:245-265)
+inline V3 ea_square_to_sphere(float px, float py)
+{
+    float u = 2 * px - 1, v = 2 * py - 1;
+    float up = std::abs(u), vp = std::abs(v);
+    float signed_distance = 1 - (up + vp);
+    float d = std::abs(signed_distance);
+    float r = 1 - d;
+    float phi = (r == 0 ? 1 : (vp - up) / r + 1) * pi / 4;
+    float z = std::copysign(1 - sqr(r), signed_distance);
+    float cos_phi = std::copysign(std::cos(phi), u);
+    float sin_phi = std::copysign(std::sin(phi), v);
+    return V3(cos_phi * r * safe_sqrt(2 - sqr(r)), sin_phi * r * safe_sqrt(2 - sqr(r)), z);
+}
+
+// equal_area_sphere_to_square (gpu/shaders/common.slang:267-322)
+inline void ea_sphere_to_square(V3 d, float &ou, float &ov)
+{
+    float x = std::abs(d.x), y = std::abs(d.y), z = std::abs(d.z);
+    float r = safe_sqrt(1 - z);
+    float a = std::max(x, y), b = std::min(x, y);
+    b = a == 0 ? 0 : b / a;
+    const float t1 = 0.406758566246788489601959989e-5f, t2 = 0.636226545274016134946890922156f,
+                t3 = 0.61572017898280213493197203466e-2f, t4 = -0.247333733281268944196501420480f,
+                t5 = 0.881770664775316294736387951347e-1f, t6 = 0.419038818029165735901852432784e-1f,
+                t7 = -0.251390972343483509333252996350e-1f;
+    float phi = std::fma(t7, b, t6);
+    phi = std::fma(phi, b, t5);
+    phi = std::fma(phi, b, t4);
+    phi = std::fma(phi, b, t3);
+    phi = std::fma(phi, b, t2);
+    phi = std::fma(phi, b, t1);
+    if (x < y)
+        phi = 1 - phi;
+    float v = phi * r;
+    float u = r - v;
+    if (d.z < 0) {
+        std::swap(u, v);
+        u = 1 - u;
+        v = 1 - v;
+    }
+    u = std::copysign(u, d.x);
+    v = std::copysign(v, d.y);
+    ou = 0.5f * (u + 1);
+    ov = 0.5f * (v + 1);
+}
+
+// equal_area_bilerp (gpu/shaders/common.slang:350-395)
+inline void ea_bilerp(float ux, float uy, int N, int ix[4], int iy[4], float w[4])
+{
+    float x = ux * N - 0.5f, y = uy * N - 0.5f;
+    int x0 = (int)std::floor(x), y0 = (int)std::floor(y);
+    float tx = x - x0, ty = y - y0;
+    int x1 = x0 + 1, y1 = y0 + 1;
+    x0 = std::clamp(x0, 0, N - 1);
+    y0 = std::clamp(y0, 0, N - 1);
+    x1 = std::clamp(x1, 0, N - 1);
+    y1 = std::clamp(y1, 0, N - 1);
+    float inv_tx = 1.0f - tx, inv_ty = 1.0f - ty;
+    w[0] = inv_tx * inv_ty;
+    w[1] = tx * inv_ty;
+    w[2] = inv_tx * ty;
+    w[3] = tx * ty;
+    const int xs[4] = {x0, x1, x0, x1}, ys[4] = {y0, y0, y1, y1}, n1 = N - 1;
+    for (int k = 0; k < 4; ++k) {
+        bool mirror = (xs[k] ^ ys[k]) & N;
+        int a = xs[k] & n1, b = ys[k] & n1;
+        ix[k] = mirror ? n1 - a : a;
+        iy[k] = mirror ? n1 - b : b;
+    }
+}
+
+// compact_1_by_1 / demux_float (gpu/shaders/common.slang:529-537, 569-576)
+inline uint32_t compact_1_by_1(uint32_t x)
+{
+    x &= 0x55555555u;
+    x = (x ^ (x >> 1)) & 0x33333333u;
+    x = (x ^ (x >> 2)) & 0x0f0f0f0fu;
+    x = (x ^ (x >> 4)) & 0x00ff00ffu;
+    x = (x ^ (x >> 8)) & 0x0000ffffu;
+    return x;
+}
+inline void demux_float(float f, float &a, float &b)
+{
+    uint32_t v = (uint32_t)(f * (float)(1ull << 32));
+    a = compact_1_by_1(v) / float(1 << 16);
+    b = compact_1_by_1(v >> 1) / float(1 << 16);
+}
+
+// AliasTable (distrib.cpp:109-193)
+struct AliasTable
+{
+    struct Bin
+    {
+        float q = 0, p = 0;
+        int alias = -1;
+    };
+    std::vector<Bin> bins;
+    AliasTable() = default;
+    explicit AliasTable(const std::vector<float> &weights) : bins(weights.size())
+    {
+        double sum = std::accumulate(weights.begin(), weights.end(), 0.);
+        for (size_t i = 0; i < weights.size(); ++i)
+            bins[i].p = weights[i] / sum;
+        struct Outcome
+        {
+            float pHat;
+            size_t index;
+        };
+        std::vector<Outcome> under, over;
+        for (size_t i = 0; i < bins.size(); ++i) {
+            float pHat = bins[i].p * bins.size();
+            if (pHat < 1)
+                under.push_back(Outcome{pHat, i});
+            else
+                over.push_back(Outcome{pHat, i});
+        }
+        while (!under.empty() && !over.empty()) {
+            Outcome un = under.back(), ov = over.back();
+            under.pop_back();
+            over.pop_back();
+            bins[un.index].q = un.pHat;
+            bins[un.index].alias = (int)ov.index;
+            float pExcess = un.pHat + ov.pHat - 1;
+            if (pExcess < 1)
+                under.push_back(Outcome{pExcess, ov.index});
+            else
+                over.push_back(Outcome{pExcess, ov.index});
+        }
+        while (!over.empty()) {
+            Outcome ov = over.back();
+            over.pop_back();
+            bins[ov.index].q = 1;
+            bins[ov.index].alias = -1;
+        }
+        while (!under.empty()) {
+            Outcome un = under.back();
+            under.pop_back();
+            bins[un.index].q = 1;
+            bins[un.index].alias = -1;
+        }
+    }
+    int sample(float u, float *pmf) const
+    {
+        size_t offset = std::min((size_t)std::floor(u * bins.size()), bins.size() - 1);
+        float up = std::min(u * bins.size() - offset, fp32_before_one);
+        if (up < bins[offset].q) {
+            *pmf = bins[offset].p;
+            return (int)offset;
+        }
+        int alias = bins[offset].alias;
+        *pmf = bins[alias].p;
+        return alias;
+    }
+};
+
 struct Sky
 {
-    int kind = 0; // 1 ambient, 2 map
+    int kind = 0; // 1 ambient, 2 lat-long map, 3 equal-area map
+    AliasTable ea_pmf; // kind 3: over the texels' luminance
     int w = 1, h = 1;
     std::vector<V3> map; // row-major, map(u, v) = map[v * w + u]
     float l2w[16], w2l[16];
@@ -223,8 +383,30 @@ struct Sky
         }
     }
     V3 at(int u, int v) const { return map[(size_t)v * w + u]; }
+    // kind 3 (light.slang:138-178): the light-to-world rotation's transpose takes wi to the map
+    V3 ea_local(V3 wi) const
+    {
+        return V3(l2w[0] * wi.x + l2w[4] * wi.y + l2w[8] * wi.z, l2w[1] * wi.x + l2w[5] * wi.y + l2w[9] * wi.z,
+                  l2w[2] * wi.x + l2w[6] * wi.y + l2w[10] * wi.z);
+    }
+    V3 ea_eval_square(float px, float py) const
+    {
+        int ix[4], iy[4];
+        float wt[4];
+        ea_bilerp(px, py, w, ix, iy, wt);
+        V3 L;
+        for (int k = 0; k < 4; ++k)
+            L += wt[k] * at(ix[k], iy[k]);
+        L *= strength;
+        return L;
+    }
     V3 eval(V3 wi) const
     {
+        if (kind == 3) {
+            float px, py;
+            ea_sphere_to_square(ea_local(wi), px, py);
+            return ea_eval_square(px, py);
+        }
         V3 wl = transform_dir(w2l, wi);
         float phi, theta;
         if (y_up)
@@ -246,6 +428,22 @@ struct Sky
     }
     V3 sample(float u0, float u1, V3 &wi, float &wi_dist, float &pdf) const
     {
+        if (kind == 3) {
+            float pmf;
+            int index = ea_pmf.sample(u0, &pmf);
+            int iy = index / w, ix = index % w;
+            float dx, dy;
+            demux_float(u1, dx, dy);
+            float px = (ix + dx) / w, py = (iy + dy) / w;
+            pdf = pmf * sqr((float)w) / (4.0f * pi);
+            V3 wl = ea_square_to_sphere(px, py);
+            wi = V3(l2w[0] * wl.x + l2w[1] * wl.y + l2w[2] * wl.z, l2w[4] * wl.x + l2w[5] * wl.y + l2w[6] * wl.z,
+                    l2w[8] * wl.x + l2w[9] * wl.y + l2w[10] * wl.z);
+            wi_dist = inf;
+            if (pdf == 0.0f)
+                return V3();
+            return ea_eval_square(px, py) / pdf;
+        }
         float s0, s1;
         distrib.sample_linear(u0, u1, pdf, s0, s1);
         if (pdf == 0.0f)
@@ -265,6 +463,13 @@ struct Sky
     }
     float pdf(V3 wi) const
     {
+        if (kind == 3) {
+            float px, py;
+            ea_sphere_to_square(ea_local(wi), px, py);
+            int iy = std::clamp((int)std::floor(py * w), 0, w - 1);
+            int ix = std::clamp((int)std::floor(px * w), 0, w - 1);
+            return ea_pmf.bins[(size_t)iy * w + ix].p * sqr((float)w) / (4.0f * pi);
+        }
         V3 wl = transform_dir(w2l, wi);
         float phi, theta;
         if (y_up)
@@ -281,6 +486,24 @@ struct Sky
     // SkyLight::power (light.cpp:136-159); the rows' float sums are added in row order in double.
     V3 power(const float bound[6]) const
     {
+        if (kind == 3) {
+            // EqualAreaSkyLight::unit_power / power (light.cpp:182-206): float row sums, the rows
+            // added in row order in double
+            double sum[3] = {0, 0, 0};
+            for (int row = 0; row < w; ++row) {
+                V3 row_sum;
+                for (int col = 0; col < w; ++col)
+                    row_sum += at(col, row);
+                for (int c = 0; c < 3; ++c)
+                    sum[c] += row_sum[c];
+            }
+            V3 Phi((float)sum[0], (float)sum[1], (float)sum[2]);
+            Phi *= (4 * pi) / sqr((float)w);
+            V3 ext(bound[3] - bound[0], bound[4] - bound[1], bound[5] - bound[2]);
+            float scene_radius = 0.5f * norm(ext);
+            Phi *= pi * sqr(scene_radius);
+            return Phi;
+        }
         double sum[3] = {0, 0, 0};
         for (int row = 0; row < h; ++row) {
             float theta = (row + 0.5f) / (float)h * pi;
@@ -794,6 +1017,21 @@ Scene *create_scene(const ks_scene_desc *d, const ks_sbvh_options *opts)
 
     // sky light (light.cpp:19-57)
     const ks_sky_desc &sd = d->sky;
+    if (sd.kind == 3) {
+        auto sky = std::make_unique<Sky>();
+        sky->kind = 3;
+        sky->w = sky->h = (int)sd.width;
+        sky->map.resize((size_t)sky->w * sky->h);
+        std::vector<float> lum(sky->map.size());
+        for (size_t i = 0; i < sky->map.size(); ++i) {
+            sky->map[i] = V3(sd.map_rgb[3 * i], sd.map_rgb[3 * i + 1], sd.map_rgb[3 * i + 2]);
+            lum[i] = luminance(sky->map[i]);
+        }
+        std::memcpy(sky->l2w, sd.to_world, sizeof(float) * 16);
+        sky->strength = sd.strength;
+        sky->ea_pmf = AliasTable(lum);
+        s->sky = std::move(sky);
+    }
     if (sd.kind == 1 || sd.kind == 2) {
         auto sky = std::make_unique<Sky>();
         sky->kind = sd.kind;
@@ -1078,6 +1316,44 @@ int oracle_render_range(void *sp, const ks_camera_desc *cam, const ks_small_pt_p
             work_out[3 + k] = work_total.shadow[k];
         }
         work_out[6] = work_total.mismatches;
+    }
+    return 0;
+}
+
+// Sky-light hooks for tests: n samples from uniforms u (2 per sample): direction, pdf and
+// radiance / pdf; and pdf and radiance of n given directions.  1 when the scene has no sky.
+int oracle_sky_sample(void *sp, const float *u, uint32_t n, float *wi, float *pdf, float *Le_beta)
+{
+    const Scene &s = *(Scene *)sp;
+    if (!s.sky)
+        return 1;
+    for (uint32_t i = 0; i < n; ++i) {
+        V3 w, L;
+        float dist = 0.0f, p = 0.0f;
+        L = s.sky->sample(u[2 * i], u[2 * i + 1], w, dist, p);
+        wi[3 * i] = w.x;
+        wi[3 * i + 1] = w.y;
+        wi[3 * i + 2] = w.z;
+        pdf[i] = p;
+        Le_beta[3 * i] = L.x;
+        Le_beta[3 * i + 1] = L.y;
+        Le_beta[3 * i + 2] = L.z;
+    }
+    return 0;
+}
+
+int oracle_sky_eval(void *sp, const float *wi, uint32_t n, float *pdf, float *Le)
+{
+    const Scene &s = *(Scene *)sp;
+    if (!s.sky)
+        return 1;
+    for (uint32_t i = 0; i < n; ++i) {
+        V3 w(wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]);
+        pdf[i] = s.sky->pdf(w);
+        V3 L = s.sky->eval(w);
+        Le[3 * i] = L.x;
+        Le[3 * i + 1] = L.y;
+        Le[3 * i + 2] = L.z;
     }
     return 0;
 }

@@ -57,6 +57,10 @@ class Oracle:
         L.oracle_render.argtypes = [_vp, _vp, _vp, _vp, _vp, ctypes.c_int, _vp]
         L.oracle_render_range.argtypes = [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, ctypes.c_int, _vp, _vp]
         L.oracle_render_range.restype = ctypes.c_int
+        L.oracle_sky_sample.argtypes = [_vp, _vp, _u32, _vp, _vp, _vp]
+        L.oracle_sky_sample.restype = ctypes.c_int
+        L.oracle_sky_eval.argtypes = [_vp, _vp, _u32, _vp, _vp]
+        L.oracle_sky_eval.restype = ctypes.c_int
         L.oracle_bsdf_eval.argtypes = [_vp, _vp, _vp, _u32, _vp, _vp]
         L.oracle_bsdf_eval.restype = None
         L.oracle_bsdf_sample.argtypes = [_vp, _vp, _vp, _u32, _vp, _vp, _vp]
@@ -162,6 +166,22 @@ class OracleScene:
         self.o.lib.oracle_render(self.h, ctypes.byref(camera), ctypes.byref(params), P(accum), P(weights),
                                  threads, P(counts))
         return accum, weights, counts
+
+    def sky_sample(self, u):
+        """The sky light's sample for each row of u (n x 2): (wi [n, 3], pdf [n], Le / pdf [n, 3])."""
+        u = np.ascontiguousarray(u, np.float32)
+        n = len(u)
+        wi, pdf, lb = np.empty((n, 3), np.float32), np.empty(n, np.float32), np.empty((n, 3), np.float32)
+        assert self.o.lib.oracle_sky_sample(self.h, P(u), n, P(wi), P(pdf), P(lb)) == 0
+        return wi, pdf, lb
+
+    def sky_eval(self, wi):
+        """The sky light's pdf [n] and radiance [n, 3] in the directions wi (n x 3)."""
+        wi = np.ascontiguousarray(wi, np.float32)
+        n = len(wi)
+        pdf, le = np.empty(n, np.float32), np.empty((n, 3), np.float32)
+        assert self.o.lib.oracle_sky_eval(self.h, P(wi), n, P(pdf), P(le)) == 0
+        return pdf, le
 
     def render_range(self, camera, params, s_begin, s_end, threads=None, count_work=False, accum=None,
                      weights=None):
