@@ -166,6 +166,64 @@ typedef struct ks_light_desc {
     float vec[3];    /* point: position; directional: unit direction toward the light */
 } ks_light_desc;
 
+/* ---------------------------------------------------------------------------------------------
+ * Textures and textured shader fields (Texture, texture.h:43-65; TextureField, shader_field.h:38-86;
+ * NormalMap, normal_map.cpp:9-40; OpacityMap, opacity_map.cpp:6-30).
+ * ------------------------------------------------------------------------------------------- */
+/* A texture without mipmaps (create_texture with build_mipmaps = false, texture.cpp:1068-1084):
+ * width x height texels of `channels` values, rows first, in `format`; sRGB-encoded texels are read
+ * as linear (Texture::fetch_as_float, texture.cpp:403-460). */
+typedef struct ks_texture_desc {
+    const void *texels;
+    uint32_t width;
+    uint32_t height;
+    uint32_t channels; /* 1..4 */
+    int32_t format;    /* 0 u8, 1 u16, 2 f32 (TextureDataType) */
+    int32_t srgb;      /* 1: ColorSpace::sRGB */
+} ks_texture_desc;
+
+/* What a texture binding drives: a shader field of the material's BSDF (the constant value in
+ * ks_material_desc is then ignored), the material's normal map or its opacity map. */
+enum {
+    KS_FIELD_BASECOLOR = 0, /* 3 channels; Lambertian: albedo */
+    KS_FIELD_ROUGHNESS = 1,
+    KS_FIELD_METALLIC = 2,
+    KS_FIELD_IOR = 3,
+    KS_FIELD_SPECULAR_R0_MUL = 4,
+    KS_FIELD_SPECULAR_TRANS = 5,
+    KS_FIELD_DIFFUSE_TRANS = 6,
+    KS_FIELD_DIFFUSE_TRANS_FWD = 7,
+    KS_FIELD_SPECULAR = 8,   /* PrincipledBRDF's specular */
+    KS_FIELD_NORMAL_MAP = 9, /* Material::normal_map (material.h:41) */
+    KS_FIELD_OPACITY_MAP = 10 /* Material::opacity_map (material.h:42): stochastic any-hit test */
+};
+
+/* A texture bound to a material: the TextureField's lookup (flip_v, uv_scale, uv_offset, the
+ * sampler, swizzle, scale) and, for normal maps, NormalMap's parameters.  Zero-initialise, then set:
+ * the defaults of create_texture_shader_field_color / create_texture_sampler /
+ * create_normal_map are flip_v 1, uv_scale (1, 1), swizzle (0, 1, 2, 3), scale (1, 1, 1, 1),
+ * filter nearest... as listed per field. */
+typedef struct ks_texture_binding {
+    uint32_t material;   /* index into ks_scene_desc.materials */
+    int32_t field;       /* KS_FIELD_* */
+    uint32_t texture;    /* index into ks_scene_desc.textures */
+    int32_t filter;      /* 0 nearest (NearestSampler), 1 linear (LinearSampler), 2 cubic (CubicSampler);
+                            textures have one level, so linear is bilinear and cubic bicubic at level 0 */
+    int32_t cubic_kernel; /* 0 Mitchell-Netravali, 1 B-spline, 2 Catmull-Rom (texture.h:91-121) */
+    int32_t wrap_u;      /* 0 repeat, 1 clamp (TextureWrapMode) */
+    int32_t wrap_v;
+    int32_t flip_v;      /* TextureField::flip_v (reference default true) */
+    int32_t swizzle[4];  /* output channel c reads texel channel swizzle[c]; -1: 0 */
+    float uv_scale[2];
+    float uv_offset[2];
+    float scale[4];      /* TextureField::scale */
+    /* normal maps (create_normal_map, normal_map.cpp:42-56) */
+    int32_t normal_space; /* 0 tangent, 1 world */
+    int32_t range01;      /* 1: texel values in [0, 1] are remapped to [-1, 1] */
+    float strength;       /* tangent space: lerp from (0, 0, 1) toward the mapped normal */
+    float to_world[16];   /* world space: the map's to_world (row-major 4x4; normals by its inverse transpose) */
+} ks_texture_binding;
+
 typedef struct ks_scene_desc {
     const ks_mesh_desc *meshes;
     uint32_t n_meshes;
@@ -179,6 +237,12 @@ typedef struct ks_scene_desc {
     uint32_t n_instances;
     const ks_light_desc *lights; /* the task's `light` list (small_pt.cpp:186-199); may be NULL */
     uint32_t n_lights;
+    /* textures and their bindings to materials (may be NULL / 0).  Textured emission and the
+     * instanced scenes' textured materials are KS_ERR_UNSUPPORTED. */
+    const ks_texture_desc *textures;
+    uint32_t n_textures;
+    const ks_texture_binding *bindings;
+    uint32_t n_bindings;
 } ks_scene_desc;
 
 /* SBVHBuildOption (cuda/sbvh.cuh:9-16); clamped like SBVH::build (cuda/sbvh.cu:411-414). */

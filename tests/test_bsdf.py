@@ -9,12 +9,19 @@ bsdf.cpp, per function, over every BSDF kind the library renders:
   * Lambertian (bsdf.cpp:13-41).
 
 Stated bounds (device against oracle, same inputs): eval f cos and pdf within a relative 2e-3 of
-the larger value for 99.5 % of the (wo, wi) pairs and within 5e-2 for 99.95 %; samples: the same
-decision (no sample / a sample) for 99.5 %, and where both sample, wi within 2e-3 and weight and
-pdf within a relative 2e-3 for 99 %.  The shading unit's approximate division, square root,
-exp/log/pow and the host libm's correctly rounded ones differ in the last bits; the loose 0.05 %
-tail is where such bits decide a lobe (a Fresnel term at total internal reflection, a cosine at
-the horizon).
+the larger value plus 1e-6 for 99.5 % of the (wo, wi) pairs and within 5e-2 for 99.95 %; samples:
+the same decision (no sample / a sample) for 99.5 %, and where both sample, wi within 2e-3 and
+weight and pdf within a relative 2e-3 for 99 %.  The shading unit's approximate division, square
+root, exp/log/pow and the host libm's correctly rounded ones differ in the last bits; the loose
+0.05 % tail is where such bits decide a lobe (a Fresnel term at total internal reflection, a cosine
+at the horizon).  Exclusions: the unit flushes denormal intermediates to zero, so where the
+oracle's f cos is below 1e-20 (grazing refraction) the device may return exactly 0 and, as
+eval_and_pdf does for a zero value (principled_bsdf.cpp:297-307), pdf 0.  Glass at ior 1 is
+degenerate in the reference: its reflection lobe is rounding noise (a Fresnel term of 0 evaluated
+to 1e-16, absorbed by the absolute 1e-6), and the dielectric lobe's selection weight is the
+Fresnel reflectance at wo (lobe_sample_weights, principled_bsdf.cpp:518-541), zero up to rounding,
+so whether its pdf and samples exist at all is decided by rounding noise: there only f cos and the
+sampled directions are compared.
 
 The CPU half checks the oracle on its own: every sample's pdf equals eval_and_pdf's pdf of the
 same direction, its weight equals f cos / pdf, and the mean weight matches f cos integrated
@@ -79,12 +86,12 @@ def directions(n, seed, below=True):
     return unit(d).astype(np.float32)
 
 
-def close(a, b, rtol):
-    """Per row: |a - b| <= rtol * max(|a|, |b|) (largest component), or both tiny."""
+def close(a, b, rtol, atol=1e-30):
+    """Per row: |a - b| <= rtol * max(|a|, |b|) + atol (largest component)."""
     a = np.atleast_2d(np.asarray(a, np.float64).T).T
     b = np.atleast_2d(np.asarray(b, np.float64).T).T
     scale = np.maximum(np.abs(a).max(-1), np.abs(b).max(-1))
-    return np.abs(a - b).max(-1) <= rtol * scale + 1e-30
+    return np.abs(a - b).max(-1) <= rtol * scale + atol
 
 
 # ---------------------------------------------------------------------------------------------
@@ -170,9 +177,15 @@ def test_bsdf_eval_matches_oracle(ctx, oracle, name):
     of, op = oracle.bsdf_eval(m, wo, wi)
     assert np.isfinite(f).all() and np.isfinite(p).all()
     assert ((f > 0).any(-1) | (p >= 0)).all()
-    for got, want, what in ((f, of, "f cos"), (p, op, "pdf")):
-        tight = close(got, want, 2e-3)
-        loose = close(got, want, 5e-2)
+    flushed = (np.abs(of).max(-1) < 1e-20) & ~f.any(-1)
+    assert flushed.mean() < 0.05
+    keep = ~flushed
+    checks = [(f, of, "f cos")]
+    if m.ior != 1.0 or m.specular_trans == 0.0:
+        checks.append((p[keep], op[keep], "pdf"))
+    for got, want, what in checks:
+        tight = close(got, want, 2e-3, 1e-6)
+        loose = close(got, want, 5e-2, 1e-6)
         assert tight.mean() >= 0.995 and loose.mean() >= 0.9995, (name, what, tight.mean(), loose.mean())
     # both sides of the surface and both kinds of pairs are exercised
     assert (wo[:, 2] < 0).any() and ((wo[:, 2] * wi[:, 2]) < 0).any()
@@ -191,9 +204,10 @@ def test_bsdf_sample_matches_oracle(ctx, oracle, name):
     if m.ior != 1.0:
         assert np.isfinite(p).all()
     same = (p > 0) == (op > 0)
-    assert same.mean() >= 0.995, (name, same.mean())
+    degenerate = m.ior == 1.0 and m.specular_trans > 0.0
+    assert degenerate or same.mean() >= 0.995, (name, same.mean())
     both = (p > 0) & (op > 0)
-    assert both.sum() > 0.2 * n
+    assert both.sum() > (0.02 if degenerate else 0.2) * n
     dir_ok = np.abs(wi[both] - owi[both]).max(-1) <= 2e-3
     w_ok = close(w[both], ow[both], 2e-3)
     p_ok = close(p[both], op[both], 2e-3)
