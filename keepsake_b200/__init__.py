@@ -179,12 +179,69 @@ class LightDesc(ctypes.Structure):
     _fields_ = [("type", _i32), ("color", _f32 * 3), ("vec", _f32 * 3)]
 
 
+class TextureDesc(ctypes.Structure):
+    _fields_ = [("texels", _vp), ("width", _u32), ("height", _u32), ("channels", _u32), ("format", _i32),
+                ("srgb", _i32)]
+
+
+FIELDS = {"basecolor": 0, "roughness": 1, "metallic": 2, "ior": 3, "specular_r0_mul": 4, "specular_trans": 5,
+          "diffuse_trans": 6, "diffuse_trans_fwd": 7, "specular": 8, "normal_map": 9, "opacity_map": 10}
+
+
+class TextureBinding(ctypes.Structure):
+    _fields_ = [("material", _u32), ("field", _i32), ("texture", _u32), ("filter", _i32), ("cubic_kernel", _i32),
+                ("wrap_u", _i32), ("wrap_v", _i32), ("flip_v", _i32), ("swizzle", _i32 * 4), ("uv_scale", _f32 * 2),
+                ("uv_offset", _f32 * 2), ("scale", _f32 * 4), ("normal_space", _i32), ("range01", _i32),
+                ("strength", _f32), ("to_world", _f32 * 16)]
+
+    @classmethod
+    def make(cls, material, field, texture, **kw):
+        """A binding with the reference's defaults (flip_v, identity swizzle and scale, uv_scale 1,
+        range01, strength 1, identity to_world), then the given fields; `field` by name or id."""
+        b = cls()
+        b.material, b.texture = material, texture
+        b.field = FIELDS[field] if isinstance(field, str) else field
+        b.flip_v, b.range01, b.strength = 1, 1, 1.0
+        b.swizzle[:] = (0, 1, 2, 3)
+        b.uv_scale[:] = (1.0, 1.0)
+        b.scale[:] = (1.0, 1.0, 1.0, 1.0)
+        b.to_world[:] = [float(x) for x in np.eye(4).reshape(16)]
+        for k, v in kw.items():
+            if k in ("swizzle", "uv_scale", "uv_offset", "scale", "to_world"):
+                getattr(b, k)[:] = [float(x) if k != "swizzle" else int(x) for x in np.asarray(v).reshape(-1)]
+            else:
+                setattr(b, k, v)
+        return b
+
+
 class SceneDesc(ctypes.Structure):
     _fields_ = [("meshes", ctypes.POINTER(MeshDesc)), ("n_meshes", _u32),
                 ("materials", ctypes.POINTER(MaterialDesc)), ("n_materials", _u32), ("sky", SkyDesc),
                 ("prototypes", ctypes.POINTER(PrototypeDesc)), ("n_prototypes", _u32),
                 ("instances", ctypes.POINTER(InstanceDesc)), ("n_instances", _u32),
-                ("lights", ctypes.POINTER(LightDesc)), ("n_lights", _u32)]
+                ("lights", ctypes.POINTER(LightDesc)), ("n_lights", _u32),
+                ("textures", ctypes.POINTER(TextureDesc)), ("n_textures", _u32),
+                ("bindings", ctypes.POINTER(TextureBinding)), ("n_bindings", _u32)]
+
+
+def attach_textures(desc, textures, bindings):
+    """Sets the textures (numpy arrays [H, W, C] of uint8, uint16 or float32, with an `srgb` flag:
+    (array, srgb)) and bindings (TextureBinding) of a SceneDesc; returns what must stay alive."""
+    keep = []
+    td = (TextureDesc * max(len(textures), 1))()
+    for k, (arr, srgb) in enumerate(textures):
+        a = np.ascontiguousarray(arr)
+        if a.ndim == 2:
+            a = a[..., None]
+        fmt = {np.dtype(np.uint8): 0, np.dtype(np.uint16): 1, np.dtype(np.float32): 2}[a.dtype]
+        keep.append(a)
+        td[k] = TextureDesc(a.ctypes.data, a.shape[1], a.shape[0], a.shape[2], fmt, int(srgb))
+    bd = (TextureBinding * max(len(bindings), 1))(*bindings)
+    keep += [td, bd]
+    d = desc.contents if isinstance(desc, ctypes._Pointer) else desc
+    d.textures, d.n_textures = td, len(textures)
+    d.bindings, d.n_bindings = bd, len(bindings)
+    return keep
 
 
 class ContextLimits(ctypes.Structure):

@@ -275,7 +275,8 @@ __global__ void __launch_bounds__(128) k_extend(const __grid_constant__ SceneVie
 // Closest hit of every queued ray into hits[i] (slot ~0u: miss); k_build_queues then sorts the
 // paths into the hit and miss queues in index order, so that shading reads the path state in
 // order.  kBatch: paths of many jobs, the count read from the batch state.
-template <bool kBatch = false>
+// kAlpha: the scene has opacity maps; candidate hits go through their stochastic test (SceneAlpha).
+template <bool kBatch = false, bool kAlpha = false>
 __global__ void __launch_bounds__(128, KS_TRAV_MIN_BLOCKS) k_extend_pt(const __grid_constant__ SceneView sv_in, PathBuf pb, uint32_t count,
                                                    float4 *hits, uint32_t *fetch, int *overflow,
                                                    unsigned long long *work, BatchView bv)
@@ -314,7 +315,12 @@ __global__ void __launch_bounds__(128, KS_TRAV_MIN_BLOCKS) k_extend_pt(const __g
             continue;
         }
         while (true) {
-            if (trav_warp_step<false>(nodes, tris, s, stack, 2, of, &tc, ray != ~0u)) {
+            bool done;
+            if constexpr (kAlpha)
+                done = trav_warp_step<false>(nodes, tris, s, stack, 2, of, &tc, ray != ~0u, SceneAlpha{&sv_in});
+            else
+                done = trav_warp_step<false>(nodes, tris, s, stack, 2, of, &tc, ray != ~0u);
+            if (done) {
                 hits[ray] = s.hit.tri != ~0u ? make_float4(s.hit.t, s.hit.b1, s.hit.b2, fbits(s.hit.slot))
                                              : make_float4(0, 0, 0, fbits(~0u));
                 ray = ~0u;
@@ -436,7 +442,7 @@ KS_D void shadow_done(const ShadowBuf &sb, uint32_t i, bool occ, PathBuf nxt, do
 
 // Any-hit traversal of the NEE shadow rays with dynamic ray fetch (flat scenes); each ray is
 // finished by shadow_done as soon as its traversal ends.
-template <bool kBatch = false>
+template <bool kBatch = false, bool kAlpha = false>
 __global__ void __launch_bounds__(128, KS_TRAV_MIN_BLOCKS) k_shadow_pt(const __grid_constant__ SceneView sv_in, ShadowBuf sb,
                                                    const uint32_t *shadow_count, uint32_t *fetch, PathBuf nxt,
                                                    double *accum_in, double *weights_in, int *overflow,
@@ -475,7 +481,12 @@ __global__ void __launch_bounds__(128, KS_TRAV_MIN_BLOCKS) k_shadow_pt(const __g
             continue;
         }
         while (true) {
-            if (trav_warp_step<true>(nodes, tris, s, stack, 2, of, &tc, ray != ~0u)) {
+            bool done;
+            if constexpr (kAlpha)
+                done = trav_warp_step<true>(nodes, tris, s, stack, 2, of, &tc, ray != ~0u, SceneAlpha{&sv_in});
+            else
+                done = trav_warp_step<true>(nodes, tris, s, stack, 2, of, &tc, ray != ~0u);
+            if (done) {
                 shadow_done<kBatch>(sb, ray, s.hit.tri != ~0u, nxt, accum_in, weights_in, gv, bv);
                 ray = ~0u;
             }
@@ -996,8 +1007,12 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
     cudaEventRecord(t_begin, st);
     ks_render_stats stats{};
     const unsigned max_grid = (unsigned)ctx->sm_count * 16;
-    const unsigned ext_grid = resident_grid(k_extend_pt<false>, 128, ctx->sm_count);
-    const unsigned shadow_grid = resident_grid(k_shadow_pt<false>, 128, ctx->sm_count);
+    // opacity maps: the traversal kernels with the candidate-hit filter (flat scenes)
+    const bool alpha = scene->any_opacity;
+    const unsigned ext_grid = alpha ? resident_grid(k_extend_pt<false, true>, 128, ctx->sm_count)
+                                    : resident_grid(k_extend_pt<false>, 128, ctx->sm_count);
+    const unsigned shadow_grid = alpha ? resident_grid(k_shadow_pt<false, true>, 128, ctx->sm_count)
+                                       : resident_grid(k_shadow_pt<false>, 128, ctx->sm_count);
     const unsigned inst_ext_grid = resident_grid(k_extend_inst_pt, 128, ctx->sm_count);
     const unsigned inst_shadow_grid = resident_grid(k_shadow_inst_pt, 128, ctx->sm_count);
     int cur = 0;
@@ -1054,9 +1069,13 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
                                                       w.queue[1].ptr, w.counters.ptr + 2, w.overflow.ptr, work.ptr,
                                                       BatchView{});
             else {
-                k_extend_pt<false><<<std::min(grid, ext_grid), 128, 0, st>>>(sv, pb[cur], count, w.hits.ptr,
-                                                                             w.counters.ptr + 4, w.overflow.ptr,
-                                                                             work.ptr, BatchView{});
+                if (alpha)
+                    k_extend_pt<false, true><<<std::min(grid, ext_grid), 128, 0, st>>>(
+                        sv, pb[cur], count, w.hits.ptr, w.counters.ptr + 4, w.overflow.ptr, work.ptr, BatchView{});
+                else
+                    k_extend_pt<false><<<std::min(grid, ext_grid), 128, 0, st>>>(sv, pb[cur], count, w.hits.ptr,
+                                                                                 w.counters.ptr + 4, w.overflow.ptr,
+                                                                                 work.ptr, BatchView{});
                 k_build_queues<false><<<std::min((count + 255) / 256, max_grid), 256, 0, st>>>(
                     w.hits.ptr, count, w.queue[0].ptr, w.queue[1].ptr, w.counters.ptr + 2, BatchView{});
                 stats.kernel_launches++;
@@ -1109,6 +1128,10 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
             } else if (!kPersistentTraversal)
                 k_shadow<false><<<grid, 128, 0, st>>>(sv, sb, w.counters.ptr + 1, pb[1 - cur], d_accum, d_weights,
                                                       w.overflow.ptr, work.ptr + 2, gv, BatchView{});
+            else if (alpha)
+                k_shadow_pt<false, true><<<std::min(grid, shadow_grid), 128, 0, st>>>(
+                    sv, sb, w.counters.ptr + 1, w.counters.ptr + 5, pb[1 - cur], d_accum, d_weights, w.overflow.ptr,
+                    work.ptr + 2, gv, BatchView{});
             else
                 k_shadow_pt<false><<<std::min(grid, shadow_grid), 128, 0, st>>>(sv, sb, w.counters.ptr + 1, w.counters.ptr + 5,
                                                                 pb[1 - cur], d_accum, d_weights, w.overflow.ptr,
@@ -1285,6 +1308,9 @@ static ks_status batch_tables(ks_context *ctx, const ks_batch_job *jobs, uint32_
                                                           ": bad pixel filter");
         filter_off[j] = filter_host.size();
         filter_host.insert(filter_host.end(), ftab.begin(), ftab.end());
+        if (jb.scene->any_opacity)
+            return fail(ctx, KS_ERR_UNSUPPORTED, "ks_batch_render_device: job " + std::to_string(j) +
+                                                     ": opacity maps (render the scene with ks_small_pt_render)");
         views[j] = make_view(jb.scene);
         w.variant = std::max(w.variant, views[j].shade_variant);
         acc[j] = jb.accum_rgb_device;

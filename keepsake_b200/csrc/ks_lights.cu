@@ -261,7 +261,10 @@ SceneView make_view(const ks_scene *s)
     v.normals = s->normals.ptr;
     v.texcoords = s->texcoords.ptr;
     v.materials = s->materials.ptr;
-    v.shade_variant = s->ext_materials ? kShadeGeneral
+    v.tex_texels = s->tex_texels.ptr;
+    v.tex_info = s->tex_info.ptr;
+    v.bindings = s->bindings.ptr;
+    v.shade_variant = (s->ext_materials || s->any_bindings) ? kShadeGeneral
                       : (s->normals.ptr != nullptr || s->texcoords.ptr != nullptr) ? kShadeAttribs
                                                                                      : kShadePlain;
     v.light_count = s->light_count;

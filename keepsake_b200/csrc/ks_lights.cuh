@@ -37,6 +37,9 @@ struct SceneView
     const float *normals;    // global vertex normals (3 floats each; null when no mesh shades smooth)
     const float *texcoords;  // global texture coordinates (2 floats each; null when no mesh has them)
     const MaterialGPU *materials;
+    const float4 *tex_texels;        // textures: linear float texels
+    const TexInfo *tex_info;         // per texture
+    const BindingGPU *bindings;      // per material binding (MaterialGPU::bind_begin / bind_count)
     // the shading kernel variant the scene needs: kShadePlain; kShadeAttribs for vertex normals or
     // texcoords; kShadeGeneral for a material other than the GGX PrincipledBSDF
     int shade_variant;

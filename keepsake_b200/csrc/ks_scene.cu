@@ -196,6 +196,121 @@ bool valid_material(const ks_material_desc &m)
            finite(m.specular);
 }
 
+// srgb_to_linear (maths.h:631-638) in float; for 8-bit texels the reference reads a 256-entry table
+// of the same curve evaluated in double precision (texture.cpp:369-401), which the table below is.
+float srgb_to_linear_f(float x) { return x < 0.04045f ? x / 12.92f : std::pow((x + 0.055f) / 1.055f, 2.4f); }
+
+const float *srgb_u8_table()
+{
+    static const std::vector<float> table = [] {
+        std::vector<float> t(256);
+        for (int i = 0; i < 256; ++i) {
+            const double c = i / 255.0;
+            t[i] = (float)(c <= 0.04045 ? c / 12.92 : std::pow((c + 0.055) / 1.055, 2.4));
+        }
+        return t;
+    }();
+    return table.data();
+}
+
+// Texture::fetch_as_float (texture.cpp:403-460) of every texel: 4 floats per texel, unused 0.
+bool convert_texture(const ks_texture_desc &t, std::vector<float4> &out)
+{
+    if (!t.texels || t.width == 0 || t.height == 0 || t.channels < 1 || t.channels > 4 || t.format < 0 ||
+        t.format > 2 || (uint64_t)t.width * t.height > (1ull << 28))
+        return false;
+    const size_t n = (size_t)t.width * t.height, nc = t.channels;
+    const float *lut = srgb_u8_table();
+    for (size_t i = 0; i < n; ++i) {
+        float v[4] = {0, 0, 0, 0};
+        for (size_t c = 0; c < nc; ++c) {
+            const size_t k = i * nc + c;
+            if (t.format == 0) {
+                const uint8_t u = ((const uint8_t *)t.texels)[k];
+                v[c] = t.srgb ? lut[u] : (float)u / 255.0f;
+            } else if (t.format == 1) {
+                const float f = (float)((const uint16_t *)t.texels)[k] / 65535.0f;
+                v[c] = t.srgb ? srgb_to_linear_f(f) : f;
+            } else {
+                const float f = ((const float *)t.texels)[k];
+                v[c] = t.srgb ? srgb_to_linear_f(f) : f;
+            }
+        }
+        out.push_back(make_float4(v[0], v[1], v[2], v[3]));
+    }
+    return true;
+}
+
+// A binding's device form; false for an index or enum out of range or a non-finite value.
+bool binding_to_gpu(const ks_texture_binding &b, const ks_scene_desc &d, BindingGPU &g)
+{
+    if (b.material >= d.n_materials || b.texture >= d.n_textures || b.field < 0 || b.field > KS_FIELD_OPACITY_MAP ||
+        b.filter < 0 || b.filter > 2 || b.cubic_kernel < 0 || b.cubic_kernel > 2 || b.wrap_u < 0 || b.wrap_u > 1 ||
+        b.wrap_v < 0 || b.wrap_v > 1 || b.normal_space < 0 || b.normal_space > 1)
+        return false;
+    auto finite = [](float x) { return std::isfinite(x); };
+    for (int k = 0; k < 2; ++k)
+        if (!finite(b.uv_scale[k]) || !finite(b.uv_offset[k]))
+            return false;
+    for (int k = 0; k < 4; ++k)
+        if (!finite(b.scale[k]) || b.swizzle[k] < -1 || b.swizzle[k] > 3)
+            return false;
+    if (!finite(b.strength))
+        return false;
+    g = BindingGPU{};
+    g.tex = (int)b.texture;
+    g.field = b.field;
+    g.filter = b.filter;
+    g.wrap_u = b.wrap_u;
+    g.wrap_v = b.wrap_v;
+    g.flip_v = b.flip_v != 0;
+    for (int k = 0; k < 4; ++k) {
+        g.swz[k] = b.swizzle[k];
+        g.scale[k] = b.scale[k];
+    }
+    for (int k = 0; k < 2; ++k) {
+        g.uv_scale[k] = b.uv_scale[k];
+        g.uv_offset[k] = b.uv_offset[k];
+    }
+    // CubicSampler's kernels (texture.h:91-121): Mitchell-Netravali (B = C = 1/3), cubic B-spline,
+    // Catmull-Rom, as polynomials in (x^3, x^2, x, 1) for |x| < 1 (ca) and 1 <= |x| < 2 (cb)
+    static const double kCa[3][4] = {{21, -36, 0, 16}, {3, -6, 0, 4}, {3, -5, 0, 2}};
+    static const double kCb[3][4] = {{-7, 36, -60, 32}, {-1, 6, -12, 8}, {-1, 5, -8, 4}};
+    static const double kDiv[3] = {18, 6, 2};
+    for (int k = 0; k < 4; ++k) {
+        g.ca[k] = (float)(kCa[b.cubic_kernel][k] / kDiv[b.cubic_kernel]);
+        g.cb[k] = (float)(kCb[b.cubic_kernel][k] / kDiv[b.cubic_kernel]);
+    }
+    g.space = b.normal_space;
+    g.range01 = b.range01 != 0;
+    g.strength = b.strength;
+    if (b.field == KS_FIELD_NORMAL_MAP && b.normal_space == 1) {
+        // Transform::normal (maths.h:987): the inverse transpose of the 3x3 part
+        double m[3][3], inv[3][3];
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c)
+                m[r][c] = b.to_world[4 * r + c];
+        const double det = m[0][0] * (m[1][1] * m[2][2] - m[1][2] * m[2][1]) -
+                           m[0][1] * (m[1][0] * m[2][2] - m[1][2] * m[2][0]) +
+                           m[0][2] * (m[1][0] * m[2][1] - m[1][1] * m[2][0]);
+        if (!(std::fabs(det) > 0.0) || !std::isfinite(det))
+            return false;
+        inv[0][0] = (m[1][1] * m[2][2] - m[1][2] * m[2][1]) / det;
+        inv[0][1] = (m[0][2] * m[2][1] - m[0][1] * m[2][2]) / det;
+        inv[0][2] = (m[0][1] * m[1][2] - m[0][2] * m[1][1]) / det;
+        inv[1][0] = (m[1][2] * m[2][0] - m[1][0] * m[2][2]) / det;
+        inv[1][1] = (m[0][0] * m[2][2] - m[0][2] * m[2][0]) / det;
+        inv[1][2] = (m[0][2] * m[1][0] - m[0][0] * m[1][2]) / det;
+        inv[2][0] = (m[1][0] * m[2][1] - m[1][1] * m[2][0]) / det;
+        inv[2][1] = (m[0][1] * m[2][0] - m[0][0] * m[2][1]) / det;
+        inv[2][2] = (m[0][0] * m[1][1] - m[0][1] * m[1][0]) / det;
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c)
+                g.nrm[3 * r + c] = (float)inv[c][r];
+    }
+    return true;
+}
+
 } // namespace
 
 // The device copy of a material; false for a non-finite field or an enum out of range.
@@ -331,6 +446,21 @@ ks_status ks_scene_create(ks_context *ctx, const ks_scene_desc *desc, ks_scene *
                                                           "has_emission out of range (zero-initialise the "
                                                           "descriptor)");
     }
+    if ((desc->n_textures && !desc->textures) || (desc->n_bindings && !desc->bindings))
+        return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_create: n_textures / n_bindings without arrays");
+    for (uint32_t k = 0; k < desc->n_textures; ++k) {
+        const ks_texture_desc &t = desc->textures[k];
+        if (!t.texels || t.width == 0 || t.height == 0 || t.channels < 1 || t.channels > 4 || t.format < 0 ||
+            t.format > 2 || (uint64_t)t.width * t.height > (1ull << 28))
+            return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_create: bad texture " + std::to_string(k));
+    }
+    for (uint32_t k = 0; k < desc->n_bindings; ++k) {
+        BindingGPU g;
+        if (!binding_to_gpu(desc->bindings[k], *desc, g))
+            return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_create: bad texture binding " + std::to_string(k));
+        if (g.field == KS_FIELD_OPACITY_MAP && desc->n_instances)
+            return fail(ctx, KS_ERR_UNSUPPORTED, "ks_scene_create: opacity maps in instanced scenes");
+    }
     KS_CUDA_TRY(ctx, enter_device(ctx));
     ks_scene *s = new (std::nothrow) ks_scene();
     if (!s)
@@ -414,6 +544,31 @@ ks_status ks_scene_create(ks_context *ctx, const ks_scene_desc *desc, ks_scene *
         material_to_gpu(m, mats[k]);
         s->ext_materials |= m.bsdf != 0 || m.microfacet != 0;
     }
+    // textures and bindings (validated above), the bindings grouped by material in their order
+    std::vector<float4> texels;
+    std::vector<TexInfo> tex_info;
+    std::vector<BindingGPU> binds;
+    for (uint32_t k = 0; k < desc->n_textures; ++k) {
+        const ks_texture_desc &t = desc->textures[k];
+        tex_info.push_back(TexInfo{(uint32_t)texels.size(), (int)t.width, (int)t.height, (int)t.channels});
+        convert_texture(t, texels);
+    }
+    for (uint32_t m = 0; m < desc->n_materials; ++m) {
+        mats[m].bind_begin = (int)binds.size();
+        for (uint32_t k = 0; k < desc->n_bindings; ++k)
+            if (desc->bindings[k].material == m) {
+                BindingGPU g;
+                binding_to_gpu(desc->bindings[k], *desc, g);
+                binds.push_back(g);
+                if (g.field == KS_FIELD_NORMAL_MAP)
+                    mats[m].tex_flags |= kMatNormalMap;
+                else if (g.field == KS_FIELD_OPACITY_MAP)
+                    mats[m].tex_flags |= kMatOpacityMap;
+            }
+        mats[m].bind_count = (int)binds.size() - mats[m].bind_begin;
+        s->any_opacity |= (mats[m].tex_flags & kMatOpacityMap) != 0;
+    }
+    s->any_bindings = !binds.empty();
     cudaError_t e = s->materials.alloc(mats.size());
     if (e == cudaSuccess)
         e = s->mesh_material.alloc(s->host.mesh_material.size());
@@ -427,6 +582,22 @@ ks_status ks_scene_create(ks_context *ctx, const ks_scene_desc *desc, ks_scene *
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(s->mesh_flags.ptr, s->host.mesh_flags.data(), s->mesh_flags.bytes(),
                             cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess && !binds.empty()) {
+        e = s->tex_texels.alloc(texels.size());
+        if (e == cudaSuccess)
+            e = s->tex_info.alloc(tex_info.size());
+        if (e == cudaSuccess)
+            e = s->bindings.alloc(binds.size());
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(s->tex_texels.ptr, texels.data(), s->tex_texels.bytes(), cudaMemcpyHostToDevice,
+                                ctx->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(s->tex_info.ptr, tex_info.data(), s->tex_info.bytes(), cudaMemcpyHostToDevice,
+                                ctx->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(s->bindings.ptr, binds.data(), s->bindings.bytes(), cudaMemcpyHostToDevice,
+                                ctx->stream);
+    }
     if (e == cudaSuccess && any_smooth) {
         e = s->normals.alloc(normals.size());
         if (e == cudaSuccess)

@@ -2,6 +2,7 @@
 #pragma once
 #include "ks_internal.h"
 #include "ks_math.cuh"
+#include "ks_texture.cuh"
 
 #include <vector>
 
@@ -63,6 +64,13 @@ struct MaterialGPU
     int mesh_light; // index of the MeshLightShared for emissive meshes, -1 otherwise
     int bsdf;       // 0 PrincipledBSDF, 1 PrincipledBRDF, 2 Lambertian (albedo = basecolor)
     float specular; // PrincipledBRDF's specular field
+    int bind_begin, bind_count; // the material's texture bindings (SceneView::bindings)
+    int tex_flags;              // kMatNormalMap | kMatOpacityMap
+};
+enum : int
+{
+    kMatNormalMap = 1,
+    kMatOpacityMap = 2
 };
 
 struct SceneHost
@@ -109,6 +117,11 @@ struct ks_scene
     ksb::DevBuf<uint32_t> mesh_material;
     ksb::DevBuf<int> mesh_flags;
     bool ext_materials = false; // some material is not a GGX PrincipledBSDF
+    // textures (linear float texels, 4 per texel), their sizes, the bindings grouped by material
+    ksb::DevBuf<float4> tex_texels;
+    ksb::DevBuf<ksb::TexInfo> tex_info;
+    ksb::DevBuf<ksb::BindingGPU> bindings;
+    bool any_bindings = false, any_opacity = false;
     // per-vertex shading attributes, indexed like verts (allocated only when some mesh has them)
     ksb::DevBuf<float> normals;   // 3 per vertex: MeshData::vertex_normals of smooth-shaded meshes
     ksb::DevBuf<float> texcoords; // 2 per vertex: MeshData::texcoords

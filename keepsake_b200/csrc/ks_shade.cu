@@ -28,6 +28,69 @@ using namespace wave;
 #define KS_SHADE_MIN_BLOCKS 8
 #endif
 
+// NormalMap::apply (normal_map.cpp:24-40): the shading frame around the mapped normal, its tangent
+// the old one tilted by the normal's slope (the frame's n is respected, t and b re-orthogonalised).
+KS_D void apply_normal_map(const SceneView &sv, const BindingGPU &b, float u, float v, ShadeFrame &it)
+{
+    const float4 c = field_eval(sv.tex_texels, sv.tex_info, b, u, v);
+    f3 s = mk(c.x, c.y, c.z);
+    if (b.range01)
+        s = mk(s.x * 2.0f - 1.0f, s.y * 2.0f - 1.0f, s.z * 2.0f - 1.0f);
+    f3 normal = normalize(s);
+    if (b.space == 0 && b.strength < 1.0f)
+        normal = normalize((1.0f - b.strength) * mk(0.0f, 0.0f, 1.0f) + b.strength * normal);
+    f3 np;
+    if (b.space == 0)
+        np = it.st * normal.x + it.sb * normal.y + it.sn * normal.z;
+    else
+        np = normalize(mk(b.nrm[0] * normal.x + b.nrm[1] * normal.y + b.nrm[2] * normal.z,
+                          b.nrm[3] * normal.x + b.nrm[4] * normal.y + b.nrm[5] * normal.z,
+                          b.nrm[6] * normal.x + b.nrm[7] * normal.y + b.nrm[8] * normal.z));
+    const float bump_x = -normal.x / normal.z;
+    f3 tp = normalize(it.st + bump_x * it.sn);
+    const f3 bp = normalize(cross(np, tp));
+    tp = normalize(cross(bp, np));
+    it.st = tp;
+    it.sb = bp;
+    it.sn = np;
+}
+
+// The material's textured shader fields at the hit (TextureField, shader_field.h:61-80) over its
+// constant ones, and its normal map applied to the shading frame.
+KS_BIG MaterialGPU textured_material(const SceneView &sv, const MaterialGPU &mat, uint32_t tri, int flags, float u,
+                                   float v, ShadeFrame &it)
+{
+    MaterialGPU m = mat;
+    float tu, tv;
+    hit_uv(sv, tri, flags, u, v, tu, tv);
+    for (int k = 0; k < mat.bind_count; ++k) {
+        const BindingGPU &b = sv.bindings[mat.bind_begin + k];
+        if (b.field == KS_FIELD_OPACITY_MAP)
+            continue; // applied by the traversal
+        if (b.field == KS_FIELD_NORMAL_MAP) {
+            apply_normal_map(sv, b, tu, tv, it);
+            continue;
+        }
+        const float4 c = field_eval(sv.tex_texels, sv.tex_info, b, tu, tv);
+        switch (b.field) {
+        case KS_FIELD_BASECOLOR:
+            m.basecolor[0] = c.x;
+            m.basecolor[1] = c.y;
+            m.basecolor[2] = c.z;
+            break;
+        case KS_FIELD_ROUGHNESS: m.roughness = c.x; break;
+        case KS_FIELD_METALLIC: m.metallic = c.x; break;
+        case KS_FIELD_IOR: m.ior = c.x; break;
+        case KS_FIELD_SPECULAR_R0_MUL: m.specular_r0_mul = c.x; break;
+        case KS_FIELD_SPECULAR_TRANS: m.specular_trans = c.x; break;
+        case KS_FIELD_DIFFUSE_TRANS: m.diffuse_trans = c.x; break;
+        case KS_FIELD_DIFFUSE_TRANS_FWD: m.diffuse_trans_fwd = c.x; break;
+        default: m.specular = c.x; break;
+        }
+    }
+    return m;
+}
+
 // Sobol samples and the NEE light sample of one bounce for every path in the hit queue (whose
 // bounce is below the limit).  Sobol dimensions: light selection (d), light uv (d+1, d+2), BSDF
 // lobe (d+3), BSDF direction (d+4, d+5) and Russian roulette (d+6), exactly as sample_with_nee +
@@ -243,9 +306,17 @@ __global__ void __launch_bounds__(128, KS_SHADE_MIN_BLOCKS) k_shade(const __grid
                     p2 = xf_point(m, p2);
                 }
                 uint32_t mesh = __ldg(&sv.tri_mesh[tri]);
-                const MaterialGPU &mat = sv.materials[__ldg(&sv.mesh_material[mesh])];
-                ShadeFrame it = hit_frame<(kVariant >= kShadeAttribs)>(sv, tri, __ldg(&sv.mesh_flags[mesh]), p0, p1, p2, h.y, h.z, rd,
+                const MaterialGPU &mat_c = sv.materials[__ldg(&sv.mesh_material[mesh])];
+                const int mesh_flags = __ldg(&sv.mesh_flags[mesh]);
+                ShadeFrame it = hit_frame<(kVariant >= kShadeAttribs)>(sv, tri, mesh_flags, p0, p1, p2, h.y, h.z, rd,
                                           sv.inst.n ? m : nullptr);
+                // textured fields and normal maps (general variant; Scene::intersect1 applies the
+                // normal map right after the hit record, scene.cpp:229-233)
+                MaterialGPU mat_t;
+                if constexpr (kVariant == kShadeGeneral)
+                    if (mat_c.bind_count)
+                        mat_t = textured_material(sv, mat_c, tri, mesh_flags, h.y, h.z, it);
+                const MaterialGPU &mat = (kVariant == kShadeGeneral && mat_c.bind_count) ? mat_t : mat_c;
                 // emitter hit (small_pt.cpp:112-138)
                 if (mat.has_emission && sv.tri_light) {
                     int32_t light = __ldg(&sv.tri_light[tri]);

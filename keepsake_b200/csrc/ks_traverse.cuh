@@ -185,10 +185,18 @@ struct TravCount
     uint32_t nodes = 0, tris = 0;
 };
 
-template <bool kAnyHit>
+// Candidate-hit filter of the traversal (the role of Embree's intersection filter that runs the
+// opacity maps' stochastic test, scene.cpp:175-208): a hit on triangle tri at barycentrics (u, v)
+// counts only when the filter accepts it.  NoAlpha accepts every hit and compiles away.
+struct NoAlpha
+{
+    KS_D bool operator()(uint32_t, float, float, const RayQuery &) const { return true; }
+};
+
+template <bool kAnyHit, class Alpha = NoAlpha>
 KS_D bool traverse(const TravNode *__restrict__ nodes, const float4 *__restrict__ tris, uint32_t root_ref,
                    uint32_t root_count, const float root_bmin[3], const float root_bmax[3], RayQuery ray,
-                   int culling, Hit &hit, int &overflow, TravCount *count = nullptr)
+                   int culling, Hit &hit, int &overflow, TravCount *count = nullptr, const Alpha &alpha = Alpha{})
 {
     hit.tri = ~0u;
     const TriHelper th = make_tri_helper(ray.d);
@@ -214,10 +222,12 @@ KS_D bool traverse(const TravNode *__restrict__ nodes, const float4 *__restrict_
                 float t, b0, b1, b2;
                 if (isect_tri(ray, th, v0, v1, v2, t, b0, b1, b2)) {
                     if (kAnyHit) {
+                        if (!alpha(__float_as_uint(a.w), b1, b2, ray))
+                            continue;
                         hit.tri = __float_as_uint(a.w);
                         return true;
                     }
-                    if (t < ray.tmax) {
+                    if (t < ray.tmax && alpha(__float_as_uint(a.w), b1, b2, ray)) {
                         ray.tmax = t;
                         hit.tri = __float_as_uint(a.w);
                         hit.slot = first + k;
@@ -535,8 +545,9 @@ KS_D bool trav_pop(TravState &s, const TravStack &stack)
 }
 
 // Leaf triangles of trav_step; true when an any-hit query found an occluder.
-template <bool kAnyHit>
-KS_D bool trav_leaf(const float4 *__restrict__ tris, TravState &s, int culling, TravCount *count)
+template <bool kAnyHit, class Alpha = NoAlpha>
+KS_D bool trav_leaf(const float4 *__restrict__ tris, TravState &s, int culling, TravCount *count,
+                    const Alpha &alpha = Alpha{})
 {
     const uint32_t first = s.ref & ~kLeafBit;
     for (uint32_t k = 0; k < s.cnt; ++k) {
@@ -550,10 +561,12 @@ KS_D bool trav_leaf(const float4 *__restrict__ tris, TravState &s, int culling, 
         float t, b0, b1, b2;
         if (isect_tri(s.ray, s.th, v0, v1, v2, t, b0, b1, b2)) {
             if (kAnyHit) {
+                if (!alpha(__float_as_uint(a.w), b1, b2, s.ray))
+                    continue;
                 s.hit.tri = __float_as_uint(a.w);
                 return true;
             }
-            if (t < s.ray.tmax) {
+            if (t < s.ray.tmax && alpha(__float_as_uint(a.w), b1, b2, s.ray)) {
                 s.ray.tmax = t;
                 s.hit.tri = __float_as_uint(a.w);
                 s.hit.slot = first + k;
@@ -569,12 +582,12 @@ KS_D bool trav_leaf(const float4 *__restrict__ tris, TravState &s, int culling, 
 
 // One step; returns true when the traversal of the ray is over (any-hit: found an occluder).
 // A step visits one node (an interior node or a leaf), then descends or pops.
-template <bool kAnyHit, class Node>
+template <bool kAnyHit, class Node, class Alpha = NoAlpha>
 KS_D bool trav_step(const Node *__restrict__ nodes, const float4 *__restrict__ tris, TravState &s,
-                    TravStack &stack, int culling, int &overflow, TravCount *count)
+                    TravStack &stack, int culling, int &overflow, TravCount *count, const Alpha &alpha = Alpha{})
 {
     if (s.ref & kLeafBit) {
-        if (trav_leaf<kAnyHit>(tris, s, culling, count))
+        if (trav_leaf<kAnyHit>(tris, s, culling, count, alpha))
             return true;
     } else {
         const int r = trav_node<kAnyHit>(nodes, s, stack, overflow, count);
@@ -598,13 +611,14 @@ KS_D bool trav_step(const Node *__restrict__ nodes, const float4 *__restrict__ t
 #ifndef KS_LEAF_BATCH_ANY
 #define KS_LEAF_BATCH_ANY 0
 #endif
-template <bool kAnyHit, class Node>
+template <bool kAnyHit, class Node, class Alpha = NoAlpha>
 KS_D bool trav_warp_step(const Node *__restrict__ nodes, const float4 *__restrict__ tris, TravState &s,
-                         TravStack &stack, int culling, int &overflow, TravCount *count, bool busy)
+                         TravStack &stack, int culling, int &overflow, TravCount *count, bool busy,
+                         const Alpha &alpha = Alpha{})
 {
     constexpr int kBatch = kAnyHit ? KS_LEAF_BATCH_ANY : KS_LEAF_BATCH;
     if constexpr (kBatch == 0) {
-        return busy && trav_step<kAnyHit>(nodes, tris, s, stack, culling, overflow, count);
+        return busy && trav_step<kAnyHit>(nodes, tris, s, stack, culling, overflow, count, alpha);
     } else {
         const bool at_leaf = busy && (s.ref & kLeafBit);
         const uint32_t leaves = __ballot_sync(0xffffffffu, at_leaf);
@@ -612,7 +626,7 @@ KS_D bool trav_warp_step(const Node *__restrict__ nodes, const float4 *__restric
         if (__popc(leaves) >= kBatch || inner == 0) {
             if (!at_leaf)
                 return false;
-            if (trav_leaf<kAnyHit>(tris, s, culling, count))
+            if (trav_leaf<kAnyHit>(tris, s, culling, count, alpha))
                 return true;
             return !trav_pop(s, stack);
         }

@@ -288,6 +288,74 @@ KS_D ShadeFrame hit_frame(const SceneView &sv, uint32_t tri, int flags, f3 p0, f
                       a.vn);
 }
 
+// The hit's texture coordinates: the mesh's interpolated texcoords (rtcInterpolate0 of the
+// texcoord buffer, geometry.cpp:92-99; MeshGeometry::compute_hit_texcoord), else the barycentrics
+// (u, v) of vertices 1 and 2.
+KS_D void hit_uv(const SceneView &sv, uint32_t tri, int flags, float u, float v, float &tu, float &tv)
+{
+    tu = u;
+    tv = v;
+    if (flags & kMeshTexcoords) {
+        const float2 *tc = reinterpret_cast<const float2 *>(sv.texcoords);
+        const uint32_t i0 = __ldg(&sv.indices[3 * (size_t)tri]), i1 = __ldg(&sv.indices[3 * (size_t)tri + 1]),
+                       i2 = __ldg(&sv.indices[3 * (size_t)tri + 2]);
+        const float2 t0 = __ldg(&tc[i0]), t1 = __ldg(&tc[i1]), t2 = __ldg(&tc[i2]);
+        const float w = 1.0f - u - v;
+        tu = w * t0.x + u * t1.x + v * t2.x;
+        tv = w * t0.y + u * t1.y + v * t2.y;
+    }
+}
+
+// hash_float(ro, rd) (hash.h:140-258): murmur_hash_64A of the 24 bytes of the ray's origin and
+// direction (seed 0), its low 32 bits times 2^-32
+KS_D float hash_float_ray(f3 o, f3 d)
+{
+    const uint64_t k[3] = {(uint64_t)__float_as_uint(o.x) | ((uint64_t)__float_as_uint(o.y) << 32),
+                           (uint64_t)__float_as_uint(o.z) | ((uint64_t)__float_as_uint(d.x) << 32),
+                           (uint64_t)__float_as_uint(d.y) | ((uint64_t)__float_as_uint(d.z) << 32)};
+    const uint64_t m = 0xc6a4a7935bd1e995ull;
+    uint64_t h = 24ull * m;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        uint64_t x = k[i] * m;
+        x ^= x >> 47;
+        x *= m;
+        h ^= x;
+        h *= m;
+    }
+    h ^= h >> 47;
+    h *= m;
+    h ^= h >> 47;
+    return (float)(uint32_t)h * 0x1p-32f;
+}
+
+// The opacity maps' candidate-hit filter (Embree filter_opacity_map, scene.cpp:175-208, with
+// OpacityMap::stochastic_test, opacity_map.cpp:20-30): a hit on a triangle whose material has an
+// opacity map counts with probability saturate(map(uv)), decided by the ray's own hash.
+struct SceneAlpha
+{
+    const SceneView *sv;
+    KS_D bool operator()(uint32_t tri, float u, float v, const RayQuery &ray) const
+    {
+        const uint32_t mesh = __ldg(&sv->tri_mesh[tri]);
+        const MaterialGPU &mat = sv->materials[__ldg(&sv->mesh_material[mesh])];
+        if (!(mat.tex_flags & kMatOpacityMap))
+            return true;
+        int k = 0;
+        while (sv->bindings[mat.bind_begin + k].field != KS_FIELD_OPACITY_MAP)
+            ++k;
+        float tu, tv;
+        hit_uv(*sv, tri, __ldg(&sv->mesh_flags[mesh]), u, v, tu, tv);
+        const float opacity = saturate(field_eval(sv->tex_texels, sv->tex_info, sv->bindings[mat.bind_begin + k], tu,
+                                                  tv).x);
+        if (opacity <= 0.0f)
+            return false;
+        if (opacity >= 1.0f)
+            return true;
+        return hash_float_ray(ray.o, ray.d) < opacity;
+    }
+};
+
 KS_D f3 sh_to_local(const ShadeFrame &f, f3 w)
 {
     bool hw = dot(f.n, w) >= 0.0f;

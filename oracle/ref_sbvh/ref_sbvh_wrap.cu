@@ -144,8 +144,12 @@ uint32_t ksref_sbvh_intersect1(void *handle, const float *r, int any_hit, float 
 // counts[1] += triangles tested.  These are the algorithmic units of a query (32-byte nodes,
 // triangles of three vertices + an index triple).  The stack holds 64 entries like the reference's;
 // a deeper push ends the query and sets counts[2].  Returns what ksref_sbvh_intersect1 returns.
+// filter (may be NULL): a candidate hit on triangle tri at barycentrics (u, v) of vertices 1 and 2
+// counts only when filter(user, tri, u, v) is nonzero (the role of Embree's intersection filter,
+// scene.cpp:175-208, which the reference's own SBVH queries do not have).
+typedef int (*ksref_filter_fn)(void *user, uint32_t tri, float u, float v);
 uint32_t ksref_sbvh_intersect1_counted(void *handle, const float *r, int any_hit, int culling, float *t, float *bary,
-                                       uint64_t *counts)
+                                       uint64_t *counts, ksref_filter_fn filter, void *user)
 {
     auto *h = (RefHandle *)handle;
     const ksc::SBVH &b = h->bvh;
@@ -179,9 +183,10 @@ uint32_t ksref_sbvh_intersect1_counted(void *handle, const float *r, int any_hit
                 ++counts[1];
                 ksc::RayTriIsect isect;
                 if (any_hit) {
-                    if (tri_test(tri, nullptr))
+                    if (tri_test(tri, &isect) && (!filter || filter(user, tri, isect.coord.y, isect.coord.z)))
                         return 1u;
-                } else if (tri_test(tri, &isect) && isect.tHit < ray.tmax) {
+                } else if (tri_test(tri, &isect) && isect.tHit < ray.tmax &&
+                           (!filter || filter(user, tri, isect.coord.y, isect.coord.z))) {
                     ray.tmax = isect.tHit;
                     thit = isect.tHit;
                     coord = isect.coord;

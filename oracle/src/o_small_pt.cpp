@@ -20,6 +20,7 @@
 // (rows sequentially in double) so the product can reproduce them exactly.
 #include "../../include/ks_b200.h"
 #include "o_bsdf.h"
+#include "o_texture.h"
 #include "o_math.h"
 #include "o_sampler.h"
 
@@ -36,7 +37,8 @@ extern "C" {
 int ksref_sbvh_build(const float *, uint32_t, const uint32_t *, uint32_t, uint32_t, uint32_t, float, float, void **,
                      uint32_t *, uint32_t *);
 uint32_t ksref_sbvh_intersect1(void *, const float *, int, float *, float *);
-uint32_t ksref_sbvh_intersect1_counted(void *, const float *, int, int, float *, float *, uint64_t *);
+uint32_t ksref_sbvh_intersect1_counted(void *, const float *, int, int, float *, float *, uint64_t *,
+                                       int (*)(void *, uint32_t, float, float), void *);
 void ksref_sbvh_bound(void *, float *);
 void ksref_sbvh_destroy(void *);
 }
@@ -579,6 +581,9 @@ struct Scene
     std::vector<float> normals;   // 3 per vertex (zeros for meshes without)
     std::vector<float> texcoords; // 2 per vertex (zeros for meshes without)
     std::vector<ks_material_desc> materials;
+    std::vector<Texture> textures;
+    std::vector<std::vector<Binding>> mat_bindings; // per material, in the order given
+    bool any_opacity = false;
     void *bvh = nullptr;
     float bound[6];
     std::unique_ptr<Sky> sky;
@@ -605,6 +610,7 @@ struct Intersection
 {
     float thit;
     V3 p;
+    float uv[2]; // the mesh's interpolated texcoords, else the barycentrics of vertices 1 and 2
     Frame frame, sh_frame;
     V3 sh_to_local(V3 w) const
     {
@@ -653,9 +659,13 @@ inline Intersection make_intersection(const Scene &s, uint32_t tri, float t, flo
     V3 dpdu = p1 - p0;
     const uint32_t mesh = s.tri_mesh[tri];
     const uint32_t i0 = s.idx[3 * tri], i1 = s.idx[3 * tri + 1], i2 = s.idx[3 * tri + 2];
+    it.uv[0] = u;
+    it.uv[1] = v;
     if (s.mesh_uv[mesh]) {
         // dP/du of the texture parameterisation (geometry.cpp:94-116)
         const float *tc = s.texcoords.data();
+        it.uv[0] = w0 * tc[2 * i0] + u * tc[2 * i1] + v * tc[2 * i2];
+        it.uv[1] = w0 * tc[2 * i0 + 1] + u * tc[2 * i1 + 1] + v * tc[2 * i2 + 1];
         float du02 = tc[2 * i0] - tc[2 * i2], dv02 = tc[2 * i0 + 1] - tc[2 * i2 + 1];
         float du12 = tc[2 * i1] - tc[2 * i2], dv12 = tc[2 * i1 + 1] - tc[2 * i2 + 1];
         V3 dp02 = p0 - p2, dp12 = p1 - p2;
@@ -698,6 +708,86 @@ inline Intersection make_intersection(const Scene &s, uint32_t tri, float t, flo
     return it;
 }
 
+// NormalMap::apply (normal_map.cpp:9-40) to the hit's shading frame.
+inline void apply_normal_map(const Scene &s, const Binding &bd, Intersection &it)
+{
+    float c[4];
+    bd.eval(s.textures[bd.b.texture], it.uv[0], it.uv[1], c);
+    V3 smp(c[0], c[1], c[2]);
+    if (bd.b.range01)
+        smp = V3(smp.x * 2.0f - 1.0f, smp.y * 2.0f - 1.0f, smp.z * 2.0f - 1.0f);
+    V3 normal = normalized(smp);
+    if (bd.b.normal_space == 0 && bd.b.strength < 1.0f)
+        normal = normalized(lerp3(V3(0.0f, 0.0f, 1.0f), normal, bd.b.strength));
+    V3 n_perturb;
+    if (bd.b.normal_space == 0) {
+        n_perturb = it.sh_frame.to_world(normal);
+    } else {
+        // Transform::normal (maths.h:987): the inverse transpose of to_world's 3x3, normalised
+        double m[3][3];
+        for (int r = 0; r < 3; ++r)
+            for (int k = 0; k < 3; ++k)
+                m[r][k] = bd.b.to_world[4 * r + k];
+        const double det = m[0][0] * (m[1][1] * m[2][2] - m[1][2] * m[2][1]) -
+                           m[0][1] * (m[1][0] * m[2][2] - m[1][2] * m[2][0]) +
+                           m[0][2] * (m[1][0] * m[2][1] - m[1][1] * m[2][0]);
+        // rows of inv^T are the cofactor rows over det
+        const double it_[3][3] = {{(m[1][1] * m[2][2] - m[1][2] * m[2][1]) / det,
+                                   (m[1][2] * m[2][0] - m[1][0] * m[2][2]) / det,
+                                   (m[1][0] * m[2][1] - m[1][1] * m[2][0]) / det},
+                                  {(m[0][2] * m[2][1] - m[0][1] * m[2][2]) / det,
+                                   (m[0][0] * m[2][2] - m[0][2] * m[2][0]) / det,
+                                   (m[0][1] * m[2][0] - m[0][0] * m[2][1]) / det},
+                                  {(m[0][1] * m[1][2] - m[0][2] * m[1][1]) / det,
+                                   (m[0][2] * m[1][0] - m[0][0] * m[1][2]) / det,
+                                   (m[0][0] * m[1][1] - m[0][1] * m[1][0]) / det}};
+        float f[9];
+        for (int r = 0; r < 3; ++r)
+            for (int k = 0; k < 3; ++k)
+                f[3 * r + k] = (float)it_[r][k];
+        n_perturb = normalized(V3(f[0] * normal.x + f[1] * normal.y + f[2] * normal.z,
+                                  f[3] * normal.x + f[4] * normal.y + f[5] * normal.z,
+                                  f[6] * normal.x + f[7] * normal.y + f[8] * normal.z));
+    }
+    V3 bump_deriv = -normal / normal.z;
+    V3 t_perturb = normalized(it.sh_frame.t + bump_deriv.x * it.sh_frame.n);
+    V3 b_perturb = normalized(cross(n_perturb, t_perturb));
+    t_perturb = normalized(cross(b_perturb, n_perturb));
+    it.sh_frame.t = t_perturb;
+    it.sh_frame.b = b_perturb;
+    it.sh_frame.n = n_perturb;
+}
+
+// The material at a hit: its textured shader fields (TextureField at the hit's uv) over the constant
+// ones; the normal map applied to the hit's shading frame.
+inline ks_material_desc textured_material(const Scene &s, uint32_t m, Intersection &it)
+{
+    ks_material_desc mat = s.materials[m];
+    for (const Binding &bd : s.mat_bindings[m]) {
+        const int f = bd.b.field;
+        if (f == KS_FIELD_OPACITY_MAP)
+            continue;
+        if (f == KS_FIELD_NORMAL_MAP) {
+            apply_normal_map(s, bd, it);
+            continue;
+        }
+        float c[4];
+        bd.eval(s.textures[bd.b.texture], it.uv[0], it.uv[1], c);
+        switch (f) {
+        case KS_FIELD_BASECOLOR: mat.basecolor[0] = c[0]; mat.basecolor[1] = c[1]; mat.basecolor[2] = c[2]; break;
+        case KS_FIELD_ROUGHNESS: mat.roughness = c[0]; break;
+        case KS_FIELD_METALLIC: mat.metallic = c[0]; break;
+        case KS_FIELD_IOR: mat.ior = c[0]; break;
+        case KS_FIELD_SPECULAR_R0_MUL: mat.specular_r0_mul = c[0]; break;
+        case KS_FIELD_SPECULAR_TRANS: mat.specular_trans = c[0]; break;
+        case KS_FIELD_DIFFUSE_TRANS: mat.diffuse_trans = c[0]; break;
+        case KS_FIELD_DIFFUSE_TRANS_FWD: mat.diffuse_trans_fwd = c[0]; break;
+        default: mat.specular = c[0]; break;
+        }
+    }
+    return mat;
+}
+
 // Work of the ray queries, counted by the restatement of the reference traversal (nodes whose
 // bound is tested, triangles tested), and the queries where that restatement's answer differed
 // from the reference's own SBVH::intersect / intersectBool (none expected).
@@ -707,14 +797,58 @@ struct Work
     uint64_t mismatches = 0;
 };
 
+// The opacity maps' candidate-hit filter (filter_opacity_map, scene.cpp:175-208, with
+// OpacityMap::stochastic_test, opacity_map.cpp:20-30) for one ray.
+struct AlphaFilter
+{
+    const Scene *s;
+    V3 ro, rd;
+    static int call(void *user, uint32_t tri, float u, float v)
+    {
+        const AlphaFilter &f = *(const AlphaFilter *)user;
+        const Scene &s = *f.s;
+        const uint32_t m = s.mesh_material[s.tri_mesh[tri]];
+        for (const Binding &bd : s.mat_bindings[m]) {
+            if (bd.b.field != KS_FIELD_OPACITY_MAP)
+                continue;
+            // MeshGeometry::compute_hit_texcoord (geometry.cpp:165-175)
+            float tu = u, tv = v;
+            const uint32_t mesh = s.tri_mesh[tri];
+            if (s.mesh_uv[mesh]) {
+                const uint32_t i0 = s.idx[3 * tri], i1 = s.idx[3 * tri + 1], i2 = s.idx[3 * tri + 2];
+                const float *tc = s.texcoords.data();
+                const float w = 1.0f - u - v;
+                tu = w * tc[2 * i0] + u * tc[2 * i1] + v * tc[2 * i2];
+                tv = w * tc[2 * i0 + 1] + u * tc[2 * i1 + 1] + v * tc[2 * i2 + 1];
+            }
+            float c[4];
+            bd.eval(s.textures[bd.b.texture], tu, tv, c);
+            const float opacity = std::clamp(c[0], 0.0f, 1.0f);
+            if (opacity <= 0.0f)
+                return 0;
+            if (opacity >= 1.0f)
+                return 1;
+            return hash_float_ray(f.ro, f.rd) < opacity;
+        }
+        return 1;
+    }
+};
+
 inline bool intersect(const Scene &s, V3 o, V3 d, float tmax, uint32_t &tri, float &t, float bary[3],
                       Work *work = nullptr)
 {
     float r[8] = {o.x, o.y, o.z, 0.0f, d.x, d.y, d.z, tmax};
+    if (s.any_opacity) {
+        // the reference's SBVH queries take no filter: its traversal restated, with the filter
+        AlphaFilter f{&s, o, d};
+        uint64_t dummy[3] = {0, 0, 0};
+        tri = ksref_sbvh_intersect1_counted(s.bvh, r, 0, 2, &t, bary, work ? work->ext : dummy, AlphaFilter::call, &f);
+        return tri != ~0u;
+    }
     tri = ksref_sbvh_intersect1(s.bvh, r, 0, &t, bary);
     if (work) {
         float t2 = 0.0f, b2[3] = {0, 0, 0};
-        uint32_t tri2 = ksref_sbvh_intersect1_counted(s.bvh, r, 0, 2, &t2, b2, work->ext);
+        uint32_t tri2 = ksref_sbvh_intersect1_counted(s.bvh, r, 0, 2, &t2, b2, work->ext, nullptr, nullptr);
         if (tri2 != tri || (tri != ~0u && std::memcmp(&t2, &t, sizeof(float)) != 0))
             ++work->mismatches;
     }
@@ -723,8 +857,15 @@ inline bool intersect(const Scene &s, V3 o, V3 d, float tmax, uint32_t &tri, flo
 inline bool occluded(const Scene &s, V3 o, V3 d, float tmax, Work *work = nullptr)
 {
     float r[8] = {o.x, o.y, o.z, 0.0f, d.x, d.y, d.z, tmax};
+    if (s.any_opacity) {
+        AlphaFilter f{&s, o, d};
+        uint64_t dummy[3] = {0, 0, 0};
+        return ksref_sbvh_intersect1_counted(s.bvh, r, 1, 2, nullptr, nullptr, work ? work->shadow : dummy,
+                                             AlphaFilter::call, &f) != 0;
+    }
     const bool occ = ksref_sbvh_intersect1(s.bvh, r, 1, nullptr, nullptr) != 0;
-    if (work && (ksref_sbvh_intersect1_counted(s.bvh, r, 1, 2, nullptr, nullptr, work->shadow) != 0) != occ)
+    if (work && (ksref_sbvh_intersect1_counted(s.bvh, r, 1, 2, nullptr, nullptr, work->shadow, nullptr, nullptr) !=
+                 0) != occ)
         ++work->mismatches;
     return occ;
 }
@@ -914,7 +1055,7 @@ struct Tracer
             }
             Intersection it = make_intersection(s, tri, t, bary[1], bary[2], rd);
             uint32_t mesh = s.tri_mesh[tri];
-            const ks_material_desc &mat = s.materials[s.mesh_material[mesh]];
+            const ks_material_desc mat = textured_material(s, s.mesh_material[mesh], it);
             if (mat.has_emission) {
                 int32_t light = s.tri_light[tri];
                 if (light >= 0) {
@@ -1006,6 +1147,13 @@ Scene *create_scene(const ks_scene_desc *d, const ks_sbvh_options *opts)
     }
     s->mesh_tri_off.push_back((uint32_t)s->tri_mesh.size());
     s->materials.assign(d->materials, d->materials + d->n_materials);
+    for (uint32_t k = 0; k < d->n_textures; ++k)
+        s->textures.emplace_back(d->textures[k]);
+    s->mat_bindings.resize(d->n_materials);
+    for (uint32_t k = 0; k < d->n_bindings; ++k) {
+        s->mat_bindings[d->bindings[k].material].emplace_back(d->bindings[k]);
+        s->any_opacity |= d->bindings[k].field == KS_FIELD_OPACITY_MAP;
+    }
     ks_sbvh_options o{4, 12, 1.0f, 1e-5f};
     if (opts)
         o = *opts;
