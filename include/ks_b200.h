@@ -565,6 +565,17 @@ ks_status ks_image_save_exr(const char *path, const float *pixels, int32_t width
  * ks_config_last_error(). */
 ks_status ks_image_load_rgb(const char *path, float **pixels, int32_t *width, int32_t *height);
 void ks_image_free(float *pixels);
+/* create_texture_from_image (texture.cpp:922-944) without mipmaps: a texture file read into *out,
+ * texels in a buffer the library allocates (release it with ks_texture_free).  `channels` 1-4.
+ * .png: 8-bit texels (format 0) as stb_image's 8-bit loader converts to the requested channel
+ * count (grey replicated, RGB to grey by (77 R + 150 G + 29 B) >> 8, missing alpha opaque, 16-bit
+ * samples reduced to their high byte); keep_16bit = 1 keeps 16-bit PNGs as format 1, as glTF
+ * images are kept.  .exr: the first `channels` of R, G, B, A (A = 1 when absent; a one-channel file
+ * in all four), format 2.  .hdr / .pfm: RGB, or for 1-2 channels their mean (then alpha 1), format 2.
+ * `srgb` is copied to out->srgb.  KS_ERR_IO, KS_ERR_UNSUPPORTED (message in ks_config_last_error). */
+ks_status ks_texture_load(const char *path, int32_t channels, int32_t srgb, int32_t keep_16bit,
+                          ks_texture_desc *out);
+void ks_texture_free(ks_texture_desc *texture);
 
 /* ---------------------------------------------------------------------------------------------
  * Batched rendering: many (scene, camera, parameters) jobs in one wavefront.  The paths of all

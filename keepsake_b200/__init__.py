@@ -379,7 +379,8 @@ def _arr(p, n, dtype):
     """Copy n elements of a C array into numpy."""
     if not p or n == 0:
         return np.zeros(0, dtype=dtype)
-    ct = {np.float32: ctypes.c_float, np.uint32: ctypes.c_uint32}[dtype]
+    ct = {np.float32: ctypes.c_float, np.uint32: ctypes.c_uint32, np.uint16: ctypes.c_uint16,
+          np.uint8: ctypes.c_uint8}[dtype]
     buf = (ct * n).from_address(ctypes.cast(p, ctypes.c_void_p).value)
     return np.frombuffer(buf, dtype=dtype).copy()
 
@@ -432,6 +433,13 @@ class Generated:
         self.prototypes = [(d.prototypes[k].first_mesh, d.prototypes[k].n_meshes) for k in range(d.n_prototypes)]
         self.instances = [(d.instances[k].prototype, np.array(d.instances[k].to_world[:], np.float32).reshape(3, 4))
                           for k in range(d.n_instances)]
+        self.textures = []
+        for k in range(d.n_textures):
+            t = d.textures[k]
+            dt = {0: np.uint8, 1: np.uint16, 2: np.float32}[t.format]
+            self.textures.append((_arr(t.texels, t.height * t.width * t.channels, dt)
+                                  .reshape(t.height, t.width, t.channels), bool(t.srgb)))
+        self.bindings = [d.bindings[k] for k in range(d.n_bindings)]
         self.sky_kind = d.sky.kind
         self.sky_map = (_arr(d.sky.map_rgb, 3 * d.sky.width * d.sky.height, np.float32)
                         .reshape(d.sky.height, d.sky.width, 3) if d.sky.kind == 2 else None)
@@ -875,6 +883,28 @@ def load_image(path) -> np.ndarray:
         return np.ctypeslib.as_array(buf, shape=(h.value, w.value, 3)).copy()
     finally:
         lib.ks_image_free(buf)
+
+
+_sig("ks_texture_load", [ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                         ctypes.POINTER(TextureDesc)])
+_sig("ks_texture_free", [ctypes.POINTER(TextureDesc)], None)
+
+
+def load_texture(path, channels, srgb=False, keep_16bit=False):
+    """A texture file (ks_texture_load) -> (array [H, W, channels] of uint8, uint16 or float32, srgb),
+    the form attach_textures takes."""
+    t = TextureDesc()
+    st = lib.ks_texture_load(str(path).encode(), int(channels), int(srgb), int(keep_16bit), ctypes.byref(t))
+    if st != KS_OK:
+        raise KsError(st, lib.ks_config_last_error().decode())
+    try:
+        dt = {0: np.uint8, 1: np.uint16, 2: np.float32}[t.format]
+        n = t.height * t.width * t.channels
+        buf = ctypes.cast(t.texels, ctypes.POINTER({0: ctypes.c_uint8, 1: ctypes.c_uint16, 2: _f32}[t.format]))
+        a = np.ctypeslib.as_array(buf, shape=(n,)).astype(dt, copy=True)
+        return a.reshape(t.height, t.width, t.channels), bool(t.srgb)
+    finally:
+        lib.ks_texture_free(ctypes.byref(t))
 
 
 # ---------------------------------------------------------------------------------------------

@@ -250,7 +250,21 @@ ks_status ks_compound_asset_load(const char *path, int32_t load_materials, ks_ge
         ksb::gltf::Compound c = ksb::gltf::load(path, load_materials != 0);
         if (c.instances.empty())
             throw ksb::gltf::Error(std::string(path) + ": the default scene instances no mesh");
+        for (auto &t : c.textures) {
+            ks_texture_desc d{};
+            d.width = (uint32_t)t.width;
+            d.height = (uint32_t)t.height;
+            d.channels = (uint32_t)t.channels;
+            d.format = t.format;
+            d.srgb = t.srgb ? 1 : 0;
+            sc.textures.push_back(d);
+            sc.texture_bytes.push_back(std::move(t.bytes));
+        }
         for (const auto &p : c.prototypes) {
+            for (ks_texture_binding b : p.bindings) {
+                b.material += (uint32_t)sc.materials.size(); // primitive index -> scene material
+                sc.bindings.push_back(b);
+            }
             sc.prototypes.push_back({(uint32_t)sc.meshes.size(), (uint32_t)p.meshes.size()});
             for (size_t k = 0; k < p.meshes.size(); ++k) {
                 const ksb::mesh::MeshData &md = p.meshes[k];

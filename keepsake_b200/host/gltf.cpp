@@ -3,6 +3,7 @@
 // materials, following the glTF 2.0 specification and the reference's use of it
 // (CompoundMeshAsset::load_from_gltf, mesh_asset.cpp:551-1091).
 #include "gltf.h"
+#include "image_io.h"
 
 #include <algorithm>
 #include <array>
@@ -550,23 +551,159 @@ std::vector<uint32_t> indices(const Model &m, long index)
 }
 
 // ---- materials ---------------------------------------------------------------------------------
-bool has_texture(const Json *o, const char *key) { return o && o->get(key); }
+// Textures of the document's images, decoded once each when a material first binds them
+// (create_texture_from_gltf, mesh_asset.cpp:370-388): tinygltf's default loading forces four
+// channels, keeps 16-bit PNGs at 16 bits (u16) and gives 8-bit images as u8; an image is sRGB when
+// any material of the document uses it as a base colour or emissive texture
+// (mesh_asset.cpp:566-582).
+struct TextureSet
+{
+    const Model &m;
+    const fs::path &path;
+    std::vector<Texture> &out;
+    std::vector<long> slot;   // glTF image -> index into `out`, -1 before its first use
+    std::vector<int> srgb;    // per glTF image
+};
 
-// The metallic-roughness material as a principled BSDF with constant fields (mesh_asset.cpp:672-
-// 940): basecolor, roughness, metallic; emissive = KHR_materials_emissive_strength x
-// emissiveFactor, an emitter when both are positive; ior (KHR_materials_ior, 1.5); specular_r0_mul
-// (KHR_materials_specular: specularFactor x mean(specularColorFactor), 0.5 without it);
-// specular_trans (KHR_materials_transmission, which also makes the mesh one-sided); no diffuse
-// transmission; GGX.
-ks_material_desc material(const Json &src, const std::string &where, bool &twosided)
+long texture_image(TextureSet &ts, long tex_index, const std::string &where)
+{
+    const auto &texs = ts.m.doc.array("textures");
+    if (tex_index < 0 || tex_index >= (long)texs.size())
+        throw Error(where + ": texture index out of range");
+    const long img = texs[(size_t)tex_index].integer("source", -1);
+    const auto &imgs = ts.m.doc.array("images");
+    if (img < 0 || img >= (long)imgs.size())
+        throw Error(where + ": texture without a valid image source", true);
+    if (ts.slot[(size_t)img] >= 0)
+        return ts.slot[(size_t)img];
+    const Json &im = imgs[(size_t)img];
+    std::string bytes;
+    if (const Json *bv = im.get("bufferView")) {
+        if (bv->kind != Json::Number)
+            throw Error(where + ": bad image bufferView");
+        const auto &views = ts.m.doc.array("bufferViews");
+        const long vi = (long)bv->num;
+        if (vi < 0 || vi >= (long)views.size())
+            throw Error(where + ": image bufferView out of range");
+        const Json &v = views[(size_t)vi];
+        const long bi = v.integer("buffer", -1);
+        const size_t off = (size_t)v.integer("byteOffset", 0), len = (size_t)v.integer("byteLength", 0);
+        if (bi < 0 || bi >= (long)ts.m.buffers.size() || off + len > ts.m.buffers[(size_t)bi].size())
+            throw Error(where + ": image bufferView outside its buffer");
+        bytes = ts.m.buffers[(size_t)bi].substr(off, len);
+    } else {
+        const std::string u = im.string("uri", "");
+        if (u.empty())
+            throw Error(where + ": image without a uri or bufferView");
+        if (u.rfind("data:", 0) == 0) {
+            const size_t comma = u.find(',');
+            if (comma == std::string::npos || u.substr(0, comma).find(";base64") == std::string::npos)
+                throw Error(where + ": only base64 data URIs are supported", true);
+            bytes = base64_decode(u, comma + 1);
+        } else {
+            bytes = read_all(ts.path.parent_path() / uri_decode(u));
+        }
+    }
+    static const uint8_t png_sig[4] = {137, 'P', 'N', 'G'};
+    if (bytes.size() < 8 || std::memcmp(bytes.data(), png_sig, 4) != 0)
+        throw Error(where + ": image " + std::to_string(img) + " is not a PNG (JPEG and other image formats are "
+                                                                "not supported)",
+                    true);
+    image::Png png;
+    try {
+        png = image::read_png((const uint8_t *)bytes.data(), bytes.size(), where + ": image " + std::to_string(img));
+    } catch (const image::Error &e) {
+        throw Error(e.what(), e.unsupported);
+    }
+    Texture t;
+    t.width = png.width;
+    t.height = png.height;
+    t.channels = 4;
+    t.srgb = ts.srgb[(size_t)img] != 0;
+    const std::vector<uint16_t> s = image::convert_channels(png, 4, png.depth);
+    if (png.depth == 16) {
+        t.format = 1;
+        t.bytes.resize(s.size() * 2);
+        std::memcpy(t.bytes.data(), s.data(), t.bytes.size());
+    } else {
+        t.format = 0;
+        t.bytes.resize(s.size());
+        for (size_t k = 0; k < s.size(); ++k)
+            t.bytes[k] = (uint8_t)s[k];
+    }
+    ts.slot[(size_t)img] = (long)ts.out.size();
+    ts.out.push_back(std::move(t));
+    return ts.slot[(size_t)img];
+}
+
+// A texture-info object bound to `field` (create_texture_shader_field, mesh_asset.cpp:446-464):
+// the glTF sampler's minification filter picks EWA for the mipmap filters and nearest otherwise; no
+// v flip; KHR_texture_transform's scale and offset (get_texture_transform, :390-444); the glTF
+// sampler's wrap modes are not read (repeat).  EWA filtering reads the camera ray's differentials
+// on mipmapped textures, which this build does not have: such bindings are unsupported.  A texture
+// without a sampler is read with the nearest filter.
+ks_texture_binding texture_binding(TextureSet &ts, const Json &info, uint32_t material, int32_t field,
+                                   const float scale[4], const int32_t swizzle[4], const std::string &where)
+{
+    ks_texture_binding b{};
+    b.material = material;
+    b.field = field;
+    const long ti = info.integer("index", -1);
+    b.texture = (uint32_t)texture_image(ts, ti, where);
+    const long si = ts.m.doc.array("textures")[(size_t)ti].integer("sampler", -1);
+    if (si >= 0) {
+        const auto &samplers = ts.m.doc.array("samplers");
+        if (si >= (long)samplers.size())
+            throw Error(where + ": sampler index out of range");
+        const long mf = samplers[(size_t)si].integer("minFilter", -1);
+        if (mf >= 9984 && mf <= 9987)
+            throw Error(where + ": textures with a mipmap minification filter (EWA filtering of mipmapped textures) "
+                                "are not supported",
+                        true);
+    }
+    b.filter = 0;
+    b.flip_v = 0;
+    for (int c = 0; c < 4; ++c) {
+        b.swizzle[c] = swizzle[c];
+        b.scale[c] = scale[c];
+    }
+    b.uv_scale[0] = b.uv_scale[1] = 1.0f;
+    if (const Json *ext = info.get("extensions"))
+        if (const Json *tt = ext->get("KHR_texture_transform")) {
+            const std::vector<double> sc = tt->numbers("scale"), of = tt->numbers("offset");
+            for (size_t k = 0; k < 2 && k < sc.size(); ++k)
+                b.uv_scale[k] = (float)sc[k];
+            for (size_t k = 0; k < 2 && k < of.size(); ++k)
+                b.uv_offset[k] = (float)of[k];
+        }
+    b.normal_space = 0;
+    b.range01 = 1;
+    b.strength = 1.0f;
+    for (int k = 0; k < 4; ++k)
+        b.to_world[5 * k] = 1.0f;
+    return b;
+}
+
+// The metallic-roughness material as a principled BSDF (mesh_asset.cpp:672-940): basecolor,
+// roughness, metallic; emissive = KHR_materials_emissive_strength x emissiveFactor, an emitter when
+// both are positive; ior (KHR_materials_ior, 1.5); specular_r0_mul (KHR_materials_specular:
+// specularFactor x mean(specularColorFactor), 0.5 without it); specular_trans
+// (KHR_materials_transmission, which also makes the mesh one-sided); no diffuse transmission; GGX.
+// Textures (with TextureSet): baseColorTexture x baseColorFactor, metallicRoughnessTexture's G x
+// roughnessFactor and B x metallicFactor, specularTexture x the specular factor,
+// transmissionTexture x transmissionFactor, normalTexture as a tangent-space normal map of strength
+// normalTexture.scale, and for alpha modes other than OPAQUE an opacity map of the base colour
+// texture's alpha x baseColorFactor[3] (the constant factor without a texture).  Emitters with an
+// emissive texture are unsupported (textured emission needs the emitter's texture importance).
+ks_material_desc material(const Json &src, const std::string &where, bool &twosided, TextureSet *ts,
+                          uint32_t index, std::vector<ks_texture_binding> &binds)
 {
     ks_material_desc d{};
     const Json *pbr = src.get("pbrMetallicRoughness");
-    if (has_texture(pbr, "baseColorTexture") || has_texture(pbr, "metallicRoughnessTexture") ||
-        src.get("emissiveTexture") || src.get("normalTexture"))
-        throw Error(where + ": textured materials are not supported (constant fields only)", true);
-    if (src.string("alphaMode", "OPAQUE") != "OPAQUE")
-        throw Error(where + ": alpha modes other than OPAQUE (opacity maps) are not supported", true);
+    const Json *ext = src.get("extensions");
+    auto extension = [&](const char *name) { return ext ? ext->get(name) : nullptr; };
+    const Json *bct = pbr ? pbr->get("baseColorTexture") : nullptr;
+    const Json *mrt = pbr ? pbr->get("metallicRoughnessTexture") : nullptr;
     std::vector<double> bc = pbr ? pbr->numbers("baseColorFactor") : std::vector<double>{};
     if (bc.empty())
         bc = {1.0, 1.0, 1.0, 1.0};
@@ -576,8 +713,6 @@ ks_material_desc material(const Json &src, const std::string &where, bool &twosi
         d.basecolor[c] = (float)bc[c];
     d.roughness = pbr ? (float)pbr->number("roughnessFactor", 1.0) : 1.0f;
     d.metallic = pbr ? (float)pbr->number("metallicFactor", 1.0) : 1.0f;
-    const Json *ext = src.get("extensions");
-    auto extension = [&](const char *name) { return ext ? ext->get(name) : nullptr; };
     float strength = 1.0f;
     if (const Json *e = extension("KHR_materials_emissive_strength"))
         strength = (float)e->number("emissiveStrength", 1.0);
@@ -592,31 +727,98 @@ ks_material_desc material(const Json &src, const std::string &where, bool &twosi
         d.has_emission = 1;
         for (int c = 0; c < 3; ++c)
             d.emission[c] = d.emissive[c];
+        if (src.get("emissiveTexture"))
+            throw Error(where + ": emitters with an emissive texture are not supported", true);
     }
     d.ior = 1.5f;
     if (const Json *e = extension("KHR_materials_ior"))
         d.ior = (float)e->number("ior", 1.5);
     d.specular_r0_mul = 0.5f;
+    const Json *spec_tex = nullptr, *trans_tex = nullptr;
     if (const Json *e = extension("KHR_materials_specular")) {
-        if (e->get("specularTexture") || e->get("specularColorTexture"))
-            throw Error(where + ": textured specular is not supported", true);
         const std::vector<double> scf = e->numbers("specularColorFactor");
+        float sf = 0.5f;
         if (e->get("specularFactor") || !scf.empty()) {
-            float sf = (float)e->number("specularFactor", 1.0);
+            sf = (float)e->number("specularFactor", 1.0);
             if (scf.size() == 3)
                 sf *= (float)((scf[0] + scf[1] + scf[2]) / 3.0);
-            d.specular_r0_mul = sf;
         }
+        d.specular_r0_mul = sf;
+        spec_tex = e->get("specularTexture");
     }
+    float trans = 0.0f;
     if (const Json *e = extension("KHR_materials_transmission")) {
-        if (e->get("transmissionTexture"))
-            throw Error(where + ": textured transmission is not supported", true);
         twosided = false;
-        d.specular_trans = (float)e->number("transmissionFactor", 0.0);
+        trans = (float)e->number("transmissionFactor", 0.0);
+        d.specular_trans = trans;
+        trans_tex = e->get("transmissionTexture");
     }
     d.diffuse_trans = 0.0f;
     d.diffuse_trans_fwd = 0.0f;
     d.microfacet = 0;
+    const bool alpha = src.string("alphaMode", "OPAQUE") != "OPAQUE";
+    const Json *nt = src.get("normalTexture");
+    if (!ts) {
+        if (bct || mrt || nt || spec_tex || trans_tex)
+            throw Error(where + ": textured materials are not supported (constant fields only)", true);
+        if (alpha)
+            throw Error(where + ": alpha modes other than OPAQUE (opacity maps) are not supported", true);
+        return d;
+    }
+    const int32_t id4[4] = {0, 1, 2, 3};
+    const float one4[4] = {1, 1, 1, 1};
+    if (bct) {
+        const float sc[4] = {(float)bc[0], (float)bc[1], (float)bc[2], 1.0f};
+        binds.push_back(texture_binding(*ts, *bct, index, KS_FIELD_BASECOLOR, sc, id4, where));
+        if (alpha) {
+            const float sa[4] = {(float)bc[3], 1, 1, 1};
+            const int32_t sw[4] = {3, -1, -1, -1};
+            binds.push_back(texture_binding(*ts, *bct, index, KS_FIELD_OPACITY_MAP, sa, sw, where));
+        }
+    } else if (alpha) {
+        // the constant opacity baseColorFactor[3]: a one-texel texture of 1 scaled by it
+        Texture t;
+        t.width = t.height = t.channels = 1;
+        t.format = 2;
+        t.srgb = false;
+        const float v = 1.0f;
+        t.bytes.resize(4);
+        std::memcpy(t.bytes.data(), &v, 4);
+        ks_texture_binding b{};
+        b.material = index;
+        b.field = KS_FIELD_OPACITY_MAP;
+        b.texture = (uint32_t)ts->out.size();
+        ts->out.push_back(std::move(t));
+        b.swizzle[0] = 0;
+        b.swizzle[1] = b.swizzle[2] = b.swizzle[3] = -1;
+        b.scale[0] = (float)bc[3];
+        b.scale[1] = b.scale[2] = b.scale[3] = 1.0f;
+        b.uv_scale[0] = b.uv_scale[1] = 1.0f;
+        b.range01 = 1;
+        b.strength = 1.0f;
+        for (int k = 0; k < 4; ++k)
+            b.to_world[5 * k] = 1.0f;
+        binds.push_back(b);
+    }
+    if (mrt) {
+        const float sr[4] = {d.roughness, 1, 1, 1}, sm[4] = {d.metallic, 1, 1, 1};
+        const int32_t g[4] = {1, -1, -1, -1}, bl[4] = {2, -1, -1, -1};
+        binds.push_back(texture_binding(*ts, *mrt, index, KS_FIELD_ROUGHNESS, sr, g, where));
+        binds.push_back(texture_binding(*ts, *mrt, index, KS_FIELD_METALLIC, sm, bl, where));
+    }
+    if (spec_tex) {
+        const float ss[4] = {d.specular_r0_mul, 1, 1, 1};
+        binds.push_back(texture_binding(*ts, *spec_tex, index, KS_FIELD_SPECULAR_R0_MUL, ss, id4, where));
+    }
+    if (trans_tex) {
+        const float st[4] = {trans, 1, 1, 1};
+        binds.push_back(texture_binding(*ts, *trans_tex, index, KS_FIELD_SPECULAR_TRANS, st, id4, where));
+    }
+    if (nt) {
+        ks_texture_binding b = texture_binding(*ts, *nt, index, KS_FIELD_NORMAL_MAP, one4, id4, where);
+        b.strength = (float)nt->number("scale", 1.0);
+        binds.push_back(b);
+    }
     return d;
 }
 
@@ -672,12 +874,30 @@ Mat4 local_transform(const Json &node)
 
 } // namespace
 
-Compound load(const fs::path &path, bool load_materials)
+Compound load(const fs::path &path, bool load_materials, bool load_textures)
 {
     Model m = load_model(path);
     Compound out;
     const auto &meshes = m.doc.array("meshes");
     const auto &mats = m.doc.array("materials");
+    TextureSet ts{m, path, out.textures, std::vector<long>(m.doc.array("images").size(), -1),
+                  std::vector<int>(m.doc.array("images").size(), 0)};
+    for (const Json &mat : mats) {
+        auto mark = [&](const Json *info) {
+            if (!info)
+                return;
+            const long ti = info->integer("index", -1);
+            const auto &texs = m.doc.array("textures");
+            if (ti >= 0 && ti < (long)texs.size()) {
+                const long img = texs[(size_t)ti].integer("source", -1);
+                if (img >= 0 && img < (long)ts.srgb.size())
+                    ts.srgb[(size_t)img] = 1;
+            }
+        };
+        const Json *pbr = mat.get("pbrMetallicRoughness");
+        mark(pbr ? pbr->get("baseColorTexture") : nullptr);
+        mark(mat.get("emissiveTexture"));
+    }
     for (size_t i = 0; i < meshes.size(); ++i) {
         Prototype proto;
         const auto &prims = meshes[i].array("primitives");
@@ -713,7 +933,8 @@ Compound load(const fs::path &path, bool load_materials)
                 const long mi = pr.integer("material", -1);
                 if (mi < 0 || mi >= (long)mats.size())
                     throw Error(where + ": primitive without a material", true);
-                proto.materials.push_back(material(mats[(size_t)mi], where, md.twosided));
+                proto.materials.push_back(material(mats[(size_t)mi], where, md.twosided,
+                                                   load_textures ? &ts : nullptr, (uint32_t)j, proto.bindings));
             }
             proto.meshes.push_back(std::move(md));
         }

@@ -5,9 +5,12 @@
 // primitives' metallic-roughness materials as principled BSDFs with constant fields.
 //
 // .gltf (JSON, buffers in files next to it or in base64 data URIs) and .glb (binary container).
-// Not handled, each an error marked unsupported: textures (textured shader fields), alpha modes
-// other than OPAQUE (opacity maps), sparse accessors, non-triangle primitives, index types other
-// than unsigned short / unsigned int (the reference asserts on those too).  Animations are not
+// Textures: PNG images (8- and 16-bit) bound to the base colour, metallic-roughness, specular,
+// transmission and normal slots with the nearest filter, and alpha modes other than OPAQUE as
+// opacity maps.  Not handled, each an error marked unsupported: JPEG and other image formats,
+// samplers with a mipmap minification filter (EWA filtering), emitters with an emissive texture,
+// sparse accessors, non-triangle primitives, index types other than unsigned short / unsigned int
+// (the reference asserts on those too).  Animations are not
 // read (camera and transform animation are outside the small_pt path).
 #pragma once
 #include "../../include/ks_b200.h"
@@ -29,10 +32,21 @@ struct Error : std::runtime_error
     Error(const std::string &what, bool unsupported = false) : std::runtime_error(what), unsupported(unsupported) {}
 };
 
+// A decoded texture image: width x height x channels samples of `format` (0 u8, 1 u16, 2 f32).
+struct Texture
+{
+    int width = 0, height = 0, channels = 0, format = 0;
+    bool srgb = false;
+    std::vector<uint8_t> bytes;
+};
+
 struct Prototype
 {
     std::vector<mesh::MeshData> meshes;        // one per primitive
     std::vector<ks_material_desc> materials;   // one per primitive (load_materials), else empty
+    // textured fields of the materials (load_textures): `material` is the primitive's index in
+    // this prototype, `texture` an index into Compound::textures
+    std::vector<ks_texture_binding> bindings;
 };
 
 struct Instance
@@ -45,9 +59,12 @@ struct Compound
 {
     std::vector<Prototype> prototypes;
     std::vector<Instance> instances;
+    std::vector<Texture> textures;
 };
 
-Compound load(const std::filesystem::path &path, bool load_materials);
+// load_textures: textured materials read their PNG images (see material() in gltf.cpp); without
+// it a textured material is an unsupported-status error.
+Compound load(const std::filesystem::path &path, bool load_materials, bool load_textures = true);
 
 // CameraAnimation (camera.h:44-61, camera.cpp:207-465): the translation and rotation keys of a
 // named perspective camera's node in a .glb file, evaluated with linear interpolation of the

@@ -268,7 +268,9 @@ void write_exr(const fs::path &path, const float *pixels, int w, int h, int c, b
     write_file(path, out);
 }
 
-std::vector<float> read_exr(const fs::path &path, int &width, int &height)
+// RGBA as tinyexr's LoadEXR returns it: R, G, B and A (1 without an A channel); a file of one
+// channel gives that channel in all four.
+std::vector<float> read_exr_rgba(const fs::path &path, int &width, int &height)
 {
     const std::vector<uint8_t> f = read_file(path);
     const std::string where = path.string() + ": ";
@@ -347,7 +349,7 @@ std::vector<float> read_exr(const fs::path &path, int &width, int &height)
     const int64_t w = (int64_t)win[2] - win[0] + 1, h = (int64_t)win[3] - win[1] + 1;
     if (w <= 0 || h <= 0 || w * h > (1ll << 31))
         throw Error(where + "bad EXR data window");
-    int ri = -1, gi = -1, bi = -1, yi = -1;
+    int ri = -1, gi = -1, bi = -1, yi = -1, ai = -1;
     size_t line_bytes = 0;
     for (size_t k = 0; k < chans.size(); ++k) {
         const std::string &n = chans[k].name;
@@ -359,11 +361,15 @@ std::vector<float> read_exr(const fs::path &path, int &width, int &height)
             bi = (int)k;
         else if (n == "Y")
             yi = (int)k;
+        else if (n == "A")
+            ai = (int)k;
         line_bytes += (size_t)w * chans[k].bytes();
     }
     if (!(ri >= 0 && gi >= 0 && bi >= 0)) {
         if (yi < 0 && chans.size() == 1)
             yi = 0;
+        if (chans.size() == 1)
+            ai = yi;
         if (yi < 0)
             throw Error(where + "EXR file without R, G, B (or a single) channel", true);
         ri = gi = bi = yi;
@@ -372,7 +378,7 @@ std::vector<float> read_exr(const fs::path &path, int &width, int &height)
     need(8 * (size_t)n_chunks);
     std::vector<uint64_t> offsets((size_t)n_chunks);
     std::memcpy(offsets.data(), &f[pos], 8 * (size_t)n_chunks);
-    std::vector<float> rgb((size_t)(w * h * 3), 0.0f);
+    std::vector<float> rgba((size_t)(w * h * 4), 0.0f);
     std::vector<float> line((size_t)w * chans.size());
     for (int64_t ch = 0; ch < n_chunks; ++ch) {
         pos = (size_t)offsets[(size_t)ch];
@@ -418,16 +424,27 @@ std::vector<float> read_exr(const fs::path &path, int &width, int &height)
                     q += (size_t)chans[k].bytes();
                     line[k * (size_t)w + (size_t)x] = v;
                 }
-            float *row = &rgb[(size_t)((y0 + l) * w * 3)];
+            float *row = &rgba[(size_t)((y0 + l) * w * 4)];
             for (int64_t x = 0; x < w; ++x) {
-                row[3 * x] = line[(size_t)ri * w + x];
-                row[3 * x + 1] = line[(size_t)gi * w + x];
-                row[3 * x + 2] = line[(size_t)bi * w + x];
+                row[4 * x] = line[(size_t)ri * w + x];
+                row[4 * x + 1] = line[(size_t)gi * w + x];
+                row[4 * x + 2] = line[(size_t)bi * w + x];
+                row[4 * x + 3] = ai >= 0 ? line[(size_t)ai * w + x] : 1.0f;
             }
         }
     }
     width = (int)w;
     height = (int)h;
+    return rgba;
+}
+
+std::vector<float> read_exr(const fs::path &path, int &width, int &height)
+{
+    const std::vector<float> rgba = read_exr_rgba(path, width, height);
+    std::vector<float> rgb((size_t)width * height * 3);
+    for (size_t i = 0; i < (size_t)width * height; ++i)
+        for (int c = 0; c < 3; ++c)
+            rgb[3 * i + c] = rgba[4 * i + c];
     return rgb;
 }
 
@@ -561,6 +578,45 @@ std::vector<float> read_pfm(const fs::path &path, int &w, int &h)
     for (int y = 0; y < h; ++y)
         std::memcpy(&top_first[(size_t)y * w * 3], &rows[(size_t)(h - 1 - y) * w * 3], sizeof(float) * 3 * w);
     return top_first;
+}
+
+std::vector<float> read_float_texture(const fs::path &path, int channels, int &w, int &h)
+{
+    if (channels < 1 || channels > 4)
+        throw Error(path.string() + ": a texture has 1 to 4 channels");
+    const std::string ext = path.extension().string();
+    std::vector<float> out;
+    if (ext == ".exr") {
+        // load_from_exr (image_util.cpp:71-100): the first `channels` of LoadEXR's RGBA
+        const std::vector<float> rgba = read_exr_rgba(path, w, h);
+        out.resize((size_t)w * h * channels);
+        for (size_t i = 0; i < (size_t)w * h; ++i)
+            for (int c = 0; c < channels; ++c)
+                out[i * channels + c] = rgba[4 * i + c];
+        return out;
+    }
+    // load_from_hdr (image_util.cpp:54-63): stb_image's float loader with a requested channel
+    // count converts RGB to one or two channels as the mean of R, G and B (then alpha 1), and to
+    // four with alpha 1
+    const std::vector<float> rgb = ext == ".hdr" ? read_hdr(path, w, h) : ext == ".pfm" ? read_pfm(path, w, h)
+                                  : throw Error(path.string() + ": float textures are read from .exr, .hdr or .pfm "
+                                                                "files",
+                                                true);
+    out.resize((size_t)w * h * channels);
+    for (size_t i = 0; i < (size_t)w * h; ++i) {
+        const float *p = &rgb[3 * i];
+        float *o = &out[i * channels];
+        if (channels <= 2) {
+            o[0] = (p[0] + p[1] + p[2]) / 3.0f;
+            if (channels == 2)
+                o[1] = 1.0f;
+        } else {
+            o[0] = p[0], o[1] = p[1], o[2] = p[2];
+            if (channels == 4)
+                o[3] = 1.0f;
+        }
+    }
+    return out;
 }
 
 std::vector<float> read_rgb(const fs::path &path, int &w, int &h)

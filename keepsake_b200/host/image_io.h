@@ -40,6 +40,28 @@ std::vector<float> read_pfm(const std::filesystem::path &path, int &width, int &
 // By extension: .exr, .hdr or .pfm.
 std::vector<float> read_rgb(const std::filesystem::path &path, int &width, int &height);
 
+// RGBA of an OpenEXR file as tinyexr's LoadEXR gives it: alpha 1 without an A channel, the one
+// channel of a single-channel file in all four.
+std::vector<float> read_exr_rgba(const std::filesystem::path &path, int &width, int &height);
+// Float texels of a texture file (create_texture_from_image, texture.cpp:922-944): .exr through
+// load_from_exr (the first `channels` of the RGBA), .hdr (and .pfm) through stb_image's float
+// loader's channel conversion.
+std::vector<float> read_float_texture(const std::filesystem::path &path, int channels, int &width, int &height);
+
+// PNG (8- or 16-bit samples, all colour types, Adam7): samples row-major, top row first, channels
+// interleaved; palette images expanded to RGB (RGBA with a tRNS chunk), grey / RGB with a tRNS
+// colour key given an alpha channel, 1-, 2- and 4-bit grey scaled to 8 bits.
+struct Png
+{
+    int width = 0, height = 0, channels = 0, depth = 8; // depth 8 or 16
+    std::vector<uint16_t> samples;
+};
+Png read_png(const uint8_t *data, size_t size, const std::string &name);
+Png read_png(const std::filesystem::path &path);
+// The samples converted to `channels` (1-4) at `depth` (8 or 16; 16-bit samples reduced to 8 by
+// their high byte), as stb_image converts for a requested channel count.
+std::vector<uint16_t> convert_channels(const Png &png, int channels, int depth);
+
 // IEEE binary16 conversions (round to nearest even; exact widening).
 uint16_t float_to_half(float f);
 float half_to_float(uint16_t h);

@@ -524,6 +524,12 @@ void GeneratedScene::finalize()
     desc.n_prototypes = (uint32_t)prototypes.size();
     desc.instances = instances.empty() ? nullptr : instances.data();
     desc.n_instances = (uint32_t)instances.size();
+    for (size_t k = 0; k < textures.size(); ++k)
+        textures[k].texels = texture_bytes[k].data();
+    desc.textures = textures.empty() ? nullptr : textures.data();
+    desc.n_textures = (uint32_t)textures.size();
+    desc.bindings = bindings.empty() ? nullptr : bindings.data();
+    desc.n_bindings = (uint32_t)bindings.size();
 }
 
 bool generate_scene(const std::string &kind, uint64_t seed, const ProceduralOptions &opts, GeneratedScene &out)

@@ -48,6 +48,11 @@ struct GeneratedScene
     std::vector<ks_mesh_desc> mesh_descs;
     std::vector<ks_prototype_desc> prototypes; // empty: flat scene
     std::vector<ks_instance_desc> instances;
+    // textures (loaded assets): texels per texture, described by `textures` (texels set by
+    // finalize), and the bindings of textured material fields
+    std::vector<std::vector<uint8_t>> texture_bytes;
+    std::vector<ks_texture_desc> textures;
+    std::vector<ks_texture_binding> bindings;
     ks_scene_desc desc{};
     float camera_to_world[16]{};
     float vfov = 0.7f;

@@ -74,6 +74,9 @@ struct MeshAsset
 {
     std::vector<Geometry> geometries;
     std::vector<ks_material_desc> materials; // procedural assets bring their own
+    // textured fields of `materials` (glTF assets): `material` indexes `materials`, `texture` the
+    // service's texture store
+    std::vector<ks_texture_binding> bindings;
     std::vector<float> sky_map;              // procedural assets: their sky
     ks_sky_desc sky{};
     // compound (glTF) assets: prototypes as runs of geometries, and their instances
@@ -90,14 +93,28 @@ struct ConfigServiceImpl
     fs::path output_dir = fs::current_path();
     std::map<std::string, ConfigTask> tasks;
     std::map<std::string, std::shared_ptr<MeshAsset>> meshes;
-    std::map<std::string, ks_material_desc> materials;
+    // a material and the bindings of its textured fields (`material` unset, `texture` an index
+    // into `textures`)
+    struct TaskMaterial
+    {
+        ks_material_desc d{};
+        std::vector<ks_texture_binding> binds;
+    };
+    std::map<std::string, TaskMaterial> materials;
+    // every texture the configuration loaded: texture assets, glTF images, one-texel constants
+    std::vector<ksb::gltf::Texture> textures;
+    std::vector<int> texture_mips; // per texture: created with build_mipmaps
+    std::map<std::string, uint32_t> texture_assets;
 
     const Value *find_asset(const std::string &path) const;
     std::shared_ptr<MeshAsset> mesh_asset(const std::string &path);
     std::shared_ptr<MeshAsset> compound_asset(const std::string &path);
     std::shared_ptr<ksb::gltf::CameraAnimation> camera_animation(const std::string &path);
     std::map<std::string, std::shared_ptr<ksb::gltf::CameraAnimation>> animations;
-    ks_material_desc material(const std::string &path);
+    const TaskMaterial &material(const std::string &path);
+    uint32_t texture(const std::string &path);
+    uint32_t constant_texture(const float *value, int channels);
+    ks_texture_binding texture_field(const ConfigArgs &f, int n, int32_t field, const std::string &where);
 };
 
 struct ConfigArgsInternal
@@ -441,6 +458,7 @@ std::shared_ptr<MeshAsset> ConfigServiceImpl::mesh_asset(const std::string &path
         m->sky.map_rgb = nullptr;
     } else if (type == "inline") {
         // extension for small scenes written in the file: geometry = [{vertices = [...], indices = [...]}]
+        // (optional texcoords = [...], 2 numbers per vertex)
         ConfigArgs list = a["geometry"];
         for (int i = 0; i < list.array_size(); ++i) {
             ConfigArgs gi = list[i];
@@ -456,6 +474,14 @@ std::shared_ptr<MeshAsset> ConfigServiceImpl::mesh_asset(const std::string &path
                 if (x < 0 || x >= (double)(v.size() / 3))
                     throw ParseError("config: inline geometry index out of range");
                 geo.indices.push_back((uint32_t)x);
+            }
+            if (gi.contains("texcoords")) {
+                std::vector<double> tc;
+                flat_numbers(child(*gi.internal, "texcoords"), tc, "texcoords");
+                if (tc.size() != 2 * (v.size() / 3))
+                    throw ParseError("config: inline geometry needs 2 texcoords per vertex");
+                for (double x : tc)
+                    geo.texcoords.push_back((float)x);
             }
             m->geometries.push_back(std::move(geo));
         }
@@ -494,7 +520,17 @@ std::shared_ptr<MeshAsset> ConfigServiceImpl::compound_asset(const std::string &
     if (c.instances.empty())
         throw ParseError("config: compound mesh asset '" + path + "' instances no mesh");
     auto m = std::make_shared<MeshAsset>();
+    const uint32_t tex_base = (uint32_t)textures.size();
+    for (auto &t : c.textures) {
+        textures.push_back(std::move(t));
+        texture_mips.push_back(0);
+    }
     for (auto &p : c.prototypes) {
+        for (ks_texture_binding b : p.bindings) {
+            b.material += (uint32_t)m->materials.size(); // primitive index -> asset material
+            b.texture += tex_base;
+            m->bindings.push_back(b);
+        }
         m->prototypes.push_back({(uint32_t)m->geometries.size(), (uint32_t)p.meshes.size()});
         for (size_t k = 0; k < p.meshes.size(); ++k) {
             std::vector<ksb::mesh::MeshData> one(1);
@@ -539,7 +575,158 @@ std::shared_ptr<ksb::gltf::CameraAnimation> ConfigServiceImpl::camera_animation(
     return anim;
 }
 
-ks_material_desc ConfigServiceImpl::material(const std::string &path)
+// create_texture_from_image (texture.cpp:922-944): .exr / .hdr (and .pfm) as float texels, PNG as
+// 8-bit texels through stb_image's 8-bit loader with the requested channel count (16-bit PNGs kept
+// at 16 bits with keep_16bit, as tinygltf keeps glTF images).  Throws image::Error.
+ksb::gltf::Texture load_texture_file(const fs::path &file, int ch, bool srgb, bool keep_16bit)
+{
+    const std::string ext = file.extension().string();
+    ksb::gltf::Texture t;
+    t.channels = ch;
+    t.srgb = srgb;
+    if (ext == ".exr" || ext == ".hdr" || ext == ".pfm") {
+        const std::vector<float> v = ksb::image::read_float_texture(file, ch, t.width, t.height);
+        t.format = 2;
+        t.bytes.resize(v.size() * 4);
+        std::memcpy(t.bytes.data(), v.data(), t.bytes.size());
+    } else if (ext == ".png") {
+        const ksb::image::Png png = ksb::image::read_png(file);
+        const int depth = keep_16bit ? png.depth : 8;
+        const std::vector<uint16_t> v = ksb::image::convert_channels(png, ch, depth);
+        t.width = png.width;
+        t.height = png.height;
+        if (depth == 16) {
+            t.format = 1;
+            t.bytes.resize(v.size() * 2);
+            std::memcpy(t.bytes.data(), v.data(), t.bytes.size());
+        } else {
+            t.format = 0;
+            t.bytes.assign(v.begin(), v.end());
+        }
+    } else {
+        throw ksb::image::Error(file.string() + ": texture images are read from .png, .exr, .hdr or .pfm files",
+                                true);
+    }
+    return t;
+}
+
+// create_texture (texture.cpp:1068-1084) with create_texture_from_image (:922-944): `path`,
+// `channels`, `build_mipmaps`, `colorspace` ("Linear" or "sRGB"); .exr / .hdr (and .pfm) as float
+// texels, PNG as 8-bit texels (stb_image's 8-bit loader with the requested channel count).
+// Serialized (lz4) textures and other image formats are unsupported.
+uint32_t ConfigServiceImpl::texture(const std::string &path)
+{
+    auto it = texture_assets.find(path);
+    if (it != texture_assets.end())
+        return it->second;
+    const Value *node = find_asset(path);
+    if (!node || path.rfind("texture.", 0) != 0)
+        throw ParseError("config: unknown texture '" + path + "'");
+    ConfigArgs a = args_of(this, node, path);
+    if (a.load_bool("serialized", false))
+        throw StatusError(KS_ERR_UNSUPPORTED, "config: serialized textures are not supported");
+    const int ch = a.load_integer("channels");
+    const bool mips = a.load_bool("build_mipmaps");
+    const bool srgb = a.load_string("colorspace", "Linear") == "sRGB";
+    if (ch < 1 || ch > 4)
+        throw ParseError("config: texture '" + path + "' needs 1 to 4 channels");
+    ksb::gltf::Texture t;
+    try {
+        t = load_texture_file(a.load_path("path"), ch, srgb, false);
+    } catch (const ksb::image::Error &e) {
+        if (e.unsupported)
+            throw StatusError(KS_ERR_UNSUPPORTED, std::string("config: ") + e.what());
+        throw IoError(e.what());
+    }
+    textures.push_back(std::move(t));
+    texture_mips.push_back(mips ? 1 : 0);
+    texture_assets[path] = (uint32_t)textures.size() - 1;
+    return (uint32_t)textures.size() - 1;
+}
+
+// A constant field as a one-texel float texture (read with the nearest filter, scale 1).
+uint32_t ConfigServiceImpl::constant_texture(const float *value, int channels)
+{
+    ksb::gltf::Texture t;
+    t.width = t.height = 1;
+    t.channels = channels;
+    t.format = 2;
+    t.bytes.resize(4 * (size_t)channels);
+    std::memcpy(t.bytes.data(), value, t.bytes.size());
+    textures.push_back(std::move(t));
+    texture_mips.push_back(0);
+    return (uint32_t)textures.size() - 1;
+}
+
+// create_texture_shader_field_color<N> (shader_field.h:107-142): map (a texture asset), sampler
+// (create_texture_sampler, texture.cpp:1086-1121: nearest | linear | cubic with kernel mitchell |
+// bspline | catmull_rom; wrap_mode_u / wrap_mode_v repeat | clamp), flip_v (true), swizzle,
+// uv_scale, uv_offset, scale.  Linear and cubic lookups of a mipmapped texture choose their level
+// from the camera ray's differentials, and EWA filters with them: those are unsupported (the
+// nearest filter always reads level 0, and a texture without mipmaps has only level 0).
+ks_texture_binding ConfigServiceImpl::texture_field(const ConfigArgs &f, int n, int32_t field,
+                                                    const std::string &where)
+{
+    ks_texture_binding b{};
+    b.field = field;
+    b.texture = texture(f.load_string("map"));
+    ConfigArgs sm = f["sampler"];
+    const std::string st = sm.load_string("type");
+    if (st == "nearest") {
+        b.filter = 0;
+    } else if (st == "linear") {
+        b.filter = 1;
+    } else if (st == "cubic") {
+        b.filter = 2;
+        const std::string k = sm.load_string("kernel", "mitchell");
+        b.cubic_kernel = k == "bspline" ? 1 : (k == "catmull_rom" ? 2 : 0);
+    } else if (st == "ewa") {
+        throw StatusError(KS_ERR_UNSUPPORTED, "config: '" + where + "': EWA texture filtering is not supported");
+    } else {
+        throw ParseError("config: '" + where + "': unknown texture sampler type '" + st + "'");
+    }
+    if (b.filter != 0 && texture_mips[b.texture])
+        throw StatusError(KS_ERR_UNSUPPORTED, "config: '" + where + "': linear and cubic filtering of a texture "
+                                                                     "with mipmaps are not supported");
+    b.wrap_u = sm.load_string("wrap_mode_u", "repeat") == "clamp" ? 1 : 0;
+    b.wrap_v = sm.load_string("wrap_mode_v", "repeat") == "clamp" ? 1 : 0;
+    b.flip_v = f.load_bool("flip_v", true) ? 1 : 0;
+    for (int c = 0; c < 4; ++c) {
+        b.swizzle[c] = c < n ? c : -1;
+        b.scale[c] = 1.0f;
+    }
+    if (f.contains("swizzle")) {
+        if (n == 1) {
+            b.swizzle[0] = f.load_integer("swizzle");
+        } else {
+            float sw[4];
+            vec_n(child(*f.internal, "swizzle"), n, sw, "swizzle");
+            for (int c = 0; c < n; ++c)
+                b.swizzle[c] = (int32_t)sw[c];
+        }
+    }
+    b.uv_scale[0] = b.uv_scale[1] = 1.0f;
+    if (f.contains("uv_scale"))
+        vec_n(child(*f.internal, "uv_scale"), 2, b.uv_scale, "uv_scale");
+    if (f.contains("uv_offset"))
+        vec_n(child(*f.internal, "uv_offset"), 2, b.uv_offset, "uv_offset");
+    if (f.contains("scale")) {
+        if (n == 1)
+            b.scale[0] = f.load_float("scale");
+        else
+            vec_n(child(*f.internal, "scale"), n, b.scale, "scale");
+    }
+    b.range01 = 1;
+    b.strength = 1.0f;
+    for (int k = 0; k < 4; ++k)
+        b.to_world[5 * k] = 1.0f;
+    return b;
+}
+
+// create_material (material.cpp:169-178) over create_bsdf (bsdf.cpp:50-62): the BSDF's shader
+// fields, constant or textured, and the material's normal map (create_normal_map,
+// normal_map.cpp:40-55: map, space tangent | world, range01, strength, to_world).
+const ConfigServiceImpl::TaskMaterial &ConfigServiceImpl::material(const std::string &path)
 {
     auto it = materials.find(path);
     if (it != materials.end())
@@ -558,20 +745,28 @@ ks_material_desc ConfigServiceImpl::material(const std::string &path)
     if (type != "principled_bsdf" && type != "principled_brdf" && type != "lambertian")
         throw StatusError(KS_ERR_UNSUPPORTED, "config: bsdf type '" + type +
                                                   "' is not supported (principled_bsdf, principled_brdf, lambertian)");
-    if (a.contains("subsurface") || a.contains("normal_map"))
-        throw StatusError(KS_ERR_UNSUPPORTED, "config: subsurface and normal maps are not supported");
-    ks_material_desc d{};
-    // a constant shader field { type = "constant", value = ... } (or, as an extension, the bare value)
-    auto field = [&](const char *key, int n, float *out, const float *dflt) {
-        if (!b.contains(key)) {
-            std::memcpy(out, dflt, sizeof(float) * n);
+    if (!a.load_string("subsurface", "").empty())
+        throw StatusError(KS_ERR_UNSUPPORTED, "config: subsurface scattering is not supported");
+    TaskMaterial tm;
+    ks_material_desc &d = tm.d;
+    // a shader field: { type = "constant", value = ... } (or, as an extension, the bare value), or
+    // { type = "texture", ... }
+    auto field = [&](const char *key, int n, float *out, const float *dflt, int32_t field_id) {
+        std::memcpy(out, dflt, sizeof(float) * n);
+        if (!b.contains(key))
             return;
-        }
         const Value &v = child(*b.internal, key);
         const Value *val = &v;
         if (v.kind == Value::Kind::Table) {
             ConfigArgs f = b[key];
             std::string ft = f.load_string("type");
+            if (ft == "texture") {
+                if (field_id < 0)
+                    throw StatusError(KS_ERR_UNSUPPORTED, std::string("config: textured '") + key +
+                                                              "' is not supported");
+                tm.binds.push_back(texture_field(f, n, field_id, bsdf_path + "." + key));
+                return;
+            }
             if (ft != "constant")
                 throw StatusError(KS_ERR_UNSUPPORTED, std::string("config: shader field type '") + ft + "' of '" +
                                                           key + "' is not supported");
@@ -591,24 +786,25 @@ ks_material_desc ConfigServiceImpl::material(const std::string &path)
     if (type == "lambertian") {
         // create_lambertian (bsdf.cpp:43-48): albedo
         d.bsdf = 2;
-        field("albedo", 3, d.basecolor, c08);
+        field("albedo", 3, d.basecolor, c08, KS_FIELD_BASECOLOR);
     } else if (type == "principled_brdf") {
         // create_principled_brdf (principled_bsdf.cpp:227-244)
         d.bsdf = 1;
-        field("basecolor", 3, d.basecolor, c08);
-        field("roughness", 1, &d.roughness, &one);
-        field("metallic", 1, &d.metallic, &zero);
-        field("specular", 1, &d.specular, &half);
+        field("basecolor", 3, d.basecolor, c08, KS_FIELD_BASECOLOR);
+        field("roughness", 1, &d.roughness, &one, KS_FIELD_ROUGHNESS);
+        field("metallic", 1, &d.metallic, &zero, KS_FIELD_METALLIC);
+        field("specular", 1, &d.specular, &half, KS_FIELD_SPECULAR);
     } else {
-        field("basecolor", 3, d.basecolor, c08);
-        field("roughness", 1, &d.roughness, &one);
-        field("metallic", 1, &d.metallic, &zero);
-        field("ior", 1, &d.ior, &ior);
-        field("specular_r0_mul", 1, &d.specular_r0_mul, &half);
-        field("specular_trans", 1, &d.specular_trans, &zero);
-        field("diffuse_trans", 1, &d.diffuse_trans, &zero);
-        field("diffuse_trans_fwd", 1, &d.diffuse_trans_fwd, &half);
-        field("emissive", 3, d.emissive, z3);
+        field("basecolor", 3, d.basecolor, c08, KS_FIELD_BASECOLOR);
+        field("roughness", 1, &d.roughness, &one, KS_FIELD_ROUGHNESS);
+        field("metallic", 1, &d.metallic, &zero, KS_FIELD_METALLIC);
+        field("ior", 1, &d.ior, &ior, KS_FIELD_IOR);
+        field("specular_r0_mul", 1, &d.specular_r0_mul, &half, KS_FIELD_SPECULAR_R0_MUL);
+        field("specular_trans", 1, &d.specular_trans, &zero, KS_FIELD_SPECULAR_TRANS);
+        field("diffuse_trans", 1, &d.diffuse_trans, &zero, KS_FIELD_DIFFUSE_TRANS);
+        field("diffuse_trans_fwd", 1, &d.diffuse_trans_fwd, &half, KS_FIELD_DIFFUSE_TRANS_FWD);
+        // a textured emissive field would make a textured emitter, which needs its texture's importance
+        field("emissive", 3, d.emissive, z3, -1);
     }
     if (type != "lambertian") {
         std::string mf = b.load_string("microfacet", "ggx");
@@ -623,8 +819,43 @@ ks_material_desc ConfigServiceImpl::material(const std::string &path)
         a.load_vec3("emission", d.emission);
         d.has_emission = 1;
     }
-    materials[path] = d;
-    return d;
+    const std::string nm_path = a.load_string("normal_map", "");
+    if (!nm_path.empty()) {
+        const Value *nnode = find_asset(nm_path);
+        if (!nnode || nm_path.rfind("normal_map.", 0) != 0)
+            throw ParseError("config: unknown normal map '" + nm_path + "'");
+        ConfigArgs nm = args_of(this, nnode, nm_path);
+        ConfigArgs mf = nm["map"];
+        ks_texture_binding nb{};
+        if (mf.load_string("type") == "texture") {
+            nb = texture_field(mf, 3, KS_FIELD_NORMAL_MAP, nm_path + ".map");
+        } else {
+            if (mf.load_string("type") != "constant")
+                throw StatusError(KS_ERR_UNSUPPORTED, "config: '" + nm_path + "': shader field type '" +
+                                                          mf.load_string("type") + "' is not supported");
+            float v[3];
+            mf.load_vec3("value", v);
+            nb.field = KS_FIELD_NORMAL_MAP;
+            nb.texture = constant_texture(v, 3);
+            for (int c = 0; c < 4; ++c) {
+                nb.swizzle[c] = c < 3 ? c : -1;
+                nb.scale[c] = 1.0f;
+            }
+            nb.uv_scale[0] = nb.uv_scale[1] = 1.0f;
+        }
+        const std::string space = nm.load_string("space", "tangent");
+        if (space != "tangent" && space != "world")
+            throw ParseError("config: '" + nm_path + "': normal map space is tangent or world");
+        nb.normal_space = space == "world" ? 1 : 0;
+        nb.range01 = nm.load_bool("range01", true) ? 1 : 0;
+        nb.strength = nm.load_float("strength", 1.0f);
+        float id[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};
+        if (nm.contains("to_world"))
+            nm.load_transform("to_world", id);
+        std::memcpy(nb.to_world, id, sizeof(id));
+        tm.binds.push_back(nb);
+    }
+    return materials[path] = std::move(tm);
 }
 
 // ---- small_pt task ---------------------------------------------------------------------------
@@ -734,6 +965,7 @@ void small_pt_b200(const ConfigArgs &args, const fs::path &task_dir, int task_id
     if (!compound)
         subscenes = {ks_prototype_desc{0, (uint32_t)asset->geometries.size()}};
     std::vector<ks_material_desc> mats;
+    std::vector<ks_texture_binding> binds; // `texture` indexes svc->textures until remapped below
     std::vector<uint32_t> geom_mat(asset->geometries.size());
     if (args.contains("material")) {
         // assign_material_list (mesh_asset.cpp:286-299): one list per subscene, one material per
@@ -750,7 +982,12 @@ void small_pt_b200(const ConfigArgs &args, const fs::path &task_dir, int task_id
                 auto it = index.find(name);
                 if (it == index.end()) {
                     it = index.emplace(name, (uint32_t)mats.size()).first;
-                    mats.push_back(svc->material(name));
+                    const auto &tm = svc->material(name);
+                    for (ks_texture_binding b : tm.binds) {
+                        b.material = (uint32_t)mats.size();
+                        binds.push_back(b);
+                    }
+                    mats.push_back(tm.d);
                 }
                 geom_mat[subscenes[sub].first_mesh + k] = it->second;
             }
@@ -762,6 +999,28 @@ void small_pt_b200(const ConfigArgs &args, const fs::path &task_dir, int task_id
             geom_mat[g] = (uint32_t)asset->geometries[g].own_material;
         }
         mats = asset->materials;
+        binds = asset->bindings;
+    }
+    // the textures the bindings use, in order of first use
+    std::vector<ks_texture_desc> tex_descs;
+    {
+        std::map<uint32_t, uint32_t> used;
+        for (ks_texture_binding &b : binds) {
+            auto u = used.find(b.texture);
+            if (u == used.end()) {
+                const ksb::gltf::Texture &t = svc->textures[b.texture];
+                ks_texture_desc td{};
+                td.texels = t.bytes.data();
+                td.width = (uint32_t)t.width;
+                td.height = (uint32_t)t.height;
+                td.channels = (uint32_t)t.channels;
+                td.format = t.format;
+                td.srgb = t.srgb ? 1 : 0;
+                u = used.emplace(b.texture, (uint32_t)tex_descs.size()).first;
+                tex_descs.push_back(td);
+            }
+            b.texture = u->second;
+        }
     }
     std::vector<ks_mesh_desc> meshes(asset->geometries.size());
     for (size_t g = 0; g < meshes.size(); ++g) {
@@ -781,6 +1040,10 @@ void small_pt_b200(const ConfigArgs &args, const fs::path &task_dir, int task_id
     desc.n_meshes = (uint32_t)meshes.size();
     desc.materials = mats.data();
     desc.n_materials = (uint32_t)mats.size();
+    desc.textures = tex_descs.empty() ? nullptr : tex_descs.data();
+    desc.n_textures = (uint32_t)tex_descs.size();
+    desc.bindings = binds.empty() ? nullptr : binds.data();
+    desc.n_bindings = (uint32_t)binds.size();
     if (compound) {
         desc.prototypes = asset->prototypes.data();
         desc.n_prototypes = (uint32_t)asset->prototypes.size();
@@ -1209,6 +1472,45 @@ ks_status ks_image_save_exr(const char *path, const float *pixels, int32_t width
         g_config_error = e.what();
         return KS_ERR_IO;
     }
+}
+
+ks_status ks_texture_load(const char *path, int32_t channels, int32_t srgb, int32_t keep_16bit,
+                          ks_texture_desc *out)
+{
+    g_config_error.clear();
+    if (!path || !out || channels < 1 || channels > 4) {
+        g_config_error = "ks_texture_load: null argument or channels outside 1-4";
+        return KS_ERR_INVALID_ARGUMENT;
+    }
+    *out = ks_texture_desc{};
+    try {
+        ksb::gltf::Texture t = ks_b200::load_texture_file(path, channels, srgb != 0, keep_16bit != 0);
+        void *texels = std::malloc(t.bytes.size());
+        if (!texels)
+            return KS_ERR_OUT_OF_MEMORY;
+        std::memcpy(texels, t.bytes.data(), t.bytes.size());
+        out->texels = texels;
+        out->width = (uint32_t)t.width;
+        out->height = (uint32_t)t.height;
+        out->channels = (uint32_t)t.channels;
+        out->format = t.format;
+        out->srgb = t.srgb ? 1 : 0;
+        return KS_OK;
+    } catch (const ksb::image::Error &e) {
+        g_config_error = e.what();
+        return e.unsupported ? KS_ERR_UNSUPPORTED : KS_ERR_IO;
+    } catch (const std::exception &e) {
+        g_config_error = e.what();
+        return KS_ERR_IO;
+    }
+}
+
+void ks_texture_free(ks_texture_desc *t)
+{
+    if (!t)
+        return;
+    std::free(const_cast<void *>(t->texels));
+    t->texels = nullptr;
 }
 
 ks_status ks_image_load_rgb(const char *path, float **pixels, int32_t *width, int32_t *height)
