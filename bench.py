@@ -723,7 +723,8 @@ def main():
     e2e = {"value": e2e_rays / e2e_t / 1e6 if e2e_t > 0 else None, "unit": "Mrays/s", "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": d2h, "steps": e2e_steps, "timing": "host wall clock around synchronous C-ABI calls",
            "step_seconds": {key: statistics.median(p[key] for p in e2e_parts) for key in e2e_parts[0]} if e2e_parts
-           else None}
+           else None,
+           "step_seconds_max": {key: max(p[key] for p in e2e_parts) for key in e2e_parts[0]} if e2e_parts else None}
 
     ttr = c1 = c4 = c5 = None
     if rank == 0 and world == 1 and not args.no_c1:

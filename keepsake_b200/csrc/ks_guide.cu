@@ -16,6 +16,8 @@
 #include "ks_internal.h"
 #include "ks_tc.cuh"
 
+#include <cuda_fp16.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -87,6 +89,7 @@ struct MlpArgs
 {
     GridParams gp;
     const float *grid;        // kLevels * T * 2
+    const __half2 *grid_h;    // its FP16 copy (inference)
     const uint8_t *w_image;   // bf16 weight image (kWImage bytes)
     uint32_t n;               // rows
     uint32_t stride;          // floats between consecutive rows of pos / wo / nrm / wi (3 or 4)
@@ -188,7 +191,19 @@ __device__ __forceinline__ float2 ld_grid(const float2 *ptr, uint64_t pol)
     return v;
 }
 
-__device__ __forceinline__ void encode_row(const GridParams &gp, const float *grid, bool valid, f3 pn, f3 wo,
+// An entry of the FP16 inference copy of the table (two features in one 32-bit word).
+__device__ __forceinline__ float2 ld_grid(const __half2 *ptr, uint64_t pol)
+{
+    uint32_t u;
+    asm volatile("ld.global.nc.L2::cache_hint.b32 %0, [%1], %2;" : "=r"(u) : "l"(ptr), "l"(pol));
+    __half2 h;
+    memcpy(&h, &u, 4);
+    return __half22float2(h);
+}
+
+// Table: float2 (the FP32 master table: training) or __half2 (its FP16 copy: inference).
+template <class Entry>
+__device__ __forceinline__ void encode_row(const GridParams &gp, const Entry *grid, bool valid, f3 pn, f3 wo,
                                            f3 nrm, uint8_t *x0)
 {
     const uint64_t pol = l2_keep_policy();
@@ -198,7 +213,7 @@ __device__ __forceinline__ void encode_row(const GridParams &gp, const float *gr
         if (valid) {
             Corner c;
             level_corners(gp, l, pn, c);
-            const float2 *tab = reinterpret_cast<const float2 *>(grid) + (size_t)l * kTableSize;
+            const Entry *tab = grid + (size_t)l * kTableSize;
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
                 float2 e = ld_grid(&tab[c.idx[k]], pol);
@@ -298,7 +313,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp(MlpArgs a)
             wo = normalize(load_row3(a.wo, row, a.stride));
             nrm = normalize(load_row3(a.nrm, row, a.stride));
         }
-        encode_row(a.gp, a.grid, valid, pn, wo, nrm, xb[0]);
+        // training encodes from the FP32 master table its gradients update; inference from the FP16 copy
+        if constexpr (kTrain)
+            encode_row(a.gp, reinterpret_cast<const float2 *>(a.grid), valid, pn, wo, nrm, xb[0]);
+        else
+            encode_row(a.gp, a.grid_h, valid, pn, wo, nrm, xb[0]);
         float o[kOut];
         if (!mlp_forward(xb, sw, tmem, bar, phase, cta_err, a.err, o))
             goto done;
@@ -367,10 +386,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp(MlpArgs a)
                         Corner c;
                         level_corners(a.gp, lev, pn, c);
                         float2 *gt = reinterpret_cast<float2 *>(a.grid_grad) + (size_t)lev * kTableSize;
-                        for (int k = 0; k < 8; ++k) {
-                            atomicAdd(&gt[c.idx[k]].x, c.w[k] * v[i]);
-                            atomicAdd(&gt[c.idx[k]].y, c.w[k] * v[i + 1]);
-                        }
+                        // one vector reduction per corner (both features of the entry)
+                        for (int k = 0; k < 8; ++k)
+                            atomicAdd(&gt[c.idx[k]], make_float2(c.w[k] * v[i], c.w[k] * v[i + 1]));
                     }
                 }
             }
@@ -411,7 +429,7 @@ done:
 struct PathArgs
 {
     GridParams gp;
-    const float *grid;
+    const __half2 *grid_h; // FP16 copy of the table
     const uint8_t *w_image;
     const uint32_t *queue, *queue_count;
     const float4 *o_pdf, *d_info, *hits;
@@ -472,7 +490,7 @@ __global__ void __launch_bounds__(kThreads, kPathCtasPerSm) k_guide_paths(PathAr
             }
             nrm = facing_normal(p0, p1, p2, wo);
         }
-        encode_row(a.gp, a.grid, valid, pn, wo, nrm, xb[0]);
+        encode_row(a.gp, a.grid_h, valid, pn, wo, nrm, xb[0]);
         float o[kOut];
         if (!mlp_forward(xb, sw, tmem, bar, phase, cta_err, a.err, o))
             break;
@@ -506,6 +524,15 @@ __global__ void k_pack(const float *w, uint8_t *image)
     *reinterpret_cast<__nv_bfloat16 *>(image + w_soff(l) + w_off(l, n, k)) = __float2bfloat16_rn(w[i]);
 }
 
+// FP32 master table -> FP16 copy read by inference (round to nearest even, clamped to the FP16 range)
+__global__ void k_pack_grid(const float2 *grid, __half2 *out, size_t n)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const float2 v = grid[i];
+        out[i] = __floats2half2_rn(fminf(fmaxf(v.x, -65504.0f), 65504.0f), fminf(fmaxf(v.y, -65504.0f), 65504.0f));
+    }
+}
+
 // Adam (adam.slang:25-51)
 __global__ void k_adam(float *p, float *g, float *m, float *v, size_t n, float lr, float b1, float b2, float eps,
                        float c1, float c2)
@@ -532,6 +559,7 @@ struct ks_guide
     DevBuf<float> grid, grid_grad, grid_m, grid_v;
     DevBuf<float> w, w_grad, w_m, w_v;
     DevBuf<uint8_t> w_image;
+    DevBuf<__half2> grid_h; // FP16 copy of grid for inference, refreshed with w_image
     DevBuf<int> err;
     DevBuf<double> loss;
     int iter = 0;
@@ -545,13 +573,17 @@ namespace guide_impl
 {
 size_t grid_count() { return (size_t)kLevels * kTableSize * kFeatPerLevel; }
 
-ks_status pack(ks_guide *g)
+// The inference images of the parameters: BF16 weights, FP16 table.
+ks_status pack(ks_guide *g, cudaStream_t st)
 {
-    k_pack<<<(kWeights + 255) / 256, 256, 0, g->ctx->stream>>>(g->w.ptr, g->w_image.ptr);
+    k_pack<<<(kWeights + 255) / 256, 256, 0, st>>>(g->w.ptr, g->w_image.ptr);
+    k_pack_grid<<<g->ctx->sm_count * 8, 256, 0, st>>>(reinterpret_cast<const float2 *>(g->grid.ptr), g->grid_h.ptr,
+                                                      (size_t)kLevels * kTableSize);
     KS_CUDA_TRY(g->ctx, cudaGetLastError());
     g->packed = true;
     return KS_OK;
 }
+ks_status pack(ks_guide *g) { return pack(g, g->ctx->stream); }
 
 ks_status check_err(ks_guide *g)
 {
@@ -577,6 +609,7 @@ ks_status run_mlp(ks_guide *g, bool train, uint32_t n, const float *pos, const f
     MlpArgs a{};
     a.gp = g->gp;
     a.grid = g->grid.ptr;
+    a.grid_h = g->grid_h.ptr;
     a.w_image = g->w_image.ptr;
     a.n = n;
     a.stride = stride;
@@ -630,13 +663,13 @@ ks_status infer_paths(ks_guide *g, const uint32_t *queue, const uint32_t *queue_
     if (!stream)
         stream = g->ctx->stream;
     if (!g->packed) {
-        k_pack<<<(kWeights + 255) / 256, 256, 0, stream>>>(g->w.ptr, g->w_image.ptr);
-        KS_CUDA_TRY(g->ctx, cudaGetLastError());
-        g->packed = true;
+        ks_status s = pack(g, stream);
+        if (s != KS_OK)
+            return s;
     }
     PathArgs a{};
     a.gp = g->gp;
-    a.grid = g->grid.ptr;
+    a.grid_h = g->grid_h.ptr;
     a.w_image = g->w_image.ptr;
     a.queue = queue;
     a.queue_count = queue_count;
@@ -763,6 +796,8 @@ ks_status ks_guide_create(ks_context *ctx, const ks_guide_params *params, ks_gui
             e = buf->alloc(kWeights);
     if (e == cudaSuccess)
         e = g->w_image.alloc(kWImage);
+    if (e == cudaSuccess)
+        e = g->grid_h.alloc((size_t)kLevels * kTableSize);
     if (e == cudaSuccess)
         e = g->err.alloc(1);
     if (e == cudaSuccess)

@@ -56,14 +56,22 @@ struct GridParams
 
 __host__ __device__ inline uint32_t level_res(const GridParams &g, int l) { return g.res[l]; }
 
-// Grid cell corner -> table entry: dense indexing while the level fits, else the spatial hash of
-// Teschner et al. with the primes used by instant-ngp.
-__device__ __forceinline__ uint32_t grid_index(uint32_t res, uint32_t x, uint32_t y, uint32_t z)
+// Grid cell corner -> table entry.  Corners are grouped in 2 x 2 x 2 blocks of 8 consecutive
+// entries (a block of 4-byte FP16 feature pairs is one 32-byte L2 sector), so the 8 corners of a
+// cell fall into 3.4 blocks on average instead of 8 sectors.  Blocks are indexed densely while
+// a level's blocks fit the table, else by the spatial hash of Teschner et al. with the primes
+// used by instant-ngp, applied to the block coordinates.
+__host__ __device__ __forceinline__ uint32_t grid_index(uint32_t res, uint32_t x, uint32_t y, uint32_t z)
 {
-    uint64_t side = (uint64_t)res + 1;
-    if (side * side * side <= kTableSize)
-        return (uint32_t)(x + side * (y + side * z));
-    return (x * 1u ^ y * 2654435761u ^ z * 805459861u) & (kTableSize - 1u);
+    const uint32_t inner = (x & 1u) | ((y & 1u) << 1) | ((z & 1u) << 2);
+    const uint32_t bx = x >> 1, by = y >> 1, bz = z >> 1;
+    const uint64_t side = ((uint64_t)res + 2) >> 1; // blocks per axis over corners 0..res
+    uint32_t block;
+    if (side * side * side * 8 <= kTableSize)
+        block = (uint32_t)(bx + side * (by + side * bz));
+    else
+        block = (bx * 1u ^ by * 2654435761u ^ bz * 805459861u) & (kTableSize / 8u - 1u);
+    return block * 8u + inner;
 }
 
 struct Corner

@@ -66,19 +66,25 @@ def corners(pos, bmin, bmax, res, table_size):
         f0 = np.minimum(np.floor(p), np.float32(r - 1)).astype(np.float32)
         t = (p - f0).astype(np.float32)
         i0 = f0.astype(np.uint64)
-        side = r + 1
-        dense = side ** 3 <= table_size
+        # corners grouped in 2 x 2 x 2 blocks of 8 consecutive entries; blocks indexed densely while
+        # they fit, else hashed (32-bit products, as the device computes them)
+        side = (r + 2) >> 1
+        dense = side ** 3 * 8 <= table_size
         idx = np.empty((len(pos), 8), np.int64)
         w = np.empty((len(pos), 8), np.float64)
         for k in range(8):
             d = np.array([k & 1, (k >> 1) & 1, (k >> 2) & 1], np.uint64)
             c = i0 + d
+            inner = (c[:, 0] & 1) | ((c[:, 1] & 1) << 1) | ((c[:, 2] & 1) << 2)
+            b = c >> np.uint64(1)
             if dense:
-                idx[:, k] = (c[:, 0] + side * (c[:, 1] + side * c[:, 2])).astype(np.int64)
+                blk = b[:, 0] + np.uint64(side) * (b[:, 1] + np.uint64(side) * b[:, 2])
             else:
-                h = (c[:, 0] * np.uint64(PRIMES[0])) ^ (c[:, 1] * np.uint64(PRIMES[1])) ^ \
-                    (c[:, 2] * np.uint64(PRIMES[2]))
-                idx[:, k] = (h & np.uint64(table_size - 1)).astype(np.int64)
+                m32 = np.uint64(0xFFFFFFFF)
+                h = ((b[:, 0] * np.uint64(PRIMES[0])) & m32) ^ ((b[:, 1] * np.uint64(PRIMES[1])) & m32) ^ \
+                    ((b[:, 2] * np.uint64(PRIMES[2])) & m32)
+                blk = h & np.uint64(table_size // 8 - 1)
+            idx[:, k] = (blk * np.uint64(8) + inner).astype(np.int64)
             wk = np.ones(len(pos), np.float32)
             for a in range(3):
                 wk = (wk * np.where(d[a] == 1, t[:, a], np.float32(1) - t[:, a])).astype(np.float32)
@@ -127,15 +133,20 @@ class Network:
         self.bmin = np.asarray(bound[:3], np.float32)
         self.bmax = np.asarray(bound[3:], np.float32)
 
-    def encode(self, pos, wo, nrm):
+    def encode(self, pos, wo, nrm, half_grid=False):
         cs = corners(pos, self.bmin, self.bmax, self.res, self.table_size)
-        feats = [np.einsum("nk,nkf->nf", w, self.grid[l][idx]) for l, (idx, w) in enumerate(cs)]
+        grid = self.grid
+        if half_grid:
+            # the inference kernels read an FP16 copy of the table (round to nearest even)
+            grid = np.clip(grid, -65504.0, 65504.0).astype(np.float32).astype(np.float16).astype(np.float64)
+        feats = [np.einsum("nk,nkf->nf", w, grid[l][idx]) for l, (idx, w) in enumerate(cs)]
         x0 = np.concatenate(feats + [sh16(unit(wo)), sh16(unit(nrm))], axis=1)
         return x0, cs
 
-    def forward(self, pos, wo, nrm, bf=False):
-        """Raw outputs (n, 41) and the per-layer inputs X_l kept for the backward pass."""
-        x, cs = self.encode(pos, wo, nrm)
+    def forward(self, pos, wo, nrm, bf=False, half_grid=False):
+        """Raw outputs (n, 41) and the per-layer inputs X_l kept for the backward pass.
+        half_grid: the hash-grid features as the inference kernels read them (FP16)."""
+        x, cs = self.encode(pos, wo, nrm, half_grid)
         rnd = bf16 if bf else (lambda a: a)
         xs = []
         for l, W in enumerate(self.W):

@@ -177,7 +177,11 @@ def test_bsdf_eval_matches_oracle(ctx, oracle, name):
     of, op = oracle.bsdf_eval(m, wo, wi)
     assert np.isfinite(f).all() and np.isfinite(p).all()
     assert ((f > 0).any(-1) | (p >= 0)).all()
-    flushed = (np.abs(of).max(-1) < 1e-20) & ~f.any(-1)
+    # the fast-math shading unit flushes denormal results to zero: rows whose oracle value is
+    # nonzero but below 1e-20 and whose device value is exactly zero (exact zeros, e.g. wi below an
+    # opaque surface, are compared like every other row)
+    tiny = np.abs(of).max(-1)
+    flushed = (tiny > 0) & (tiny < 1e-20) & ~f.any(-1)
     assert flushed.mean() < 0.05
     keep = ~flushed
     checks = [(f, of, "f cos")]

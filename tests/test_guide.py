@@ -190,9 +190,9 @@ def test_guide_infer_matches_fp64(guide, n):
     pos, wo, nrm = random_inputs(rng, n)
     out = guide.infer(pos, wo, nrm)
     net = go.Network(w, grid, guide.level_res(), BOUND)
-    ref_bf, _, _ = net.forward(pos, wo, nrm, bf=True)
+    ref_bf, _, _ = net.forward(pos, wo, nrm, bf=True, half_grid=True)
     ref64, _, _ = net.forward(pos, wo, nrm, bf=False)
-    # same BF16 operands: only FP32 summation order differs
+    # same FP16 table entries and BF16 operands: only FP32 summation order differs
     assert rel(out, ref_bf) < 2e-3, rel(out, ref_bf)
     # against exact FP64 of the same FP32 weights: BF16 operand precision
     assert rel(out, ref64) < 3e-2, rel(out, ref64)

@@ -50,8 +50,11 @@ CASES = {
     # Same-seed parity at depth 3 (in, out and one more vertex: every path identical to the
     # oracle's up to the last bits); beyond that chains of refractions amplify the shading unit's
     # last-bit differences until paths part ways, so the full depth is checked by convergence.
+    # conv: overrides for the convergence test.  Unclamped, the caustics through the glass make
+    # rare, very bright paths whose count alone sets a 16-spp error; the reference's default
+    # indirect clamp (10) keeps the same estimator on both sides without them.
     "box_room_glass": dict(kind="box_room", W=48, H=48, spp=16, bounces=8, clamp_indirect=0.0, one_sided=(5, 6),
-                           same_seed_bounces=3,
+                           same_seed_bounces=3, conv=dict(clamp_indirect=10.0, spp=32),
                            materials={5: dict(specular_trans=1.0, roughness=0.15, ior=1.5),
                                       6: dict(specular_trans=1.0, roughness=0.4, ior=4.0, metallic=0.0)}),
     # diffuse transmission: cosine (fwd 0) and forward Henyey-Greenstein (fwd 0.7) lobes
@@ -230,11 +233,15 @@ def test_render_same_seed_matches_oracle(ctx, oracle, name):
 def test_render_convergence_matches_oracle(ctx, oracle, name):
     import keepsake_b200 as ks
     c = dict(CASES[name])
+    c.update(c.pop("conv", {}))
     g, cam, p = make_case(c)
     osc = oracle.scene(g.desc)
     p.spp = 16 * c["spp"]
     ref = composite(*osc.render(cam, p)[:2])
+    # the compared renders take another seed than the reference: neither shares its samples (a
+    # same-seed oracle render would, and so would the GPU's on cases whose paths stay equal)
     p.spp = c["spp"]
+    p.rng_seed = 1
     s = ks.Scene(ctx, g.desc)
     s.build_bvh()
     gpu = rel_mse(composite(*s.render(cam, p)), ref)

@@ -474,7 +474,9 @@ camera = {{ type = "perspective", to_world = {{ matrix_rm = {c2w} }}, vfov = 45.
     mats = [mat(metallic=0.1, specular=0.0), mat(basecolor=(0.3, 0.3, 0.3), bsdf=2, has_emission=1, specular=0.0),
             mat(bsdf=1)]
     mats[1].emission[:] = (17.0, 12.0, 4.0)
-    meshes = [(np.array([[-1, 0, -1], [1, 0, -1], [1, 0, 1], [-1, 0, 1]], np.float32), np.array([[0, 2, 1], [0, 3, 2]]), 0),
+    tc = np.array([[0, 0], [1, 0], [1, 1], [0, 1]], np.float32)
+    meshes = [(np.array([[-1, 0, -1], [1, 0, -1], [1, 0, 1], [-1, 0, 1]], np.float32), np.array([[0, 2, 1], [0, 3, 2]]), 0,
+               {"texcoords": tc}),
               (np.array([[-0.3, 1.5, -0.3], [0.3, 1.5, -0.3], [0.3, 1.5, 0.3], [-0.3, 1.5, 0.3]], np.float32),
                np.array([[0, 1, 2], [0, 2, 3]]), 1),
               (np.array([[-0.2, 0, 0], [0.2, 0, 0], [0, 0.5, 0.1]], np.float32), np.array([[0, 1, 2]]), 2)]
@@ -482,8 +484,6 @@ camera = {{ type = "perspective", to_world = {{ matrix_rm = {c2w} }}, vfov = 45.
     sky.kind = 1
     sky.ambient[:] = (0.1, 0.2, 0.3)
     desc, keep = ks.scene_desc(meshes, mats, sky)
-    tc = np.array([[0, 0], [1, 0], [1, 1], [0, 1]], np.float32)
-    desc.contents.meshes[0].texcoords = tc.ctypes.data
     B = ks.TextureBinding.make
     textures = [ks.load_texture(tmp_path / "albedo.png", 3, srgb=True), ks.load_texture(tmp_path / "rough.exr", 3),
                 ks.load_texture(tmp_path / "nrm.exr", 3)]
@@ -492,7 +492,7 @@ camera = {{ type = "perspective", to_world = {{ matrix_rm = {c2w} }}, vfov = 45.
              B(0, "normal_map", 2, filter=0, strength=0.7),
              B(2, "basecolor", 0, filter=0, flip_v=0, swizzle=(2, 1, 0, -1))]
     keep2 = ks.attach_textures(desc, textures, binds)
-    s = ks.Scene(ctx, desc, (keep, keep2, tc))
+    s = ks.Scene(ctx, desc, (keep, keep2))
     s.build_bvh()
     vfov = np.float32(45.0) / np.float32(180.0) * np.float32(np.pi)
     cam = ks.camera_perspective(np.array(c2w, np.float32), float(vfov), 1.5)
@@ -508,7 +508,7 @@ camera = {{ type = "perspective", to_world = {{ matrix_rm = {c2w} }}, vfov = 45.
 @pytest.mark.parametrize("field,status", [
     ('{ type = "texture", map = "texture.t", sampler = { type = "ewa" } }', 7),
     ('{ type = "texture", map = "texture.m", sampler = { type = "linear" } }', 7),
-    ('{ type = "texture", map = "texture.missing", sampler = { type = "nearest" } }', 2),
+    ('{ type = "texture", map = "texture.missing", sampler = { type = "nearest" } }', 8),
 ])
 def test_task_texture_field_errors(ctx, tmp_path, field, status):
     ks = _ks()

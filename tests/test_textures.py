@@ -152,17 +152,32 @@ def test_oracle_opacity_render(oracle):
 
 @pytest.mark.gpu
 def test_opacity_render_matches_oracle(ctx, oracle):
+    """Camera rays: the opacity test hashes the ray's origin and direction, which the camera
+    kernel computes bit for bit like the oracle, so every camera ray is decided the same way (equal
+    hit / miss weights; at depth 0 equal images).  Later rays start from directions the fast-math
+    shading unit computes to within a few ulps of the oracle's, so their hashes (and stochastic
+    decisions) differ: the full-depth image is compared by convergence to a 16x spp oracle image."""
     import keepsake_b200 as ks
     g, cam, p = opacity_case(ks)
     s = ks.Scene(ctx, g.desc)
     s.build_bvh()
-    acc, w = s.render(cam, p)
-    oacc, ow, ocnt = oracle.scene(g.desc).render(cam, p)
+    osc = oracle.scene(g.desc)
+    p0 = ks.SmallPTParams.make(render_width=p.render_width, render_height=p.render_height, spp=p.spp, bounces=0,
+                               clamp_indirect=0.0, include_background=0, backdrop=(0.0, 0.0, 0.0))
+    acc, w = s.render(cam, p0)
+    oacc, ow, _ = osc.render(cam, p0)
     assert np.array_equal(w, ow), "hit / miss weights differ: the opacity test decided a camera ray differently"
-    img, ref = composite(acc, w), composite(oacc, ow)
-    err = rel_mse(img, ref)
-    assert err < 2e-3, err
-    assert np.median(np.abs(img - ref) / (np.abs(ref) + 1e-3)) < 1e-4
+    assert rel_mse(composite(acc, w), composite(oacc, ow)) < 1e-6
+    acc, w = s.render(cam, p)
+    oacc, ow, ocnt = osc.render(cam, p)
+    assert np.array_equal(w, ow)
     st = s.stats()
-    assert abs(st.shadow_rays - int(ocnt[1])) <= 0.01 * ocnt[1] + 16
+    assert abs(st.extension_rays - int(ocnt[0])) <= 0.03 * ocnt[0] + 16
+    spp = p.spp
+    p.spp = 16 * spp
+    p.rng_seed = 3  # a reference that shares no samples with the compared renders
+    hi = composite(*osc.render(cam, p)[:2])
+    gpu = rel_mse(composite(acc, w), hi)
+    cpu = rel_mse(composite(oacc, ow), hi)
+    assert gpu <= 1.25 * cpu + 1e-6, (gpu, cpu)
     s.close()
