@@ -183,7 +183,7 @@ typedef struct ks_texture_desc {
 } ks_texture_desc;
 
 /* What a texture binding drives: a shader field of the material's BSDF (the constant value in
- * ks_material_desc is then ignored), the material's normal map or its opacity map. */
+ * ks_material_desc is then ignored), the material's normal map, its opacity map or its emission. */
 enum {
     KS_FIELD_BASECOLOR = 0, /* 3 channels; Lambertian: albedo */
     KS_FIELD_ROUGHNESS = 1,
@@ -195,14 +195,18 @@ enum {
     KS_FIELD_DIFFUSE_TRANS_FWD = 7,
     KS_FIELD_SPECULAR = 8,   /* PrincipledBRDF's specular */
     KS_FIELD_NORMAL_MAP = 9, /* Material::normal_map (material.h:41) */
-    KS_FIELD_OPACITY_MAP = 10 /* Material::opacity_map (material.h:42): stochastic any-hit test */
+    KS_FIELD_OPACITY_MAP = 10, /* Material::opacity_map (material.h:42): stochastic any-hit test */
+    KS_FIELD_EMISSION = 11     /* Material::emission of an emitter (has_emission = 1; 3 channels, in place
+                                  of ks_material_desc.emission): its triangles' light-selection power
+                                  comes from a summed-area table of the texture's luminance
+                                  (compute_mesh_light_importance, light.cpp:307-522) */
 };
 
 /* A texture bound to a material: the TextureField's lookup (flip_v, uv_scale, uv_offset, the
- * sampler, swizzle, scale) and, for normal maps, NormalMap's parameters.  Zero-initialise, then set:
- * the defaults of create_texture_shader_field_color / create_texture_sampler /
- * create_normal_map are flip_v 1, uv_scale (1, 1), swizzle (0, 1, 2, 3), scale (1, 1, 1, 1),
- * filter nearest... as listed per field. */
+ * sampler, swizzle, scale) and, for normal maps, NormalMap's parameters.  Zero-initialise, then set
+ * every field: the reference's defaults (create_texture_shader_field_color, create_texture_sampler,
+ * create_normal_map) are flip_v 1, uv_scale (1, 1), uv_offset (0, 0), swizzle (0, 1, 2, 3),
+ * scale (1, 1, 1, 1), repeat wrapping, tangent space, range01 1, strength 1, to_world identity. */
 typedef struct ks_texture_binding {
     uint32_t material;   /* index into ks_scene_desc.materials */
     int32_t field;       /* KS_FIELD_* */

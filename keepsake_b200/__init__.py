@@ -185,7 +185,7 @@ class TextureDesc(ctypes.Structure):
 
 
 FIELDS = {"basecolor": 0, "roughness": 1, "metallic": 2, "ior": 3, "specular_r0_mul": 4, "specular_trans": 5,
-          "diffuse_trans": 6, "diffuse_trans_fwd": 7, "specular": 8, "normal_map": 9, "opacity_map": 10}
+          "diffuse_trans": 6, "diffuse_trans_fwd": 7, "specular": 8, "normal_map": 9, "opacity_map": 10, "emission": 11}
 
 
 class TextureBinding(ctypes.Structure):

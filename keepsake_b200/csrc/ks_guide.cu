@@ -201,6 +201,12 @@ __device__ __forceinline__ float2 ld_grid(const __half2 *ptr, uint64_t pol)
     return __half22float2(h);
 }
 
+// Levels whose corner gathers are in flight together (2: within the inference kernel's 128-register
+// budget at 4 CTAs per SM; 4 spills).
+#ifndef KS_GUIDE_GATHER_GROUP
+#define KS_GUIDE_GATHER_GROUP 2
+#endif
+
 // Table: float2 (the FP32 master table: training) or __half2 (its FP16 copy: inference).
 template <class Entry>
 __device__ __forceinline__ void encode_row(const GridParams &gp, const Entry *grid, bool valid, f3 pn, f3 wo,
@@ -208,21 +214,38 @@ __device__ __forceinline__ void encode_row(const GridParams &gp, const Entry *gr
 {
     const uint64_t pol = l2_keep_policy();
     const uint32_t tid = threadIdx.x;
-    for (int l = 0; l < kLevels; ++l) {
-        float f0 = 0.0f, f1 = 0.0f;
-        if (valid) {
-            Corner c;
-            level_corners(gp, l, pn, c);
-            const Entry *tab = grid + (size_t)l * kTableSize;
+    // kGroup levels at a time: all their corner loads are issued before any is consumed, so a
+    // thread waits for kLevels / kGroup round trips to L2 instead of kLevels
+    constexpr int kGroup = KS_GUIDE_GATHER_GROUP;
+    for (int l0 = 0; l0 < kLevels; l0 += kGroup) {
+        float f0[kGroup], f1[kGroup];
 #pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                float2 e = ld_grid(&tab[c.idx[k]], pol);
-                f0 += c.w[k] * e.x;
-                f1 += c.w[k] * e.y;
+        for (int g = 0; g < kGroup; ++g)
+            f0[g] = f1[g] = 0.0f;
+        if (valid) {
+            Corner c[kGroup];
+            float2 e[kGroup][8];
+#pragma unroll
+            for (int g = 0; g < kGroup; ++g) {
+                level_corners(gp, l0 + g, pn, c[g]);
+                const Entry *tab = grid + (size_t)(l0 + g) * kTableSize;
+#pragma unroll
+                for (int k = 0; k < 8; ++k)
+                    e[g][k] = ld_grid(&tab[c[g].idx[k]], pol);
             }
+#pragma unroll
+            for (int g = 0; g < kGroup; ++g)
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    f0[g] += c[g].w[k] * e[g][k].x;
+                    f1[g] += c[g].w[k] * e[g][k].y;
+                }
         }
-        store_bf16(x0, xt_off(2 * l, tid), f0);
-        store_bf16(x0, xt_off(2 * l + 1, tid), f1);
+#pragma unroll
+        for (int g = 0; g < kGroup; ++g) {
+            store_bf16(x0, xt_off(2 * (l0 + g), tid), f0[g]);
+            store_bf16(x0, xt_off(2 * (l0 + g) + 1, tid), f1[g]);
+        }
     }
     float sh[kShCoeffs];
     sh16(wo, sh);

@@ -9,12 +9,14 @@
 //     The mean is a double sum (rows in order) - the reference uses an unordered float atomic.
 //   SkyLight::power (light.cpp:136-159): float row sums in column order (one thread per row),
 //     rows added in order in double.
-//   compute_mesh_light_importance (light.cpp:307-414), uniform emission branch, and the
+//   compute_mesh_light_importance (light.cpp:307-522): the uniform branch for constant emission,
+//     the summed-area-table branch for emission / opacity textures (mesh_uv_importance), and the
 //     zero-importance compaction of MeshLightShared (light.cpp:524-560).
 //   PowerLightSampler::build (light.cpp:636-672).
 #include "ks_lights.cuh"
 #include "ks_scene.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -219,6 +221,198 @@ bool invert4(const float *m, float *out)
         for (int c = 0; c < 4; ++c)
             out[4 * r + c] = (float)a[r][c + 4];
     return true;
+}
+
+// SummedAreaTable (sat.h): double prefix sums of float values, looked up bilinearly over the
+// (nx + 1) x (ny + 1) grid of corners with clamping and boundary ticks (lerp_helper,
+// maths.h:760-788); a box's sum from its four corners, never below zero.
+struct SatTable
+{
+    int nx = 0, ny = 0;
+    std::vector<double> table;
+    SatTable(const std::vector<float> &v, int nx_, int ny_) : nx(nx_), ny(ny_), table(v.size())
+    {
+        table[0] = v[0];
+        for (int x = 1; x < nx; ++x)
+            table[x] = v[x] + table[x - 1];
+        for (int y = 1; y < ny; ++y)
+            table[(size_t)y * nx] = v[(size_t)y * nx] + table[(size_t)(y - 1) * nx];
+        for (int y = 1; y < ny; ++y)
+            for (int x = 1; x < nx; ++x)
+                table[(size_t)y * nx + x] = (v[(size_t)y * nx + x] + table[(size_t)y * nx + (x - 1)] +
+                                             table[(size_t)(y - 1) * nx + x] - table[(size_t)(y - 1) * nx + (x - 1)]);
+    }
+    double fetch(int x, int y) const
+    {
+        if (x == 0 || y == 0)
+            return 0;
+        x = std::min(x - 1, nx - 1);
+        y = std::min(y - 1, ny - 1);
+        return table[(size_t)y * nx + x];
+    }
+    static void lerp(float u, int res, int &u0, int &u1, float &t)
+    {
+        const float us = u * (float)(res - 1);
+        u0 = (int)std::floor(us);
+        u1 = u0 + 1;
+        t = us - (float)u0;
+        u0 = std::clamp(u0, 0, res - 1);
+        u1 = std::clamp(u1, 0, res - 1);
+    }
+    double lookup(float px, float py) const
+    {
+        int x0, x1, y0, y1;
+        float wx, wy;
+        lerp(px, nx + 1, x0, x1, wx);
+        lerp(py, ny + 1, y0, y1, wy);
+        return fetch(x0, y0) * (1.0 - wx) * (1.0 - wy) + fetch(x1, y0) * (wx) * (1.0 - wy) +
+               fetch(x0, y1) * (1.0 - wx) * (wy) + fetch(x1, y1) * (wx) * (wy);
+    }
+    float sum(float x0, float y0, float x1, float y1) const
+    {
+        const double v = (lookup(x1, y1) - lookup(x0, y1)) + (lookup(x0, y0) - lookup(x1, y0));
+        return std::max((float)v, 0.0f);
+    }
+};
+
+// mod (maths.h:133-138) for floats
+float fmod_pos(float a, float b)
+{
+    const float r = a - std::floor(a / b) * b;
+    return r < 0 ? r + b : r;
+}
+
+float luminance3(float r, float g, float b) { return 0.212671f * r + 0.715160f * g + 0.072169f * b; }
+
+// compute_mesh_light_importance (light.cpp:307-522), per triangle of one emissive mesh: the factor
+// that multiplies 2 pi x the triangle's area.  A constant emission (and no opacity texture) is the
+// uniform branch: the luminance of the emission.  With an emission or opacity texture, the
+// luminance of the emission (times the opacity) at the texel centres of the larger texture goes
+// into a summed-area table, and each triangle takes the table's mean over the bounding box of its
+// texture coordinates (after flip_v, uv_scale, uv_offset), tile by tile with the texture's
+// wrapping; textures whose lookups disagree in those settings fall back to the mean over the grid.
+void mesh_uv_importance(const ks_scene *s, const MaterialGPU &mat, uint32_t first, uint32_t n,
+                        const std::vector<float> &h_verts, const std::vector<uint32_t> &h_idx, std::vector<float> &out)
+{
+    out.assign(n, 0.0f);
+    const ks_scene::EmissionTextures &et = s->emit_tex;
+    const BindingGPU *em = nullptr, *op = nullptr;
+    if (s->any_emission_map || s->any_opacity)
+        for (int k = 0; k < mat.bind_count && !et.binds.empty(); ++k) {
+            const BindingGPU &b = et.binds[mat.bind_begin + k];
+            if (b.field == KS_FIELD_EMISSION)
+                em = &b;
+            else if (b.field == KS_FIELD_OPACITY_MAP)
+                op = &b;
+        }
+    if (!em && !op) {
+        const float avg = luminance3(mat.emission[0], mat.emission[1], mat.emission[2]);
+        for (uint32_t k = 0; k < n; ++k)
+            out[k] = avg;
+        return;
+    }
+    bool fallback = false;
+    int rx = 1, ry = 1;
+    const BindingGPU *first_b = em ? em : op;
+    if (em) {
+        rx = et.info[em->tex].w;
+        ry = et.info[em->tex].h;
+    }
+    if (op) {
+        rx = std::max(rx, et.info[op->tex].w);
+        ry = std::max(ry, et.info[op->tex].h);
+        if (em && (em->wrap_u != op->wrap_u || em->wrap_v != op->wrap_v || em->flip_v != op->flip_v ||
+                   em->uv_scale[0] != op->uv_scale[0] || em->uv_scale[1] != op->uv_scale[1] ||
+                   em->uv_offset[0] != op->uv_offset[0] || em->uv_offset[1] != op->uv_offset[1]))
+            fallback = true;
+    }
+    std::vector<float> imp((size_t)rx * ry);
+    double sum = 0.0;
+    for (int y = 0; y < ry; ++y)
+        for (int x = 0; x < rx; ++x) {
+            const float u = (x + 0.5f) / (float)rx, v = (y + 0.5f) / (float)ry;
+            float e;
+            if (em) {
+                const float4 c = field_eval(et.texels.data(), et.info.data(), *em, u, v);
+                e = luminance3(c.x, c.y, c.z);
+            } else {
+                e = luminance3(mat.emission[0], mat.emission[1], mat.emission[2]);
+            }
+            if (op)
+                e *= field_eval(et.texels.data(), et.info.data(), *op, u, v).x;
+            imp[(size_t)y * rx + x] = e;
+            sum += e;
+        }
+    if (fallback) {
+        // the mean over the grid (the reference sums it with an unordered float atomic)
+        const float avg = (float)(sum / (double)imp.size());
+        for (uint32_t k = 0; k < n; ++k)
+            out[k] = avg;
+        return;
+    }
+    const SatTable sat(imp, rx, ry);
+    constexpr float kBeforeOne = 0x1.fffffep-1f; // fp32_before_one
+    for (uint32_t k = 0; k < n; ++k) {
+        float tc[3][2];
+        for (int c = 0; c < 3; ++c) {
+            const uint32_t vi = h_idx[3 * (size_t)(first + k) + c];
+            tc[c][0] = et.texcoords.empty() ? 0.0f : et.texcoords[2 * (size_t)vi];
+            tc[c][1] = et.texcoords.empty() ? 0.0f : et.texcoords[2 * (size_t)vi + 1];
+            if (first_b->flip_v)
+                tc[c][1] = 1.0f - tc[c][1];
+            tc[c][0] = tc[c][0] * first_b->uv_scale[0] + first_b->uv_offset[0];
+            tc[c][1] = tc[c][1] * first_b->uv_scale[1] + first_b->uv_offset[1];
+        }
+        float bmin[2] = {INFINITY, INFINITY}, bmax[2] = {-INFINITY, -INFINITY};
+        for (int c = 0; c < 3; ++c)
+            for (int a = 0; a < 2; ++a) {
+                bmin[a] = std::min(bmin[a], tc[c][a]);
+                bmax[a] = std::max(bmax[a], tc[c][a]);
+            }
+        const int txmin = (int)std::floor(bmin[0]), txmax = (int)std::ceil(bmax[0]);
+        const int tymin = (int)std::floor(bmin[1]), tymax = (int)std::ceil(bmax[1]);
+        float acc = 0.0f, sum_area = 0.0f;
+        for (int ty = tymin; ty < tymax; ++ty)
+            for (int tx = txmin; tx < txmax; ++tx) {
+                // the box within this tile (an empty intersection has zero extents)
+                float lo[2] = {std::max(bmin[0], (float)tx), std::max(bmin[1], (float)ty)};
+                float hi[2] = {std::min(bmax[0], tx + kBeforeOne), std::min(bmax[1], ty + kBeforeOne)};
+                if (lo[0] > hi[0] || lo[1] > hi[1])
+                    continue;
+                const float b_area = (hi[0] - lo[0]) * (hi[1] - lo[1]);
+                if (b_area == 0.0f)
+                    continue;
+                const int wrap[2] = {first_b->wrap_u, first_b->wrap_v};
+                for (int a = 0; a < 2; ++a) {
+                    if (wrap[a] == 0) {
+                        lo[a] = fmod_pos(lo[a], 1.0f);
+                        hi[a] = fmod_pos(hi[a], 1.0f);
+                    } else {
+                        lo[a] = std::clamp(lo[a], 0.0f, 1.0f);
+                        hi[a] = std::clamp(hi[a], 0.0f, 1.0f);
+                    }
+                }
+                const int res[2] = {rx, ry};
+                for (int a = 0; a < 2; ++a) {
+                    if (lo[a] == 0.0f && hi[a] == 0.0f)
+                        hi[a] = 1.0f / (res[a] + 1);
+                    if (lo[a] == 1.0f && hi[a] == 1.0f)
+                        lo[a] = 1.0f - 1.0f / (res[a] + 1);
+                }
+                const float ex = lo[0] > hi[0] || lo[1] > hi[1] ? 0.0f : hi[0] - lo[0];
+                const float ey = lo[0] > hi[0] || lo[1] > hi[1] ? 0.0f : hi[1] - lo[1];
+                // (the reference asserts a non-empty wrapped box: tx + fp32_before_one rounds up to
+                // tx + 1 for tiles at |tx| >= 1, which wraps to an empty box; such a tile is skipped)
+                if (ex * ey == 0.0f)
+                    continue;
+                const float mean = sat.sum(lo[0], lo[1], hi[0], hi[1]) / ((ex * (float)rx) * (ey * (float)ry));
+                acc += mean * b_area;
+                sum_area += b_area;
+            }
+        if (sum_area > 0.0f)
+            acc /= sum_area;
+        out[k] = acc;
+    }
 }
 
 } // namespace
@@ -533,6 +727,7 @@ ks_status build_lights(ks_scene *s)
         const bool instanced = s->n_instances > 0;
         std::vector<std::vector<uint32_t>> proto_tris(s->n_protos);
         std::vector<std::vector<float4>> proto_em(s->n_protos);
+        std::vector<std::vector<float>> proto_uvw(s->n_protos);
         std::vector<int> mesh_proto(s->host.mesh_material.size(), -1);
         if (instanced)
             for (uint32_t q = 0; q < s->n_protos; ++q)
@@ -547,9 +742,24 @@ ks_status build_lights(ks_scene *s)
                 continue;
             if (instanced && mesh_proto[m] < 0)
                 continue;
-            float avg_importance = 0.212671f * mat.emission[0] + 0.715160f * mat.emission[1] +
-                                   0.072169f * mat.emission[2];
             uint32_t first = s->host.mesh_tri_offset[m], n = s->host.mesh_tri_offset[m + 1] - first;
+            // the per-triangle factor of 2 pi x area: the emission's luminance, or its texture's mean
+            const MaterialGPU &mg = s->any_emission_map ? s->emit_tex.mats[s->host.mesh_material[m]] : MaterialGPU{};
+            std::vector<float> uvw;
+            if (s->any_emission_map) {
+                mesh_uv_importance(s, mg, first, n, h_verts, h_idx, uvw);
+            } else {
+                uvw.assign(n, 0.212671f * mat.emission[0] + 0.715160f * mat.emission[1] + 0.072169f * mat.emission[2]);
+            }
+            // the emission binding of a textured emitter (index into the scene's bindings), else -1
+            int em_bind = -1;
+            if (s->any_emission_map)
+                for (int b = 0; b < mg.bind_count; ++b)
+                    if (s->emit_tex.binds[mg.bind_begin + b].field == KS_FIELD_EMISSION)
+                        em_bind = mg.bind_begin + b;
+            float em_bits;
+            std::memcpy(&em_bits, &em_bind, 4);
+            const float4 em4 = make_float4(mat.emission[0], mat.emission[1], mat.emission[2], em_bits);
             std::vector<float> importance(n), areas(n);
             std::vector<uint32_t> prim_ids(n);
             for (uint32_t k = 0; k < n; ++k) {
@@ -562,7 +772,7 @@ ks_status build_lights(ks_scene *s)
                 float c[3] = {e01[1] * e12[2] - e01[2] * e12[1], e01[2] * e12[0] - e01[0] * e12[2],
                               e01[0] * e12[1] - e01[1] * e12[0]};
                 float area = 0.5f * std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
-                importance[k] = 6.28318530718f * area * avg_importance;
+                importance[k] = 6.28318530718f * area * uvw[k];
                 areas[k] = area;
                 prim_ids[k] = k;
             }
@@ -582,13 +792,14 @@ ks_status build_lights(ks_scene *s)
                     int q = mesh_proto[m];
                     tri_light[first + prim_ids[k]] = (int32_t)proto_tris[q].size(); // rank in the prototype
                     proto_tris[q].push_back(first + prim_ids[k]);
-                    proto_em[q].push_back(make_float4(mat.emission[0], mat.emission[1], mat.emission[2], 0.0f));
+                    proto_em[q].push_back(em4);
+                    proto_uvw[q].push_back(uvw[prim_ids[k]]);
                     continue;
                 }
                 ml_tri.push_back(first + prim_ids[k]);
                 ml_area.push_back(areas[k]);
                 ml_importance.push_back(importance[k]);
-                ml_em.push_back(make_float4(mat.emission[0], mat.emission[1], mat.emission[2], 0.0f));
+                ml_em.push_back(em4);
                 float v0[3], v1[3], v2[3];
                 vert(h_idx[3 * (first + prim_ids[k])], v0);
                 vert(h_idx[3 * (first + prim_ids[k]) + 1], v1);
@@ -615,10 +826,9 @@ ks_status build_lights(ks_scene *s)
                     f3 c = cross(e01, e12);
                     float area = 0.5f * std::sqrt(c.x * c.x + c.y * c.y + c.z * c.z);
                     float4 em = proto_em[q][r];
-                    float avg = 0.212671f * em.x + 0.715160f * em.y + 0.072169f * em.z;
                     ml_tri.push_back(t);
                     ml_area.push_back(area);
-                    ml_importance.push_back(6.28318530718f * area * avg);
+                    ml_importance.push_back(6.28318530718f * area * proto_uvw[q][r]);
                     ml_em.push_back(em);
                     for (int c2 = 0; c2 < 3; ++c2)
                         ml_verts.push_back(make_float4(w[c2].x, w[c2].y, w[c2].z, 0.0f));

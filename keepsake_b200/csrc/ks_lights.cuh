@@ -456,6 +456,31 @@ struct TriVerts
     f3 v0, v1, v2;
 };
 
+// MeshTriLight::eval (light.cpp:560-565): the emission of mesh light k at barycentrics (u, v) of its
+// triangle; a constant, or the emission texture (ml_emission.w holds its binding, -1 for none) at
+// the texture coordinate there: the mesh's texcoords interpolated, else the barycentrics for a hit
+// (compute_intersection) and zero for a light sample (interpolate_texcoord, geometry.cpp:182-191).
+KS_D f3 mesh_light_Le(const SceneView &s, uint32_t k, float u, float v, bool bary_fallback)
+{
+    const float4 e = __ldg(&s.ml_emission[k]);
+    const int b = __float_as_int(e.w);
+    if (b < 0)
+        return mk(e.x, e.y, e.z);
+    const uint32_t tri = __ldg(&s.ml_tri[k]);
+    float tu = bary_fallback ? u : 0.0f, tv = bary_fallback ? v : 0.0f;
+    if (__ldg(&s.mesh_flags[__ldg(&s.tri_mesh[tri])]) & kMeshTexcoords) {
+        const float2 *tc = reinterpret_cast<const float2 *>(s.texcoords);
+        const uint32_t i0 = __ldg(&s.indices[3 * (size_t)tri]), i1 = __ldg(&s.indices[3 * (size_t)tri + 1]),
+                       i2 = __ldg(&s.indices[3 * (size_t)tri + 2]);
+        const float2 t0 = __ldg(&tc[i0]), t1 = __ldg(&tc[i1]), t2 = __ldg(&tc[i2]);
+        const float w = 1.0f - u - v;
+        tu = w * t0.x + u * t1.x + v * t2.x;
+        tv = w * t0.y + u * t1.y + v * t2.y;
+    }
+    const float4 c = field_eval(s.tex_texels, s.tex_info, s.bindings[b], tu, tv);
+    return mk(c.x, c.y, c.z);
+}
+
 KS_D f3 mesh_light_sample(const SceneView &s, uint32_t k, const TriVerts &tv, f3 p_shade, float u0, float u1,
                           f3 &wi, float &wi_dist, float &pdf)
 {
@@ -489,8 +514,7 @@ KS_D f3 mesh_light_sample(const SceneView &s, uint32_t k, const TriVerts &tv, f3
     pdf *= (d2 / absdot);
     wi_dist = wi_dist - 1e-4f;
     wi_dist = wi_dist < 0.0f ? 0.0f : wi_dist;
-    float4 e = __ldg(&s.ml_emission[k]);
-    return mk(e.x, e.y, e.z) / pdf;
+    return mesh_light_Le(s, k, b0, b1, false) / pdf;
 }
 
 KS_D float mesh_light_pdf(const SceneView &s, uint32_t k, const TriVerts &tv, f3 wi, float wi_dist)

@@ -244,7 +244,8 @@ bool convert_texture(const ks_texture_desc &t, std::vector<float4> &out)
 // A binding's device form; false for an index or enum out of range or a non-finite value.
 bool binding_to_gpu(const ks_texture_binding &b, const ks_scene_desc &d, BindingGPU &g)
 {
-    if (b.material >= d.n_materials || b.texture >= d.n_textures || b.field < 0 || b.field > KS_FIELD_OPACITY_MAP ||
+    if (b.material >= d.n_materials || b.texture >= d.n_textures || b.field < 0 || b.field > KS_FIELD_EMISSION ||
+        (b.field == KS_FIELD_EMISSION && !d.materials[b.material].has_emission) ||
         b.filter < 0 || b.filter > 2 || b.cubic_kernel < 0 || b.cubic_kernel > 2 || b.wrap_u < 0 || b.wrap_u > 1 ||
         b.wrap_v < 0 || b.wrap_v > 1 || b.normal_space < 0 || b.normal_space > 1)
         return false;
@@ -564,11 +565,21 @@ ks_status ks_scene_create(ks_context *ctx, const ks_scene_desc *desc, ks_scene *
                     mats[m].tex_flags |= kMatNormalMap;
                 else if (g.field == KS_FIELD_OPACITY_MAP)
                     mats[m].tex_flags |= kMatOpacityMap;
+                else if (g.field == KS_FIELD_EMISSION)
+                    mats[m].tex_flags |= kMatEmissionMap;
             }
         mats[m].bind_count = (int)binds.size() - mats[m].bind_begin;
         s->any_opacity |= (mats[m].tex_flags & kMatOpacityMap) != 0;
+        s->any_emission_map |= (mats[m].tex_flags & kMatEmissionMap) != 0;
     }
     s->any_bindings = !binds.empty();
+    if (s->any_emission_map) {
+        s->emit_tex.texels = texels;
+        s->emit_tex.info = tex_info;
+        s->emit_tex.binds = binds;
+        s->emit_tex.mats = mats;
+        s->emit_tex.texcoords = texcoords;
+    }
     cudaError_t e = s->materials.alloc(mats.size());
     if (e == cudaSuccess)
         e = s->mesh_material.alloc(s->host.mesh_material.size());

@@ -70,7 +70,8 @@ struct MaterialGPU
 enum : int
 {
     kMatNormalMap = 1,
-    kMatOpacityMap = 2
+    kMatOpacityMap = 2,
+    kMatEmissionMap = 4
 };
 
 struct SceneHost
@@ -122,6 +123,17 @@ struct ks_scene
     ksb::DevBuf<ksb::TexInfo> tex_info;
     ksb::DevBuf<ksb::BindingGPU> bindings;
     bool any_bindings = false, any_opacity = false;
+    // host copies for the light build of textured emitters (filled only when some emitter has an
+    // emission texture): converted texels, texture sizes, bindings, materials, texcoords
+    struct EmissionTextures
+    {
+        std::vector<float4> texels;
+        std::vector<ksb::TexInfo> info;
+        std::vector<ksb::BindingGPU> binds;
+        std::vector<ksb::MaterialGPU> mats;
+        std::vector<float> texcoords; // 2 per global vertex (zeros for meshes without)
+    } emit_tex;
+    bool any_emission_map = false;
     // per-vertex shading attributes, indexed like verts (allocated only when some mesh has them)
     ksb::DevBuf<float> normals;   // 3 per vertex: MeshData::vertex_normals of smooth-shaded meshes
     ksb::DevBuf<float> texcoords; // 2 per vertex: MeshData::texcoords

@@ -65,8 +65,8 @@ KS_BIG MaterialGPU textured_material(const SceneView &sv, const MaterialGPU &mat
     hit_uv(sv, tri, flags, u, v, tu, tv);
     for (int k = 0; k < mat.bind_count; ++k) {
         const BindingGPU &b = sv.bindings[mat.bind_begin + k];
-        if (b.field == KS_FIELD_OPACITY_MAP)
-            continue; // applied by the traversal
+        if (b.field == KS_FIELD_OPACITY_MAP || b.field == KS_FIELD_EMISSION)
+            continue; // applied by the traversal / the emitter's light (mesh_light_Le)
         if (b.field == KS_FIELD_NORMAL_MAP) {
             apply_normal_map(sv, b, tu, tv, it);
             continue;
@@ -324,8 +324,14 @@ __global__ void __launch_bounds__(128, KS_SHADE_MIN_BLOCKS) k_shade(const __grid
                         light += __ldg(&sv.inst_light_base[inst]); // rank within the prototype
                     if (light >= 0) {
                         uint32_t k = (uint32_t)light - sv.n_nonmesh;
-                        float4 e = __ldg(&sv.ml_emission[k]);
-                        f3 Le = mk(e.x, e.y, e.z);
+                        // textured emitters have bindings, so only the general variant meets them
+                        f3 Le;
+                        if constexpr (kVariant == kShadeGeneral) {
+                            Le = mesh_light_Le(sv, k, h.y, h.z, true);
+                        } else {
+                            const float4 e = __ldg(&sv.ml_emission[k]);
+                            Le = mk(e.x, e.y, e.z);
+                        }
                         if (bounce == 0) {
                             L += beta * Le;
                         } else {

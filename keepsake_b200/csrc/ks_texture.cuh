@@ -5,7 +5,8 @@
 // lookup reads the values the reference's fetch returns.  A binding is one TextureField
 // (shader_field.h:38-86): flip_v, uv_scale / uv_offset, a sampler (texture.cpp:520-677: nearest,
 // bilinear or bicubic at level 0, repeat or clamp per axis), swizzle and scale; the textures have one
-// level, so the samplers' level selection (texture.cpp:587-627) always picks level 0.
+// level, so the samplers' level selection (texture.cpp:587-627) always picks level 0.  The lookups
+// run on the device (shading) and on the host (the importance of textured emitters).
 #pragma once
 #include "ks_math.cuh"
 
@@ -39,15 +40,19 @@ KS_HD int tex_wrap(int x, int dim, int clamp)
     return r < 0 ? r + dim : r;
 }
 
-KS_D float4 texel(const float4 *texels, const TexInfo &t, int x, int y)
+KS_HD float4 texel(const float4 *texels, const TexInfo &t, int x, int y)
 {
+#ifdef __CUDA_ARCH__
     return __ldg(&texels[t.offset + (size_t)y * t.w + x]);
+#else
+    return texels[t.offset + (size_t)y * t.w + x];
+#endif
 }
 
-KS_D float4 f4_axpy(float a, float4 x, float4 y) { return make_float4(a * x.x + y.x, a * x.y + y.y, a * x.z + y.z, a * x.w + y.w); }
+KS_HD float4 f4_axpy(float a, float4 x, float4 y) { return make_float4(a * x.x + y.x, a * x.y + y.y, a * x.z + y.z, a * x.w + y.w); }
 
 // TextureSampler::bilinear (texture.cpp:541-573) at level 0
-KS_D float4 tex_bilinear(const float4 *texels, const TexInfo &t, const BindingGPU &b, float ux, float uy)
+KS_HD float4 tex_bilinear(const float4 *texels, const TexInfo &t, const BindingGPU &b, float ux, float uy)
 {
     float u = ux * t.w - 0.5f, v = uy * t.h - 0.5f;
     int u0 = (int)floorf(u), v0 = (int)floorf(v);
@@ -63,16 +68,16 @@ KS_D float4 tex_bilinear(const float4 *texels, const TexInfo &t, const BindingGP
 }
 
 // NearestSampler (texture.cpp:575-585)
-KS_D float4 tex_nearest(const float4 *texels, const TexInfo &t, const BindingGPU &b, float ux, float uy)
+KS_HD float4 tex_nearest(const float4 *texels, const TexInfo &t, const BindingGPU &b, float ux, float uy)
 {
     int u0 = (int)floorf(ux * t.w - 0.5f), v0 = (int)floorf(uy * t.h - 0.5f);
     return texel(texels, t, tex_wrap(u0, t.w, b.wrap_u), tex_wrap(v0, t.h, b.wrap_v));
 }
 
 // spline / CubicSampler::bicubic (texture.cpp:629-677) at level 0
-KS_D float cubic_weight(const float c[4], float x) { return c[0] * (x * x * x) + c[1] * (x * x) + c[2] * x + c[3]; }
+KS_HD float cubic_weight(const float c[4], float x) { return c[0] * (x * x * x) + c[1] * (x * x) + c[2] * x + c[3]; }
 
-KS_D float4 tex_bicubic(const float4 *texels, const TexInfo &t, const BindingGPU &b, float ux, float uy)
+KS_HD float4 tex_bicubic(const float4 *texels, const TexInfo &t, const BindingGPU &b, float ux, float uy)
 {
     float u = ux * t.w - 0.5f, v = uy * t.h - 0.5f;
     int u0 = (int)floorf(u), v0 = (int)floorf(v);
@@ -93,7 +98,7 @@ KS_D float4 tex_bicubic(const float4 *texels, const TexInfo &t, const BindingGPU
 }
 
 // TextureField::operator() (shader_field.h:61-80): the field's value (4 channels, unused ones 0)
-KS_D float4 field_eval(const float4 *texels, const TexInfo *infos, const BindingGPU &b, float u, float v)
+KS_HD float4 field_eval(const float4 *texels, const TexInfo *infos, const BindingGPU &b, float u, float v)
 {
     float fu = u, fv = b.flip_v ? 1.0f - v : v;
     fu = fu * b.uv_scale[0] + b.uv_offset[0];

@@ -291,10 +291,14 @@ KS_D ShadeFrame hit_frame(const SceneView &sv, uint32_t tri, int flags, f3 p0, f
 // The hit's texture coordinates: the mesh's interpolated texcoords (rtcInterpolate0 of the
 // texcoord buffer, geometry.cpp:92-99; MeshGeometry::compute_hit_texcoord), else the barycentrics
 // (u, v) of vertices 1 and 2.
-KS_D void hit_uv(const SceneView &sv, uint32_t tri, int flags, float u, float v, float &tu, float &tv)
+// Texture coordinate of a hit: the mesh's texcoords interpolated, else the hit's barycentrics
+// (compute_intersection, geometry.cpp:78-101) or, for the opacity test and light samples, zero
+// (compute_hit_texcoord / interpolate_texcoord, geometry.cpp:165-191).
+KS_D void hit_uv(const SceneView &sv, uint32_t tri, int flags, float u, float v, float &tu, float &tv,
+                 bool bary_fallback = true)
 {
-    tu = u;
-    tv = v;
+    tu = bary_fallback ? u : 0.0f;
+    tv = bary_fallback ? v : 0.0f;
     if (flags & kMeshTexcoords) {
         const float2 *tc = reinterpret_cast<const float2 *>(sv.texcoords);
         const uint32_t i0 = __ldg(&sv.indices[3 * (size_t)tri]), i1 = __ldg(&sv.indices[3 * (size_t)tri + 1]),
@@ -345,7 +349,7 @@ struct SceneAlpha
         while (sv->bindings[mat.bind_begin + k].field != KS_FIELD_OPACITY_MAP)
             ++k;
         float tu, tv;
-        hit_uv(*sv, tri, __ldg(&sv->mesh_flags[mesh]), u, v, tu, tv);
+        hit_uv(*sv, tri, __ldg(&sv->mesh_flags[mesh]), u, v, tu, tv, false);
         const float opacity = saturate(field_eval(sv->tex_texels, sv->tex_info, sv->bindings[mat.bind_begin + k], tu,
                                                   tv).x);
         if (opacity <= 0.0f)

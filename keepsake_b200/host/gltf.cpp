@@ -692,9 +692,9 @@ ks_texture_binding texture_binding(TextureSet &ts, const Json &info, uint32_t ma
 // Textures (with TextureSet): baseColorTexture x baseColorFactor, metallicRoughnessTexture's G x
 // roughnessFactor and B x metallicFactor, specularTexture x the specular factor,
 // transmissionTexture x transmissionFactor, normalTexture as a tangent-space normal map of strength
-// normalTexture.scale, and for alpha modes other than OPAQUE an opacity map of the base colour
-// texture's alpha x baseColorFactor[3] (the constant factor without a texture).  Emitters with an
-// emissive texture are unsupported (textured emission needs the emitter's texture importance).
+// normalTexture.scale, for alpha modes other than OPAQUE an opacity map of the base colour
+// texture's alpha x baseColorFactor[3] (the constant factor without a texture), and an emitter's
+// emissiveTexture x strength x emissiveFactor as its emission.
 ks_material_desc material(const Json &src, const std::string &where, bool &twosided, TextureSet *ts,
                           uint32_t index, std::vector<ks_texture_binding> &binds)
 {
@@ -727,8 +727,6 @@ ks_material_desc material(const Json &src, const std::string &where, bool &twosi
         d.has_emission = 1;
         for (int c = 0; c < 3; ++c)
             d.emission[c] = d.emissive[c];
-        if (src.get("emissiveTexture"))
-            throw Error(where + ": emitters with an emissive texture are not supported", true);
     }
     d.ior = 1.5f;
     if (const Json *e = extension("KHR_materials_ior"))
@@ -759,7 +757,7 @@ ks_material_desc material(const Json &src, const std::string &where, bool &twosi
     const bool alpha = src.string("alphaMode", "OPAQUE") != "OPAQUE";
     const Json *nt = src.get("normalTexture");
     if (!ts) {
-        if (bct || mrt || nt || spec_tex || trans_tex)
+        if (bct || mrt || nt || spec_tex || trans_tex || (d.has_emission && src.get("emissiveTexture")))
             throw Error(where + ": textured materials are not supported (constant fields only)", true);
         if (alpha)
             throw Error(where + ": alpha modes other than OPAQUE (opacity maps) are not supported", true);
@@ -818,6 +816,11 @@ ks_material_desc material(const Json &src, const std::string &where, bool &twosi
         ks_texture_binding b = texture_binding(*ts, *nt, index, KS_FIELD_NORMAL_MAP, one4, id4, where);
         b.strength = (float)nt->number("scale", 1.0);
         binds.push_back(b);
+    }
+    // an emitter's emissive texture x (emissive strength x emissiveFactor), sRGB
+    if (const Json *et = src.get("emissiveTexture"); et && d.has_emission) {
+        const float se[4] = {d.emissive[0], d.emissive[1], d.emissive[2], 1.0f};
+        binds.push_back(texture_binding(*ts, *et, index, KS_FIELD_EMISSION, se, id4, where));
     }
     return d;
 }

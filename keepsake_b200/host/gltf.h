@@ -6,11 +6,11 @@
 //
 // .gltf (JSON, buffers in files next to it or in base64 data URIs) and .glb (binary container).
 // Textures: PNG images (8- and 16-bit) bound to the base colour, metallic-roughness, specular,
-// transmission and normal slots with the nearest filter, and alpha modes other than OPAQUE as
-// opacity maps.  Not handled, each an error marked unsupported: JPEG and other image formats,
-// samplers with a mipmap minification filter (EWA filtering), emitters with an emissive texture,
-// sparse accessors, non-triangle primitives, index types other than unsigned short / unsigned int
-// (the reference asserts on those too).  Animations are not
+// transmission, normal and (for emitters) emissive slots with the nearest filter, and alpha modes
+// other than OPAQUE as opacity maps.  Not handled, each an error marked unsupported: JPEG and other
+// image formats, samplers with a mipmap minification filter (EWA filtering), sparse accessors,
+// non-triangle primitives, index types other than unsigned short / unsigned int (the reference
+// asserts on those too).  Animations are not
 // read (camera and transform animation are outside the small_pt path).
 #pragma once
 #include "../../include/ks_b200.h"

@@ -564,6 +564,7 @@ struct MeshLight
 {
     uint32_t mesh = 0;
     V3 emission;
+    int em_binding = -1; // the emission texture's binding in the material's list, -1: constant
     std::vector<uint32_t> prim_ids; // local triangle ids of the mesh
     std::vector<float> importance;
     std::vector<float> areas;
@@ -765,7 +766,7 @@ inline ks_material_desc textured_material(const Scene &s, uint32_t m, Intersecti
     ks_material_desc mat = s.materials[m];
     for (const Binding &bd : s.mat_bindings[m]) {
         const int f = bd.b.field;
-        if (f == KS_FIELD_OPACITY_MAP)
+        if (f == KS_FIELD_OPACITY_MAP || f == KS_FIELD_EMISSION)
             continue;
         if (f == KS_FIELD_NORMAL_MAP) {
             apply_normal_map(s, bd, it);
@@ -811,8 +812,8 @@ struct AlphaFilter
         for (const Binding &bd : s.mat_bindings[m]) {
             if (bd.b.field != KS_FIELD_OPACITY_MAP)
                 continue;
-            // MeshGeometry::compute_hit_texcoord (geometry.cpp:165-175)
-            float tu = u, tv = v;
+            // MeshGeometry::compute_hit_texcoord (geometry.cpp:165-173): zero without texcoords
+            float tu = 0.0f, tv = 0.0f;
             const uint32_t mesh = s.tri_mesh[tri];
             if (s.mesh_uv[mesh]) {
                 const uint32_t i0 = s.idx[3 * tri], i1 = s.idx[3 * tri + 1], i2 = s.idx[3 * tri + 2];
@@ -882,6 +883,180 @@ inline V3 light_normal(const Scene &s, uint32_t tri)
     return normalized(ng);
 }
 
+// compute_mesh_light_importance (light.cpp:307-522), per triangle: the factor of 2 pi x area.
+// Uniform branch (constant emission, no opacity texture): luminance(emission).  Textured branch:
+// the luminance of emission x opacity at the texel centres of the larger texture in a
+// SummedAreaTable (sat.h: double sums, corners looked up bilinearly with clamping over the
+// (n + 1)^2 grid), each triangle's mean over the tiles of its texcoord bounding box (flip_v, uv
+// scale and offset of the texture field; repeat: mod 1, clamp: saturate; degenerate boxes widened
+// by one cell), weighted by the unwrapped tile areas.  Tiles whose wrapped box is empty are skipped
+// (the reference asserts there).  Lookups that disagree in those settings: the grid's mean.
+struct OracleSat
+{
+    int nx, ny;
+    std::vector<double> t;
+    double at(int x, int y) const
+    {
+        if (x == 0 || y == 0)
+            return 0.0;
+        return t[(size_t)std::min(y - 1, ny - 1) * nx + std::min(x - 1, nx - 1)];
+    }
+    double corner(float px, float py) const
+    {
+        auto split = [](float p, int res, int &a, int &b, float &w) {
+            const float q = p * (float)(res - 1);
+            a = (int)std::floor(q);
+            b = a + 1;
+            w = q - (float)a;
+            a = std::clamp(a, 0, res - 1);
+            b = std::clamp(b, 0, res - 1);
+        };
+        int x0, x1, y0, y1;
+        float wx, wy;
+        split(px, nx + 1, x0, x1, wx);
+        split(py, ny + 1, y0, y1, wy);
+        return at(x0, y0) * (1.0 - wx) * (1.0 - wy) + at(x1, y0) * (wx) * (1.0 - wy) + at(x0, y1) * (1.0 - wx) * (wy) +
+               at(x1, y1) * (wx) * (wy);
+    }
+};
+
+inline std::vector<float> mesh_importance_factor(const Scene &s, uint32_t material, uint32_t first, uint32_t n)
+{
+    const ks_material_desc &mat = s.materials[material];
+    const V3 emission(mat.emission[0], mat.emission[1], mat.emission[2]);
+    const Binding *em = nullptr, *op = nullptr;
+    for (const Binding &b : s.mat_bindings[material]) {
+        if (b.b.field == KS_FIELD_EMISSION)
+            em = &b;
+        if (b.b.field == KS_FIELD_OPACITY_MAP)
+            op = &b;
+    }
+    if (!em && !op)
+        return std::vector<float>(n, luminance(emission));
+    int rx = 1, ry = 1;
+    if (em) {
+        rx = s.textures[em->b.texture].w;
+        ry = s.textures[em->b.texture].h;
+    }
+    bool fallback = false;
+    if (op) {
+        rx = std::max(rx, s.textures[op->b.texture].w);
+        ry = std::max(ry, s.textures[op->b.texture].h);
+        if (em && (em->b.wrap_u != op->b.wrap_u || em->b.wrap_v != op->b.wrap_v || (em->b.flip_v != 0) != (op->b.flip_v != 0) ||
+                   em->b.uv_scale[0] != op->b.uv_scale[0] || em->b.uv_scale[1] != op->b.uv_scale[1] ||
+                   em->b.uv_offset[0] != op->b.uv_offset[0] || em->b.uv_offset[1] != op->b.uv_offset[1]))
+            fallback = true;
+    }
+    std::vector<float> grid((size_t)rx * ry);
+    double total = 0.0;
+    for (int y = 0; y < ry; ++y)
+        for (int x = 0; x < rx; ++x) {
+            const float u = (x + 0.5f) / (float)rx, v = (y + 0.5f) / (float)ry;
+            float c[4];
+            float lum = luminance(emission);
+            if (em) {
+                em->eval(s.textures[em->b.texture], u, v, c);
+                lum = luminance(V3(c[0], c[1], c[2]));
+            }
+            if (op) {
+                op->eval(s.textures[op->b.texture], u, v, c);
+                lum *= c[0];
+            }
+            grid[(size_t)y * rx + x] = lum;
+            total += lum;
+        }
+    if (fallback)
+        return std::vector<float>(n, (float)(total / (double)grid.size()));
+    OracleSat sat{rx, ry, std::vector<double>(grid.size())};
+    for (int y = 0; y < ry; ++y)
+        for (int x = 0; x < rx; ++x) {
+            double v = grid[(size_t)y * rx + x];
+            if (x > 0)
+                v += sat.t[(size_t)y * rx + x - 1];
+            if (y > 0)
+                v += sat.t[(size_t)(y - 1) * rx + x];
+            if (x > 0 && y > 0)
+                v -= sat.t[(size_t)(y - 1) * rx + x - 1];
+            sat.t[(size_t)y * rx + x] = v;
+        }
+    const Binding &lb = em ? *em : *op;
+    const float before_one = std::nextafter(1.0f, 0.0f);
+    std::vector<float> out(n, 0.0f);
+    for (uint32_t k = 0; k < n; ++k) {
+        float lo[2] = {INFINITY, INFINITY}, hi[2] = {-INFINITY, -INFINITY};
+        for (int c = 0; c < 3; ++c) {
+            const uint32_t vi = s.idx[3 * (first + k) + c];
+            float t[2] = {s.texcoords[2 * vi], s.texcoords[2 * vi + 1]};
+            if (lb.b.flip_v)
+                t[1] = 1.0f - t[1];
+            for (int a = 0; a < 2; ++a) {
+                t[a] = t[a] * lb.b.uv_scale[a] + lb.b.uv_offset[a];
+                lo[a] = std::min(lo[a], t[a]);
+                hi[a] = std::max(hi[a], t[a]);
+            }
+        }
+        float acc = 0.0f, area_sum = 0.0f;
+        for (int ty = (int)std::floor(lo[1]); ty < (int)std::ceil(hi[1]); ++ty)
+            for (int tx = (int)std::floor(lo[0]); tx < (int)std::ceil(hi[0]); ++tx) {
+                float b0[2] = {std::max(lo[0], (float)tx), std::max(lo[1], (float)ty)};
+                float b1[2] = {std::min(hi[0], tx + before_one), std::min(hi[1], ty + before_one)};
+                if (b0[0] > b1[0] || b0[1] > b1[1])
+                    continue;
+                const float unwrapped = (b1[0] - b0[0]) * (b1[1] - b0[1]);
+                if (unwrapped == 0.0f)
+                    continue;
+                const int wrap[2] = {lb.b.wrap_u, lb.b.wrap_v}, res[2] = {rx, ry};
+                for (int a = 0; a < 2; ++a) {
+                    if (wrap[a] == 0) {
+                        for (float *p : {&b0[a], &b1[a]}) {
+                            float r = *p - std::floor(*p / 1.0f) * 1.0f;
+                            *p = r < 0 ? r + 1.0f : r;
+                        }
+                    } else {
+                        b0[a] = std::clamp(b0[a], 0.0f, 1.0f);
+                        b1[a] = std::clamp(b1[a], 0.0f, 1.0f);
+                    }
+                    if (b0[a] == 0.0f && b1[a] == 0.0f)
+                        b1[a] = 1.0f / (res[a] + 1);
+                    if (b0[a] == 1.0f && b1[a] == 1.0f)
+                        b0[a] = 1.0f - 1.0f / (res[a] + 1);
+                }
+                if (b0[0] > b1[0] || b0[1] > b1[1] || (b1[0] - b0[0]) * (b1[1] - b0[1]) == 0.0f)
+                    continue;
+                const double box = (sat.corner(b1[0], b1[1]) - sat.corner(b0[0], b1[1])) +
+                                   (sat.corner(b0[0], b0[1]) - sat.corner(b1[0], b0[1]));
+                const float mean = std::max((float)box, 0.0f) / (((b1[0] - b0[0]) * (float)rx) * ((b1[1] - b0[1]) * (float)ry));
+                acc += mean * unwrapped;
+                area_sum += unwrapped;
+            }
+        if (area_sum > 0.0f)
+            acc /= area_sum;
+        out[k] = acc;
+    }
+    return out;
+}
+
+// MeshTriLight::eval (light.cpp:560-565) at barycentrics (u, v): the emission texture at the
+// interpolated texcoords, or (without texcoords) at the barycentrics for a hit record
+// (compute_intersection) and at zero for a light sample (interpolate_texcoord, geometry.cpp:182-191)
+inline V3 light_Le(const Scene &s, const MeshLight &ml, uint32_t tri, float u, float v, bool bary_fallback)
+{
+    if (ml.em_binding < 0)
+        return ml.emission;
+    float tu = bary_fallback ? u : 0.0f, tv = bary_fallback ? v : 0.0f;
+    if (s.mesh_uv[s.tri_mesh[tri]]) {
+        const uint32_t i0 = s.idx[3 * tri], i1 = s.idx[3 * tri + 1], i2 = s.idx[3 * tri + 2];
+        const float *tc = s.texcoords.data();
+        const float w0 = 1.0f - u - v;
+        tu = w0 * tc[2 * i0] + u * tc[2 * i1] + v * tc[2 * i2];
+        tv = w0 * tc[2 * i0 + 1] + u * tc[2 * i1 + 1] + v * tc[2 * i2 + 1];
+    }
+    const Binding &bd = s.mat_bindings[s.mesh_material[ml.mesh]][ml.em_binding];
+    float c[4];
+    bd.eval(s.textures[bd.b.texture], tu, tv, c);
+    return V3(c[0], c[1], c[2]);
+}
+
 inline V3 mesh_light_sample(const Scene &s, uint32_t light_flat, V3 p_shade, float u0, float u1, V3 &wi,
                             float &wi_dist, float &pdf)
 {
@@ -922,7 +1097,7 @@ inline V3 mesh_light_sample(const Scene &s, uint32_t light_flat, V3 p_shade, flo
     pdf *= (wi_dist2 / absdot);
     constexpr float shadow_eps = 1e-4f;
     wi_dist = std::max(0.0f, wi_dist - shadow_eps);
-    return ml.emission / pdf;
+    return light_Le(s, ml, tri, b0, b1, false) / pdf;
 }
 
 inline float mesh_light_pdf(const Scene &s, uint32_t tri, uint32_t k, const MeshLight &ml, V3 wi, float wi_dist)
@@ -1065,7 +1240,7 @@ struct Tracer
                                                              (uint32_t)light) -
                                             s.index_psum.begin()) - 1;
                     const MeshLight &ml = s.mesh_lights[g - 1];
-                    V3 Le(ml.emission);
+                    const V3 Le = light_Le(s, ml, tri, bary[1], bary[2], true);
                     if (bounce == 0) {
                         L += beta * Le;
                     } else if (pr_light > 0.0f) {
@@ -1223,7 +1398,8 @@ Scene *create_scene(const ks_scene_desc *d, const ks_sbvh_options *opts)
         }
         s->sky = std::move(sky);
     }
-    // mesh lights (scene.cpp:315-336, light.cpp:307-560): constant emission -> uniform importance
+    // mesh lights (scene.cpp:315-336, light.cpp:307-560): constant emission -> uniform importance;
+    // emission / opacity textures -> the summed-area-table importance (mesh_importance_factor)
     for (uint32_t m = 0; m < d->n_meshes; ++m) {
         const ks_material_desc &mat = s->materials[s->mesh_material[m]];
         if (!mat.has_emission)
@@ -1231,14 +1407,18 @@ Scene *create_scene(const ks_scene_desc *d, const ks_sbvh_options *opts)
         MeshLight ml;
         ml.mesh = m;
         ml.emission = V3(mat.emission[0], mat.emission[1], mat.emission[2]);
-        float avg_importance = luminance(ml.emission);
+        const auto &mb = s->mat_bindings[s->mesh_material[m]];
+        for (size_t b = 0; b < mb.size(); ++b)
+            if (mb[b].b.field == KS_FIELD_EMISSION)
+                ml.em_binding = (int)b;
         uint32_t first = s->mesh_tri_off[m], n = s->mesh_tri_off[m + 1] - first;
+        const std::vector<float> factor = mesh_importance_factor(*s, s->mesh_material[m], first, n);
         std::vector<float> importance(n), areas(n);
         for (uint32_t k = 0; k < n; ++k) {
             V3 v0 = s->tri_vert(first + k, 0), v1 = s->tri_vert(first + k, 1), v2 = s->tri_vert(first + k, 2);
             V3 e01 = v1 - v0, e12 = v2 - v1;
             float area = 0.5f * norm(cross(e01, e12));
-            importance[k] = two_pi * area * avg_importance;
+            importance[k] = two_pi * area * factor[k];
             areas[k] = area;
         }
         std::vector<uint32_t> prim_ids(n);

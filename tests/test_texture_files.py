@@ -320,7 +320,22 @@ def test_gltf_material_textures(tmp_path):
     assert g.textures == [] and g.bindings == []
 
 
-@pytest.mark.parametrize("change", [dict(min_filter=9987), dict(image_kind="jpeg"), dict(emissive_tex=True)])
+def test_gltf_emissive_texture(tmp_path):
+    """An emitter's emissiveTexture becomes its emission (x emissive strength x emissiveFactor, sRGB
+    image)."""
+    from test_gltf import write_glb
+    ks = _ks()
+    doc, buf, *_ = _textured_document(tmp_path, emissive_tex=True)
+    write_glb(tmp_path / "e.glb", doc, buf)
+    g = ks.Generated.load_compound(tmp_path / "e.glb")
+    em = [b for b in g.bindings if b.field == 11]
+    assert len(em) == 1 and em[0].material == 1
+    assert list(em[0].scale) == pytest.approx([4.0, 2.0, 1.0, 1.0])
+    assert g.textures[em[0].texture][1]  # the normal-map image, now also an emissive one: sRGB
+    assert g.materials[1].has_emission
+
+
+@pytest.mark.parametrize("change", [dict(min_filter=9987), dict(image_kind="jpeg")])
 def test_gltf_unsupported_textures(tmp_path, change):
     from test_gltf import write_glb
     ks = _ks()

@@ -119,8 +119,21 @@ def test_texture_bindings_are_validated(ctx):
 
 def opacity_case(ks, W=48, H=48, spp=16):
     """The box room with an opacity map on both boxes (OpacityMap, opacity_map.cpp): an 8-bit mask of
-    fully opaque, fully clear and half-transparent stripes, and a float ramp on the back wall."""
+    fully opaque, fully clear and half-transparent stripes, and a float ramp on the back wall.  The
+    opacity test reads the mesh's texcoords (compute_hit_texcoord, geometry.cpp:165-173: (0, 0)
+    without them), so the boxes get texcoords from their vertex positions and the back wall its
+    corners'."""
     g = ks.Generated("box_room", 0)
+    d = g.desc.contents
+    tcs = []
+    for k in (5, 6):
+        v = g.meshes[k]["vertices"]
+        tc = np.ascontiguousarray(np.stack([(v[:, 0] + v[:, 2]) * 1.7, v[:, 1] * 1.3], -1), np.float32)
+        d.meshes[k].texcoords = tc.ctypes.data
+        tcs.append(tc)
+    tc = np.array([[0.0, 0.0], [1.0, 0.0], [1.0, 1.0], [0.0, 1.0]], np.float32)
+    d.meshes[2].texcoords = tc.ctypes.data
+    tcs.append(tc)
     ys, xs = np.mgrid[0:32, 0:32]
     stripes = np.where((xs // 4) % 3 == 0, 255, np.where((xs // 4) % 3 == 1, 0, 128)).astype(np.uint8)
     ramp = np.clip(xs / 31.0, 0.0, 1.0).astype(np.float32)
@@ -128,7 +141,7 @@ def opacity_case(ks, W=48, H=48, spp=16):
     binds = [B(5, "opacity_map", 0, filter=0), B(6, "opacity_map", 0, filter=0, uv_scale=(2.0, 2.0)),
              B(2, "opacity_map", 1, filter=1)]
     keep = ks.attach_textures(g.desc, [(stripes, False), (ramp, False)], binds)
-    g._tex = keep
+    g._tex = (keep, tcs)
     cam = ks.camera_perspective(g.camera_to_world, g.vfov, g.aspect)
     # a backdrop instead of the background: camera rays that leave the scene count as misses
     p = ks.SmallPTParams.make(render_width=W, render_height=H, spp=spp, bounces=6, clamp_indirect=0.0,
@@ -181,3 +194,67 @@ def test_opacity_render_matches_oracle(ctx, oracle):
     cpu = rel_mse(composite(oacc, ow), hi)
     assert gpu <= 1.25 * cpu + 1e-6, (gpu, cpu)
     s.close()
+
+
+def emitter_case(ks, W=48, H=48, spp=16, uv_scale=(1.0, 1.0), wrap=0):
+    """The box room's lamp with an emission texture (MeshTriLight with a TextureField emission,
+    light.cpp:307-565): a float texture of bright and dim cells and a zero corner, on the lamp's
+    texcoords; its two triangles' selection powers come from the texture's summed-area table."""
+    g = ks.Generated("box_room", 0)
+    d = g.desc.contents
+    ys, xs = np.mgrid[0:16, 0:16]
+    cells = ((xs // 4 + ys // 4) % 2).astype(np.float32)
+    tex = np.stack([20 + 40 * cells, 15 + 25 * cells, 4 + 10 * cells * (xs / 15.0)], -1).astype(np.float32)
+    tex[:4, :4] = 0.0
+    tc = np.array([[0.0, 0.0], [1.0, 0.0], [1.0, 1.0], [0.0, 1.0]], np.float32)
+    d.meshes[7].texcoords = tc.ctypes.data
+    b = ks.TextureBinding.make(7, "emission", 0, filter=1, uv_scale=uv_scale, wrap_u=wrap, wrap_v=wrap,
+                               scale=(0.8, 0.8, 0.8, 1.0))
+    g._tex = (ks.attach_textures(g.desc, [(tex, False)], [b]), tc)
+    cam = ks.camera_perspective(g.camera_to_world, g.vfov, g.aspect)
+    p = ks.SmallPTParams.make(render_width=W, render_height=H, spp=spp, bounces=6, clamp_indirect=0.0)
+    return g, cam, p
+
+
+def test_oracle_textured_emitter(oracle):
+    """A textured lamp changes the image and keeps its light weights (same camera samples)."""
+    import keepsake_b200 as ks
+    g, cam, p = emitter_case(ks, W=24, H=24, spp=4)
+    a, w, _ = oracle.scene(g.desc).render(cam, p, threads=4)
+    plain = ks.Generated("box_room", 0)
+    a0, w0, _ = oracle.scene(plain.desc).render(cam, p, threads=4)
+    assert np.isfinite(a).all() and (a >= 0).all()
+    assert np.array_equal(w, w0)
+    assert rel_mse(composite(a, w), composite(a0, w0)) > 1e-2
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("uv_scale,wrap", [((1.0, 1.0), 0), ((2.5, 1.5), 0), ((1.7, 1.0), 1)])
+def test_textured_emitter_matches_oracle(ctx, oracle, uv_scale, wrap):
+    """Same samples: the light-selection powers (summed-area-table importance, built by the library's
+    light build and by the oracle's restatement), the emission at light samples and at lamp hits."""
+    import keepsake_b200 as ks
+    g, cam, p = emitter_case(ks, uv_scale=uv_scale, wrap=wrap)
+    s = ks.Scene(ctx, g.desc)
+    s.build_bvh()
+    acc, w = s.render(cam, p)
+    oacc, ow, ocnt = oracle.scene(g.desc).render(cam, p)
+    assert np.array_equal(w, ow)
+    img, ref = composite(acc, w), composite(oacc, ow)
+    assert rel_mse(img, ref) < 2e-3
+    assert np.median(np.abs(img - ref) / (np.abs(ref) + 1e-3)) < 1e-4
+    st = s.stats()
+    assert abs(st.shadow_rays - int(ocnt[1])) <= 0.01 * ocnt[1] + 16
+    s.close()
+
+
+@pytest.mark.gpu
+def test_emission_binding_needs_an_emitter(ctx):
+    import ctypes
+    import keepsake_b200 as ks
+    g = ks.Generated("box_room", 0)
+    keep = ks.attach_textures(g.desc, [(np.ones((2, 2, 3), np.float32), False)],
+                              [ks.TextureBinding.make(0, "emission", 0)])  # material 0 emits nothing
+    h = ctypes.c_void_p()
+    assert ks.lib.ks_scene_create(ctx.handle, g.desc, ctypes.byref(h)) == 1
+    del keep
