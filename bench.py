@@ -37,6 +37,7 @@ parameters made by the oracle library, without loading the CUDA library) on the 
 configuration, each step one 16-spp interval of the 256-spp render of the full frame.
 """
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -696,7 +697,7 @@ def main():
     # ---- end to end through the host-buffer C ABI ----
     e2e_steps = args.e2e_steps if args.e2e_steps is not None else args.steps
     h2d = sum(m["vertices"].nbytes + m["indices"].nbytes for m in g.meshes)
-    h2d += len(g.materials) * 72 + (g.sky_map.nbytes if g.sky_map is not None else 0)
+    h2d += len(g.materials) * ctypes.sizeof(ks.MaterialDesc) + (g.sky_map.nbytes if g.sky_map is not None else 0)
     d2h = W_RES * H_RES * 5 * 8
     e2e_rays, e2e_t = 0, 0.0
     e2e_parts = []

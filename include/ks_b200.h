@@ -122,6 +122,16 @@ typedef struct ks_material_desc {
     float emission[3];
     int32_t bsdf;         /* 0 principled_bsdf, 1 principled_brdf, 2 lambertian */
     float specular;       /* principled_brdf: specular, clamped to [0, 1] and scaled by 0.08 */
+    /* Material::subsurface (a BSSRDF, subsurface.h:35-43; create_bssrdf, subsurface.cpp:536-545):
+     * at each hit the material picks its BSDF or, with probability 1/2, a random walk inside its
+     * mesh (subsurface_random_walk, subsurface.cpp:222-500) whose exit point shades with a
+     * Lambertian exit lobe (material.cpp:101-160).  Flat scenes, materials without emission. */
+    int32_t has_subsurface;
+    float ss_albedo[3];      /* BSSRDF::albedo, clamped to [0, 1] */
+    float ss_radius[3];      /* BSSRDF::radius: mean free path per channel (scene units) */
+    float ss_anisotropy;     /* Henyey-Greenstein g of the walk, in (-1, 1) */
+    float ss_ior;            /* BSSRDF::ior (> 0) */
+    float ss_rfr_entry_prob; /* probability of the refractive entry (else a cosine entry) */
 } ks_material_desc;
 
 /* The sky light: SkyLight (light.h:34-58), an ambient colour or a lat-long RGB map, or

@@ -159,7 +159,9 @@ class MaterialDesc(ctypes.Structure):
     _fields_ = [("basecolor", _f32 * 3), ("roughness", _f32), ("metallic", _f32), ("ior", _f32),
                 ("specular_r0_mul", _f32), ("specular_trans", _f32), ("diffuse_trans", _f32),
                 ("diffuse_trans_fwd", _f32), ("emissive", _f32 * 3), ("microfacet", _i32),
-                ("has_emission", _i32), ("emission", _f32 * 3), ("bsdf", _i32), ("specular", _f32)]
+                ("has_emission", _i32), ("emission", _f32 * 3), ("bsdf", _i32), ("specular", _f32),
+                ("has_subsurface", _i32), ("ss_albedo", _f32 * 3), ("ss_radius", _f32 * 3), ("ss_anisotropy", _f32),
+                ("ss_ior", _f32), ("ss_rfr_entry_prob", _f32)]
 
 
 class SkyDesc(ctypes.Structure):

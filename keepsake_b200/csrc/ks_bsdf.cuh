@@ -25,7 +25,8 @@ enum : int
     kBsdfPrincipledBeckmann = 1,
     kBrdfPrincipledGGX = 2,
     kBrdfPrincipledBeckmann = 3,
-    kBsdfLambertian = 4
+    kBsdfLambertian = 4,
+    kBsdfSubsurfaceExit = 5 // LambertianSubsurfaceExitAdapter: basecolor holds eta^2
 };
 
 struct Closure
@@ -846,6 +847,37 @@ struct LambertianD
     }
 };
 
+// LambertianSubsurfaceExitAdapter (subsurface.cpp:502-532): the cosine lobe at a random walk's exit
+// point, scaled by eta^2 (undoing the 1 / eta^2 of the entry); it reads wi only.
+KS_D Closure subsurface_exit_closure(float eta)
+{
+    Closure c{};
+    c.kind = kBsdfSubsurfaceExit;
+    c.basecolor = mk(eta * eta, eta * eta, eta * eta);
+    return c;
+}
+
+struct SubsurfaceExitD
+{
+    Closure c;
+    KS_D void eval_and_pdf(f3, f3 wi, f3 &f, float &p) const
+    {
+        if (wi.z <= 0.0f) {
+            f = mk(0, 0, 0);
+            p = 0.0f;
+            return;
+        }
+        f = (kInvPi * wi.z) * c.basecolor;
+        p = wi.z * kInvPi;
+    }
+    KS_D f3 sample(f3, f3 &wi, float, float u0, float u1, float &pdf) const
+    {
+        wi = sample_cosine_hemisphere(u0, u1);
+        pdf = wi.z * kInvPi;
+        return c.basecolor;
+    }
+};
+
 // Any BSDF of a material (the Material::bsdf pointer of material.h:39, dispatched on the kind).
 // Its two entry points stay out of line: the general shading kernel then calls one function per
 // use instead of holding five inlined variants' live state around each call.
@@ -867,6 +899,9 @@ struct AnyBsdf
         case kBrdfPrincipledBeckmann:
             PrincipledBrdfT<Beckmannd>{c}.eval_and_pdf(wo, wi, f, p);
             break;
+        case kBsdfSubsurfaceExit:
+            SubsurfaceExitD{c}.eval_and_pdf(wo, wi, f, p);
+            break;
         default:
             LambertianD{c}.eval_and_pdf(wo, wi, f, p);
             break;
@@ -883,6 +918,8 @@ struct AnyBsdf
             return PrincipledBrdfT<GGXd>{c}.sample(wo, wi, u_lobe, u0, u1, pdf);
         case kBrdfPrincipledBeckmann:
             return PrincipledBrdfT<Beckmannd>{c}.sample(wo, wi, u_lobe, u0, u1, pdf);
+        case kBsdfSubsurfaceExit:
+            return SubsurfaceExitD{c}.sample(wo, wi, u_lobe, u0, u1, pdf);
         default:
             return LambertianD{c}.sample(wo, wi, u_lobe, u0, u1, pdf);
         }

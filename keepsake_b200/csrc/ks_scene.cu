@@ -191,9 +191,20 @@ bool valid_material(const ks_material_desc &m)
     for (int c = 0; c < 3; ++c)
         if (!finite(m.basecolor[c]) || !finite(m.emission[c]))
             return false;
-    return finite(m.roughness) && finite(m.metallic) && finite(m.ior) && finite(m.specular_r0_mul) &&
-           finite(m.specular_trans) && finite(m.diffuse_trans) && finite(m.diffuse_trans_fwd) &&
-           finite(m.specular);
+    if (!(finite(m.roughness) && finite(m.metallic) && finite(m.ior) && finite(m.specular_r0_mul) &&
+          finite(m.specular_trans) && finite(m.diffuse_trans) && finite(m.diffuse_trans_fwd) && finite(m.specular)))
+        return false;
+    if (m.has_subsurface < 0 || m.has_subsurface > 1)
+        return false;
+    if (m.has_subsurface) {
+        for (int c = 0; c < 3; ++c)
+            if (!finite(m.ss_albedo[c]) || !finite(m.ss_radius[c]) || !(m.ss_radius[c] >= 0.0f))
+                return false;
+        if (!(m.ss_anisotropy > -1.0f && m.ss_anisotropy < 1.0f) || !(m.ss_ior > 0.0f) || !finite(m.ss_ior) ||
+            !(m.ss_rfr_entry_prob >= 0.0f && m.ss_rfr_entry_prob <= 1.0f))
+            return false;
+    }
+    return true;
 }
 
 // srgb_to_linear (maths.h:631-638) in float; for 8-bit texels the reference reads a 256-entry table
@@ -337,6 +348,15 @@ bool ksb::material_to_gpu(const ks_material_desc &m, MaterialGPU &g)
     g.specular = m.specular;
     g.has_emission = m.has_emission;
     g.mesh_light = -1;
+    g.has_ss = m.has_subsurface;
+    for (int c = 0; c < 3; ++c) {
+        // BSSRDF::sample clamps the albedo to [0, 1] (subsurface.cpp:526-527)
+        g.ss_albedo[c] = std::min(std::max(m.ss_albedo[c], 0.0f), 1.0f);
+        g.ss_radius[c] = m.ss_radius[c];
+    }
+    g.ss_g = m.ss_anisotropy;
+    g.ss_ior = m.ss_ior;
+    g.ss_rfr = m.ss_rfr_entry_prob;
     return true;
 }
 
@@ -455,6 +475,12 @@ ks_status ks_scene_create(ks_context *ctx, const ks_scene_desc *desc, ks_scene *
             t.format > 2 || (uint64_t)t.width * t.height > (1ull << 28))
             return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_create: bad texture " + std::to_string(k));
     }
+    for (uint32_t k = 0; k < desc->n_materials; ++k) {
+        const ks_material_desc &m = desc->materials[k];
+        if (m.has_subsurface && (m.has_emission || desc->n_instances))
+            return fail(ctx, KS_ERR_UNSUPPORTED, "ks_scene_create: material " + std::to_string(k) +
+                                                     ": subsurface scattering with emission or in an instanced scene");
+    }
     for (uint32_t k = 0; k < desc->n_bindings; ++k) {
         BindingGPU g;
         if (!binding_to_gpu(desc->bindings[k], *desc, g))
@@ -543,7 +569,8 @@ ks_status ks_scene_create(ks_context *ctx, const ks_scene_desc *desc, ks_scene *
     for (uint32_t k = 0; k < desc->n_materials; ++k) {
         const ks_material_desc &m = desc->materials[k];
         material_to_gpu(m, mats[k]);
-        s->ext_materials |= m.bsdf != 0 || m.microfacet != 0;
+        s->ext_materials |= m.bsdf != 0 || m.microfacet != 0 || m.has_subsurface != 0;
+        s->any_subsurface |= m.has_subsurface != 0;
     }
     // textures and bindings (validated above), the bindings grouped by material in their order
     std::vector<float4> texels;

@@ -65,7 +65,9 @@ struct MaterialGPU
     int bsdf;       // 0 PrincipledBSDF, 1 PrincipledBRDF, 2 Lambertian (albedo = basecolor)
     float specular; // PrincipledBRDF's specular field
     int bind_begin, bind_count; // the material's texture bindings (SceneView::bindings)
-    int tex_flags;              // kMatNormalMap | kMatOpacityMap
+    int tex_flags;              // kMatNormalMap | kMatOpacityMap | kMatEmissionMap
+    int has_ss;                 // a BSSRDF (ks_material_desc.has_subsurface)
+    float ss_albedo[3], ss_radius[3], ss_g, ss_ior, ss_rfr;
 };
 enum : int
 {
@@ -134,6 +136,7 @@ struct ks_scene
         std::vector<float> texcoords; // 2 per global vertex (zeros for meshes without)
     } emit_tex;
     bool any_emission_map = false;
+    bool any_subsurface = false; // some material has a BSSRDF
     // per-vertex shading attributes, indexed like verts (allocated only when some mesh has them)
     ksb::DevBuf<float> normals;   // 3 per vertex: MeshData::vertex_normals of smooth-shaded meshes
     ksb::DevBuf<float> texcoords; // 2 per vertex: MeshData::texcoords

@@ -12,6 +12,7 @@
 #include "ks_bsdf.cuh"
 #include "ks_sampler.cuh"
 #include "ks_wavefront.cuh"
+#include "ks_subsurface.cuh"
 
 #include <type_traits>
 
@@ -354,7 +355,10 @@ __global__ void __launch_bounds__(128, KS_SHADE_MIN_BLOCKS) k_shade(const __grid
                     finish = true;
                 } else {
                     f3 wo = -normalize(rd);
-                    const std::conditional_t<kVariant == kShadeGeneral, AnyBsdf, Principled> bsdf{make_closure(mat)};
+                    // a random walk's exit (k_subsurface marks its hit distance negative) shades with the
+                    // Lambertian exit lobe
+                    const std::conditional_t<kVariant == kShadeGeneral, AnyBsdf, Principled> bsdf{
+                        kVariant == kShadeGeneral && h.x < 0.0f ? subsurface_exit_closure(mat.ss_ior) : make_closure(mat)};
                     // this bounce's Sobol values and light sample, drawn by k_sample
                     const float4 sa = samples[4 * (size_t)i], sl = samples[4 * (size_t)i + 1];
                     const float4 se = samples[4 * (size_t)i + 2];
@@ -586,6 +590,100 @@ ks_status bsdf_hook(ks_context *ctx, const ks_material_desc *mat, uint32_t n, co
 
 namespace wave
 {
+
+// Subsurface entries (Material::sample_with_nee, material.cpp:101-140), before the light samples of
+// a bounce: every hit on a material with a BSSRDF draws one Sobol value (the path's dimension moves
+// on by one): below 1/2 the path keeps its BSDF (beta x 2); else beta x 2 / ior^2 and a random walk
+// from the hit (subsurface_walk).  A successful walk replaces the hit record by its exit (a negative
+// distance marks it: the shading there uses the Lambertian exit lobe) and the ray direction by its
+// last direction (the exit's wo), and multiplies beta by its throughput; a failed walk zeroes beta,
+// which ends the path.
+struct MeshOnly
+{
+    const uint32_t *tri_mesh;
+    uint32_t mesh;
+    KS_D bool operator()(uint32_t tri, float, float, const RayQuery &) const { return __ldg(&tri_mesh[tri]) == mesh; }
+};
+
+__global__ void __launch_bounds__(128) k_subsurface(const __grid_constant__ SceneView sv, const __grid_constant__ RenderParams rp,
+                                                    PathBuf cur, float4 *hits, const uint32_t *queue,
+                                                    const uint32_t *queue_count, int *overflow)
+{
+    const uint32_t count = *queue_count;
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x) {
+        const uint32_t i = queue[q];
+        const float4 h = hits[i];
+        const float4 *pt = sv.prim_tris + 3 * (size_t)bits(h.w);
+        const float4 v0 = __ldg(pt), v1 = __ldg(pt + 1), v2 = __ldg(pt + 2);
+        const uint32_t tri = bits(v0.w);
+        const uint32_t mesh = __ldg(&sv.tri_mesh[tri]);
+        const MaterialGPU &mat = sv.materials[__ldg(&sv.mesh_material[mesh])];
+        if (!mat.has_ss)
+            continue;
+        float4 d4 = cur.d_info[i];
+        const uint32_t info = bits(d4.w);
+        const uint32_t bounce = info & 0xffffu;
+        if ((int)bounce == rp.bounces)
+            continue; // the path ends at this hit (small_pt.cpp:140-142): nothing is sampled
+        const int dim = (int)(info >> 16);
+        const float4 bp = cur.beta_pix[i];
+        const uint32_t pix = bits(bp.w), smp = bits(cur.L_smp[i].w);
+        SobolSampler sob = SobolSampler::start(pix % (uint32_t)rp.W, pix / (uint32_t)rp.W, smp, rp.log2_spp,
+                                               rp.n_digits, (uint32_t)rp.seed, dim);
+        const float u_sel = sob.next();
+        d4.w = fbits(((uint32_t)(dim + 1) << 16) | bounce);
+        f3 beta = mk(bp.x, bp.y, bp.z);
+        if (u_sel < 0.5f) {
+            beta *= 2.0f;
+        } else {
+            f3 tp = mk(2.0f, 2.0f, 2.0f);
+            tp /= sqr(mat.ss_ior);
+            const f3 p0 = mk(v0.x, v0.y, v0.z), p1 = mk(v1.x, v1.y, v1.z), p2 = mk(v2.x, v2.y, v2.z);
+            const int flags = __ldg(&sv.mesh_flags[mesh]);
+            ShadeFrame it = hit_frame<true>(sv, tri, flags, p0, p1, p2, h.y, h.z, mk(d4.x, d4.y, d4.z), nullptr);
+            if (mat.tex_flags & kMatNormalMap)
+                (void)textured_material(sv, mat, tri, flags, h.y, h.z, it);
+            SsProfile prof;
+            prof.albedo = mk(mat.ss_albedo[0], mat.ss_albedo[1], mat.ss_albedo[2]);
+            prof.radius = mk(mat.ss_radius[0], mat.ss_radius[1], mat.ss_radius[2]);
+            prof.g = mat.ss_g;
+            prof.ior = mat.ss_ior;
+            prof.rfr_entry_prob = mat.ss_rfr;
+            Pcg32 rng = subsurface_stream(pix % (uint32_t)rp.W, pix / (uint32_t)rp.W, (uint32_t)rp.seed, smp, bounce);
+            int of = 0;
+            auto cast = [&](const RayQuery &ray, WalkExit &e) {
+                Hit hh;
+                traverse<false>(sv.nodes, sv.prim_tris, sv.root_ref, sv.root_count, sv.bmin, sv.bmax, ray, 2, hh, of,
+                                nullptr, MeshOnly{sv.tri_mesh, mesh});
+                if (hh.tri == ~0u)
+                    return false;
+                e = WalkExit{hh.slot, hh.t, hh.b1, hh.b2};
+                return true;
+            };
+            WalkExit ex;
+            f3 wi;
+            if (subsurface_walk(prof, it.p, it.sn, it.n, rng, cast, tp, ex, wi)) {
+                beta = beta * tp;
+                hits[i] = make_float4(-1.0f, ex.b1, ex.b2, fbits(ex.slot));
+                d4.x = wi.x;
+                d4.y = wi.y;
+                d4.z = wi.z;
+            } else {
+                beta = mk(0, 0, 0);
+            }
+            if (of)
+                atomicOr(overflow, 1);
+        }
+        cur.d_info[i] = d4;
+        cur.beta_pix[i] = make_float4(beta.x, beta.y, beta.z, bp.w);
+    }
+}
+
+void launch_subsurface(unsigned grid, cudaStream_t st, const SceneView &sv, const RenderParams &rp, PathBuf cur,
+                       float4 *hits, const uint32_t *queue, const uint32_t *queue_count, int *overflow)
+{
+    k_subsurface<<<grid, 128, 0, st>>>(sv, rp, cur, hits, queue, queue_count, overflow);
+}
 
 void launch_sample(bool batch, unsigned grid, cudaStream_t st, const SceneView &sv, const RenderParams &rp,
                    PathBuf cur, const float4 *hits, const uint32_t *hit_inst, const uint32_t *queue,

@@ -437,6 +437,9 @@ KS_D const WideNode *tree_of<WideNode>(const SceneView &sv)
 
 // ---- shading launchers (ks_shade.cu) ----------------------------------------------------------
 // k_sample: Sobol values and the NEE light sample of every path in the hit queue.
+// Subsurface entries of a bounce's hit queue (k_subsurface, ks_shade.cu), before its light samples.
+void launch_subsurface(unsigned grid, cudaStream_t st, const SceneView &sv, const RenderParams &rp, PathBuf cur,
+                       float4 *hits, const uint32_t *queue, const uint32_t *queue_count, int *overflow);
 void launch_sample(bool batch, unsigned grid, cudaStream_t st, const SceneView &sv, const RenderParams &rp,
                    PathBuf cur, const float4 *hits, const uint32_t *hit_inst, const uint32_t *queue,
                    const uint32_t *queue_count, float4 *samples, const BatchView &bv);

@@ -745,10 +745,35 @@ const ConfigServiceImpl::TaskMaterial &ConfigServiceImpl::material(const std::st
     if (type != "principled_bsdf" && type != "principled_brdf" && type != "lambertian")
         throw StatusError(KS_ERR_UNSUPPORTED, "config: bsdf type '" + type +
                                                   "' is not supported (principled_bsdf, principled_brdf, lambertian)");
-    if (!a.load_string("subsurface", "").empty())
-        throw StatusError(KS_ERR_UNSUPPORTED, "config: subsurface scattering is not supported");
     TaskMaterial tm;
     ks_material_desc &d = tm.d;
+    // create_bssrdf (subsurface.cpp:536-545): albedo and radius (constant shader fields), anisotropy,
+    // ior, rfr_entry_prob
+    const std::string ss_path = a.load_string("subsurface", "");
+    if (!ss_path.empty()) {
+        const Value *snode = find_asset(ss_path);
+        if (!snode || ss_path.rfind("bssrdf.", 0) != 0)
+            throw ParseError("config: unknown bssrdf '" + ss_path + "'");
+        ConfigArgs ss = args_of(this, snode, ss_path);
+        auto constant3 = [&](const char *key, float out[3]) {
+            const Value &v = child(*ss.internal, key);
+            if (v.kind == Value::Kind::Table) {
+                ConfigArgs f = ss[key];
+                if (f.load_string("type") != "constant")
+                    throw StatusError(KS_ERR_UNSUPPORTED, "config: '" + ss_path + "': textured " + key +
+                                                              " is not supported");
+                f.load_vec3("value", out);
+            } else {
+                vec_n(v, 3, out, key);
+            }
+        };
+        d.has_subsurface = 1;
+        constant3("albedo", d.ss_albedo);
+        constant3("radius", d.ss_radius);
+        d.ss_anisotropy = ss.load_float("anisotropy");
+        d.ss_ior = ss.load_float("ior");
+        d.ss_rfr_entry_prob = ss.load_float("rfr_entry_prob");
+    }
     // a shader field: { type = "constant", value = ... } (or, as an extension, the bare value), or
     // { type = "texture", ... }
     auto field = [&](const char *key, int n, float *out, const float *dflt, int32_t field_id) {

@@ -870,12 +870,39 @@ struct Lambertian
 };
 
 // A material's BSDF (Material::bsdf, material.h:39), by type and microfacet distribution.
+// LambertianSubsurfaceExitAdapter (subsurface.cpp:502-532): the cosine lobe at a random walk's
+// exit, times eta^2 (c.ior holds eta); only wi is read.
+struct SubsurfaceExit
+{
+    Closure c;
+    void eval_and_pdf(V3, V3 wi, V3 &f, float &p) const
+    {
+        if (wi.z <= 0.0f) {
+            f = V3();
+            p = 0.0f;
+            return;
+        }
+        f = V3(inv_pi * wi.z, inv_pi * wi.z, inv_pi * wi.z);
+        f *= c.ior * c.ior;
+        p = wi.z * inv_pi;
+    }
+    V3 sample(V3, V3 &wi, float, float u0, float u1, float &pdf) const
+    {
+        wi = sample_cosine_hemisphere(u0, u1);
+        pdf = wi.z * inv_pi;
+        const float e2 = c.ior * c.ior;
+        return V3(e2, e2, e2);
+    }
+};
+
 struct Bsdf
 {
     Closure c;
     template <class F>
     auto visit(F &&fn) const
     {
+        if (c.bsdf == 3)
+            return fn(SubsurfaceExit{c});
         if (c.bsdf == 2)
             return fn(Lambertian{c});
         if (c.bsdf == 1)

@@ -2,7 +2,7 @@
 //
 //   SmallPT::run / trace          small_pt.cpp:15-178
 //   next_event_estimate           nee.cpp:11-57, power_heur nee.h:18-23
-//   Material::sample_with_nee     material.cpp:101-167 (no subsurface)
+//   Material::sample_with_nee     material.cpp:101-167 (subsurface: o_subsurface.h)
 //   Camera::spawn_ray             camera.cpp:129-170 (perspective, no ray differentials: the
 //                                 constant shader fields never read them)
 //   pixel filters                 render_target.h:79-180 (box, Gaussian, Blackman-Harris)
@@ -21,6 +21,7 @@
 #include "../../include/ks_b200.h"
 #include "o_bsdf.h"
 #include "o_texture.h"
+#include "o_subsurface.h"
 #include "o_math.h"
 #include "o_sampler.h"
 
@@ -1192,7 +1193,7 @@ struct Tracer
         return beta_nee;
     }
 
-    bool trace(V3 ro, V3 rd, OwenScrambledSobol02Morton &sobol, V3 &Lout)
+    bool trace(V3 ro, V3 rd, OwenScrambledSobol02Morton &sobol, Pcg32 &rng, V3 &Lout)
     {
         V3 L;
         V3 beta(1, 1, 1);
@@ -1260,15 +1261,61 @@ struct Tracer
                 break;
             V3 wo = -normalized(rd);
             Bsdf bsdf{eval_closure(mat)};
-            // Material::sample_with_nee (material.cpp:101-167)
-            V3 Ld = nee(bsdf, it, wo, sobol);
+            // Material::sample_with_nee (material.cpp:101-167): with a BSSRDF, the BSDF or (1/2) a
+            // random walk whose exit shades with the Lambertian exit lobe
+            V3 ss_beta(1.0f, 1.0f, 1.0f);
+            if (mat.has_subsurface) {
+                if (sobol.next() < 0.5f) {
+                    ss_beta *= 2.0f;
+                } else {
+                    ss_beta *= 2.0f;
+                    ss_beta /= mat.ss_ior * mat.ss_ior;
+                    auto cast = [&](V3 o, V3 d, float tmax, uint32_t &tri_out, float &t_out, float &b1, float &b2) {
+                        float r[8] = {o.x, o.y, o.z, 0.0f, d.x, d.y, d.z, tmax};
+                        struct MeshFilter
+                        {
+                            const Scene *s;
+                            uint32_t mesh;
+                            static int call(void *user, uint32_t tri, float, float)
+                            {
+                                const MeshFilter &f = *(const MeshFilter *)user;
+                                return f.s->tri_mesh[tri] == f.mesh;
+                            }
+                        } mf{&s, mesh};
+                        float bary[3];
+                        uint64_t dummy[3] = {0, 0, 0};
+                        tri_out = ksref_sbvh_intersect1_counted(s.bvh, r, 0, 2, &t_out, bary, dummy, MeshFilter::call,
+                                                                &mf);
+                        b1 = bary[1];
+                        b2 = bary[2];
+                        return tri_out != ~0u;
+                    };
+                    const V3 alb(std::clamp(mat.ss_albedo[0], 0.0f, 1.0f), std::clamp(mat.ss_albedo[1], 0.0f, 1.0f),
+                                 std::clamp(mat.ss_albedo[2], 0.0f, 1.0f));
+                    const V3 rad(mat.ss_radius[0], mat.ss_radius[1], mat.ss_radius[2]);
+                    uint32_t etri = 0;
+                    float et = 0.0f, eb1 = 0.0f, eb2 = 0.0f;
+                    V3 ss_wi;
+                    if (!ss_walk(alb, rad, mat.ss_anisotropy, mat.ss_ior, mat.ss_rfr_entry_prob, it.p, it.sh_frame.n,
+                                 it.frame.n, rng, cast, ss_beta, etri, et, eb1, eb2, ss_wi))
+                        break; // MaterialSample {0, 0}: no light and a zero throughput end the path
+                    wo = -ss_wi;
+                    it = make_intersection(s, etri, et, eb1, eb2, ss_wi);
+                    (void)textured_material(s, s.mesh_material[s.tri_mesh[etri]], it); // the exit's normal map
+                    Closure ce{};
+                    ce.bsdf = 3;
+                    ce.ior = mat.ss_ior;
+                    bsdf = Bsdf{ce};
+                }
+            }
+            V3 Ld = ss_beta * nee(bsdf, it, wo, sobol);
             V3 wo_local = it.sh_to_local(wo);
             float u_lobe = sobol.next();
             float u0, u1;
             sobol.next2d(u0, u1);
             V3 wi_local;
             float pdf_wi = 0.0f;
-            V3 sbeta = bsdf.sample(wo_local, wi_local, u_lobe, u0, u1, pdf_wi);
+            V3 sbeta = ss_beta * bsdf.sample(wo_local, wi_local, u_lobe, u0, u1, pdf_wi);
             V3 wi;
             if (!(max_coeff(sbeta) == 0.0f || pdf_wi == 0.0f))
                 wi = it.sh_to_world(wi_local);
@@ -1606,7 +1653,8 @@ int oracle_render_range(void *sp, const ks_camera_desc *cam, const ks_small_pt_p
                             dir = normalized(world_pos - cp);
                         }
                         V3 L;
-                        bool hit = tr.trace(cp, dir, sampler.sobol, L);
+                        Pcg32 rng = sample_rng(px, py, (uint32_t)in->rng_seed, smp);
+                        bool hit = tr.trace(cp, dir, sampler.sobol, rng, L);
                         if (hit) {
                             weights[2 * pix + 0] += 1.0;
                             weights[2 * pix + 1] += 0.0;

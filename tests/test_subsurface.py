@@ -1,0 +1,211 @@
+"""Subsurface scattering (Material::subsurface, a BSSRDF: subsurface.cpp, material.cpp:101-160).
+
+At a hit on a material with a BSSRDF the path picks the BSDF or, with probability 1/2, a random
+walk inside the mesh (Blender's random-walk subsurface with Dwivedi guiding, the walk's exit shaded
+with a Lambertian lobe x eta^2).  The walk draws from the sample's PCG32 stream; the oracle follows
+the reference's one stream per sample, the GPU gives each walk its own stretch of that stream, so
+the two agree in distribution, not sample by sample: the GPU image is checked by convergence to a
+high-spp oracle image.
+
+CPU: the oracle's image is finite, differs from the same box without the BSSRDF, and loses energy
+with a darker albedo; the refractive entry (which the reference starts from a zero direction) ends
+every walk, so with rfr_entry_prob 1 only the BSDF branch (weight 2, probability 1/2) remains and the
+image converges to the box without the BSSRDF."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from imaging import composite, rel_mse
+
+
+def ss_case(ks, albedo=(0.8, 0.6, 0.4), radius=(0.3, 0.2, 0.1), g=0.2, rfr=0.0, W=40, H=40, spp=16, bounces=6):
+    """The box room with the taller box (mesh 5) made of a subsurface material; the box is closed and
+    one-sided, raised off the floor so its bottom face does not share the floor's plane."""
+    g_ = ks.Generated("box_room", 0)
+    d = g_.desc.contents
+    m = d.materials[d.meshes[5].material]
+    m.has_subsurface = 1
+    m.ss_albedo[:] = albedo
+    m.ss_radius[:] = radius
+    m.ss_anisotropy = g
+    m.ss_ior = 1.4
+    m.ss_rfr_entry_prob = rfr
+    d.meshes[5].twosided = 0
+    md = d.meshes[5]
+    buf = (ctypes.c_float * (3 * md.n_vertices)).from_address(ctypes.cast(md.vertices, ctypes.c_void_p).value)
+    v = np.frombuffer(buf, np.float32).reshape(-1, 3)
+    v[:, 1] += np.float32(1e-3)
+    cam = ks.camera_perspective(g_.camera_to_world, g_.vfov, g_.aspect)
+    p = ks.SmallPTParams.make(render_width=W, render_height=H, spp=spp, bounces=bounces, clamp_indirect=0.0)
+    return g_, cam, p
+
+
+def test_oracle_subsurface_render(oracle):
+    import keepsake_b200 as ks
+    g, cam, p = ss_case(ks, W=20, H=20, spp=8)
+    a, w, _ = oracle.scene(g.desc).render(cam, p, threads=4)
+    img = composite(a, w)
+    assert np.isfinite(img).all() and (img >= 0).all()
+    plain = ks.Generated("box_room", 0)
+    a0, w0, _ = oracle.scene(plain.desc).render(cam, p, threads=4)
+    assert rel_mse(img, composite(a0, w0)) > 1e-3
+    # a darker medium returns less light
+    gd, _, _ = ss_case(ks, albedo=(0.1, 0.1, 0.1), W=20, H=20, spp=8)
+    ad, wd, _ = oracle.scene(gd.desc).render(cam, p, threads=4)
+    assert composite(ad, wd).sum() < img.sum()
+
+
+def test_oracle_refractive_entry_ends_the_walk(oracle):
+    import keepsake_b200 as ks
+    g, cam, p = ss_case(ks, rfr=1.0, W=16, H=16, spp=64)
+    a, w, _ = oracle.scene(g.desc).render(cam, p, threads=4)
+    plain = ks.Generated("box_room", 0)
+    a0, w0, _ = oracle.scene(plain.desc).render(cam, p, threads=4)
+    f, f0 = composite(a, w).mean(), composite(a0, w0).mean()
+    assert abs(f / f0 - 1.0) < 0.03, (f, f0)
+
+
+@pytest.mark.gpu
+def test_subsurface_converges_to_oracle(ctx, oracle):
+    """GPU at 16 spp and the oracle at 16 spp (another seed than the reference) against a 256-spp
+    oracle image: the GPU's error within 1.25x the oracle's own."""
+    import keepsake_b200 as ks
+    g, cam, p = ss_case(ks)
+    osc = oracle.scene(g.desc)
+    p.spp = 256
+    ref = composite(*osc.render(cam, p)[:2])
+    p.spp = 16
+    p.rng_seed = 1
+    s = ks.Scene(ctx, g.desc)
+    s.build_bvh()
+    acc, w = s.render(cam, p)
+    oacc, ow, _ = osc.render(cam, p)
+    assert np.array_equal(w, ow)
+    gpu = rel_mse(composite(acc, w), ref)
+    cpu = rel_mse(composite(oacc, ow), ref)
+    assert gpu <= 1.25 * cpu + 1e-6, (gpu, cpu)
+    # the flux agrees within 2 %
+    assert abs(composite(acc, w).mean() / ref.mean() - 1.0) < 0.02
+    s.close()
+
+
+@pytest.mark.gpu
+def test_subsurface_limits(ctx):
+    """Subsurface with emission, in instanced scenes or in a guided render is unsupported."""
+    import keepsake_b200 as ks
+    g, cam, p = ss_case(ks)
+    d = g.desc.contents
+    mi = d.meshes[5].material
+    d.materials[mi].has_emission = 1
+    h = ctypes.c_void_p()
+    assert ks.lib.ks_scene_create(ctx.handle, g.desc, ctypes.byref(h)) == 7
+    d.materials[mi].has_emission = 0
+    d.materials[mi].ss_anisotropy = 1.0  # outside (-1, 1)
+    assert ks.lib.ks_scene_create(ctx.handle, g.desc, ctypes.byref(h)) == 1
+    d.materials[mi].ss_anisotropy = 0.2
+    s = ks.Scene(ctx, g.desc)
+    s.build_bvh()
+    lo, hi = g.bound
+    guide = ks.Guide(ctx, list(lo - 0.05) + list(hi + 0.05), seed=1)
+    with pytest.raises(ks.KsError) as e:
+        s.render_guided(cam, p, guide)
+    assert e.value.status == 7
+    guide.close()
+    s.close()
+
+
+@pytest.mark.gpu
+def test_task_bssrdf_asset(ctx, tmp_path):
+    """`[bssrdf.X]` (create_bssrdf) and a material's `subsurface` key through the TOML task render
+    the same material as the C ABI (the same walks: the library draws them)."""
+    import keepsake_b200 as ks
+    c2w = [1.0, 0.0, 0.0, 0.0, 0.0, 0.9578, 0.2873, 1.8, 0.0, -0.2873, 0.9578, 3.0, 0.0, 0.0, 0.0, 1.0]
+    doc = f"""
+[bsdf.floor]
+type = "lambertian"
+albedo = {{ type = "constant", value = [0.6, 0.5, 0.4] }}
+
+[bsdf.lamp]
+type = "lambertian"
+albedo = {{ type = "constant", value = [0.3, 0.3, 0.3] }}
+
+[bsdf.jade]
+type = "principled_bsdf"
+basecolor = {{ type = "constant", value = [0.3, 0.7, 0.4] }}
+roughness = {{ type = "constant", value = 0.3 }}
+
+[bssrdf.jade]
+albedo = {{ type = "constant", value = [0.5, 0.9, 0.6] }}
+radius = [0.2, 0.3, 0.15]
+anisotropy = 0.1
+ior = 1.5
+rfr_entry_prob = 0.25
+
+[material.floor]
+bsdf = "bsdf.floor"
+
+[material.lamp]
+bsdf = "bsdf.lamp"
+emission = [17.0, 12.0, 4.0]
+
+[material.jade]
+bsdf = "bsdf.jade"
+subsurface = "bssrdf.jade"
+
+[mesh_asset.trio]
+type = "inline"
+geometry = [
+  {{ vertices = [[-1, 0, -1], [1, 0, -1], [1, 0, 1], [-1, 0, 1]], indices = [[0, 2, 1], [0, 3, 2]] }},
+  {{ vertices = [[-0.3, 1.5, -0.3], [0.3, 1.5, -0.3], [0.3, 1.5, 0.3], [-0.3, 1.5, 0.3]], indices = [[0, 1, 2], [0, 2, 3]] }},
+  {{ vertices = [[-0.25, 0.01, -0.25], [0.25, 0.01, -0.25], [0.0, 0.01, 0.25], [0.0, 0.5, 0.0]], indices = [[0, 2, 1], [0, 1, 3], [1, 2, 3], [2, 0, 3]] }},
+]
+
+[[task]]
+type = "small_pt_b200"
+object = "mesh_asset.trio"
+material = [["material.floor", "material.lamp", "material.jade"]]
+sky = {{ ambient = [0.1, 0.2, 0.3] }}
+bounces = 5
+clamp_indirect = 0.0
+render_width = 40
+render_height = 32
+spp = 8
+spp_prog_interval = 8
+camera = {{ type = "perspective", to_world = {{ matrix_rm = {c2w} }}, vfov = 45.0, aspect = 1.25 }}
+"""
+    ks.config_run(doc, str(tmp_path))
+    img = ks.load_image(tmp_path / "task_0" / "small_pt_spp8.exr")
+
+    def mat(**kw):
+        m = ks.MaterialDesc()
+        m.basecolor[:] = kw.pop("basecolor")
+        m.roughness, m.ior, m.specular_r0_mul, m.diffuse_trans_fwd = 1.0, 1.5, 0.5, 0.5
+        for k, v in kw.items():
+            setattr(m, k, v)
+        return m
+    mats = [mat(basecolor=(0.6, 0.5, 0.4), bsdf=2), mat(basecolor=(0.3, 0.3, 0.3), bsdf=2, has_emission=1),
+            mat(basecolor=(0.3, 0.7, 0.4), roughness=0.3, has_subsurface=1, ss_anisotropy=0.1,
+                ss_ior=1.5, ss_rfr_entry_prob=0.25)]
+    mats[1].emission[:] = (17.0, 12.0, 4.0)
+    mats[2].ss_albedo[:] = (0.5, 0.9, 0.6)
+    mats[2].ss_radius[:] = (0.2, 0.3, 0.15)
+    meshes = [(np.array([[-1, 0, -1], [1, 0, -1], [1, 0, 1], [-1, 0, 1]], np.float32), np.array([[0, 2, 1], [0, 3, 2]]), 0),
+              (np.array([[-0.3, 1.5, -0.3], [0.3, 1.5, -0.3], [0.3, 1.5, 0.3], [-0.3, 1.5, 0.3]], np.float32),
+               np.array([[0, 1, 2], [0, 2, 3]]), 1),
+              (np.array([[-0.25, 0.01, -0.25], [0.25, 0.01, -0.25], [0.0, 0.01, 0.25], [0.0, 0.5, 0.0]], np.float32),
+               np.array([[0, 2, 1], [0, 1, 3], [1, 2, 3], [2, 0, 3]]), 2)]
+    sky = ks.SkyDesc()
+    sky.kind = 1
+    sky.ambient[:] = (0.1, 0.2, 0.3)
+    desc, keep = ks.scene_desc(meshes, mats, sky)
+    s = ks.Scene(ctx, desc, keep)
+    s.build_bvh()
+    vfov = np.float32(45.0) / np.float32(180.0) * np.float32(np.pi)
+    cam = ks.camera_perspective(np.array(c2w, np.float32), float(vfov), 1.25)
+    p = ks.SmallPTParams.make(render_width=40, render_height=32, spp=8, bounces=5, clamp_indirect=0.0,
+                              spp_prog_interval=8)
+    ref = composite(*s.render(cam, p)).astype(np.float32)
+    s.close()
+    assert ref.mean() > 0.0
+    assert np.array_equal(img, ref)
