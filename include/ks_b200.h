@@ -313,10 +313,10 @@ ks_status ks_trace_rays_wide(ks_scene *scene, const float *rays, uint32_t n, int
  * 3.4 MB, resident on every GPU that loads the library until the process exits); larger n is
  * rejected with KS_ERR_INVALID_ARGUMENT.  Each call returns once the results are in the caller's
  * host arrays.  The first call on a device looks up that array's device address
- * (cudaGetSymbolAddress) and keeps it for the life of the process: make that first call before
- * any stream capture begins, and do not reset the device (cudaDeviceReset) between calls, which
- * would leave the kept address stale.  All calls share the array, so calls that overlap on the
- * GPU (two contexts on one device, two threads) race; serialise them. */
+ * (cudaGetSymbolAddress) and keeps it for the life of the process; do not reset the device
+ * (cudaDeviceReset) between calls, which would leave the kept address stale.  All calls share the
+ * array, so calls that overlap on the GPU (two contexts on one device, two threads) race;
+ * serialise them. */
 #define KS_TRACE_NOALLOC_MAX_RAYS 65536
 ks_status ks_trace_rays_noalloc(ks_scene *scene, const float *rays, uint32_t n, int any_hit, int culling,
                                 uint32_t *tri_idx, float *t, float *bary);
