@@ -56,22 +56,20 @@ struct GridParams
 
 __host__ __device__ inline uint32_t level_res(const GridParams &g, int l) { return g.res[l]; }
 
-// Grid cell corner -> table entry.  Corners are grouped in 2 x 2 x 2 blocks of 8 consecutive
-// entries (a block of 4-byte FP16 feature pairs is one 32-byte L2 sector), so the 8 corners of a
-// cell fall into 3.4 blocks on average instead of 8 sectors.  Blocks are indexed densely while
-// a level's blocks fit the table, else by the spatial hash of Teschner et al. with the primes
-// used by instant-ngp, applied to the block coordinates.
+// Grid cell corner -> table entry.  While a level's corners fit the table they are stored in
+// 2 x 2 x 2 blocks of 8 consecutive entries (a block of 4-byte FP16 feature pairs is one 32-byte L2
+// sector, so a cell's 8 corners fall into 3.4 blocks on average instead of 8 sectors); finer levels
+// hash each corner with the spatial hash of Teschner et al. and the primes of instant-ngp (corners
+// collide independently, which keeps the trilinear blend of a cell from taking all 8 corners from one
+// colliding block).
 __host__ __device__ __forceinline__ uint32_t grid_index(uint32_t res, uint32_t x, uint32_t y, uint32_t z)
 {
-    const uint32_t inner = (x & 1u) | ((y & 1u) << 1) | ((z & 1u) << 2);
-    const uint32_t bx = x >> 1, by = y >> 1, bz = z >> 1;
     const uint64_t side = ((uint64_t)res + 2) >> 1; // blocks per axis over corners 0..res
-    uint32_t block;
-    if (side * side * side * 8 <= kTableSize)
-        block = (uint32_t)(bx + side * (by + side * bz));
-    else
-        block = (bx * 1u ^ by * 2654435761u ^ bz * 805459861u) & (kTableSize / 8u - 1u);
-    return block * 8u + inner;
+    if (side * side * side * 8 <= kTableSize) {
+        const uint32_t inner = (x & 1u) | ((y & 1u) << 1) | ((z & 1u) << 2);
+        return (uint32_t)((x >> 1) + side * ((y >> 1) + side * (z >> 1))) * 8u + inner;
+    }
+    return (x * 1u ^ y * 2654435761u ^ z * 805459861u) & (kTableSize - 1u);
 }
 
 struct Corner

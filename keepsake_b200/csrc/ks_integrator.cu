@@ -276,13 +276,10 @@ __global__ void __launch_bounds__(128) k_extend(const __grid_constant__ SceneVie
 // paths into the hit and miss queues in index order, so that shading reads the path state in
 // order.  kBatch: paths of many jobs, the count read from the batch state.
 // kAlpha: the scene has opacity maps; candidate hits go through their stochastic test (SceneAlpha).
-// order / n_order: the rays are fetched as order[0 .. n_order) (the continuing paths sorted by
-// k_ray_scatter), then n_order .. count in slot order (the new camera rays); null: slot order.
 template <bool kBatch = false, bool kAlpha = false>
 __global__ void __launch_bounds__(128, KS_TRAV_MIN_BLOCKS) k_extend_pt(const __grid_constant__ SceneView sv_in, PathBuf pb, uint32_t count,
                                                    float4 *hits, uint32_t *fetch, int *overflow,
-                                                   unsigned long long *work, BatchView bv,
-                                                   const uint32_t *order = nullptr, uint32_t n_order = 0)
+                                                   unsigned long long *work, BatchView bv)
 {
     if constexpr (kBatch)
         count = bv.state->count;
@@ -295,9 +292,7 @@ __global__ void __launch_bounds__(128, KS_TRAV_MIN_BLOCKS) k_extend_pt(const __g
     bool drained = false;
     int of = 0;
     while (true) {
-        uint32_t id = warp_fetch(fetch, count, ray == ~0u, drained);
-        if (id != ~0u && id < n_order)
-            id = order[id];
+        const uint32_t id = warp_fetch(fetch, count, ray == ~0u, drained);
         if (id != ~0u) {
             const uint32_t job = kBatch ? (bits(pb.beta_pix[id].w) >> kJobShift) : 0u;
             const SceneView &sv = job_of<kBatch>(sv_in, bv.views, job);
@@ -338,89 +333,6 @@ __global__ void __launch_bounds__(128, KS_TRAV_MIN_BLOCKS) k_extend_pt(const __g
     if (of)
         atomicOr(overflow, 1);
     flush_counts(tc, work);
-}
-
-// Ray order of an extension wave: the continuing paths grouped by the octant of their direction
-// and the cell of their origin in a 16^3 grid over the scene bound (cells in Morton order), so that
-// the rays a warp fetches together descend the same parts of the tree.  A counting sort: keys and a
-// histogram (lanes with equal keys add once), an exclusive scan of the bins, a scatter.  Only the
-// order in which rays are traversed changes; every ray's hit is the same.
-constexpr int kSortCellBits = 4;
-constexpr uint32_t kSortBins = 8u << (3 * kSortCellBits);
-#ifndef KS_SORT_MIN_RAYS
-#define KS_SORT_MIN_RAYS (1u << 16)
-#endif
-constexpr uint32_t kSortMinRays = KS_SORT_MIN_RAYS; // smaller waves keep their slot order
-
-KS_D uint32_t spread3_4(uint32_t x)
-{
-    x &= 0xfu;
-    return (x & 1u) | ((x & 2u) << 2) | ((x & 4u) << 4) | ((x & 8u) << 6);
-}
-
-__global__ void __launch_bounds__(256) k_ray_keys(PathBuf pb, uint32_t n, float3 bmin, float3 scale, uint32_t *keys,
-                                                  uint32_t *bins)
-{
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = i < n;
-    const uint32_t active = __ballot_sync(0xffffffffu, valid);
-    if (!valid)
-        return;
-    const float4 o = pb.o_pdf[i], d = pb.d_info[i];
-    auto cell = [](float v, float lo, float sc) {
-        const float c = (v - lo) * sc;
-        return c <= 0.0f ? 0u : (c >= 15.0f ? 15u : (uint32_t)c);
-    };
-    const uint32_t oct = (d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u);
-    const uint32_t key = (oct << (3 * kSortCellBits)) | spread3_4(cell(o.x, bmin.x, scale.x)) |
-                         (spread3_4(cell(o.y, bmin.y, scale.y)) << 1) | (spread3_4(cell(o.z, bmin.z, scale.z)) << 2);
-    keys[i] = key;
-    const uint32_t same = __match_any_sync(active, key);
-    if ((threadIdx.x & 31) == (uint32_t)(__ffs(same) - 1))
-        atomicAdd(&bins[key], (uint32_t)__popc(same));
-}
-
-// Exclusive prefix sum of the kSortBins counts, in place (one block of 1024 threads).
-__global__ void __launch_bounds__(1024) k_bin_scan(uint32_t *bins)
-{
-    constexpr uint32_t kPer = kSortBins / 1024;
-    __shared__ uint32_t part[1024];
-    uint32_t local[kPer], sum = 0;
-    for (uint32_t k = 0; k < kPer; ++k) {
-        local[k] = bins[threadIdx.x * kPer + k];
-        sum += local[k];
-    }
-    part[threadIdx.x] = sum;
-    __syncthreads();
-    for (uint32_t off = 1; off < 1024; off <<= 1) {
-        const uint32_t v = threadIdx.x >= off ? part[threadIdx.x - off] : 0u;
-        __syncthreads();
-        part[threadIdx.x] += v;
-        __syncthreads();
-    }
-    uint32_t run = part[threadIdx.x] - sum;
-    for (uint32_t k = 0; k < kPer; ++k) {
-        bins[threadIdx.x * kPer + k] = run;
-        run += local[k];
-    }
-}
-
-__global__ void __launch_bounds__(256) k_ray_scatter(const uint32_t *keys, uint32_t n, uint32_t *offsets,
-                                                     uint32_t *order)
-{
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = i < n;
-    const uint32_t active = __ballot_sync(0xffffffffu, valid);
-    if (!valid)
-        return;
-    const uint32_t key = keys[i];
-    const uint32_t same = __match_any_sync(active, key);
-    const uint32_t lane = threadIdx.x & 31, leader = (uint32_t)(__ffs(same) - 1);
-    uint32_t base = 0;
-    if (lane == leader)
-        base = atomicAdd(&offsets[key], (uint32_t)__popc(same));
-    base = __shfl_sync(same, base, leader);
-    order[base + __popc(same & ((1u << lane) - 1u))] = i;
 }
 
 // Hit and miss queues from the per-ray results of k_extend_pt, one CTA-aggregated append per
@@ -783,7 +695,6 @@ struct RenderWork
     DevBuf<uint32_t> queue[2]; // hit / miss path indices
     DevBuf<int> overflow;
     DevBuf<float> filter; // the pixel filter's sample table (Gaussian / Blackman-Harris)
-    DevBuf<uint32_t> sort_keys, sort_order, sort_bins; // ray order of the extension waves
     uint32_t capacity = 0;
 };
 
@@ -1019,9 +930,6 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
     }
     KS_CUDA_TRY(ctx, w.queue[0].reserve(w.capacity));
     KS_CUDA_TRY(ctx, w.queue[1].reserve(w.capacity));
-    KS_CUDA_TRY(ctx, w.sort_keys.reserve(w.capacity));
-    KS_CUDA_TRY(ctx, w.sort_order.reserve(w.capacity));
-    KS_CUDA_TRY(ctx, w.sort_bins.reserve(kSortBins));
     for (int f = 0; f < 4; ++f)
         KS_CUDA_TRY(ctx, w.shadow[f].reserve(w.capacity));
     KS_CUDA_TRY(ctx, w.counters.reserve(kCounters));
@@ -1163,30 +1071,13 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
                                                       w.queue[1].ptr, w.counters.ptr + 2, w.overflow.ptr, work.ptr,
                                                       BatchView{});
             else {
-                // the continuing paths in coherent order (new camera rays keep their pixel order)
-                const uint32_t n_order = cur_count >= kSortMinRays ? cur_count : 0u;
-                if (n_order) {
-                    const float3 lo = make_float3(sv.bmin[0], sv.bmin[1], sv.bmin[2]);
-                    auto sc = [](float a, float b) { return b > a ? 16.0f / (b - a) : 0.0f; };
-                    const float3 scale = make_float3(sc(sv.bmin[0], sv.bmax[0]), sc(sv.bmin[1], sv.bmax[1]),
-                                                     sc(sv.bmin[2], sv.bmax[2]));
-                    cudaMemsetAsync(w.sort_bins.ptr, 0, sizeof(uint32_t) * kSortBins, st);
-                    k_ray_keys<<<(n_order + 255) / 256, 256, 0, st>>>(pb[cur], n_order, lo, scale, w.sort_keys.ptr,
-                                                                     w.sort_bins.ptr);
-                    k_bin_scan<<<1, 1024, 0, st>>>(w.sort_bins.ptr);
-                    k_ray_scatter<<<(n_order + 255) / 256, 256, 0, st>>>(w.sort_keys.ptr, n_order, w.sort_bins.ptr,
-                                                                        w.sort_order.ptr);
-                    stats.kernel_launches += 3;
-                }
                 if (alpha)
                     k_extend_pt<false, true><<<std::min(grid, ext_grid), 128, 0, st>>>(
-                        sv, pb[cur], count, w.hits.ptr, w.counters.ptr + 4, w.overflow.ptr, work.ptr, BatchView{},
-                        w.sort_order.ptr, n_order);
+                        sv, pb[cur], count, w.hits.ptr, w.counters.ptr + 4, w.overflow.ptr, work.ptr, BatchView{});
                 else
                     k_extend_pt<false><<<std::min(grid, ext_grid), 128, 0, st>>>(sv, pb[cur], count, w.hits.ptr,
                                                                                  w.counters.ptr + 4, w.overflow.ptr,
-                                                                                 work.ptr, BatchView{},
-                                                                                 w.sort_order.ptr, n_order);
+                                                                                 work.ptr, BatchView{});
                 k_build_queues<false><<<std::min((count + 255) / 256, max_grid), 256, 0, st>>>(
                     w.hits.ptr, count, w.queue[0].ptr, w.queue[1].ptr, w.counters.ptr + 2, BatchView{});
                 stats.kernel_launches++;

@@ -66,8 +66,8 @@ def corners(pos, bmin, bmax, res, table_size):
         f0 = np.minimum(np.floor(p), np.float32(r - 1)).astype(np.float32)
         t = (p - f0).astype(np.float32)
         i0 = f0.astype(np.uint64)
-        # corners grouped in 2 x 2 x 2 blocks of 8 consecutive entries; blocks indexed densely while
-        # they fit, else hashed (32-bit products, as the device computes them)
+        # while the level fits: corners in 2 x 2 x 2 blocks of 8 consecutive entries, blocks indexed
+        # densely; finer levels: each corner hashed
         side = (r + 2) >> 1
         dense = side ** 3 * 8 <= table_size
         idx = np.empty((len(pos), 8), np.int64)
@@ -75,16 +75,15 @@ def corners(pos, bmin, bmax, res, table_size):
         for k in range(8):
             d = np.array([k & 1, (k >> 1) & 1, (k >> 2) & 1], np.uint64)
             c = i0 + d
-            inner = (c[:, 0] & 1) | ((c[:, 1] & 1) << 1) | ((c[:, 2] & 1) << 2)
-            b = c >> np.uint64(1)
             if dense:
+                inner = (c[:, 0] & 1) | ((c[:, 1] & 1) << 1) | ((c[:, 2] & 1) << 2)
+                b = c >> np.uint64(1)
                 blk = b[:, 0] + np.uint64(side) * (b[:, 1] + np.uint64(side) * b[:, 2])
+                idx[:, k] = (blk * np.uint64(8) + inner).astype(np.int64)
             else:
-                m32 = np.uint64(0xFFFFFFFF)
-                h = ((b[:, 0] * np.uint64(PRIMES[0])) & m32) ^ ((b[:, 1] * np.uint64(PRIMES[1])) & m32) ^ \
-                    ((b[:, 2] * np.uint64(PRIMES[2])) & m32)
-                blk = h & np.uint64(table_size // 8 - 1)
-            idx[:, k] = (blk * np.uint64(8) + inner).astype(np.int64)
+                h = (c[:, 0] * np.uint64(PRIMES[0])) ^ (c[:, 1] * np.uint64(PRIMES[1])) ^ \
+                    (c[:, 2] * np.uint64(PRIMES[2]))
+                idx[:, k] = (h & np.uint64(table_size - 1)).astype(np.int64)
             wk = np.ones(len(pos), np.float32)
             for a in range(3):
                 wk = (wk * np.where(d[a] == 1, t[:, a], np.float32(1) - t[:, a])).astype(np.float32)
