@@ -72,6 +72,8 @@ def parse():
     ap.add_argument("--profile-guided", action="store_true",
                     help="profiling case only: one guided render of the glossy occluded scene at --res x "
                          "(--res * 9 / 16), --spp samples (default 16), then exit")
+    ap.add_argument("--profile-unguided", action="store_true",
+                    help="with --profile-guided: the same render without the guide")
     ap.add_argument("--c5-spp", type=int, default=1024)
     # reduced frames of the same scene, for profiling captures only (not a bench line)
     ap.add_argument("--spp", type=int, default=None)
@@ -602,8 +604,12 @@ def main():
         acc = torch.zeros((H, W, 3), dtype=torch.float64, device="cuda")
         wts = torch.zeros((H, W, 2), dtype=torch.float64, device="cuda")
         cam = ks.camera_perspective(gg.camera_to_world, gg.vfov, gg.aspect)
-        sc.render_guided_device(cam, pp, guide, opts, acc.data_ptr(), wts.data_ptr())
-        print(json.dumps({"profile_case": "guided", "resolution": [W, H], "stats": sc.stats().as_dict()}))
+        if args.profile_unguided:
+            sc.render_device(cam, pp, acc.data_ptr(), wts.data_ptr())
+        else:
+            sc.render_guided_device(cam, pp, guide, opts, acc.data_ptr(), wts.data_ptr())
+        print(json.dumps({"profile_case": "unguided" if args.profile_unguided else "guided", "resolution": [W, H],
+                          "stats": sc.stats().as_dict()}))
         guide.close()
         sc.close()
         ctx.close()
