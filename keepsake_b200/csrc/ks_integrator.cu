@@ -696,6 +696,15 @@ struct RenderWork
     DevBuf<int> overflow;
     DevBuf<float> filter; // the pixel filter's sample table (Gaussian / Blackman-Harris)
     uint32_t capacity = 0;
+    uint32_t *h_counts = nullptr; // pinned: the loop's path counts read back each iteration
+    RenderWork() = default;
+    RenderWork(const RenderWork &) = delete;
+    RenderWork &operator=(const RenderWork &) = delete;
+    ~RenderWork()
+    {
+        if (h_counts)
+            cudaFreeHost(h_counts);
+    }
 };
 
 // Buffers of the single-job renders kept by the context between calls: allocating and freeing the
@@ -984,8 +993,11 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
         gv.rec_threshold = (uint32_t)std::min(65536.0, std::ceil(65536.0 * 2.0 * go.max_records / per_pass));
     }
     ShadowBuf sb{w.shadow[0].ptr, w.shadow[1].ptr, w.shadow[2].ptr, w.shadow[3].ptr};
-    uint32_t *h_counts = nullptr;
-    KS_CUDA_TRY(ctx, cudaMallocHost((void **)&h_counts, sizeof(uint32_t) * 3));
+    // kept with the wavefront buffers: a pinned allocation and free per render cost milliseconds,
+    // now and then far more
+    if (!w.h_counts)
+        KS_CUDA_TRY(ctx, cudaMallocHost((void **)&w.h_counts, sizeof(uint32_t) * 4));
+    uint32_t *h_counts = w.h_counts;
     h_counts[2] = 0;
     // guided renders: the guide's filter and inference run on a second stream, overlapping the
     // sampling and the miss shading, and join before the hit shading
@@ -1236,7 +1248,6 @@ static ks_status render_impl(ks_scene *scene, const ks_camera_desc *cam, const k
     int overflow = 0;
     if (err == cudaSuccess)
         err = cudaMemcpy(&overflow, w.overflow.ptr, sizeof(int), cudaMemcpyDeviceToHost);
-    cudaFreeHost(h_counts);
     unsigned long long h_work[4] = {0, 0, 0, 0};
     if (err == cudaSuccess)
         err = cudaMemcpy(h_work, work.ptr, sizeof(h_work), cudaMemcpyDeviceToHost);
