@@ -77,6 +77,15 @@ ks_status ks_sobol_points(ks_context *ctx, uint32_t full_width, uint32_t full_he
                           uint32_t x0, uint32_t y0, uint32_t nx, uint32_t ny, uint32_t s0, uint32_t ns, uint32_t nd,
                           float *out);
 
+/* Sobol parity hook for the renderer's per-bounce draw.  For every pixel and sample index of the
+ * window above it starts the sampler at dimension dim and writes the seven values one path vertex
+ * draws, in the order next(), next2d(), next(), next2d(), next() (light selection, light uv, BSDF
+ * lobe, BSDF direction, roulette: nee.cpp:28-34, material.cpp:157-158, small_pt.cpp:168-174),
+ * through the same code as the sampling kernel.  Layout: out[((py * nx + px) * ns + s) * 7 + c]. */
+ks_status ks_sobol_bounce(ks_context *ctx, uint32_t full_width, uint32_t full_height, uint32_t spp, uint32_t seed,
+                          uint32_t x0, uint32_t y0, uint32_t nx, uint32_t ny, uint32_t s0, uint32_t ns, uint32_t dim,
+                          float *out);
+
 /* ---------------------------------------------------------------------------------------------
  * Scene description (host arrays; ks_scene_create copies everything it needs to the device).
  * One mesh = one reference `MeshGeometry` with one `Material` (scene.cpp:315-336 pairs

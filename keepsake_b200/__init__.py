@@ -44,6 +44,8 @@ lib.ks_last_error.argtypes = [_vp]
 lib.ks_last_error.restype = ctypes.c_char_p
 lib.ks_sobol_points.argtypes = [_vp] + [_u32] * 11 + [_vp]
 lib.ks_sobol_points.restype = ctypes.c_int
+lib.ks_sobol_bounce.argtypes = [_vp] + [_u32] * 11 + [_vp]
+lib.ks_sobol_bounce.restype = ctypes.c_int
 
 
 class KsError(RuntimeError):
@@ -143,6 +145,13 @@ class Context:
         out = np.empty((ny, nx, ns, nd, 3), dtype=np.float32)
         st = lib.ks_sobol_points(self.handle, full_w, full_h, spp, seed, x0, y0, nx, ny, s0, ns, nd, ptr(out))
         self.check(st, "ks_sobol_points")
+        return out
+
+    def sobol_bounce(self, full_w, full_h, spp, seed, x0, y0, nx, ny, s0, ns, dim) -> np.ndarray:
+        """The seven values one path vertex draws from dimension dim (the sampling kernel's code)."""
+        out = np.empty((ny, nx, ns, 7), dtype=np.float32)
+        st = lib.ks_sobol_bounce(self.handle, full_w, full_h, spp, seed, x0, y0, nx, ny, s0, ns, dim, ptr(out))
+        self.check(st, "ks_sobol_bounce")
         return out
 
 

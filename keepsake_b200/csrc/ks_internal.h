@@ -4,8 +4,46 @@
 #include "../../include/ks_b200.h"
 
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <memory>
 #include <string>
+#include <system_error>
+#include <thread>
+#include <vector>
+
+// Page-locked host memory a context keeps between calls (grow-only), held by one call at a time:
+// the host side of large uploads.  Fresh host vectors pay a page fault per 4 KB on first touch and
+// pageable copies go through the driver's own staging, which together cost more than the copy.
+struct KsPinned
+{
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    bool busy = false;
+    KsPinned() = default;
+    KsPinned(const KsPinned &) = delete;
+    KsPinned &operator=(const KsPinned &) = delete;
+    ~KsPinned() { release(); }
+    cudaError_t reserve(size_t n)
+    {
+        if (ptr && n <= bytes)
+            return cudaSuccess;
+        release();
+        cudaError_t e = cudaMallocHost(&ptr, n);
+        if (e != cudaSuccess) {
+            ptr = nullptr;
+            return e;
+        }
+        bytes = n;
+        return cudaSuccess;
+    }
+    void release()
+    {
+        if (ptr)
+            cudaFreeHost(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+};
 
 struct ks_context
 {
@@ -18,10 +56,43 @@ struct ks_context
     std::shared_ptr<void> render_cache, build_cache;
     // failure-detection limits (ks_context_set_limits; 0 = the library's own bound)
     ks_context_limits limits{};
+    // host side of ks_scene_create's uploads
+    KsPinned upload;
 };
 
 namespace ksb
 {
+
+// f(begin, end) over contiguous chunks of [0, n) on up to 8 host threads (the caller runs the first
+// chunk), for the memory-bound host passes over scene and image arrays; inline below 2 grains, or
+// when no thread can be started.
+template <class F>
+void host_parallel(size_t n, size_t grain, F &&f)
+{
+    const unsigned hw = std::thread::hardware_concurrency();
+    const size_t chunks = std::min<size_t>(std::min<unsigned>(hw ? hw : 1u, 8u), grain ? n / grain : 1);
+    if (chunks <= 1) {
+        f((size_t)0, n);
+        return;
+    }
+    const size_t step = (n + chunks - 1) / chunks;
+    std::vector<std::thread> pool;
+    size_t done = step; // [0, done) is the caller's; the rest goes to threads while they start
+    for (size_t b = step; b < n; b += step) {
+        const size_t e = std::min(n, b + step);
+        try {
+            pool.emplace_back([&f, b, e] { f(b, e); });
+            done = e;
+        } catch (const std::system_error &) {
+            break;
+        }
+    }
+    f((size_t)0, std::min(n, step));
+    if (done < n)
+        f(done, n);
+    for (auto &t : pool)
+        t.join();
+}
 
 // Records a failure on the context and returns its status.
 inline ks_status fail(ks_context *ctx, ks_status s, const std::string &msg)
@@ -49,12 +120,23 @@ inline ks_status cuda_fail(ks_context *ctx, cudaError_t e, const char *what)
                 std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+// Device memory of the library: one stream-ordered pool per GPU that keeps the blocks it is given
+// back (release threshold unlimited), so scenes, builds and renders created and destroyed in a loop
+// reuse memory instead of calling the driver's allocator each time; ks_context_destroy returns the
+// free blocks to the driver.  Both calls keep cudaMalloc / cudaFree's host-synchronous behaviour:
+// pool_alloc returns usable memory, pool_free first waits for the device (as cudaFree does), so no
+// launch still in flight can see the block handed out again.
+cudaError_t pool_alloc(void **ptr, size_t bytes);
+void pool_free(void *ptr, int device);
+void pool_trim(int device);
+
 // Device buffer owned by the caller of these helpers; freed explicitly.
 template <typename T>
 struct DevBuf
 {
     T *ptr = nullptr;
     size_t count = 0;
+    int device = 0; // the GPU whose pool the block came from
     DevBuf() = default;
     DevBuf(const DevBuf &) = delete;
     DevBuf &operator=(const DevBuf &) = delete;
@@ -69,15 +151,21 @@ struct DevBuf
     cudaError_t alloc(size_t n)
     {
         release();
-        count = n;
         if (n == 0)
             return cudaSuccess;
-        return cudaMalloc((void **)&ptr, n * sizeof(T));
+        cudaGetDevice(&device);
+        cudaError_t e = pool_alloc((void **)&ptr, n * sizeof(T));
+        if (e != cudaSuccess) {
+            ptr = nullptr;
+            return e;
+        }
+        count = n;
+        return cudaSuccess;
     }
     void release()
     {
         if (ptr)
-            cudaFree(ptr);
+            pool_free(ptr, device);
         ptr = nullptr;
         count = 0;
     }
@@ -86,6 +174,7 @@ struct DevBuf
     {
         std::swap(ptr, o.ptr);
         std::swap(count, o.count);
+        std::swap(device, o.device);
     }
 };
 

@@ -131,8 +131,13 @@ KS_HD int digit_permutation(int p, int digit)
     // 64-bit word, so the lookup stays in registers.  Bytes, permutation 0 first:
     //   E4 B4 D8 78 6C 9C E1 B1 | C9 39 2D 8D C6 36 D2 72 | 4E 1E 27 87 1B 4B 63 93
     constexpr uint64_t w0 = 0xB1E19C6C78D8B4E4ull, w1 = 0x72D236C68D2D39C9ull, w2 = 0x93634B1B87271E4Eull;
-    uint64_t w = p < 8 ? w0 : (p < 16 ? w1 : w2);
-    uint32_t byte = (uint32_t)(w >> (8 * (p & 7))) & 0xffu;
+    const uint64_t w = p < 8 ? w0 : (p < 16 ? w1 : w2);
+#ifdef __CUDA_ARCH__
+    // byte p & 7 of the word in the low byte (one byte-permute instead of a 64-bit shift)
+    const uint32_t byte = __byte_perm((uint32_t)w, (uint32_t)(w >> 32), (uint32_t)(p & 7));
+#else
+    const uint32_t byte = (uint32_t)(w >> (8 * (p & 7))) & 0xffu;
+#endif
     return (int)((byte >> (2 * digit)) & 3u);
 }
 
@@ -161,25 +166,43 @@ struct SobolSampler
     // get_sample_index (sobol.h:168-222).  The Morton index is built in 32 bits (sobol.h:145), so
     // every `higher digits` value is below 2^32 and the loop runs in 32-bit integers; only the
     // permuted index itself can exceed 32 bits (up to 2 * n_base4_digits).
-    KS_HD uint64_t sample_index() const
+    // For N dimensions at once (dim_mix[k] = 0x55555555 * dimension, a 32-bit product): one pass
+    // over the digits, whose values and higher digits do not depend on the dimension.  The digits
+    // are visited from the top, each one lands 2 bits below the previous one, so the index is
+    // built by shifting in 2 bits at a time (and the final bit of an odd log2 spp by one more).
+    template <int N>
+    KS_HD void sample_indices(const uint32_t (&dim_mix)[N], uint64_t (&out)[N]) const
     {
-        uint64_t out = 0;
         const uint32_t m = (uint32_t)morton_index;
         const bool pow2 = (log2_spp & 1) != 0;
         const int last_digit = pow2 ? 1 : 0;
-        const uint32_t dim_mix = 0x55555555u * (uint32_t)dimension;
+#pragma unroll
+        for (int k = 0; k < N; ++k)
+            out[k] = 0;
         for (int i = n_base4_digits - 1; i >= last_digit; --i) {
             int shift = 2 * i - (pow2 ? 1 : 0);
             uint32_t digit = shift >= 32 ? 0u : ((m >> shift) & 3u);
             uint32_t higher = shift + 2 >= 32 ? 0u : (m >> (shift + 2));
-            int p = digit_perm_index(higher ^ dim_mix);
-            out |= (uint64_t)digit_permutation(p, (int)digit) << shift;
+#pragma unroll
+            for (int k = 0; k < N; ++k)
+                out[k] = (out[k] << 2) |
+                         (uint64_t)digit_permutation(digit_perm_index(higher ^ dim_mix[k]), (int)digit);
         }
         if (pow2) {
             uint32_t digit = m & 1u;
-            out |= (uint64_t)(digit ^ (uint32_t)(mix_bits64((uint64_t)((m >> 1) ^ dim_mix)) & 1u));
+#pragma unroll
+            for (int k = 0; k < N; ++k)
+                out[k] = (out[k] << 1) |
+                         (uint64_t)(digit ^ (uint32_t)(mix_bits64((uint64_t)((m >> 1) ^ dim_mix[k])) & 1u));
         }
-        return out;
+    }
+
+    KS_HD uint64_t sample_index() const
+    {
+        const uint32_t dim_mix[1] = {0x55555555u * (uint32_t)dimension};
+        uint64_t out[1];
+        sample_indices<1>(dim_mix, out);
+        return out[0];
     }
 
     KS_HD float next()
@@ -197,6 +220,28 @@ struct SobolSampler
         uint64_t bits = murmur64a_2x32((uint32_t)dimension, seed);
         u0 = sobol_sample_01(a, 0, (uint32_t)bits);
         u1 = sobol_sample_01(a, 1, (uint32_t)(bits >> 32));
+    }
+
+    // The seven values of one bounce, equal to next(), next2d(), next(), next2d(), next() in turn
+    // (light selection, light uv, BSDF lobe, BSDF direction, roulette: nee.cpp:28-34,
+    // material.cpp:157-158, small_pt.cpp:168-174), with the five permuted indices from one pass.
+    KS_HD void bounce_values(float (&u)[7])
+    {
+        const uint32_t d = (uint32_t)dimension;
+        const uint32_t mix[5] = {0x55555555u * d, 0x55555555u * (d + 1), 0x55555555u * (d + 3),
+                                 0x55555555u * (d + 4), 0x55555555u * (d + 6)};
+        uint64_t a[5];
+        sample_indices<5>(mix, a);
+        u[0] = sobol_sample_01(a[0], 0, (uint32_t)murmur64a_2x32(d + 1, seed));
+        uint64_t h = murmur64a_2x32(d + 3, seed);
+        u[1] = sobol_sample_01(a[1], 0, (uint32_t)h);
+        u[2] = sobol_sample_01(a[1], 1, (uint32_t)(h >> 32));
+        u[3] = sobol_sample_01(a[2], 0, (uint32_t)murmur64a_2x32(d + 4, seed));
+        h = murmur64a_2x32(d + 6, seed);
+        u[4] = sobol_sample_01(a[3], 0, (uint32_t)h);
+        u[5] = sobol_sample_01(a[3], 1, (uint32_t)(h >> 32));
+        u[6] = sobol_sample_01(a[4], 0, (uint32_t)murmur64a_2x32(d + 7, seed));
+        dimension += 7;
     }
 };
 

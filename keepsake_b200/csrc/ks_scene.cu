@@ -3,6 +3,7 @@
 #include "ks_scene.h"
 #include "ks_traverse.cuh"
 
+#include <atomic>
 #include <cmath>
 
 #include <cstring>
@@ -360,6 +361,42 @@ bool ksb::material_to_gpu(const ks_material_desc &m, MaterialGPU &g)
     return true;
 }
 
+namespace
+{
+// Mesh index of every triangle from the meshes' first-triangle offsets (offset[0] = 0, strictly
+// increasing: meshes are not empty).
+__global__ void k_tri_mesh(const uint32_t *offset, uint32_t n_meshes, uint32_t n_tris, uint32_t *tri_mesh)
+{
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n_tris; t += gridDim.x * blockDim.x) {
+        uint32_t lo = 0, hi = n_meshes;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) / 2;
+            if (offset[mid] <= t)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        tri_mesh[t] = lo;
+    }
+}
+
+// Holds the context's pinned upload memory for a scope.
+struct KsPinnedLease
+{
+    bool *flag;
+    explicit KsPinnedLease(bool *f) : flag(f)
+    {
+        if (flag)
+            *flag = true;
+    }
+    ~KsPinnedLease()
+    {
+        if (flag)
+            *flag = false;
+    }
+};
+} // namespace
+
 extern "C" {
 
 // Validates the prototypes and instances and keeps them on the host (with inverse transforms).
@@ -450,10 +487,17 @@ ks_status ks_scene_create(ks_context *ctx, const ks_scene_desc *desc, ks_scene *
             return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_create: empty mesh " + std::to_string(m));
         if (md.material >= desc->n_materials)
             return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_create: material index out of range");
-        for (uint64_t k = 0; k < 3ull * md.n_triangles; ++k)
-            if (md.indices[k] >= md.n_vertices)
-                return fail(ctx, KS_ERR_INVALID_ARGUMENT,
-                            "ks_scene_create: vertex index out of range in mesh " + std::to_string(m));
+        std::atomic<bool> bad_index{false};
+        host_parallel(3ull * md.n_triangles, 1u << 20, [&](size_t b, size_t e) {
+            bool bad = false;
+            for (size_t k = b; k < e; ++k)
+                bad |= md.indices[k] >= md.n_vertices;
+            if (bad)
+                bad_index.store(true, std::memory_order_relaxed);
+        });
+        if (bad_index.load())
+            return fail(ctx, KS_ERR_INVALID_ARGUMENT,
+                        "ks_scene_create: vertex index out of range in mesh " + std::to_string(m));
         n_tris += md.n_triangles;
         n_verts += md.n_vertices;
     }
@@ -495,8 +539,15 @@ ks_status ks_scene_create(ks_context *ctx, const ks_scene_desc *desc, ks_scene *
     s->ctx = ctx;
     s->n_tris = (uint32_t)n_tris;
     s->n_verts = (uint32_t)n_verts;
-    std::vector<float> verts(3 * n_verts);
-    std::vector<uint32_t> idx(3 * n_tris), tri_mesh(n_tris);
+    // sky (checked before the uploads are laid out: the map is one of them)
+    const ks_sky_desc &sd = desc->sky;
+    if (sd.kind < 0 || sd.kind > 3 || (sd.kind >= 2 && (!sd.map_rgb || sd.width == 0 || sd.height == 0)) ||
+        (sd.kind == 3 && (sd.width != sd.height || (sd.width & (sd.width - 1)) != 0 || sd.width > (1u << 14)))) {
+        delete s;
+        return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_create: bad sky description (an equal-area map is a "
+                                                  "square of a power-of-two side, at most 16384)");
+    }
+    const size_t n_sky = sd.kind >= 2 ? 3 * (size_t)sd.width * sd.height : 0;
     // per-vertex shading attributes: only meshes that shade smooth contribute normals (a mesh with
     // use_smooth_normal off or no vertex normals shades flat, geometry.cpp:139-141)
     bool any_smooth = false, any_uv = false;
@@ -504,23 +555,50 @@ ks_status ks_scene_create(ks_context *ctx, const ks_scene_desc *desc, ks_scene *
         any_smooth |= desc->meshes[m].use_smooth_normal && desc->meshes[m].vertex_normals;
         any_uv |= desc->meshes[m].texcoords != nullptr;
     }
-    std::vector<float> normals(any_smooth ? 3 * n_verts : 0), texcoords(any_uv ? 2 * n_verts : 0);
+    // The concatenated vertex, index, normal and texcoord arrays and the sky map are assembled in
+    // the context's pinned upload memory when it is free (else in host vectors), then copied.
+    auto align = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    const size_t off_i = align(sizeof(float) * 3 * n_verts), off_n = off_i + align(sizeof(uint32_t) * 3 * n_tris);
+    const size_t off_t = off_n + (any_smooth ? align(sizeof(float) * 3 * n_verts) : 0);
+    const size_t off_s = off_t + (any_uv ? align(sizeof(float) * 2 * n_verts) : 0);
+    const size_t stage_bytes = off_s + sizeof(float) * n_sky;
+    const bool staged = !ctx->upload.busy && ctx->upload.reserve(stage_bytes) == cudaSuccess;
+    if (!staged)
+        cudaGetLastError(); // a failed pinned allocation only means the pageable path
+    KsPinnedLease upload_lease(staged ? &ctx->upload.busy : nullptr);
+    std::vector<char> own_stage;
+    if (!staged)
+        own_stage.resize(stage_bytes);
+    char *stage = staged ? static_cast<char *>(ctx->upload.ptr) : own_stage.data();
+    float *verts = reinterpret_cast<float *>(stage);
+    uint32_t *idx = reinterpret_cast<uint32_t *>(stage + off_i);
+    float *normals = any_smooth ? reinterpret_cast<float *>(stage + off_n) : nullptr;
+    float *texcoords = any_uv ? reinterpret_cast<float *>(stage + off_t) : nullptr;
+    float *sky_map = n_sky ? reinterpret_cast<float *>(stage + off_s) : nullptr;
     uint64_t vo = 0, to = 0;
     for (uint32_t m = 0; m < desc->n_meshes; ++m) {
         const ks_mesh_desc &md = desc->meshes[m];
-        std::memcpy(&verts[3 * vo], md.vertices, sizeof(float) * 3 * md.n_vertices);
-        for (uint64_t k = 0; k < 3ull * md.n_triangles; ++k)
-            idx[3 * to + k] = (uint32_t)(md.indices[k] + vo);
-        for (uint64_t k = 0; k < md.n_triangles; ++k)
-            tri_mesh[to + k] = m;
+        const uint64_t nv = md.n_vertices, v0 = vo;
+        host_parallel(3 * nv, 1u << 20, [&](size_t b, size_t e) {
+            std::memcpy(verts + 3 * v0 + b, md.vertices + b, sizeof(float) * (e - b));
+        });
+        uint32_t *dst = idx + 3 * to;
+        host_parallel(3ull * md.n_triangles, 1u << 20, [&](size_t b, size_t e) {
+            for (size_t k = b; k < e; ++k)
+                dst[k] = (uint32_t)(md.indices[k] + v0);
+        });
         int flags = md.twosided ? kMeshTwosided : 0;
         if (md.use_smooth_normal && md.vertex_normals) {
             flags |= kMeshSmooth;
-            std::memcpy(&normals[3 * vo], md.vertex_normals, sizeof(float) * 3 * md.n_vertices);
+            std::memcpy(normals + 3 * vo, md.vertex_normals, sizeof(float) * 3 * nv);
+        } else if (normals) {
+            std::memset(normals + 3 * vo, 0, sizeof(float) * 3 * nv);
         }
         if (md.texcoords) {
             flags |= kMeshTexcoords;
-            std::memcpy(&texcoords[2 * vo], md.texcoords, sizeof(float) * 2 * md.n_vertices);
+            std::memcpy(texcoords + 2 * vo, md.texcoords, sizeof(float) * 2 * nv);
+        } else if (texcoords) {
+            std::memset(texcoords + 2 * vo, 0, sizeof(float) * 2 * nv);
         }
         s->host.mesh_tri_offset.push_back((uint32_t)to);
         s->host.mesh_material.push_back(md.material);
@@ -529,6 +607,10 @@ ks_status ks_scene_create(ks_context *ctx, const ks_scene_desc *desc, ks_scene *
         to += md.n_triangles;
     }
     s->host.mesh_tri_offset.push_back((uint32_t)to);
+    if (n_sky)
+        host_parallel(n_sky, 1u << 20, [&](size_t b, size_t e) {
+            std::memcpy(sky_map + b, sd.map_rgb + b, sizeof(float) * (e - b));
+        });
     s->host.materials.assign(desc->materials, desc->materials + desc->n_materials);
     // instancing
     if (desc->n_instances > 0) {
@@ -538,16 +620,8 @@ ks_status ks_scene_create(ks_context *ctx, const ks_scene_desc *desc, ks_scene *
             return st;
         }
     }
-    // sky
-    const ks_sky_desc &sd = desc->sky;
-    if (sd.kind < 0 || sd.kind > 3 || (sd.kind >= 2 && (!sd.map_rgb || sd.width == 0 || sd.height == 0)) ||
-        (sd.kind == 3 && (sd.width != sd.height || (sd.width & (sd.width - 1)) != 0 || sd.width > (1u << 14)))) {
-        delete s;
-        return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_create: bad sky description (an equal-area map is a "
-                                                  "square of a power-of-two side, at most 16384)");
-    }
     if (sd.kind == 3) // the alias table over the texels is built on the host
-        s->sky_host.assign(sd.map_rgb, sd.map_rgb + 3 * (size_t)sd.width * sd.height);
+        s->sky_host.assign(sky_map, sky_map + n_sky);
     s->sky_desc = sd;
     if (desc->n_lights && !desc->lights) {
         delete s;
@@ -605,7 +679,8 @@ ks_status ks_scene_create(ks_context *ctx, const ks_scene_desc *desc, ks_scene *
         s->emit_tex.info = tex_info;
         s->emit_tex.binds = binds;
         s->emit_tex.mats = mats;
-        s->emit_tex.texcoords = texcoords;
+        if (texcoords)
+            s->emit_tex.texcoords.assign(texcoords, texcoords + 2 * n_verts);
     }
     cudaError_t e = s->materials.alloc(mats.size());
     if (e == cudaSuccess)
@@ -637,35 +712,42 @@ ks_status ks_scene_create(ks_context *ctx, const ks_scene_desc *desc, ks_scene *
                                 ctx->stream);
     }
     if (e == cudaSuccess && any_smooth) {
-        e = s->normals.alloc(normals.size());
+        e = s->normals.alloc(3 * n_verts);
         if (e == cudaSuccess)
-            e = cudaMemcpyAsync(s->normals.ptr, normals.data(), s->normals.bytes(), cudaMemcpyHostToDevice,
+            e = cudaMemcpyAsync(s->normals.ptr, normals, s->normals.bytes(), cudaMemcpyHostToDevice,
                                 ctx->stream);
     }
     if (e == cudaSuccess && any_uv) {
-        e = s->texcoords.alloc(texcoords.size());
+        e = s->texcoords.alloc(2 * n_verts);
         if (e == cudaSuccess)
-            e = cudaMemcpyAsync(s->texcoords.ptr, texcoords.data(), s->texcoords.bytes(), cudaMemcpyHostToDevice,
+            e = cudaMemcpyAsync(s->texcoords.ptr, texcoords, s->texcoords.bytes(), cudaMemcpyHostToDevice,
                                 ctx->stream);
     }
+    DevBuf<uint32_t> tri_offset; // mesh_tri_offset on the device, for k_tri_mesh
     if (e == cudaSuccess)
-        e = s->verts.alloc(verts.size());
+        e = s->verts.alloc(3 * n_verts);
     if (e == cudaSuccess)
-        e = s->indices.alloc(idx.size());
+        e = s->indices.alloc(3 * n_tris);
     if (e == cudaSuccess)
-        e = s->tri_mesh.alloc(tri_mesh.size());
+        e = s->tri_mesh.alloc(n_tris);
     if (e == cudaSuccess)
-        e = cudaMemcpyAsync(s->verts.ptr, verts.data(), s->verts.bytes(), cudaMemcpyHostToDevice, ctx->stream);
+        e = tri_offset.alloc(s->host.mesh_tri_offset.size());
     if (e == cudaSuccess)
-        e = cudaMemcpyAsync(s->indices.ptr, idx.data(), s->indices.bytes(), cudaMemcpyHostToDevice, ctx->stream);
+        e = cudaMemcpyAsync(s->verts.ptr, verts, s->verts.bytes(), cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess)
-        e = cudaMemcpyAsync(s->tri_mesh.ptr, tri_mesh.data(), s->tri_mesh.bytes(), cudaMemcpyHostToDevice,
-                            ctx->stream);
-    if (e == cudaSuccess && (sd.kind == 2 || sd.kind == 3)) {
-        const size_t n = 3 * (size_t)sd.width * sd.height;
-        e = s->sky_rgb.alloc(n);
+        e = cudaMemcpyAsync(s->indices.ptr, idx, s->indices.bytes(), cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(tri_offset.ptr, s->host.mesh_tri_offset.data(), tri_offset.bytes(),
+                            cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) {
+        k_tri_mesh<<<(unsigned)std::min<uint64_t>((n_tris + 255) / 256, (uint64_t)ctx->sm_count * 16), 256, 0,
+                     ctx->stream>>>(tri_offset.ptr, desc->n_meshes, (uint32_t)n_tris, s->tri_mesh.ptr);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && n_sky) {
+        e = s->sky_rgb.alloc(n_sky);
         if (e == cudaSuccess)
-            e = cudaMemcpyAsync(s->sky_rgb.ptr, sd.map_rgb, sizeof(float) * n, cudaMemcpyHostToDevice, ctx->stream);
+            e = cudaMemcpyAsync(s->sky_rgb.ptr, sky_map, sizeof(float) * n_sky, cudaMemcpyHostToDevice, ctx->stream);
     }
     if (e == cudaSuccess)
         e = cudaStreamSynchronize(ctx->stream);

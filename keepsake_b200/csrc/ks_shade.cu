@@ -124,13 +124,9 @@ __global__ void __launch_bounds__(128) k_sample(const __grid_constant__ SceneVie
         int dim = (int)(info >> 16);
         SobolSampler smp_s = SobolSampler::start(pix % (uint32_t)rp.W, pix / (uint32_t)rp.W, smp, rp.log2_spp,
                                                  rp.n_digits, (uint32_t)rp.seed, dim);
-        float ul = smp_s.next();
-        float u0, u1;
-        smp_s.next2d(u0, u1);
-        float u_lobe = smp_s.next();
-        float b0, b1;
-        smp_s.next2d(b0, b1);
-        float u_rr = smp_s.next();
+        float uv[7];
+        smp_s.bounce_values(uv);
+        const float ul = uv[0], u0 = uv[1], u1 = uv[2], u_lobe = uv[3], b0 = uv[4], b1 = uv[5], u_rr = uv[6];
         // next_event_estimate: light selection and the light's sample (nee.cpp:28-40)
         const SceneView &sv = job_of<kBatch>(sv_in, bv.views, job);
         uint32_t light = cdf_find(sv.power_cdf, sv.light_count, clamp_u(ul));

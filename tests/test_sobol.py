@@ -63,3 +63,19 @@ def test_sobol_kernel_bit_exact(ctx, oracle, case):
     assert got.shape == want.shape
     diff = got.view(np.uint32) != want.view(np.uint32)
     assert not diff.any(), f"{diff.sum()} of {diff.size} Sobol values differ"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+def test_sobol_bounce_bit_exact(ctx, oracle, case):
+    """The sampling kernel's per-vertex draw (five permuted indices from one digit pass) equals the
+    reference's next(), next2d(), next(), next2d(), next() in turn, at the first dimension of a
+    bounce (2 + 7 b in the renderer, camera dimensions first) and at a late one."""
+    _, fw, fh, spp, seed, x0, y0, nx, ny, s0, ns, _nd = case
+    for dim in (2, 9, 2 + 7 * 11):
+        got = ctx.sobol_bounce(fw, fh, spp, seed, x0, y0, nx, ny, s0, ns, dim)
+        pts = oracle.sobol_points(fw, fh, spp, seed, x0, y0, nx, ny, s0, ns, dim + 7)
+        want = np.stack([pts[..., dim, 0], pts[..., dim + 1, 1], pts[..., dim + 1, 2], pts[..., dim + 3, 0],
+                         pts[..., dim + 4, 1], pts[..., dim + 4, 2], pts[..., dim + 6, 0]], axis=-1)
+        diff = got.view(np.uint32) != want.view(np.uint32)
+        assert not diff.any(), f"dim {dim}: {diff.sum()} of {diff.size} values differ"
