@@ -36,7 +36,10 @@ typedef struct ks_context ks_context;
  * EmbreeDevice in small_pt.cpp:182 and the TBB arena of parallel.h:93-113.)  The context keeps the
  * scratch of its SBVH builds and the buffers of its renders (wavefront state, about 300 bytes per
  * path slot up to 4 M slots, the accumulators and a pinned staging copy of them) from one call to
- * the next, and frees them in ks_context_destroy.  One thread at a time per context. */
+ * the next, and frees them in ks_context_destroy.  One thread at a time per context.
+ * Device memory comes from a pool per GPU that keeps freed blocks for reuse (a scene destroyed
+ * and a new one created reuse the same memory without the driver's allocator); ks_context_destroy
+ * returns the pool's free blocks to the driver. */
 ks_status ks_context_create(int device, ks_context **out);
 void ks_context_destroy(ks_context *ctx);
 const char *ks_status_string(ks_status s);
