@@ -1579,11 +1579,11 @@ static ks_status render_host(ks_scene *scene, const ks_camera_desc *camera, cons
     KS_CUDA_TRY(ctx, cudaMemcpyAsync(h, da.ptr, na * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     KS_CUDA_TRY(ctx, cudaMemcpyAsync(h + na, dw.ptr, nw * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     KS_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-    host_parallel(na, 1u << 18, [&](size_t b, size_t e) {
+    host_parallel(na, 1u << 17, [&](size_t b, size_t e) {
         for (size_t k = b; k < e; ++k)
             accum_rgb[k] += h[k];
     });
-    host_parallel(nw, 1u << 18, [&](size_t b, size_t e) {
+    host_parallel(nw, 1u << 17, [&](size_t b, size_t e) {
         for (size_t k = b; k < e; ++k)
             weights[k] += h[na + k];
     });

@@ -363,10 +363,16 @@ bool ksb::material_to_gpu(const ks_material_desc &m, MaterialGPU &g)
 
 namespace
 {
-// Mesh index of every triangle from the meshes' first-triangle offsets (offset[0] = 0, strictly
-// increasing: meshes are not empty).
-__global__ void k_tri_mesh(const uint32_t *offset, uint32_t n_meshes, uint32_t n_tris, uint32_t *tri_mesh)
+// Per triangle: its mesh (from the meshes' first-triangle offsets; offset[0] = 0, strictly
+// increasing: meshes are not empty), the check of its three vertex indices against the mesh's
+// vertex count, and the indices made global by the mesh's first vertex.  *bad_mesh ends as the
+// lowest mesh with an index out of range (untouched when there is none).
+// mesh_info: [0, n] first triangle, [n + 1, 2n] first vertex, [2n + 1, 3n] vertex count.
+__global__ void k_mesh_fixup(const uint32_t *mesh_info, uint32_t n_meshes, uint32_t n_tris, uint32_t *indices,
+                             uint32_t *tri_mesh, int *bad_mesh)
 {
+    const uint32_t *offset = mesh_info, *first_vert = mesh_info + n_meshes + 1,
+                   *n_verts = mesh_info + 2 * n_meshes + 1;
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n_tris; t += gridDim.x * blockDim.x) {
         uint32_t lo = 0, hi = n_meshes;
         while (hi - lo > 1) {
@@ -377,6 +383,14 @@ __global__ void k_tri_mesh(const uint32_t *offset, uint32_t n_meshes, uint32_t n
                 hi = mid;
         }
         tri_mesh[t] = lo;
+        const uint32_t nv = n_verts[lo], base = first_vert[lo];
+        uint32_t *ix = indices + 3 * (size_t)t;
+        const uint32_t a = ix[0], b = ix[1], c = ix[2];
+        if (a >= nv || b >= nv || c >= nv)
+            atomicMin(bad_mesh, (int)lo);
+        ix[0] = a + base;
+        ix[1] = b + base;
+        ix[2] = c + base;
     }
 }
 
@@ -487,17 +501,6 @@ ks_status ks_scene_create(ks_context *ctx, const ks_scene_desc *desc, ks_scene *
             return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_create: empty mesh " + std::to_string(m));
         if (md.material >= desc->n_materials)
             return fail(ctx, KS_ERR_INVALID_ARGUMENT, "ks_scene_create: material index out of range");
-        std::atomic<bool> bad_index{false};
-        host_parallel(3ull * md.n_triangles, 1u << 20, [&](size_t b, size_t e) {
-            bool bad = false;
-            for (size_t k = b; k < e; ++k)
-                bad |= md.indices[k] >= md.n_vertices;
-            if (bad)
-                bad_index.store(true, std::memory_order_relaxed);
-        });
-        if (bad_index.load())
-            return fail(ctx, KS_ERR_INVALID_ARGUMENT,
-                        "ks_scene_create: vertex index out of range in mesh " + std::to_string(m));
         n_tris += md.n_triangles;
         n_verts += md.n_vertices;
     }
@@ -579,24 +582,30 @@ ks_status ks_scene_create(ks_context *ctx, const ks_scene_desc *desc, ks_scene *
     for (uint32_t m = 0; m < desc->n_meshes; ++m) {
         const ks_mesh_desc &md = desc->meshes[m];
         const uint64_t nv = md.n_vertices, v0 = vo;
-        host_parallel(3 * nv, 1u << 20, [&](size_t b, size_t e) {
+        host_parallel(3 * nv, 1u << 17, [&](size_t b, size_t e) {
             std::memcpy(verts + 3 * v0 + b, md.vertices + b, sizeof(float) * (e - b));
         });
+        // the indices as given: k_mesh_fixup checks them and adds the mesh's first vertex
         uint32_t *dst = idx + 3 * to;
-        host_parallel(3ull * md.n_triangles, 1u << 20, [&](size_t b, size_t e) {
-            for (size_t k = b; k < e; ++k)
-                dst[k] = (uint32_t)(md.indices[k] + v0);
+        host_parallel(3ull * md.n_triangles, 1u << 17, [&](size_t b, size_t e) {
+            std::memcpy(dst + b, md.indices + b, sizeof(uint32_t) * (e - b));
         });
         int flags = md.twosided ? kMeshTwosided : 0;
         if (md.use_smooth_normal && md.vertex_normals) {
             flags |= kMeshSmooth;
-            std::memcpy(normals + 3 * vo, md.vertex_normals, sizeof(float) * 3 * nv);
+            float *dn = normals + 3 * vo;
+            host_parallel(3 * nv, 1u << 17, [&](size_t b, size_t e) {
+                std::memcpy(dn + b, md.vertex_normals + b, sizeof(float) * (e - b));
+            });
         } else if (normals) {
             std::memset(normals + 3 * vo, 0, sizeof(float) * 3 * nv);
         }
         if (md.texcoords) {
             flags |= kMeshTexcoords;
-            std::memcpy(texcoords + 2 * vo, md.texcoords, sizeof(float) * 2 * nv);
+            float *dt = texcoords + 2 * vo;
+            host_parallel(2 * nv, 1u << 17, [&](size_t b, size_t e) {
+                std::memcpy(dt + b, md.texcoords + b, sizeof(float) * (e - b));
+            });
         } else if (texcoords) {
             std::memset(texcoords + 2 * vo, 0, sizeof(float) * 2 * nv);
         }
@@ -608,7 +617,7 @@ ks_status ks_scene_create(ks_context *ctx, const ks_scene_desc *desc, ks_scene *
     }
     s->host.mesh_tri_offset.push_back((uint32_t)to);
     if (n_sky)
-        host_parallel(n_sky, 1u << 20, [&](size_t b, size_t e) {
+        host_parallel(n_sky, 1u << 17, [&](size_t b, size_t e) {
             std::memcpy(sky_map + b, sd.map_rgb + b, sizeof(float) * (e - b));
         });
     s->host.materials.assign(desc->materials, desc->materials + desc->n_materials);
@@ -723,7 +732,13 @@ ks_status ks_scene_create(ks_context *ctx, const ks_scene_desc *desc, ks_scene *
             e = cudaMemcpyAsync(s->texcoords.ptr, texcoords, s->texcoords.bytes(), cudaMemcpyHostToDevice,
                                 ctx->stream);
     }
-    DevBuf<uint32_t> tri_offset; // mesh_tri_offset on the device, for k_tri_mesh
+    DevBuf<uint32_t> mesh_info; // k_mesh_fixup's per-mesh table
+    DevBuf<int> bad_mesh;
+    std::vector<uint32_t> info(s->host.mesh_tri_offset);
+    for (uint32_t m = 0, v = 0; m < desc->n_meshes; v += desc->meshes[m].n_vertices, ++m)
+        info.push_back(v);
+    for (uint32_t m = 0; m < desc->n_meshes; ++m)
+        info.push_back(desc->meshes[m].n_vertices);
     if (e == cudaSuccess)
         e = s->verts.alloc(3 * n_verts);
     if (e == cudaSuccess)
@@ -731,17 +746,21 @@ ks_status ks_scene_create(ks_context *ctx, const ks_scene_desc *desc, ks_scene *
     if (e == cudaSuccess)
         e = s->tri_mesh.alloc(n_tris);
     if (e == cudaSuccess)
-        e = tri_offset.alloc(s->host.mesh_tri_offset.size());
+        e = mesh_info.alloc(info.size());
+    if (e == cudaSuccess)
+        e = bad_mesh.alloc(1);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(s->verts.ptr, verts, s->verts.bytes(), cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(s->indices.ptr, idx, s->indices.bytes(), cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess)
-        e = cudaMemcpyAsync(tri_offset.ptr, s->host.mesh_tri_offset.data(), tri_offset.bytes(),
-                            cudaMemcpyHostToDevice, ctx->stream);
+        e = cudaMemcpyAsync(mesh_info.ptr, info.data(), mesh_info.bytes(), cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaMemsetAsync(bad_mesh.ptr, 0x7f, sizeof(int), ctx->stream); // 0x7f7f7f7f: no mesh
     if (e == cudaSuccess) {
-        k_tri_mesh<<<(unsigned)std::min<uint64_t>((n_tris + 255) / 256, (uint64_t)ctx->sm_count * 16), 256, 0,
-                     ctx->stream>>>(tri_offset.ptr, desc->n_meshes, (uint32_t)n_tris, s->tri_mesh.ptr);
+        k_mesh_fixup<<<(unsigned)std::min<uint64_t>((n_tris + 255) / 256, (uint64_t)ctx->sm_count * 16), 256, 0,
+                       ctx->stream>>>(mesh_info.ptr, desc->n_meshes, (uint32_t)n_tris, s->indices.ptr,
+                                      s->tri_mesh.ptr, bad_mesh.ptr);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess && n_sky) {
@@ -751,9 +770,17 @@ ks_status ks_scene_create(ks_context *ctx, const ks_scene_desc *desc, ks_scene *
     }
     if (e == cudaSuccess)
         e = cudaStreamSynchronize(ctx->stream);
+    int bad = 0x7f7f7f7f;
+    if (e == cudaSuccess)
+        e = cudaMemcpy(&bad, bad_mesh.ptr, sizeof(int), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) {
         delete s;
         return cuda_fail(ctx, e, "ks_scene_create: upload");
+    }
+    if (bad != 0x7f7f7f7f) {
+        delete s;
+        return fail(ctx, KS_ERR_INVALID_ARGUMENT,
+                    "ks_scene_create: vertex index out of range in mesh " + std::to_string(bad));
     }
     *out = s;
     return KS_OK;

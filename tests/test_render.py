@@ -304,6 +304,33 @@ def test_render_errors(ctx):
 
 
 @pytest.mark.gpu
+def test_scene_create_checks_indices(ctx):
+    """A vertex index at or past its mesh's vertex count fails ks_scene_create with
+    KS_ERR_INVALID_ARGUMENT naming the lowest such mesh (the check runs on the device with the
+    index offsets); the same description with the index fixed renders as before."""
+    import keepsake_b200 as ks
+    g, cam, p = make_case(CASES["box_room"])
+    d = g.desc.contents
+    ref = ks.Scene(ctx, g.desc)
+    ref.build_bvh()
+    want = composite(*ref.render(cam, p))
+    ref.close()
+    for m in (d.n_meshes - 1, 2):
+        md = d.meshes[m]
+        ix = np.ctypeslib.as_array(ctypes.cast(md.indices, ctypes.POINTER(ctypes.c_uint32)), (3 * md.n_triangles,))
+        keep = int(ix[-1])
+        ix[-1] = md.n_vertices
+        h = ctypes.c_void_p()
+        assert ks.lib.ks_scene_create(ctx.handle, g.desc, ctypes.byref(h)) == 1
+        assert ks.lib.ks_last_error(ctx.handle).decode().endswith(f"mesh {m}")
+        ix[-1] = keep
+    s = ks.Scene(ctx, g.desc)
+    s.build_bvh()
+    assert np.array_equal(composite(*s.render(cam, p)), want)
+    s.close()
+
+
+@pytest.mark.gpu
 def test_device_progress_and_rel_mse(ctx):
     """ks_small_pt_render_device_progress stops where the callback asks; ks_image_rel_mse_device
     equals the host composite + relMSE."""
