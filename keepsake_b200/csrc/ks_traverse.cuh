@@ -396,7 +396,7 @@ KS_D int trav_interior(const TravNode *__restrict__ nodes, TravState &s, TravSta
 // Interior step of the 4-wide view (WideNode): the slots' boxes are tested with the same slab test,
 // the ray descends into the nearest hit slot (smallest entry time, then lowest slot) and the other
 // hit slots are pushed farthest first, each with its entry time (re-checked against tmax when
-// popped, as in trav_interior); any-hit queries visit them in the same order.  Returns 1 / 0 / -1 like
+// popped, as in trav_interior); any-hit queries take them in slot order.  Returns 1 / 0 / -1 like
 // trav_interior.  The set of leaves a closest-hit ray can reach is that of the binary tree (a
 // slot's slab interval lies inside its parent's: same operations, monotone rounding), so the
 // closest hit is the binary traversal's up to the order of exact ties.
@@ -436,11 +436,22 @@ KS_D int trav_wide(const WideNode *__restrict__ wide, TravState &s, TravStack &s
         overflow = 1;
         return -1;
     }
-    {
+    if constexpr (kAnyHit) {
+        // any-hit: the first slot hit next, the others pushed in slot order.  Nearest first (the
+        // network below) took 2.5 % off the bench frame's shadow rays but made a pass of the
+        // occluded glossy scene 17 % slower: shadow rays blocked by a distant occluder then search
+        // the nearby geometry's subtrees first.
+        const int f = ok[0] ? 0 : (ok[1] ? 1 : (ok[2] ? 2 : 3));
+        s.ref = f == 0 ? refs[0] : (f == 1 ? refs[1] : (f == 2 ? refs[2] : refs[3]));
+        s.cnt = f == 0 ? cnts[0] : (f == 1 ? cnts[1] : (f == 2 ? cnts[2] : cnts[3]));
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (ok[k] && k != f)
+                stack.set(s.sp++, make_uint4(refs[k], cnts[k], __float_as_uint(t0[k]), 0u));
+    } else {
         // the slots in visiting order (entry time, then slot index; the slots not hit last) by a
         // 4-input sorting network: the same instructions in every lane, where branches on the
-        // number of slots hit split the warp (measured 6 % off the closest-hit kernel; nearest
-        // first also takes 2.5 % off the any-hit one, whose slots went in slot order before)
+        // number of slots hit split the warp (measured 6 % off the closest-hit kernel)
         float kt[4];
         uint32_t kr[4], kc[4], ks[4];
 #pragma unroll
