@@ -35,7 +35,7 @@ typedef struct ks_context ks_context;
 /* Context: one CUDA device + one stream.  (Replaces the reference's implicit global state:
  * EmbreeDevice in small_pt.cpp:182 and the TBB arena of parallel.h:93-113.)  The context keeps the
  * scratch of its SBVH builds and the buffers of its renders (wavefront state, about 300 bytes per
- * path slot up to 4 M slots, the accumulators and a pinned staging copy of them) from one call to
+ * path slot up to 32 M slots, the accumulators and a pinned staging copy of them) from one call to
  * the next, and frees them in ks_context_destroy.  One thread at a time per context.
  * Device memory comes from a pool per GPU that keeps freed blocks for reuse (a scene destroyed
  * and a new one created reuse the same memory without the driver's allocator); ks_context_destroy
