@@ -304,6 +304,29 @@ def test_render_errors(ctx):
 
 
 @pytest.mark.gpu
+def test_large_wavefront_matches_split_passes(ctx):
+    """One pass of 8.4 M paths (a wavefront of that many slots, above 4 M) renders the same image as
+    the same samples in two passes of 4.2 M: every path draws the same Sobol values whatever slot
+    it has, so only the order of the FP64 sums differs (the weights, counts of paths, are exact)."""
+    import keepsake_b200 as ks
+    g = ks.Generated("icosphere", 0, level=5, sky=(256, 128), resolution=(1024, 1024))
+    cam = ks.camera_perspective(g.camera_to_world, g.vfov, g.aspect)
+    s = ks.Scene(ctx, g.desc)
+    s.build_bvh()
+    one = ks.SmallPTParams.make(render_width=1024, render_height=1024, spp=8, bounces=6, spp_prog_interval=8)
+    two = ks.SmallPTParams.make(render_width=1024, render_height=1024, spp=8, bounces=6, spp_prog_interval=4)
+    a1, w1 = s.render(cam, one)
+    st1 = s.stats()
+    a2, w2 = s.render(cam, two)
+    st2 = s.stats()
+    assert st1.paths == st2.paths == 1024 * 1024 * 8
+    assert st1.extension_rays == st2.extension_rays and st1.shadow_rays == st2.shadow_rays
+    assert np.array_equal(w1, w2)
+    np.testing.assert_allclose(a1, a2, rtol=1e-12, atol=1e-12)
+    s.close()
+
+
+@pytest.mark.gpu
 def test_scene_create_checks_indices(ctx):
     """A vertex index at or past its mesh's vertex count fails ks_scene_create with
     KS_ERR_INVALID_ARGUMENT naming the lowest such mesh (the check runs on the device with the
