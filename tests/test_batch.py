@@ -64,7 +64,7 @@ def test_batch_autotune_and_errors(ctx):
     jobs, keep = _jobs(ctx)
     desc = [(s, c, p, a.data_ptr(), w.data_ptr()) for s, c, p, a, w in jobs]
     o, ms = ks.batch_autotune(ctx, desc)
-    assert o.capacity in (1 << 20, 1 << 21, 1 << 22, 1 << 23) and o.grid_per_sm in (4, 8, 16, 32) and ms > 0
+    assert o.capacity in (1 << 21, 1 << 22, 1 << 23, 1 << 24, 1 << 25) and o.grid_per_sm in (4, 8, 16, 32) and ms > 0
     st = ks.batch_render(ctx, desc, capacity=o.capacity, grid_per_sm=o.grid_per_sm)
     assert st.paths > 0
     big = ks.SmallPTParams.make(render_width=2048, render_height=1025, spp=1, bounces=1)
